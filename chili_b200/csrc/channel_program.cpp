@@ -1,0 +1,198 @@
+// channel_program.cpp -- host builder of ChannelProgram tables from
+// ChannelDescription + Cuts (see channel_program.h).
+#include "channel_program.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <set>
+#include <sstream>
+#include <tuple>
+
+namespace {
+
+using Key = std::tuple<uint32_t, double, double>;  // ParticleInfo order (ChannelNode.cc:293-301)
+Key key_of(const chili_particle_info &p) { return Key{p.idx, p.mass, p.width}; }
+
+bool is_power2(uint32_t v) { return (v & (v - 1)) == 0; }
+
+struct Lookup {
+    std::map<uint32_t, double> smin, ptmin, etamax;
+    std::map<std::pair<int, int>, double> delta_r;
+    std::vector<double> sexternal;
+};
+
+}  // namespace
+
+std::string build_channel_programs(const chili_channel_desc *descs, int nch, const chili_cuts *cuts,
+                                   double sqrts, int n_ext, std::vector<ChannelProgram> &out) {
+    std::ostringstream err;
+    if (!descs || !cuts || nch <= 0) return "null channel descriptions or cuts";
+    if (nch > CHILI_MAX_CHANNELS) return "too many channels";
+    if (n_ext < 3 || n_ext > CHILI_MAX_EXT) return "n_ext outside [3, CHILI_MAX_EXT]";
+    const int nout = n_ext - 2;
+    if (cuts->n_sexternal != nout) return "cuts.sexternal must hold n_ext-2 entries";
+    Lookup L;
+    for (int i = 0; i < cuts->n_sexternal; ++i) L.sexternal.push_back(cuts->sexternal[i]);
+    for (int i = 0; i < cuts->n_smin; ++i) L.smin[cuts->smin[i].idx] = cuts->smin[i].value;
+    for (int i = 0; i < cuts->n_ptmin; ++i) L.ptmin[cuts->ptmin[i].idx] = cuts->ptmin[i].value;
+    for (int i = 0; i < cuts->n_etamax; ++i) L.etamax[cuts->etamax[i].idx] = cuts->etamax[i].value;
+    for (int i = 0; i < cuts->n_deltaR; ++i)
+        L.delta_r[{cuts->deltaR[i].pid1, cuts->deltaR[i].pid2}] = cuts->deltaR[i].value;
+
+    const uint32_t all_out = ((1u << n_ext) - 1u) & ~3u;
+    const int ndims = 3 * nout - 2;  // FSMapper::NDims (Channel.hh:33)
+    out.assign(nch, ChannelProgram{});
+    for (int c = 0; c < nch; ++c) {
+        const chili_channel_desc &d = descs[c];
+        ChannelProgram &P = out[c];
+        std::memset(&P, 0, sizeof(P));
+        P.n_ext = n_ext;
+        P.ndims = ndims;
+        P.sqrts = sqrts;
+        P.ptmax = sqrts / 2.0;
+        P.inv16pi3 = 1.0 / (16 * std::pow(M_PI, 3));  // Channel.cc:243
+        if (d.n_info < 1 || d.n_info > nout || !d.info) {
+            err << "channel " << c << ": n_info outside [1, n_ext-2]";
+            return err.str();
+        }
+        if (d.n_decays < 0 || d.n_decays > CHILI_MAX_DECAYS || (d.n_decays > 0 && !d.decays)) {
+            err << "channel " << c << ": bad decay count";
+            return err.str();
+        }
+        // slots: externals first
+        std::map<uint32_t, int> slot;
+        for (int i = 0; i < n_ext; ++i) slot[1u << i] = i;
+        for (int i = 0; i < nout; ++i) P.slot_m2[i + 2] = L.sexternal[i];  // Channel.cc:25-26
+        int n_slots = n_ext;
+
+        // DecayMap in std::map order, keyed by (idx, mass, width)
+        std::map<Key, const chili_decay *> decays;
+        for (int k = 0; k < d.n_decays; ++k) {
+            const chili_decay &dec = d.decays[k];
+            if (!decays.emplace(key_of(dec.parent), &dec).second) {
+                err << "channel " << c << ": duplicate decay parent " << dec.parent.idx;
+                return err.str();
+            }
+            const uint32_t p = dec.parent.idx, a = dec.child1.idx, b = dec.child2.idx;
+            if ((a & b) || (a | b) != p || (p & ~all_out) || is_power2(p) || a == 0 || b == 0) {
+                err << "channel " << c << ": decay " << p << " -> (" << a << ", " << b
+                    << ") is not a split of outgoing legs";
+                return err.str();
+            }
+        }
+        for (const auto &kv : decays) {
+            const uint32_t p = std::get<0>(kv.first);
+            if (!slot.count(p)) {
+                if (n_slots >= CHILI_MAX_SLOTS) return "too many currents";
+                slot[p] = n_slots++;
+            }
+        }
+        P.n_slots = n_slots;
+        int k = 0;
+        for (const auto &kv : decays) {
+            const chili_decay &dec = *kv.second;
+            const auto pt1 = L.ptmin.find(dec.child1.idx), pt2 = L.ptmin.find(dec.child2.idx);
+            if (pt1 == L.ptmin.end() || pt2 == L.ptmin.end()) {
+                err << "channel " << c << ": cuts.ptmin lacks a decay product";
+                return err.str();
+            }
+            for (uint32_t child : {dec.child1.idx, dec.child2.idx}) {
+                if (!slot.count(child)) {
+                    err << "channel " << c << ": decay product " << child << " has no decay of its own";
+                    return err.str();
+                }
+            }
+            const auto dr = L.delta_r.find({dec.child1.pid, dec.child2.pid});
+            const double delta_r = dr == L.delta_r.end() ? 0 : dr->second;
+            // Channel.cc:150-152, the same expressions evaluated on the host
+            const double smin2 = pt1->second * pt2->second * 2 / M_PI / M_PI * std::pow(delta_r, 2);
+            const auto sm = L.smin.find(dec.child1.idx | dec.child2.idx);
+            double smax = sqrts;  // SMax (Cuts.hh:21-29)
+            for (unsigned i = 0; i < L.sexternal.size(); ++i)
+                if (!(dec.parent.idx & (1u << (i + 2)))) smax -= std::sqrt(L.sexternal[i]);
+            smax = smax * smax;
+            P.dec_parent[k] = static_cast<int8_t>(slot[dec.parent.idx]);
+            P.dec_c1[k] = static_cast<int8_t>(slot[dec.child1.idx]);
+            P.dec_c2[k] = static_cast<int8_t>(slot[dec.child2.idx]);
+            P.dec_massless[k] = (std::abs(dec.parent.mass) < 1e-16 || dec.parent.width < 1e-16) ? 1 : 0;
+            P.dec_mass[k] = dec.parent.mass;
+            P.dec_width[k] = dec.parent.width;
+            P.dec_smin2[k] = smin2;
+            P.dec_cut_smin[k] = sm == L.smin.end() ? 0.0 : sm->second;
+            P.dec_smax[k] = smax;
+            ++k;
+        }
+        P.n_decay = k;
+
+        // t-channel list (FSMapper ctor, Channel.hh:18-30)
+        P.n_info = d.n_info;
+        uint32_t covered = 0;
+        for (int i = 0; i < d.n_info; ++i) {
+            const chili_particle_info &in = d.info[i];
+            if (!slot.count(in.idx) || (in.idx & 3u)) {
+                err << "channel " << c << ": t-channel entry " << in.idx << " is neither an outgoing leg nor a decaying current";
+                return err.str();
+            }
+            if (!is_power2(in.idx) && !decays.count(key_of(in))) {
+                err << "channel " << c << ": t-channel current " << in.idx << " has no matching decay";
+                return err.str();
+            }
+            const auto pt = L.ptmin.find(in.idx);
+            const auto eta = L.etamax.find(in.idx);
+            if (pt == L.ptmin.end() || eta == L.etamax.end()) {
+                err << "channel " << c << ": cuts.ptmin/etamax lack entry " << in.idx;
+                return err.str();
+            }
+            if (covered & in.idx) {
+                err << "channel " << c << ": t-channel entries overlap";
+                return err.str();
+            }
+            covered |= in.idx;
+            P.info_slot[i] = static_cast<int8_t>(slot[in.idx]);
+            P.info_ptmin[i] = pt->second != 0 ? pt->second : 1.0;
+            P.info_etamax[i] = eta->second;
+        }
+        if (covered != all_out) {
+            err << "channel " << c << ": t-channel entries do not cover all outgoing legs";
+            return err.str();
+        }
+
+        // s-channel schedule: GenSChan/DecayParts recursion (Channel.cc:204-245)
+        int ns = 0;
+        bool bad = false;
+        std::vector<const chili_particle_info *> stack;
+        auto visit = [&](auto &&self, const chili_particle_info &ab) -> void {
+            const auto it = decays.find(key_of(ab));
+            if (it == decays.end()) {
+                bad = true;
+                return;
+            }
+            const chili_decay &dec = *it->second;
+            if (ns >= CHILI_MAX_DECAYS) {
+                bad = true;
+                return;
+            }
+            P.sdec_ab[ns] = static_cast<int8_t>(slot[ab.idx]);
+            P.sdec_a[ns] = static_cast<int8_t>(slot[dec.child1.idx]);
+            P.sdec_b[ns] = static_cast<int8_t>(slot[dec.child2.idx]);
+            ++ns;
+            if (!is_power2(dec.child1.idx)) self(self, dec.child1);
+            if (!is_power2(dec.child2.idx)) self(self, dec.child2);
+        };
+        for (int i = 0; i < d.n_info; ++i)
+            if (!is_power2(d.info[i].idx)) visit(visit, d.info[i]);
+        if (bad) {
+            err << "channel " << c << ": a decaying current has no matching DecayMap entry";
+            return err.str();
+        }
+        P.n_sdec = ns;
+        const int used = P.n_decay + 3 * (P.n_info - 1) + 1 + 2 * P.n_sdec;
+        if (used != ndims) {
+            err << "channel " << c << ": consumes " << used << " uniforms, NDims is " << ndims;
+            return err.str();
+        }
+    }
+    return std::string();
+}

@@ -1,0 +1,52 @@
+// channel_program.h -- the flattened, table-driven form of one FSMapper
+// channel (include/Channel/Channel.hh:15-77) that the kernels execute.
+//
+// FSMapper keeps momenta and masses in hash maps keyed by the current bitmask
+// and recurses through std::map lookups (Channel.cc:63-256).  The host builder
+// (channel_program.cpp) resolves all of that once: every current used by the
+// channel gets a slot (slots 0..n_ext-1 are the external legs, idx 1<<i), the
+// decays are listed in std::map order, and the recursive s-channel decay tree
+// is unrolled into the order in which DecayParts consumes uniforms.  Every
+// per-decay constant that depends only on the cuts (smin2, cuts.smin, SMax) is
+// computed on the host with the reference's expression.
+#pragma once
+
+#include <cstdint>
+
+#include "chili_gpu.h"
+
+#define CHILI_MAX_SLOTS (2 * CHILI_MAX_EXT)
+#define CHILI_MAX_DECAYS CHILI_MAX_EXT
+
+struct ChannelProgram {
+    int32_t n_ext;    // external legs, incoming included
+    int32_t ndims;    // 3*(n_ext-2) - 2
+    int32_t n_slots;  // externals + compound currents
+    int32_t n_info;   // t-channel entries
+    int32_t n_decay;  // DecayMap entries, std::map order
+    int32_t n_sdec;   // DecayParts calls in uniform-consumption order
+    double sqrts, ptmax, inv16pi3;
+
+    double slot_m2[CHILI_MAX_SLOTS];  // squared masses of the outgoing legs
+
+    int8_t info_slot[CHILI_MAX_EXT];
+    double info_ptmin[CHILI_MAX_EXT];   // FSMapper::m_ptmin (Channel.hh:20-26)
+    double info_etamax[CHILI_MAX_EXT];  // cuts.etamax.at(idx)
+
+    int8_t dec_parent[CHILI_MAX_DECAYS], dec_c1[CHILI_MAX_DECAYS], dec_c2[CHILI_MAX_DECAYS];
+    int8_t dec_massless[CHILI_MAX_DECAYS];
+    double dec_mass[CHILI_MAX_DECAYS], dec_width[CHILI_MAX_DECAYS];
+    double dec_smin2[CHILI_MAX_DECAYS];     // ptmin1*ptmin2*2/pi/pi*dR^2 (Channel.cc:150)
+    double dec_cut_smin[CHILI_MAX_DECAYS];  // cuts.smin[idx1|idx2] (Channel.cc:151)
+    double dec_smax[CHILI_MAX_DECAYS];      // SMax(sqrts, cuts, idx) (Cuts.hh:21-29)
+
+    int8_t sdec_ab[CHILI_MAX_DECAYS], sdec_a[CHILI_MAX_DECAYS], sdec_b[CHILI_MAX_DECAYS];
+};
+
+#ifdef __cplusplus
+#include <string>
+#include <vector>
+// Builds the programs; returns an empty string on success, else the reason.
+std::string build_channel_programs(const chili_channel_desc *descs, int nch, const chili_cuts *cuts,
+                                   double sqrts, int n_ext, std::vector<ChannelProgram> &out);
+#endif

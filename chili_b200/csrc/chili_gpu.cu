@@ -1,0 +1,793 @@
+// chili_gpu.cu -- implementation of the C ABI declared in include/chili_gpu.h.
+//
+// One context = one device, one stream, one grid set, one channel set, one
+// integrand.  Host-side work is limited to argument checks, staging of host
+// buffers, kernel launches and, in a multichannel iteration, reading a 32-byte
+// round record to decide whether another round of points is needed.
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "chili_gpu.h"
+#include "channel_program.h"
+#include "kernels.cuh"
+
+using namespace chili_dev;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+// A growable device buffer.
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= cap) return cudaSuccess;
+        if (p) {
+            cudaError_t e = cudaFree(p);
+            if (e != cudaSuccess) return e;
+            p = nullptr;
+            cap = 0;
+        }
+        const size_t want = std::max<size_t>(bytes, 256);
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+constexpr int kStageSlots = 6;
+
+}  // namespace
+
+struct chili_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+    unsigned long long launches = 0;
+
+    // grids
+    int g_nch = 0, dims = 0, bins = 0;
+    DevBuf edges, edges_tmp;
+    // channels
+    int nch = 0, n_ext = 0, ndims = 0;
+    double sqrts = 0;
+    DevBuf progs;
+    // channel weights: alpha[CH], best[CH], cp[CH], min_diff
+    DevBuf alpha_buf;
+    bool alpha_set = false;
+    // integrand
+    IntegrandDesc f_host{};
+    DevBuf f_dev;
+    bool f_set = false;
+    // multichannel iteration scratch
+    DevBuf mom_soa, ich, flag, list, block_count, block_off, part, hist, round_res, acc, ctl, status;
+    RoundCtl *ctl_host = nullptr;  // pinned
+    double accept_rate = 0.5;
+    // plain VEGAS scratch
+    DevBuf v_part, v_hist, v_train, v_out;
+    // staging of host buffers
+    DevBuf stage[kStageSlots];
+    int max_smem_optin = 0;
+};
+
+namespace {
+
+int fail(chili_ctx *ctx, int code, const std::string &msg) {
+    if (ctx) ctx->err = msg;
+    g_last_error = msg;
+    return code;
+}
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        const cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                                    \
+            return fail(ctx, CHILI_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define LAUNCHED()                                                                                     \
+    do {                                                                                               \
+        ++ctx->launches;                                                                               \
+        const cudaError_t e_ = cudaGetLastError();                                                     \
+        if (e_ != cudaSuccess) return fail(ctx, CHILI_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+bool is_device_ptr(const void *p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Resolves a caller buffer to a device pointer: device buffers pass through,
+// host buffers are staged in slot `slot` (copied in when `in`).
+struct Arg {
+    void *dev = nullptr;
+    void *host = nullptr;
+    size_t bytes = 0;
+};
+
+int resolve(chili_ctx *ctx, const void *p, size_t bytes, int slot, bool in, Arg &a) {
+    a = Arg{};
+    a.bytes = bytes;
+    if (!p) return CHILI_OK;
+    if (is_device_ptr(p)) {
+        a.dev = const_cast<void *>(p);
+        return CHILI_OK;
+    }
+    CK(ctx->stage[slot].ensure(bytes));
+    a.dev = ctx->stage[slot].p;
+    a.host = const_cast<void *>(p);
+    if (in && bytes) CK(cudaMemcpyAsync(a.dev, p, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    return CHILI_OK;
+}
+
+int finish_out(chili_ctx *ctx, const Arg &a) {
+    if (a.host && a.bytes) CK(cudaMemcpyAsync(a.host, a.dev, a.bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    return CHILI_OK;
+}
+
+int sync_if_host(chili_ctx *ctx, std::initializer_list<const Arg *> args) {
+    for (const Arg *a : args)
+        if (a->host) {
+            CK(cudaStreamSynchronize(ctx->stream));
+            return CHILI_OK;
+        }
+    return CHILI_OK;
+}
+
+unsigned grid_for(long long n, int block) { return static_cast<unsigned>((n + block - 1) / block); }
+
+double *alpha_ptr(chili_ctx *ctx) { return ctx->alpha_buf.as<double>(); }
+double *best_ptr(chili_ctx *ctx) { return ctx->alpha_buf.as<double>() + CHILI_MAX_CHANNELS; }
+double *cp_ptr(chili_ctx *ctx) { return ctx->alpha_buf.as<double>() + 2 * CHILI_MAX_CHANNELS; }
+double *mindiff_ptr(chili_ctx *ctx) { return ctx->alpha_buf.as<double>() + 3 * CHILI_MAX_CHANNELS; }
+double *acc_train_ptr(chili_ctx *ctx) {
+    return reinterpret_cast<double *>(static_cast<char *>(ctx->acc.p) + offsetof(IterAcc, atrain));
+}
+
+int need_grids(chili_ctx *ctx) {
+    if (!ctx->edges.p || ctx->g_nch <= 0) return fail(ctx, CHILI_ERR_STATE, "no grids set");
+    return CHILI_OK;
+}
+int need_channels(chili_ctx *ctx) {
+    if (!ctx->progs.p || ctx->nch <= 0) return fail(ctx, CHILI_ERR_STATE, "no channels set");
+    return CHILI_OK;
+}
+
+int set_device(chili_ctx *ctx) {
+    CK(cudaSetDevice(ctx->device));
+    return CHILI_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int chili_gpu_create(int device, chili_ctx **out) {
+    chili_ctx *ctx = nullptr;
+    if (!out) return fail(nullptr, CHILI_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return fail(nullptr, CHILI_ERR_CUDA, "no CUDA device available");
+    }
+    if (device < 0 || device >= ndev) return fail(nullptr, CHILI_ERR_INVALID_ARG, "device index out of range");
+    ctx = new chili_ctx();
+    ctx->device = device;
+    int rc;
+    if ((rc = set_device(ctx)) != CHILI_OK) {
+        delete ctx;
+        return rc;
+    }
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return fail(nullptr, CHILI_ERR_CUDA, "cudaStreamCreate failed");
+    }
+    ctx->own_stream = true;
+    if (cudaMallocHost(reinterpret_cast<void **>(&ctx->ctl_host), sizeof(RoundCtl)) != cudaSuccess) {
+        cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        return fail(nullptr, CHILI_ERR_CUDA, "cudaMallocHost failed");
+    }
+    cudaDeviceGetAttribute(&ctx->max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    cudaFuncSetAttribute(k_mc_weight, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->max_smem_optin);
+    cudaFuncSetAttribute(k_vegas_iter, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->max_smem_optin);
+    cudaFuncSetAttribute(k_grid_adapt, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->max_smem_optin);
+    cudaGetLastError();
+    *out = ctx;
+    return CHILI_OK;
+}
+
+int chili_gpu_destroy(chili_ctx *ctx) {
+    if (!ctx) return CHILI_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    DevBuf *bufs[] = {&ctx->edges, &ctx->edges_tmp, &ctx->progs, &ctx->alpha_buf, &ctx->f_dev, &ctx->mom_soa,
+                      &ctx->ich, &ctx->flag, &ctx->list, &ctx->block_count, &ctx->block_off, &ctx->part,
+                      &ctx->hist, &ctx->round_res, &ctx->acc, &ctx->ctl, &ctx->status, &ctx->v_part,
+                      &ctx->v_hist, &ctx->v_train, &ctx->v_out};
+    for (DevBuf *b : bufs) b->release();
+    for (auto &b : ctx->stage) b.release();
+    if (ctx->ctl_host) cudaFreeHost(ctx->ctl_host);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return CHILI_OK;
+}
+
+const char *chili_gpu_last_error(const chili_ctx *ctx) {
+    return ctx ? ctx->err.c_str() : g_last_error.c_str();
+}
+
+int chili_gpu_set_stream(chili_ctx *ctx, void *stream) {
+    if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (stream) {
+        if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+        ctx->stream = static_cast<cudaStream_t>(stream);
+        ctx->own_stream = false;
+    } else if (!ctx->own_stream) {
+        CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        ctx->own_stream = true;
+    }
+    return CHILI_OK;
+}
+
+int chili_gpu_synchronize(chili_ctx *ctx) {
+    if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHILI_OK;
+}
+
+uint64_t chili_gpu_launch_count(const chili_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+// --------------------------------------------------------------------- grids
+int chili_gpu_set_grids(chili_ctx *ctx, const double *edges, int nch, int dims, int bins) {
+    if (!ctx || !edges) return fail(ctx, CHILI_ERR_INVALID_ARG, "NULL argument");
+    if (nch < 1 || nch > CHILI_MAX_CHANNELS || dims < 1 || dims > CHILI_MAX_DIMS || bins < 2 ||
+        bins > CHILI_MAX_BINS)
+        return fail(ctx, CHILI_ERR_LIMIT, "grid shape outside the compiled limits");
+    if (ctx->nch > 0 && (nch != ctx->nch || dims != ctx->ndims))
+        return fail(ctx, CHILI_ERR_INVALID_ARG, "grid count/dims do not match the channels");
+    int rc;
+    if ((rc = set_device(ctx))) return rc;
+    const size_t bytes = sizeof(double) * nch * dims * (bins + 1);
+    CK(ctx->edges.ensure(bytes));
+    CK(ctx->edges_tmp.ensure(bytes));
+    Arg a;
+    if ((rc = resolve(ctx, edges, bytes, 0, true, a))) return rc;
+    CK(cudaMemcpyAsync(ctx->edges.p, a.dev, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    ctx->g_nch = nch;
+    ctx->dims = dims;
+    ctx->bins = bins;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHILI_OK;
+}
+
+int chili_gpu_get_grids(chili_ctx *ctx, double *edges, int nch, int dims, int bins) {
+    if (!ctx || !edges) return fail(ctx, CHILI_ERR_INVALID_ARG, "NULL argument");
+    int rc;
+    if ((rc = need_grids(ctx))) return rc;
+    if (nch != ctx->g_nch || dims != ctx->dims || bins != ctx->bins)
+        return fail(ctx, CHILI_ERR_INVALID_ARG, "grid shape mismatch");
+    const size_t bytes = sizeof(double) * nch * dims * (bins + 1);
+    Arg a;
+    if ((rc = resolve(ctx, edges, bytes, 0, false, a))) return rc;
+    CK(cudaMemcpyAsync(a.dev, ctx->edges.p, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    if ((rc = finish_out(ctx, a))) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHILI_OK;
+}
+
+int chili_gpu_grid_map(chili_ctx *ctx, int ch, const double *u, double *x, double *jac, int64_t n) {
+    if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
+    int rc;
+    if ((rc = need_grids(ctx))) return rc;
+    if (ch < 0 || ch >= ctx->g_nch || n < 0 || !u || !x || !jac) return fail(ctx, CHILI_ERR_INVALID_ARG, "bad argument");
+    if (n == 0) return CHILI_OK;
+    const int D = ctx->dims, B = ctx->bins;
+    Arg au, ax, aj;
+    if ((rc = resolve(ctx, u, sizeof(double) * n * D, 0, true, au))) return rc;
+    if ((rc = resolve(ctx, x, sizeof(double) * n * D, 1, false, ax))) return rc;
+    if ((rc = resolve(ctx, jac, sizeof(double) * n, 2, false, aj))) return rc;
+    const double *g = ctx->edges.as<double>() + static_cast<size_t>(ch) * D * (B + 1);
+    k_grid_map<<<grid_for(n, 128), 128, 0, ctx->stream>>>(g, D, B, static_cast<const double *>(au.dev),
+                                                          static_cast<double *>(ax.dev),
+                                                          static_cast<double *>(aj.dev), n);
+    LAUNCHED();
+    if ((rc = finish_out(ctx, ax)) || (rc = finish_out(ctx, aj))) return rc;
+    return sync_if_host(ctx, {&au, &ax, &aj});
+}
+
+int chili_gpu_grid_weight(chili_ctx *ctx, int ch, const double *x, double *w, int32_t *bin, int64_t n) {
+    if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
+    int rc;
+    if ((rc = need_grids(ctx))) return rc;
+    if (ch < 0 || ch >= ctx->g_nch || n < 0 || !x || (!w && !bin)) return fail(ctx, CHILI_ERR_INVALID_ARG, "bad argument");
+    if (n == 0) return CHILI_OK;
+    const int D = ctx->dims, B = ctx->bins;
+    Arg ax, aw, ab;
+    if ((rc = resolve(ctx, x, sizeof(double) * n * D, 0, true, ax))) return rc;
+    if ((rc = resolve(ctx, w, sizeof(double) * n, 1, false, aw))) return rc;
+    if ((rc = resolve(ctx, bin, sizeof(int32_t) * n * D, 2, false, ab))) return rc;
+    const double *g = ctx->edges.as<double>() + static_cast<size_t>(ch) * D * (B + 1);
+    k_grid_weight<<<grid_for(n, 128), 128, 0, ctx->stream>>>(g, D, B, static_cast<const double *>(ax.dev),
+                                                             static_cast<double *>(aw.dev),
+                                                             static_cast<int32_t *>(ab.dev), n);
+    LAUNCHED();
+    if ((rc = finish_out(ctx, aw)) || (rc = finish_out(ctx, ab))) return rc;
+    return sync_if_host(ctx, {&ax, &aw, &ab});
+}
+
+static int adapt_grids(chili_ctx *ctx, int first, int count, double alpha, const double *train_dev, int skip_zero) {
+    const int D = ctx->dims, B = ctx->bins;
+    CK(ctx->status.ensure(sizeof(int)));
+    CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(int), ctx->stream));
+    const size_t gsz = static_cast<size_t>(D) * (B + 1);
+    // grids outside [first, first+count) keep their edges
+    if (count != ctx->g_nch)
+        CK(cudaMemcpyAsync(ctx->edges_tmp.p, ctx->edges.p, sizeof(double) * gsz * ctx->g_nch,
+                           cudaMemcpyDeviceToDevice, ctx->stream));
+    dim3 grid(D, count);
+    k_grid_adapt<<<grid, 32, sizeof(double) * B, ctx->stream>>>(
+        ctx->edges.as<double>() + first * gsz, ctx->edges_tmp.as<double>() + first * gsz, D, B, alpha, train_dev,
+        skip_zero, ctx->status.as<int>());
+    LAUNCHED();
+    std::swap(ctx->edges, ctx->edges_tmp);
+    return CHILI_OK;
+}
+
+int chili_gpu_grid_adapt(chili_ctx *ctx, int ch, double alpha, const double *train) {
+    if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
+    int rc;
+    if ((rc = need_grids(ctx))) return rc;
+    if (ch < 0 || ch >= ctx->g_nch || !train) return fail(ctx, CHILI_ERR_INVALID_ARG, "bad argument");
+    Arg at;
+    if ((rc = resolve(ctx, train, sizeof(double) * ctx->dims * ctx->bins, 0, true, at))) return rc;
+    if ((rc = adapt_grids(ctx, ch, 1, alpha, static_cast<const double *>(at.dev), 0))) return rc;
+    return sync_if_host(ctx, {&at});
+}
+
+int chili_gpu_grid_split(chili_ctx *ctx, int nsplit) {
+    if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
+    int rc;
+    if ((rc = need_grids(ctx))) return rc;
+    if (nsplit < 2 || nsplit > 4) return fail(ctx, CHILI_ERR_INVALID_ARG, "nsplit must be 2, 3 or 4");
+    const int nb = ctx->bins * nsplit;
+    if (nb > CHILI_MAX_BINS) return fail(ctx, CHILI_ERR_LIMIT, "split grid exceeds CHILI_MAX_BINS");
+    const size_t bytes = sizeof(double) * ctx->g_nch * ctx->dims * (nb + 1);
+    CK(ctx->edges_tmp.ensure(bytes));
+    const long long total = static_cast<long long>(ctx->g_nch) * ctx->dims * ctx->bins;
+    k_grid_split<<<grid_for(total, 128), 128, 0, ctx->stream>>>(ctx->edges.as<double>(), ctx->edges_tmp.as<double>(),
+                                                                ctx->g_nch, ctx->dims, ctx->bins, nsplit);
+    LAUNCHED();
+    CK(cudaStreamSynchronize(ctx->stream));
+    std::swap(ctx->edges, ctx->edges_tmp);
+    CK(ctx->edges_tmp.ensure(bytes));
+    ctx->bins = nb;
+    return CHILI_OK;
+}
+
+// ----------------------------------------------------------------- integrand
+int chili_gpu_set_integrand(chili_ctx *ctx, int kind, const double *params, int nparams) {
+    if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
+    if (kind < CHILI_FUNC_UNIT || kind > CHILI_FUNC_PROPAGATOR_TOP2)
+        return fail(ctx, CHILI_ERR_INVALID_ARG, "unknown integrand kind");
+    if (nparams < 0 || nparams > CHILI_MAX_INTEGRAND_PARAMS || (nparams > 0 && !params))
+        return fail(ctx, CHILI_ERR_LIMIT, "integrand parameter count outside [0, CHILI_MAX_INTEGRAND_PARAMS]");
+    const int need = kind == CHILI_FUNC_CAMEL ? 2 : (kind == CHILI_FUNC_UNIT ? 0 : 3);
+    if (nparams < need) return fail(ctx, CHILI_ERR_INVALID_ARG, "too few integrand parameters");
+    int rc;
+    if ((rc = set_device(ctx))) return rc;
+    ctx->f_host.kind = kind;
+    ctx->f_host.nparams = nparams;
+    for (int i = 0; i < nparams; ++i) ctx->f_host.p[i] = params[i];
+    CK(ctx->f_dev.ensure(sizeof(IntegrandDesc)));
+    CK(cudaMemcpyAsync(ctx->f_dev.p, &ctx->f_host, sizeof(IntegrandDesc), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->f_set = true;
+    return CHILI_OK;
+}
+
+int chili_gpu_set_preprocess(chili_ctx *ctx, int kind) {
+    if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
+    if (kind != CHILI_PRE_ACCEPT_ALL && kind != CHILI_PRE_FINITE)
+        return fail(ctx, CHILI_ERR_INVALID_ARG, "unknown preprocess kind");
+    int rc;
+    if ((rc = set_device(ctx))) return rc;
+    ctx->f_host.pre = kind;
+    CK(ctx->f_dev.ensure(sizeof(IntegrandDesc)));
+    CK(cudaMemcpyAsync(ctx->f_dev.p, &ctx->f_host, sizeof(IntegrandDesc), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHILI_OK;
+}
+
+// ----------------------------------------------------------------- plain VEGAS
+int chili_gpu_vegas_iterate(chili_ctx *ctx, uint64_t ncalls, uint64_t seed, uint64_t counter_base,
+                            const double *u, double alpha, int adapt, chili_stats *stats_out, double *train_out) {
+    if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
+    int rc;
+    if ((rc = need_grids(ctx))) return rc;
+    if (!ctx->f_set || ctx->f_host.kind != CHILI_FUNC_CAMEL)
+        return fail(ctx, CHILI_ERR_STATE, "plain VEGAS needs the camel integrand");
+    if (ctx->f_host.nparams < 2 + 2 * ctx->dims)
+        return fail(ctx, CHILI_ERR_INVALID_ARG, "camel needs 2 + 2*dims parameters");
+    if (ncalls < 2) return fail(ctx, CHILI_ERR_INVALID_ARG, "ncalls must be at least 2");
+    const int D = ctx->dims, B = ctx->bins, nh = D * B;
+    const long long n = static_cast<long long>(ncalls);
+    Arg au, ast, atr;
+    if ((rc = resolve(ctx, u, sizeof(double) * n * D, 0, true, au))) return rc;
+    if ((rc = resolve(ctx, stats_out, sizeof(chili_stats), 1, false, ast))) return rc;
+    if ((rc = resolve(ctx, train_out, sizeof(double) * nh, 2, false, atr))) return rc;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    const size_t hist_bytes = sizeof(double) * nh;
+    const bool smem = hist_bytes <= 48 * 1024;
+    long long nblocks = std::min<long long>(grid_for(n, kVegasBlock), static_cast<long long>(sms) * 4);
+    CK(ctx->v_part.ensure(sizeof(double) * 6 * nblocks));
+    CK(ctx->v_hist.ensure(smem ? hist_bytes * nblocks : hist_bytes));
+    CK(ctx->v_train.ensure(hist_bytes));
+    CK(ctx->v_out.ensure(sizeof(double) * 6));
+    if (!smem) CK(cudaMemsetAsync(ctx->v_hist.p, 0, hist_bytes, ctx->stream));
+    k_vegas_iter<<<static_cast<unsigned>(nblocks), kVegasBlock, smem ? hist_bytes : 0, ctx->stream>>>(
+        ctx->edges.as<double>(), D, B, seed, counter_base, static_cast<const double *>(au.dev), n,
+        ctx->f_dev.as<IntegrandDesc>(), ctx->v_part.as<double>(), ctx->v_hist.as<double>(), smem ? 1 : 0);
+    LAUNCHED();
+    double *train = smem ? ctx->v_train.as<double>() : ctx->v_hist.as<double>();
+    k_vegas_finalize<<<1, 256, 0, ctx->stream>>>(ctx->v_part.as<double>(), static_cast<int>(nblocks),
+                                                 ctx->v_hist.as<double>(), smem ? 1 : 0, nh, train,
+                                                 ctx->v_out.as<double>());
+    LAUNCHED();
+    if (train_out) CK(cudaMemcpyAsync(atr.dev, train, hist_bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    if (stats_out) CK(cudaMemcpyAsync(ast.dev, ctx->v_out.p, sizeof(chili_stats), cudaMemcpyDeviceToDevice, ctx->stream));
+    if (adapt) {
+        if ((rc = adapt_grids(ctx, 0, 1, alpha, train, 0))) return rc;
+    }
+    if ((rc = finish_out(ctx, ast)) || (rc = finish_out(ctx, atr))) return rc;
+    return sync_if_host(ctx, {&au, &ast, &atr});
+}
+
+// ------------------------------------------------------------------ channels
+int chili_gpu_set_channels(chili_ctx *ctx, const chili_channel_desc *descs, int nch, const chili_cuts *cuts,
+                           double sqrts, int n_ext) {
+    if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
+    if (!(sqrts > 0)) return fail(ctx, CHILI_ERR_INVALID_ARG, "sqrts must be positive");
+    std::vector<ChannelProgram> progs;
+    const std::string why = build_channel_programs(descs, nch, cuts, sqrts, n_ext, progs);
+    if (!why.empty()) return fail(ctx, CHILI_ERR_INVALID_ARG, why);
+    int rc;
+    if ((rc = set_device(ctx))) return rc;
+    CK(ctx->progs.ensure(sizeof(ChannelProgram) * nch));
+    CK(cudaMemcpyAsync(ctx->progs.p, progs.data(), sizeof(ChannelProgram) * nch, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    ctx->nch = nch;
+    ctx->n_ext = n_ext;
+    ctx->ndims = progs[0].ndims;
+    ctx->sqrts = sqrts;
+    // alpha = 1/nch (MultiChannel.cc:62-67), best = alpha, min_diff = +inf
+    std::vector<double> a(4 * CHILI_MAX_CHANNELS, 0.0);
+    for (int i = 0; i < nch; ++i) a[i] = 1.0 / static_cast<double>(nch);
+    a[3 * CHILI_MAX_CHANNELS] = INFINITY;
+    CK(ctx->alpha_buf.ensure(sizeof(double) * a.size()));
+    CK(cudaMemcpyAsync(ctx->alpha_buf.p, a.data(), sizeof(double) * a.size(), cudaMemcpyHostToDevice, ctx->stream));
+    k_alpha_update<<<1, 32, 0, ctx->stream>>>(alpha_ptr(ctx), best_ptr(ctx), mindiff_ptr(ctx), cp_ptr(ctx), nullptr,
+                                              nch, 0.0, 0.0, 0);
+    LAUNCHED();
+    ctx->alpha_set = true;
+    // best_weights start empty in the reference; they read back as NaN until
+    // the first MaxDifference update
+    std::vector<double> nanv(nch, NAN);
+    CK(cudaMemcpyAsync(best_ptr(ctx), nanv.data(), sizeof(double) * nch, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->g_nch > 0 && (ctx->g_nch != nch || ctx->dims != ctx->ndims)) {
+        ctx->edges.release();
+        ctx->g_nch = 0;
+    }
+    return CHILI_OK;
+}
+
+int chili_gpu_ndims(const chili_ctx *ctx) { return ctx ? ctx->ndims : -1; }
+
+int chili_gpu_fsmapper_generate(chili_ctx *ctx, int ch, const double *x, double *mom, int64_t n) {
+    if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
+    int rc;
+    if ((rc = need_channels(ctx))) return rc;
+    if (ch < 0 || ch >= ctx->nch || !x || !mom || n < 0) return fail(ctx, CHILI_ERR_INVALID_ARG, "bad argument");
+    if (n == 0) return CHILI_OK;
+    Arg ax, am;
+    if ((rc = resolve(ctx, x, sizeof(double) * n * ctx->ndims, 0, true, ax))) return rc;
+    if ((rc = resolve(ctx, mom, sizeof(double) * n * ctx->n_ext * 4, 1, false, am))) return rc;
+    k_fs_generate<<<grid_for(n, 128), 128, 0, ctx->stream>>>(ctx->progs.as<ChannelProgram>() + ch,
+                                                             static_cast<const double *>(ax.dev),
+                                                             static_cast<double *>(am.dev), n);
+    LAUNCHED();
+    if ((rc = finish_out(ctx, am))) return rc;
+    return sync_if_host(ctx, {&ax, &am});
+}
+
+int chili_gpu_fsmapper_weight(chili_ctx *ctx, int ch, const double *mom, double *x_out, double *w, int64_t n) {
+    if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
+    int rc;
+    if ((rc = need_channels(ctx))) return rc;
+    if (ch < 0 || ch >= ctx->nch || !mom || !w || n < 0) return fail(ctx, CHILI_ERR_INVALID_ARG, "bad argument");
+    if (n == 0) return CHILI_OK;
+    Arg am, ax, aw;
+    if ((rc = resolve(ctx, mom, sizeof(double) * n * ctx->n_ext * 4, 0, true, am))) return rc;
+    if ((rc = resolve(ctx, x_out, sizeof(double) * n * ctx->ndims, 1, false, ax))) return rc;
+    if ((rc = resolve(ctx, w, sizeof(double) * n, 2, false, aw))) return rc;
+    k_fs_weight<<<grid_for(n, 128), 128, 0, ctx->stream>>>(ctx->progs.as<ChannelProgram>() + ch,
+                                                           static_cast<const double *>(am.dev),
+                                                           static_cast<double *>(ax.dev),
+                                                           static_cast<double *>(aw.dev), n);
+    LAUNCHED();
+    if ((rc = finish_out(ctx, ax)) || (rc = finish_out(ctx, aw))) return rc;
+    return sync_if_host(ctx, {&am, &ax, &aw});
+}
+
+// -------------------------------------------------------------- multichannel
+int chili_gpu_set_alpha(chili_ctx *ctx, const double *alpha, int nch) {
+    if (!ctx || !alpha) return fail(ctx, CHILI_ERR_INVALID_ARG, "NULL argument");
+    int rc;
+    if ((rc = need_channels(ctx))) return rc;
+    if (nch != ctx->nch) return fail(ctx, CHILI_ERR_INVALID_ARG, "alpha length != channel count");
+    Arg a;
+    if ((rc = resolve(ctx, alpha, sizeof(double) * nch, 0, true, a))) return rc;
+    CK(cudaMemcpyAsync(alpha_ptr(ctx), a.dev, sizeof(double) * nch, cudaMemcpyDeviceToDevice, ctx->stream));
+    k_alpha_update<<<1, 32, 0, ctx->stream>>>(alpha_ptr(ctx), best_ptr(ctx), mindiff_ptr(ctx), cp_ptr(ctx), nullptr,
+                                              nch, 0.0, 0.0, 0);
+    LAUNCHED();
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHILI_OK;
+}
+
+int chili_gpu_get_alpha(chili_ctx *ctx, double *alpha, double *best_alpha, double *min_diff, int nch) {
+    if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
+    int rc;
+    if ((rc = need_channels(ctx))) return rc;
+    if (nch != ctx->nch) return fail(ctx, CHILI_ERR_INVALID_ARG, "alpha length != channel count");
+    std::vector<double> h(4 * CHILI_MAX_CHANNELS);
+    CK(cudaMemcpyAsync(h.data(), ctx->alpha_buf.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (alpha) std::memcpy(alpha, h.data(), sizeof(double) * nch);
+    if (best_alpha) std::memcpy(best_alpha, h.data() + CHILI_MAX_CHANNELS, sizeof(double) * nch);
+    if (min_diff) *min_diff = h[3 * CHILI_MAX_CHANNELS];
+    return CHILI_OK;
+}
+
+int chili_gpu_select_channel(chili_ctx *ctx, const double *v, int32_t *ich, int64_t n) {
+    if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
+    int rc;
+    if ((rc = need_channels(ctx))) return rc;
+    if (!v || !ich || n < 0) return fail(ctx, CHILI_ERR_INVALID_ARG, "bad argument");
+    if (n == 0) return CHILI_OK;
+    Arg av, ai;
+    if ((rc = resolve(ctx, v, sizeof(double) * n, 0, true, av))) return rc;
+    if ((rc = resolve(ctx, ich, sizeof(int32_t) * n, 1, false, ai))) return rc;
+    k_select<<<grid_for(n, 256), 256, 0, ctx->stream>>>(cp_ptr(ctx), ctx->nch, static_cast<const double *>(av.dev),
+                                                        static_cast<int32_t *>(ai.dev), n);
+    LAUNCHED();
+    if ((rc = finish_out(ctx, ai))) return rc;
+    return sync_if_host(ctx, {&av, &ai});
+}
+
+static int need_mc(chili_ctx *ctx) {
+    int rc;
+    if ((rc = need_channels(ctx))) return rc;
+    if ((rc = need_grids(ctx))) return rc;
+    if (ctx->g_nch != ctx->nch || ctx->dims != ctx->ndims)
+        return fail(ctx, CHILI_ERR_STATE, "grids do not match the channels (nch x ndims)");
+    return CHILI_OK;
+}
+
+int chili_gpu_multichannel_weight(chili_ctx *ctx, const double *mom, const int32_t *ich, double *wgt, double *dens,
+                                  double *x_ich, int64_t n) {
+    if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
+    int rc;
+    if ((rc = need_mc(ctx))) return rc;
+    if (!mom || !ich || !wgt || n < 0) return fail(ctx, CHILI_ERR_INVALID_ARG, "bad argument");
+    if (n == 0) return CHILI_OK;
+    Arg am, ai, aw, ad, ax;
+    if ((rc = resolve(ctx, mom, sizeof(double) * n * ctx->n_ext * 4, 0, true, am))) return rc;
+    if ((rc = resolve(ctx, ich, sizeof(int32_t) * n, 1, true, ai))) return rc;
+    if ((rc = resolve(ctx, wgt, sizeof(double) * n, 2, false, aw))) return rc;
+    if ((rc = resolve(ctx, dens, sizeof(double) * n * ctx->nch, 3, false, ad))) return rc;
+    if ((rc = resolve(ctx, x_ich, sizeof(double) * n * ctx->ndims, 4, false, ax))) return rc;
+    k_mc_weight_batch<<<grid_for(n, 128), 128, 0, ctx->stream>>>(
+        ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), alpha_ptr(ctx), ctx->nch, ctx->ndims, ctx->bins,
+        ctx->n_ext, static_cast<const double *>(am.dev), static_cast<const int32_t *>(ai.dev),
+        static_cast<double *>(aw.dev), static_cast<double *>(ad.dev), static_cast<double *>(ax.dev), n);
+    LAUNCHED();
+    if ((rc = finish_out(ctx, aw)) || (rc = finish_out(ctx, ad)) || (rc = finish_out(ctx, ax))) return rc;
+    return sync_if_host(ctx, {&am, &ai, &aw, &ad, &ax});
+}
+
+int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_params *params, uint64_t seed,
+                                   uint64_t counter_base, const double *u, int64_t n_u, int guard_alpha,
+                                   chili_stats *stats_out, chili_mc_iter_info *info) {
+    if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
+    int rc;
+    if ((rc = need_mc(ctx))) return rc;
+    if (!params) return fail(ctx, CHILI_ERR_INVALID_ARG, "params is NULL");
+    if (!ctx->f_set) return fail(ctx, CHILI_ERR_STATE, "no integrand set");
+    if (ctx->f_host.kind == CHILI_FUNC_CAMEL) return fail(ctx, CHILI_ERR_STATE, "the camel is not a phase-space integrand");
+    if (u && n_u <= 0) return fail(ctx, CHILI_ERR_INVALID_ARG, "n_u must be positive when u is given");
+    const long long ncalls = static_cast<long long>(params->ncalls);
+    if (ncalls < 1) return fail(ctx, CHILI_ERR_INVALID_ARG, "ncalls must be positive");
+    const int nch = ctx->nch, D = ctx->ndims, B = ctx->bins, NE = ctx->n_ext;
+    const bool opt = params->should_optimize != 0;
+    const double *ud = nullptr;
+    Arg au;
+    if (u) {
+        if ((rc = resolve(ctx, u, sizeof(double) * n_u * (D + 1), 0, true, au))) return rc;
+        ud = static_cast<const double *>(au.dev);
+    }
+    const size_t hist_n = static_cast<size_t>(nch) * D * B;
+    CK(ctx->hist.ensure(sizeof(double) * hist_n));
+    CK(ctx->acc.ensure(sizeof(IterAcc)));
+    CK(ctx->ctl.ensure(sizeof(RoundCtl)));
+    CK(ctx->round_res.ensure(sizeof(double) * (kPartFixed + nch)));
+    CK(cudaMemsetAsync(ctx->hist.p, 0, sizeof(double) * hist_n, ctx->stream));
+    {
+        IterAcc a0{};
+        a0.st[1] = 1.7976931348623157e308;  // StatsData min = lim::max()
+        a0.st[2] = 2.2250738585072014e-308; // StatsData max = lim::min()
+        CK(cudaMemcpyAsync(ctx->acc.p, &a0, sizeof(IterAcc), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    const size_t wgt_smem = sizeof(double) * (static_cast<size_t>(nch) * kWgtBlock + (kWgtBlock / 32) * nch);
+    if (wgt_smem > static_cast<size_t>(ctx->max_smem_optin))
+        return fail(ctx, CHILI_ERR_LIMIT, "too many channels for the weight kernel's shared memory");
+
+    long long needed = ncalls, tried = 0;
+    unsigned long long rounds = 0;
+    while (needed > 0) {
+        long long m = static_cast<long long>(static_cast<double>(needed) / std::max(ctx->accept_rate, 0.02) * 1.03) + 1024;
+        m = std::min<long long>(m, 1ll << 23);
+        if (u) {
+            m = std::min<long long>(m, n_u - tried);
+            if (m <= 0) return fail(ctx, CHILI_ERR_LIMIT, "the given uniforms ran out before ncalls points were accepted");
+        }
+        const long long nb_f = (m + kFwdBlock - 1) / kFwdBlock;
+        CK(ctx->mom_soa.ensure(sizeof(double) * 4 * NE * m));
+        CK(ctx->ich.ensure(sizeof(int32_t) * m));
+        CK(ctx->flag.ensure(m));
+        CK(ctx->list.ensure(sizeof(int32_t) * std::min(m, needed)));
+        CK(ctx->block_count.ensure(sizeof(int32_t) * nb_f));
+        CK(ctx->block_off.ensure(sizeof(long long) * nb_f));
+        const long long nb_w = (std::min(m, needed) + kWgtBlock - 1) / kWgtBlock;
+        CK(ctx->part.ensure(sizeof(double) * (kPartFixed + nch) * nb_w));
+        k_mc_forward<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(
+            ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), cp_ptr(ctx), nch, D, B, seed,
+            counter_base + tried, ud ? ud + tried * (D + 1) : nullptr, m, ctx->f_dev.as<IntegrandDesc>(), NE,
+            ctx->mom_soa.as<double>(), ctx->ich.as<int32_t>(), ctx->flag.as<uint8_t>(), ctx->block_count.as<int32_t>());
+        LAUNCHED();
+        k_mc_scan<<<1, 1024, 0, ctx->stream>>>(ctx->block_count.as<int32_t>(), static_cast<int>(nb_f),
+                                               ctx->flag.as<uint8_t>(), m, needed, ctx->block_off.as<long long>(),
+                                               ctx->ctl.as<RoundCtl>());
+        LAUNCHED();
+        k_mc_compact<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(
+            ctx->flag.as<uint8_t>(), ctx->block_off.as<long long>(), ctx->ctl.as<RoundCtl>(), m, ctx->list.as<int32_t>());
+        LAUNCHED();
+        k_mc_weight<<<static_cast<unsigned>(nb_w), kWgtBlock, wgt_smem, ctx->stream>>>(
+            ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), alpha_ptr(ctx), nch, D, B, NE,
+            ctx->mom_soa.as<double>(), m, ctx->ich.as<int32_t>(), ctx->list.as<int32_t>(), ctx->ctl.as<RoundCtl>(),
+            ctx->f_dev.as<IntegrandDesc>(), opt ? 1 : 0, guard_alpha ? 1 : 0, ctx->hist.as<double>(),
+            ctx->part.as<double>());
+        LAUNCHED();
+        k_mc_reduce<<<kPartFixed + nch, 256, 0, ctx->stream>>>(ctx->part.as<double>(), nch, ctx->ctl.as<RoundCtl>(),
+                                                               ctx->round_res.as<double>());
+        LAUNCHED();
+        k_mc_accumulate<<<1, 256, 0, ctx->stream>>>(ctx->round_res.as<double>(), nch, ctx->ctl.as<RoundCtl>(),
+                                                    ctx->acc.as<IterAcc>());
+        LAUNCHED();
+        CK(cudaMemcpyAsync(ctx->ctl_host, ctx->ctl.p, sizeof(RoundCtl), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        const RoundCtl r = *ctx->ctl_host;
+        if (r.cut <= 0 || r.cut > m || r.n_acc < 0 || r.nan_round < 0 || r.nan_round > r.n_acc)
+            return fail(ctx, CHILI_ERR_CUDA, "inconsistent round record");
+        tried += r.cut;
+        needed -= (r.n_acc - r.nan_round);
+        if (r.cut > 0) ctx->accept_rate = std::max(0.02, static_cast<double>(r.n_acc) / static_cast<double>(r.cut));
+        if (++rounds > 100000) return fail(ctx, CHILI_ERR_TIMEOUT, "no accepted points after 100000 rounds");
+    }
+    IterAcc acc_h;
+    if (opt) {
+        k_alpha_update<<<1, 32, 0, ctx->stream>>>(alpha_ptr(ctx), best_ptr(ctx), mindiff_ptr(ctx), cp_ptr(ctx),
+                                                  acc_train_ptr(ctx), nch, params->beta,
+                                                  params->min_alpha, 1);
+        LAUNCHED();
+        if ((rc = adapt_grids(ctx, 0, nch, params->grid_alpha, ctx->hist.as<double>(), 1))) return rc;
+    }
+    CK(cudaMemcpyAsync(&acc_h, ctx->acc.p, sizeof(IterAcc), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (stats_out) std::memcpy(stats_out, acc_h.st, sizeof(chili_stats));
+    if (info) {
+        info->points_tried = static_cast<uint64_t>(tried);
+        info->points_accepted = static_cast<uint64_t>(ncalls);
+        info->rejected_pre = static_cast<uint64_t>(acc_h.rejected_pre);
+        info->rejected_nan = static_cast<uint64_t>(acc_h.nan_count);
+        info->weight_max = acc_h.wmax;
+        info->nonfinite_alpha_terms = acc_h.nonfinite;
+    }
+    return CHILI_OK;
+}
+
+int chili_gpu_get_training(chili_ctx *ctx, double *hist, double *alpha_train) {
+    if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
+    int rc;
+    if ((rc = need_mc(ctx))) return rc;
+    if (!ctx->hist.p || !ctx->acc.p) return fail(ctx, CHILI_ERR_STATE, "no iteration has run");
+    const size_t hist_n = static_cast<size_t>(ctx->nch) * ctx->ndims * ctx->bins;
+    Arg ah, aa;
+    if ((rc = resolve(ctx, hist, sizeof(double) * hist_n, 0, false, ah))) return rc;
+    if ((rc = resolve(ctx, alpha_train, sizeof(double) * ctx->nch, 1, false, aa))) return rc;
+    if (hist) CK(cudaMemcpyAsync(ah.dev, ctx->hist.p, sizeof(double) * hist_n, cudaMemcpyDeviceToDevice, ctx->stream));
+    if (alpha_train)
+        CK(cudaMemcpyAsync(aa.dev, acc_train_ptr(ctx), sizeof(double) * ctx->nch,
+                           cudaMemcpyDeviceToDevice, ctx->stream));
+    if ((rc = finish_out(ctx, ah)) || (rc = finish_out(ctx, aa))) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHILI_OK;
+}
+
+int chili_gpu_generate(chili_ctx *ctx, int64_t n, uint64_t seed, uint64_t counter_base, double *mom, double *wgt,
+                       int32_t *ch) {
+    if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
+    int rc;
+    if ((rc = need_mc(ctx))) return rc;
+    if (!ctx->f_set) return fail(ctx, CHILI_ERR_STATE, "no integrand set");
+    if (n < 0) return fail(ctx, CHILI_ERR_INVALID_ARG, "n < 0");
+    if (n == 0) return CHILI_OK;
+    Arg am, aw, ac;
+    if ((rc = resolve(ctx, mom, sizeof(double) * n * ctx->n_ext * 4, 0, false, am))) return rc;
+    if ((rc = resolve(ctx, wgt, sizeof(double) * n, 1, false, aw))) return rc;
+    if ((rc = resolve(ctx, ch, sizeof(int32_t) * n, 2, false, ac))) return rc;
+    k_generate<<<grid_for(n, 128), 128, 0, ctx->stream>>>(
+        ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), alpha_ptr(ctx), cp_ptr(ctx), ctx->nch, ctx->ndims,
+        ctx->bins, ctx->n_ext, seed, counter_base, n, ctx->f_dev.as<IntegrandDesc>(), static_cast<double *>(am.dev),
+        static_cast<double *>(aw.dev), static_cast<int32_t *>(ac.dev));
+    LAUNCHED();
+    if ((rc = finish_out(ctx, am)) || (rc = finish_out(ctx, aw)) || (rc = finish_out(ctx, ac))) return rc;
+    return sync_if_host(ctx, {&am, &aw, &ac});
+}
+
+int chili_gpu_evaluate_batch(chili_ctx *ctx, int ch, const double *u, double *out, int64_t n) {
+    if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
+    int rc;
+    if ((rc = need_channels(ctx))) return rc;
+    if (!ctx->f_set) return fail(ctx, CHILI_ERR_STATE, "no integrand set");
+    if (ch < 0 || ch >= ctx->nch || !u || !out || n < 0) return fail(ctx, CHILI_ERR_INVALID_ARG, "bad argument");
+    if (n == 0) return CHILI_OK;
+    Arg au, ao;
+    if ((rc = resolve(ctx, u, sizeof(double) * n * ctx->ndims, 0, true, au))) return rc;
+    if ((rc = resolve(ctx, out, sizeof(double) * n, 1, false, ao))) return rc;
+    k_evaluate_batch<<<grid_for(n, 128), 128, 0, ctx->stream>>>(ctx->progs.as<ChannelProgram>() + ch,
+                                                                static_cast<const double *>(au.dev),
+                                                                static_cast<double *>(ao.dev), n,
+                                                                ctx->f_dev.as<IntegrandDesc>());
+    LAUNCHED();
+    if ((rc = finish_out(ctx, ao))) return rc;
+    return sync_if_host(ctx, {&au, &ao});
+}
+
+}  // extern "C"

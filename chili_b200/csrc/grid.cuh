@@ -1,0 +1,104 @@
+// grid.cuh -- device form of chili::AdaptiveMap (VEGAS grid).
+//
+// A grid set holds nch grids of `dims` x (bins+1) edges, each grid in the
+// reference layout edges[dim*(bins+1) + k] (AdaptiveMap.hh:29-40), grids back
+// to back.  The forward map and the bin search use explicitly rounded
+// multiply/add so that x, J and bin indices are bit-identical to the
+// reference's (compiled without FMA contraction) for identical inputs.
+#pragma once
+
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace chili_dev {
+
+// std::lower_bound over edges[0..bins) with libstdc++'s probe sequence, then
+// "- 1" as in AdaptiveMap::FindBin (AdaptiveMap.cc:34-38).  Returns -1 where
+// the reference returns SIZE_MAX (x <= edges[0] or x NaN).
+__device__ __forceinline__ int find_bin(const double *__restrict__ e, int bins, double x) {
+    int first = 0, len = bins;
+    while (len > 0) {
+        const int half = len >> 1;
+        const int mid = first + half;
+        if (__ldg(e + mid) < x) {
+            first = mid + 1;
+            len = len - half - 1;
+        } else {
+            len = half;
+        }
+    }
+    return first - 1;
+}
+
+// The 8 bytes before the reference's edge table.  AdaptiveMap::width(0,
+// SIZE_MAX) reads m_hist[-1]; under glibc malloc that is the size word of the
+// vector's heap chunk: (8*dims*(bins+1) + 8) rounded up to 16, with the
+// PREV_INUSE bit set (mmapped chunks, from 128 KiB up, round to pages and set
+// IS_MMAPPED).  As a double it is a positive denormal; whether a channel's
+// term then overflows to -inf or stays finite depends on its exact value, so
+// the host computes it per grid shape (edge_before_table()).
+__host__ __device__ inline double edge_before_table(int dims, int bins) {
+    const unsigned long long req = 8ull * static_cast<unsigned long long>(dims) * (bins + 1);
+    unsigned long long word;
+    if (req + 8 >= 128ull * 1024) word = ((req + 16 + 4095) & ~4095ull) | 2ull;
+    else word = (std::max(32ull, (req + 8 + 15) & ~15ull)) | 1ull;
+    union {
+        unsigned long long u;
+        double d;
+    } cv;
+    cv.u = word;
+    return cv.d;
+}
+
+// width(dim, bin) of the flat edge table, including the reference's reading
+// of bin == SIZE_MAX: lower_edge at flat index dim*(bins+1) - 1 (the previous
+// dimension's last edge, or the word before the table for dim 0).
+__device__ __forceinline__ double bin_width(const double *__restrict__ g, int bins, int dim, int bin,
+                                            double before) {
+    const int base = dim * (bins + 1);
+    if (bin >= 0) return __dsub_rn(__ldg(g + base + bin + 1), __ldg(g + base + bin));
+    const double lower = dim > 0 ? __ldg(g + base - 1) : before;
+    return __dsub_rn(__ldg(g + base), lower);
+}
+
+// AdaptiveMap::operator() (AdaptiveMap.cc:40-56) on one point: x in place,
+// returns the Jacobian.
+__device__ __forceinline__ double grid_map(const double *__restrict__ g, int dims, int bins, double *x) {
+    double jac = 1.0;
+    const double fb = static_cast<double>(bins);
+    for (int d = 0; d < dims; ++d) {
+        const double pos = __dmul_rn(x[d], fb);
+        const int idx = static_cast<int>(pos);
+        const double loc = __dsub_rn(pos, static_cast<double>(idx));
+        const double *e = g + d * (bins + 1);
+        const double left = __ldg(e + idx);
+        const double size = __dsub_rn(__ldg(e + idx + 1), left);
+        x[d] = __dadd_rn(left, __dmul_rn(loc, size));
+        jac = __dmul_rn(jac, __dmul_rn(size, fb));
+    }
+    return jac;
+}
+
+// AdaptiveMap::GenerateWeight (AdaptiveMap.cc:58-65).
+__device__ __forceinline__ double grid_weight(const double *__restrict__ g, int dims, int bins,
+                                              const double *x, double before) {
+    double jac = 1.0;
+    const double fb = static_cast<double>(bins);
+    for (int d = 0; d < dims; ++d) {
+        const int b = find_bin(g + d * (bins + 1), bins, x[d]);
+        jac = __dmul_rn(jac, __dmul_rn(bin_width(g, bins, d, b, before), fb));
+    }
+    return jac;
+}
+
+// Flat histogram slot of dimension d's bin b the way Integrand::AddTrainData
+// and Vegas::operator() index it (train[d*bins + FindBin]); a FindBin of
+// SIZE_MAX wraps to d*bins - 1, which for d == 0 lies before the histogram:
+// that slot is reported as -1 (skipped).
+__device__ __forceinline__ int train_slot(int d, int bins, int b) {
+    const int s = d * bins + b;
+    return s;  // b == -1 and d == 0 gives -1
+}
+
+}  // namespace chili_dev

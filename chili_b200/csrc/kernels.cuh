@@ -1,0 +1,820 @@
+// kernels.cuh -- the sm_100a kernels of libchili_b200.
+//
+// Plain VEGAS (Vegas::operator(), src/Integrator/Vegas.cc:18-52) runs as one
+// fused kernel: counter-based uniforms -> grid map -> integrand -> StatsData
+// partials and the per-bin f^2 J^2 histogram in shared memory.
+//
+// A multichannel iteration (MultiChannel::operator(),
+// include/Channel/MultiChannel.hh:196-251) runs in rounds over contiguous
+// counter ranges, so that the retry semantics of the sequential loop (points
+// are tried in order until ncalls are accepted) hold exactly:
+//   k_mc_forward   uniforms -> channel choice -> VEGAS map -> FSMapper
+//                  forward -> PreProcess flag, momenta kept in HBM (SoA)
+//   k_mc_scan      accepted count per block -> cut position of the
+//                  `needed`-th accepted point
+//   k_mc_compact   ordered list of accepted points before the cut
+//   k_mc_weight    every channel's inverse map + grid weight -> combined
+//                  weight, integrand, StatsData, channel histograms, alpha
+//                  training terms (block partials)
+//   k_mc_finalize  ordered fold of the block partials into the iteration
+//                  accumulator; PreProcess rejections count as zero calls
+// Points whose value is NaN are retried (MultiChannel.hh:230-236), so the host
+// runs further rounds until ncalls points are accepted.
+#pragma once
+
+#include "channel_program.h"
+#include "common.cuh"
+#include "fsmapper.cuh"
+#include "grid.cuh"
+#include "integrands.cuh"
+
+namespace chili_dev {
+
+constexpr int kFwdBlock = 256;
+constexpr int kWgtBlock = 128;
+constexpr int kVegasBlock = 256;
+
+// Iteration accumulator of a multichannel iteration (device resident).
+struct IterAcc {
+    double st[6];      // n, min, max, sum, sum2, n_finite
+    double nan_count;  // NaN-value retries
+    double nonfinite;  // dropped alpha-training terms (guard mode)
+    double wmax;       // max value
+    double dropped;    // histogram adds before the histogram (dim 0, FindBin SIZE_MAX)
+    double rejected_pre;
+    double pad;
+    double atrain[CHILI_MAX_CHANNELS];
+};
+
+// Round control written by k_mc_scan / k_mc_finalize, read by the host.
+struct RoundCtl {
+    long long cut;        // counters consumed by this round
+    long long n_acc;      // PreProcess-accepted points before the cut
+    long long nan_round;  // of those, NaN retries
+    long long pad;
+};
+
+constexpr int kPartFixed = 10;  // n, min, max, sum, sum2, nfin, nan, nonfin, wmax, dropped
+
+// libstdc++ lower_bound over cp[0..n) (probe order of bits/stl_algobase.h).
+__device__ __forceinline__ int lower_bound_d(const double *__restrict__ a, int n, double v) {
+    int first = 0, len = n;
+    while (len > 0) {
+        const int half = len >> 1;
+        const int mid = first + half;
+        if (__ldg(a + mid) < v) {
+            first = mid + 1;
+            len = len - half - 1;
+        } else {
+            len = half;
+        }
+    }
+    return first;
+}
+
+// Random::SelectIndex == std::discrete_distribution (Random.hh:43-45): the
+// index of the first cumulative probability not below v.
+__device__ __forceinline__ int select_channel(const double *__restrict__ cp, int nch, double v) {
+    if (nch < 2) return 0;
+    const int i = lower_bound_d(cp, nch, v);
+    return i < nch ? i : nch - 1;
+}
+
+// Forward grid map with the bin index checked: returns false (x untouched
+// beyond the failing dimension) when a uniform is outside [0, 1).
+__device__ __forceinline__ bool grid_map_checked(const double *__restrict__ g, int dims, int bins, double *x,
+                                                 double &jac) {
+    jac = 1.0;
+    const double fb = static_cast<double>(bins);
+    for (int d = 0; d < dims; ++d) {
+        const double pos = __dmul_rn(x[d], fb);
+        if (!(pos >= 0.0 && pos < fb)) return false;
+        const int idx = static_cast<int>(pos);
+        const double loc = __dsub_rn(pos, static_cast<double>(idx));
+        const double *e = g + d * (bins + 1);
+        const double left = __ldg(e + idx);
+        const double size = __dsub_rn(__ldg(e + idx + 1), left);
+        x[d] = __dadd_rn(left, __dmul_rn(loc, size));
+        jac = __dmul_rn(jac, __dmul_rn(size, fb));
+    }
+    return true;
+}
+
+__device__ __forceinline__ void load_uniforms(uint64_t seed, uint64_t k, const double *__restrict__ u_in,
+                                              int n, double *out) {
+    if (u_in) {
+        for (int j = 0; j < n; ++j) out[j] = __ldg(u_in + k * n + j);
+    } else {
+        for (int q = 0; 2 * q < n; ++q) {
+            double a, b;
+            uniform_pair(seed, k, kStreamPoints, static_cast<uint32_t>(q), a, b);
+            out[2 * q] = a;
+            if (2 * q + 1 < n) out[2 * q + 1] = b;
+        }
+    }
+}
+
+// ------------------------------------------------------------- grid kernels
+__global__ void k_grid_map(const double *__restrict__ g, int dims, int bins, const double *__restrict__ u,
+                           double *__restrict__ x, double *__restrict__ jac, long long n) {
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    double r[CHILI_MAX_DIMS];
+    for (int d = 0; d < dims; ++d) r[d] = u[i * dims + d];
+    double j;
+    if (!grid_map_checked(g, dims, bins, r, j)) {
+        for (int d = 0; d < dims; ++d) r[d] = CUDART_NAN;
+        j = CUDART_NAN;
+    }
+    for (int d = 0; d < dims; ++d) x[i * dims + d] = r[d];
+    jac[i] = j;
+}
+
+__global__ void k_grid_weight(const double *__restrict__ g, int dims, int bins, const double *__restrict__ x,
+                              double *__restrict__ w, int32_t *__restrict__ bin, long long n) {
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    double jac = 1.0;
+    const double fb = static_cast<double>(bins);
+    for (int d = 0; d < dims; ++d) {
+        const int b = find_bin(g + d * (bins + 1), bins, x[i * dims + d]);
+        if (bin) bin[i * dims + d] = b;
+        jac = __dmul_rn(jac, __dmul_rn(bin_width(g, bins, d, b, edge_before_table(dims, bins)), fb));
+    }
+    if (w) w[i] = jac;
+}
+
+// AdaptiveMap::Adapt (AdaptiveMap.cc:67-125) for grid blockIdx.y, dimension
+// blockIdx.x: smoothing and importance factors in parallel over bins, the
+// order-dependent sums and the rebinning serially in lane 0, in the
+// reference's order.  With skip_zero, grids whose whole histogram is zero
+// are copied unchanged (Integrand::Train, Integrand.hh:97-104).
+// status bit 1: the rebinning ran past the last bin or before the first.
+__global__ void k_grid_adapt(const double *__restrict__ g_old, double *__restrict__ g_new, int dims, int bins,
+                             double alpha, const double *__restrict__ train, int skip_zero,
+                             int *__restrict__ status) {
+    extern __shared__ double tmp[];  // bins
+    const int d = blockIdx.x, c = blockIdx.y;
+    const double *T = train + static_cast<size_t>(c) * dims * bins;
+    const double *E = g_old + static_cast<size_t>(c) * dims * (bins + 1);
+    double *EN = g_new + static_cast<size_t>(c) * dims * (bins + 1);
+    const double *Ed = E + d * (bins + 1);
+    double *ENd = EN + d * (bins + 1);
+    if (skip_zero) {
+        int nz = 0;
+        for (int k = threadIdx.x; k < dims * bins; k += blockDim.x) nz |= (T[k] != 0);
+        nz = __syncthreads_or(nz);
+        if (!nz) {
+            for (int k = threadIdx.x; k <= bins; k += blockDim.x) ENd[k] = Ed[k];
+            return;
+        }
+    }
+    const double *o = T + d * bins;
+    for (int b = threadIdx.x; b < bins; b += blockDim.x) {
+        double s;
+        if (b == 0) s = (o[0] + o[1]) / 2;
+        else if (b == bins - 1) s = (o[bins - 2] + o[bins - 1]) / 2;
+        else s = ((o[b - 1] + o[b]) + o[b + 1]) / 3;
+        tmp[b] = s;
+    }
+    __syncthreads();
+    __shared__ double norm_s;
+    if (threadIdx.x == 0) {
+        double norm = 0;
+        for (int b = 0; b < bins; ++b) norm = (b == 0) ? tmp[0] : norm + tmp[b];
+        norm_s = norm;
+    }
+    __syncthreads();
+    const double norm = norm_s;
+    if (norm == 0) {  // the reference leaves this dimension of new_hist at zero
+        for (int k = threadIdx.x; k <= bins; k += blockDim.x) ENd[k] = 0.0;
+        return;
+    }
+    for (int b = threadIdx.x; b < bins; b += blockDim.x) {
+        if (tmp[b] != 0) {
+            const double r = tmp[b] / norm;
+            tmp[b] = pow((r - 1.0) / log(r), alpha);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double avg = 0;
+        for (int b = 0; b < bins; ++b) avg += tmp[b];
+        avg /= static_cast<double>(bins);
+        double cbin = 0;
+        int ibin = 0;
+        int bad = 0;
+        const double nan = CUDART_NAN;
+        ENd[0] = 0.0;
+        for (int nb = 1; nb < bins; ++nb) {
+            while (cbin < avg && ibin < bins) cbin += tmp[ibin++];
+            if (cbin < avg) bad = 1;  // the reference would read past the histogram
+            const int flat_prev = d * (bins + 1) + ibin - 1;
+            const double prev = flat_prev >= 0 ? E[flat_prev] : nan;
+            const double curr = Ed[ibin];
+            if (ibin == 0) bad = 1;
+            cbin -= avg;
+            const double delta = (curr - prev) * cbin;
+            const double t = ibin > 0 ? tmp[ibin - 1] : nan;
+            ENd[nb] = curr - delta / t;
+        }
+        ENd[bins] = 1.0;
+        if (bad) atomicOr(status, 1);
+    }
+}
+
+// AdaptiveMap::Split (AdaptiveMap.cc:127-160) of every grid.
+__global__ void k_grid_split(const double *__restrict__ g_old, double *__restrict__ g_new, int ngrids, int dims,
+                             int bins, int nsplit) {
+    const long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    const long long total = static_cast<long long>(ngrids) * dims * bins;
+    if (t >= total) return;
+    const int bin = static_cast<int>(t % bins);
+    const long long gd = t / bins;  // grid*dims + dim
+    const int nb = nsplit * bins;
+    const double *e = g_old + gd * (bins + 1);
+    double *en = g_new + gd * (nb + 1);
+    const double curr = e[bin];
+    const double size = __dsub_rn(e[bin + 1], curr);
+    for (int i = 0; i < nsplit; ++i)
+        en[bin * nsplit + i] = __dadd_rn(curr, __ddiv_rn(__dmul_rn(static_cast<double>(i), size),
+                                                          static_cast<double>(nsplit)));
+    if (bin == bins - 1) en[nb] = 1.0;
+}
+
+// ------------------------------------------------------------- plain VEGAS
+// One Vegas::operator() over n points (grid-stride).  Histogram in shared
+// memory when it fits (smem_hist), else global atomics into hist.
+__global__ void k_vegas_iter(const double *__restrict__ g, int dims, int bins, uint64_t seed, uint64_t ctr0,
+                             const double *__restrict__ u_in, long long n, const IntegrandDesc *__restrict__ f,
+                             double *__restrict__ part, double *__restrict__ hist, int smem_hist) {
+    extern __shared__ double sh[];
+    const int nh = dims * bins;
+    if (smem_hist)
+        for (int k = threadIdx.x; k < nh; k += blockDim.x) sh[k] = 0.0;
+    __syncthreads();
+    double* H = smem_hist ? sh : hist;
+    double cnt = 0, sum = 0, sum2 = 0, mn = 1.7976931348623157e308, mx = 2.2250738585072014e-308, nf = 0;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        double r[CHILI_MAX_DIMS];
+        if (u_in) {
+            for (int d = 0; d < dims; ++d) r[d] = __ldg(u_in + i * dims + d);
+        } else {
+            load_uniforms(seed, ctr0 + i, nullptr, dims, r);
+        }
+        double jac;
+        double val;
+        if (grid_map_checked(g, dims, bins, r, jac)) val = camel(f, r, dims) * jac;
+        else val = CUDART_NAN;
+        const double val2 = val * val;
+        cnt += 1;
+        sum += val;
+        sum2 += val * val;
+        mn = std_min(mn, val);
+        mx = std_max(mx, val);
+        nf += (val != 0);
+        for (int j = 0; j < dims; ++j) {
+            const int b = find_bin(g + j * (bins + 1), bins, r[j]);
+            const int s = j * bins + b;
+            if (s >= 0) atomicAdd(H + s, val2);
+        }
+    }
+    cnt = warp_sum(cnt);
+    sum = warp_sum(sum);
+    sum2 = warp_sum(sum2);
+    mn = warp_min(mn);
+    mx = warp_max(mx);
+    nf = warp_sum(nf);
+    __shared__ double ws[32][6];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+        ws[w][0] = cnt; ws[w][1] = mn; ws[w][2] = mx; ws[w][3] = sum; ws[w][4] = sum2; ws[w][5] = nf;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a[6] = {ws[0][0], ws[0][1], ws[0][2], ws[0][3], ws[0][4], ws[0][5]};
+        for (int k = 1; k < (blockDim.x >> 5); ++k) {
+            a[0] += ws[k][0]; a[1] = std_min(a[1], ws[k][1]); a[2] = std_max(a[2], ws[k][2]);
+            a[3] += ws[k][3]; a[4] += ws[k][4]; a[5] += ws[k][5];
+        }
+        for (int k = 0; k < 6; ++k) part[blockIdx.x * 6 + k] = a[k];
+    }
+    if (smem_hist) {
+        double *dst = hist + static_cast<size_t>(blockIdx.x) * nh;
+        for (int k = threadIdx.x; k < nh; k += blockDim.x) dst[k] = sh[k];
+    }
+}
+
+// Ordered fold of k_vegas_iter's partials: stats into out6, histogram
+// partials (when per block) into train[dims*bins].
+__global__ void k_vegas_finalize(const double *__restrict__ part, int nblocks, const double *__restrict__ hist_part,
+                                 int per_block_hist, int nh, double *__restrict__ train, double *__restrict__ out6) {
+    if (per_block_hist) {
+        for (int k = threadIdx.x; k < nh; k += blockDim.x) {
+            double s = 0;
+            for (int b = 0; b < nblocks; ++b) s += hist_part[static_cast<size_t>(b) * nh + k];
+            train[k] = s;
+        }
+    }
+    if (threadIdx.x == 0) {
+        double n = 0, mn = 1.7976931348623157e308, mx = 2.2250738585072014e-308, sum = 0, csum = 0, sum2 = 0,
+               csum2 = 0, nf = 0;
+        for (int b = 0; b < nblocks; ++b) {
+            const double *p = part + b * 6;
+            n += p[0];
+            mn = std_min(mn, p[1]);
+            mx = std_max(mx, p[2]);
+            double y = p[3] - csum, t = sum + y;  // Kahan
+            csum = (t - sum) - y;
+            sum = t;
+            y = p[4] - csum2;
+            t = sum2 + y;
+            csum2 = (t - sum2) - y;
+            sum2 = t;
+            nf += p[5];
+        }
+        out6[0] = n; out6[1] = mn; out6[2] = mx; out6[3] = sum; out6[4] = sum2; out6[5] = nf;
+    }
+}
+
+// ------------------------------------------------------------- channels
+__global__ void k_fs_generate(const ChannelProgram *__restrict__ prog, const double *__restrict__ x,
+                              double *__restrict__ mom, long long n) {
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    const int nd = prog->ndims, ne = prog->n_ext;
+    double r[CHILI_MAX_DIMS];
+    for (int d = 0; d < nd; ++d) r[d] = x[i * nd + d];
+    V4 m[CHILI_MAX_SLOTS];
+    double m2[CHILI_MAX_SLOTS];
+    fs_generate(prog, r, m, m2);
+    for (int k = 0; k < ne; ++k) {
+        double *o = mom + (i * ne + k) * 4;
+        o[0] = m[k].e; o[1] = m[k].x; o[2] = m[k].y; o[3] = m[k].z;
+    }
+}
+
+__global__ void k_fs_weight(const ChannelProgram *__restrict__ prog, const double *__restrict__ mom,
+                            double *__restrict__ x_out, double *__restrict__ w, long long n) {
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    const int nd = prog->ndims, ne = prog->n_ext;
+    V4 m[CHILI_MAX_SLOTS];
+    for (int k = 0; k < ne; ++k) {
+        const double *q = mom + (i * ne + k) * 4;
+        m[k] = V4{q[0], q[1], q[2], q[3]};
+    }
+    double r[CHILI_MAX_DIMS];
+    for (int d = 0; d < nd; ++d) r[d] = 0.0;  // the reference's rans start zeroed
+    const double wt = fs_weight(prog, m, r);
+    w[i] = wt;
+    if (x_out)
+        for (int d = 0; d < nd; ++d) x_out[i * nd + d] = r[d];
+}
+
+__global__ void k_select(const double *__restrict__ cp, int nch, const double *__restrict__ v,
+                         int32_t *__restrict__ out, long long n) {
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    out[i] = select_channel(cp, nch, v[i]);
+}
+
+// Integrand::GenerateWeight (Integrand.hh:112-123) for one point.  The
+// uniform buffer x is shared by all channels and not cleared between them,
+// as the reference's _rans; the chosen channel's copy lands in xs.
+__device__ __forceinline__ double combined_weight(const ChannelProgram *__restrict__ progs,
+                                                  const double *__restrict__ grids, const double *__restrict__ alpha,
+                                                  int nch, int dims, int bins, int ich, V4 *mom, double *x,
+                                                  double *xs, double *dens, int dens_stride) {
+    for (int d = 0; d < dims; ++d) x[d] = 0.0;
+    double acc = 0;
+    const size_t gsz = static_cast<size_t>(dims) * (bins + 1);
+    const double before = edge_before_table(dims, bins);
+    for (int c = 0; c < nch; ++c) {
+        const double dc = fs_weight(progs + c, mom, x);
+        if (c == ich)
+            for (int d = 0; d < dims; ++d) xs[d] = x[d];
+        const double vw = grid_weight(grids + c * gsz, dims, bins, x, before);
+        acc += __ldg(alpha + c) / dc / vw;
+        if (dens) dens[c * dens_stride] = dc;
+    }
+    return 1.0 / acc;
+}
+
+__global__ void k_mc_weight_batch(const ChannelProgram *__restrict__ progs, const double *__restrict__ grids,
+                                  const double *__restrict__ alpha, int nch, int dims, int bins, int n_ext,
+                                  const double *__restrict__ mom, const int32_t *__restrict__ ich,
+                                  double *__restrict__ wgt, double *__restrict__ dens, double *__restrict__ x_ich,
+                                  long long n) {
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    V4 m[CHILI_MAX_SLOTS];
+    for (int k = 0; k < n_ext; ++k) {
+        const double *q = mom + (i * n_ext + k) * 4;
+        m[k] = V4{q[0], q[1], q[2], q[3]};
+    }
+    double x[CHILI_MAX_DIMS], xs[CHILI_MAX_DIMS];
+    for (int d = 0; d < dims; ++d) xs[d] = 0.0;
+    const int c = ich[i];
+    const double w = combined_weight(progs, grids, alpha, nch, dims, bins, (c >= 0 && c < nch) ? c : -1, m, x,
+                                     xs, dens ? dens + i * nch : nullptr, 1);
+    wgt[i] = w;
+    if (x_ich)
+        for (int d = 0; d < dims; ++d) x_ich[i * dims + d] = xs[d];
+}
+
+// ------------------------------------------------------------- multichannel
+__global__ void __launch_bounds__(kFwdBlock) k_mc_forward(
+    const ChannelProgram *__restrict__ progs, const double *__restrict__ grids, const double *__restrict__ cp,
+    int nch, int dims, int bins, uint64_t seed, uint64_t ctr0, const double *__restrict__ u_in, long long m,
+    const IntegrandDesc *__restrict__ f, int n_ext, double *__restrict__ mom_soa, int32_t *__restrict__ ich_out,
+    uint8_t *__restrict__ flag, int32_t *__restrict__ block_count) {
+    const long long k = blockIdx.x * static_cast<long long>(kFwdBlock) + threadIdx.x;
+    int acc = 0;
+    if (k < m) {
+        double r[CHILI_MAX_DIMS + 1];
+        if (u_in) {
+            for (int j = 0; j <= dims; ++j) r[j] = __ldg(u_in + k * (dims + 1) + j);
+        } else {
+            load_uniforms(seed, ctr0 + k, nullptr, dims + 1, r);
+        }
+        const int c = select_channel(cp, nch, r[dims]);
+        const double *g = grids + static_cast<size_t>(c) * dims * (bins + 1);
+        double jac;
+        V4 mom[CHILI_MAX_SLOTS];
+        double m2[CHILI_MAX_SLOTS];
+        if (grid_map_checked(g, dims, bins, r, jac)) {
+            fs_generate(progs + c, r, mom, m2);
+        } else {
+            for (int s = 0; s < n_ext; ++s) mom[s] = V4{CUDART_NAN, CUDART_NAN, CUDART_NAN, CUDART_NAN};
+        }
+        acc = preprocess(f, mom) ? 1 : 0;
+        if (acc) {
+            for (int s = 0; s < n_ext; ++s) {
+                mom_soa[(4 * s + 0) * m + k] = mom[s].e;
+                mom_soa[(4 * s + 1) * m + k] = mom[s].x;
+                mom_soa[(4 * s + 2) * m + k] = mom[s].y;
+                mom_soa[(4 * s + 3) * m + k] = mom[s].z;
+            }
+        }
+        ich_out[k] = c;
+        flag[k] = static_cast<uint8_t>(acc);
+    }
+    const int cnt = __syncthreads_count(acc);
+    if (threadIdx.x == 0) block_count[blockIdx.x] = cnt;
+}
+
+// One block of 1024 threads: exclusive scan of the per-block accepted counts
+// and the cut at the `needed`-th accepted point.
+__global__ void __launch_bounds__(1024) k_mc_scan(const int32_t *__restrict__ block_count, int nb,
+                                                  const uint8_t *__restrict__ flag, long long m, long long needed,
+                                                  long long *__restrict__ block_off, RoundCtl *__restrict__ ctl) {
+    __shared__ long long wsum[32];
+    __shared__ long long running_s;
+    __shared__ int cut_block_s;
+    __shared__ long long cut_off_s;
+    if (threadIdx.x == 0) {
+        running_s = 0;
+        cut_block_s = -1;
+        cut_off_s = 0;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int base = 0; base < nb; base += 1024) {
+        const int i = base + threadIdx.x;
+        const long long c = i < nb ? block_count[i] : 0;
+        long long incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) wsum[w] = incl;
+        __syncthreads();
+        if (w == 0) {
+            long long v = wsum[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const long long t = __shfl_up_sync(0xffffffffu, v, o);
+                if (lane >= o) v += t;
+            }
+            wsum[lane] = v;  // inclusive warp totals
+        }
+        __syncthreads();
+        const long long warp_excl = w > 0 ? wsum[w - 1] : 0;
+        const long long off = running_s + warp_excl + incl - c;
+        if (i < nb) {
+            block_off[i] = off;
+            if (off < needed && needed <= off + c) {
+                cut_block_s = i;
+                cut_off_s = off;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) running_s += wsum[31];
+        __syncthreads();
+    }
+    const long long total = running_s;
+    if (cut_block_s < 0) {
+        if (threadIdx.x == 0) {
+            ctl->cut = m;
+            ctl->n_acc = total;
+        }
+        return;
+    }
+    // position of the r-th accepted point inside the cut block
+    const long long r = needed - cut_off_s;
+    const long long k = static_cast<long long>(cut_block_s) * kFwdBlock + threadIdx.x;
+    int f = 0;
+    if (threadIdx.x < kFwdBlock && k < m) f = flag[k];
+    long long incl = f;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    __syncthreads();
+    if (lane == 31) wsum[w] = incl;
+    __syncthreads();
+    long long pre = 0;
+    for (int q = 0; q < w; ++q) pre += wsum[q];
+    incl += pre;
+    if (threadIdx.x < kFwdBlock && f && incl == r) {
+        ctl->cut = k + 1;
+        ctl->n_acc = needed;
+    }
+}
+
+__global__ void __launch_bounds__(kFwdBlock) k_mc_compact(const uint8_t *__restrict__ flag,
+                                                          const long long *__restrict__ block_off,
+                                                          const RoundCtl *__restrict__ ctl, long long m,
+                                                          int32_t *__restrict__ list) {
+    const long long k = blockIdx.x * static_cast<long long>(kFwdBlock) + threadIdx.x;
+    const long long cut = ctl->cut;
+    const int a = (k < m && k < cut) ? flag[k] : 0;
+    const unsigned ballot = __ballot_sync(0xffffffffu, a);
+    __shared__ int wc[kFwdBlock / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) wc[w] = __popc(ballot);
+    __syncthreads();
+    int pre = 0;
+    for (int q = 0; q < w; ++q) pre += wc[q];
+    if (a) {
+        const long long pos = block_off[blockIdx.x] + pre + __popc(ballot & ((1u << lane) - 1u));
+        list[pos] = static_cast<int32_t>(k);
+    }
+}
+
+// The expensive pass: combined weight, integrand and training data of the
+// accepted points list[0..n_acc).  Dynamic shared memory: dens[nch][block]
+// then alpha-training per warp [nwarps][nch].
+__global__ void __launch_bounds__(kWgtBlock) k_mc_weight(
+    const ChannelProgram *__restrict__ progs, const double *__restrict__ grids, const double *__restrict__ alpha,
+    int nch, int dims, int bins, int n_ext, const double *__restrict__ mom_soa, long long m,
+    const int32_t *__restrict__ ich_arr, const int32_t *__restrict__ list, const RoundCtl *__restrict__ ctl,
+    const IntegrandDesc *__restrict__ f, int should_opt, int guard, double *__restrict__ hist,
+    double *__restrict__ part) {
+    extern __shared__ double sh[];
+    double *dens_s = sh;                    // nch * kWgtBlock
+    double *atr_s = sh + nch * kWgtBlock;   // (kWgtBlock/32) * nch
+    const long long n_list = ctl->n_acc;
+    const long long i = blockIdx.x * static_cast<long long>(kWgtBlock) + threadIdx.x;
+    const bool active = i < n_list;
+    double val = 0, wgt = 0;
+    double cnt = 0, nan_cnt = 0, dropped = 0;
+    if (active) {
+        const long long k = list[i];
+        const int c_sel = ich_arr[k];
+        V4 mom[CHILI_MAX_SLOTS];
+        for (int s = 0; s < n_ext; ++s)
+            mom[s] = V4{mom_soa[(4 * s + 0) * m + k], mom_soa[(4 * s + 1) * m + k], mom_soa[(4 * s + 2) * m + k],
+                        mom_soa[(4 * s + 3) * m + k]};
+        double x[CHILI_MAX_DIMS], xs[CHILI_MAX_DIMS];
+        wgt = combined_weight(progs, grids, alpha, nch, dims, bins, c_sel, mom, x, xs, dens_s + threadIdx.x,
+                              kWgtBlock);
+        const double fv = eval_momenta(f, mom, n_ext);
+        val = wgt == 0 ? 0 : fv * wgt;
+        if (isnan(val)) {
+            val = wgt = 0;
+            nan_cnt = 1;
+        }
+        cnt = 1;
+        if (should_opt) {
+            const double val2 = val * val;
+            const double *g = grids + static_cast<size_t>(c_sel) * dims * (bins + 1);
+            double *H = hist + static_cast<size_t>(c_sel) * dims * bins;
+            for (int j = 0; j < dims; ++j) {
+                const int b = find_bin(g + j * (bins + 1), bins, xs[j]);
+                const int s = j * bins + b;
+                if (s >= 0) atomicAdd(H + s, val2);
+                else dropped += 1;
+            }
+        }
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double nonfin = 0;
+    if (should_opt) {
+        const double val2 = val * val;
+        for (int j = 0; j < nch; ++j) {
+            double term = active ? val2 * wgt / dens_s[j * kWgtBlock + threadIdx.x] : 0.0;
+            if (guard && !isfinite(term)) {
+                nonfin += 1;
+                term = 0.0;
+            }
+            term = warp_sum(term);
+            if (lane == 0) atr_s[w * nch + j] = term;
+        }
+    }
+    double sum = warp_sum(val), sum2 = warp_sum(val * val);
+    double mn = warp_min(active ? val : 1.7976931348623157e308);
+    double mx = warp_max(active ? val : 2.2250738585072014e-308);
+    cnt = warp_sum(cnt);
+    double nf = warp_sum((active && val != 0) ? 1.0 : 0.0);
+    nan_cnt = warp_sum(nan_cnt);
+    nonfin = warp_sum(nonfin);
+    dropped = warp_sum(dropped);
+    double wm = warp_max(active ? val : 0.0);
+    __shared__ double ws[kWgtBlock / 32][kPartFixed];
+    if (lane == 0) {
+        ws[w][0] = cnt; ws[w][1] = mn; ws[w][2] = mx; ws[w][3] = sum; ws[w][4] = sum2;
+        ws[w][5] = nf; ws[w][6] = nan_cnt; ws[w][7] = nonfin; ws[w][8] = wm; ws[w][9] = dropped;
+    }
+    __syncthreads();
+    const int stride = kPartFixed + nch;
+    double *P = part + static_cast<size_t>(blockIdx.x) * stride;
+    if (threadIdx.x == 0) {
+        double a[kPartFixed];
+        for (int q = 0; q < kPartFixed; ++q) a[q] = ws[0][q];
+        for (int v = 1; v < kWgtBlock / 32; ++v) {
+            a[0] += ws[v][0]; a[1] = std_min(a[1], ws[v][1]); a[2] = std_max(a[2], ws[v][2]);
+            a[3] += ws[v][3]; a[4] += ws[v][4]; a[5] += ws[v][5]; a[6] += ws[v][6]; a[7] += ws[v][7];
+            a[8] = std_max(a[8], ws[v][8]); a[9] += ws[v][9];
+        }
+        for (int q = 0; q < kPartFixed; ++q) P[q] = a[q];
+    }
+    if (should_opt) {
+        for (int j = threadIdx.x; j < nch; j += kWgtBlock) {
+            double s = 0;
+            for (int v = 0; v < kWgtBlock / 32; ++v) s += atr_s[v * nch + j];
+            P[kPartFixed + j] = s;
+        }
+    }
+}
+
+// Ordered tree fold of k_mc_weight's partials: block f reduces field f
+// (kPartFixed statistics fields, then one alpha-training sum per channel)
+// over the round's blocks into round_res[f].
+__global__ void __launch_bounds__(256) k_mc_reduce(const double *__restrict__ part, int nch,
+                                                   const RoundCtl *__restrict__ ctl, double *__restrict__ round_res) {
+    const long long n_list = ctl->n_acc;
+    const long long nb = (n_list + kWgtBlock - 1) / kWgtBlock;
+    const int stride = kPartFixed + nch;
+    const int fld = blockIdx.x;
+    // 0 sum-like, 1 min, 2 max
+    const int op = (fld == 1) ? 1 : ((fld == 2 || fld == 8) ? 2 : 0);
+    const double ident = op == 1 ? 1.7976931348623157e308 : (op == 2 ? (fld == 2 ? 2.2250738585072014e-308 : 0.0) : 0.0);
+    double v = ident;
+    for (long long b = threadIdx.x; b < nb; b += blockDim.x) {
+        const double p = part[b * stride + fld];
+        v = op == 0 ? v + p : (op == 1 ? std_min(v, p) : std_max(v, p));
+    }
+    __shared__ double red[256];
+    red[threadIdx.x] = v;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            const double a = red[threadIdx.x], c = red[threadIdx.x + s];
+            red[threadIdx.x] = op == 0 ? a + c : (op == 1 ? std_min(a, c) : std_max(a, c));
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) round_res[fld] = red[0];
+}
+
+// Merge one round into the iteration accumulator; PreProcess rejections
+// before the cut count as zero-valued calls (MultiChannel.hh:219-223).
+__global__ void k_mc_accumulate(const double *__restrict__ round_res, int nch, RoundCtl *__restrict__ ctl,
+                                IterAcc *__restrict__ acc) {
+    for (int j = threadIdx.x; j < nch; j += blockDim.x) acc->atrain[j] += round_res[kPartFixed + j];
+    if (threadIdx.x != 0) return;
+    const long long rej = ctl->cut - ctl->n_acc;
+    double mn = std_min(acc->st[1], round_res[1]);
+    double mx = std_max(acc->st[2], round_res[2]);
+    if (rej > 0) {
+        mn = std_min(mn, 0.0);
+        mx = std_max(mx, 0.0);
+    }
+    acc->st[0] += round_res[0] + static_cast<double>(rej);
+    acc->st[1] = mn;
+    acc->st[2] = mx;
+    acc->st[3] += round_res[3];
+    acc->st[4] += round_res[4];
+    acc->st[5] += round_res[5];
+    acc->nan_count += round_res[6];
+    acc->nonfinite += round_res[7];
+    acc->wmax = std_max(acc->wmax, round_res[8]);
+    acc->dropped += round_res[9];
+    acc->rejected_pre += static_cast<double>(rej);
+    ctl->nan_round = static_cast<long long>(round_res[6]);
+}
+
+// MultiChannel::Adapt and MaxDifference (MultiChannel.cc:109-154), then the
+// cumulative table of std::discrete_distribution (libstdc++ _M_initialize:
+// normalise by the accumulated sum, partial_sum, last entry forced to 1).
+// mode 0: only rebuild cp from alpha.
+__global__ void k_alpha_update(double *__restrict__ alpha, double *__restrict__ best, double *__restrict__ min_diff,
+                               double *__restrict__ cp, const double *__restrict__ train, int nch, double beta,
+                               double min_alpha, int mode) {
+    if (threadIdx.x != 0) return;
+    if (mode == 1) {
+        double nw[CHILI_MAX_CHANNELS];
+        double sum_w = 0;
+        for (int i = 0; i < nch; ++i) {
+            nw[i] = alpha[i] * pow(train[i], beta);
+            sum_w += nw[i];
+        }
+        double new_sum = 0;
+        for (int i = 0; i < nch; ++i) {
+            if (nw[i] == 0) continue;
+            nw[i] /= sum_w;
+            nw[i] = std_max(nw[i], min_alpha);
+            new_sum += nw[i];
+        }
+        for (int i = 0; i < nch; ++i) alpha[i] = nw[i] / new_sum;
+        double mx = 0;
+        for (int i = 0; i + 1 < nch; ++i)
+            for (int j = i + 1; j < nch; ++j) mx = std_max(mx, fabs(train[i] - train[j]));
+        if (mx < *min_diff) {
+            for (int i = 0; i < nch; ++i) best[i] = alpha[i];
+            *min_diff = mx;
+        }
+    }
+    if (nch >= 2) {
+        double s = 0;
+        for (int i = 0; i < nch; ++i) s += alpha[i];
+        double c = 0;
+        for (int i = 0; i < nch; ++i) {
+            const double p = alpha[i] / s;
+            c = (i == 0) ? p : c + p;
+            cp[i] = c;
+        }
+        cp[nch - 1] = 1.0;
+    }
+}
+
+// Event generation: MultiChannel::GeneratePoint + GenerateWeight for n points.
+__global__ void k_generate(const ChannelProgram *__restrict__ progs, const double *__restrict__ grids,
+                           const double *__restrict__ alpha, const double *__restrict__ cp, int nch, int dims,
+                           int bins, int n_ext, uint64_t seed, uint64_t ctr0, long long n,
+                           const IntegrandDesc *__restrict__ f, double *__restrict__ mom_out,
+                           double *__restrict__ wgt_out, int32_t *__restrict__ ch_out) {
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    double r[CHILI_MAX_DIMS + 1];
+    load_uniforms(seed, ctr0 + i, nullptr, dims + 1, r);
+    const int c = select_channel(cp, nch, r[dims]);
+    double jac;
+    V4 mom[CHILI_MAX_SLOTS];
+    double m2[CHILI_MAX_SLOTS];
+    double w = 0;
+    if (grid_map_checked(grids + static_cast<size_t>(c) * dims * (bins + 1), dims, bins, r, jac)) {
+        fs_generate(progs + c, r, mom, m2);
+        double x[CHILI_MAX_DIMS], xs[CHILI_MAX_DIMS];
+        const double wt = combined_weight(progs, grids, alpha, nch, dims, bins, c, mom, x, xs, nullptr, 0);
+        const double fv = eval_momenta(f, mom, n_ext);
+        w = wt == 0 ? 0 : fv * wt;
+        if (!isfinite(w)) w = 0;
+    } else {
+        for (int s = 0; s < n_ext; ++s) mom[s] = V4{CUDART_NAN, CUDART_NAN, CUDART_NAN, CUDART_NAN};
+    }
+    if (mom_out)
+        for (int s = 0; s < n_ext; ++s) {
+            double *o = mom_out + (i * n_ext + s) * 4;
+            o[0] = mom[s].e; o[1] = mom[s].x; o[2] = mom[s].y; o[3] = mom[s].z;
+        }
+    if (wgt_out) wgt_out[i] = w;
+    if (ch_out) ch_out[i] = c;
+}
+
+// Interface::Evaluate (nanobind.hh:23-50): uniforms through one channel's
+// FSMapper, no grid.
+__global__ void k_evaluate_batch(const ChannelProgram *__restrict__ prog, const double *__restrict__ u,
+                                 double *__restrict__ out, long long n, const IntegrandDesc *__restrict__ f) {
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    const int nd = prog->ndims, ne = prog->n_ext;
+    double r[CHILI_MAX_DIMS];
+    for (int d = 0; d < nd; ++d) r[d] = u[i * nd + d];
+    V4 mom[CHILI_MAX_SLOTS];
+    double m2[CHILI_MAX_SLOTS];
+    fs_generate(prog, r, mom, m2);
+    if (!preprocess(f, mom)) {
+        out[i] = 0;
+        return;
+    }
+    const double w = fs_weight(prog, mom, r);
+    out[i] = w == 0 ? 0 : eval_momenta(f, mom, ne) * w;
+}
+
+}  // namespace chili_dev

@@ -1,0 +1,285 @@
+"""Python binding of libchili_b200 (include/chili_gpu.h) over ctypes.
+
+Arrays may be numpy arrays (host memory; staged by the library) or CUDA torch
+tensors (device memory; used in place).  Every call checks the returned status
+and raises ChiliError with the library's message.  There is no CPU fallback:
+without the built library or a CUDA device the calls raise.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libchili_b200.so")
+
+_lib = None
+
+
+class ChiliError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"chili_gpu error {code} ({abi.STATUS_NAMES.get(code, '?')}): {msg}")
+        self.code = code
+
+
+def _declare(lib):
+    vp, i32, i64, u64, dbl = C.c_void_p, C.c_int, C.c_int64, C.c_uint64, C.c_double
+    P = C.POINTER
+    sigs = {
+        "chili_gpu_create": ([i32, P(vp)], i32),
+        "chili_gpu_destroy": ([vp], i32),
+        "chili_gpu_last_error": ([vp], C.c_char_p),
+        "chili_gpu_set_stream": ([vp, vp], i32),
+        "chili_gpu_synchronize": ([vp], i32),
+        "chili_gpu_launch_count": ([vp], u64),
+        "chili_gpu_set_grids": ([vp, vp, i32, i32, i32], i32),
+        "chili_gpu_get_grids": ([vp, vp, i32, i32, i32], i32),
+        "chili_gpu_grid_map": ([vp, i32, vp, vp, vp, i64], i32),
+        "chili_gpu_grid_weight": ([vp, i32, vp, vp, vp, i64], i32),
+        "chili_gpu_grid_adapt": ([vp, i32, dbl, vp], i32),
+        "chili_gpu_grid_split": ([vp, i32], i32),
+        "chili_gpu_set_integrand": ([vp, i32, vp, i32], i32),
+        "chili_gpu_set_preprocess": ([vp, i32], i32),
+        "chili_gpu_vegas_iterate": ([vp, u64, u64, u64, vp, dbl, i32, vp, vp], i32),
+        "chili_gpu_set_channels": ([vp, P(abi.ChannelDesc), i32, P(abi.Cuts), dbl, i32], i32),
+        "chili_gpu_ndims": ([vp], i32),
+        "chili_gpu_fsmapper_generate": ([vp, i32, vp, vp, i64], i32),
+        "chili_gpu_fsmapper_weight": ([vp, i32, vp, vp, vp, i64], i32),
+        "chili_gpu_set_alpha": ([vp, vp, i32], i32),
+        "chili_gpu_get_alpha": ([vp, vp, vp, vp, i32], i32),
+        "chili_gpu_select_channel": ([vp, vp, vp, i64], i32),
+        "chili_gpu_multichannel_weight": ([vp, vp, vp, vp, vp, vp, i64], i32),
+        "chili_gpu_multichannel_iterate": ([vp, P(abi.MultiChannelParams), u64, u64, vp, i64, i32,
+                                            P(abi.Stats), P(abi.MCIterInfo)], i32),
+        "chili_gpu_get_training": ([vp, vp, vp], i32),
+        "chili_gpu_generate": ([vp, i64, u64, u64, vp, vp, vp], i32),
+        "chili_gpu_evaluate_batch": ([vp, i32, vp, vp, i64], i32),
+    }
+    for name, (args, res) in sigs.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    return sigs
+
+
+EXPORTED = None
+
+
+def load(path=LIB_PATH):
+    """Load the CUDA library (raises if it is missing)."""
+    global _lib, EXPORTED
+    if _lib is None:
+        if not os.path.exists(path):
+            raise ChiliError(abi.CHILI_ERR_STATE,
+                             f"{path} is not built; run `python -m chili_b200.build`")
+        lib = C.CDLL(path)
+        EXPORTED = sorted(_declare(lib))
+        _lib = lib
+    return _lib
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if not a.flags.c_contiguous:
+            raise ValueError("arrays must be C-contiguous")
+        return C.c_void_p(a.ctypes.data)
+    if hasattr(a, "data_ptr"):  # torch tensor
+        if not a.is_contiguous():
+            raise ValueError("tensors must be contiguous")
+        return C.c_void_p(a.data_ptr())
+    raise TypeError(f"unsupported buffer type {type(a)}")
+
+
+def _f64(a):
+    return None if a is None else (np.ascontiguousarray(a, dtype=np.float64) if isinstance(a, (np.ndarray, list, tuple)) else a)
+
+
+class Context:
+    """One chili_ctx: a device, a stream, grids, channels and an integrand."""
+
+    def __init__(self, device=0):
+        self.lib = load()
+        h = C.c_void_p()
+        self._check(self.lib.chili_gpu_create(device, C.byref(h)), None)
+        self.h = h
+        self._keep = []
+        self.nch = 0
+        self.dims = 0
+        self.bins = 0
+        self.n_ext = 0
+
+    def _check(self, rc, h):
+        if rc != abi.CHILI_OK:
+            msg = self.lib.chili_gpu_last_error(h)
+            raise ChiliError(rc, msg.decode() if msg else "")
+
+    def call(self, name, *args):
+        self._check(getattr(self.lib, name)(self.h, *args), self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.chili_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---------------------------------------------------------------- basics
+    def set_stream(self, stream_ptr):
+        self.call("chili_gpu_set_stream", C.c_void_p(stream_ptr) if stream_ptr else None)
+
+    def synchronize(self):
+        self.call("chili_gpu_synchronize")
+
+    @property
+    def launches(self):
+        return int(self.lib.chili_gpu_launch_count(self.h))
+
+    # ----------------------------------------------------------------- grids
+    def set_grids(self, edges):
+        edges = _f64(edges)
+        nch, dims, b1 = edges.shape
+        self.call("chili_gpu_set_grids", _ptr(edges), nch, dims, b1 - 1)
+        self.dims, self.bins = dims, b1 - 1
+
+    def uniform_grids(self, nch, dims, bins):
+        e = np.tile(np.arange(bins + 1, dtype=np.float64) / bins, (nch, dims, 1))
+        self.set_grids(e)
+
+    def get_grids(self):
+        nch = self.nch if self.nch else 1
+        out = np.empty((self._grid_count(), self.dims, self.bins + 1))
+        self.call("chili_gpu_get_grids", _ptr(out), out.shape[0], self.dims, self.bins)
+        return out
+
+    def _grid_count(self):
+        return getattr(self, "_g_nch", None) or (self.nch if self.nch else 1)
+
+    def grid_map(self, ch, u):
+        u = _f64(u)
+        n = u.shape[0]
+        x = np.empty_like(u)
+        jac = np.empty(n)
+        self.call("chili_gpu_grid_map", ch, _ptr(u), _ptr(x), _ptr(jac), n)
+        return x, jac
+
+    def grid_weight(self, ch, x):
+        x = _f64(x)
+        n = x.shape[0]
+        w = np.empty(n)
+        b = np.empty(x.shape, dtype=np.int32)
+        self.call("chili_gpu_grid_weight", ch, _ptr(x), _ptr(w), _ptr(b), n)
+        return w, b
+
+    def grid_adapt(self, ch, alpha, train):
+        self.call("chili_gpu_grid_adapt", ch, float(alpha), _ptr(_f64(train)))
+
+    def grid_split(self, nsplit=2):
+        self.call("chili_gpu_grid_split", nsplit)
+        self.bins *= nsplit
+
+    # ------------------------------------------------------------- integrand
+    def set_integrand(self, kind, params=()):
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        self._keep.append(p)
+        self.call("chili_gpu_set_integrand", kind, _ptr(p) if p.size else None, int(p.size))
+
+    def set_preprocess(self, kind):
+        self.call("chili_gpu_set_preprocess", kind)
+
+    # --------------------------------------------------------- plain VEGAS
+    def vegas_iterate(self, ncalls, seed=42, counter=0, u=None, alpha=1.5, adapt=True, train=False):
+        st = abi.Stats()
+        tr = np.empty(self.dims * self.bins) if train else None
+        u = _f64(u)
+        self.call("chili_gpu_vegas_iterate", int(ncalls), int(seed), int(counter), _ptr(u),
+                  float(alpha), 1 if adapt else 0, C.byref(st), _ptr(tr))
+        return (st, tr) if train else st
+
+    # -------------------------------------------------------------- channels
+    def set_channels(self, cs):
+        self._keep.append(cs)
+        self.call("chili_gpu_set_channels", cs.descs, cs.nch, C.byref(cs.cuts), cs.sqrts, cs.n_ext)
+        self.nch, self.n_ext = cs.nch, cs.n_ext
+        self.ndims = int(self.lib.chili_gpu_ndims(self.h))
+
+    def fsmapper_generate(self, ch, x):
+        x = _f64(x)
+        n = x.shape[0]
+        mom = np.empty((n, self.n_ext, 4))
+        self.call("chili_gpu_fsmapper_generate", ch, _ptr(x), _ptr(mom), n)
+        return mom
+
+    def fsmapper_weight(self, ch, mom):
+        mom = _f64(mom)
+        n = mom.shape[0]
+        x = np.empty((n, self.ndims))
+        w = np.empty(n)
+        self.call("chili_gpu_fsmapper_weight", ch, _ptr(mom), _ptr(x), _ptr(w), n)
+        return w, x
+
+    # ---------------------------------------------------------- multichannel
+    def set_alpha(self, alpha):
+        a = _f64(alpha)
+        self.call("chili_gpu_set_alpha", _ptr(a), self.nch)
+
+    def get_alpha(self):
+        a, b, md = np.empty(self.nch), np.empty(self.nch), C.c_double()
+        self.call("chili_gpu_get_alpha", _ptr(a), _ptr(b), C.byref(md), self.nch)
+        return a, b, md.value
+
+    def select_channel(self, v):
+        v = _f64(v)
+        out = np.empty(v.shape[0], dtype=np.int32)
+        self.call("chili_gpu_select_channel", _ptr(v), _ptr(out), v.shape[0])
+        return out
+
+    def multichannel_weight(self, mom, ich):
+        mom = _f64(mom)
+        ich = np.ascontiguousarray(ich, dtype=np.int32)
+        n = mom.shape[0]
+        w, dens, x = np.empty(n), np.empty((n, self.nch)), np.empty((n, self.ndims))
+        self.call("chili_gpu_multichannel_weight", _ptr(mom), _ptr(ich), _ptr(w), _ptr(dens), _ptr(x), n)
+        return w, dens, x
+
+    def multichannel_iterate(self, params, seed=7, counter=0, u=None, guard=True):
+        st, info = abi.Stats(), abi.MCIterInfo()
+        u = _f64(u)
+        n_u = 0 if u is None else u.shape[0]
+        self.call("chili_gpu_multichannel_iterate", C.byref(params), int(seed), int(counter), _ptr(u),
+                  n_u, 1 if guard else 0, C.byref(st), C.byref(info))
+        return st, info
+
+    def get_training(self):
+        h = np.empty((self.nch, self.ndims, self.bins))
+        a = np.empty(self.nch)
+        self.call("chili_gpu_get_training", _ptr(h), _ptr(a))
+        return h, a
+
+    def generate(self, n, seed=7, counter=0):
+        mom = np.empty((n, self.n_ext, 4))
+        w = np.empty(n)
+        ch = np.empty(n, dtype=np.int32)
+        self.call("chili_gpu_generate", int(n), int(seed), int(counter), _ptr(mom), _ptr(w), _ptr(ch))
+        return mom, w, ch
+
+    def evaluate_batch(self, ch, u):
+        u = _f64(u)
+        out = np.empty(u.shape[0])
+        self.call("chili_gpu_evaluate_batch", ch, _ptr(u), _ptr(out), u.shape[0])
+        return out
+
+
+def stats_mean_error(st):
+    """StatsData::Mean and ::Error (Statistics.hh:90-126)."""
+    n, s, s2 = st[0], st[3], st[4]
+    mean = s / n
+    var = (s2 / n - mean * mean) / (n - 1)
+    return mean, float(np.sqrt(var)) if var > 0 else 0.0

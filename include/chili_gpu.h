@@ -1,0 +1,286 @@
+/*
+ * chili_gpu.h -- C ABI of the B200 implementation of Chili's integration hot
+ * path: VEGAS point generation and grid adaptation, and the multichannel
+ * t/s-channel phase-space mappings (FSMapper), with the combined channel
+ * weight and channel-weight adaptation.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, and returns
+ * a status code (CHILI_OK == 0).  No exception crosses the boundary; the text
+ * of the last error is available from chili_gpu_last_error().
+ *
+ * Pointer arguments marked "host or device" may point to host memory (pageable
+ * or pinned) or to device memory of the context's GPU; the library detects
+ * which through CUDA unified addressing and stages host buffers through its own
+ * device buffers.  All work of a context is issued on one CUDA stream; a
+ * context must not be used from two host threads at the same time.
+ *
+ * Reference interfaces replaced (paths inside the Chili project):
+ *   AdaptiveMap   include/Integrator/AdaptiveMap.hh:26-73, src/Integrator/AdaptiveMap.cc:34-160
+ *   Vegas         include/Integrator/Vegas.hh:30-95, src/Integrator/Vegas.cc:18-82
+ *   StatsData     include/Integrator/Statistics.hh:62-142
+ *   FSMapper      include/Channel/Channel.hh:15-77, src/Channel/Channel.cc:22-256
+ *   Integrand     include/Channel/Integrand.hh:107-123
+ *   MultiChannel  include/Channel/MultiChannel.hh:29-251, src/Channel/MultiChannel.cc:109-154
+ *   Interface::Evaluate (nanobind) include/Interfaces/nanobind.hh:23-50
+ *   CallChili (TensorFlow op)      src/Interfaces/Tensorflow.cc:22-135
+ */
+#ifndef CHILI_GPU_H
+#define CHILI_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+enum chili_status {
+    CHILI_OK = 0,
+    CHILI_ERR_INVALID_ARG = 1, /* bad pointer, size or description          */
+    CHILI_ERR_CUDA = 2,        /* a CUDA runtime call failed                */
+    CHILI_ERR_TIMEOUT = 3,     /* a bounded device wait gave up             */
+    CHILI_ERR_NAN_GRID = 4,    /* adaptation produced a non-finite edge     */
+    CHILI_ERR_STATE = 5,       /* call made before the state it needs       */
+    CHILI_ERR_LIMIT = 6        /* size beyond a compiled limit (see below)  */
+};
+
+/* ---------------------------------------------------------------- limits */
+#define CHILI_MAX_EXT 10      /* external particles, incoming included     */
+#define CHILI_MAX_DIMS 32     /* integration dimensions per channel        */
+#define CHILI_MAX_CHANNELS 200
+#define CHILI_MAX_BINS 4096   /* VEGAS bins per dimension                  */
+#define CHILI_MAX_INTEGRAND_PARAMS 128
+
+/* ------------------------------------------------------- phase-space data */
+/* ParticleInfo (include/Channel/ChannelNode.hh:26-32): idx is the bitmask of
+ * external legs (leg i <-> 1<<i; legs 0 and 1 are incoming). */
+typedef struct {
+    uint32_t idx;
+    int32_t pid;
+    double mass;
+    double width;
+} chili_particle_info;
+
+/* One DecayMap entry (ChannelNode.hh:35): parent -> (child1, child2). */
+typedef struct {
+    chili_particle_info parent, child1, child2;
+} chili_decay;
+
+/* ChannelDescription (ChannelNode.hh:46-51).  info is the t-channel list in
+ * the caller's order (the last entry balances momentum); decays may come in
+ * any order: they are processed in the reference's std::map order, i.e.
+ * ascending (idx, mass, width) of the parent. */
+typedef struct {
+    int32_t n_info;
+    const chili_particle_info *info;
+    int32_t n_decays;
+    const chili_decay *decays;
+} chili_channel_desc;
+
+typedef struct {
+    uint32_t idx;
+    double value;
+} chili_idx_value;
+
+typedef struct {
+    int32_t pid1, pid2;
+    double value;
+} chili_pid_pair_value;
+
+/* Cuts (include/Tools/Cuts.hh:13-19) as flat key/value tables.  sexternal
+ * holds the squared masses of the outgoing legs.  Keys absent from smin read
+ * as 0 and from deltaR as 0 (Channel.cc:148-151); ptmin and etamax must hold
+ * every idx that the channel descriptions reference (Channel.hh:22,
+ * Channel.cc:150,209). */
+typedef struct {
+    int32_t n_sexternal;
+    const double *sexternal;
+    int32_t n_deltaR;
+    const chili_pid_pair_value *deltaR;
+    int32_t n_smin;
+    const chili_idx_value *smin;
+    int32_t n_ptmin;
+    const chili_idx_value *ptmin;
+    int32_t n_etamax;
+    const chili_idx_value *etamax;
+} chili_cuts;
+
+/* ------------------------------------------------------------ statistics */
+/* StatsData (Statistics.hh:62-142), same field order as its binary form. */
+typedef struct {
+    double n, min, max, sum, sum2, n_finite;
+} chili_stats;
+
+/* MultiChannelParams (MultiChannel.hh:29-49) and its defaults. */
+typedef struct {
+    uint64_t ncalls;        /* 10000 */
+    uint64_t niterations;   /* 10    */
+    double rtol;            /* 1e-5  */
+    uint64_t nrefine;       /* 1     */
+    double beta;            /* 0.25  */
+    double min_alpha;       /* 1e-5  */
+    double refine_size;     /* 1.5   */
+    uint64_t max_bins;      /* 200   */
+    uint64_t iteration;     /* 0     */
+    int32_t should_optimize;/* 1     */
+    double grid_alpha;      /* VegasParams::alpha of every channel grid, 1.0 */
+} chili_multichannel_params;
+
+/* What one multichannel iteration did, besides its StatsData. */
+typedef struct {
+    uint64_t points_tried;    /* counters consumed (incl. rejected points)  */
+    uint64_t points_accepted; /* == ncalls on success                       */
+    uint64_t rejected_pre;    /* PreProcess rejections                      */
+    uint64_t rejected_nan;    /* NaN-value retries (MultiChannel.hh:230-236)*/
+    double weight_max;        /* max combined weight f*w over the iteration */
+    double nonfinite_alpha_terms; /* non-finite alpha-training contributions */
+} chili_mc_iter_info;
+
+/* ------------------------------------------------------------ integrands */
+enum chili_integrand_kind {
+    /* f = 1 (the unit integrand of src/example.cc:120-122). */
+    CHILI_FUNC_UNIT = 0,
+    /* f(x) = N [exp(-|x-a|^2/s^2) + exp(-|x-b|^2/s^2)] over [0,1]^D.
+     * params = {s, N, a[0..D-1], b[0..D-1]}, D = grid dimensions. */
+    CHILI_FUNC_CAMEL = 1,
+    /* Sum over outgoing pairs (i<j) of 1/((s_ij-M^2)^2+M^2 G^2) times the
+     * product over outgoing j of 1/(|t_0j|+m^2), t_0j = (p_0+p_j)^2 in the
+     * all-outgoing convention.  params = {M, G, m}. */
+    CHILI_FUNC_PROPAGATOR = 2,
+    /* As CHILI_FUNC_PROPAGATOR but the product of the two largest pair
+     * factors instead of their sum.  params = {M, G, m}. */
+    CHILI_FUNC_PROPAGATOR_TOP2 = 3
+};
+
+/* PreProcess cut applied to every generated point (MultiChannel.hh:219-223). */
+enum chili_preprocess_kind {
+    CHILI_PRE_ACCEPT_ALL = 0,
+    /* reject when the first momentum's energy is NaN (src/example.cc:26-29) */
+    CHILI_PRE_FINITE = 1
+};
+
+/* ------------------------------------------------------------ context */
+typedef struct chili_ctx chili_ctx;
+
+/* Create a context on CUDA device `device`. */
+int chili_gpu_create(int device, chili_ctx **out);
+int chili_gpu_destroy(chili_ctx *ctx);
+/* Last error text of ctx (or of the library when ctx is NULL). */
+const char *chili_gpu_last_error(const chili_ctx *ctx);
+/* Use the given cudaStream_t for all later work (NULL: the context's own). */
+int chili_gpu_set_stream(chili_ctx *ctx, void *stream);
+int chili_gpu_synchronize(chili_ctx *ctx);
+/* Number of kernels this context has launched so far. */
+uint64_t chili_gpu_launch_count(const chili_ctx *ctx);
+
+/* ------------------------------------------------- grids (AdaptiveMap) */
+/* nch grids of dims x (bins+1) edges, each in the reference AdaptiveMap
+ * layout edges[dim*(bins+1)+k] (AdaptiveMap.hh:29-40,47-48).  Host or device. */
+int chili_gpu_set_grids(chili_ctx *ctx, const double *edges, int nch, int dims,
+                        int bins);
+int chili_gpu_get_grids(chili_ctx *ctx, double *edges, int nch, int dims,
+                        int bins);
+/* AdaptiveMap::operator() (AdaptiveMap.cc:40-56) on n points of grid ch:
+ * u[n*dims] -> x[n*dims], jac[n].  Host or device. */
+int chili_gpu_grid_map(chili_ctx *ctx, int ch, const double *u, double *x,
+                       double *jac, int64_t n);
+/* AdaptiveMap::FindBin (:34-38) and ::GenerateWeight (:58-65): x[n*dims] ->
+ * w[n] and (optional) bin[n*dims]; a FindBin of SIZE_MAX reads as -1. */
+int chili_gpu_grid_weight(chili_ctx *ctx, int ch, const double *x, double *w,
+                          int32_t *bin, int64_t n);
+/* AdaptiveMap::Adapt (:67-125) of grid ch with damping alpha from
+ * train[dims*bins].  Host or device. */
+int chili_gpu_grid_adapt(chili_ctx *ctx, int ch, double alpha,
+                         const double *train);
+/* AdaptiveMap::Split (:127-160) of every grid into nsplit (2, 3 or 4). */
+int chili_gpu_grid_split(chili_ctx *ctx, int nsplit);
+
+/* ------------------------------------------------------------ integrand */
+int chili_gpu_set_integrand(chili_ctx *ctx, int kind, const double *params,
+                            int nparams);
+int chili_gpu_set_preprocess(chili_ctx *ctx, int kind);
+
+/* ------------------------------------------------------ plain VEGAS */
+/* One Vegas::operator() (Vegas.cc:18-52) on grid 0: ncalls points, uniforms
+ * from the counter-based generator (seed, counter_base + i) or, when u is not
+ * NULL, from u[ncalls*dims]; f*J accumulated into stats_out, f^2 J^2 into the
+ * per-bin training histogram (copied to train_out[dims*bins] when not NULL),
+ * and, when adapt != 0, AdaptiveMap::Adapt(alpha) applied to grid 0. */
+int chili_gpu_vegas_iterate(chili_ctx *ctx, uint64_t ncalls, uint64_t seed,
+                            uint64_t counter_base, const double *u,
+                            double alpha, int adapt, chili_stats *stats_out,
+                            double *train_out);
+
+/* ------------------------------------------------ channels (FSMapper) */
+/* Build the device programs of nch FSMapper channels (Channel.hh:18-30) over
+ * n_ext external legs at collider energy sqrts. */
+int chili_gpu_set_channels(chili_ctx *ctx, const chili_channel_desc *descs,
+                           int nch, const chili_cuts *cuts, double sqrts,
+                           int n_ext);
+/* Phase-space dimensions of the channels, 3*(n_ext-2)-2 (Channel.hh:33). */
+int chili_gpu_ndims(const chili_ctx *ctx);
+/* FSMapper::GeneratePoint (Channel.cc:22-38): x[n*ndims] -> mom[n*n_ext*4]
+ * (E, px, py, pz per leg).  Host or device. */
+int chili_gpu_fsmapper_generate(chili_ctx *ctx, int ch, const double *x,
+                                double *mom, int64_t n);
+/* FSMapper::GenerateWeight (Channel.cc:40-61): mom -> x_out[n*ndims]
+ * (optional), w[n].  Host or device. */
+int chili_gpu_fsmapper_weight(chili_ctx *ctx, int ch, const double *mom,
+                              double *x_out, double *w, int64_t n);
+
+/* -------------------------------------------------------- multichannel */
+/* Channel weights alpha (MultiChannel.cc:62-67 initialises them to 1/nch). */
+int chili_gpu_set_alpha(chili_ctx *ctx, const double *alpha, int nch);
+/* Current alpha, best weights and min_diff (MultiChannel.cc:138-154). */
+int chili_gpu_get_alpha(chili_ctx *ctx, double *alpha, double *best_alpha,
+                        double *min_diff, int nch);
+/* Channel selection by the libstdc++ discrete_distribution rule used by
+ * Random::SelectIndex (Random.hh:43-45) for uniforms v[n] -> ich[n]. */
+int chili_gpu_select_channel(chili_ctx *ctx, const double *v, int32_t *ich,
+                             int64_t n);
+/* Integrand::GenerateWeight (Integrand.hh:112-123): the combined weight of
+ * n points mom[n*n_ext*4] generated in channels ich[n]; optional per-channel
+ * densities dens[n*nch] and the chosen channel's inverse x_ich[n*ndims]. */
+int chili_gpu_multichannel_weight(chili_ctx *ctx, const double *mom,
+                                  const int32_t *ich, double *wgt,
+                                  double *dens, double *x_ich, int64_t n);
+/* One MultiChannel::operator() (MultiChannel.hh:196-251): points are tried in
+ * counter order until params->ncalls are accepted; rejected points count as
+ * zero-valued calls.  Uniforms come from the generator (seed, counter_base+k)
+ * or, when u is not NULL, from u[k*(ndims+1)...] (ndims uniforms then the
+ * channel uniform, MultiChannel.hh:145-147) for k < n_u; running out of u is
+ * CHILI_ERR_LIMIT.  With should_optimize the channel grids, alpha and best
+ * weights are adapted on the device (MultiChannel.hh:182-194).
+ * guard_alpha != 0 drops non-finite alpha-training terms, a documented
+ * deviation from the reference (which propagates them). */
+int chili_gpu_multichannel_iterate(chili_ctx *ctx,
+                                   const chili_multichannel_params *params,
+                                   uint64_t seed, uint64_t counter_base,
+                                   const double *u, int64_t n_u,
+                                   int guard_alpha, chili_stats *stats_out,
+                                   chili_mc_iter_info *info);
+/* Per-channel training histograms [nch*dims*bins] and alpha-training sums
+ * [nch] of the last iteration (before adaptation).  Host or device. */
+int chili_gpu_get_training(chili_ctx *ctx, double *hist, double *alpha_train);
+
+/* Event generation: MultiChannel::GeneratePoint + GenerateWeight
+ * (MultiChannel.hh:141-165) for n points in counter order, with no PreProcess
+ * and no retry.  mom[n*n_ext*4], wgt[n] = f*w (0 if not finite), ch[n];
+ * any output may be NULL.  Host or device. */
+int chili_gpu_generate(chili_ctx *ctx, int64_t n, uint64_t seed,
+                       uint64_t counter_base, double *mom, double *wgt,
+                       int32_t *ch);
+
+/* Interface::Evaluate (nanobind.hh:23-50) / CallChili (Tensorflow.cc:22-135):
+ * uniforms u[n*ndims] through channel ch's FSMapper alone (no VEGAS grid):
+ * out[n] = f * FSMapper weight, 0 where PreProcess rejects or the weight is 0.
+ * The output buffer is the caller's.  Host or device. */
+int chili_gpu_evaluate_batch(chili_ctx *ctx, int ch, const double *u,
+                             double *out, int64_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CHILI_GPU_H */
