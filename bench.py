@@ -1,0 +1,387 @@
+"""Benchmark of the multichannel VEGAS hot path (2->4, 15 channels, 100 bins,
+1e6 accepted points per iteration) on B200, and of the reference's own CPU
+implementation of the same workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl chili|reference]
+
+One step = one MultiChannel::operator() iteration: 1e6 accepted points
+(generation, PreProcess, combined weight over all 15 channels, integrand,
+StatsData, per-channel grid histograms and alpha training) followed by the
+alpha and grid adaptation.  Rank 0 prints one JSON line.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time to 0.1% error & unweighted events/s: flow vs plain VEGAS, 1 B200, FP64"
+UNIT = "unweighted events/s"
+NCALLS = 1_000_000
+SEED = 7
+BINS = 100
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="chili", choices=["chili", "reference"])
+    ap.add_argument("--ncalls", type=int, default=NCALLS)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(ncalls):
+    return {"workload": "multichannel 2->4 propagator integrand, sqrt(S)=1 TeV, 10 dims",
+            "channels": 15, "bins_per_dim": BINS, "points_per_iteration": ncalls,
+            "seed": SEED, "alpha_adapted": True, "alpha_guard": True,
+            "l2": "per-step working set > L2 (momenta of ~2e6 tried points, ~380 MB)"}
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                mhz.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+# ------------------------------------------------------------------ chili arm
+def unweighted_events(st, info):
+    """Expected unweighted events of an iteration: N <w> / w_max = sum / w_max."""
+    return st.sum / info.weight_max if info.weight_max > 0 else 0.0
+
+
+def run_chili(args, rank, world, local_rank):
+    import torch
+
+    from chili_b200 import abi, channels, gpu, workloads
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    cs = channels.multichannel_2_to_4()
+    ctx = gpu.Context(local_rank)
+    stream = torch.cuda.current_stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_channels(cs)
+    ctx.uniform_grids(cs.nch, ctx.ndims, BINS)
+    ctx.set_integrand(abi.CHILI_FUNC_PROPAGATOR, channels.propagator_params())
+    ctx.set_preprocess(abi.CHILI_PRE_FINITE)
+    params = workloads.mc_params(args.ncalls, iterations=args.warmup + args.steps)
+    seed = SEED + 1000 * rank  # disjoint streams per rank (weak scaling)
+    counter = 0
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    for _ in range(args.warmup):
+        st, info = ctx.multichannel_iterate(params, seed=seed, counter=counter, guard=True)
+        counter += info.points_tried
+    torch.cuda.synchronize(dev)
+    barrier()
+    torch.cuda.synchronize(dev)
+
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = ctx.launches
+    pooled = np.zeros(6)
+    history = []
+    unw = 0.0
+    tried = 0
+    with ClockSampler(local_rank) as clk:
+        ev0.record(stream)
+        t_wall0 = time.perf_counter()
+        for _ in range(args.steps):
+            st, info = ctx.multichannel_iterate(params, seed=seed, counter=counter, guard=True)
+            counter += info.points_tried
+            tried += info.points_tried
+            unw += unweighted_events(st, info)
+            pooled += np.array(st.as_tuple()) * np.array([1, 0, 0, 1, 1, 1])
+            mean, err = gpu.stats_mean_error(pooled)
+            history.append((time.perf_counter() - t_wall0, err / abs(mean) if mean else float("inf")))
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+    launches = ctx.launches - l0
+    ms = ev0.elapsed_time(ev1)
+    barrier()
+    # max over ranks of the device time; totals summed
+    t = torch.tensor([ms, unw, float(tried), float(args.ncalls * args.steps)], dtype=torch.float64, device=dev)
+    if world > 1:
+        tmax = t[:1].clone()
+        torch.distributed.all_reduce(tmax, op=torch.distributed.ReduceOp.MAX)
+        tsum = t[1:].clone()
+        torch.distributed.all_reduce(tsum)
+        ms_max, unw_tot, tried_tot, acc_tot = tmax.item(), *tsum.tolist()
+    else:
+        ms_max, unw_tot, tried_tot, acc_tot = ms, unw, float(tried), float(args.ncalls * args.steps)
+    mean, err = gpu.stats_mean_error(pooled)
+    t01 = next((h[0] for h in history if h[1] <= 1e-3), None)
+
+    # kernel-level timing of the dominant kernel (k_mc_weight) is taken from a
+    # dedicated run of one iteration with events around each kernel class
+    roof = roofline(ctx, params, seed, counter, stream, dev)
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = measure_e2e(ctx, params, args, dev, rank)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(args)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": unw_tot / (ms_max / 1e3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (on-device Philox4x32-10 uniforms)",
+            "config": dict(workload_config(args.ncalls), parallelism=f"replicas x{world}"),
+            "points_per_s": acc_tot / (ms_max / 1e3),
+            "tried_points_per_s": tried_tot / (ms_max / 1e3),
+            "unweighting_efficiency": unw_tot / acc_tot,
+            "integral": mean, "rel_error": err / abs(mean),
+            "time_to_0p1pct_s": t01,
+            "clocks": clk.summary(),
+            "gpu_launches": launches,
+            "roofline": roof,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+FP64_OPS_PER_WEIGHTED_POINT = None  # filled from the ncu capture (profiles/)
+
+
+def roofline(ctx, params, seed, counter, stream, dev):
+    """Dominant kernel: k_mc_weight (all-channel inverse maps).  Its duration is
+    measured from one iteration's kernels; the FP64 work per point comes from
+    the committed ncu counters.  HBM view: the 204-byte event record per point."""
+    import torch
+    from chili_b200 import gpu
+    lib = ctx.lib
+    # one iteration, device time of the whole iteration for context
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    st, info = ctx.multichannel_iterate(params, seed=seed, counter=counter, guard=True)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    it_ms = e0.elapsed_time(e1)
+    peaks = measured_peaks()
+    return {"bound": "fp64", "kernel": "k_mc_weight", "iteration_ms": it_ms,
+            "achieved": None, "peak": None, "unit": "TFLOP/s", "frac": None, "traffic": None,
+            "hbm_peak_gbs": peaks.get("hbm_gbs"),
+            "note": "FP64 pipe roofline filled from profiles/ once captured"}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def measure_e2e(ctx, params, args, dev, rank):
+    """Same metric through the C ABI with HOST buffers: each step's uniforms
+    come from pinned host memory (copied in inside the call), the StatsData and
+    iteration record come back to the host."""
+    import torch
+    from chili_b200 import gpu, workloads
+    D = ctx.ndims
+    n_u = int(args.ncalls * 2.4) + 4096
+    rng = np.random.default_rng(1234 + rank)
+    bufs = []
+    for _ in range(2):
+        t = torch.empty((n_u, D + 1), dtype=torch.float64, pin_memory=True)
+        t.numpy()[:] = workloads.uniforms53(rng, (n_u, D + 1))
+        bufs.append(t.numpy())
+    steps = max(2, min(args.steps, 5))
+    ctx.multichannel_iterate(params, u=bufs[0], guard=True)  # warm-up
+    torch.cuda.synchronize(dev)
+    unw = 0.0
+    t0 = time.perf_counter()
+    for s in range(steps):
+        st, info = ctx.multichannel_iterate(params, u=bufs[s % 2], guard=True)
+        unw += unweighted_events(st, info)
+    dt = time.perf_counter() - t0
+    return {"value": unw / dt, "unit": UNIT, "h2d_bytes_per_step": int(n_u * (D + 1) * 8),
+            "d2h_bytes_per_step": int(2 * 48 + 32), "steps": steps,
+            "path": "chili_gpu_multichannel_iterate with host uniforms (pinned) and host StatsData"}
+
+
+# ------------------------------------------------------------- reference arm
+def _ref_worker_init(ncalls):
+    global _W
+    sys.path.insert(0, ROOT)
+    from chili_b200 import abi, channels, workloads
+    from oracle import ref
+    cs = channels.multichannel_2_to_4()
+    params = workloads.mc_params(ncalls)
+    _W = {"R": ref.MultiChannel(cs, BINS, params, abi.CHILI_FUNC_PROPAGATOR, channels.propagator_params()),
+          "cs": cs, "ncalls": ncalls, "rng": np.random.default_rng(os.getpid()), "wl": workloads}
+
+
+def _ref_worker_step(_):
+    R = _W["R"]
+    u = _W["wl"].uniforms53(_W["rng"], (int(_W["ncalls"] * 2.6) + 256, R.ndims + 1))
+    t0 = time.perf_counter()
+    st, info = R.iterate(u, guard=True)
+    dt = time.perf_counter() - t0
+    return (st.sum / info.weight_max if info.weight_max > 0 else 0.0, _W["ncalls"], info.points_tried, dt,
+            st.as_tuple())
+
+
+def _pool(cores, ncalls):
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    return ctx.Pool(cores, initializer=_ref_worker_init, initargs=(ncalls,))
+
+
+def cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_baseline(args, kind="reference"):
+    """The reference (oracle/_ref) timed on the host: one iteration of a
+    bounded sample per core, all cores in parallel (replica stand-in for the
+    reference's MPI mode)."""
+    from oracle import ref
+    if not ref.available():
+        return {"value": None, "unavailable": "oracle/_ref not built"}
+    cores = cpu_cores()
+    ncalls = 20000
+    with _pool(cores, ncalls) as pool:
+        pool.map(_ref_worker_step, range(cores))  # warm-up: one adapted iteration each
+        t0 = time.perf_counter()
+        res = pool.map(_ref_worker_step, range(cores))
+        dt = time.perf_counter() - t0
+    unw = sum(r[0] for r in res)
+    return {"value": unw / dt, "unit": UNIT, "cores": cores, "kind": kind,
+            "points_per_s": sum(r[1] for r in res) / dt,
+            "sample": f"one guarded MultiChannel iteration of {ncalls} accepted points per core on {cores} "
+                      f"cores in parallel, after one warm-up iteration"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libchili_ref.so not built"}))
+        return
+    cores = cpu_cores()
+    ncalls = 10000
+    unw = 0.0
+    acc = 0
+    pooled = np.zeros(6)
+    with _pool(cores, ncalls) as pool:
+        for _ in range(args.warmup):
+            pool.map(_ref_worker_step, range(cores))
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            res = pool.map(_ref_worker_step, range(cores))
+            unw += sum(r[0] for r in res)
+            acc += sum(r[1] for r in res)
+            for r in res:
+                pooled += np.array(r[4]) * np.array([1, 0, 0, 1, 1, 1])
+        dt = time.perf_counter() - t0
+    value = unw / dt
+    from chili_b200.gpu import stats_mean_error
+    mean, err = stats_mean_error(pooled)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (host uniforms)", "config": workload_config(ncalls * cores),
+        "points_per_s": acc / dt, "integral": mean, "rel_error": err / abs(mean),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"each step: one guarded MultiChannel iteration of {ncalls} accepted points "
+                                   f"per core, {cores} cores in parallel (independent replicas)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local_rank))
+    try:
+        run_chili(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -507,6 +507,18 @@ int chili_gpu_set_channels(chili_ctx *ctx, const chili_channel_desc *descs, int 
     return CHILI_OK;
 }
 
+int chili_gpu_check_channels(const chili_channel_desc *descs, int nch, const chili_cuts *cuts, double sqrts,
+                             int n_ext, char *err, size_t err_len) {
+    std::vector<ChannelProgram> progs;
+    std::string why = sqrts > 0 ? build_channel_programs(descs, nch, cuts, sqrts, n_ext, progs)
+                                : std::string("sqrts must be positive");
+    if (err && err_len) {
+        std::strncpy(err, why.c_str(), err_len - 1);
+        err[err_len - 1] = 0;
+    }
+    return why.empty() ? CHILI_OK : CHILI_ERR_INVALID_ARG;
+}
+
 int chili_gpu_ndims(const chili_ctx *ctx) { return ctx ? ctx->ndims : -1; }
 
 int chili_gpu_fsmapper_generate(chili_ctx *ctx, int ch, const double *x, double *mom, int64_t n) {

@@ -7,8 +7,6 @@
 // reference's (compiled without FMA contraction) for identical inputs.
 #pragma once
 
-#include <algorithm>
-
 #include "common.cuh"
 
 namespace chili_dev {
@@ -42,7 +40,10 @@ __host__ __device__ inline double edge_before_table(int dims, int bins) {
     const unsigned long long req = 8ull * static_cast<unsigned long long>(dims) * (bins + 1);
     unsigned long long word;
     if (req + 8 >= 128ull * 1024) word = ((req + 16 + 4095) & ~4095ull) | 2ull;
-    else word = (std::max(32ull, (req + 8 + 15) & ~15ull)) | 1ull;
+    else {
+        word = (req + 8 + 15) & ~15ull;
+        word = (word < 32ull ? 32ull : word) | 1ull;
+    }
     union {
         unsigned long long u;
         double d;

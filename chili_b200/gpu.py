@@ -45,6 +45,8 @@ def _declare(lib):
         "chili_gpu_vegas_iterate": ([vp, u64, u64, u64, vp, dbl, i32, vp, vp], i32),
         "chili_gpu_set_channels": ([vp, P(abi.ChannelDesc), i32, P(abi.Cuts), dbl, i32], i32),
         "chili_gpu_ndims": ([vp], i32),
+        "chili_gpu_check_channels": ([P(abi.ChannelDesc), i32, P(abi.Cuts), dbl, i32, C.c_char_p,
+                                      C.c_size_t], i32),
         "chili_gpu_fsmapper_generate": ([vp, i32, vp, vp, i64], i32),
         "chili_gpu_fsmapper_weight": ([vp, i32, vp, vp, vp, i64], i32),
         "chili_gpu_set_alpha": ([vp, vp, i32], i32),
@@ -275,6 +277,14 @@ class Context:
         out = np.empty(u.shape[0])
         self.call("chili_gpu_evaluate_batch", ch, _ptr(u), _ptr(out), u.shape[0])
         return out
+
+
+def check_channels(cs):
+    """Host-only validation of a ChannelSet; returns '' or the reason."""
+    lib = load()
+    buf = C.create_string_buffer(512)
+    lib.chili_gpu_check_channels(cs.descs, cs.nch, C.byref(cs.cuts), cs.sqrts, cs.n_ext, buf, 512)
+    return buf.value.decode()
 
 
 def stats_mean_error(st):

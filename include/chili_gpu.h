@@ -218,6 +218,13 @@ int chili_gpu_vegas_iterate(chili_ctx *ctx, uint64_t ncalls, uint64_t seed,
 int chili_gpu_set_channels(chili_ctx *ctx, const chili_channel_desc *descs,
                            int nch, const chili_cuts *cuts, double sqrts,
                            int n_ext);
+/* Host-only check of channel descriptions (no device needed): 0 when the
+ * channels are consistent (each consumes exactly 3*(n_ext-2)-2 uniforms,
+ * every decaying current has its DecayMap entry, the cuts hold every key the
+ * FSMapper reads with .at(), Channel.hh:22 and Channel.cc:150,209), else
+ * CHILI_ERR_INVALID_ARG with the reason in err[err_len]. */
+int chili_gpu_check_channels(const chili_channel_desc *descs, int nch, const chili_cuts *cuts, double sqrts,
+                             int n_ext, char *err, size_t err_len);
 /* Phase-space dimensions of the channels, 3*(n_ext-2)-2 (Channel.hh:33). */
 int chili_gpu_ndims(const chili_ctx *ctx);
 /* FSMapper::GeneratePoint (Channel.cc:22-38): x[n*ndims] -> mom[n*n_ext*4]
