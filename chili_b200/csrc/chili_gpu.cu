@@ -78,7 +78,8 @@ struct chili_ctx {
     // multichannel iteration scratch
     DevBuf mom_soa, ich, flag, list, block_count, block_off, part, hist, round_res, acc, ctl, status;
     RoundCtl *ctl_host = nullptr;  // pinned
-    double accept_rate = 0.5;
+    double accept_rate = 0.5, nan_rate = 0.0;
+    DevBuf rec, ctl3;
     // plain VEGAS scratch
     DevBuf v_part, v_hist, v_train, v_out;
     // staging of host buffers
@@ -211,7 +212,7 @@ int chili_gpu_create(int device, chili_ctx **out) {
         return fail(nullptr, CHILI_ERR_CUDA, "cudaMallocHost failed");
     }
     cudaDeviceGetAttribute(&ctx->max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
-    cudaFuncSetAttribute(k_mc_weight, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->max_smem_optin);
+    cudaFuncSetAttribute(k_mc_accum, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->max_smem_optin);
     cudaFuncSetAttribute(k_vegas_iter, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->max_smem_optin);
     cudaFuncSetAttribute(k_grid_adapt, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->max_smem_optin);
     cudaGetLastError();
@@ -226,7 +227,7 @@ int chili_gpu_destroy(chili_ctx *ctx) {
     DevBuf *bufs[] = {&ctx->edges, &ctx->edges_tmp, &ctx->progs, &ctx->alpha_buf, &ctx->f_dev, &ctx->mom_soa,
                       &ctx->ich, &ctx->flag, &ctx->list, &ctx->block_count, &ctx->block_off, &ctx->part,
                       &ctx->hist, &ctx->round_res, &ctx->acc, &ctx->ctl, &ctx->status, &ctx->v_part,
-                      &ctx->v_hist, &ctx->v_train, &ctx->v_out};
+                      &ctx->v_hist, &ctx->v_train, &ctx->v_out, &ctx->rec, &ctx->ctl3};
     for (DevBuf *b : bufs) b->release();
     for (auto &b : ctx->stage) b.release();
     if (ctx->ctl_host) cudaFreeHost(ctx->ctl_host);
@@ -666,45 +667,68 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         a0.st[2] = 2.2250738585072014e-308; // StatsData max = lim::min()
         CK(cudaMemcpyAsync(ctx->acc.p, &a0, sizeof(IterAcc), cudaMemcpyHostToDevice, ctx->stream));
     }
-    const size_t wgt_smem = sizeof(double) * (static_cast<size_t>(nch) * kWgtBlock + (kWgtBlock / 32) * nch);
-    if (wgt_smem > static_cast<size_t>(ctx->max_smem_optin))
-        return fail(ctx, CHILI_ERR_LIMIT, "too many channels for the weight kernel's shared memory");
+    const size_t acc_smem = sizeof(double) * (kWgtBlock / 32) * nch;
 
     long long needed = ncalls, tried = 0;
     unsigned long long rounds = 0;
     while (needed > 0) {
-        long long m = static_cast<long long>(static_cast<double>(needed) / std::max(ctx->accept_rate, 0.02) * 1.03) + 1024;
-        m = std::min<long long>(m, 1ll << 23);
+        // chunk: enough counters for `needed` accepted, non-NaN points at the
+        // rates of the previous iteration, with a 2% margin
+        const double rate = std::max(ctx->accept_rate * (1.0 - ctx->nan_rate), 0.02);
+        long long m = static_cast<long long>(static_cast<double>(needed) / rate * 1.02) + 2048;
+        m = std::min<long long>(m, 1ll << 24);
         if (u) {
             m = std::min<long long>(m, n_u - tried);
             if (m <= 0) return fail(ctx, CHILI_ERR_LIMIT, "the given uniforms ran out before ncalls points were accepted");
         }
         const long long nb_f = (m + kFwdBlock - 1) / kFwdBlock;
+        const long long nb_w = (m + kWgtBlock - 1) / kWgtBlock;
         CK(ctx->mom_soa.ensure(sizeof(double) * 4 * NE * m));
         CK(ctx->ich.ensure(sizeof(int32_t) * m));
         CK(ctx->flag.ensure(m));
-        CK(ctx->list.ensure(sizeof(int32_t) * std::min(m, needed)));
+        CK(ctx->list.ensure(sizeof(int32_t) * m));
         CK(ctx->block_count.ensure(sizeof(int32_t) * nb_f));
         CK(ctx->block_off.ensure(sizeof(long long) * nb_f));
-        const long long nb_w = (std::min(m, needed) + kWgtBlock - 1) / kWgtBlock;
         CK(ctx->part.ensure(sizeof(double) * (kPartFixed + nch) * nb_w));
+        CK(ctx->rec.ensure(m * (2 * sizeof(double) + 1 + sizeof(int32_t) * D + sizeof(double) * nch) + 256));
+        CK(ctx->ctl3.ensure(3 * sizeof(RoundCtl)));
+        RoundCtl *ctl_pre = ctx->ctl3.as<RoundCtl>(), *ctl_list = ctl_pre + 1;
+        double *rec_val = ctx->rec.as<double>();
+        double *rec_wgt = rec_val + m;
+        double *rec_dens = rec_wgt + m;
+        int32_t *rec_slot = reinterpret_cast<int32_t *>(rec_dens + static_cast<size_t>(nch) * m);
+        uint8_t *rec_ok = reinterpret_cast<uint8_t *>(rec_slot + static_cast<size_t>(D) * m);
         k_mc_forward<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(
             ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), cp_ptr(ctx), nch, D, B, seed,
             counter_base + tried, ud ? ud + tried * (D + 1) : nullptr, m, ctx->f_dev.as<IntegrandDesc>(), NE,
             ctx->mom_soa.as<double>(), ctx->ich.as<int32_t>(), ctx->flag.as<uint8_t>(), ctx->block_count.as<int32_t>());
         LAUNCHED();
+        // offsets of every PreProcess-accepted point (no cut at this stage)
         k_mc_scan<<<1, 1024, 0, ctx->stream>>>(ctx->block_count.as<int32_t>(), static_cast<int>(nb_f),
-                                               ctx->flag.as<uint8_t>(), m, needed, ctx->block_off.as<long long>(),
-                                               ctx->ctl.as<RoundCtl>());
+                                               ctx->flag.as<uint8_t>(), m, m + 1, ctx->block_off.as<long long>(),
+                                               ctl_pre);
         LAUNCHED();
         k_mc_compact<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(
-            ctx->flag.as<uint8_t>(), ctx->block_off.as<long long>(), ctx->ctl.as<RoundCtl>(), m, ctx->list.as<int32_t>());
+            ctx->flag.as<uint8_t>(), ctx->block_off.as<long long>(), ctl_pre, m, ctx->list.as<int32_t>());
         LAUNCHED();
-        k_mc_weight<<<static_cast<unsigned>(nb_w), kWgtBlock, wgt_smem, ctx->stream>>>(
+        k_mc_weight<<<static_cast<unsigned>(nb_w), kWgtBlock, 0, ctx->stream>>>(
             ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), alpha_ptr(ctx), nch, D, B, NE,
-            ctx->mom_soa.as<double>(), m, ctx->ich.as<int32_t>(), ctx->list.as<int32_t>(), ctx->ctl.as<RoundCtl>(),
-            ctx->f_dev.as<IntegrandDesc>(), opt ? 1 : 0, guard_alpha ? 1 : 0, ctx->hist.as<double>(),
-            ctx->part.as<double>());
+            ctx->mom_soa.as<double>(), m, ctx->ich.as<int32_t>(), ctx->list.as<int32_t>(), ctl_pre,
+            ctx->f_dev.as<IntegrandDesc>(), opt ? 1 : 0, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens);
+        LAUNCHED();
+        // the cut: the needed-th record whose value is not NaN
+        k_block_count<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(rec_ok, ctl_pre,
+                                                                                 ctx->block_count.as<int32_t>());
+        LAUNCHED();
+        k_mc_scan<<<1, 1024, 0, ctx->stream>>>(ctx->block_count.as<int32_t>(), static_cast<int>(nb_f), rec_ok, m,
+                                               needed, ctx->block_off.as<long long>(), ctl_list);
+        LAUNCHED();
+        k_cut_finalize<<<1, 1, 0, ctx->stream>>>(ctl_list, ctl_pre, ctx->list.as<int32_t>(), m, needed,
+                                                 ctx->ctl.as<RoundCtl>());
+        LAUNCHED();
+        k_mc_accum<<<static_cast<unsigned>(nb_w), kWgtBlock, acc_smem, ctx->stream>>>(
+            ctx->ctl.as<RoundCtl>(), m, nch, D, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens, opt ? 1 : 0,
+            guard_alpha ? 1 : 0, ctx->hist.as<double>(), ctx->part.as<double>());
         LAUNCHED();
         k_mc_reduce<<<kPartFixed + nch, 256, 0, ctx->stream>>>(ctx->part.as<double>(), nch, ctx->ctl.as<RoundCtl>(),
                                                                ctx->round_res.as<double>());
@@ -720,6 +744,7 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         tried += r.cut;
         needed -= (r.n_acc - r.nan_round);
         if (r.cut > 0) ctx->accept_rate = std::max(0.02, static_cast<double>(r.n_acc) / static_cast<double>(r.cut));
+        if (r.n_acc > 0) ctx->nan_rate = std::min(0.5, static_cast<double>(r.nan_round) / static_cast<double>(r.n_acc));
         if (++rounds > 100000) return fail(ctx, CHILI_ERR_TIMEOUT, "no accepted points after 100000 rounds");
     }
     IterAcc acc_h;

@@ -10,16 +10,20 @@
 // are tried in order until ncalls are accepted) hold exactly:
 //   k_mc_forward   uniforms -> channel choice -> VEGAS map -> FSMapper
 //                  forward -> PreProcess flag, momenta kept in HBM (SoA)
-//   k_mc_scan      accepted count per block -> cut position of the
-//                  `needed`-th accepted point
-//   k_mc_compact   ordered list of accepted points before the cut
+//   k_mc_scan      accepted counts per block -> exclusive offsets
+//   k_mc_compact   ordered list of the PreProcess-accepted points
 //   k_mc_weight    every channel's inverse map + grid weight -> combined
-//                  weight, integrand, StatsData, channel histograms, alpha
-//                  training terms (block partials)
-//   k_mc_finalize  ordered fold of the block partials into the iteration
+//                  weight and integrand, as per-point records
+//   k_block_count, k_mc_scan, k_cut_finalize
+//                  the cut: the `needed`-th point whose value is not NaN
+//                  (NaN values are retried, MultiChannel.hh:230-236)
+//   k_mc_accum     StatsData, channel histograms and alpha training over the
+//                  records before the cut (block partials)
+//   k_mc_reduce, k_mc_accumulate
+//                  ordered fold of the partials into the iteration
 //                  accumulator; PreProcess rejections count as zero calls
-// Points whose value is NaN are retried (MultiChannel.hh:230-236), so the host
-// runs further rounds until ncalls points are accepted.
+// The chunk is sized from the previous acceptance and NaN rates so that one
+// round normally covers the iteration; a short chunk leads to another round.
 #pragma once
 
 #include "channel_program.h"
@@ -527,7 +531,7 @@ __global__ void __launch_bounds__(1024) k_mc_scan(const int32_t *__restrict__ bl
     const long long r = needed - cut_off_s;
     const long long k = static_cast<long long>(cut_block_s) * kFwdBlock + threadIdx.x;
     int f = 0;
-    if (threadIdx.x < kFwdBlock && k < m) f = flag[k];
+    if (threadIdx.x < kFwdBlock && k < m) f = flag[k] ? 1 : 0;
     long long incl = f;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -566,58 +570,112 @@ __global__ void __launch_bounds__(kFwdBlock) k_mc_compact(const uint8_t *__restr
     }
 }
 
-// The expensive pass: combined weight, integrand and training data of the
-// accepted points list[0..n_acc).  Dynamic shared memory: dens[nch][block]
-// then alpha-training per warp [nwarps][nch].
+// The expensive pass: combined weight and integrand of every PreProcess-
+// accepted point list[0..n) of the chunk, written as per-point records so
+// that the exact cut (the `needed`-th point whose value is not NaN, in
+// counter order) can be taken afterwards and only that prefix accumulated:
+//   rec_val, rec_wgt   value f*w and weight (both 0 for a NaN retry)
+//   rec_ok             0 for a NaN retry (MultiChannel.hh:230-236), else 1
+//   rec_slot[j*n+i]    histogram slot of dimension j in the chosen channel's
+//                      histogram (Integrand.hh:91-95), -1 when it would lie
+//                      before the histogram
+//   rec_dens[c*n+i]    channel c's density, for the alpha-training terms
 __global__ void __launch_bounds__(kWgtBlock) k_mc_weight(
     const ChannelProgram *__restrict__ progs, const double *__restrict__ grids, const double *__restrict__ alpha,
     int nch, int dims, int bins, int n_ext, const double *__restrict__ mom_soa, long long m,
     const int32_t *__restrict__ ich_arr, const int32_t *__restrict__ list, const RoundCtl *__restrict__ ctl,
-    const IntegrandDesc *__restrict__ f, int should_opt, int guard, double *__restrict__ hist,
+    const IntegrandDesc *__restrict__ f, int should_opt, double *__restrict__ rec_val, double *__restrict__ rec_wgt,
+    uint8_t *__restrict__ rec_ok, int32_t *__restrict__ rec_slot, double *__restrict__ rec_dens) {
+    const long long n = ctl->n_acc;
+    const long long i = blockIdx.x * static_cast<long long>(kWgtBlock) + threadIdx.x;
+    if (i >= n) return;
+    const long long k = list[i];
+    const int c_sel = ich_arr[k];
+    V4 mom[CHILI_MAX_SLOTS];
+    for (int s = 0; s < n_ext; ++s)
+        mom[s] = V4{mom_soa[(4 * s + 0) * m + k], mom_soa[(4 * s + 1) * m + k], mom_soa[(4 * s + 2) * m + k],
+                    mom_soa[(4 * s + 3) * m + k]};
+    double x[CHILI_MAX_DIMS], xs[CHILI_MAX_DIMS];
+    double wgt = combined_weight(progs, grids, alpha, nch, dims, bins, c_sel, mom, x, xs, rec_dens + i, n);
+    const double fv = eval_momenta(f, mom, n_ext);
+    double val = wgt == 0 ? 0 : fv * wgt;
+    uint8_t ok = 1;
+    if (isnan(val)) {
+        val = wgt = 0;
+        ok = 0;
+    }
+    rec_val[i] = val;
+    rec_wgt[i] = wgt;
+    rec_ok[i] = ok;
+    if (should_opt) {
+        const double *g = grids + static_cast<size_t>(c_sel) * dims * (bins + 1);
+        const int base = c_sel * dims * bins;
+        for (int j = 0; j < dims; ++j) {
+            const int b = find_bin(g + j * (bins + 1), bins, xs[j]);
+            const int s = j * bins + b;
+            rec_slot[j * n + i] = s >= 0 ? base + s : -1;
+        }
+    }
+}
+
+// Per-256-entry counts of a byte flag array (input of k_mc_scan).
+__global__ void __launch_bounds__(kFwdBlock) k_block_count(const uint8_t *__restrict__ flag,
+                                                           const RoundCtl *__restrict__ ctl,
+                                                           int32_t *__restrict__ block_count) {
+    const long long n = ctl->n_acc;
+    const long long k = blockIdx.x * static_cast<long long>(kFwdBlock) + threadIdx.x;
+    const int cnt = __syncthreads_count(k < n ? flag[k] : 0);
+    if (threadIdx.x == 0) block_count[blockIdx.x] = cnt;
+}
+
+// Turns the cut over the record list (ctl_list: cut = records included,
+// n_acc = non-NaN among them) into the round record: counters consumed,
+// PreProcess-accepted points among them, NaN retries among those.
+__global__ void k_cut_finalize(const RoundCtl *__restrict__ ctl_list, const RoundCtl *__restrict__ ctl_pre,
+                               const int32_t *__restrict__ list, long long m, long long needed,
+                               RoundCtl *__restrict__ ctl) {
+    const long long n_pre = ctl_pre->n_acc;
+    const long long ok = n_pre > 0 ? ctl_list->n_acc : 0;
+    const bool enough = ok >= needed;
+    const long long L = enough ? ctl_list->cut : n_pre;  // records included
+    RoundCtl r;
+    r.cut = (enough && L > 0) ? static_cast<long long>(list[L - 1]) + 1 : m;
+    r.n_acc = L;
+    r.nan_round = L - ok;
+    r.pad = 0;
+    *ctl = r;
+}
+
+// Ordered-prefix accumulation of the records [0, ctl->n_acc): StatsData
+// partials, histogram adds, alpha-training terms val^2 w / dens_j
+// (MultiChannel.hh:167-180).  Dynamic shared memory: (kWgtBlock/32) * nch.
+__global__ void __launch_bounds__(kWgtBlock) k_mc_accum(
+    const RoundCtl *__restrict__ ctl, long long n_rec, int nch, int dims, const double *__restrict__ rec_val,
+    const double *__restrict__ rec_wgt, const uint8_t *__restrict__ rec_ok, const int32_t *__restrict__ rec_slot,
+    const double *__restrict__ rec_dens, int should_opt, int guard, double *__restrict__ hist,
     double *__restrict__ part) {
-    extern __shared__ double sh[];
-    double *dens_s = sh;                    // nch * kWgtBlock
-    double *atr_s = sh + nch * kWgtBlock;   // (kWgtBlock/32) * nch
+    extern __shared__ double atr_s[];  // (kWgtBlock/32) * nch
     const long long n_list = ctl->n_acc;
     const long long i = blockIdx.x * static_cast<long long>(kWgtBlock) + threadIdx.x;
     const bool active = i < n_list;
-    double val = 0, wgt = 0;
-    double cnt = 0, nan_cnt = 0, dropped = 0;
-    if (active) {
-        const long long k = list[i];
-        const int c_sel = ich_arr[k];
-        V4 mom[CHILI_MAX_SLOTS];
-        for (int s = 0; s < n_ext; ++s)
-            mom[s] = V4{mom_soa[(4 * s + 0) * m + k], mom_soa[(4 * s + 1) * m + k], mom_soa[(4 * s + 2) * m + k],
-                        mom_soa[(4 * s + 3) * m + k]};
-        double x[CHILI_MAX_DIMS], xs[CHILI_MAX_DIMS];
-        wgt = combined_weight(progs, grids, alpha, nch, dims, bins, c_sel, mom, x, xs, dens_s + threadIdx.x,
-                              kWgtBlock);
-        const double fv = eval_momenta(f, mom, n_ext);
-        val = wgt == 0 ? 0 : fv * wgt;
-        if (isnan(val)) {
-            val = wgt = 0;
-            nan_cnt = 1;
-        }
-        cnt = 1;
-        if (should_opt) {
-            const double val2 = val * val;
-            const double *g = grids + static_cast<size_t>(c_sel) * dims * (bins + 1);
-            double *H = hist + static_cast<size_t>(c_sel) * dims * bins;
-            for (int j = 0; j < dims; ++j) {
-                const int b = find_bin(g + j * (bins + 1), bins, xs[j]);
-                const int s = j * bins + b;
-                if (s >= 0) atomicAdd(H + s, val2);
-                else dropped += 1;
-            }
+    const double val = active ? rec_val[i] : 0.0;
+    const double wgt = active ? rec_wgt[i] : 0.0;
+    double cnt = active ? 1.0 : 0.0;
+    double nan_cnt = (active && !rec_ok[i]) ? 1.0 : 0.0;
+    double dropped = 0;
+    const double val2 = val * val;
+    if (active && should_opt) {
+        for (int j = 0; j < dims; ++j) {
+            const int s = rec_slot[j * n_rec + i];
+            if (s >= 0) atomicAdd(hist + s, val2);
+            else dropped += 1;
         }
     }
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     double nonfin = 0;
     if (should_opt) {
-        const double val2 = val * val;
         for (int j = 0; j < nch; ++j) {
-            double term = active ? val2 * wgt / dens_s[j * kWgtBlock + threadIdx.x] : 0.0;
+            double term = active ? val2 * wgt / rec_dens[j * n_rec + i] : 0.0;
             if (guard && !isfinite(term)) {
                 nonfin += 1;
                 term = 0.0;
