@@ -196,3 +196,120 @@ std::string build_channel_programs(const chili_channel_desc *descs, int nch, con
     }
     return std::string();
 }
+
+bool build_point_program(const std::vector<ChannelProgram> &progs, PointProgram &pp) {
+    std::memset(&pp, 0, sizeof(pp));
+    if (progs.empty()) return false;
+    const ChannelProgram &p0 = progs[0];
+    pp.n_ext = p0.n_ext;
+    pp.ndims = p0.ndims;
+    pp.nch = static_cast<int32_t>(progs.size());
+    pp.sqrts = p0.sqrts;
+    pp.ptmax = p0.ptmax;
+    pp.inv16pi3 = p0.inv16pi3;
+    std::map<std::pair<int, int>, int> node_of_pair;
+    std::map<std::tuple<int, double, double>, int> tent_of;
+    std::map<std::pair<std::vector<int>, int>, int> chain_of;
+    std::map<std::tuple<int, int, int, int, double, double, double, double, double>, int> dw_of;
+    std::map<std::pair<int, int>, int> sw_of;
+    int n_nodes = p0.n_ext;
+    for (size_t c = 0; c < progs.size(); ++c) {
+        const ChannelProgram &P = progs[c];
+        if (P.n_ext != p0.n_ext || P.sqrts != p0.sqrts) return false;
+        int node[CHILI_MAX_SLOTS];
+        for (int s = 0; s < P.n_slots; ++s) node[s] = s < P.n_ext ? s : -1;
+        PPChannel &C = pp.ch[c];
+        // compound currents in decay (std::map) order: children come first
+        for (int k = 0; k < P.n_decay; ++k) {
+            const int a = node[P.dec_c1[k]], b = node[P.dec_c2[k]];
+            if (a < 0 || b < 0) return false;
+            auto it = node_of_pair.find({a, b});
+            int nd;
+            if (it == node_of_pair.end()) {
+                if (n_nodes >= PP_MAX_NODES) return false;
+                nd = n_nodes++;
+                pp.node_a[nd] = static_cast<int8_t>(a);
+                pp.node_b[nd] = static_cast<int8_t>(b);
+                node_of_pair[{a, b}] = nd;
+            } else {
+                nd = it->second;
+            }
+            node[P.dec_parent[k]] = nd;
+        }
+        for (int k = 0; k < P.n_decay; ++k) {
+            const auto key = std::make_tuple(node[P.dec_parent[k]], node[P.dec_c1[k]], node[P.dec_c2[k]],
+                                             static_cast<int>(P.dec_massless[k]), P.dec_mass[k], P.dec_width[k],
+                                             P.dec_smin2[k], P.dec_cut_smin[k], P.dec_smax[k]);
+            auto it = dw_of.find(key);
+            int id;
+            if (it == dw_of.end()) {
+                if (pp.n_dws >= PP_MAX_DWS) return false;
+                id = pp.n_dws++;
+                pp.dw_node[id] = static_cast<int8_t>(node[P.dec_parent[k]]);
+                pp.dw_c1[id] = static_cast<int8_t>(node[P.dec_c1[k]]);
+                pp.dw_c2[id] = static_cast<int8_t>(node[P.dec_c2[k]]);
+                pp.dw_massless[id] = P.dec_massless[k];
+                pp.dw_mass[id] = P.dec_mass[k];
+                pp.dw_width[id] = P.dec_width[k];
+                pp.dw_smin2[id] = P.dec_smin2[k];
+                pp.dw_cut[id] = P.dec_cut_smin[k];
+                pp.dw_smax[id] = P.dec_smax[k];
+                dw_of[key] = id;
+            } else {
+                id = it->second;
+            }
+            C.dw[k] = static_cast<int16_t>(id);
+        }
+        C.n_dec = static_cast<int8_t>(P.n_decay);
+        std::vector<int> tents;
+        for (int i = 0; i + 1 < P.n_info; ++i) {
+            const auto key = std::make_tuple(node[P.info_slot[i]], P.info_ptmin[i], P.info_etamax[i]);
+            auto it = tent_of.find(key);
+            int id;
+            if (it == tent_of.end()) {
+                if (pp.n_tents >= PP_MAX_TENTS) return false;
+                id = pp.n_tents++;
+                pp.tent_node[id] = static_cast<int8_t>(node[P.info_slot[i]]);
+                pp.tent_ptmin[id] = P.info_ptmin[i];
+                pp.tent_etacut[id] = P.info_etamax[i];
+                tent_of[key] = id;
+            } else {
+                id = it->second;
+            }
+            tents.push_back(id);
+        }
+        const int last = node[P.info_slot[P.n_info - 1]];
+        auto ck = std::make_pair(tents, last);
+        auto cit = chain_of.find(ck);
+        int cid;
+        if (cit == chain_of.end()) {
+            if (pp.n_chains >= PP_MAX_CHAINS) return false;
+            cid = pp.n_chains++;
+            pp.chain_len[cid] = static_cast<int8_t>(tents.size());
+            for (size_t t = 0; t < tents.size(); ++t) pp.chain_tent[cid][t] = static_cast<int8_t>(tents[t]);
+            pp.chain_last[cid] = static_cast<int8_t>(last);
+            chain_of[ck] = cid;
+        } else {
+            cid = cit->second;
+        }
+        C.chain = static_cast<int16_t>(cid);
+        for (int k = 0; k < P.n_sdec; ++k) {
+            const std::pair<int, int> key{node[P.sdec_a[k]], node[P.sdec_b[k]]};
+            auto it = sw_of.find(key);
+            int id;
+            if (it == sw_of.end()) {
+                if (pp.n_sws >= PP_MAX_SWS) return false;
+                id = pp.n_sws++;
+                pp.sw_a[id] = static_cast<int8_t>(key.first);
+                pp.sw_b[id] = static_cast<int8_t>(key.second);
+                sw_of[key] = id;
+            } else {
+                id = it->second;
+            }
+            C.sw[k] = static_cast<int16_t>(id);
+        }
+        C.n_sd = static_cast<int8_t>(P.n_sdec);
+    }
+    pp.n_nodes = n_nodes;
+    return true;
+}

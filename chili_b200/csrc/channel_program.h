@@ -43,10 +43,51 @@ struct ChannelProgram {
     int8_t sdec_ab[CHILI_MAX_DECAYS], sdec_a[CHILI_MAX_DECAYS], sdec_b[CHILI_MAX_DECAYS];
 };
 
+// The whole channel set seen from one point: quantities that several
+// channels share are listed once.
+//   nodes   momenta of the external legs and of every distinct compound
+//           current, node = node_a + node_b (the reference's tmp_mom sum)
+//   tents   t-channel entries other than the last, keyed by (node, ptmin,
+//           etamax cut): pT jacobian factor, eta factor and 3 uniforms
+//   chains  whole t-channel chains (ordered tents + last node): weight and
+//           last uniform, or failure (Channel.cc:197)
+//   dws     decay propagator weights and their uniform (Channel.cc:83-113)
+//   sws     two-body decay weights and their 2 uniforms (Channel.cc:222-256)
+// A channel is then the product of its parts in the reference's order.
+#define PP_MAX_NODES 32
+#define PP_MAX_TENTS 48
+#define PP_MAX_CHAINS 64
+#define PP_MAX_DWS 96
+#define PP_MAX_SWS 64
+
+struct PPChannel {
+    int8_t n_dec, n_sd;
+    int16_t chain;
+    int16_t dw[CHILI_MAX_DECAYS];
+    int16_t sw[CHILI_MAX_DECAYS];
+};
+
+struct PointProgram {
+    int32_t n_ext, ndims, nch, n_nodes, n_tents, n_chains, n_dws, n_sws;
+    double sqrts, ptmax, inv16pi3;
+    int8_t node_a[PP_MAX_NODES], node_b[PP_MAX_NODES];
+    int8_t tent_node[PP_MAX_TENTS];
+    double tent_ptmin[PP_MAX_TENTS], tent_etacut[PP_MAX_TENTS];
+    int8_t chain_len[PP_MAX_CHAINS], chain_last[PP_MAX_CHAINS];
+    int8_t chain_tent[PP_MAX_CHAINS][CHILI_MAX_EXT];
+    int8_t dw_node[PP_MAX_DWS], dw_c1[PP_MAX_DWS], dw_c2[PP_MAX_DWS], dw_massless[PP_MAX_DWS];
+    double dw_mass[PP_MAX_DWS], dw_width[PP_MAX_DWS], dw_smin2[PP_MAX_DWS], dw_cut[PP_MAX_DWS], dw_smax[PP_MAX_DWS];
+    int8_t sw_a[PP_MAX_SWS], sw_b[PP_MAX_SWS];
+    PPChannel ch[CHILI_MAX_CHANNELS];
+};
+
 #ifdef __cplusplus
 #include <string>
 #include <vector>
 // Builds the programs; returns an empty string on success, else the reason.
 std::string build_channel_programs(const chili_channel_desc *descs, int nch, const chili_cuts *cuts,
                                    double sqrts, int n_ext, std::vector<ChannelProgram> &out);
+// Deduplicates the per-channel programs into one PointProgram; false when the
+// set exceeds the PP_MAX_* limits (the per-channel kernels are used then).
+bool build_point_program(const std::vector<ChannelProgram> &progs, PointProgram &pp);
 #endif

@@ -68,6 +68,9 @@ struct chili_ctx {
     int nch = 0, n_ext = 0, ndims = 0;
     double sqrts = 0;
     DevBuf progs;
+    DevBuf point_prog;         // PointProgram of the channel set, when it fits
+    bool have_pp = false;      // the set fits the PointProgram limits
+    bool use_pp = true;        // option "point_program"
     // channel weights: alpha[CH], best[CH], cp[CH], min_diff
     DevBuf alpha_buf;
     bool alpha_set = false;
@@ -162,6 +165,9 @@ double *alpha_ptr(chili_ctx *ctx) { return ctx->alpha_buf.as<double>(); }
 double *best_ptr(chili_ctx *ctx) { return ctx->alpha_buf.as<double>() + CHILI_MAX_CHANNELS; }
 double *cp_ptr(chili_ctx *ctx) { return ctx->alpha_buf.as<double>() + 2 * CHILI_MAX_CHANNELS; }
 double *mindiff_ptr(chili_ctx *ctx) { return ctx->alpha_buf.as<double>() + 3 * CHILI_MAX_CHANNELS; }
+const PointProgram *pp_ptr(chili_ctx *ctx) {
+    return (ctx->have_pp && ctx->use_pp) ? ctx->point_prog.as<PointProgram>() : nullptr;
+}
 double *acc_train_ptr(chili_ctx *ctx) {
     return reinterpret_cast<double *>(static_cast<char *>(ctx->acc.p) + offsetof(IterAcc, atrain));
 }
@@ -224,7 +230,7 @@ int chili_gpu_destroy(chili_ctx *ctx) {
     if (!ctx) return CHILI_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    DevBuf *bufs[] = {&ctx->edges, &ctx->edges_tmp, &ctx->progs, &ctx->alpha_buf, &ctx->f_dev, &ctx->mom_soa,
+    DevBuf *bufs[] = {&ctx->edges, &ctx->edges_tmp, &ctx->progs, &ctx->point_prog, &ctx->alpha_buf, &ctx->f_dev, &ctx->mom_soa,
                       &ctx->ich, &ctx->flag, &ctx->list, &ctx->block_count, &ctx->block_off, &ctx->part,
                       &ctx->hist, &ctx->round_res, &ctx->acc, &ctx->ctl, &ctx->status, &ctx->v_part,
                       &ctx->v_hist, &ctx->v_train, &ctx->v_out, &ctx->rec, &ctx->ctl3};
@@ -262,6 +268,15 @@ int chili_gpu_synchronize(chili_ctx *ctx) {
 }
 
 uint64_t chili_gpu_launch_count(const chili_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value) {
+    if (!ctx || !name) return fail(ctx, CHILI_ERR_INVALID_ARG, "NULL argument");
+    if (std::strcmp(name, "point_program") == 0) {
+        ctx->use_pp = value != 0;
+        return CHILI_OK;
+    }
+    return fail(ctx, CHILI_ERR_INVALID_ARG, std::string("unknown option ") + name);
+}
 
 // --------------------------------------------------------------------- grids
 int chili_gpu_set_grids(chili_ctx *ctx, const double *edges, int nch, int dims, int bins) {
@@ -486,6 +501,16 @@ int chili_gpu_set_channels(chili_ctx *ctx, const chili_channel_desc *descs, int 
     ctx->n_ext = n_ext;
     ctx->ndims = progs[0].ndims;
     ctx->sqrts = sqrts;
+    {
+        std::vector<PointProgram> pp(1);
+        ctx->have_pp = build_point_program(progs, pp[0]);
+        if (ctx->have_pp) {
+            CK(ctx->point_prog.ensure(sizeof(PointProgram)));
+            CK(cudaMemcpyAsync(ctx->point_prog.p, pp.data(), sizeof(PointProgram), cudaMemcpyHostToDevice,
+                               ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+        }
+    }
     // alpha = 1/nch (MultiChannel.cc:62-67), best = alpha, min_diff = +inf
     std::vector<double> a(4 * CHILI_MAX_CHANNELS, 0.0);
     for (int i = 0; i < nch; ++i) a[i] = 1.0 / static_cast<double>(nch);
@@ -629,7 +654,7 @@ int chili_gpu_multichannel_weight(chili_ctx *ctx, const double *mom, const int32
     k_mc_weight_batch<<<grid_for(n, 128), 128, 0, ctx->stream>>>(
         ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), alpha_ptr(ctx), ctx->nch, ctx->ndims, ctx->bins,
         ctx->n_ext, static_cast<const double *>(am.dev), static_cast<const int32_t *>(ai.dev),
-        static_cast<double *>(aw.dev), static_cast<double *>(ad.dev), static_cast<double *>(ax.dev), n);
+        static_cast<double *>(aw.dev), static_cast<double *>(ad.dev), static_cast<double *>(ax.dev), n, pp_ptr(ctx));
     LAUNCHED();
     if ((rc = finish_out(ctx, aw)) || (rc = finish_out(ctx, ad)) || (rc = finish_out(ctx, ax))) return rc;
     return sync_if_host(ctx, {&am, &ai, &aw, &ad, &ax});
@@ -714,7 +739,7 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         k_mc_weight<<<static_cast<unsigned>(nb_w), kWgtBlock, 0, ctx->stream>>>(
             ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), alpha_ptr(ctx), nch, D, B, NE,
             ctx->mom_soa.as<double>(), m, ctx->ich.as<int32_t>(), ctx->list.as<int32_t>(), ctl_pre,
-            ctx->f_dev.as<IntegrandDesc>(), opt ? 1 : 0, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens);
+            ctx->f_dev.as<IntegrandDesc>(), opt ? 1 : 0, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens, pp_ptr(ctx));
         LAUNCHED();
         // the cut: the needed-th record whose value is not NaN
         k_block_count<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(rec_ok, ctl_pre,
@@ -802,7 +827,7 @@ int chili_gpu_generate(chili_ctx *ctx, int64_t n, uint64_t seed, uint64_t counte
     k_generate<<<grid_for(n, 128), 128, 0, ctx->stream>>>(
         ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), alpha_ptr(ctx), cp_ptr(ctx), ctx->nch, ctx->ndims,
         ctx->bins, ctx->n_ext, seed, counter_base, n, ctx->f_dev.as<IntegrandDesc>(), static_cast<double *>(am.dev),
-        static_cast<double *>(aw.dev), static_cast<int32_t *>(ac.dev));
+        static_cast<double *>(aw.dev), static_cast<int32_t *>(ac.dev), pp_ptr(ctx));
     LAUNCHED();
     if ((rc = finish_out(ctx, am)) || (rc = finish_out(ctx, aw)) || (rc = finish_out(ctx, ac))) return rc;
     return sync_if_host(ctx, {&am, &aw, &ac});

@@ -8,6 +8,7 @@
 
 #include "channel_program.h"
 #include "common.cuh"
+#include "grid.cuh"
 
 namespace chili_dev {
 
@@ -325,6 +326,136 @@ __device__ __forceinline__ double fs_weight(const ChannelProgram *__restrict__ P
         x[ir++] = r2;
     }
     return wdec * wt * ws;
+}
+
+}  // namespace chili_dev
+
+namespace chili_dev {
+
+// Integrand::GenerateWeight (Integrand.hh:112-123) over a PointProgram: the
+// shared parts of all channels are evaluated once per point, then every
+// channel's density is assembled as the reference multiplies it
+// (Channel.cc:40-61: WgtDecays * WgtTChan * WgtSChan, each in its own order)
+// and its uniforms are written into the buffer x that all channels share
+// (not cleared between channels, as the reference's _rans).  ext holds the
+// external momenta; xs receives channel ich's uniforms; dens[c*stride] the
+// per-channel densities.  Returns 1 / sum_c alpha_c / dens_c / vw_c.
+__device__ __forceinline__ double combined_weight_pp(const PointProgram *__restrict__ pp,
+                                                     const double *__restrict__ grids,
+                                                     const double *__restrict__ alpha, int dims, int bins, int ich,
+                                                     const V4 *ext, double *x, double *xs, double *dens,
+                                                     int dens_stride, double before) {
+    V4 nm[PP_MAX_NODES];
+    const int ne = pp->n_ext, nn = pp->n_nodes;
+    for (int i = 0; i < ne; ++i) nm[i] = ext[i];
+    for (int i = ne; i < nn; ++i) nm[i] = nm[pp->node_a[i]] + nm[pp->node_b[i]];
+    const double sqrts = pp->sqrts, ptmax = pp->ptmax;
+
+    // t-channel entries (WgtTChan loop body, Channel.cc:160-186)
+    double tfac[PP_MAX_TENTS], tg[PP_MAX_TENTS], tx0[PP_MAX_TENTS], tx1[PP_MAX_TENTS], tx2[PP_MAX_TENTS];
+    const int nt = pp->n_tents;
+    for (int t = 0; t < nt; ++t) {
+        const double ptmin = pp->tent_ptmin[t];
+        const V4 q = nm[pp->tent_node[t]];
+        const double pt = sqrt(pt2(q));
+        const double f2 = 2 * ptmin + pt;
+        tfac[t] = pt * ptmax / 2 / ptmin / (2 * ptmin + ptmax) * (f2 * f2);
+        tx0[t] = pt * (ptmax + 2 * ptmin) / (ptmax * (pt + 2 * ptmin));
+        double etamax = sqrts / 2 / pt;
+        etamax = log(etamax + sqrt(etamax * etamax - 1));
+        etamax = isnan(etamax) ? 99 : etamax;
+        etamax = std_min(etamax, pp->tent_etacut[t]);
+        tg[t] = 2 * etamax * 2 * kPi;
+        tx1[t] = (rapidity(q) / etamax + 1) / 2;
+        tx2[t] = phi_0_2pi(q) / 2 / kPi;
+    }
+    // whole chains, last entry included (Channel.cc:186-202)
+    double cw[PP_MAX_CHAINS], cx[PP_MAX_CHAINS];
+    unsigned long long cfail = 0;
+    const int nc = pp->n_chains;
+    for (int c = 0; c < nc; ++c) {
+        double wt = kTwoPi;
+        V4 psum{0., 0., 0., 0.};
+        const int len = pp->chain_len[c];
+        for (int i = 0; i < len; ++i) {
+            const int t = pp->chain_tent[c][i];
+            wt *= pp->inv16pi3;
+            wt *= tfac[t];
+            wt *= tg[t];
+            psum = psum + nm[pp->tent_node[t]];
+        }
+        const V4 q = nm[pp->chain_last[c]];
+        const double mjets2 = mass2(psum);
+        const double yjets = rapidity(psum);
+        const double ptj2 = pt2(psum);
+        const double qt = sqrt(mass2(q) + ptj2);
+        const double mt = sqrt(mjets2 + ptj2);
+        const double yv = rapidity(q);
+        const double ymin = -log(sqrts / qt * (1 - mt / sqrts * exp(-yjets)));
+        const double ymax = log(sqrts / qt * (1 - mt / sqrts * exp(yjets)));
+        const double dely = ymax - ymin;
+        if (isnan(ymax) || isnan(ymin)) {
+            cfail |= 1ull << c;
+            cw[c] = 0;
+            cx[c] = 0;
+        } else {
+            cw[c] = wt * (dely / sqrts / sqrts);
+            cx[c] = (yv - ymin) / dely;
+        }
+    }
+    // decay propagator weights (WgtDecays, Channel.cc:83-113)
+    double dw[PP_MAX_DWS], dx[PP_MAX_DWS];
+    const int nd = pp->n_dws;
+    for (int k = 0; k < nd; ++k) {
+        const double r = sqrt(fabs(mass2(nm[pp->dw_c1[k]]))) + sqrt(fabs(mass2(nm[pp->dw_c2[k]])));
+        const double smin = std_max(std_max(r * r, pp->dw_smin2[k]), pp->dw_cut[k]);
+        const double s = mass2(nm[pp->dw_node[k]]);
+        double u;
+        dw[k] = pp->dw_massless[k] ? massless_prop_weight(0.99, smin, pp->dw_smax[k], s, u)
+                                   : massive_prop_weight(pp->dw_mass[k], pp->dw_width[k], smin, pp->dw_smax[k], s, u);
+        dx[k] = u;
+    }
+    // two-body decays (WgtDecayParts, Channel.cc:222-237)
+    double sw[PP_MAX_SWS], sr1[PP_MAX_SWS], sr2[PP_MAX_SWS];
+    const int ns = pp->n_sws;
+    for (int k = 0; k < ns; ++k) sw[k] = schannel_weight(nm[pp->sw_a[k]], nm[pp->sw_b[k]], sr1[k], sr2[k]);
+
+    for (int d = 0; d < dims; ++d) x[d] = 0.0;
+    double acc = 0;
+    const size_t gsz = static_cast<size_t>(dims) * (bins + 1);
+    const int nch = pp->nch;
+    for (int c = 0; c < nch; ++c) {
+        const PPChannel &C = pp->ch[c];
+        int ir = 0;
+        double wdec = 1;
+        for (int k = 0; k < C.n_dec; ++k) {
+            wdec *= dw[C.dw[k]];
+            x[ir++] = dx[C.dw[k]];
+            wdec /= kTwoPi;
+        }
+        const int ch = C.chain;
+        const int len = pp->chain_len[ch];
+        for (int i = 0; i < len; ++i) {
+            const int t = pp->chain_tent[ch][i];
+            x[ir++] = tx0[t];
+            x[ir++] = tx1[t];
+            x[ir++] = tx2[t];
+        }
+        if (!((cfail >> ch) & 1ull)) x[ir++] = cx[ch];
+        double ws = 1;
+        for (int k = 0; k < C.n_sd; ++k) {
+            ws *= sw[C.sw[k]];
+            x[ir++] = sr1[C.sw[k]];
+            x[ir++] = sr2[C.sw[k]];
+        }
+        const double dc = wdec * cw[ch] * ws;
+        if (c == ich)
+            for (int d = 0; d < dims; ++d) xs[d] = x[d];
+        const double vw = grid_weight(grids + c * gsz, dims, bins, x, before);
+        acc += __ldg(alpha + c) / dc / vw;
+        if (dens) dens[c * dens_stride] = dc;
+    }
+    return 1.0 / acc;
 }
 
 }  // namespace chili_dev

@@ -410,7 +410,7 @@ __global__ void k_mc_weight_batch(const ChannelProgram *__restrict__ progs, cons
                                   const double *__restrict__ alpha, int nch, int dims, int bins, int n_ext,
                                   const double *__restrict__ mom, const int32_t *__restrict__ ich,
                                   double *__restrict__ wgt, double *__restrict__ dens, double *__restrict__ x_ich,
-                                  long long n) {
+                                  long long n, const PointProgram *__restrict__ pp) {
     const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
     if (i >= n) return;
     V4 m[CHILI_MAX_SLOTS];
@@ -421,8 +421,11 @@ __global__ void k_mc_weight_batch(const ChannelProgram *__restrict__ progs, cons
     double x[CHILI_MAX_DIMS], xs[CHILI_MAX_DIMS];
     for (int d = 0; d < dims; ++d) xs[d] = 0.0;
     const int c = ich[i];
-    const double w = combined_weight(progs, grids, alpha, nch, dims, bins, (c >= 0 && c < nch) ? c : -1, m, x,
-                                     xs, dens ? dens + i * nch : nullptr, 1);
+    const int cs = (c >= 0 && c < nch) ? c : -1;
+    const double w = pp ? combined_weight_pp(pp, grids, alpha, dims, bins, cs, m, x, xs,
+                                             dens ? dens + i * nch : nullptr, 1, edge_before_table(dims, bins))
+                        : combined_weight(progs, grids, alpha, nch, dims, bins, cs, m, x, xs,
+                                          dens ? dens + i * nch : nullptr, 1);
     wgt[i] = w;
     if (x_ich)
         for (int d = 0; d < dims; ++d) x_ich[i * dims + d] = xs[d];
@@ -585,7 +588,8 @@ __global__ void __launch_bounds__(kWgtBlock) k_mc_weight(
     int nch, int dims, int bins, int n_ext, const double *__restrict__ mom_soa, long long m,
     const int32_t *__restrict__ ich_arr, const int32_t *__restrict__ list, const RoundCtl *__restrict__ ctl,
     const IntegrandDesc *__restrict__ f, int should_opt, double *__restrict__ rec_val, double *__restrict__ rec_wgt,
-    uint8_t *__restrict__ rec_ok, int32_t *__restrict__ rec_slot, double *__restrict__ rec_dens) {
+    uint8_t *__restrict__ rec_ok, int32_t *__restrict__ rec_slot, double *__restrict__ rec_dens,
+    const PointProgram *__restrict__ pp) {
     const long long n = ctl->n_acc;
     const long long i = blockIdx.x * static_cast<long long>(kWgtBlock) + threadIdx.x;
     if (i >= n) return;
@@ -596,7 +600,9 @@ __global__ void __launch_bounds__(kWgtBlock) k_mc_weight(
         mom[s] = V4{mom_soa[(4 * s + 0) * m + k], mom_soa[(4 * s + 1) * m + k], mom_soa[(4 * s + 2) * m + k],
                     mom_soa[(4 * s + 3) * m + k]};
     double x[CHILI_MAX_DIMS], xs[CHILI_MAX_DIMS];
-    double wgt = combined_weight(progs, grids, alpha, nch, dims, bins, c_sel, mom, x, xs, rec_dens + i, n);
+    double wgt = pp ? combined_weight_pp(pp, grids, alpha, dims, bins, c_sel, mom, x, xs, rec_dens + i, n,
+                                         edge_before_table(dims, bins))
+                    : combined_weight(progs, grids, alpha, nch, dims, bins, c_sel, mom, x, xs, rec_dens + i, n);
     const double fv = eval_momenta(f, mom, n_ext);
     double val = wgt == 0 ? 0 : fv * wgt;
     uint8_t ok = 1;
@@ -826,7 +832,8 @@ __global__ void k_generate(const ChannelProgram *__restrict__ progs, const doubl
                            const double *__restrict__ alpha, const double *__restrict__ cp, int nch, int dims,
                            int bins, int n_ext, uint64_t seed, uint64_t ctr0, long long n,
                            const IntegrandDesc *__restrict__ f, double *__restrict__ mom_out,
-                           double *__restrict__ wgt_out, int32_t *__restrict__ ch_out) {
+                           double *__restrict__ wgt_out, int32_t *__restrict__ ch_out,
+                           const PointProgram *__restrict__ pp) {
     const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
     if (i >= n) return;
     double r[CHILI_MAX_DIMS + 1];
@@ -839,7 +846,9 @@ __global__ void k_generate(const ChannelProgram *__restrict__ progs, const doubl
     if (grid_map_checked(grids + static_cast<size_t>(c) * dims * (bins + 1), dims, bins, r, jac)) {
         fs_generate(progs + c, r, mom, m2);
         double x[CHILI_MAX_DIMS], xs[CHILI_MAX_DIMS];
-        const double wt = combined_weight(progs, grids, alpha, nch, dims, bins, c, mom, x, xs, nullptr, 0);
+        const double wt = pp ? combined_weight_pp(pp, grids, alpha, dims, bins, c, mom, x, xs, nullptr, 0,
+                                                  edge_before_table(dims, bins))
+                             : combined_weight(progs, grids, alpha, nch, dims, bins, c, mom, x, xs, nullptr, 0);
         const double fv = eval_momenta(f, mom, n_ext);
         w = wt == 0 ? 0 : fv * wt;
         if (!isfinite(w)) w = 0;

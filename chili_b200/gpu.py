@@ -34,6 +34,7 @@ def _declare(lib):
         "chili_gpu_set_stream": ([vp, vp], i32),
         "chili_gpu_synchronize": ([vp], i32),
         "chili_gpu_launch_count": ([vp], u64),
+        "chili_gpu_set_option": ([vp, C.c_char_p, i64], i32),
         "chili_gpu_set_grids": ([vp, vp, i32, i32, i32], i32),
         "chili_gpu_get_grids": ([vp, vp, i32, i32, i32], i32),
         "chili_gpu_grid_map": ([vp, i32, vp, vp, vp, i64], i32),
@@ -139,6 +140,9 @@ class Context:
 
     def synchronize(self):
         self.call("chili_gpu_synchronize")
+
+    def set_option(self, name, value):
+        self.call("chili_gpu_set_option", name.encode(), int(value))
 
     @property
     def launches(self):

@@ -173,6 +173,10 @@ int chili_gpu_set_stream(chili_ctx *ctx, void *stream);
 int chili_gpu_synchronize(chili_ctx *ctx);
 /* Number of kernels this context has launched so far. */
 uint64_t chili_gpu_launch_count(const chili_ctx *ctx);
+/* Tuning switches (no counterpart in the reference).  "point_program": 1
+ * (default) evaluates the parts that channels share once per point, 0 runs
+ * every channel's mapping on its own; both give the same numbers. */
+int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value);
 
 /* ------------------------------------------------- grids (AdaptiveMap) */
 /* nch grids of dims x (bins+1) edges, each in the reference AdaptiveMap

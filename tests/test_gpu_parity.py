@@ -171,8 +171,10 @@ def _mc_pair(ctx_factory, cs, bins, ncalls, rng):
     return ctx, R, params
 
 
-def test_combined_weight(ctx_factory, rng, mc2):
+@pytest.mark.parametrize("point_program", [1, 0])
+def test_combined_weight(ctx_factory, rng, mc2, point_program):
     ctx, R, _ = _mc_pair(ctx_factory, mc2, 100, 1000, rng)
+    ctx.set_option("point_program", point_program)
     alpha = rng.random(mc2.nch) + 0.1
     alpha /= alpha.sum()
     ctx.set_alpha(alpha)
@@ -187,15 +189,17 @@ def test_combined_weight(ctx_factory, rng, mc2):
     w, dens, xs = ctx.multichannel_weight(mom, ich)
     w_r, dens_r, xs_r = R.weight(mom, ich)
     fin = np.isfinite(w_r) & np.isfinite(w)
-    assert np.mean(np.isfinite(w_r) != np.isfinite(w)) < 1e-3
+    assert np.mean(np.isfinite(w_r) != np.isfinite(w)) < 2e-4
     assert np.percentile(rel(w[fin], w_r[fin]), 99) < RTOL
     df = np.isfinite(dens_r) & (dens_r != 0)
     assert np.percentile(rel(dens[df], dens_r[df]), 99) < RTOL
 
 
-def test_multichannel_iteration_matches_reference(ctx_factory, rng, mc2):
+@pytest.mark.parametrize("point_program", [1, 0])
+def test_multichannel_iteration_matches_reference(ctx_factory, rng, mc2, point_program):
     ncalls = 20_000
     ctx, R, params = _mc_pair(ctx_factory, mc2, 100, ncalls, rng)
+    ctx.set_option("point_program", point_program)
     for it in range(3):
         u = uniforms53(rng, (3 * ncalls, R.ndims + 1))
         st, info = ctx.multichannel_iterate(params, u=u, guard=True)
