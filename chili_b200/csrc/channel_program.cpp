@@ -311,5 +311,29 @@ bool build_point_program(const std::vector<ChannelProgram> &progs, PointProgram 
         C.n_sd = static_cast<int8_t>(P.n_sdec);
     }
     pp.n_nodes = n_nodes;
+    pp.memo_tent = 0;
+    pp.memo_dw = pp.memo_tent + 5 * pp.n_tents;
+    pp.memo_sw = pp.memo_dw + 2 * pp.n_dws;
+    pp.memo_chain = pp.memo_sw + 3 * pp.n_sws;
+    pp.n_memo = pp.memo_chain + 2 * pp.n_chains;
+    for (int c = 0; c < pp.nch; ++c) {
+        const PPChannel &C = pp.ch[c];
+        for (int fail = 0; fail < 2; ++fail) {
+            int16_t *pos = fail ? pp.pos_src_fail[c] : pp.pos_src[c];
+            int p = 0;
+            for (int k = 0; k < C.n_dec; ++k) pos[p++] = static_cast<int16_t>(pp.memo_dw + 2 * C.dw[k] + 1);
+            for (int i = 0; i < pp.chain_len[C.chain]; ++i) {
+                const int t = pp.chain_tent[C.chain][i];
+                for (int q = 0; q < 3; ++q) pos[p++] = static_cast<int16_t>(pp.memo_tent + 5 * t + 2 + q);
+            }
+            if (!fail) pos[p++] = static_cast<int16_t>(pp.memo_chain + 2 * C.chain + 1);
+            for (int k = 0; k < C.n_sd; ++k) {
+                pos[p++] = static_cast<int16_t>(pp.memo_sw + 3 * C.sw[k] + 1);
+                pos[p++] = static_cast<int16_t>(pp.memo_sw + 3 * C.sw[k] + 2);
+            }
+            if (fail) pos[p++] = -1;
+            if (p != pp.ndims) return false;
+        }
+    }
     return true;
 }

@@ -79,6 +79,16 @@ struct PointProgram {
     double dw_mass[PP_MAX_DWS], dw_width[PP_MAX_DWS], dw_smin2[PP_MAX_DWS], dw_cut[PP_MAX_DWS], dw_smax[PP_MAX_DWS];
     int8_t sw_a[PP_MAX_SWS], sw_b[PP_MAX_SWS];
     PPChannel ch[CHILI_MAX_CHANNELS];
+    // Phased evaluation: every item's outputs live in a memo buffer of
+    // n_memo slots per point (tent t: fac, g, x0, x1, x2 at memo_tent+5t;
+    // dw d: w, x at memo_dw+2d; sw s: w, r1, r2 at memo_sw+3s; chain c: w,
+    // x at memo_chain+2c).  pos_src[c][p] is the memo slot of channel c's
+    // uniform p; pos_src_fail[c][p] the same when c's chain fails, where the
+    // s-channel uniforms move down by one and the last position keeps the
+    // value the previous channels left there (-1).
+    int32_t memo_tent, memo_dw, memo_sw, memo_chain, n_memo;
+    int16_t pos_src[CHILI_MAX_CHANNELS][CHILI_MAX_DIMS];
+    int16_t pos_src_fail[CHILI_MAX_CHANNELS][CHILI_MAX_DIMS];
 };
 
 #ifdef __cplusplus

@@ -18,6 +18,7 @@
 #include "chili_gpu.h"
 #include "channel_program.h"
 #include "kernels.cuh"
+#include "pipeline.cuh"
 
 using namespace chili_dev;
 
@@ -71,6 +72,9 @@ struct chili_ctx {
     DevBuf point_prog;         // PointProgram of the channel set, when it fits
     bool have_pp = false;      // the set fits the PointProgram limits
     bool use_pp = true;        // option "point_program"
+    bool use_pipeline = true;  // option "pipeline": phased weight pass
+    PointProgram pp_host;      // host copy (sizes of the memo buffers)
+    DevBuf node_soa, memo, cfail;
     // channel weights: alpha[CH], best[CH], cp[CH], min_diff
     DevBuf alpha_buf;
     bool alpha_set = false;
@@ -186,6 +190,62 @@ int set_device(chili_ctx *ctx) {
     return CHILI_OK;
 }
 
+bool pipeline_dims_ok(int d) {
+    switch (d) {
+    case 1: case 4: case 7: case 10: case 13: case 16: case 19: case 22: return true;
+    default: return false;
+    }
+}
+
+template <int D>
+void launch_assemble(chili_ctx *ctx, long long m, int bins, int opt, const long long *n_list, double *rec_val,
+                     double *rec_wgt, uint8_t *rec_ok, int32_t *rec_slot, double *rec_dens) {
+    k_pp_assemble<D><<<static_cast<unsigned>((m + 127) / 128), 128, 0, ctx->stream>>>(
+        ctx->point_prog.as<PointProgram>(), ctx->edges.as<double>(), alpha_ptr(ctx), bins, ctx->node_soa.as<double>(),
+        ctx->memo.as<double>(), ctx->cfail.as<uint8_t>(), ctx->ich.as<int32_t>(), ctx->list.as<int32_t>(), n_list, m,
+        ctx->f_dev.as<IntegrandDesc>(), opt, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens);
+}
+
+// The phased weight pass (pipeline.cuh) over the PreProcess-accepted points
+// of a chunk of m counters.
+int launch_pipeline(chili_ctx *ctx, long long m, int bins, bool opt, RoundCtl *ctl_pre, double *rec_val,
+                    double *rec_wgt, uint8_t *rec_ok, int32_t *rec_slot, double *rec_dens) {
+    const PointProgram &P = ctx->pp_host;
+    const PointProgram *pp = ctx->point_prog.as<PointProgram>();
+    CK(ctx->node_soa.ensure(sizeof(double) * 4 * P.n_nodes * m));
+    CK(ctx->memo.ensure(sizeof(double) * std::max(1, P.n_memo) * m));
+    CK(ctx->cfail.ensure(static_cast<size_t>(std::max(1, P.n_chains)) * m));
+    const long long *n_list = reinterpret_cast<const long long *>(
+        reinterpret_cast<const char *>(ctl_pre) + offsetof(RoundCtl, n_acc));
+    const unsigned gx = static_cast<unsigned>((m + 255) / 256);
+    k_pp_nodes<<<gx, 256, 0, ctx->stream>>>(pp, ctx->mom_soa.as<double>(), m, ctx->list.as<int32_t>(), n_list,
+                                             ctx->node_soa.as<double>(), m);
+    LAUNCHED();
+    const int n_items = P.n_tents + P.n_dws + P.n_sws;
+    if (n_items > 0) {
+        k_pp_items<<<dim3(gx, n_items), 256, 0, ctx->stream>>>(pp, ctx->node_soa.as<double>(), n_list, m,
+                                                                ctx->memo.as<double>());
+        LAUNCHED();
+    }
+    k_pp_chains<<<dim3(gx, P.n_chains), 256, 0, ctx->stream>>>(pp, ctx->node_soa.as<double>(), n_list, m,
+                                                                ctx->memo.as<double>(), ctx->cfail.as<uint8_t>());
+    LAUNCHED();
+    const int o = opt ? 1 : 0;
+    switch (P.ndims) {
+    case 1: launch_assemble<1>(ctx, m, bins, o, n_list, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens); break;
+    case 4: launch_assemble<4>(ctx, m, bins, o, n_list, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens); break;
+    case 7: launch_assemble<7>(ctx, m, bins, o, n_list, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens); break;
+    case 10: launch_assemble<10>(ctx, m, bins, o, n_list, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens); break;
+    case 13: launch_assemble<13>(ctx, m, bins, o, n_list, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens); break;
+    case 16: launch_assemble<16>(ctx, m, bins, o, n_list, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens); break;
+    case 19: launch_assemble<19>(ctx, m, bins, o, n_list, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens); break;
+    case 22: launch_assemble<22>(ctx, m, bins, o, n_list, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens); break;
+    default: return fail(ctx, CHILI_ERR_STATE, "no phased weight kernel for this dimension");
+    }
+    LAUNCHED();
+    return CHILI_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -230,7 +290,7 @@ int chili_gpu_destroy(chili_ctx *ctx) {
     if (!ctx) return CHILI_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    DevBuf *bufs[] = {&ctx->edges, &ctx->edges_tmp, &ctx->progs, &ctx->point_prog, &ctx->alpha_buf, &ctx->f_dev, &ctx->mom_soa,
+    DevBuf *bufs[] = {&ctx->edges, &ctx->edges_tmp, &ctx->progs, &ctx->point_prog, &ctx->node_soa, &ctx->memo, &ctx->cfail, &ctx->alpha_buf, &ctx->f_dev, &ctx->mom_soa,
                       &ctx->ich, &ctx->flag, &ctx->list, &ctx->block_count, &ctx->block_off, &ctx->part,
                       &ctx->hist, &ctx->round_res, &ctx->acc, &ctx->ctl, &ctx->status, &ctx->v_part,
                       &ctx->v_hist, &ctx->v_train, &ctx->v_out, &ctx->rec, &ctx->ctl3};
@@ -273,6 +333,10 @@ int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value) {
     if (!ctx || !name) return fail(ctx, CHILI_ERR_INVALID_ARG, "NULL argument");
     if (std::strcmp(name, "point_program") == 0) {
         ctx->use_pp = value != 0;
+        return CHILI_OK;
+    }
+    if (std::strcmp(name, "pipeline") == 0) {
+        ctx->use_pipeline = value != 0;
         return CHILI_OK;
     }
     return fail(ctx, CHILI_ERR_INVALID_ARG, std::string("unknown option ") + name);
@@ -505,6 +569,7 @@ int chili_gpu_set_channels(chili_ctx *ctx, const chili_channel_desc *descs, int 
         std::vector<PointProgram> pp(1);
         ctx->have_pp = build_point_program(progs, pp[0]);
         if (ctx->have_pp) {
+            ctx->pp_host = pp[0];
             CK(ctx->point_prog.ensure(sizeof(PointProgram)));
             CK(cudaMemcpyAsync(ctx->point_prog.p, pp.data(), sizeof(PointProgram), cudaMemcpyHostToDevice,
                                ctx->stream));
@@ -702,6 +767,14 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         const double rate = std::max(ctx->accept_rate * (1.0 - ctx->nan_rate), 0.02);
         long long m = static_cast<long long>(static_cast<double>(needed) / rate * 1.02) + 2048;
         m = std::min<long long>(m, 1ll << 24);
+        const bool pipe = pipeline_dims_ok(D) && ctx->have_pp && ctx->use_pp && ctx->use_pipeline;
+        {
+            // keep the per-chunk buffers within ~8 GB
+            const PointProgram &P = ctx->pp_host;
+            long long per = 8ll * (4 * NE + nch + 4) + 4ll * D + 8;
+            if (pipe) per += 8ll * (4 * P.n_nodes + P.n_memo) + P.n_chains;
+            m = std::min<long long>(m, std::max<long long>(1 << 16, (8ll << 30) / per));
+        }
         if (u) {
             m = std::min<long long>(m, n_u - tried);
             if (m <= 0) return fail(ctx, CHILI_ERR_LIMIT, "the given uniforms ran out before ncalls points were accepted");
@@ -736,11 +809,17 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         k_mc_compact<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(
             ctx->flag.as<uint8_t>(), ctx->block_off.as<long long>(), ctl_pre, m, ctx->list.as<int32_t>());
         LAUNCHED();
-        k_mc_weight<<<static_cast<unsigned>(nb_w), kWgtBlock, 0, ctx->stream>>>(
-            ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), alpha_ptr(ctx), nch, D, B, NE,
-            ctx->mom_soa.as<double>(), m, ctx->ich.as<int32_t>(), ctx->list.as<int32_t>(), ctl_pre,
-            ctx->f_dev.as<IntegrandDesc>(), opt ? 1 : 0, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens, pp_ptr(ctx));
-        LAUNCHED();
+        if (pipe) {
+            int rc2 = launch_pipeline(ctx, m, B, opt, ctl_pre, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens);
+            if (rc2) return rc2;
+        } else {
+            k_mc_weight<<<static_cast<unsigned>(nb_w), kWgtBlock, 0, ctx->stream>>>(
+                ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), alpha_ptr(ctx), nch, D, B, NE,
+                ctx->mom_soa.as<double>(), m, ctx->ich.as<int32_t>(), ctx->list.as<int32_t>(), ctl_pre,
+                ctx->f_dev.as<IntegrandDesc>(), opt ? 1 : 0, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens,
+                pp_ptr(ctx));
+            LAUNCHED();
+        }
         // the cut: the needed-th record whose value is not NaN
         k_block_count<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(rec_ok, ctl_pre,
                                                                                  ctx->block_count.as<int32_t>());
@@ -752,7 +831,7 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
                                                  ctx->ctl.as<RoundCtl>());
         LAUNCHED();
         k_mc_accum<<<static_cast<unsigned>(nb_w), kWgtBlock, acc_smem, ctx->stream>>>(
-            ctx->ctl.as<RoundCtl>(), m, nch, D, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens, opt ? 1 : 0,
+            ctx->ctl.as<RoundCtl>(), m, nch, D, static_cast<int>(hist_n), rec_val, rec_wgt, rec_ok, rec_slot, rec_dens, opt ? 1 : 0,
             guard_alpha ? 1 : 0, ctx->hist.as<double>(), ctx->part.as<double>());
         LAUNCHED();
         k_mc_reduce<<<kPartFixed + nch, 256, 0, ctx->stream>>>(ctx->part.as<double>(), nch, ctx->ctl.as<RoundCtl>(),

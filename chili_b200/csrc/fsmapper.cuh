@@ -453,7 +453,7 @@ __device__ __forceinline__ double combined_weight_pp(const PointProgram *__restr
             for (int d = 0; d < dims; ++d) xs[d] = x[d];
         const double vw = grid_weight(grids + c * gsz, dims, bins, x, before);
         acc += __ldg(alpha + c) / dc / vw;
-        if (dens) dens[c * dens_stride] = dc;
+        if (dens) dens[static_cast<size_t>(c) * dens_stride] = dc;
     }
     return 1.0 / acc;
 }

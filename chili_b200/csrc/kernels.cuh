@@ -401,7 +401,7 @@ __device__ __forceinline__ double combined_weight(const ChannelProgram *__restri
             for (int d = 0; d < dims; ++d) xs[d] = x[d];
         const double vw = grid_weight(grids + c * gsz, dims, bins, x, before);
         acc += __ldg(alpha + c) / dc / vw;
-        if (dens) dens[c * dens_stride] = dc;
+        if (dens) dens[static_cast<size_t>(c) * dens_stride] = dc;
     }
     return 1.0 / acc;
 }
@@ -590,9 +590,11 @@ __global__ void __launch_bounds__(kWgtBlock) k_mc_weight(
     const IntegrandDesc *__restrict__ f, int should_opt, double *__restrict__ rec_val, double *__restrict__ rec_wgt,
     uint8_t *__restrict__ rec_ok, int32_t *__restrict__ rec_slot, double *__restrict__ rec_dens,
     const PointProgram *__restrict__ pp) {
+    // records are laid out with stride m (the chunk size, known on the host);
+    // only the first ctl->n_acc entries are written
     const long long n = ctl->n_acc;
     const long long i = blockIdx.x * static_cast<long long>(kWgtBlock) + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || i >= m) return;
     const long long k = list[i];
     const int c_sel = ich_arr[k];
     V4 mom[CHILI_MAX_SLOTS];
@@ -600,9 +602,10 @@ __global__ void __launch_bounds__(kWgtBlock) k_mc_weight(
         mom[s] = V4{mom_soa[(4 * s + 0) * m + k], mom_soa[(4 * s + 1) * m + k], mom_soa[(4 * s + 2) * m + k],
                     mom_soa[(4 * s + 3) * m + k]};
     double x[CHILI_MAX_DIMS], xs[CHILI_MAX_DIMS];
-    double wgt = pp ? combined_weight_pp(pp, grids, alpha, dims, bins, c_sel, mom, x, xs, rec_dens + i, n,
+    const int stride = static_cast<int>(m);
+    double wgt = pp ? combined_weight_pp(pp, grids, alpha, dims, bins, c_sel, mom, x, xs, rec_dens + i, stride,
                                          edge_before_table(dims, bins))
-                    : combined_weight(progs, grids, alpha, nch, dims, bins, c_sel, mom, x, xs, rec_dens + i, n);
+                    : combined_weight(progs, grids, alpha, nch, dims, bins, c_sel, mom, x, xs, rec_dens + i, stride);
     const double fv = eval_momenta(f, mom, n_ext);
     double val = wgt == 0 ? 0 : fv * wgt;
     uint8_t ok = 1;
@@ -619,7 +622,7 @@ __global__ void __launch_bounds__(kWgtBlock) k_mc_weight(
         for (int j = 0; j < dims; ++j) {
             const int b = find_bin(g + j * (bins + 1), bins, xs[j]);
             const int s = j * bins + b;
-            rec_slot[j * n + i] = s >= 0 ? base + s : -1;
+            rec_slot[j * m + i] = s >= 0 ? base + s : -1;
         }
     }
 }
@@ -656,14 +659,15 @@ __global__ void k_cut_finalize(const RoundCtl *__restrict__ ctl_list, const Roun
 // partials, histogram adds, alpha-training terms val^2 w / dens_j
 // (MultiChannel.hh:167-180).  Dynamic shared memory: (kWgtBlock/32) * nch.
 __global__ void __launch_bounds__(kWgtBlock) k_mc_accum(
-    const RoundCtl *__restrict__ ctl, long long n_rec, int nch, int dims, const double *__restrict__ rec_val,
+    const RoundCtl *__restrict__ ctl, long long n_rec, int nch, int dims, int hist_size,
+    const double *__restrict__ rec_val,
     const double *__restrict__ rec_wgt, const uint8_t *__restrict__ rec_ok, const int32_t *__restrict__ rec_slot,
     const double *__restrict__ rec_dens, int should_opt, int guard, double *__restrict__ hist,
     double *__restrict__ part) {
     extern __shared__ double atr_s[];  // (kWgtBlock/32) * nch
     const long long n_list = ctl->n_acc;
     const long long i = blockIdx.x * static_cast<long long>(kWgtBlock) + threadIdx.x;
-    const bool active = i < n_list;
+    const bool active = i < n_list && i < n_rec;
     const double val = active ? rec_val[i] : 0.0;
     const double wgt = active ? rec_wgt[i] : 0.0;
     double cnt = active ? 1.0 : 0.0;
@@ -673,7 +677,7 @@ __global__ void __launch_bounds__(kWgtBlock) k_mc_accum(
     if (active && should_opt) {
         for (int j = 0; j < dims; ++j) {
             const int s = rec_slot[j * n_rec + i];
-            if (s >= 0) atomicAdd(hist + s, val2);
+            if (s >= 0 && s < hist_size) atomicAdd(hist + s, val2);
             else dropped += 1;
         }
     }

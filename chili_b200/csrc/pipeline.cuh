@@ -1,0 +1,254 @@
+// pipeline.cuh -- the phased form of the all-channel weight pass.
+//
+// Integrand::GenerateWeight (include/Channel/Integrand.hh:112-123) evaluated
+// for a list of points in four kernels with small per-thread state, instead of
+// one thread running every channel's inverse mapping from start to end:
+//   k_pp_nodes     gathers the point's external momenta and sums the compound
+//                  currents (one thread per point)
+//   k_pp_items     every t-channel entry, decay propagator weight and
+//                  two-body decay weight (one thread per point and item)
+//   k_pp_chains    every t-channel chain's weight and last uniform (one thread
+//                  per point and chain)
+//   k_pp_assemble  per point, the channel loop: each channel's density is the
+//                  product of its items in the reference's order, its uniforms
+//                  come from the memo slots through the position maps (held in
+//                  registers: DIMS is a compile-time constant), the grid
+//                  weight follows, then the combined weight, the integrand and
+//                  the records of k_mc_weight.
+// Intermediate values live in SoA buffers [slot][point] with stride m, so
+// every access of a warp is coalesced.
+#pragma once
+
+#include "channel_program.h"
+#include "common.cuh"
+#include "fsmapper.cuh"
+#include "grid.cuh"
+#include "integrands.cuh"
+
+namespace chili_dev {
+
+__device__ __forceinline__ V4 load_v4(const double *__restrict__ soa, int node, long long m, long long i) {
+    return V4{soa[(4 * node + 0) * m + i], soa[(4 * node + 1) * m + i], soa[(4 * node + 2) * m + i],
+              soa[(4 * node + 3) * m + i]};
+}
+__device__ __forceinline__ void store_v4(double *__restrict__ soa, int node, long long m, long long i, V4 v) {
+    soa[(4 * node + 0) * m + i] = v.e;
+    soa[(4 * node + 1) * m + i] = v.x;
+    soa[(4 * node + 2) * m + i] = v.y;
+    soa[(4 * node + 3) * m + i] = v.z;
+}
+
+// Nodes of point i = list[i]: externals copied from the chunk's momenta
+// (mom_soa, stride mc), compounds summed as the reference's tmp_mom.
+__global__ void __launch_bounds__(256) k_pp_nodes(const PointProgram *__restrict__ pp, const double *__restrict__ mom_soa,
+                                                  long long mc, const int32_t *__restrict__ list,
+                                                  const long long *__restrict__ n_list, double *__restrict__ node_soa,
+                                                  long long m) {
+    const long long i = blockIdx.x * 256ll + threadIdx.x;
+    if (i >= *n_list || i >= m) return;
+    const long long k = list[i];
+    const int ne = pp->n_ext, nn = pp->n_nodes;
+    for (int s = 0; s < ne; ++s) store_v4(node_soa, s, m, i, load_v4(mom_soa, s, mc, k));
+    for (int s = ne; s < nn; ++s)
+        store_v4(node_soa, s, m, i, load_v4(node_soa, pp->node_a[s], m, i) + load_v4(node_soa, pp->node_b[s], m, i));
+}
+
+// One thread per (point, item): items 0..n_tents-1 are t-channel entries
+// (Channel.cc:160-186), then decay weights (Channel.cc:83-113), then two-body
+// decays (Channel.cc:222-237).
+__global__ void __launch_bounds__(256) k_pp_items(const PointProgram *__restrict__ pp,
+                                                  const double *__restrict__ node_soa,
+                                                  const long long *__restrict__ n_list, long long m,
+                                                  double *__restrict__ memo) {
+    const long long i = blockIdx.x * 256ll + threadIdx.x;
+    if (i >= *n_list || i >= m) return;
+    int item = blockIdx.y;
+    const double sqrts = pp->sqrts, ptmax = pp->ptmax;
+    if (item < pp->n_tents) {
+        const int t = item;
+        const double ptmin = pp->tent_ptmin[t];
+        const V4 q = load_v4(node_soa, pp->tent_node[t], m, i);
+        const double pt = sqrt(pt2(q));
+        const double f2 = 2 * ptmin + pt;
+        double *o = memo + static_cast<long long>(pp->memo_tent + 5 * t) * m + i;
+        o[0] = pt * ptmax / 2 / ptmin / (2 * ptmin + ptmax) * (f2 * f2);
+        o[2 * m] = pt * (ptmax + 2 * ptmin) / (ptmax * (pt + 2 * ptmin));
+        double etamax = sqrts / 2 / pt;
+        etamax = log(etamax + sqrt(etamax * etamax - 1));
+        etamax = isnan(etamax) ? 99 : etamax;
+        etamax = std_min(etamax, pp->tent_etacut[t]);
+        o[m] = 2 * etamax * 2 * kPi;
+        o[3 * m] = (rapidity(q) / etamax + 1) / 2;
+        o[4 * m] = phi_0_2pi(q) / 2 / kPi;
+        return;
+    }
+    item -= pp->n_tents;
+    if (item < pp->n_dws) {
+        const int k = item;
+        const V4 a = load_v4(node_soa, pp->dw_c1[k], m, i), b = load_v4(node_soa, pp->dw_c2[k], m, i);
+        const double r = sqrt(fabs(mass2(a))) + sqrt(fabs(mass2(b)));
+        const double smin = std_max(std_max(r * r, pp->dw_smin2[k]), pp->dw_cut[k]);
+        const double s = mass2(load_v4(node_soa, pp->dw_node[k], m, i));
+        double u;
+        const double w = pp->dw_massless[k] ? massless_prop_weight(0.99, smin, pp->dw_smax[k], s, u)
+                                            : massive_prop_weight(pp->dw_mass[k], pp->dw_width[k], smin,
+                                                                  pp->dw_smax[k], s, u);
+        double *o = memo + static_cast<long long>(pp->memo_dw + 2 * k) * m + i;
+        o[0] = w;
+        o[m] = u;
+        return;
+    }
+    item -= pp->n_dws;
+    if (item < pp->n_sws) {
+        const int k = item;
+        double r1, r2;
+        const double w = schannel_weight(load_v4(node_soa, pp->sw_a[k], m, i), load_v4(node_soa, pp->sw_b[k], m, i),
+                                         r1, r2);
+        double *o = memo + static_cast<long long>(pp->memo_sw + 3 * k) * m + i;
+        o[0] = w;
+        o[m] = r1;
+        o[2 * m] = r2;
+    }
+}
+
+// One thread per (point, chain): WgtTChan's weight and last uniform
+// (Channel.cc:160-202), with the entries' factors taken from the memo.
+__global__ void __launch_bounds__(256) k_pp_chains(const PointProgram *__restrict__ pp,
+                                                   const double *__restrict__ node_soa,
+                                                   const long long *__restrict__ n_list, long long m,
+                                                   double *__restrict__ memo, uint8_t *__restrict__ cfail) {
+    const long long i = blockIdx.x * 256ll + threadIdx.x;
+    if (i >= *n_list || i >= m) return;
+    const int c = blockIdx.y;
+    const double sqrts = pp->sqrts;
+    double wt = kTwoPi;
+    V4 psum{0., 0., 0., 0.};
+    const int len = pp->chain_len[c];
+    for (int e = 0; e < len; ++e) {
+        const int t = pp->chain_tent[c][e];
+        const double *tm = memo + static_cast<long long>(pp->memo_tent + 5 * t) * m + i;
+        wt *= pp->inv16pi3;
+        wt *= tm[0];
+        wt *= tm[m];
+        psum = psum + load_v4(node_soa, pp->tent_node[t], m, i);
+    }
+    const V4 q = load_v4(node_soa, pp->chain_last[c], m, i);
+    const double mjets2 = mass2(psum);
+    const double yjets = rapidity(psum);
+    const double ptj2 = pt2(psum);
+    const double qt = sqrt(mass2(q) + ptj2);
+    const double mt = sqrt(mjets2 + ptj2);
+    const double yv = rapidity(q);
+    const double ymin = -log(sqrts / qt * (1 - mt / sqrts * exp(-yjets)));
+    const double ymax = log(sqrts / qt * (1 - mt / sqrts * exp(yjets)));
+    const double dely = ymax - ymin;
+    double *o = memo + static_cast<long long>(pp->memo_chain + 2 * c) * m + i;
+    if (isnan(ymax) || isnan(ymin)) {
+        o[0] = 0;
+        o[m] = 0;
+        cfail[c * m + i] = 1;
+    } else {
+        o[0] = wt * (dely / sqrts / sqrts);
+        o[m] = (yv - ymin) / dely;
+        cfail[c * m + i] = 0;
+    }
+}
+
+// Pair Breit-Wigner / t-channel integrand reading the externals from the
+// node buffer (same arithmetic as eval_momenta).
+__device__ __forceinline__ double eval_momenta_soa(const IntegrandDesc *__restrict__ f,
+                                                   const double *__restrict__ node_soa, long long m, long long i,
+                                                   int n_ext) {
+    if (f->kind != CHILI_FUNC_PROPAGATOR && f->kind != CHILI_FUNC_PROPAGATOR_TOP2) return 1.0;
+    const bool top2 = f->kind == CHILI_FUNC_PROPAGATOR_TOP2;
+    const double mm = f->p[0], g = f->p[1], mt = f->p[2];
+    const double m2 = mm * mm, mw2 = mm * mm * g * g, mt2 = mt * mt;
+    double sum = 0, big1 = 0, big2 = 0;
+    for (int a = 2; a < n_ext; ++a) {
+        const V4 pa = load_v4(node_soa, a, m, i);
+        for (int b = a + 1; b < n_ext; ++b) {
+            const double d = mass2(pa + load_v4(node_soa, b, m, i)) - m2;
+            const double bw = 1.0 / (d * d + mw2);
+            sum += bw;
+            if (bw > big1) {
+                big2 = big1;
+                big1 = bw;
+            } else if (bw > big2) {
+                big2 = bw;
+            }
+        }
+    }
+    const V4 p0 = load_v4(node_soa, 0, m, i);
+    double tprod = 1;
+    for (int b = 2; b < n_ext; ++b) tprod *= 1.0 / (fabs(mass2(p0 + load_v4(node_soa, b, m, i))) + mt2);
+    return (top2 ? big1 * big2 : sum) * tprod;
+}
+
+// Per point: the channel loop, the combined weight, the integrand and the
+// records (rec_* as in k_mc_weight).  running is the value the shared uniform
+// buffer holds at position DIMS-1 (zero before the first channel).
+template <int DIMS>
+__global__ void __launch_bounds__(128) k_pp_assemble(
+    const PointProgram *__restrict__ pp, const double *__restrict__ grids, const double *__restrict__ alpha,
+    int bins, const double *__restrict__ node_soa, const double *__restrict__ memo,
+    const uint8_t *__restrict__ cfail, const int32_t *__restrict__ ich_arr, const int32_t *__restrict__ list,
+    const long long *__restrict__ n_list, long long m, const IntegrandDesc *__restrict__ f, int should_opt,
+    double *__restrict__ rec_val, double *__restrict__ rec_wgt, uint8_t *__restrict__ rec_ok,
+    int32_t *__restrict__ rec_slot, double *__restrict__ rec_dens) {
+    const long long i = blockIdx.x * 128ll + threadIdx.x;
+    if (i >= *n_list || i >= m) return;
+    const int ich = ich_arr[list[i]];
+    const int nch = pp->nch;
+    const double fb = static_cast<double>(bins);
+    const double before = edge_before_table(DIMS, bins);
+    const size_t gsz = static_cast<size_t>(DIMS) * (bins + 1);
+    double running = 0.0, acc = 0.0;
+    for (int c = 0; c < nch; ++c) {
+        const PPChannel &C = pp->ch[c];
+        const bool fail = cfail[C.chain * m + i] != 0;
+        double wdec = 1;
+        for (int k = 0; k < C.n_dec; ++k) {
+            wdec *= memo[static_cast<long long>(pp->memo_dw + 2 * C.dw[k]) * m + i];
+            wdec /= kTwoPi;
+        }
+        const double wt = memo[static_cast<long long>(pp->memo_chain + 2 * C.chain) * m + i];
+        double ws = 1;
+        for (int k = 0; k < C.n_sd; ++k) ws *= memo[static_cast<long long>(pp->memo_sw + 3 * C.sw[k]) * m + i];
+        const double dc = wdec * wt * ws;
+        const int16_t *pos = fail ? pp->pos_src_fail[c] : pp->pos_src[c];
+        double x[DIMS];
+#pragma unroll
+        for (int p = 0; p < DIMS; ++p) {
+            const int s = pos[p];
+            x[p] = s >= 0 ? memo[static_cast<long long>(s) * m + i] : running;
+        }
+        running = x[DIMS - 1];
+        const double *g = grids + c * gsz;
+        double vw = 1.0;
+        const bool chosen = should_opt && c == ich;
+#pragma unroll
+        for (int p = 0; p < DIMS; ++p) {
+            const int b = find_bin(g + p * (bins + 1), bins, x[p]);
+            vw = __dmul_rn(vw, __dmul_rn(bin_width(g, bins, p, b, before), fb));
+            if (chosen) {
+                const int s = p * bins + b;
+                rec_slot[p * m + i] = s >= 0 ? c * DIMS * bins + s : -1;
+            }
+        }
+        acc += __ldg(alpha + c) / dc / vw;
+        rec_dens[static_cast<long long>(c) * m + i] = dc;
+    }
+    double wgt = 1.0 / acc;
+    const double fv = eval_momenta_soa(f, node_soa, m, i, pp->n_ext);
+    double val = wgt == 0 ? 0 : fv * wgt;
+    uint8_t ok = 1;
+    if (isnan(val)) {
+        val = wgt = 0;
+        ok = 0;
+    }
+    rec_val[i] = val;
+    rec_wgt[i] = wgt;
+    rec_ok[i] = ok;
+}
+
+}  // namespace chili_dev

@@ -195,11 +195,16 @@ def test_combined_weight(ctx_factory, rng, mc2, point_program):
     assert np.percentile(rel(dens[df], dens_r[df]), 99) < RTOL
 
 
-@pytest.mark.parametrize("point_program", [1, 0])
-def test_multichannel_iteration_matches_reference(ctx_factory, rng, mc2, point_program):
+WEIGHT_PATHS = {"pipeline": dict(point_program=1, pipeline=1), "fused_point_program": dict(point_program=1, pipeline=0),
+                "per_channel": dict(point_program=0, pipeline=0)}
+
+
+@pytest.mark.parametrize("path", list(WEIGHT_PATHS))
+def test_multichannel_iteration_matches_reference(ctx_factory, rng, mc2, path):
     ncalls = 20_000
     ctx, R, params = _mc_pair(ctx_factory, mc2, 100, ncalls, rng)
-    ctx.set_option("point_program", point_program)
+    for k, v in WEIGHT_PATHS[path].items():
+        ctx.set_option(k, v)
     for it in range(3):
         u = uniforms53(rng, (3 * ncalls, R.ndims + 1))
         st, info = ctx.multichannel_iterate(params, u=u, guard=True)
