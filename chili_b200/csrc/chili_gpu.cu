@@ -75,6 +75,7 @@ struct chili_ctx {
     bool use_pipeline = true;  // option "pipeline": phased weight pass
     PointProgram pp_host;      // host copy (sizes of the memo buffers)
     DevBuf node_soa, memo, cfail;
+    DevBuf hints, sorted;      // hinted bin search tables of the grids
     // channel weights: alpha[CH], best[CH], cp[CH], min_diff
     DevBuf alpha_buf;
     bool alpha_set = false;
@@ -198,50 +199,67 @@ bool pipeline_dims_ok(int d) {
 }
 
 template <int D>
-void launch_assemble(chili_ctx *ctx, long long m, int bins, int opt, const long long *n_list, double *rec_val,
-                     double *rec_wgt, uint8_t *rec_ok, int32_t *rec_slot, double *rec_dens) {
-    k_pp_assemble<D><<<static_cast<unsigned>((m + 127) / 128), 128, 0, ctx->stream>>>(
-        ctx->point_prog.as<PointProgram>(), ctx->edges.as<double>(), alpha_ptr(ctx), bins, ctx->node_soa.as<double>(),
-        ctx->memo.as<double>(), ctx->cfail.as<uint8_t>(), ctx->ich.as<int32_t>(), ctx->list.as<int32_t>(), n_list, m,
+void launch_assemble(chili_ctx *ctx, long long base, long long T, long long mr, int bins, int opt,
+                     const long long *n_list, double *rec_val, double *rec_wgt, uint8_t *rec_ok, int32_t *rec_slot,
+                     double *rec_dens) {
+    k_pp_assemble<D><<<static_cast<unsigned>((T + 127) / 128), 128, 0, ctx->stream>>>(
+        ctx->point_prog.as<PointProgram>(), ctx->edges.as<double>(), ctx->hints.as<uint16_t>(),
+        ctx->sorted.as<uint8_t>(), alpha_ptr(ctx), bins, ctx->node_soa.as<double>(), ctx->memo.as<double>(),
+        ctx->cfail.as<uint8_t>(), ctx->ich.as<int32_t>(), ctx->list.as<int32_t>(), n_list, base, T, mr,
         ctx->f_dev.as<IntegrandDesc>(), opt, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens);
 }
 
-// The phased weight pass (pipeline.cuh) over the PreProcess-accepted points
-// of a chunk of m counters.
-int launch_pipeline(chili_ctx *ctx, long long m, int bins, bool opt, RoundCtl *ctl_pre, double *rec_val,
-                    double *rec_wgt, uint8_t *rec_ok, int32_t *rec_slot, double *rec_dens) {
+// The phased weight pass (pipeline.cuh) over the n_pre PreProcess-accepted
+// points of a chunk of m counters, in tiles of at most kPipeTile points so
+// that the memo buffers stay in L2.
+constexpr long long kPipeTile = 1 << 16;
+
+int launch_pipeline(chili_ctx *ctx, long long m, long long n_pre, int bins, bool opt, RoundCtl *ctl_pre,
+                    double *rec_val, double *rec_wgt, uint8_t *rec_ok, int32_t *rec_slot, double *rec_dens) {
     const PointProgram &P = ctx->pp_host;
     const PointProgram *pp = ctx->point_prog.as<PointProgram>();
-    CK(ctx->node_soa.ensure(sizeof(double) * 4 * P.n_nodes * m));
-    CK(ctx->memo.ensure(sizeof(double) * std::max(1, P.n_memo) * m));
-    CK(ctx->cfail.ensure(static_cast<size_t>(std::max(1, P.n_chains)) * m));
+    const long long T = std::min<long long>(kPipeTile, std::max<long long>(n_pre, 1));
+    CK(ctx->node_soa.ensure(sizeof(double) * 4 * P.n_nodes * T));
+    CK(ctx->memo.ensure(sizeof(double) * std::max(1, P.n_memo) * T));
+    CK(ctx->cfail.ensure(static_cast<size_t>(std::max(1, P.n_chains)) * T));
     const long long *n_list = reinterpret_cast<const long long *>(
         reinterpret_cast<const char *>(ctl_pre) + offsetof(RoundCtl, n_acc));
-    const unsigned gx = static_cast<unsigned>((m + 255) / 256);
-    k_pp_nodes<<<gx, 256, 0, ctx->stream>>>(pp, ctx->mom_soa.as<double>(), m, ctx->list.as<int32_t>(), n_list,
-                                             ctx->node_soa.as<double>(), m);
-    LAUNCHED();
+    const unsigned gx = static_cast<unsigned>((T + 255) / 256);
     const int n_items = P.n_tents + P.n_dws + P.n_sws;
-    if (n_items > 0) {
-        k_pp_items<<<dim3(gx, n_items), 256, 0, ctx->stream>>>(pp, ctx->node_soa.as<double>(), n_list, m,
-                                                                ctx->memo.as<double>());
+    const int o = opt ? 1 : 0;
+    for (long long base = 0; base < n_pre; base += T) {
+        k_pp_nodes<<<gx, 256, 0, ctx->stream>>>(pp, ctx->mom_soa.as<double>(), m, ctx->list.as<int32_t>(), n_list,
+                                                 base, ctx->node_soa.as<double>(), T);
+        LAUNCHED();
+        if (n_items > 0) {
+            k_pp_items<<<dim3(gx, n_items), 256, 0, ctx->stream>>>(pp, ctx->node_soa.as<double>(), n_list, base, T,
+                                                                    ctx->memo.as<double>());
+            LAUNCHED();
+        }
+        k_pp_chains<<<dim3(gx, P.n_chains), 256, 0, ctx->stream>>>(pp, ctx->node_soa.as<double>(), n_list, base, T,
+                                                                    ctx->memo.as<double>(), ctx->cfail.as<uint8_t>());
+        LAUNCHED();
+        switch (P.ndims) {
+#define CHILI_ASM(D) \
+    case D: launch_assemble<D>(ctx, base, T, m, bins, o, n_list, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens); break;
+            CHILI_ASM(1) CHILI_ASM(4) CHILI_ASM(7) CHILI_ASM(10) CHILI_ASM(13) CHILI_ASM(16) CHILI_ASM(19) CHILI_ASM(22)
+#undef CHILI_ASM
+        default: return fail(ctx, CHILI_ERR_STATE, "no phased weight kernel for this dimension");
+        }
         LAUNCHED();
     }
-    k_pp_chains<<<dim3(gx, P.n_chains), 256, 0, ctx->stream>>>(pp, ctx->node_soa.as<double>(), n_list, m,
-                                                                ctx->memo.as<double>(), ctx->cfail.as<uint8_t>());
-    LAUNCHED();
-    const int o = opt ? 1 : 0;
-    switch (P.ndims) {
-    case 1: launch_assemble<1>(ctx, m, bins, o, n_list, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens); break;
-    case 4: launch_assemble<4>(ctx, m, bins, o, n_list, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens); break;
-    case 7: launch_assemble<7>(ctx, m, bins, o, n_list, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens); break;
-    case 10: launch_assemble<10>(ctx, m, bins, o, n_list, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens); break;
-    case 13: launch_assemble<13>(ctx, m, bins, o, n_list, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens); break;
-    case 16: launch_assemble<16>(ctx, m, bins, o, n_list, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens); break;
-    case 19: launch_assemble<19>(ctx, m, bins, o, n_list, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens); break;
-    case 22: launch_assemble<22>(ctx, m, bins, o, n_list, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens); break;
-    default: return fail(ctx, CHILI_ERR_STATE, "no phased weight kernel for this dimension");
-    }
+    return CHILI_OK;
+}
+
+// Hint tables of the grid set (grid.cuh, find_bin_hinted), rebuilt after
+// every change of the edges.
+int rebuild_hints(chili_ctx *ctx) {
+    const int H = kHintPerBin * ctx->bins;
+    CK(ctx->hints.ensure(sizeof(uint16_t) * static_cast<size_t>(ctx->g_nch) * ctx->dims * (H + 1)));
+    CK(ctx->sorted.ensure(static_cast<size_t>(ctx->g_nch) * ctx->dims));
+    k_build_hints<<<dim3(ctx->dims, ctx->g_nch), 128, 0, ctx->stream>>>(ctx->edges.as<double>(), ctx->dims, ctx->bins,
+                                                                        ctx->hints.as<uint16_t>(),
+                                                                        ctx->sorted.as<uint8_t>());
     LAUNCHED();
     return CHILI_OK;
 }
@@ -290,7 +308,7 @@ int chili_gpu_destroy(chili_ctx *ctx) {
     if (!ctx) return CHILI_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    DevBuf *bufs[] = {&ctx->edges, &ctx->edges_tmp, &ctx->progs, &ctx->point_prog, &ctx->node_soa, &ctx->memo, &ctx->cfail, &ctx->alpha_buf, &ctx->f_dev, &ctx->mom_soa,
+    DevBuf *bufs[] = {&ctx->edges, &ctx->edges_tmp, &ctx->progs, &ctx->point_prog, &ctx->node_soa, &ctx->memo, &ctx->cfail, &ctx->hints, &ctx->sorted, &ctx->alpha_buf, &ctx->f_dev, &ctx->mom_soa,
                       &ctx->ich, &ctx->flag, &ctx->list, &ctx->block_count, &ctx->block_off, &ctx->part,
                       &ctx->hist, &ctx->round_res, &ctx->acc, &ctx->ctl, &ctx->status, &ctx->v_part,
                       &ctx->v_hist, &ctx->v_train, &ctx->v_out, &ctx->rec, &ctx->ctl3};
@@ -361,6 +379,7 @@ int chili_gpu_set_grids(chili_ctx *ctx, const double *edges, int nch, int dims, 
     ctx->g_nch = nch;
     ctx->dims = dims;
     ctx->bins = bins;
+    if ((rc = rebuild_hints(ctx))) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     return CHILI_OK;
 }
@@ -435,7 +454,7 @@ static int adapt_grids(chili_ctx *ctx, int first, int count, double alpha, const
         skip_zero, ctx->status.as<int>());
     LAUNCHED();
     std::swap(ctx->edges, ctx->edges_tmp);
-    return CHILI_OK;
+    return rebuild_hints(ctx);
 }
 
 int chili_gpu_grid_adapt(chili_ctx *ctx, int ch, double alpha, const double *train) {
@@ -466,7 +485,7 @@ int chili_gpu_grid_split(chili_ctx *ctx, int nsplit) {
     std::swap(ctx->edges, ctx->edges_tmp);
     CK(ctx->edges_tmp.ensure(bytes));
     ctx->bins = nb;
-    return CHILI_OK;
+    return rebuild_hints(ctx);
 }
 
 // ----------------------------------------------------------------- integrand
@@ -810,7 +829,10 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
             ctx->flag.as<uint8_t>(), ctx->block_off.as<long long>(), ctl_pre, m, ctx->list.as<int32_t>());
         LAUNCHED();
         if (pipe) {
-            int rc2 = launch_pipeline(ctx, m, B, opt, ctl_pre, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens);
+            CK(cudaMemcpyAsync(ctx->ctl_host, ctl_pre, sizeof(RoundCtl), cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            const long long n_pre = ctx->ctl_host->n_acc;
+            int rc2 = launch_pipeline(ctx, m, n_pre, B, opt, ctl_pre, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens);
             if (rc2) return rc2;
         } else {
             k_mc_weight<<<static_cast<unsigned>(nb_w), kWgtBlock, 0, ctx->stream>>>(

@@ -102,4 +102,72 @@ __device__ __forceinline__ int train_slot(int d, int bins, int b) {
     return s;  // b == -1 and d == 0 gives -1
 }
 
+// ------------------------------------------------------------ hinted search
+// For a monotone edge table the cells of a uniform H-cell grid over [0, 1)
+// bracket lower_bound: with cell(v) = clamp((int)(v*H), 0, H) (monotone in v),
+// every edge in a cell below x's cell is < x and every edge in a cell above it
+// is > x, so lower_bound(x) lies in [hint[c], hint[c+1]) where hint[j] counts
+// the edges e[k], k < bins, with cell(e[k]) < j.  hint has H+1 entries per
+// (grid, dim); sorted[] marks the tables the shortcut may use (monotone, no
+// NaN); other tables and x outside [0, 1) take the plain search.
+constexpr int kHintPerBin = 2;
+
+__device__ __forceinline__ int edge_cell(double v, int H) {
+    if (!(v > 0.0)) return 0;  // also NaN (excluded by sorted[] anyway)
+    const double p = v * static_cast<double>(H);
+    return p >= static_cast<double>(H) ? H : static_cast<int>(p);
+}
+
+__device__ __forceinline__ int find_bin_hinted(const double *__restrict__ e, const uint16_t *__restrict__ hint,
+                                               bool sorted, int bins, int H, double x) {
+    if (!sorted || !(x >= 0.0 && x < 1.0)) return find_bin(e, bins, x);
+    const int c = static_cast<int>(x * static_cast<double>(H));  // < H for x < 1
+    int first = __ldg(hint + c);
+    int len = __ldg(hint + c + 1) - first;
+    while (len > 0) {  // lower_bound inside the bracket
+        const int half = len >> 1;
+        const int mid = first + half;
+        if (__ldg(e + mid) < x) {
+            first = mid + 1;
+            len = len - half - 1;
+        } else {
+            len = half;
+        }
+    }
+    return first - 1;
+}
+
+// One block per (dim = blockIdx.x, grid = blockIdx.y): the hint table and the
+// monotone flag of that edge table.
+__global__ void k_build_hints(const double *__restrict__ grids, int dims, int bins, uint16_t *__restrict__ hints,
+                              uint8_t *__restrict__ sorted) {
+    const int d = blockIdx.x, c = blockIdx.y;
+    const int H = kHintPerBin * bins;
+    const double *e = grids + (static_cast<size_t>(c) * dims + d) * (bins + 1);
+    uint16_t *h = hints + (static_cast<size_t>(c) * dims + d) * (H + 1);
+    int bad = 0;
+    for (int k = threadIdx.x; k < bins; k += blockDim.x) {
+        const double a = e[k];
+        if (a != a) bad = 1;
+        if (k + 1 < bins && !(a <= e[k + 1])) bad = 1;
+    }
+    bad = __syncthreads_or(bad);
+    if (threadIdx.x == 0) sorted[static_cast<size_t>(c) * dims + d] = bad ? 0 : 1;
+    if (bad) return;
+    for (int j = threadIdx.x; j <= H; j += blockDim.x) {
+        // first k in [0, bins) with cell(e[k]) >= j (cells are monotone)
+        int first = 0, len = bins;
+        while (len > 0) {
+            const int half = len >> 1, mid = first + half;
+            if (edge_cell(e[mid], H) < j) {
+                first = mid + 1;
+                len = len - half - 1;
+            } else {
+                len = half;
+            }
+        }
+        h[j] = static_cast<uint16_t>(first);
+    }
+}
+
 }  // namespace chili_dev

@@ -42,11 +42,11 @@ __device__ __forceinline__ void store_v4(double *__restrict__ soa, int node, lon
 // (mom_soa, stride mc), compounds summed as the reference's tmp_mom.
 __global__ void __launch_bounds__(256) k_pp_nodes(const PointProgram *__restrict__ pp, const double *__restrict__ mom_soa,
                                                   long long mc, const int32_t *__restrict__ list,
-                                                  const long long *__restrict__ n_list, double *__restrict__ node_soa,
-                                                  long long m) {
-    const long long i = blockIdx.x * 256ll + threadIdx.x;
-    if (i >= *n_list || i >= m) return;
-    const long long k = list[i];
+                                                  const long long *__restrict__ n_list, long long base,
+                                                  double *__restrict__ node_soa, long long m) {
+    const long long i = blockIdx.x * 256ll + threadIdx.x;  // tile-local point
+    if (i >= m || base + i >= *n_list) return;
+    const long long k = list[base + i];
     const int ne = pp->n_ext, nn = pp->n_nodes;
     for (int s = 0; s < ne; ++s) store_v4(node_soa, s, m, i, load_v4(mom_soa, s, mc, k));
     for (int s = ne; s < nn; ++s)
@@ -58,10 +58,10 @@ __global__ void __launch_bounds__(256) k_pp_nodes(const PointProgram *__restrict
 // decays (Channel.cc:222-237).
 __global__ void __launch_bounds__(256) k_pp_items(const PointProgram *__restrict__ pp,
                                                   const double *__restrict__ node_soa,
-                                                  const long long *__restrict__ n_list, long long m,
+                                                  const long long *__restrict__ n_list, long long base, long long m,
                                                   double *__restrict__ memo) {
-    const long long i = blockIdx.x * 256ll + threadIdx.x;
-    if (i >= *n_list || i >= m) return;
+    const long long i = blockIdx.x * 256ll + threadIdx.x;  // tile-local point
+    if (i >= m || base + i >= *n_list) return;
     int item = blockIdx.y;
     const double sqrts = pp->sqrts, ptmax = pp->ptmax;
     if (item < pp->n_tents) {
@@ -115,10 +115,10 @@ __global__ void __launch_bounds__(256) k_pp_items(const PointProgram *__restrict
 // (Channel.cc:160-202), with the entries' factors taken from the memo.
 __global__ void __launch_bounds__(256) k_pp_chains(const PointProgram *__restrict__ pp,
                                                    const double *__restrict__ node_soa,
-                                                   const long long *__restrict__ n_list, long long m,
+                                                   const long long *__restrict__ n_list, long long base, long long m,
                                                    double *__restrict__ memo, uint8_t *__restrict__ cfail) {
-    const long long i = blockIdx.x * 256ll + threadIdx.x;
-    if (i >= *n_list || i >= m) return;
+    const long long i = blockIdx.x * 256ll + threadIdx.x;  // tile-local point
+    if (i >= m || base + i >= *n_list) return;
     const int c = blockIdx.y;
     const double sqrts = pp->sqrts;
     double wt = kTwoPi;
@@ -189,15 +189,19 @@ __device__ __forceinline__ double eval_momenta_soa(const IntegrandDesc *__restri
 // buffer holds at position DIMS-1 (zero before the first channel).
 template <int DIMS>
 __global__ void __launch_bounds__(128) k_pp_assemble(
-    const PointProgram *__restrict__ pp, const double *__restrict__ grids, const double *__restrict__ alpha,
-    int bins, const double *__restrict__ node_soa, const double *__restrict__ memo,
-    const uint8_t *__restrict__ cfail, const int32_t *__restrict__ ich_arr, const int32_t *__restrict__ list,
-    const long long *__restrict__ n_list, long long m, const IntegrandDesc *__restrict__ f, int should_opt,
+    const PointProgram *__restrict__ pp, const double *__restrict__ grids, const uint16_t *__restrict__ hints,
+    const uint8_t *__restrict__ sorted, const double *__restrict__ alpha, int bins,
+    const double *__restrict__ node_soa, const double *__restrict__ memo, const uint8_t *__restrict__ cfail,
+    const int32_t *__restrict__ ich_arr, const int32_t *__restrict__ list, const long long *__restrict__ n_list,
+    long long base, long long m, long long mr, const IntegrandDesc *__restrict__ f, int should_opt,
     double *__restrict__ rec_val, double *__restrict__ rec_wgt, uint8_t *__restrict__ rec_ok,
     int32_t *__restrict__ rec_slot, double *__restrict__ rec_dens) {
+    // i: tile-local point (node/memo/cfail stride m); r: record index (stride mr)
     const long long i = blockIdx.x * 128ll + threadIdx.x;
-    if (i >= *n_list || i >= m) return;
-    const int ich = ich_arr[list[i]];
+    const long long r = base + i;
+    if (i >= m || r >= *n_list) return;
+    const int ich = ich_arr[list[r]];
+    const int H = kHintPerBin * bins;
     const int nch = pp->nch;
     const double fb = static_cast<double>(bins);
     const double before = edge_before_table(DIMS, bins);
@@ -224,19 +228,21 @@ __global__ void __launch_bounds__(128) k_pp_assemble(
         }
         running = x[DIMS - 1];
         const double *g = grids + c * gsz;
+        const uint16_t *hc = hints + static_cast<size_t>(c) * DIMS * (H + 1);
+        const uint8_t *sc = sorted + c * DIMS;
         double vw = 1.0;
         const bool chosen = should_opt && c == ich;
 #pragma unroll
         for (int p = 0; p < DIMS; ++p) {
-            const int b = find_bin(g + p * (bins + 1), bins, x[p]);
+            const int b = find_bin_hinted(g + p * (bins + 1), hc + p * (H + 1), __ldg(sc + p) != 0, bins, H, x[p]);
             vw = __dmul_rn(vw, __dmul_rn(bin_width(g, bins, p, b, before), fb));
             if (chosen) {
                 const int s = p * bins + b;
-                rec_slot[p * m + i] = s >= 0 ? c * DIMS * bins + s : -1;
+                rec_slot[p * mr + r] = s >= 0 ? c * DIMS * bins + s : -1;
             }
         }
         acc += __ldg(alpha + c) / dc / vw;
-        rec_dens[static_cast<long long>(c) * m + i] = dc;
+        rec_dens[static_cast<long long>(c) * mr + r] = dc;
     }
     double wgt = 1.0 / acc;
     const double fv = eval_momenta_soa(f, node_soa, m, i, pp->n_ext);
@@ -246,9 +252,9 @@ __global__ void __launch_bounds__(128) k_pp_assemble(
         val = wgt = 0;
         ok = 0;
     }
-    rec_val[i] = val;
-    rec_wgt[i] = wgt;
-    rec_ok[i] = ok;
+    rec_val[r] = val;
+    rec_wgt[r] = wgt;
+    rec_ok[r] = ok;
 }
 
 }  // namespace chili_dev

@@ -249,3 +249,23 @@ def test_generate_events(ctx_factory, mc2):
     ok = ~np.isnan(mom).any(axis=(1, 2))
     tot = mom[ok].sum(axis=1)
     assert np.max(np.abs(tot)) < 1e-9 * 1000  # momentum conservation (all-outgoing)
+
+
+def test_multichannel_iteration_degenerate_grids(ctx_factory, rng, mc2):
+    """Edge tables that are not monotone (the hinted bin search must fall back
+    to the plain lower_bound) or all zero (what the reference's Adapt leaves for
+    a dimension without data) give the reference's results."""
+    ncalls = 10_000
+    ctx, R, params = _mc_pair(ctx_factory, mc2, 100, ncalls, rng)
+    edges = R.get_grids()
+    edges[3, 2, 10:20] = edges[3, 2, 10:20][::-1].copy()  # non-monotone
+    edges[5, 7, :] = 0.0                                   # all zero
+    edges[8, 0, 50] = np.nan                                # NaN edge
+    ctx.set_grids(edges)
+    R.set_grids(edges)
+    u = uniforms53(rng, (4 * ncalls, R.ndims + 1))
+    st, info = ctx.multichannel_iterate(params, u=u, guard=True)
+    st_r, info_r = R.iterate(u, guard=True)
+    assert info.points_tried == info_r.points_tried
+    assert st.n == st_r.n and st.n_finite == st_r.n_finite
+    assert rel(st.sum, st_r.sum) < 1e-11
