@@ -73,8 +73,9 @@ struct chili_ctx {
     bool have_pp = false;      // the set fits the PointProgram limits
     bool use_pp = true;        // option "point_program"
     bool use_pipeline = true;  // option "pipeline": phased weight pass
+    long long pipe_tile = 1 << 16;  // option "pipeline_tile": points per tile
     PointProgram pp_host;      // host copy (sizes of the memo buffers)
-    DevBuf node_soa, memo, cfail;
+    DevBuf node_soa, memo, cfail, dcv, vwv;
     DevBuf hints, sorted;      // hinted bin search tables of the grids
     // channel weights: alpha[CH], best[CH], cp[CH], min_diff
     DevBuf alpha_buf;
@@ -199,29 +200,29 @@ bool pipeline_dims_ok(int d) {
 }
 
 template <int D>
-void launch_assemble(chili_ctx *ctx, long long base, long long T, long long mr, int bins, int opt,
-                     const long long *n_list, double *rec_val, double *rec_wgt, uint8_t *rec_ok, int32_t *rec_slot,
-                     double *rec_dens) {
-    k_pp_assemble<D><<<static_cast<unsigned>((T + 127) / 128), 128, 0, ctx->stream>>>(
+void launch_channel(chili_ctx *ctx, long long base, long long T, long long mr, int bins, int opt,
+                    const long long *n_list, int32_t *rec_slot, double *rec_dens) {
+    k_pp_channel<D><<<dim3(static_cast<unsigned>((T + 127) / 128), ctx->nch), 128, 0, ctx->stream>>>(
         ctx->point_prog.as<PointProgram>(), ctx->edges.as<double>(), ctx->hints.as<uint16_t>(),
-        ctx->sorted.as<uint8_t>(), alpha_ptr(ctx), bins, ctx->node_soa.as<double>(), ctx->memo.as<double>(),
-        ctx->cfail.as<uint8_t>(), ctx->ich.as<int32_t>(), ctx->list.as<int32_t>(), n_list, base, T, mr,
-        ctx->f_dev.as<IntegrandDesc>(), opt, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens);
+        ctx->sorted.as<uint8_t>(), bins, ctx->memo.as<double>(), ctx->cfail.as<uint8_t>(), ctx->ich.as<int32_t>(),
+        ctx->list.as<int32_t>(), n_list, base, T, mr, opt, ctx->dcv.as<double>(), ctx->vwv.as<double>(), rec_slot,
+        rec_dens);
 }
 
 // The phased weight pass (pipeline.cuh) over the n_pre PreProcess-accepted
-// points of a chunk of m counters, in tiles of at most kPipeTile points so
-// that the memo buffers stay in L2.
-constexpr long long kPipeTile = 1 << 16;
+// points of a chunk of m counters, in tiles of at most ctx->pipe_tile points
+// so that a tile's buffers stay in L2.
 
 int launch_pipeline(chili_ctx *ctx, long long m, long long n_pre, int bins, bool opt, RoundCtl *ctl_pre,
                     double *rec_val, double *rec_wgt, uint8_t *rec_ok, int32_t *rec_slot, double *rec_dens) {
     const PointProgram &P = ctx->pp_host;
     const PointProgram *pp = ctx->point_prog.as<PointProgram>();
-    const long long T = std::min<long long>(kPipeTile, std::max<long long>(n_pre, 1));
+    const long long T = std::min<long long>(ctx->pipe_tile, std::max<long long>(n_pre, 1));
     CK(ctx->node_soa.ensure(sizeof(double) * 4 * P.n_nodes * T));
     CK(ctx->memo.ensure(sizeof(double) * std::max(1, P.n_memo) * T));
     CK(ctx->cfail.ensure(static_cast<size_t>(std::max(1, P.n_chains)) * T));
+    CK(ctx->dcv.ensure(sizeof(double) * ctx->nch * T));
+    CK(ctx->vwv.ensure(sizeof(double) * ctx->nch * T));
     const long long *n_list = reinterpret_cast<const long long *>(
         reinterpret_cast<const char *>(ctl_pre) + offsetof(RoundCtl, n_acc));
     const unsigned gx = static_cast<unsigned>((T + 255) / 256);
@@ -240,12 +241,16 @@ int launch_pipeline(chili_ctx *ctx, long long m, long long n_pre, int bins, bool
                                                                     ctx->memo.as<double>(), ctx->cfail.as<uint8_t>());
         LAUNCHED();
         switch (P.ndims) {
-#define CHILI_ASM(D) \
-    case D: launch_assemble<D>(ctx, base, T, m, bins, o, n_list, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens); break;
-            CHILI_ASM(1) CHILI_ASM(4) CHILI_ASM(7) CHILI_ASM(10) CHILI_ASM(13) CHILI_ASM(16) CHILI_ASM(19) CHILI_ASM(22)
-#undef CHILI_ASM
+#define CHILI_CH(D) \
+    case D: launch_channel<D>(ctx, base, T, m, bins, o, n_list, rec_slot, rec_dens); break;
+            CHILI_CH(1) CHILI_CH(4) CHILI_CH(7) CHILI_CH(10) CHILI_CH(13) CHILI_CH(16) CHILI_CH(19) CHILI_CH(22)
+#undef CHILI_CH
         default: return fail(ctx, CHILI_ERR_STATE, "no phased weight kernel for this dimension");
         }
+        LAUNCHED();
+        k_pp_combine<<<gx, 256, 0, ctx->stream>>>(pp, alpha_ptr(ctx), ctx->dcv.as<double>(), ctx->vwv.as<double>(),
+                                                   ctx->node_soa.as<double>(), n_list, base, T,
+                                                   ctx->f_dev.as<IntegrandDesc>(), rec_val, rec_wgt, rec_ok);
         LAUNCHED();
     }
     return CHILI_OK;
@@ -308,7 +313,7 @@ int chili_gpu_destroy(chili_ctx *ctx) {
     if (!ctx) return CHILI_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    DevBuf *bufs[] = {&ctx->edges, &ctx->edges_tmp, &ctx->progs, &ctx->point_prog, &ctx->node_soa, &ctx->memo, &ctx->cfail, &ctx->hints, &ctx->sorted, &ctx->alpha_buf, &ctx->f_dev, &ctx->mom_soa,
+    DevBuf *bufs[] = {&ctx->edges, &ctx->edges_tmp, &ctx->progs, &ctx->point_prog, &ctx->node_soa, &ctx->memo, &ctx->cfail, &ctx->dcv, &ctx->vwv, &ctx->hints, &ctx->sorted, &ctx->alpha_buf, &ctx->f_dev, &ctx->mom_soa,
                       &ctx->ich, &ctx->flag, &ctx->list, &ctx->block_count, &ctx->block_off, &ctx->part,
                       &ctx->hist, &ctx->round_res, &ctx->acc, &ctx->ctl, &ctx->status, &ctx->v_part,
                       &ctx->v_hist, &ctx->v_train, &ctx->v_out, &ctx->rec, &ctx->ctl3};
@@ -355,6 +360,11 @@ int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value) {
     }
     if (std::strcmp(name, "pipeline") == 0) {
         ctx->use_pipeline = value != 0;
+        return CHILI_OK;
+    }
+    if (std::strcmp(name, "pipeline_tile") == 0) {
+        if (value < 1024 || value > (1ll << 24)) return fail(ctx, CHILI_ERR_INVALID_ARG, "pipeline_tile outside [1024, 2^24]");
+        ctx->pipe_tile = value;
         return CHILI_OK;
     }
     return fail(ctx, CHILI_ERR_INVALID_ARG, std::string("unknown option ") + name);

@@ -9,14 +9,15 @@
 //                  two-body decay weight (one thread per point and item)
 //   k_pp_chains    every t-channel chain's weight and last uniform (one thread
 //                  per point and chain)
-//   k_pp_assemble  per point, the channel loop: each channel's density is the
-//                  product of its items in the reference's order, its uniforms
-//                  come from the memo slots through the position maps (held in
-//                  registers: DIMS is a compile-time constant), the grid
-//                  weight follows, then the combined weight, the integrand and
-//                  the records of k_mc_weight.
-// Intermediate values live in SoA buffers [slot][point] with stride m, so
-// every access of a warp is coalesced.
+//   k_pp_channel   every channel's density and VEGAS weight (one thread per
+//                  point and channel; the channel's uniforms come from the
+//                  memo slots through its position map and stay in registers:
+//                  DIMS is a compile-time constant)
+//   k_pp_combine   per point, the combined weight in channel order, the
+//                  integrand and the records of k_mc_weight.
+// Intermediate values live in SoA buffers [slot][point] of one tile of points
+// (stride m), so every access of a warp is coalesced and a tile's buffers
+// stay in L2.
 #pragma once
 
 #include "channel_program.h"
@@ -184,66 +185,91 @@ __device__ __forceinline__ double eval_momenta_soa(const IntegrandDesc *__restri
     return (top2 ? big1 * big2 : sum) * tprod;
 }
 
-// Per point: the channel loop, the combined weight, the integrand and the
-// records (rec_* as in k_mc_weight).  running is the value the shared uniform
-// buffer holds at position DIMS-1 (zero before the first channel).
+// One thread per (point, channel = blockIdx.y): channel c's density, the
+// product of its items in the reference's order (Channel.cc:40-61), and its
+// VEGAS weight on the uniforms the position map selects.  When c's chain
+// fails, its last uniform is the one the shared buffer still holds: the last
+// uniform of the latest earlier channel whose chain did not fail (zero if
+// none).  Writes dcv/vwv (tile-local, stride m), the density record and, for
+// the point's own channel, the histogram slots.
 template <int DIMS>
-__global__ void __launch_bounds__(128) k_pp_assemble(
+__global__ void __launch_bounds__(128) k_pp_channel(
     const PointProgram *__restrict__ pp, const double *__restrict__ grids, const uint16_t *__restrict__ hints,
-    const uint8_t *__restrict__ sorted, const double *__restrict__ alpha, int bins,
-    const double *__restrict__ node_soa, const double *__restrict__ memo, const uint8_t *__restrict__ cfail,
+    const uint8_t *__restrict__ sorted, int bins, const double *__restrict__ memo, const uint8_t *__restrict__ cfail,
     const int32_t *__restrict__ ich_arr, const int32_t *__restrict__ list, const long long *__restrict__ n_list,
-    long long base, long long m, long long mr, const IntegrandDesc *__restrict__ f, int should_opt,
-    double *__restrict__ rec_val, double *__restrict__ rec_wgt, uint8_t *__restrict__ rec_ok,
+    long long base, long long m, long long mr, int should_opt, double *__restrict__ dcv, double *__restrict__ vwv,
     int32_t *__restrict__ rec_slot, double *__restrict__ rec_dens) {
-    // i: tile-local point (node/memo/cfail stride m); r: record index (stride mr)
-    const long long i = blockIdx.x * 128ll + threadIdx.x;
-    const long long r = base + i;
+    const long long i = blockIdx.x * 128ll + threadIdx.x;  // tile-local point
+    const long long r = base + i;                          // record index
     if (i >= m || r >= *n_list) return;
-    const int ich = ich_arr[list[r]];
-    const int H = kHintPerBin * bins;
-    const int nch = pp->nch;
-    const double fb = static_cast<double>(bins);
-    const double before = edge_before_table(DIMS, bins);
-    const size_t gsz = static_cast<size_t>(DIMS) * (bins + 1);
-    double running = 0.0, acc = 0.0;
-    for (int c = 0; c < nch; ++c) {
-        const PPChannel &C = pp->ch[c];
-        const bool fail = cfail[C.chain * m + i] != 0;
-        double wdec = 1;
-        for (int k = 0; k < C.n_dec; ++k) {
-            wdec *= memo[static_cast<long long>(pp->memo_dw + 2 * C.dw[k]) * m + i];
-            wdec /= kTwoPi;
-        }
-        const double wt = memo[static_cast<long long>(pp->memo_chain + 2 * C.chain) * m + i];
-        double ws = 1;
-        for (int k = 0; k < C.n_sd; ++k) ws *= memo[static_cast<long long>(pp->memo_sw + 3 * C.sw[k]) * m + i];
-        const double dc = wdec * wt * ws;
-        const int16_t *pos = fail ? pp->pos_src_fail[c] : pp->pos_src[c];
-        double x[DIMS];
+    const int c = blockIdx.y;
+    const PPChannel &C = pp->ch[c];
+    const bool fail = cfail[C.chain * m + i] != 0;
+    double wdec = 1;
+    for (int k = 0; k < C.n_dec; ++k) {
+        wdec *= memo[static_cast<long long>(pp->memo_dw + 2 * C.dw[k]) * m + i];
+        wdec /= kTwoPi;
+    }
+    const double wt = memo[static_cast<long long>(pp->memo_chain + 2 * C.chain) * m + i];
+    double ws = 1;
+    for (int k = 0; k < C.n_sd; ++k) ws *= memo[static_cast<long long>(pp->memo_sw + 3 * C.sw[k]) * m + i];
+    const double dc = wdec * wt * ws;
+    double x[DIMS];
+    if (!fail) {
+        const int16_t *pos = pp->pos_src[c];
 #pragma unroll
-        for (int p = 0; p < DIMS; ++p) {
-            const int s = pos[p];
-            x[p] = s >= 0 ? memo[static_cast<long long>(s) * m + i] : running;
-        }
-        running = x[DIMS - 1];
-        const double *g = grids + c * gsz;
-        const uint16_t *hc = hints + static_cast<size_t>(c) * DIMS * (H + 1);
-        const uint8_t *sc = sorted + c * DIMS;
-        double vw = 1.0;
-        const bool chosen = should_opt && c == ich;
+        for (int p = 0; p < DIMS; ++p) x[p] = memo[static_cast<long long>(pos[p]) * m + i];
+    } else {
+        const int16_t *pos = pp->pos_src_fail[c];
 #pragma unroll
-        for (int p = 0; p < DIMS; ++p) {
-            const int b = find_bin_hinted(g + p * (bins + 1), hc + p * (H + 1), __ldg(sc + p) != 0, bins, H, x[p]);
-            vw = __dmul_rn(vw, __dmul_rn(bin_width(g, bins, p, b, before), fb));
-            if (chosen) {
-                const int s = p * bins + b;
-                rec_slot[p * mr + r] = s >= 0 ? c * DIMS * bins + s : -1;
+        for (int p = 0; p < DIMS - 1; ++p) x[p] = memo[static_cast<long long>(pos[p]) * m + i];
+        double stale = 0.0;
+        for (int q = c - 1; q >= 0; --q) {
+            if (!cfail[pp->ch[q].chain * m + i]) {
+                stale = memo[static_cast<long long>(pp->pos_src[q][DIMS - 1]) * m + i];
+                break;
             }
         }
-        acc += __ldg(alpha + c) / dc / vw;
-        rec_dens[static_cast<long long>(c) * mr + r] = dc;
+        x[DIMS - 1] = stale;
     }
+    const int H = kHintPerBin * bins;
+    const double fb = static_cast<double>(bins);
+    const double before = edge_before_table(DIMS, bins);
+    const double *g = grids + static_cast<size_t>(c) * DIMS * (bins + 1);
+    const uint16_t *hc = hints + static_cast<size_t>(c) * DIMS * (H + 1);
+    const uint8_t *sc = sorted + c * DIMS;
+    const bool chosen = should_opt && c == ich_arr[list[r]];
+    double vw = 1.0;
+#pragma unroll
+    for (int p = 0; p < DIMS; ++p) {
+        const int b = find_bin_hinted(g + p * (bins + 1), hc + p * (H + 1), __ldg(sc + p) != 0, bins, H, x[p]);
+        vw = __dmul_rn(vw, __dmul_rn(bin_width(g, bins, p, b, before), fb));
+        if (chosen) {
+            const int s = p * bins + b;
+            rec_slot[p * mr + r] = s >= 0 ? c * DIMS * bins + s : -1;
+        }
+    }
+    dcv[static_cast<long long>(c) * m + i] = dc;
+    vwv[static_cast<long long>(c) * m + i] = vw;
+    rec_dens[static_cast<long long>(c) * mr + r] = dc;
+}
+
+// Per point: 1 / sum_c alpha_c / dens_c / vw_c in channel order
+// (Integrand.hh:118-122), the integrand and the value records.
+__global__ void __launch_bounds__(256) k_pp_combine(const PointProgram *__restrict__ pp,
+                                                    const double *__restrict__ alpha,
+                                                    const double *__restrict__ dcv, const double *__restrict__ vwv,
+                                                    const double *__restrict__ node_soa,
+                                                    const long long *__restrict__ n_list, long long base, long long m,
+                                                    const IntegrandDesc *__restrict__ f, double *__restrict__ rec_val,
+                                                    double *__restrict__ rec_wgt, uint8_t *__restrict__ rec_ok) {
+    const long long i = blockIdx.x * 256ll + threadIdx.x;
+    const long long r = base + i;
+    if (i >= m || r >= *n_list) return;
+    double acc = 0.0;
+    const int nch = pp->nch;
+    for (int c = 0; c < nch; ++c)
+        acc += __ldg(alpha + c) / dcv[static_cast<long long>(c) * m + i] / vwv[static_cast<long long>(c) * m + i];
     double wgt = 1.0 / acc;
     const double fv = eval_momenta_soa(f, node_soa, m, i, pp->n_ext);
     double val = wgt == 0 ? 0 : fv * wgt;

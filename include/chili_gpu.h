@@ -175,7 +175,10 @@ int chili_gpu_synchronize(chili_ctx *ctx);
 uint64_t chili_gpu_launch_count(const chili_ctx *ctx);
 /* Tuning switches (no counterpart in the reference).  "point_program": 1
  * (default) evaluates the parts that channels share once per point, 0 runs
- * every channel's mapping on its own; both give the same numbers. */
+ * every channel's mapping on its own; both give the same numbers.
+ * "pipeline": 1 (default) runs the all-channel weight pass as a sequence of
+ * small kernels over tiles of points, 0 as one kernel per point.
+ * "pipeline_tile": points per tile of that pass (default 65536). */
 int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value);
 
 /* ------------------------------------------------- grids (AdaptiveMap) */

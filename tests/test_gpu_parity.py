@@ -263,7 +263,7 @@ def test_multichannel_iteration_degenerate_grids(ctx_factory, rng, mc2):
     edges[8, 0, 50] = np.nan                                # NaN edge
     ctx.set_grids(edges)
     R.set_grids(edges)
-    u = uniforms53(rng, (4 * ncalls, R.ndims + 1))
+    u = uniforms53(rng, (12 * ncalls, R.ndims + 1))
     st, info = ctx.multichannel_iterate(params, u=u, guard=True)
     st_r, info_r = R.iterate(u, guard=True)
     assert info.points_tried == info_r.points_tried
