@@ -73,7 +73,7 @@ struct chili_ctx {
     bool have_pp = false;      // the set fits the PointProgram limits
     bool use_pp = true;        // option "point_program"
     bool use_pipeline = true;  // option "pipeline": phased weight pass
-    long long pipe_tile = 1 << 16;  // option "pipeline_tile": points per tile
+    long long pipe_tile = 1 << 20;  // option "pipeline_tile": points per tile
     PointProgram pp_host;      // host copy (sizes of the memo buffers)
     DevBuf node_soa, memo, cfail, dcv, vwv;
     DevBuf hints, sorted;      // hinted bin search tables of the grids
@@ -441,7 +441,9 @@ int chili_gpu_grid_weight(chili_ctx *ctx, int ch, const double *x, double *w, in
     if ((rc = resolve(ctx, w, sizeof(double) * n, 1, false, aw))) return rc;
     if ((rc = resolve(ctx, bin, sizeof(int32_t) * n * D, 2, false, ab))) return rc;
     const double *g = ctx->edges.as<double>() + static_cast<size_t>(ch) * D * (B + 1);
-    k_grid_weight<<<grid_for(n, 128), 128, 0, ctx->stream>>>(g, D, B, static_cast<const double *>(ax.dev),
+    const uint16_t *hg = ctx->hints.as<uint16_t>() + static_cast<size_t>(ch) * D * (kHintPerBin * B + 1);
+    const uint8_t *sg = ctx->sorted.as<uint8_t>() + static_cast<size_t>(ch) * D;
+    k_grid_weight<<<grid_for(n, 128), 128, 0, ctx->stream>>>(g, hg, sg, D, B, static_cast<const double *>(ax.dev),
                                                              static_cast<double *>(aw.dev),
                                                              static_cast<int32_t *>(ab.dev), n);
     LAUNCHED();

@@ -178,7 +178,7 @@ uint64_t chili_gpu_launch_count(const chili_ctx *ctx);
  * every channel's mapping on its own; both give the same numbers.
  * "pipeline": 1 (default) runs the all-channel weight pass as a sequence of
  * small kernels over tiles of points, 0 as one kernel per point.
- * "pipeline_tile": points per tile of that pass (default 65536). */
+ * "pipeline_tile": points per tile of that pass (default 1048576). */
 int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value);
 
 /* ------------------------------------------------- grids (AdaptiveMap) */

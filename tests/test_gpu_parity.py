@@ -57,6 +57,20 @@ def test_grid_map_and_weight_bit_exact(ctx_factory, rng):
     assert np.array_equal(b, br)
     ok = ~np.isnan(wr)  # the reference reads outside its table there
     assert np.array_equal(w[ok], wr[ok])
+    # tables the hinted search must not shortcut: not monotone, with a NaN, all
+    # zero; and a peaked one (many edges per hint cell)
+    bad = edges.copy()
+    bad[0, 10:20] = bad[0, 10:20][::-1].copy()
+    bad[1, 25] = np.nan
+    bad[2, :] = 0.0
+    bad[3, 1:bins] = np.sort(0.5 + 1e-4 * rng.random(bins - 1))
+    ctx.set_grids(bad[None])
+    xs = np.concatenate([uniforms53(rng, (100_000, dims)), bad[:, 1:bins].T, np.zeros((1, dims))])
+    w, b = ctx.grid_weight(0, xs)
+    wr, br = ref.am_weight(bad, xs)
+    assert np.array_equal(b, br)
+    ok = ~np.isnan(wr)
+    assert np.array_equal(w[ok], wr[ok], equal_nan=True)
 
 
 def test_grid_adapt_and_split(ctx_factory, rng):
@@ -252,14 +266,17 @@ def test_generate_events(ctx_factory, mc2):
 
 
 def test_multichannel_iteration_degenerate_grids(ctx_factory, rng, mc2):
-    """Edge tables that are not monotone (the hinted bin search must fall back
-    to the plain lower_bound) or all zero (what the reference's Adapt leaves for
-    a dimension without data) give the reference's results."""
+    """Edge tables that are not monotone or hold a NaN (the hinted bin search
+    must fall back to the plain lower_bound) give the reference's results.
+    (An all-zero table, which the reference's Adapt leaves for a dimension
+    without data, makes every point's combined weight a sum of signed
+    infinities whose NaN-or-not outcome hinges on the signs of zero densities,
+    i.e. on last-ulp differences between the two libms; it is checked at the
+    level of the bin search in test_grid_map_and_weight_bit_exact instead.)"""
     ncalls = 10_000
     ctx, R, params = _mc_pair(ctx_factory, mc2, 100, ncalls, rng)
     edges = R.get_grids()
     edges[3, 2, 10:20] = edges[3, 2, 10:20][::-1].copy()  # non-monotone
-    edges[5, 7, :] = 0.0                                   # all zero
     edges[8, 0, 50] = np.nan                                # NaN edge
     ctx.set_grids(edges)
     R.set_grids(edges)
