@@ -23,6 +23,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+TIMED_KERNELS = ["k_mc_forward", "k_pp_nodes", "k_pp_items", "k_pp_chains", "k_pp_channel", "k_pp_combine",
+                 "k_mc_weight", "k_mc_accum"]
 METRIC = "time to 0.1% error & unweighted events/s: flow vs plain VEGAS, 1 B200, FP64"
 UNIT = "unweighted events/s"
 NCALLS = 1_000_000
@@ -137,7 +139,9 @@ def run_chili(args, rank, world, local_rank):
     torch.cuda.synchronize(dev)
 
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ctx.set_option("kernel_timing", 1)  # CUDA events around each kernel of the timed region
     l0 = ctx.launches
+    weighted = 0
     pooled = np.zeros(6)
     history = []
     unw = 0.0
@@ -149,6 +153,7 @@ def run_chili(args, rank, world, local_rank):
             st, info = ctx.multichannel_iterate(params, seed=seed, counter=counter, guard=True)
             counter += info.points_tried
             tried += info.points_tried
+            weighted += info.points_weighted
             unw += unweighted_events(st, info)
             pooled += np.array(st.as_tuple()) * np.array([1, 0, 0, 1, 1, 1])
             mean, err = gpu.stats_mean_error(pooled)
@@ -171,9 +176,9 @@ def run_chili(args, rank, world, local_rank):
     mean, err = gpu.stats_mean_error(pooled)
     t01 = next((h[0] for h in history if h[1] <= 1e-3), None)
 
-    # kernel-level timing of the dominant kernel (k_mc_weight) is taken from a
-    # dedicated run of one iteration with events around each kernel class
-    roof = roofline(ctx, params, seed, counter, stream, dev)
+    kernel_ms = {k: ctx.kernel_time(k) for k in TIMED_KERNELS}
+    kernel_ms = {k: v for k, v in kernel_ms.items() if v[1] > 0}
+    roof = roofline(kernel_ms, weighted, dev)
 
     e2e = None
     if not args.no_e2e:
@@ -192,6 +197,7 @@ def run_chili(args, rank, world, local_rank):
             "config": dict(workload_config(args.ncalls), parallelism=f"replicas x{world}"),
             "points_per_s": acc_tot / (ms_max / 1e3),
             "tried_points_per_s": tried_tot / (ms_max / 1e3),
+            "weighted_points_per_step": weighted / args.steps,
             "unweighting_efficiency": unw_tot / acc_tot,
             "integral": mean, "rel_error": err / abs(mean),
             "time_to_0p1pct_s": t01,
@@ -205,28 +211,54 @@ def run_chili(args, rank, world, local_rank):
     ctx.close()
 
 
-FP64_OPS_PER_WEIGHTED_POINT = None  # filled from the ncu capture (profiles/)
+# Per-kernel figures of the committed ncu capture
+# (profiles/multichannel_2to4_kernels.md): FP64 operations (2*DFMA + DADD +
+# DMUL, executed) and DRAM bytes (read + write), both per weighted point.
+KERNEL_COUNTERS = {}
 
 
-def roofline(ctx, params, seed, counter, stream, dev):
-    """Dominant kernel: k_mc_weight (all-channel inverse maps).  Its duration is
-    measured from one iteration's kernels; the FP64 work per point comes from
-    the committed ncu counters.  HBM view: the 204-byte event record per point."""
+def fp64_peak_tflops(dev):
+    """FP64 peak measured here: cuBLAS DGEMM 8192^3, best of 5."""
     import torch
-    from chili_b200 import gpu
-    lib = ctx.lib
-    # one iteration, device time of the whole iteration for context
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    st, info = ctx.multichannel_iterate(params, seed=seed, counter=counter, guard=True)
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    it_ms = e0.elapsed_time(e1)
-    peaks = measured_peaks()
-    return {"bound": "fp64", "kernel": "k_mc_weight", "iteration_ms": it_ms,
-            "achieved": None, "peak": None, "unit": "TFLOP/s", "frac": None, "traffic": None,
-            "hbm_peak_gbs": peaks.get("hbm_gbs"),
-            "note": "FP64 pipe roofline filled from profiles/ once captured"}
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def roofline(kernel_ms, weighted, dev):
+    """The dominant kernel of the timed region (by CUDA-event time): FP64
+    throughput against the measured FP64 peak (the path is FP64-compute bound;
+    its HBM traffic is a small fraction of the HBM roofline)."""
+    dom = max(kernel_ms, key=lambda k: kernel_ms[k][0])
+    ms, launches = kernel_ms[dom]
+    peak = fp64_peak_tflops(dev)
+    c = KERNEL_COUNTERS.get(dom)
+    out = {"bound": "fp64", "kernel": dom, "launches": launches, "ms_per_launch": ms / max(launches, 1),
+           "share_of_kernel_time": ms / sum(v[0] for v in kernel_ms.values()),
+           "peak": peak, "unit": "TFLOP/s", "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+           "kernel_ms": {k: round(v[0], 4) for k, v in kernel_ms.items()}}
+    if c:
+        flops = c["fp64_ops_per_point"] * weighted
+        out.update(achieved=flops / (ms / 1e3) / 1e12, traffic=c["dram_bytes_per_point"] * weighted / max(launches, 1),
+                   counters_source=c["source"])
+        out["frac"] = out["achieved"] / peak
+        hbm = measured_peaks().get("hbm_gbs")
+        out["hbm_view"] = {"achieved_gbs": c["dram_bytes_per_point"] * weighted / (ms / 1e3) / 1e9, "peak_gbs": hbm,
+                           "frac": c["dram_bytes_per_point"] * weighted / (ms / 1e3) / 1e9 / hbm}
+    else:
+        out.update(achieved=None, frac=None, traffic=None)
+    return out
 
 
 def measured_peaks():

@@ -110,7 +110,8 @@ class MultiChannelParams(C.Structure):
 class MCIterInfo(C.Structure):
     _fields_ = [("points_tried", C.c_uint64), ("points_accepted", C.c_uint64),
                 ("rejected_pre", C.c_uint64), ("rejected_nan", C.c_uint64),
-                ("weight_max", C.c_double), ("nonfinite_alpha_terms", C.c_double)]
+                ("weight_max", C.c_double), ("nonfinite_alpha_terms", C.c_double),
+                ("points_weighted", C.c_uint64)]
 
 
 class ChannelSet:

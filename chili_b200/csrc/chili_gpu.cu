@@ -94,9 +94,70 @@ struct chili_ctx {
     // staging of host buffers
     DevBuf stage[kStageSlots];
     int max_smem_optin = 0;
+    // option "kernel_timing": CUDA events around the iteration's kernels
+    bool timing = false;
+    struct Pending {
+        int kernel;
+        cudaEvent_t a, b;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> event_pool;
+    double ktime_ms[16] = {0};
+    unsigned long long klaunches[16] = {0};
 };
 
 namespace {
+
+// Kernel classes timed under the "kernel_timing" option.
+const char *const kTimedKernels[] = {"k_mc_forward", "k_pp_nodes", "k_pp_items", "k_pp_chains", "k_pp_channel",
+                                     "k_pp_combine", "k_mc_weight", "k_mc_accum", "k_vegas_iter", nullptr};
+enum { KT_FORWARD, KT_NODES, KT_ITEMS, KT_CHAINS, KT_CHANNEL, KT_COMBINE, KT_WEIGHT, KT_ACCUM, KT_VEGAS };
+
+cudaEvent_t take_event(chili_ctx *ctx) {
+    if (!ctx->event_pool.empty()) {
+        cudaEvent_t e = ctx->event_pool.back();
+        ctx->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Brackets one launch with events when timing is on.
+struct KTimer {
+    chili_ctx *ctx;
+    int kernel;
+    cudaEvent_t a = nullptr;
+    KTimer(chili_ctx *c, int k) : ctx(c), kernel(k) {
+        if (ctx->timing) {
+            a = take_event(ctx);
+            cudaEventRecord(a, ctx->stream);
+        }
+    }
+    ~KTimer() {
+        if (ctx->timing && a) {
+            cudaEvent_t b = take_event(ctx);
+            cudaEventRecord(b, ctx->stream);
+            ctx->pending.push_back({kernel, a, b});
+        }
+    }
+};
+
+// Folds the recorded intervals into the totals (the stream must be idle).
+void collect_times(chili_ctx *ctx) {
+    for (auto &p : ctx->pending) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+            ctx->ktime_ms[p.kernel] += ms;
+            ctx->klaunches[p.kernel] += 1;
+        }
+        ctx->event_pool.push_back(p.a);
+        ctx->event_pool.push_back(p.b);
+    }
+    ctx->pending.clear();
+    cudaGetLastError();
+}
 
 int fail(chili_ctx *ctx, int code, const std::string &msg) {
     if (ctx) ctx->err = msg;
@@ -229,28 +290,32 @@ int launch_pipeline(chili_ctx *ctx, long long m, long long n_pre, int bins, bool
     const int n_items = P.n_tents + P.n_dws + P.n_sws;
     const int o = opt ? 1 : 0;
     for (long long base = 0; base < n_pre; base += T) {
+        { KTimer kt_(ctx, KT_NODES);
         k_pp_nodes<<<gx, 256, 0, ctx->stream>>>(pp, ctx->mom_soa.as<double>(), m, ctx->list.as<int32_t>(), n_list,
-                                                 base, ctx->node_soa.as<double>(), T);
+                                                 base, ctx->node_soa.as<double>(), T); }
         LAUNCHED();
         if (n_items > 0) {
+            KTimer kt_(ctx, KT_ITEMS);
             k_pp_items<<<dim3(gx, n_items), 256, 0, ctx->stream>>>(pp, ctx->node_soa.as<double>(), n_list, base, T,
                                                                     ctx->memo.as<double>());
             LAUNCHED();
         }
+        { KTimer kt_(ctx, KT_CHAINS);
         k_pp_chains<<<dim3(gx, P.n_chains), 256, 0, ctx->stream>>>(pp, ctx->node_soa.as<double>(), n_list, base, T,
-                                                                    ctx->memo.as<double>(), ctx->cfail.as<uint8_t>());
+                                                                    ctx->memo.as<double>(), ctx->cfail.as<uint8_t>()); }
         LAUNCHED();
         switch (P.ndims) {
 #define CHILI_CH(D) \
-    case D: launch_channel<D>(ctx, base, T, m, bins, o, n_list, rec_slot, rec_dens); break;
+    case D: { KTimer kt_(ctx, KT_CHANNEL); launch_channel<D>(ctx, base, T, m, bins, o, n_list, rec_slot, rec_dens); } break;
             CHILI_CH(1) CHILI_CH(4) CHILI_CH(7) CHILI_CH(10) CHILI_CH(13) CHILI_CH(16) CHILI_CH(19) CHILI_CH(22)
 #undef CHILI_CH
         default: return fail(ctx, CHILI_ERR_STATE, "no phased weight kernel for this dimension");
         }
         LAUNCHED();
+        { KTimer kt_(ctx, KT_COMBINE);
         k_pp_combine<<<gx, 256, 0, ctx->stream>>>(pp, alpha_ptr(ctx), ctx->dcv.as<double>(), ctx->vwv.as<double>(),
                                                    ctx->node_soa.as<double>(), n_list, base, T,
-                                                   ctx->f_dev.as<IntegrandDesc>(), rec_val, rec_wgt, rec_ok);
+                                                   ctx->f_dev.as<IntegrandDesc>(), rec_val, rec_wgt, rec_ok); }
         LAUNCHED();
     }
     return CHILI_OK;
@@ -320,6 +385,8 @@ int chili_gpu_destroy(chili_ctx *ctx) {
     for (DevBuf *b : bufs) b->release();
     for (auto &b : ctx->stage) b.release();
     if (ctx->ctl_host) cudaFreeHost(ctx->ctl_host);
+    collect_times(ctx);
+    for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return CHILI_OK;
@@ -347,7 +414,22 @@ int chili_gpu_set_stream(chili_ctx *ctx, void *stream) {
 int chili_gpu_synchronize(chili_ctx *ctx) {
     if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
     CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->timing) collect_times(ctx);
     return CHILI_OK;
+}
+
+int chili_gpu_kernel_time(chili_ctx *ctx, const char *kernel, double *ms, uint64_t *launches) {
+    if (!ctx || !kernel) return fail(ctx, CHILI_ERR_INVALID_ARG, "NULL argument");
+    CK(cudaStreamSynchronize(ctx->stream));
+    collect_times(ctx);
+    for (int k = 0; kTimedKernels[k]; ++k) {
+        if (std::strcmp(kTimedKernels[k], kernel) == 0) {
+            if (ms) *ms = ctx->ktime_ms[k];
+            if (launches) *launches = ctx->klaunches[k];
+            return CHILI_OK;
+        }
+    }
+    return fail(ctx, CHILI_ERR_INVALID_ARG, std::string("not a timed kernel: ") + kernel);
 }
 
 uint64_t chili_gpu_launch_count(const chili_ctx *ctx) { return ctx ? ctx->launches : 0; }
@@ -360,6 +442,14 @@ int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value) {
     }
     if (std::strcmp(name, "pipeline") == 0) {
         ctx->use_pipeline = value != 0;
+        return CHILI_OK;
+    }
+    if (std::strcmp(name, "kernel_timing") == 0) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        collect_times(ctx);
+        ctx->timing = value != 0;
+        for (double &t : ctx->ktime_ms) t = 0;
+        for (auto &n : ctx->klaunches) n = 0;
         return CHILI_OK;
     }
     if (std::strcmp(name, "pipeline_tile") == 0) {
@@ -561,9 +651,12 @@ int chili_gpu_vegas_iterate(chili_ctx *ctx, uint64_t ncalls, uint64_t seed, uint
     CK(ctx->v_train.ensure(hist_bytes));
     CK(ctx->v_out.ensure(sizeof(double) * 6));
     if (!smem) CK(cudaMemsetAsync(ctx->v_hist.p, 0, hist_bytes, ctx->stream));
+    {
+    KTimer kt_(ctx, KT_VEGAS);
     k_vegas_iter<<<static_cast<unsigned>(nblocks), kVegasBlock, smem ? hist_bytes : 0, ctx->stream>>>(
         ctx->edges.as<double>(), D, B, seed, counter_base, static_cast<const double *>(au.dev), n,
         ctx->f_dev.as<IntegrandDesc>(), ctx->v_part.as<double>(), ctx->v_hist.as<double>(), smem ? 1 : 0);
+    }
     LAUNCHED();
     double *train = smem ? ctx->v_train.as<double>() : ctx->v_hist.as<double>();
     k_vegas_finalize<<<1, 256, 0, ctx->stream>>>(ctx->v_part.as<double>(), static_cast<int>(nblocks),
@@ -790,7 +883,7 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
     }
     const size_t acc_smem = sizeof(double) * (kWgtBlock / 32) * nch;
 
-    long long needed = ncalls, tried = 0;
+    long long needed = ncalls, tried = 0, weighted = 0;
     unsigned long long rounds = 0;
     while (needed > 0) {
         // chunk: enough counters for `needed` accepted, non-NaN points at the
@@ -827,10 +920,13 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         double *rec_dens = rec_wgt + m;
         int32_t *rec_slot = reinterpret_cast<int32_t *>(rec_dens + static_cast<size_t>(nch) * m);
         uint8_t *rec_ok = reinterpret_cast<uint8_t *>(rec_slot + static_cast<size_t>(D) * m);
+        {
+        KTimer kt_(ctx, KT_FORWARD);
         k_mc_forward<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(
             ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), cp_ptr(ctx), nch, D, B, seed,
             counter_base + tried, ud ? ud + tried * (D + 1) : nullptr, m, ctx->f_dev.as<IntegrandDesc>(), NE,
             ctx->mom_soa.as<double>(), ctx->ich.as<int32_t>(), ctx->flag.as<uint8_t>(), ctx->block_count.as<int32_t>());
+        }
         LAUNCHED();
         // offsets of every PreProcess-accepted point (no cut at this stage)
         k_mc_scan<<<1, 1024, 0, ctx->stream>>>(ctx->block_count.as<int32_t>(), static_cast<int>(nb_f),
@@ -844,9 +940,11 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
             CK(cudaMemcpyAsync(ctx->ctl_host, ctl_pre, sizeof(RoundCtl), cudaMemcpyDeviceToHost, ctx->stream));
             CK(cudaStreamSynchronize(ctx->stream));
             const long long n_pre = ctx->ctl_host->n_acc;
+            weighted += n_pre;
             int rc2 = launch_pipeline(ctx, m, n_pre, B, opt, ctl_pre, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens);
             if (rc2) return rc2;
         } else {
+            KTimer kt_(ctx, KT_WEIGHT);
             k_mc_weight<<<static_cast<unsigned>(nb_w), kWgtBlock, 0, ctx->stream>>>(
                 ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), alpha_ptr(ctx), nch, D, B, NE,
                 ctx->mom_soa.as<double>(), m, ctx->ich.as<int32_t>(), ctx->list.as<int32_t>(), ctl_pre,
@@ -864,9 +962,12 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         k_cut_finalize<<<1, 1, 0, ctx->stream>>>(ctl_list, ctl_pre, ctx->list.as<int32_t>(), m, needed,
                                                  ctx->ctl.as<RoundCtl>());
         LAUNCHED();
+        {
+        KTimer kt_(ctx, KT_ACCUM);
         k_mc_accum<<<static_cast<unsigned>(nb_w), kWgtBlock, acc_smem, ctx->stream>>>(
             ctx->ctl.as<RoundCtl>(), m, nch, D, static_cast<int>(hist_n), rec_val, rec_wgt, rec_ok, rec_slot, rec_dens, opt ? 1 : 0,
             guard_alpha ? 1 : 0, ctx->hist.as<double>(), ctx->part.as<double>());
+        }
         LAUNCHED();
         k_mc_reduce<<<kPartFixed + nch, 256, 0, ctx->stream>>>(ctx->part.as<double>(), nch, ctx->ctl.as<RoundCtl>(),
                                                                ctx->round_res.as<double>());
@@ -876,6 +977,7 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         LAUNCHED();
         CK(cudaMemcpyAsync(ctx->ctl_host, ctx->ctl.p, sizeof(RoundCtl), cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
+        if (ctx->timing) collect_times(ctx);
         const RoundCtl r = *ctx->ctl_host;
         if (r.cut <= 0 || r.cut > m || r.n_acc < 0 || r.nan_round < 0 || r.nan_round > r.n_acc)
             return fail(ctx, CHILI_ERR_CUDA, "inconsistent round record");
@@ -903,6 +1005,7 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         info->rejected_nan = static_cast<uint64_t>(acc_h.nan_count);
         info->weight_max = acc_h.wmax;
         info->nonfinite_alpha_terms = acc_h.nonfinite;
+        info->points_weighted = static_cast<uint64_t>(weighted);
     }
     return CHILI_OK;
 }

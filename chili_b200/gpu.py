@@ -35,6 +35,7 @@ def _declare(lib):
         "chili_gpu_synchronize": ([vp], i32),
         "chili_gpu_launch_count": ([vp], u64),
         "chili_gpu_set_option": ([vp, C.c_char_p, i64], i32),
+        "chili_gpu_kernel_time": ([vp, C.c_char_p, P(dbl), P(u64)], i32),
         "chili_gpu_set_grids": ([vp, vp, i32, i32, i32], i32),
         "chili_gpu_get_grids": ([vp, vp, i32, i32, i32], i32),
         "chili_gpu_grid_map": ([vp, i32, vp, vp, vp, i64], i32),
@@ -143,6 +144,11 @@ class Context:
 
     def set_option(self, name, value):
         self.call("chili_gpu_set_option", name.encode(), int(value))
+
+    def kernel_time(self, name):
+        ms, n = C.c_double(), C.c_uint64()
+        self.call("chili_gpu_kernel_time", name.encode(), C.byref(ms), C.byref(n))
+        return ms.value, n.value
 
     @property
     def launches(self):

@@ -135,6 +135,9 @@ typedef struct {
     uint64_t rejected_nan;    /* NaN-value retries (MultiChannel.hh:230-236)*/
     double weight_max;        /* max combined weight f*w over the iteration */
     double nonfinite_alpha_terms; /* non-finite alpha-training contributions */
+    uint64_t points_weighted; /* points whose combined weight was computed
+                                 (PreProcess-accepted points of the chunks,
+                                 including those beyond the cut)           */
 } chili_mc_iter_info;
 
 /* ------------------------------------------------------------ integrands */
@@ -178,8 +181,16 @@ uint64_t chili_gpu_launch_count(const chili_ctx *ctx);
  * every channel's mapping on its own; both give the same numbers.
  * "pipeline": 1 (default) runs the all-channel weight pass as a sequence of
  * small kernels over tiles of points, 0 as one kernel per point.
- * "pipeline_tile": points per tile of that pass (default 1048576). */
+ * "pipeline_tile": points per tile of that pass (default 1048576).
+ * "kernel_timing": 1 brackets the iteration's kernels with CUDA events on the
+ * context's stream (totals read by chili_gpu_kernel_time; setting the option
+ * resets them), 0 (default) records nothing. */
 int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value);
+/* Total device time (ms) and launch count of one kernel class under the
+ * "kernel_timing" option: k_mc_forward, k_pp_nodes, k_pp_items, k_pp_chains,
+ * k_pp_channel, k_pp_combine, k_mc_weight, k_mc_accum, k_vegas_iter.  No
+ * counterpart in the reference. */
+int chili_gpu_kernel_time(chili_ctx *ctx, const char *kernel, double *ms, uint64_t *launches);
 
 /* ------------------------------------------------- grids (AdaptiveMap) */
 /* nch grids of dims x (bins+1) edges, each in the reference AdaptiveMap

@@ -796,6 +796,7 @@ int orc_mc_iterate(void *p, const double *u, int64_t n_u, int guard, chili_stats
     }
     info->points_tried = (uint64_t)k;
     info->points_accepted = ncalls;
+    info->points_weighted = ncalls + info->rejected_nan;
     memcpy(m->atrain, train, sizeof(double) * nch);
     if (m->prm.should_optimize) {
         double nw[CHILI_MAX_CHANNELS], sw = 0, ns = 0;

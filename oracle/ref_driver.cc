@@ -525,6 +525,7 @@ int ref_mc_iterate(void *p, const double *u, int64_t n_u, int guard, chili_stats
     }
     info->points_tried = static_cast<uint64_t>(k);
     info->points_accepted = ncalls;
+    info->points_weighted = ncalls + info->rejected_nan;
     h->last_hist.assign(nch * ndims * h->bins, 0.0);
     for (size_t c = 0; c < nch; ++c) {
         const auto &td = func.GetChannel(c).train_data;

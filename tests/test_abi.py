@@ -51,7 +51,7 @@ int main(void) {
   S(chili_particle_info) S(chili_decay) S(chili_channel_desc) S(chili_idx_value)
   S(chili_pid_pair_value) S(chili_cuts) S(chili_stats) S(chili_multichannel_params) S(chili_mc_iter_info)
   O(chili_multichannel_params, should_optimize) O(chili_multichannel_params, grid_alpha)
-  O(chili_cuts, etamax) O(chili_mc_iter_info, weight_max)
+  O(chili_cuts, etamax) O(chili_mc_iter_info, weight_max) O(chili_mc_iter_info, points_weighted)
   return 0;
 }''')
     exe = tmp_path / "layout"
@@ -67,6 +67,7 @@ int main(void) {
     assert int(got["chili_multichannel_params.grid_alpha"]) == abi.MultiChannelParams.grid_alpha.offset
     assert int(got["chili_cuts.etamax"]) == abi.Cuts.etamax.offset
     assert int(got["chili_mc_iter_info.weight_max"]) == abi.MCIterInfo.weight_max.offset
+    assert int(got["chili_mc_iter_info.points_weighted"]) == abi.MCIterInfo.points_weighted.offset
 
 
 def test_header_limits_match_the_mirror():
