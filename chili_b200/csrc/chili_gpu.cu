@@ -263,7 +263,7 @@ bool pipeline_dims_ok(int d) {
 template <int D>
 void launch_channel(chili_ctx *ctx, long long base, long long T, long long mr, int bins, int opt,
                     const long long *n_list, int32_t *rec_slot, double *rec_dens) {
-    k_pp_channel<D><<<dim3(static_cast<unsigned>((T + 127) / 128), ctx->nch), 128, 0, ctx->stream>>>(
+    k_pp_channel<D><<<dim3(ctx->nch, static_cast<unsigned>((T + 127) / 128)), 128, 0, ctx->stream>>>(
         ctx->point_prog.as<PointProgram>(), ctx->edges.as<double>(), ctx->hints.as<uint16_t>(),
         ctx->sorted.as<uint8_t>(), bins, ctx->memo.as<double>(), ctx->cfail.as<uint8_t>(), ctx->ich.as<int32_t>(),
         ctx->list.as<int32_t>(), n_list, base, T, mr, opt, ctx->dcv.as<double>(), ctx->vwv.as<double>(), rec_slot,
@@ -278,7 +278,9 @@ int launch_pipeline(chili_ctx *ctx, long long m, long long n_pre, int bins, bool
                     double *rec_val, double *rec_wgt, uint8_t *rec_ok, int32_t *rec_slot, double *rec_dens) {
     const PointProgram &P = ctx->pp_host;
     const PointProgram *pp = ctx->point_prog.as<PointProgram>();
-    const long long T = std::min<long long>(ctx->pipe_tile, std::max<long long>(n_pre, 1));
+    // gridDim.y (point blocks of 128) stays below 65536
+    const long long T = std::min<long long>(std::min<long long>(ctx->pipe_tile, 65535ll * 128),
+                                            std::max<long long>(n_pre, 1));
     CK(ctx->node_soa.ensure(sizeof(double) * 4 * P.n_nodes * T));
     CK(ctx->memo.ensure(sizeof(double) * std::max(1, P.n_memo) * T));
     CK(ctx->cfail.ensure(static_cast<size_t>(std::max(1, P.n_chains)) * T));
@@ -296,12 +298,12 @@ int launch_pipeline(chili_ctx *ctx, long long m, long long n_pre, int bins, bool
         LAUNCHED();
         if (n_items > 0) {
             KTimer kt_(ctx, KT_ITEMS);
-            k_pp_items<<<dim3(gx, n_items), 256, 0, ctx->stream>>>(pp, ctx->node_soa.as<double>(), n_list, base, T,
+            k_pp_items<<<dim3(n_items, gx), 256, 0, ctx->stream>>>(pp, ctx->node_soa.as<double>(), n_list, base, T,
                                                                     ctx->memo.as<double>());
             LAUNCHED();
         }
         { KTimer kt_(ctx, KT_CHAINS);
-        k_pp_chains<<<dim3(gx, P.n_chains), 256, 0, ctx->stream>>>(pp, ctx->node_soa.as<double>(), n_list, base, T,
+        k_pp_chains<<<dim3(P.n_chains, gx), 256, 0, ctx->stream>>>(pp, ctx->node_soa.as<double>(), n_list, base, T,
                                                                     ctx->memo.as<double>(), ctx->cfail.as<uint8_t>()); }
         LAUNCHED();
         switch (P.ndims) {

@@ -61,9 +61,9 @@ __global__ void __launch_bounds__(256) k_pp_items(const PointProgram *__restrict
                                                   const double *__restrict__ node_soa,
                                                   const long long *__restrict__ n_list, long long base, long long m,
                                                   double *__restrict__ memo) {
-    const long long i = blockIdx.x * 256ll + threadIdx.x;  // tile-local point
+    const long long i = blockIdx.y * 256ll + threadIdx.x;  // tile-local point
     if (i >= m || base + i >= *n_list) return;
-    int item = blockIdx.y;
+    int item = blockIdx.x;  // consecutive blocks: items of the same points (L2 reuse)
     const double sqrts = pp->sqrts, ptmax = pp->ptmax;
     if (item < pp->n_tents) {
         const int t = item;
@@ -118,9 +118,9 @@ __global__ void __launch_bounds__(256) k_pp_chains(const PointProgram *__restric
                                                    const double *__restrict__ node_soa,
                                                    const long long *__restrict__ n_list, long long base, long long m,
                                                    double *__restrict__ memo, uint8_t *__restrict__ cfail) {
-    const long long i = blockIdx.x * 256ll + threadIdx.x;  // tile-local point
+    const long long i = blockIdx.y * 256ll + threadIdx.x;  // tile-local point
     if (i >= m || base + i >= *n_list) return;
-    const int c = blockIdx.y;
+    const int c = blockIdx.x;  // consecutive blocks: chains of the same points
     const double sqrts = pp->sqrts;
     double wt = kTwoPi;
     V4 psum{0., 0., 0., 0.};
@@ -185,7 +185,7 @@ __device__ __forceinline__ double eval_momenta_soa(const IntegrandDesc *__restri
     return (top2 ? big1 * big2 : sum) * tprod;
 }
 
-// One thread per (point, channel = blockIdx.y): channel c's density, the
+// One thread per (point, channel = blockIdx.x): channel c's density, the
 // product of its items in the reference's order (Channel.cc:40-61), and its
 // VEGAS weight on the uniforms the position map selects.  When c's chain
 // fails, its last uniform is the one the shared buffer still holds: the last
@@ -199,10 +199,10 @@ __global__ void __launch_bounds__(128) k_pp_channel(
     const int32_t *__restrict__ ich_arr, const int32_t *__restrict__ list, const long long *__restrict__ n_list,
     long long base, long long m, long long mr, int should_opt, double *__restrict__ dcv, double *__restrict__ vwv,
     int32_t *__restrict__ rec_slot, double *__restrict__ rec_dens) {
-    const long long i = blockIdx.x * 128ll + threadIdx.x;  // tile-local point
+    const long long i = blockIdx.y * 128ll + threadIdx.x;  // tile-local point
     const long long r = base + i;                          // record index
     if (i >= m || r >= *n_list) return;
-    const int c = blockIdx.y;
+    const int c = blockIdx.x;  // consecutive blocks: channels of the same points
     const PPChannel &C = pp->ch[c];
     const bool fail = cfail[C.chain * m + i] != 0;
     double wdec = 1;
