@@ -214,7 +214,43 @@ def run_chili(args, rank, world, local_rank):
 # Per-kernel figures of the committed ncu capture
 # (profiles/multichannel_2to4_kernels.md): FP64 operations (2*DFMA + DADD +
 # DMUL, executed) and DRAM bytes (read + write), both per weighted point.
-KERNEL_COUNTERS = {}
+KERNEL_COUNTERS = {
+    "k_mc_forward": {
+        "fp64_ops_per_point": 2081.0,
+        "dram_bytes_per_point": 681.2,
+        "source": "profiles/multichannel_2to4_kernels.md"
+    },
+    "k_pp_nodes": {
+        "fp64_ops_per_point": 24.0,
+        "dram_bytes_per_point": 473.9,
+        "source": "profiles/multichannel_2to4_kernels.md"
+    },
+    "k_pp_items": {
+        "fp64_ops_per_point": 11321.2,
+        "dram_bytes_per_point": 1459.6,
+        "source": "profiles/multichannel_2to4_kernels.md"
+    },
+    "k_pp_chains": {
+        "fp64_ops_per_point": 3709.5,
+        "dram_bytes_per_point": 718.1,
+        "source": "profiles/multichannel_2to4_kernels.md"
+    },
+    "k_pp_channel": {
+        "fp64_ops_per_point": 833.8,
+        "dram_bytes_per_point": 1673.1,
+        "source": "profiles/multichannel_2to4_kernels.md"
+    },
+    "k_pp_combine": {
+        "fp64_ops_per_point": 730.5,
+        "dram_bytes_per_point": 411.6,
+        "source": "profiles/multichannel_2to4_kernels.md"
+    },
+    "k_mc_accum": {
+        "fp64_ops_per_point": 336.0,
+        "dram_bytes_per_point": 117.3,
+        "source": "profiles/multichannel_2to4_kernels.md"
+    }
+}
 
 
 def fp64_peak_tflops(dev):
