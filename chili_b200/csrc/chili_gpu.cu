@@ -12,6 +12,7 @@
 #include <cstddef>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1071,3 +1072,88 @@ int chili_gpu_evaluate_batch(chili_ctx *ctx, int ch, const double *u, double *ou
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------ no allocation
+// chili_gpu_vegas_iterate_noalloc: the plain-VEGAS accumulation kernel with its
+// scratch (the integrand descriptor and one StatsData partial per block) in a
+// file-scope device array instead of memory from cudaMalloc.  Every GPU that
+// loads the library holds the array until the process exits.
+constexpr int kNoAllocMaxBlocks = 1184;  // partials for at most 1184 blocks
+constexpr size_t kNoAllocDescDoubles = (sizeof(IntegrandDesc) + sizeof(double) - 1) / sizeof(double);
+constexpr size_t kNoAllocScratchDoubles = kNoAllocDescDoubles + 6 * kNoAllocMaxBlocks;
+static __device__ __align__(256) double chili_noalloc_scratch[kNoAllocScratchDoubles];
+
+namespace {
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double *g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
+
+// Device address of the scratch array on the current device, looked up once
+// per device (with that device current) and cached.
+cudaError_t noalloc_scratch(int dev, double **out) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        double *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void **>(&p), chili_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return cudaSuccess;
+}
+
+bool on_device(const void *p, int dev) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) && a.device == dev;
+}
+}  // namespace
+
+extern "C" int chili_gpu_vegas_iterate_noalloc(void *stream, const double *edges, int dims, int bins,
+                                               const double *camel_params, int nparams, uint64_t ncalls,
+                                               uint64_t seed, uint64_t counter_base, double *stats_out,
+                                               double *train_out) {
+    chili_ctx *ctx = nullptr;  // for the error macros: errors go to the library's last error
+    if (!edges || !camel_params || !stats_out || !train_out)
+        return fail(ctx, CHILI_ERR_INVALID_ARG, "NULL argument");
+    if (dims < 1 || dims > CHILI_MAX_DIMS || bins < 2 || bins > CHILI_MAX_BINS)
+        return fail(ctx, CHILI_ERR_LIMIT, "dims must lie in [1, CHILI_MAX_DIMS] and bins in [2, CHILI_MAX_BINS]");
+    if (nparams < 2 + 2 * dims || nparams > CHILI_MAX_INTEGRAND_PARAMS)
+        return fail(ctx, CHILI_ERR_LIMIT, "camel needs 2 + 2*dims parameters, at most CHILI_MAX_INTEGRAND_PARAMS");
+    if (ncalls < 2 || ncalls > (1ull << 40)) return fail(ctx, CHILI_ERR_LIMIT, "ncalls must lie in [2, 2^40]");
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(ctx, CHILI_ERR_LIMIT, "device index beyond 63");
+    if (!on_device(edges, dev) || !on_device(stats_out, dev) || !on_device(train_out, dev))
+        return fail(ctx, CHILI_ERR_INVALID_ARG, "edges, stats_out and train_out must be device memory of the current device");
+    double *scratch = nullptr;
+    CK(noalloc_scratch(dev, &scratch));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    IntegrandDesc desc{};
+    desc.kind = CHILI_FUNC_CAMEL;
+    desc.nparams = nparams;
+    desc.pre = CHILI_PRE_ACCEPT_ALL;
+    for (int i = 0; i < nparams; ++i) desc.p[i] = camel_params[i];
+    IntegrandDesc *desc_dev = reinterpret_cast<IntegrandDesc *>(scratch);
+    double *part = scratch + kNoAllocDescDoubles;
+    // the descriptor comes from pageable host memory: the copy has left it
+    // when cudaMemcpyAsync returns
+    CK(cudaMemcpyAsync(desc_dev, &desc, sizeof(IntegrandDesc), cudaMemcpyHostToDevice, st));
+    const int nh = dims * bins;
+    CK(cudaMemsetAsync(train_out, 0, sizeof(double) * nh, st));  // the histogram starts at zero
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long n = static_cast<long long>(ncalls);
+    const long long nblocks = std::min<long long>(std::min<long long>(grid_for(n, kVegasBlock), sms * 4ll),
+                                                  kNoAllocMaxBlocks);
+    k_vegas_iter<<<static_cast<unsigned>(nblocks), kVegasBlock, 0, st>>>(edges, dims, bins, seed, counter_base,
+                                                                          nullptr, n, desc_dev, part, train_out, 0);
+    CK(cudaGetLastError());
+    k_vegas_finalize<<<1, 256, 0, st>>>(part, static_cast<int>(nblocks), nullptr, 0, nh, train_out, stats_out);
+    CK(cudaGetLastError());
+    return CHILI_OK;
+}
+

@@ -45,6 +45,7 @@ def _declare(lib):
         "chili_gpu_set_integrand": ([vp, i32, vp, i32], i32),
         "chili_gpu_set_preprocess": ([vp, i32], i32),
         "chili_gpu_vegas_iterate": ([vp, u64, u64, u64, vp, dbl, i32, vp, vp], i32),
+        "chili_gpu_vegas_iterate_noalloc": ([vp, vp, i32, i32, vp, i32, u64, u64, u64, vp, vp], i32),
         "chili_gpu_set_channels": ([vp, P(abi.ChannelDesc), i32, P(abi.Cuts), dbl, i32], i32),
         "chili_gpu_ndims": ([vp], i32),
         "chili_gpu_check_channels": ([P(abi.ChannelDesc), i32, P(abi.Cuts), dbl, i32, C.c_char_p,

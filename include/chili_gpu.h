@@ -230,6 +230,30 @@ int chili_gpu_vegas_iterate(chili_ctx *ctx, uint64_t ncalls, uint64_t seed,
                             double alpha, int adapt, chili_stats *stats_out,
                             double *train_out);
 
+/* Plain VEGAS without any device allocation.  This entry point has no
+ * counterpart in the reference.  It is for callers that cannot call
+ * cudaMalloc: code running inside another framework whose device memory that
+ * framework's allocator owns, or processes whose device-memory budget is fixed
+ * before they start.  It creates no context: the caller passes the grid
+ * (edges[dims*(bins+1)], the AdaptiveMap layout), the camel parameters (host
+ * array {s, N, a[dims], b[dims]}) and the outputs, all on the current device.
+ * The work of one Vegas::operator() without the adaptation runs on `stream`
+ * (NULL: the legacy default stream): stats_out[6] receives the iteration's
+ * StatsData and train_out[dims*bins] its f^2 J^2 histogram, the same numbers
+ * as chili_gpu_vegas_iterate (histogram sums up to the order of addition).
+ * Its scratch -- the integrand descriptor and the per-block partial sums, at
+ * most 1184 blocks -- lives in one fixed array of about 57 KB that the library
+ * declares in device memory, so every GPU that loads the library holds it until
+ * the process exits.  The first call on a device looks up that array's address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.  All
+ * calls share the array: calls whose work overlaps on the GPU race and must be
+ * ordered by the caller (one stream, or events).  Limits: dims <= CHILI_MAX_DIMS,
+ * 2 <= bins <= CHILI_MAX_BINS, 2 + 2*dims <= nparams <= CHILI_MAX_INTEGRAND_PARAMS,
+ * 2 <= ncalls <= 2^40; larger sizes return CHILI_ERR_LIMIT. */
+int chili_gpu_vegas_iterate_noalloc(void *stream, const double *edges, int dims, int bins,
+                                    const double *camel_params, int nparams, uint64_t ncalls, uint64_t seed,
+                                    uint64_t counter_base, double *stats_out, double *train_out);
+
 /* ------------------------------------------------ channels (FSMapper) */
 /* Build the device programs of nch FSMapper channels (Channel.hh:18-30) over
  * n_ext external legs at collider energy sqrts. */
