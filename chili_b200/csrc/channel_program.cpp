@@ -254,6 +254,12 @@ bool build_point_program(const std::vector<ChannelProgram> &progs, PointProgram 
                 pp.dw_smin2[id] = P.dec_smin2[k];
                 pp.dw_cut[id] = P.dec_cut_smin[k];
                 pp.dw_smax[id] = P.dec_smax[k];
+                // smin when smin1 < max(smin2, cut): evaluated with std::max
+                // semantics in the same order as the device (Channel.cc:151)
+                {
+                    const double a = (0.0 < P.dec_smin2[k]) ? P.dec_smin2[k] : 0.0;
+                    pp.dw_smin_c[id] = (a < P.dec_cut_smin[k]) ? P.dec_cut_smin[k] : a;
+                }
                 dw_of[key] = id;
             } else {
                 id = it->second;

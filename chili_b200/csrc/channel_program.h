@@ -77,6 +77,12 @@ struct PointProgram {
     int8_t chain_tent[PP_MAX_CHAINS][CHILI_MAX_EXT];
     int8_t dw_node[PP_MAX_DWS], dw_c1[PP_MAX_DWS], dw_c2[PP_MAX_DWS], dw_massless[PP_MAX_DWS];
     double dw_mass[PP_MAX_DWS], dw_width[PP_MAX_DWS], dw_smin2[PP_MAX_DWS], dw_cut[PP_MAX_DWS], dw_smax[PP_MAX_DWS];
+    // Terms of the propagator weights that depend only on (smin, smax), for
+    // smin = dw_smin_c (the value smin takes whenever the decay products'
+    // masses are below the cut; filled on the device by k_pp_prepare):
+    // massless: pow(smin, 0.01), pow(smax, 0.01); massive: atan((smin-m2)/mw),
+    // atan((smax-m2)/mw).
+    double dw_smin_c[PP_MAX_DWS], dw_t1[PP_MAX_DWS], dw_t2[PP_MAX_DWS];
     int8_t sw_a[PP_MAX_SWS], sw_b[PP_MAX_SWS];
     PPChannel ch[CHILI_MAX_CHANNELS];
     // Phased evaluation: every item's outputs live in a memo buffer of

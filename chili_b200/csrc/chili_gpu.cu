@@ -74,7 +74,7 @@ struct chili_ctx {
     bool have_pp = false;      // the set fits the PointProgram limits
     bool use_pp = true;        // option "point_program"
     bool use_pipeline = true;  // option "pipeline": phased weight pass
-    long long pipe_tile = 1 << 20;  // option "pipeline_tile": points per tile
+    long long pipe_tile = 1 << 22;  // option "pipeline_tile": points per tile
     PointProgram pp_host;      // host copy (sizes of the memo buffers)
     DevBuf node_soa, memo, cfail, dcv, vwv;
     DevBuf hints, sorted;      // hinted bin search tables of the grids
@@ -700,6 +700,8 @@ int chili_gpu_set_channels(chili_ctx *ctx, const chili_channel_desc *descs, int 
             CK(ctx->point_prog.ensure(sizeof(PointProgram)));
             CK(cudaMemcpyAsync(ctx->point_prog.p, pp.data(), sizeof(PointProgram), cudaMemcpyHostToDevice,
                                ctx->stream));
+            k_pp_prepare<<<1, PP_MAX_DWS, 0, ctx->stream>>>(ctx->point_prog.as<PointProgram>());
+            LAUNCHED();
             CK(cudaStreamSynchronize(ctx->stream));
         }
     }

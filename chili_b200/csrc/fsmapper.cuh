@@ -45,6 +45,29 @@ __device__ __forceinline__ double massless_prop_weight(double cn, double cxm, do
     return w / pow(s, -cn);
 }
 
+// The same weights with the (smin, smax)-only terms supplied: t1, t2 are
+// pow(cxm, ce), pow(cxp, ce) (massless) or atan((smin-m2)/mw),
+// atan((smax-m2)/mw) (massive), evaluated by the same functions, so the
+// results are identical to the functions above.
+__device__ __forceinline__ double massless_prop_weight_c(double cn, double t_min, double t_max, double s,
+                                                         double &ran) {
+    const double ce = 1. - cn;
+    const double amin = t_min;
+    double w = t_max - amin;
+    ran = (pow(s, ce) - amin) / w;
+    w /= ce;
+    return w / pow(s, -cn);
+}
+__device__ __forceinline__ double massive_prop_weight_c(double m, double g, double ymax, double ymin, double s,
+                                                        double &ran) {
+    const double m2 = m * m, mw = m * g;
+    const double y = atan((s - m2) / mw);
+    ran = (y - ymin) / (ymax - ymin);
+    double w = mw / ((s - m2) * (s - m2) + mw * mw);
+    w = (ymin - ymax) / w;
+    return w;
+}
+
 // Breit-Wigner propagator (ChannelElements.cc:64-85).
 __device__ __forceinline__ double massive_prop_momenta(double m, double g, double smin, double smax,
                                                        double ran) {

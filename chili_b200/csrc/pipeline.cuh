@@ -90,10 +90,15 @@ __global__ void __launch_bounds__(256) k_pp_items(const PointProgram *__restrict
         const double r = sqrt(fabs(mass2(a))) + sqrt(fabs(mass2(b)));
         const double smin = std_max(std_max(r * r, pp->dw_smin2[k]), pp->dw_cut[k]);
         const double s = mass2(load_v4(node_soa, pp->dw_node[k], m, i));
-        double u;
-        const double w = pp->dw_massless[k] ? massless_prop_weight(0.99, smin, pp->dw_smax[k], s, u)
-                                            : massive_prop_weight(pp->dw_mass[k], pp->dw_width[k], smin,
-                                                                  pp->dw_smax[k], s, u);
+        double u, w;
+        if (smin == pp->dw_smin_c[k]) {  // the usual case: smin-only terms precomputed
+            w = pp->dw_massless[k] ? massless_prop_weight_c(0.99, pp->dw_t1[k], pp->dw_t2[k], s, u)
+                                   : massive_prop_weight_c(pp->dw_mass[k], pp->dw_width[k], pp->dw_t1[k],
+                                                           pp->dw_t2[k], s, u);
+        } else {
+            w = pp->dw_massless[k] ? massless_prop_weight(0.99, smin, pp->dw_smax[k], s, u)
+                                   : massive_prop_weight(pp->dw_mass[k], pp->dw_width[k], smin, pp->dw_smax[k], s, u);
+        }
         double *o = memo + static_cast<long long>(pp->memo_dw + 2 * k) * m + i;
         o[0] = w;
         o[m] = u;
@@ -109,6 +114,24 @@ __global__ void __launch_bounds__(256) k_pp_items(const PointProgram *__restrict
         o[0] = w;
         o[m] = r1;
         o[2 * m] = r2;
+    }
+}
+
+// Fills the (smin, smax)-only propagator terms of the point program with the
+// device's own pow/atan, so that the shortcut in k_pp_items reproduces the
+// full evaluation bit for bit.
+__global__ void k_pp_prepare(PointProgram *__restrict__ pp) {
+    const int k = threadIdx.x + blockIdx.x * blockDim.x;
+    if (k >= pp->n_dws) return;
+    const double smin = pp->dw_smin_c[k], smax = pp->dw_smax[k];
+    if (pp->dw_massless[k]) {
+        const double ce = 1. - 0.99;
+        pp->dw_t1[k] = pow(smin, ce);
+        pp->dw_t2[k] = pow(smax, ce);
+    } else {
+        const double m2 = pp->dw_mass[k] * pp->dw_mass[k], mw = pp->dw_mass[k] * pp->dw_width[k];
+        pp->dw_t1[k] = atan((smin - m2) / mw);  // "ymax" of ChannelElements.cc:94
+        pp->dw_t2[k] = atan((smax - m2) / mw);  // "ymin"
     }
 }
 

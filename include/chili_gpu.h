@@ -181,7 +181,7 @@ uint64_t chili_gpu_launch_count(const chili_ctx *ctx);
  * every channel's mapping on its own; both give the same numbers.
  * "pipeline": 1 (default) runs the all-channel weight pass as a sequence of
  * small kernels over tiles of points, 0 as one kernel per point.
- * "pipeline_tile": points per tile of that pass (default 1048576).
+ * "pipeline_tile": points per tile of that pass (default 4194304).
  * "kernel_timing": 1 brackets the iteration's kernels with CUDA events on the
  * context's stream (totals read by chili_gpu_kernel_time; setting the option
  * resets them), 0 (default) records nothing. */
