@@ -77,7 +77,8 @@ struct chili_ctx {
     long long pipe_tile = 1 << 22;  // option "pipeline_tile": points per tile
     PointProgram pp_host;      // host copy (sizes of the memo buffers)
     DevBuf node_soa, memo, cfail, dcv, vwv;
-    DevBuf hints, sorted;      // hinted bin search tables of the grids
+    DevBuf hints, sorted, widths;  // hinted bin search tables and bin widths of the grids
+    DevBuf ich_tile;
     // channel weights: alpha[CH], best[CH], cp[CH], min_diff
     DevBuf alpha_buf;
     bool alpha_set = false;
@@ -265,9 +266,9 @@ template <int D>
 void launch_channel(chili_ctx *ctx, long long base, long long T, long long mr, int bins, int opt,
                     const long long *n_list, int32_t *rec_slot, double *rec_dens) {
     k_pp_channel<D><<<dim3(ctx->nch, static_cast<unsigned>((T + 127) / 128)), 128, 0, ctx->stream>>>(
-        ctx->point_prog.as<PointProgram>(), ctx->edges.as<double>(), ctx->hints.as<uint16_t>(),
-        ctx->sorted.as<uint8_t>(), bins, ctx->memo.as<double>(), ctx->cfail.as<uint8_t>(), ctx->ich.as<int32_t>(),
-        ctx->list.as<int32_t>(), n_list, base, T, mr, opt, ctx->dcv.as<double>(), ctx->vwv.as<double>(), rec_slot,
+        ctx->point_prog.as<PointProgram>(), ctx->edges.as<double>(), ctx->hints.as<uint32_t>(),
+        ctx->sorted.as<uint8_t>(), ctx->widths.as<double>(), bins, ctx->memo.as<double>(), ctx->cfail.as<uint8_t>(),
+        ctx->ich_tile.as<int32_t>(), n_list, base, T, mr, opt, ctx->dcv.as<double>(), ctx->vwv.as<double>(), rec_slot,
         rec_dens);
 }
 
@@ -286,6 +287,7 @@ int launch_pipeline(chili_ctx *ctx, long long m, long long n_pre, int bins, bool
     CK(ctx->memo.ensure(sizeof(double) * std::max(1, P.n_memo) * T));
     CK(ctx->cfail.ensure(static_cast<size_t>(std::max(1, P.n_chains)) * T));
     CK(ctx->dcv.ensure(sizeof(double) * ctx->nch * T));
+    CK(ctx->ich_tile.ensure(sizeof(int32_t) * T));
     CK(ctx->vwv.ensure(sizeof(double) * ctx->nch * T));
     const long long *n_list = reinterpret_cast<const long long *>(
         reinterpret_cast<const char *>(ctl_pre) + offsetof(RoundCtl, n_acc));
@@ -294,8 +296,9 @@ int launch_pipeline(chili_ctx *ctx, long long m, long long n_pre, int bins, bool
     const int o = opt ? 1 : 0;
     for (long long base = 0; base < n_pre; base += T) {
         { KTimer kt_(ctx, KT_NODES);
-        k_pp_nodes<<<gx, 256, 0, ctx->stream>>>(pp, ctx->mom_soa.as<double>(), m, ctx->list.as<int32_t>(), n_list,
-                                                 base, ctx->node_soa.as<double>(), T); }
+        k_pp_nodes<<<gx, 256, 0, ctx->stream>>>(pp, ctx->mom_soa.as<double>(), m, ctx->list.as<int32_t>(),
+                                                 ctx->ich.as<int32_t>(), n_list, base, ctx->node_soa.as<double>(),
+                                                 ctx->ich_tile.as<int32_t>(), T); }
         LAUNCHED();
         if (n_items > 0) {
             KTimer kt_(ctx, KT_ITEMS);
@@ -328,11 +331,13 @@ int launch_pipeline(chili_ctx *ctx, long long m, long long n_pre, int bins, bool
 // every change of the edges.
 int rebuild_hints(chili_ctx *ctx) {
     const int H = kHintPerBin * ctx->bins;
-    CK(ctx->hints.ensure(sizeof(uint16_t) * static_cast<size_t>(ctx->g_nch) * ctx->dims * (H + 1)));
+    CK(ctx->hints.ensure(sizeof(uint32_t) * static_cast<size_t>(ctx->g_nch) * ctx->dims * H));
     CK(ctx->sorted.ensure(static_cast<size_t>(ctx->g_nch) * ctx->dims));
+    CK(ctx->widths.ensure(sizeof(double) * static_cast<size_t>(ctx->g_nch) * ctx->dims * ctx->bins));
     k_build_hints<<<dim3(ctx->dims, ctx->g_nch), 128, 0, ctx->stream>>>(ctx->edges.as<double>(), ctx->dims, ctx->bins,
-                                                                        ctx->hints.as<uint16_t>(),
-                                                                        ctx->sorted.as<uint8_t>());
+                                                                        ctx->hints.as<uint32_t>(),
+                                                                        ctx->sorted.as<uint8_t>(),
+                                                                        ctx->widths.as<double>());
     LAUNCHED();
     return CHILI_OK;
 }
@@ -381,7 +386,7 @@ int chili_gpu_destroy(chili_ctx *ctx) {
     if (!ctx) return CHILI_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    DevBuf *bufs[] = {&ctx->edges, &ctx->edges_tmp, &ctx->progs, &ctx->point_prog, &ctx->node_soa, &ctx->memo, &ctx->cfail, &ctx->dcv, &ctx->vwv, &ctx->hints, &ctx->sorted, &ctx->alpha_buf, &ctx->f_dev, &ctx->mom_soa,
+    DevBuf *bufs[] = {&ctx->edges, &ctx->edges_tmp, &ctx->progs, &ctx->point_prog, &ctx->node_soa, &ctx->memo, &ctx->cfail, &ctx->dcv, &ctx->vwv, &ctx->hints, &ctx->sorted, &ctx->widths, &ctx->ich_tile, &ctx->alpha_buf, &ctx->f_dev, &ctx->mom_soa,
                       &ctx->ich, &ctx->flag, &ctx->list, &ctx->block_count, &ctx->block_off, &ctx->part,
                       &ctx->hist, &ctx->round_res, &ctx->acc, &ctx->ctl, &ctx->status, &ctx->v_part,
                       &ctx->v_hist, &ctx->v_train, &ctx->v_out, &ctx->rec, &ctx->ctl3};
@@ -534,7 +539,7 @@ int chili_gpu_grid_weight(chili_ctx *ctx, int ch, const double *x, double *w, in
     if ((rc = resolve(ctx, w, sizeof(double) * n, 1, false, aw))) return rc;
     if ((rc = resolve(ctx, bin, sizeof(int32_t) * n * D, 2, false, ab))) return rc;
     const double *g = ctx->edges.as<double>() + static_cast<size_t>(ch) * D * (B + 1);
-    const uint16_t *hg = ctx->hints.as<uint16_t>() + static_cast<size_t>(ch) * D * (kHintPerBin * B + 1);
+    const uint32_t *hg = ctx->hints.as<uint32_t>() + static_cast<size_t>(ch) * D * (kHintPerBin * B);
     const uint8_t *sg = ctx->sorted.as<uint8_t>() + static_cast<size_t>(ch) * D;
     k_grid_weight<<<grid_for(n, 128), 128, 0, ctx->stream>>>(g, hg, sg, D, B, static_cast<const double *>(ax.dev),
                                                              static_cast<double *>(aw.dev),

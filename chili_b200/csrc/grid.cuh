@@ -118,12 +118,13 @@ __device__ __forceinline__ int edge_cell(double v, int H) {
     return p >= static_cast<double>(H) ? H : static_cast<int>(p);
 }
 
-__device__ __forceinline__ int find_bin_hinted(const double *__restrict__ e, const uint16_t *__restrict__ hint,
+__device__ __forceinline__ int find_bin_hinted(const double *__restrict__ e, const uint32_t *__restrict__ hint,
                                                bool sorted, int bins, int H, double x) {
     if (!sorted || !(x >= 0.0 && x < 1.0)) return find_bin(e, bins, x);
     const int c = static_cast<int>(x * static_cast<double>(H));  // < H for x < 1
-    int first = __ldg(hint + c);
-    int len = __ldg(hint + c + 1) - first;
+    const uint32_t hp = __ldg(hint + c);  // hint[c] | hint[c+1] << 16
+    int first = static_cast<int>(hp & 0xffffu);
+    int len = static_cast<int>(hp >> 16) - first;
     while (len > 0) {  // lower_bound inside the bracket
         const int half = len >> 1;
         const int mid = first + half;
@@ -137,36 +138,52 @@ __device__ __forceinline__ int find_bin_hinted(const double *__restrict__ e, con
     return first - 1;
 }
 
-// One block per (dim = blockIdx.x, grid = blockIdx.y): the hint table and the
-// monotone flag of that edge table.
-__global__ void k_build_hints(const double *__restrict__ grids, int dims, int bins, uint16_t *__restrict__ hints,
-                              uint8_t *__restrict__ sorted) {
+// width(dim, bin) from the precomputed table wt[dim*bins + bin] (the same
+// subtraction as bin_width, done once per grid), the reference's reading of
+// bin == SIZE_MAX from the edges.
+__device__ __forceinline__ double bin_width_t(const double *__restrict__ g, const double *__restrict__ wt, int bins,
+                                              int dim, int bin, double before) {
+    if (bin >= 0) return __ldg(wt + dim * bins + bin);
+    return bin_width(g, bins, dim, bin, before);
+}
+
+// One block per (dim = blockIdx.x, grid = blockIdx.y): the hint table (as
+// pairs hint[j] | hint[j+1] << 16, j < H), the monotone flag and the bin
+// widths of that edge table.
+__global__ void k_build_hints(const double *__restrict__ grids, int dims, int bins, uint32_t *__restrict__ hints,
+                              uint8_t *__restrict__ sorted, double *__restrict__ widths) {
     const int d = blockIdx.x, c = blockIdx.y;
     const int H = kHintPerBin * bins;
     const double *e = grids + (static_cast<size_t>(c) * dims + d) * (bins + 1);
-    uint16_t *h = hints + (static_cast<size_t>(c) * dims + d) * (H + 1);
+    uint32_t *h = hints + (static_cast<size_t>(c) * dims + d) * H;
+    double *w = widths + (static_cast<size_t>(c) * dims + d) * bins;
     int bad = 0;
     for (int k = threadIdx.x; k < bins; k += blockDim.x) {
         const double a = e[k];
         if (a != a) bad = 1;
         if (k + 1 < bins && !(a <= e[k + 1])) bad = 1;
+        w[k] = __dsub_rn(e[k + 1], a);
     }
     bad = __syncthreads_or(bad);
     if (threadIdx.x == 0) sorted[static_cast<size_t>(c) * dims + d] = bad ? 0 : 1;
     if (bad) return;
-    for (int j = threadIdx.x; j <= H; j += blockDim.x) {
-        // first k in [0, bins) with cell(e[k]) >= j (cells are monotone)
-        int first = 0, len = bins;
-        while (len > 0) {
-            const int half = len >> 1, mid = first + half;
-            if (edge_cell(e[mid], H) < j) {
-                first = mid + 1;
-                len = len - half - 1;
-            } else {
-                len = half;
+    for (int j = threadIdx.x; j < H; j += blockDim.x) {
+        // first k in [0, bins) with cell(e[k]) >= j, and the same for j+1
+        int lo[2];
+        for (int q = 0; q < 2; ++q) {
+            int first = 0, len = bins;
+            while (len > 0) {
+                const int half = len >> 1, mid = first + half;
+                if (edge_cell(e[mid], H) < j + q) {
+                    first = mid + 1;
+                    len = len - half - 1;
+                } else {
+                    len = half;
+                }
             }
+            lo[q] = first;
         }
-        h[j] = static_cast<uint16_t>(first);
+        h[j] = static_cast<uint32_t>(lo[0]) | (static_cast<uint32_t>(lo[1]) << 16);
     }
 }
 

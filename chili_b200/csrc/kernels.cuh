@@ -136,7 +136,7 @@ __global__ void k_grid_map(const double *__restrict__ g, int dims, int bins, con
 
 // AdaptiveMap::FindBin / GenerateWeight through the hinted search that the
 // iteration uses (grid.cuh, find_bin_hinted).
-__global__ void k_grid_weight(const double *__restrict__ g, const uint16_t *__restrict__ hints,
+__global__ void k_grid_weight(const double *__restrict__ g, const uint32_t *__restrict__ hints,
                               const uint8_t *__restrict__ sorted, int dims, int bins, const double *__restrict__ x,
                               double *__restrict__ w, int32_t *__restrict__ bin, long long n) {
     const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
@@ -145,7 +145,7 @@ __global__ void k_grid_weight(const double *__restrict__ g, const uint16_t *__re
     const double fb = static_cast<double>(bins);
     const int H = kHintPerBin * bins;
     for (int d = 0; d < dims; ++d) {
-        const int b = find_bin_hinted(g + d * (bins + 1), hints + d * (H + 1), sorted[d] != 0, bins, H,
+        const int b = find_bin_hinted(g + d * (bins + 1), hints + d * H, sorted[d] != 0, bins, H,
                                       x[i * dims + d]);
         if (bin) bin[i * dims + d] = b;
         jac = __dmul_rn(jac, __dmul_rn(bin_width(g, bins, d, b, edge_before_table(dims, bins)), fb));

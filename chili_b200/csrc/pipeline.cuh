@@ -43,11 +43,14 @@ __device__ __forceinline__ void store_v4(double *__restrict__ soa, int node, lon
 // (mom_soa, stride mc), compounds summed as the reference's tmp_mom.
 __global__ void __launch_bounds__(256) k_pp_nodes(const PointProgram *__restrict__ pp, const double *__restrict__ mom_soa,
                                                   long long mc, const int32_t *__restrict__ list,
+                                                  const int32_t *__restrict__ ich_arr,
                                                   const long long *__restrict__ n_list, long long base,
-                                                  double *__restrict__ node_soa, long long m) {
+                                                  double *__restrict__ node_soa, int32_t *__restrict__ ich_tile,
+                                                  long long m) {
     const long long i = blockIdx.x * 256ll + threadIdx.x;  // tile-local point
     if (i >= m || base + i >= *n_list) return;
     const long long k = list[base + i];
+    ich_tile[i] = ich_arr[k];
     const int ne = pp->n_ext, nn = pp->n_nodes;
     for (int s = 0; s < ne; ++s) store_v4(node_soa, s, m, i, load_v4(mom_soa, s, mc, k));
     for (int s = ne; s < nn; ++s)
@@ -217,9 +220,9 @@ __device__ __forceinline__ double eval_momenta_soa(const IntegrandDesc *__restri
 // the point's own channel, the histogram slots.
 template <int DIMS>
 __global__ void __launch_bounds__(128) k_pp_channel(
-    const PointProgram *__restrict__ pp, const double *__restrict__ grids, const uint16_t *__restrict__ hints,
-    const uint8_t *__restrict__ sorted, int bins, const double *__restrict__ memo, const uint8_t *__restrict__ cfail,
-    const int32_t *__restrict__ ich_arr, const int32_t *__restrict__ list, const long long *__restrict__ n_list,
+    const PointProgram *__restrict__ pp, const double *__restrict__ grids, const uint32_t *__restrict__ hints,
+    const uint8_t *__restrict__ sorted, const double *__restrict__ widths, int bins, const double *__restrict__ memo,
+    const uint8_t *__restrict__ cfail, const int32_t *__restrict__ ich_tile, const long long *__restrict__ n_list,
     long long base, long long m, long long mr, int should_opt, double *__restrict__ dcv, double *__restrict__ vwv,
     int32_t *__restrict__ rec_slot, double *__restrict__ rec_dens) {
     const long long i = blockIdx.y * 128ll + threadIdx.x;  // tile-local point
@@ -259,14 +262,15 @@ __global__ void __launch_bounds__(128) k_pp_channel(
     const double fb = static_cast<double>(bins);
     const double before = edge_before_table(DIMS, bins);
     const double *g = grids + static_cast<size_t>(c) * DIMS * (bins + 1);
-    const uint16_t *hc = hints + static_cast<size_t>(c) * DIMS * (H + 1);
+    const uint32_t *hc = hints + static_cast<size_t>(c) * DIMS * H;
+    const double *wc = widths + static_cast<size_t>(c) * DIMS * bins;
     const uint8_t *sc = sorted + c * DIMS;
-    const bool chosen = should_opt && c == ich_arr[list[r]];
+    const bool chosen = should_opt && c == ich_tile[i];
     double vw = 1.0;
 #pragma unroll
     for (int p = 0; p < DIMS; ++p) {
-        const int b = find_bin_hinted(g + p * (bins + 1), hc + p * (H + 1), __ldg(sc + p) != 0, bins, H, x[p]);
-        vw = __dmul_rn(vw, __dmul_rn(bin_width(g, bins, p, b, before), fb));
+        const int b = find_bin_hinted(g + p * (bins + 1), hc + p * H, __ldg(sc + p) != 0, bins, H, x[p]);
+        vw = __dmul_rn(vw, __dmul_rn(bin_width_t(g, wc, bins, p, b, before), fb));
         if (chosen) {
             const int s = p * bins + b;
             rec_slot[p * mr + r] = s >= 0 ? c * DIMS * bins + s : -1;
