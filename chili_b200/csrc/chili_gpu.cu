@@ -302,8 +302,15 @@ int launch_pipeline(chili_ctx *ctx, long long m, long long n_pre, int bins, bool
         LAUNCHED();
         if (n_items > 0) {
             KTimer kt_(ctx, KT_ITEMS);
-            k_pp_items<<<dim3(n_items, gx), 256, 0, ctx->stream>>>(pp, ctx->node_soa.as<double>(), n_list, base, T,
-                                                                    ctx->memo.as<double>());
+            if (P.n_tents > 0)
+                k_pp_items<0><<<dim3(P.n_tents, gx), 256, 0, ctx->stream>>>(pp, ctx->node_soa.as<double>(), n_list,
+                                                                             base, T, ctx->memo.as<double>());
+            if (P.n_dws > 0)
+                k_pp_items<1><<<dim3(P.n_dws, gx), 256, 0, ctx->stream>>>(pp, ctx->node_soa.as<double>(), n_list,
+                                                                           base, T, ctx->memo.as<double>());
+            if (P.n_sws > 0)
+                k_pp_items<2><<<dim3(P.n_sws, gx), 256, 0, ctx->stream>>>(pp, ctx->node_soa.as<double>(), n_list,
+                                                                           base, T, ctx->memo.as<double>());
             LAUNCHED();
         }
         { KTimer kt_(ctx, KT_CHAINS);

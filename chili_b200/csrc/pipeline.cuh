@@ -60,15 +60,19 @@ __global__ void __launch_bounds__(256) k_pp_nodes(const PointProgram *__restrict
 // One thread per (point, item): items 0..n_tents-1 are t-channel entries
 // (Channel.cc:160-186), then decay weights (Channel.cc:83-113), then two-body
 // decays (Channel.cc:222-237).
+// KIND selects the item type (0 t-entries, 1 decay weights, 2 two-body
+// decays), so that each type gets its own register allocation.
+template <int KIND>
 __global__ void __launch_bounds__(256) k_pp_items(const PointProgram *__restrict__ pp,
                                                   const double *__restrict__ node_soa,
                                                   const long long *__restrict__ n_list, long long base, long long m,
                                                   double *__restrict__ memo) {
     const long long i = blockIdx.y * 256ll + threadIdx.x;  // tile-local point
     if (i >= m || base + i >= *n_list) return;
-    int item = blockIdx.x;  // consecutive blocks: items of the same points (L2 reuse)
+    // consecutive blocks: items of the same points (L2 reuse)
+    int item = blockIdx.x + (KIND >= 1 ? pp->n_tents : 0) + (KIND >= 2 ? pp->n_dws : 0);
     const double sqrts = pp->sqrts, ptmax = pp->ptmax;
-    if (item < pp->n_tents) {
+    if (KIND == 0 && item < pp->n_tents) {
         const int t = item;
         const double ptmin = pp->tent_ptmin[t];
         const V4 q = load_v4(node_soa, pp->tent_node[t], m, i);
@@ -87,7 +91,7 @@ __global__ void __launch_bounds__(256) k_pp_items(const PointProgram *__restrict
         return;
     }
     item -= pp->n_tents;
-    if (item < pp->n_dws) {
+    if (KIND == 1 && item < pp->n_dws) {
         const int k = item;
         const V4 a = load_v4(node_soa, pp->dw_c1[k], m, i), b = load_v4(node_soa, pp->dw_c2[k], m, i);
         const double r = sqrt(fabs(mass2(a))) + sqrt(fabs(mass2(b)));
@@ -108,7 +112,7 @@ __global__ void __launch_bounds__(256) k_pp_items(const PointProgram *__restrict
         return;
     }
     item -= pp->n_dws;
-    if (item < pp->n_sws) {
+    if (KIND == 2 && item < pp->n_sws) {
         const int k = item;
         double r1, r2;
         const double w = schannel_weight(load_v4(node_soa, pp->sw_a[k], m, i), load_v4(node_soa, pp->sw_b[k], m, i),
