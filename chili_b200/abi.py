@@ -114,6 +114,23 @@ class MCIterInfo(C.Structure):
                 ("points_weighted", C.c_uint64)]
 
 
+class FlowParams(C.Structure):
+    """chili_flow_params (learned proposal)."""
+    _fields_ = [("layers", C.c_int32), ("batch", C.c_int32), ("lr", C.c_double), ("init_seed", C.c_uint64)]
+
+    @classmethod
+    def defaults(cls, **kw):
+        p = cls(layers=6, batch=65536, lr=1e-3, init_seed=1)
+        for k, v in kw.items():
+            setattr(p, k, v)
+        return p
+
+
+class FlowIterInfo(C.Structure):
+    _fields_ = [("points", C.c_uint64), ("nonzero", C.c_uint64), ("nonfinite", C.c_uint64),
+                ("weight_max", C.c_double), ("unweighting_efficiency", C.c_double)]
+
+
 class ChannelSet:
     """Owns ctypes arrays for a list of channel descriptions and one Cuts
     table, keeping them alive while a library call reads them."""

@@ -14,7 +14,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libchili_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["chili_gpu.cu", "channel_program.cpp"]
+SOURCES = ["chili_gpu.cu", "flow.cu", "flow_layers.cu", "flow_alpha.cu", "channel_program.cpp"]
 
 
 def nvcc():
@@ -34,14 +34,30 @@ def needs_build(out=OUT):
 
 
 def build(force=False, verbose=False):
+    """Compiles every source to an object in parallel (chili_b200/_build/),
+    then links the shared library."""
     if not force and not needs_build():
         return OUT
-    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-           "-I" + os.path.join(ROOT, "include"), "-I" + CSRC, "-o", OUT + ".tmp"]
-    cmd += [os.path.join(CSRC, s) for s in SOURCES]
+    from concurrent.futures import ThreadPoolExecutor
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    common = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+              "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
+
+    def compile_one(src):
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
+        cmd = common + ["-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        objs = list(ex.map(compile_one, SOURCES))
+    link = [nvcc(), *ARCH, "-shared", "-o", OUT + ".tmp", *objs]
     if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+        print(" ".join(link))
+    subprocess.run(link, check=True)
     os.replace(OUT + ".tmp", OUT)
     return OUT
 

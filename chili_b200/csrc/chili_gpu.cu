@@ -20,240 +20,11 @@
 #include "channel_program.h"
 #include "kernels.cuh"
 #include "pipeline.cuh"
+#include "context.h"
 
 using namespace chili_dev;
 
 namespace {
-
-thread_local std::string g_last_error;
-
-// A growable device buffer.
-struct DevBuf {
-    void *p = nullptr;
-    size_t cap = 0;
-    cudaError_t ensure(size_t bytes) {
-        if (bytes <= cap) return cudaSuccess;
-        if (p) {
-            cudaError_t e = cudaFree(p);
-            if (e != cudaSuccess) return e;
-            p = nullptr;
-            cap = 0;
-        }
-        const size_t want = std::max<size_t>(bytes, 256);
-        cudaError_t e = cudaMalloc(&p, want);
-        if (e == cudaSuccess) cap = want;
-        return e;
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-    }
-    template <class T> T *as() const { return static_cast<T *>(p); }
-};
-
-constexpr int kStageSlots = 6;
-
-}  // namespace
-
-struct chili_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    std::string err;
-    unsigned long long launches = 0;
-
-    // grids
-    int g_nch = 0, dims = 0, bins = 0;
-    DevBuf edges, edges_tmp;
-    // channels
-    int nch = 0, n_ext = 0, ndims = 0;
-    double sqrts = 0;
-    DevBuf progs;
-    DevBuf point_prog;         // PointProgram of the channel set, when it fits
-    bool have_pp = false;      // the set fits the PointProgram limits
-    bool use_pp = true;        // option "point_program"
-    bool use_pipeline = true;  // option "pipeline": phased weight pass
-    long long pipe_tile = 1 << 22;  // option "pipeline_tile": points per tile
-    PointProgram pp_host;      // host copy (sizes of the memo buffers)
-    DevBuf node_soa, memo, cfail, dcv, vwv;
-    DevBuf hints, sorted, widths;  // hinted bin search tables and bin widths of the grids
-    DevBuf ich_tile;
-    // channel weights: alpha[CH], best[CH], cp[CH], min_diff
-    DevBuf alpha_buf;
-    bool alpha_set = false;
-    // integrand
-    IntegrandDesc f_host{};
-    DevBuf f_dev;
-    bool f_set = false;
-    // multichannel iteration scratch
-    DevBuf mom_soa, ich, flag, list, block_count, block_off, part, hist, round_res, acc, ctl, status;
-    RoundCtl *ctl_host = nullptr;  // pinned
-    double accept_rate = 0.5, nan_rate = 0.0;
-    DevBuf rec, ctl3;
-    // plain VEGAS scratch
-    DevBuf v_part, v_hist, v_train, v_out;
-    // staging of host buffers
-    DevBuf stage[kStageSlots];
-    int max_smem_optin = 0;
-    // option "kernel_timing": CUDA events around the iteration's kernels
-    bool timing = false;
-    struct Pending {
-        int kernel;
-        cudaEvent_t a, b;
-    };
-    std::vector<Pending> pending;
-    std::vector<cudaEvent_t> event_pool;
-    double ktime_ms[16] = {0};
-    unsigned long long klaunches[16] = {0};
-};
-
-namespace {
-
-// Kernel classes timed under the "kernel_timing" option.
-const char *const kTimedKernels[] = {"k_mc_forward", "k_pp_nodes", "k_pp_items", "k_pp_chains", "k_pp_channel",
-                                     "k_pp_combine", "k_mc_weight", "k_mc_accum", "k_vegas_iter", nullptr};
-enum { KT_FORWARD, KT_NODES, KT_ITEMS, KT_CHAINS, KT_CHANNEL, KT_COMBINE, KT_WEIGHT, KT_ACCUM, KT_VEGAS };
-
-cudaEvent_t take_event(chili_ctx *ctx) {
-    if (!ctx->event_pool.empty()) {
-        cudaEvent_t e = ctx->event_pool.back();
-        ctx->event_pool.pop_back();
-        return e;
-    }
-    cudaEvent_t e = nullptr;
-    cudaEventCreate(&e);
-    return e;
-}
-
-// Brackets one launch with events when timing is on.
-struct KTimer {
-    chili_ctx *ctx;
-    int kernel;
-    cudaEvent_t a = nullptr;
-    KTimer(chili_ctx *c, int k) : ctx(c), kernel(k) {
-        if (ctx->timing) {
-            a = take_event(ctx);
-            cudaEventRecord(a, ctx->stream);
-        }
-    }
-    ~KTimer() {
-        if (ctx->timing && a) {
-            cudaEvent_t b = take_event(ctx);
-            cudaEventRecord(b, ctx->stream);
-            ctx->pending.push_back({kernel, a, b});
-        }
-    }
-};
-
-// Folds the recorded intervals into the totals (the stream must be idle).
-void collect_times(chili_ctx *ctx) {
-    for (auto &p : ctx->pending) {
-        float ms = 0;
-        if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
-            ctx->ktime_ms[p.kernel] += ms;
-            ctx->klaunches[p.kernel] += 1;
-        }
-        ctx->event_pool.push_back(p.a);
-        ctx->event_pool.push_back(p.b);
-    }
-    ctx->pending.clear();
-    cudaGetLastError();
-}
-
-int fail(chili_ctx *ctx, int code, const std::string &msg) {
-    if (ctx) ctx->err = msg;
-    g_last_error = msg;
-    return code;
-}
-
-#define CK(call)                                                                                  \
-    do {                                                                                          \
-        const cudaError_t e_ = (call);                                                            \
-        if (e_ != cudaSuccess)                                                                    \
-            return fail(ctx, CHILI_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-    } while (0)
-
-#define LAUNCHED()                                                                                     \
-    do {                                                                                               \
-        ++ctx->launches;                                                                               \
-        const cudaError_t e_ = cudaGetLastError();                                                     \
-        if (e_ != cudaSuccess) return fail(ctx, CHILI_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e_)); \
-    } while (0)
-
-bool is_device_ptr(const void *p) {
-    if (!p) return false;
-    cudaPointerAttributes a;
-    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
-}
-
-// Resolves a caller buffer to a device pointer: device buffers pass through,
-// host buffers are staged in slot `slot` (copied in when `in`).
-struct Arg {
-    void *dev = nullptr;
-    void *host = nullptr;
-    size_t bytes = 0;
-};
-
-int resolve(chili_ctx *ctx, const void *p, size_t bytes, int slot, bool in, Arg &a) {
-    a = Arg{};
-    a.bytes = bytes;
-    if (!p) return CHILI_OK;
-    if (is_device_ptr(p)) {
-        a.dev = const_cast<void *>(p);
-        return CHILI_OK;
-    }
-    CK(ctx->stage[slot].ensure(bytes));
-    a.dev = ctx->stage[slot].p;
-    a.host = const_cast<void *>(p);
-    if (in && bytes) CK(cudaMemcpyAsync(a.dev, p, bytes, cudaMemcpyHostToDevice, ctx->stream));
-    return CHILI_OK;
-}
-
-int finish_out(chili_ctx *ctx, const Arg &a) {
-    if (a.host && a.bytes) CK(cudaMemcpyAsync(a.host, a.dev, a.bytes, cudaMemcpyDeviceToHost, ctx->stream));
-    return CHILI_OK;
-}
-
-int sync_if_host(chili_ctx *ctx, std::initializer_list<const Arg *> args) {
-    for (const Arg *a : args)
-        if (a->host) {
-            CK(cudaStreamSynchronize(ctx->stream));
-            return CHILI_OK;
-        }
-    return CHILI_OK;
-}
-
-unsigned grid_for(long long n, int block) { return static_cast<unsigned>((n + block - 1) / block); }
-
-double *alpha_ptr(chili_ctx *ctx) { return ctx->alpha_buf.as<double>(); }
-double *best_ptr(chili_ctx *ctx) { return ctx->alpha_buf.as<double>() + CHILI_MAX_CHANNELS; }
-double *cp_ptr(chili_ctx *ctx) { return ctx->alpha_buf.as<double>() + 2 * CHILI_MAX_CHANNELS; }
-double *mindiff_ptr(chili_ctx *ctx) { return ctx->alpha_buf.as<double>() + 3 * CHILI_MAX_CHANNELS; }
-const PointProgram *pp_ptr(chili_ctx *ctx) {
-    return (ctx->have_pp && ctx->use_pp) ? ctx->point_prog.as<PointProgram>() : nullptr;
-}
-double *acc_train_ptr(chili_ctx *ctx) {
-    return reinterpret_cast<double *>(static_cast<char *>(ctx->acc.p) + offsetof(IterAcc, atrain));
-}
-
-int need_grids(chili_ctx *ctx) {
-    if (!ctx->edges.p || ctx->g_nch <= 0) return fail(ctx, CHILI_ERR_STATE, "no grids set");
-    return CHILI_OK;
-}
-int need_channels(chili_ctx *ctx) {
-    if (!ctx->progs.p || ctx->nch <= 0) return fail(ctx, CHILI_ERR_STATE, "no channels set");
-    return CHILI_OK;
-}
-
-int set_device(chili_ctx *ctx) {
-    CK(cudaSetDevice(ctx->device));
-    return CHILI_OK;
-}
 
 bool pipeline_dims_ok(int d) {
     switch (d) {
@@ -398,6 +169,7 @@ int chili_gpu_destroy(chili_ctx *ctx) {
                       &ctx->hist, &ctx->round_res, &ctx->acc, &ctx->ctl, &ctx->status, &ctx->v_part,
                       &ctx->v_hist, &ctx->v_train, &ctx->v_out, &ctx->rec, &ctx->ctl3};
     for (DevBuf *b : bufs) b->release();
+    flow_release(ctx);
     for (auto &b : ctx->stage) b.release();
     if (ctx->ctl_host) cudaFreeHost(ctx->ctl_host);
     collect_times(ctx);

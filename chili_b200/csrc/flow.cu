@@ -1,0 +1,749 @@
+// flow.cu -- the learned proposal's entry points (include/chili_gpu.h,
+// "learned proposal"): parameter layout and initialisation, the training
+// step (sample batch -> flow forward -> channel-weight network and loss ->
+// flow backward and weight gradients per layer -> Adam -> bf16 tiles), the
+// flow-path integration pass, and the parity entry points.
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "context.h"
+#include "flow_phys.cuh"
+#include "flow_launch.h"
+
+using namespace chili_flow;
+
+struct FlowState {
+    int D = 0, nch = 0, L = 0, F = 0, n_ext = 0, sms = 148;
+    long long batch = 65536;
+    float lr = 1e-3f;
+    std::vector<FlowLayer> layers;
+    std::vector<int> da, db;
+    std::vector<std::vector<int>> cond, trans;
+    std::vector<long long> off_w1, off_e, off_w2, off_w3;
+    long long np_flow = 0, np = 0, off_alpha = 0;
+    AlphaLayout AL{};
+    DevBuf prm, m, v, grad, wtiles, part_f, part_a, loss_part, loss_dev;
+    DevBuf beta, logbeta, cp;  // f32 beta, f32 log beta, f64 selection table
+    std::vector<double> beta_host;
+    // training
+    long long nb = 0;
+    DevBuf X, chb, logf, fval, feat, logprior, logq, glogq, g0, g1, thetas, h1s, h2s, gths, gp2s, gp1s, scal;
+    double log_fscale = 0;
+    bool have_scale = false;
+    int adam_t = 0;
+    // sampling
+    DevBuf sx0, sx1, sz, su, sch, slq, spart, sfold;
+    DevBuf err;
+};
+
+namespace {
+
+constexpr int kNsplit = 48;
+constexpr int kAlphaSplit = 148;
+constexpr long long kSampleChunk = 1ll << 20;
+
+// Coupling masks: the rule of include/chili_gpu.h ("learned proposal").
+void flow_masks(int D, int L, std::vector<std::vector<int>> &cond, std::vector<std::vector<int>> &trans) {
+    cond.assign(L, {});
+    trans.assign(L, {});
+    for (int l = 0; l < L; ++l) {
+        std::vector<bool> m(D);
+        if (D <= 10) {
+            for (int i = 0; i < D; ++i) {
+                bool v;
+                switch (l % 6) {
+                case 0: v = i % 2 == 0; break;
+                case 1: v = i % 2 == 1; break;
+                case 2: v = i < D / 2; break;
+                case 3: v = i >= D / 2; break;
+                case 4: v = ((i + 1) / 2) % 2 == 0; break;
+                default: v = ((i + 1) / 2) % 2 == 1; break;
+                }
+                m[i] = v;
+            }
+            bool all = true, none = true;
+            for (int i = 0; i < D; ++i) {
+                all = all && m[i];
+                none = none && !m[i];
+            }
+            if (all || none)
+                for (int i = 0; i < D; ++i) m[i] = (i % 2) == (l % 2);
+        } else {
+            for (int i = 0; i < D; ++i) m[i] = true;
+            for (int k = 0; k < 5; ++k) m[(5 * l + k) % D] = false;
+        }
+        for (int i = 0; i < D; ++i) (m[i] ? cond[l] : trans[l]).push_back(i);
+    }
+}
+
+uint64_t splitmix(uint64_t &s) {
+    uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+double unif_pm1(uint64_t &s) { return (static_cast<double>(splitmix(s) >> 11) * 0x1.0p-53) * 2.0 - 1.0; }
+
+int need_flow(chili_ctx *ctx) {
+    if (!ctx->flow) return fail(ctx, CHILI_ERR_STATE, "learned proposal not initialised (chili_gpu_flow_init)");
+    return CHILI_OK;
+}
+
+template <class K>
+int smem_attr(chili_ctx *ctx, K kernel, size_t bytes) {
+    CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
+    return CHILI_OK;
+}
+
+int upload_beta(chili_ctx *ctx) {
+    FlowState &S = *ctx->flow;
+    std::vector<float> b(S.nch), lb(S.nch);
+    std::vector<double> cp(S.nch);
+    double tot = 0;
+    for (int c = 0; c < S.nch; ++c) tot += S.beta_host[c];
+    double acc = 0;
+    for (int c = 0; c < S.nch; ++c) {
+        const double bc = S.beta_host[c] / tot;
+        b[c] = static_cast<float>(bc);
+        lb[c] = bc > 0 ? static_cast<float>(std::log(bc)) : -INFINITY;
+        acc += bc;
+        cp[c] = acc;
+    }
+    cp[S.nch - 1] = 1.0;
+    CK(cudaMemcpyAsync(S.beta.p, b.data(), sizeof(float) * S.nch, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(S.logbeta.p, lb.data(), sizeof(float) * S.nch, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(S.cp.p, cp.data(), sizeof(double) * S.nch, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHILI_OK;
+}
+
+int pack_tiles(chili_ctx *ctx) {
+    FlowState &S = *ctx->flow;
+    const float *p = S.prm.as<float>();
+    for (int l = 0; l < S.L; ++l) {
+        k_flow_pack<<<(kP * 128 + 255) / 256, 256, 0, ctx->stream>>>(
+            p + S.off_w1[l], p + S.off_w2[l], p + S.off_w3[l], S.da[l], S.db[l] * kPerDim,
+            S.wtiles.as<uint8_t>() + static_cast<size_t>(l) * kWBytes);
+        LAUNCHED();
+    }
+    return CHILI_OK;
+}
+
+int check_err(chili_ctx *ctx) {
+    int e = 0;
+    CK(cudaMemcpyAsync(&e, ctx->flow->err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (e) {
+        CK(cudaMemsetAsync(ctx->flow->err.p, 0, sizeof(int), ctx->stream));
+        return fail(ctx, CHILI_ERR_TIMEOUT, "tensor-core wait gave up in flow kernel (code " + std::to_string(e) + ")");
+    }
+    return CHILI_OK;
+}
+
+// ------------------------------------------------------------ launches
+int launch_wgrad(chili_ctx *ctx, const WgradArgs &a) {
+    static bool attr = false;
+    if (!attr) {
+        if (int rc = smem_attr(ctx, k_flow_wgrad, kWgSmem)) return rc;
+        attr = true;
+    }
+    k_flow_wgrad<<<dim3(kNsplit, 3), 128, kWgSmem, ctx->stream>>>(a);
+    LAUNCHED();
+    return CHILI_OK;
+}
+
+// ------------------------------------------------------ training buffers
+int ensure_train(chili_ctx *ctx, long long n) {
+    FlowState &S = *ctx->flow;
+    if (S.nb >= n) return CHILI_OK;
+    const long long tiles = (n + 127) / 128;
+    const size_t fN = sizeof(float) * n;
+    CK(S.X.ensure(fN * S.D * (S.L + 1)));
+    CK(S.chb.ensure(sizeof(int32_t) * n));
+    CK(S.logf.ensure(fN));
+    CK(S.fval.ensure(sizeof(double) * n));
+    CK(S.feat.ensure(fN * std::max(S.F, 1)));
+    CK(S.logprior.ensure(fN * S.nch));
+    CK(S.logq.ensure(fN));
+    CK(S.glogq.ensure(fN));
+    CK(S.g0.ensure(fN * S.D));
+    CK(S.g1.ensure(fN * S.D));
+    CK(S.thetas.ensure(fN * static_cast<size_t>(kMaxDB * kPerDim) * S.L));
+    CK(S.h1s.ensure(static_cast<size_t>(tiles) * kHTile * S.L));
+    CK(S.h2s.ensure(static_cast<size_t>(tiles) * kHTile * S.L));
+    CK(S.gths.ensure(static_cast<size_t>(tiles) * kGTile));
+    CK(S.gp2s.ensure(static_cast<size_t>(tiles) * kHTile));
+    CK(S.gp1s.ensure(static_cast<size_t>(tiles) * kHTile));
+    S.nb = n;
+    return CHILI_OK;
+}
+
+FlowLayer layer_dev(FlowState &S, int l) {
+    FlowLayer L = S.layers[l];
+    L.wt = S.wtiles.as<uint8_t>() + static_cast<size_t>(l) * kWBytes;
+    L.E = S.prm.as<float>() + S.off_e[l];
+    return L;
+}
+
+// Flow forward (density direction, saving), channel-weight network + loss,
+// flow backward and weight gradients, Adam (lr = 0: gradients only, into
+// S.grad), the step's loss into loss_dev[slot]. Inputs already in the
+// training buffers: X_0 = u, ch, logf, feat, logprior.
+int train_pass(chili_ctx *ctx, long long n, float lr, int slot) {
+    FlowState &S = *ctx->flow;
+    const long long tiles = (n + 127) / 128;
+    float *X = S.X.as<float>();
+    const size_t xs = static_cast<size_t>(S.D) * n;
+    const size_t thn = static_cast<size_t>(kMaxDB * kPerDim) * n;
+    CK(cudaMemsetAsync(S.logq.p, 0, sizeof(float) * n, ctx->stream));
+    for (int l = 0; l < S.L; ++l) {
+        LayerArgs a{};
+        a.L = layer_dev(S, l);
+        a.n = n;
+        a.xin = X + xs * l;
+        a.xout = X + xs * (l + 1);
+        a.ch = S.chb.as<int32_t>();
+        a.logq = S.logq.as<float>();
+        a.h1s = S.h1s.as<uint8_t>() + static_cast<size_t>(l) * tiles * kHTile;
+        a.h2s = S.h2s.as<uint8_t>() + static_cast<size_t>(l) * tiles * kHTile;
+        a.theta = S.thetas.as<float>() + thn * l;
+        a.err = S.err.as<int>();
+        if (int rc = flow_launch_layer(ctx, 0, true, a, S.sms)) return rc;
+    }
+    AlphaTrainArgs aa{};
+    aa.n = n;
+    aa.L = S.AL;
+    aa.w = S.prm.as<float>() + S.off_alpha;
+    aa.feat = S.feat.as<float>();
+    aa.logprior = S.logprior.as<float>();
+    aa.ch = S.chb.as<int32_t>();
+    aa.logf = S.logf.as<float>();
+    aa.logbeta = S.logbeta.as<float>();
+    aa.logq = S.logq.as<float>();
+    aa.glogq = S.glogq.as<float>();
+    aa.part = S.part_a.as<float>();
+    aa.loss_part = S.loss_part.as<double>();
+    if (int rc = flow_launch_alpha(ctx, aa)) return rc;
+    float *gcur = S.g0.as<float>(), *gnext = S.g1.as<float>();
+    for (int l = S.L - 1; l >= 0; --l) {
+        BwdArgs b{};
+        b.L = layer_dev(S, l);
+        b.n = n;
+        b.xin = X + xs * l;
+        b.theta = S.thetas.as<float>() + thn * l;
+        b.h1s = S.h1s.as<uint8_t>() + static_cast<size_t>(l) * tiles * kHTile;
+        b.h2s = S.h2s.as<uint8_t>() + static_cast<size_t>(l) * tiles * kHTile;
+        b.gout = l == S.L - 1 ? nullptr : gcur;
+        b.glogq = S.glogq.as<float>();
+        b.gin = gnext;
+        b.gths = S.gths.as<uint8_t>();
+        b.gp2s = S.gp2s.as<uint8_t>();
+        b.gp1s = S.gp1s.as<uint8_t>();
+        b.err = S.err.as<int>();
+        if (int rc = flow_launch_bwd(ctx, b, S.sms)) return rc;
+        WgradArgs w{};
+        w.n = n;
+        w.da = S.da[l];
+        w.nch = S.nch;
+        w.ncol2 = ((16 + S.nch) + 63) & ~63;
+        for (int i = 0; i < S.da[l]; ++i) w.cond[i] = static_cast<int8_t>(S.cond[l][i]);
+        w.xin = X + xs * l;
+        w.ch = S.chb.as<int32_t>();
+        w.h1s = b.h1s;
+        w.h2s = b.h2s;
+        w.gths = b.gths;
+        w.gp2s = b.gp2s;
+        w.gp1s = b.gp1s;
+        w.part = S.part_f.as<float>();
+        w.nparam = S.np_flow;
+        w.off_w1 = S.off_w1[l];
+        w.off_e = S.off_e[l];
+        w.off_w2 = S.off_w2[l];
+        w.off_w3 = S.off_w3[l];
+        w.P = S.db[l] * kPerDim;
+        w.err = S.err.as<int>();
+        if (int rc = launch_wgrad(ctx, w)) return rc;
+        std::swap(gcur, gnext);
+    }
+    ++S.adam_t;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - std::pow(b1, static_cast<float>(S.adam_t));
+    const float c2 = 1.f - std::pow(b2, static_cast<float>(S.adam_t));
+    float *grad = lr == 0.f ? S.grad.as<float>() : nullptr;
+    k_flow_adam<<<static_cast<unsigned>((S.np_flow + 255) / 256), 256, 0, ctx->stream>>>(
+        S.prm.as<float>(), S.m.as<float>(), S.v.as<float>(), S.part_f.as<float>(), kNsplit, S.np_flow, lr, b1, b2,
+        1e-8f, c1, c2, grad);
+    LAUNCHED();
+    k_flow_adam<<<static_cast<unsigned>((S.AL.total + 255) / 256), 256, 0, ctx->stream>>>(
+        S.prm.as<float>() + S.off_alpha, S.m.as<float>() + S.off_alpha, S.v.as<float>() + S.off_alpha,
+        S.part_a.as<float>(), kAlphaSplit, S.AL.total, lr, b1, b2, 1e-8f, c1, c2, grad ? grad + S.off_alpha : nullptr);
+    LAUNCHED();
+    if (lr == 0.f) --S.adam_t;
+    else if (int rc = pack_tiles(ctx)) return rc;
+    k_loss_fold<<<1, 1, 0, ctx->stream>>>(S.loss_part.as<double>(), kAlphaSplit, 1.0 / static_cast<double>(n),
+                                          S.loss_dev.as<double>() + slot);
+    LAUNCHED();
+    return CHILI_OK;
+}
+
+BatchArgs batch_args(chili_ctx *ctx, long long n, uint64_t seed, uint64_t ctr0) {
+    FlowState &S = *ctx->flow;
+    BatchArgs b{};
+    b.progs = ctx->progs.as<ChannelProgram>();
+    b.pp = ctx->point_prog.as<PointProgram>();
+    b.grids = ctx->edges.as<double>();
+    b.cp = S.cp.as<double>();
+    b.logbeta = S.logbeta.as<float>();
+    b.f = ctx->f_dev.as<IntegrandDesc>();
+    b.nch = S.nch;
+    b.dims = S.D;
+    b.bins = ctx->bins;
+    b.seed = seed;
+    b.ctr0 = ctr0;
+    b.n = n;
+    b.log_fscale = S.log_fscale;
+    b.u = S.X.as<float>();
+    b.ch = S.chb.as<int32_t>();
+    b.logf = S.logf.as<float>();
+    b.fval = nullptr;
+    b.feat = S.feat.as<float>();
+    b.logprior = S.logprior.as<float>();
+    return b;
+}
+
+// The flow over n points (xin, xout [D][n] on the device): the layers in
+// order (mode 0, density direction) or in reverse (mode 1, sampling).
+int flow_pass(chili_ctx *ctx, const float *xin_dev, const int32_t *ch_dev, long long n, int mode, float *xout_dev,
+              float *logq_dev) {
+    FlowState &S = *ctx->flow;
+    const size_t xs = static_cast<size_t>(S.D) * n;
+    CK(S.sx0.ensure(sizeof(float) * xs));
+    CK(S.sx1.ensure(sizeof(float) * xs));
+    CK(cudaMemsetAsync(logq_dev, 0, sizeof(float) * n, ctx->stream));
+    const float *cur = xin_dev;
+    float *bufs[2] = {S.sx0.as<float>(), S.sx1.as<float>()};
+    for (int k = 0; k < S.L; ++k) {
+        const int l = mode == 0 ? k : S.L - 1 - k;
+        LayerArgs a{};
+        a.L = layer_dev(S, l);
+        a.n = n;
+        a.xin = cur;
+        a.xout = k == S.L - 1 ? xout_dev : bufs[k & 1];
+        a.ch = ch_dev;
+        a.logq = logq_dev;
+        a.err = S.err.as<int>();
+        const int rc = flow_launch_layer(ctx, mode, false, a, S.sms);
+        if (rc) return rc;
+        cur = a.xout;
+    }
+    return CHILI_OK;
+}
+
+}  // namespace
+
+void flow_release(chili_ctx *ctx) {
+    if (!ctx || !ctx->flow) return;
+    FlowState &S = *ctx->flow;
+    for (DevBuf *b : {&S.prm, &S.m, &S.v, &S.grad, &S.wtiles, &S.part_f, &S.part_a, &S.loss_part, &S.loss_dev,
+                      &S.beta, &S.logbeta, &S.cp, &S.X, &S.chb, &S.logf, &S.fval, &S.feat, &S.logprior, &S.logq,
+                      &S.glogq, &S.g0, &S.g1, &S.thetas, &S.h1s, &S.h2s, &S.gths, &S.gp2s, &S.gp1s, &S.scal,
+                      &S.sx0, &S.sx1, &S.sz, &S.su, &S.sch, &S.slq, &S.spart, &S.sfold, &S.err})
+        b->release();
+    delete ctx->flow;
+    ctx->flow = nullptr;
+}
+
+extern "C" {
+
+int chili_gpu_flow_init(chili_ctx *ctx, const chili_flow_params *params) {
+    if (!ctx || !params) return fail(ctx, CHILI_ERR_INVALID_ARG, "null argument");
+    if (int rc = set_device(ctx)) return rc;
+    if (int rc = need_channels(ctx)) return rc;
+    if (int rc = need_grids(ctx)) return rc;
+    if (!ctx->f_set) return fail(ctx, CHILI_ERR_STATE, "no integrand set");
+    if (!ctx->have_pp) return fail(ctx, CHILI_ERR_LIMIT, "channel set exceeds the point-program limits");
+    if (ctx->g_nch != ctx->nch || ctx->dims != ctx->ndims)
+        return fail(ctx, CHILI_ERR_STATE, "grids do not match the channel set");
+    if (params->layers < 1 || params->layers > 32 || params->batch < 128 || params->batch > (1 << 24))
+        return fail(ctx, CHILI_ERR_INVALID_ARG, "layers in [1, 32], batch in [128, 2^24]");
+    const int F = n_features(ctx->n_ext);
+    if (ctx->nch > kMaxAlphaCh || F > kMaxFeat)
+        return fail(ctx, CHILI_ERR_LIMIT, "channel-weight network limited to 64 channels and 32 features");
+    flow_release(ctx);
+    ctx->flow = new FlowState();
+    FlowState &S = *ctx->flow;
+    S.D = ctx->ndims;
+    S.nch = ctx->nch;
+    S.L = params->layers;
+    S.F = F;
+    S.n_ext = ctx->n_ext;
+    S.batch = params->batch;
+    S.lr = static_cast<float>(params->lr);
+    cudaDeviceGetAttribute(&S.sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    flow_masks(S.D, S.L, S.cond, S.trans);
+    long long off = 0;
+    S.layers.resize(S.L);
+    for (int l = 0; l < S.L; ++l) {
+        const int da = static_cast<int>(S.cond[l].size()), db = static_cast<int>(S.trans[l].size());
+        if (da > kMaxDA || db > kMaxDB || da < 1 || db < 1) {
+            flow_release(ctx);
+            return fail(ctx, CHILI_ERR_LIMIT, "coupling split outside 1..16 conditioning / 1..5 transformed dims");
+        }
+        S.da.push_back(da);
+        S.db.push_back(db);
+        FlowLayer &L = S.layers[l];
+        std::memset(&L, 0, sizeof(L));
+        L.da = da;
+        L.db = db;
+        for (int i = 0; i < da; ++i) L.cond[i] = static_cast<int8_t>(S.cond[l][i]);
+        for (int j = 0; j < db; ++j) L.trans[j] = static_cast<int8_t>(S.trans[l][j]);
+        S.off_w1.push_back(off);
+        off += static_cast<long long>(kH) * da;
+        S.off_e.push_back(off);
+        off += static_cast<long long>(S.nch) * kH;
+        S.off_w2.push_back(off);
+        off += static_cast<long long>(kH) * kH;
+        S.off_w3.push_back(off);
+        off += static_cast<long long>(db) * kPerDim * kH;
+    }
+    S.np_flow = off;
+    S.off_alpha = off;
+    S.AL = alpha_layout(F, S.nch);
+    S.np = off + S.AL.total;
+    // initial parameters: identity flow, channel weights = the prior
+    std::vector<float> p(S.np, 0.f);
+    uint64_t rs = params->init_seed;
+    for (int l = 0; l < S.L; ++l) {
+        const int da = S.da[l], db = S.db[l];
+        const double b1 = std::sqrt(6.0 / da), b2 = std::sqrt(6.0 / kH);
+        for (int i = 0; i < kH * da; ++i) p[S.off_w1[l] + i] = static_cast<float>(b1 * unif_pm1(rs));
+        for (int i = 0; i < kH * kH; ++i) p[S.off_w2[l] + i] = static_cast<float>(b2 * unif_pm1(rs));
+        const float did = static_cast<float>(std::log(std::expm1(1.0 - 1e-3)));
+        for (int j = 0; j < db; ++j)
+            for (int k = 0; k <= kBins; ++k) p[S.off_w3[l] + (j * kPerDim + 2 * kBins + k) * kH + (kH - 1)] = did;
+    }
+    {
+        const double ba1 = std::sqrt(6.0 / F), ba2 = std::sqrt(6.0 / kAH);
+        for (int i = 0; i < kAH * F; ++i) p[S.off_alpha + S.AL.a1 + i] = static_cast<float>(ba1 * unif_pm1(rs));
+        for (int i = 0; i < kAH * kAH; ++i) p[S.off_alpha + S.AL.a2 + i] = static_cast<float>(ba2 * unif_pm1(rs));
+    }
+    CK(S.prm.ensure(sizeof(float) * S.np));
+    CK(S.m.ensure(sizeof(float) * S.np));
+    CK(S.v.ensure(sizeof(float) * S.np));
+    CK(S.grad.ensure(sizeof(float) * S.np));
+    CK(cudaMemcpyAsync(S.prm.p, p.data(), sizeof(float) * S.np, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemsetAsync(S.m.p, 0, sizeof(float) * S.np, ctx->stream));
+    CK(cudaMemsetAsync(S.v.p, 0, sizeof(float) * S.np, ctx->stream));
+    CK(S.wtiles.ensure(static_cast<size_t>(S.L) * kWBytes));
+    CK(cudaMemsetAsync(S.wtiles.p, 0, static_cast<size_t>(S.L) * kWBytes, ctx->stream));
+    CK(S.part_f.ensure(sizeof(float) * kNsplit * S.np_flow));
+    CK(S.part_a.ensure(sizeof(float) * kAlphaSplit * S.AL.total));
+    CK(S.loss_part.ensure(sizeof(double) * kAlphaSplit));
+    CK(S.loss_dev.ensure(sizeof(double) * 4096));
+    CK(S.beta.ensure(sizeof(float) * S.nch));
+    CK(S.logbeta.ensure(sizeof(float) * S.nch));
+    CK(S.cp.ensure(sizeof(double) * S.nch));
+    CK(S.err.ensure(sizeof(int)));
+    CK(cudaMemsetAsync(S.err.p, 0, sizeof(int), ctx->stream));
+    CK(S.scal.ensure(sizeof(double) * 2));
+    // beta = the multichannel channel weights
+    S.beta_host.assign(S.nch, 1.0 / S.nch);
+    if (ctx->alpha_set) {
+        std::vector<double> a(S.nch);
+        CK(cudaMemcpyAsync(a.data(), alpha_ptr(ctx), sizeof(double) * S.nch, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        double tot = 0;
+        for (double x : a) tot += x;
+        if (tot > 0 && std::isfinite(tot)) S.beta_host = a;
+    }
+    if (int rc = upload_beta(ctx)) return rc;
+    if (int rc = pack_tiles(ctx)) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHILI_OK;
+}
+
+int64_t chili_gpu_flow_nparams(const chili_ctx *ctx) { return (ctx && ctx->flow) ? ctx->flow->np : -1; }
+
+int chili_gpu_flow_get_params(chili_ctx *ctx, float *prm) {
+    if (!ctx || !prm) return fail(ctx, CHILI_ERR_INVALID_ARG, "null argument");
+    if (int rc = need_flow(ctx)) return rc;
+    if (int rc = set_device(ctx)) return rc;
+    Arg o;
+    if (int rc = resolve(ctx, prm, sizeof(float) * ctx->flow->np, 0, false, o)) return rc;
+    CK(cudaMemcpyAsync(o.dev, ctx->flow->prm.p, o.bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    if (int rc = finish_out(ctx, o)) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHILI_OK;
+}
+
+int chili_gpu_flow_set_params(chili_ctx *ctx, const float *prm) {
+    if (!ctx || !prm) return fail(ctx, CHILI_ERR_INVALID_ARG, "null argument");
+    if (int rc = need_flow(ctx)) return rc;
+    if (int rc = set_device(ctx)) return rc;
+    Arg in;
+    if (int rc = resolve(ctx, prm, sizeof(float) * ctx->flow->np, 0, true, in)) return rc;
+    CK(cudaMemcpyAsync(ctx->flow->prm.p, in.dev, in.bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemsetAsync(ctx->flow->m.p, 0, sizeof(float) * ctx->flow->np, ctx->stream));
+    CK(cudaMemsetAsync(ctx->flow->v.p, 0, sizeof(float) * ctx->flow->np, ctx->stream));
+    ctx->flow->adam_t = 0;
+    if (int rc = pack_tiles(ctx)) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHILI_OK;
+}
+
+int chili_gpu_flow_get_beta(chili_ctx *ctx, double *beta) {
+    if (!ctx || !beta) return fail(ctx, CHILI_ERR_INVALID_ARG, "null argument");
+    if (int rc = need_flow(ctx)) return rc;
+    double tot = 0;
+    for (double b : ctx->flow->beta_host) tot += b;
+    for (int c = 0; c < ctx->flow->nch; ++c) beta[c] = ctx->flow->beta_host[c] / tot;
+    return CHILI_OK;
+}
+
+int chili_gpu_flow_set_beta(chili_ctx *ctx, const double *beta) {
+    if (!ctx || !beta) return fail(ctx, CHILI_ERR_INVALID_ARG, "null argument");
+    if (int rc = need_flow(ctx)) return rc;
+    if (int rc = set_device(ctx)) return rc;
+    double tot = 0;
+    for (int c = 0; c < ctx->flow->nch; ++c) {
+        if (!(beta[c] >= 0) || !std::isfinite(beta[c]))
+            return fail(ctx, CHILI_ERR_INVALID_ARG, "beta must be finite and >= 0");
+        tot += beta[c];
+    }
+    if (!(tot > 0)) return fail(ctx, CHILI_ERR_INVALID_ARG, "beta sums to 0");
+    ctx->flow->beta_host.assign(beta, beta + ctx->flow->nch);
+    return upload_beta(ctx);
+}
+
+static int density_or_sample(chili_ctx *ctx, const float *xin, const int32_t *ch, int64_t n, float *xout, float *logq,
+                             int mode) {
+    if (!ctx || !xin || !ch || n <= 0) return fail(ctx, CHILI_ERR_INVALID_ARG, "null argument or n <= 0");
+    if (int rc = need_flow(ctx)) return rc;
+    if (int rc = set_device(ctx)) return rc;
+    FlowState &S = *ctx->flow;
+    const size_t xb = sizeof(float) * S.D * n;
+    Arg ai, ac, ao, aq;
+    if (int rc = resolve(ctx, xin, xb, 0, true, ai)) return rc;
+    if (int rc = resolve(ctx, ch, sizeof(int32_t) * n, 1, true, ac)) return rc;
+    if (int rc = resolve(ctx, xout, xout ? xb : 0, 2, false, ao)) return rc;
+    if (int rc = resolve(ctx, logq, logq ? sizeof(float) * n : 0, 3, false, aq)) return rc;
+    CK(S.sz.ensure(xb));
+    CK(S.su.ensure(xb));
+    CK(S.slq.ensure(sizeof(float) * n));
+    k_transpose_f<<<static_cast<unsigned>((n * S.D + 255) / 256), 256, 0, ctx->stream>>>(
+        static_cast<const float *>(ai.dev), S.sz.as<float>(), n, S.D, 1);
+    LAUNCHED();
+    if (int rc = flow_pass(ctx, S.sz.as<float>(), static_cast<const int32_t *>(ac.dev), n, mode, S.su.as<float>(),
+                           S.slq.as<float>()))
+        return rc;
+    if (ao.dev) {
+        k_transpose_f<<<static_cast<unsigned>((n * S.D + 255) / 256), 256, 0, ctx->stream>>>(
+            S.su.as<float>(), static_cast<float *>(ao.dev), n, S.D, 0);
+        LAUNCHED();
+    }
+    if (aq.dev) CK(cudaMemcpyAsync(aq.dev, S.slq.p, sizeof(float) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+    if (int rc = finish_out(ctx, ao)) return rc;
+    if (int rc = finish_out(ctx, aq)) return rc;
+    return check_err(ctx);
+}
+
+int chili_gpu_flow_density(chili_ctx *ctx, const float *u, const int32_t *ch, int64_t n, float *z, float *logq) {
+    return density_or_sample(ctx, u, ch, n, z, logq, 0);
+}
+
+int chili_gpu_flow_sample_u(chili_ctx *ctx, const float *z, const int32_t *ch, int64_t n, float *u, float *logq) {
+    return density_or_sample(ctx, z, ch, n, u, logq, 1);
+}
+
+int chili_gpu_flow_loss_grad(chili_ctx *ctx, const float *u, const int32_t *ch, const float *logf,
+                             const float *feat, const float *logprior, int64_t n, double *loss, float *grad) {
+    if (!ctx || !u || !ch || !logf || !feat || !logprior || n < 128)
+        return fail(ctx, CHILI_ERR_INVALID_ARG, "null argument or n < 128");
+    if (int rc = need_flow(ctx)) return rc;
+    if (int rc = set_device(ctx)) return rc;
+    FlowState &S = *ctx->flow;
+    if (int rc = ensure_train(ctx, n)) return rc;
+    Arg au, ac, al, af, ap;
+    if (int rc = resolve(ctx, u, sizeof(float) * S.D * n, 0, true, au)) return rc;
+    if (int rc = resolve(ctx, ch, sizeof(int32_t) * n, 1, true, ac)) return rc;
+    if (int rc = resolve(ctx, logf, sizeof(float) * n, 2, true, al)) return rc;
+    if (int rc = resolve(ctx, feat, sizeof(float) * S.F * n, 3, true, af)) return rc;
+    if (int rc = resolve(ctx, logprior, sizeof(float) * S.nch * n, 4, true, ap)) return rc;
+    const unsigned g = static_cast<unsigned>((n * std::max(S.D, std::max(S.F, S.nch)) + 255) / 256);
+    k_transpose_f<<<g, 256, 0, ctx->stream>>>(static_cast<const float *>(au.dev), S.X.as<float>(), n, S.D, 1);
+    LAUNCHED();
+    k_transpose_f<<<g, 256, 0, ctx->stream>>>(static_cast<const float *>(af.dev), S.feat.as<float>(), n, S.F, 1);
+    LAUNCHED();
+    k_transpose_f<<<g, 256, 0, ctx->stream>>>(static_cast<const float *>(ap.dev), S.logprior.as<float>(), n, S.nch, 1);
+    LAUNCHED();
+    CK(cudaMemcpyAsync(S.chb.p, ac.dev, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(S.logf.p, al.dev, sizeof(float) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+    if (int rc = train_pass(ctx, n, 0.f, 0)) return rc;
+    if (int rc = check_err(ctx)) return rc;
+    if (loss) CK(cudaMemcpy(loss, S.loss_dev.p, sizeof(double), cudaMemcpyDeviceToHost));
+    if (grad) {
+        Arg ag;
+        if (int rc = resolve(ctx, grad, sizeof(float) * S.np, 5, false, ag)) return rc;
+        CK(cudaMemcpyAsync(ag.dev, S.grad.p, sizeof(float) * S.np, cudaMemcpyDeviceToDevice, ctx->stream));
+        if (int rc = finish_out(ctx, ag)) return rc;
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    return CHILI_OK;
+}
+
+int chili_gpu_flow_train(chili_ctx *ctx, int steps, uint64_t seed, uint64_t counter_base, double *loss) {
+    if (!ctx || steps < 0 || steps > 4096) return fail(ctx, CHILI_ERR_INVALID_ARG, "steps in [0, 4096]");
+    if (int rc = need_flow(ctx)) return rc;
+    if (int rc = set_device(ctx)) return rc;
+    FlowState &S = *ctx->flow;
+    const long long n = S.batch;
+    if (int rc = ensure_train(ctx, n)) return rc;
+    if (!S.have_scale) {
+        // F scale: mean of F over one batch of the plain proposal
+        BatchArgs b = batch_args(ctx, n, seed, counter_base);
+        b.fval = S.fval.as<double>();
+        k_flow_batch<<<static_cast<unsigned>((n + 127) / 128), 128, 0, ctx->stream>>>(b);
+        LAUNCHED();
+        k_sum_pos<<<1, 256, 0, ctx->stream>>>(S.fval.as<double>(), n, S.scal.as<double>());
+        LAUNCHED();
+        double sc[2];
+        CK(cudaMemcpyAsync(sc, S.scal.p, sizeof(sc), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        const double mean = sc[0] / static_cast<double>(n);
+        S.log_fscale = (mean > 0 && std::isfinite(mean)) ? std::log(mean) : 0.0;
+        S.have_scale = true;
+    }
+    for (int s = 0; s < steps; ++s) {
+        BatchArgs b = batch_args(ctx, n, seed, counter_base + static_cast<uint64_t>(s) * n);
+        k_flow_batch<<<static_cast<unsigned>((n + 127) / 128), 128, 0, ctx->stream>>>(b);
+        LAUNCHED();
+        if (int rc = train_pass(ctx, n, S.lr, s)) return rc;
+    }
+    if (int rc = check_err(ctx)) return rc;
+    if (loss && steps > 0) {
+        Arg o;
+        if (int rc = resolve(ctx, loss, sizeof(double) * steps, 0, false, o)) return rc;
+        CK(cudaMemcpyAsync(o.dev, S.loss_dev.p, sizeof(double) * steps, cudaMemcpyDeviceToDevice, ctx->stream));
+        if (int rc = finish_out(ctx, o)) return rc;
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    return CHILI_OK;
+}
+
+int chili_gpu_flow_iterate(chili_ctx *ctx, uint64_t ncalls, uint64_t seed, uint64_t counter_base, int adapt_beta,
+                           chili_stats *stats_out, chili_flow_iter_info *info) {
+    if (!ctx || ncalls < 1 || ncalls > (1ull << 40)) return fail(ctx, CHILI_ERR_INVALID_ARG, "ncalls in [1, 2^40]");
+    if (int rc = need_flow(ctx)) return rc;
+    if (int rc = set_device(ctx)) return rc;
+    FlowState &S = *ctx->flow;
+    const int width = kPhysFixed + 2 * S.nch;
+    const long long chunk = std::min<long long>(kSampleChunk, static_cast<long long>(ncalls));
+    const unsigned blocks = static_cast<unsigned>((chunk + kPhysBlock - 1) / kPhysBlock);
+    const size_t xs = static_cast<size_t>(S.D) * chunk;
+    CK(S.sch.ensure(sizeof(int32_t) * chunk));
+    CK(S.slq.ensure(sizeof(float) * chunk));
+    CK(S.spart.ensure(sizeof(double) * blocks * width));
+    CK(S.sfold.ensure(sizeof(double) * width));
+    CK(S.sz.ensure(sizeof(float) * xs));
+    CK(S.su.ensure(sizeof(float) * xs));
+    std::vector<double> tot(width, 0.0), fold(width);
+    for (uint64_t done = 0; done < ncalls;) {
+        const long long m = std::min<long long>(chunk, static_cast<long long>(ncalls - done));
+        k_flow_draw<<<static_cast<unsigned>((m + 255) / 256), 256, 0, ctx->stream>>>(
+            S.cp.as<double>(), S.nch, S.D, seed, counter_base + done, m, S.sz.as<float>(), S.sch.as<int32_t>(),
+            S.slq.as<float>());
+        LAUNCHED();
+        if (int rc = flow_pass(ctx, S.sz.as<float>(), S.sch.as<int32_t>(), m, 1, S.su.as<float>(), S.slq.as<float>()))
+            return rc;
+        PhysArgs a{};
+        a.progs = ctx->progs.as<ChannelProgram>();
+        a.pp = ctx->point_prog.as<PointProgram>();
+        a.grids = ctx->edges.as<double>();
+        a.logbeta = S.logbeta.as<float>();
+        a.beta = S.beta.as<float>();
+        a.f = ctx->f_dev.as<IntegrandDesc>();
+        a.nch = S.nch;
+        a.dims = S.D;
+        a.bins = ctx->bins;
+        a.n = m;
+        a.u = S.su.as<float>();
+        a.ch = S.sch.as<int32_t>();
+        a.logq = S.slq.as<float>();
+        a.w = S.prm.as<float>() + S.off_alpha;
+        a.L = S.AL;
+        a.part = S.spart.as<double>();
+        const unsigned nbk = static_cast<unsigned>((m + kPhysBlock - 1) / kPhysBlock);
+        if (int rc = flow_launch_phys(ctx, a, nbk)) return rc;
+        k_flow_fold<<<1, 256, 0, ctx->stream>>>(S.spart.as<double>(), static_cast<int>(nbk), width,
+                                                S.sfold.as<double>());
+        LAUNCHED();
+        CK(cudaMemcpyAsync(fold.data(), S.sfold.p, sizeof(double) * width, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        for (int q = 0; q < width; ++q) tot[q] = q == 3 ? std::max(tot[q], fold[q]) : tot[q] + fold[q];
+        done += static_cast<uint64_t>(m);
+    }
+    if (int rc = check_err(ctx)) return rc;
+    if (stats_out) {
+        stats_out->n = tot[0];
+        stats_out->min = 0;
+        stats_out->max = tot[3];
+        stats_out->sum = tot[1];
+        stats_out->sum2 = tot[2];
+        stats_out->n_finite = tot[4];
+    }
+    if (info) {
+        info->points = static_cast<uint64_t>(tot[0]);
+        info->nonzero = static_cast<uint64_t>(tot[4]);
+        info->nonfinite = static_cast<uint64_t>(tot[5]);
+        info->weight_max = tot[3];
+        info->unweighting_efficiency = tot[3] > 0 ? (tot[1] / tot[0]) / tot[3] : 0.0;
+    }
+    if (adapt_beta) {
+        std::vector<double> nb(S.nch);
+        double mx = 0;
+        for (int c = 0; c < S.nch; ++c) {
+            const double nc = tot[kPhysFixed + c], t2 = tot[kPhysFixed + S.nch + c];
+            nb[c] = nc > 0 ? std::sqrt(t2 / nc) : 0.0;
+            mx = std::max(mx, nb[c]);
+        }
+        if (mx > 0) {
+            for (int c = 0; c < S.nch; ++c) nb[c] = std::max(nb[c], 1e-4 * mx);
+            S.beta_host = nb;
+            if (int rc = upload_beta(ctx)) return rc;
+        }
+    }
+    return CHILI_OK;
+}
+
+int chili_gpu_tc_selftest(chili_ctx *ctx, int mode, int K, int N, const float *A, const float *B, float *C) {
+    if (!ctx || !A || !B || !C) return fail(ctx, CHILI_ERR_INVALID_ARG, "null argument");
+    if (mode < 0 || mode > 2 || K < 16 || K > 256 || K % 16 || N < 16 || N > 256 || N % 16)
+        return fail(ctx, CHILI_ERR_INVALID_ARG, "mode 0..2, K and N multiples of 16 in [16, 256]");
+    if (int rc = set_device(ctx)) return rc;
+    const size_t na = 128 * static_cast<size_t>(K), nbb = static_cast<size_t>(N) * K, nc = 128 * static_cast<size_t>(N);
+    DevBuf &da = ctx->stage[0], &db = ctx->stage[1], &dc = ctx->stage[2], &de = ctx->stage[3];
+    CK(da.ensure(sizeof(float) * na));
+    CK(db.ensure(sizeof(float) * nbb));
+    CK(dc.ensure(sizeof(float) * nc));
+    CK(de.ensure(sizeof(int)));
+    CK(cudaMemcpyAsync(da.p, A, sizeof(float) * na, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(db.p, B, sizeof(float) * nbb, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemsetAsync(de.p, 0, sizeof(int), ctx->stream));
+    CK(cudaFuncSetAttribute(k_tc_selftest, cudaFuncAttributeMaxDynamicSharedMemorySize, kSelftestSmem));
+    k_tc_selftest<<<1, 128, kSelftestSmem, ctx->stream>>>(mode, K, N, da.as<float>(), db.as<float>(), dc.as<float>(),
+                                                          de.as<int>());
+    LAUNCHED();
+    int e = 0;
+    CK(cudaMemcpyAsync(C, dc.p, sizeof(float) * nc, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&e, de.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (e) return fail(ctx, CHILI_ERR_TIMEOUT, "tensor-core self test: wait gave up");
+    return CHILI_OK;
+}
+
+}  // extern "C"

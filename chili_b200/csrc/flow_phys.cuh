@@ -1,0 +1,511 @@
+// flow_phys.cuh -- the FP64 phase-space side of the learned proposal and its
+// channel-weight network.
+//
+// Estimator (multi-channel importance sampling with point-dependent channel
+// weights, Heimel et al., "MadNIS", SciPost Phys. 15 (2023) 141): channel c is
+// drawn with probability beta_c, u from the channel's flow q_c, x = VEGAS_c(u)
+// (Jacobian J), p = FSMapper_c(x); the point's value is
+//     v = alpha_c(p) f(p) dens_c(p) J / (beta_c q_c(u)),
+// dens_c the reference's FSMapper weight of channel c at p (Channel.cc:40-61).
+// For any alpha(p) >= 0 with sum_c alpha_c(p) = 1, E[v] is the integral.
+//
+// alpha(p) = softmax(MLP(phi(p)) + log prior(p)): phi = log pair invariants
+// log(s_ij/S) and log(|t_1j|/S) of the outgoing legs, scaled to ~[-1, 1];
+// prior_c = beta_c * prod over c's massive decays of m^2 G^2 / ((s - m^2)^2 +
+// m^2 G^2) (a peak-normalised Breit-Wigner of the decaying current).
+#pragma once
+
+#include "flow.cuh"
+#include "mc_device.cuh"
+
+namespace chili_flow {
+
+using namespace chili_dev;
+
+constexpr int kAH = 64;        // hidden units of the channel-weight network
+constexpr int kMaxFeat = 32;
+constexpr int kMaxAlphaCh = 64;
+constexpr int kAlphaBlock = 64;
+
+// Offsets of the channel-weight network's parameters in its flat f32 block.
+struct AlphaLayout {
+    int F, nch;
+    int a1, c1, a2, c2, a3, c3, total;
+};
+
+__host__ __device__ inline AlphaLayout alpha_layout(int F, int nch) {
+    AlphaLayout L;
+    L.F = F;
+    L.nch = nch;
+    L.a1 = 0;
+    L.c1 = L.a1 + kAH * F;
+    L.a2 = L.c1 + kAH;
+    L.c2 = L.a2 + kAH * kAH;
+    L.a3 = L.c2 + kAH;
+    L.c3 = L.a3 + nch * kAH;
+    L.total = L.c3 + nch;
+    return L;
+}
+
+__host__ __device__ inline int n_features(int n_ext) {
+    const int n_out = n_ext - 2;
+    return n_out * (n_out - 1) / 2 + n_out;
+}
+
+// Features and log prior of one point (momenta mom[0..n_ext), nodes rebuilt
+// from the PointProgram).
+__device__ __forceinline__ void point_features(const PointProgram *__restrict__ pp, const V4 *mom,
+                                               const float *__restrict__ logbeta, float *feat, float *logprior) {
+    const int n_ext = pp->n_ext;
+    const double S = pp->sqrts * pp->sqrts;
+    int f = 0;
+    for (int i = 2; i < n_ext; ++i)
+        for (int j = i + 1; j < n_ext; ++j) {
+            const double s = mass2(mom[i] + mom[j]) / S;
+            feat[f++] = static_cast<float>(log(fmax(s, 1e-12)) / 8.0 + 1.0);
+        }
+    for (int j = 2; j < n_ext; ++j) {
+        const double tt = fabs(mass2(mom[0] + mom[j])) / S;
+        feat[f++] = static_cast<float>(log(fmax(tt, 1e-12)) / 8.0 + 1.0);
+    }
+    V4 node[PP_MAX_NODES];
+    for (int i = 0; i < pp->n_nodes; ++i) node[i] = i < n_ext ? mom[i] : node[pp->node_a[i]] + node[pp->node_b[i]];
+    for (int c = 0; c < pp->nch; ++c) {
+        double lp = 0;
+        const PPChannel &C = pp->ch[c];
+        for (int q = 0; q < C.n_dec; ++q) {
+            const int d = C.dw[q];
+            if (pp->dw_massless[d]) continue;
+            const double m = pp->dw_mass[d], g = pp->dw_width[d];
+            const double mw2 = m * m * g * g;
+            const double ds = mass2(node[pp->dw_node[d]]) - m * m;
+            lp += log(mw2 / (ds * ds + mw2));
+        }
+        logprior[c] = logbeta[c] + static_cast<float>(lp);
+    }
+}
+
+// Channel-weight network forward for one point: the logits of every channel
+// and their log-sum-exp.
+template <int NCH, int NF>
+__device__ __forceinline__ void alpha_forward(const float *__restrict__ w, const AlphaLayout &L, const float (&feat)[NF],
+                                              const float *logprior, float (&a1)[kAH], float (&a2)[kAH],
+                                              float (&lg)[NCH], float &lse) {
+#pragma unroll 4
+    for (int i = 0; i < kAH; ++i) {
+        float s = w[L.c1 + i];
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+            if (f < L.F) s += w[L.a1 + i * L.F + f] * feat[f];
+        a1[i] = lrelu(s);
+    }
+#pragma unroll 4
+    for (int j = 0; j < kAH; ++j) {
+        float s = w[L.c2 + j];
+#pragma unroll
+        for (int i = 0; i < kAH; ++i) s += w[L.a2 + j * kAH + i] * a1[i];
+        a2[j] = lrelu(s);
+    }
+    float mx = -INFINITY;
+#pragma unroll
+    for (int k = 0; k < NCH; ++k) {
+        float s = -INFINITY;
+        if (k < L.nch) {
+            s = w[L.c3 + k] + logprior[k];
+#pragma unroll
+            for (int j = 0; j < kAH; ++j) s += w[L.a3 + k * kAH + j] * a2[j];
+        }
+        lg[k] = s;
+        mx = fmaxf(mx, s);
+    }
+    float se = 0.f;
+#pragma unroll
+    for (int k = 0; k < NCH; ++k)
+        if (k < L.nch) se += expf(lg[k] - mx);
+    lse = mx + logf(se);
+}
+
+// Channel-weight network: forward, variance-loss terms, backward, weight
+// gradients (this block's partial), for one training batch. Also writes
+// d loss / d log q for the flow's backward pass.
+//   l_i = alpha_c^2 F^2 / (beta_c^2 q)  (F = f dens J / F_scale), loss = mean l_i
+struct AlphaTrainArgs {
+    long long n;
+    AlphaLayout L;
+    const float *w;         // parameters (flat)
+    const float *feat;      // [F][n]
+    const float *logprior;  // [nch][n]
+    const int32_t *ch;
+    const float *logf;      // [n], -inf for a zero / invalid point
+    const float *logbeta;   // [nch]
+    const float *logq;      // [n]
+    float *glogq;           // [n]
+    float *part;            // [gridDim.x][L.total]
+    double *loss_part;      // [gridDim.x]
+};
+
+template <int NCH, int NF>
+__global__ void __launch_bounds__(kAlphaBlock) k_alpha_train(AlphaTrainArgs a) {
+    constexpr int R = kAlphaBlock, LD = kAH + 1, LF = NF + 1, LC = NCH + 1;
+    extern __shared__ float sa[];
+    const AlphaLayout L = a.L;
+    float *w = sa;                        // L.total
+    float *s_a1 = w + ((L.total + 3) & ~3);
+    float *s_a2 = s_a1 + R * LD;
+    float *s_g1 = s_a2 + R * LD;
+    float *s_g2 = s_g1 + R * LD;
+    float *s_gl = s_g2 + R * LD;          // [R][NCH+1]
+    float *s_f = s_gl + R * LC;           // [R][NF+1]
+    const int t = threadIdx.x;
+    for (int i = t; i < L.total; i += R) w[i] = a.w[i];
+    __syncthreads();
+    float acc2[kAH], acc3[NCH], acc1[NF];
+#pragma unroll
+    for (int i = 0; i < kAH; ++i) acc2[i] = 0.f;
+#pragma unroll
+    for (int k = 0; k < NCH; ++k) acc3[k] = 0.f;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) acc1[f] = 0.f;
+    float gc1 = 0.f, gc2 = 0.f, gc3 = 0.f;
+    double lsum = 0.0;
+    const long long ntiles = (a.n + R - 1) / R;
+    const float invn = 1.f / static_cast<float>(a.n);
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long long row = tile * R + t;
+        const bool valid = row < a.n;
+        float lg[NCH], lse;
+        {
+            float feat[NF], lp[NCH];
+#pragma unroll
+            for (int f = 0; f < NF; ++f) feat[f] = (valid && f < L.F) ? a.feat[f * a.n + row] : 0.f;
+#pragma unroll
+            for (int k = 0; k < NCH; ++k) lp[k] = (valid && k < L.nch) ? a.logprior[k * a.n + row] : 0.f;
+            float a1[kAH], a2[kAH];
+            alpha_forward<NCH, NF>(w, L, feat, lp, a1, a2, lg, lse);
+#pragma unroll
+            for (int i = 0; i < kAH; ++i) {
+                s_a1[t * LD + i] = a1[i];
+                s_a2[t * LD + i] = a2[i];
+            }
+#pragma unroll
+            for (int f = 0; f < NF; ++f) s_f[t * LF + f] = feat[f];
+        }
+        const int c = valid ? a.ch[row] : 0;
+        float lac = lg[0];
+#pragma unroll
+        for (int k = 1; k < NCH; ++k)
+            if (k == c) lac = lg[k];
+        lac -= lse;
+        float ell = 0.f;
+        if (valid) {
+            const float e = 2.f * lac + 2.f * a.logf[row] - 2.f * a.logbeta[c] - a.logq[row];
+            ell = isfinite(e) ? expf(e) : 0.f;
+            if (!isfinite(ell)) ell = 0.f;
+            a.glogq[row] = -ell * invn;
+        }
+        lsum += ell;
+        const float gsel = 2.f * ell * invn;
+        // g_logits = gsel (delta_kc - alpha_k)
+#pragma unroll
+        for (int k = 0; k < NCH; ++k) {
+            const float al = k < L.nch ? expf(lg[k] - lse) : 0.f;
+            lg[k] = gsel * ((k == c ? 1.f : 0.f) - al);
+            s_gl[t * LC + k] = lg[k];
+        }
+#pragma unroll 4
+        for (int j = 0; j < kAH; ++j) {
+            float sg = 0.f;
+#pragma unroll
+            for (int k = 0; k < NCH; ++k)
+                if (k < L.nch) sg += w[L.a3 + k * kAH + j] * lg[k];
+            s_g2[t * LD + j] = sg * (s_a2[t * LD + j] > 0.f ? 1.f : kSlope);
+        }
+#pragma unroll 4
+        for (int i = 0; i < kAH; ++i) {
+            float sg = 0.f;
+#pragma unroll 8
+            for (int j = 0; j < kAH; ++j) sg += w[L.a2 + j * kAH + i] * s_g2[t * LD + j];
+            s_g1[t * LD + i] = sg * (s_a1[t * LD + i] > 0.f ? 1.f : kSlope);
+        }
+        __syncthreads();
+        // thread t owns row t of dA2, column t of dA3, row t of dA1
+        for (int r = 0; r < R; ++r) {
+            const float gr2 = s_g2[r * LD + t], gr1 = s_g1[r * LD + t], ar2 = s_a2[r * LD + t];
+#pragma unroll
+            for (int i = 0; i < kAH; ++i) acc2[i] += gr2 * s_a1[r * LD + i];
+#pragma unroll
+            for (int k = 0; k < NCH; ++k) acc3[k] += s_gl[r * LC + k] * ar2;
+#pragma unroll
+            for (int f = 0; f < NF; ++f) acc1[f] += gr1 * s_f[r * LF + f];
+            gc1 += gr1;
+            gc2 += gr2;
+            if (t < NCH) gc3 += s_gl[r * LC + t];
+        }
+        __syncthreads();
+    }
+    float *out = a.part + static_cast<long long>(blockIdx.x) * L.total;
+#pragma unroll
+    for (int i = 0; i < kAH; ++i) out[L.a2 + t * kAH + i] = acc2[i];
+#pragma unroll
+    for (int k = 0; k < NCH; ++k)
+        if (k < L.nch) out[L.a3 + k * kAH + t] = acc3[k];
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+        if (f < L.F) out[L.a1 + t * L.F + f] = acc1[f];
+    out[L.c1 + t] = gc1;
+    out[L.c2 + t] = gc2;
+    if (t < L.nch) out[L.c3 + t] = gc3;
+    // loss partial
+    __shared__ double red[kAlphaBlock];
+    red[t] = lsum;
+    __syncthreads();
+    if (t == 0) {
+        double sl = 0;
+        for (int i = 0; i < R; ++i) sl += red[i];
+        a.loss_part[blockIdx.x] = sl;
+    }
+}
+
+template <int NCH, int NF>
+constexpr size_t alpha_train_smem(int total) {
+    return sizeof(float) * (((total + 3) & ~3) + 4 * kAlphaBlock * (kAH + 1) + kAlphaBlock * (NCH + 1) +
+                            kAlphaBlock * (NF + 1));
+}
+
+#ifndef CHILI_FLOW_LAYERS_ONLY
+// Training batch from the plain multichannel proposal: channel c with
+// probability beta (table cp), u uniform, x = VEGAS_c(u), p = FSMapper_c(x).
+struct BatchArgs {
+    const ChannelProgram *progs;
+    const PointProgram *pp;
+    const double *grids;
+    const double *cp;
+    const float *logbeta;
+    const IntegrandDesc *f;
+    int nch, dims, bins;
+    uint64_t seed, ctr0;
+    long long n;
+    double log_fscale;
+    float *u;          // [D][n]
+    int32_t *ch;
+    float *logf;       // [n]
+    double *fval;      // [n] F = f dens J (for the scale), or null
+    float *feat;       // [F][n]
+    float *logprior;   // [nch][n]
+};
+
+__global__ void __launch_bounds__(128) k_flow_batch(BatchArgs a) {
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i >= a.n) return;
+    const int D = a.dims;
+    double r[CHILI_MAX_DIMS + 1];
+    load_uniforms(a.seed, a.ctr0 + i, nullptr, D + 1, r);
+    const int c = select_channel(a.cp, a.nch, r[D]);
+    for (int d = 0; d < D; ++d) a.u[d * a.n + i] = static_cast<float>(r[d]);
+    a.ch[i] = c;
+    double Fv = 0;
+    V4 mom[CHILI_MAX_SLOTS];
+    double m2[CHILI_MAX_SLOTS];
+    double jac = 0;
+    bool okp = grid_map_checked(a.grids + static_cast<size_t>(c) * D * (a.bins + 1), D, a.bins, r, jac);
+    if (okp) {
+        fs_generate(a.progs + c, r, mom, m2);
+        okp = preprocess(a.f, mom);
+    }
+    float feat[kMaxFeat], lp[kMaxAlphaCh];
+    if (okp) {
+        double xx[CHILI_MAX_DIMS];
+        const double dens = fs_weight(a.progs + c, mom, xx);
+        Fv = dens == 0 ? 0 : eval_momenta(a.f, mom, a.progs[c].n_ext) * dens * jac;
+        if (!(Fv > 0) || !isfinite(Fv)) Fv = 0;
+        point_features(a.pp, mom, a.logbeta, feat, lp);
+    } else {
+        for (int q = 0; q < kMaxFeat; ++q) feat[q] = 0.f;
+        for (int q = 0; q < a.nch; ++q) lp[q] = a.logbeta[q];
+    }
+    if (a.fval) a.fval[i] = Fv;
+    a.logf[i] = Fv > 0 ? static_cast<float>(log(Fv) - a.log_fscale) : -INFINITY;
+    const int F = n_features(a.pp->n_ext);
+    for (int q = 0; q < F; ++q) a.feat[q * a.n + i] = feat[q];
+    for (int q = 0; q < a.nch; ++q) a.logprior[q * a.n + i] = lp[q];
+}
+
+// Flow-path sampling, step 1: channel c ~ beta, z uniform in [0,1)^D
+// (the flow's base point), log q = 0.
+__global__ void k_flow_draw(const double *__restrict__ cp, int nch, int dims, uint64_t seed, uint64_t ctr0,
+                            long long n, float *__restrict__ z, int32_t *__restrict__ ch, float *__restrict__ logq) {
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    double r[CHILI_MAX_DIMS + 1];
+    load_uniforms(seed, ctr0 + i, nullptr, dims + 1, r);
+    ch[i] = select_channel(cp, nch, r[dims]);
+    for (int d = 0; d < dims; ++d) z[d * n + i] = fminf(static_cast<float>(r[d]), 0.99999994f);
+    logq[i] = 0.f;
+}
+
+#endif  // CHILI_FLOW_LAYERS_ONLY
+
+// Flow-path sampling, step 2 (after the inverse flow): the phase-space
+// point, its value v and this block's StatsData partial.
+// part per block: [n, sum, sum2, max, n_nonzero, n_nonfinite] + per channel [n_c, sum T_c^2]
+constexpr int kPhysBlock = 128;
+constexpr int kPhysFixed = 6;
+
+struct PhysArgs {
+    const ChannelProgram *progs;
+    const PointProgram *pp;
+    const double *grids;
+    const float *logbeta;
+    const float *beta;
+    const IntegrandDesc *f;
+    int nch, dims, bins;
+    long long n;
+    const float *u;      // [D][n]
+    const int32_t *ch;
+    const float *logq;
+    const float *w;      // channel-weight network parameters
+    AlphaLayout L;
+    double *part;        // [gridDim.x][kPhysFixed + 2 nch]
+    double *vout;        // [n] or null
+    double *mom_out;     // [n][n_ext][4] or null
+};
+
+template <int NCH, int NF>
+__global__ void __launch_bounds__(kPhysBlock) k_flow_phys(PhysArgs a) {
+    extern __shared__ double sp[];
+    double *s_ch = sp;                                                // [2 nch]
+    float *w = reinterpret_cast<float *>(sp + 2 * kMaxAlphaCh);      // network
+    const int t = threadIdx.x;
+    for (int q = t; q < 2 * a.nch; q += blockDim.x) s_ch[q] = 0;
+    for (int q = t; q < a.L.total; q += blockDim.x) w[q] = a.w[q];
+    __syncthreads();
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + t;
+    double v = 0;
+    bool nan_v = false;
+    if (i < a.n) {
+        const int D = a.dims;
+        const int c = a.ch[i];
+        double r[CHILI_MAX_DIMS];
+        for (int d = 0; d < D; ++d) r[d] = fmin(static_cast<double>(a.u[d * a.n + i]), 0.99999999999999989);
+        double jac = 0;
+        V4 mom[CHILI_MAX_SLOTS];
+        double m2[CHILI_MAX_SLOTS];
+        bool okp = grid_map_checked(a.grids + static_cast<size_t>(c) * D * (a.bins + 1), D, a.bins, r, jac);
+        if (okp) {
+            fs_generate(a.progs + c, r, mom, m2);
+            okp = preprocess(a.f, mom);
+        }
+        if (okp) {
+            double xx[CHILI_MAX_DIMS];
+            const double dens = fs_weight(a.progs + c, mom, xx);
+            double Fv = dens == 0 ? 0 : eval_momenta(a.f, mom, a.progs[c].n_ext) * dens * jac;
+            if (!(Fv > 0) || !isfinite(Fv)) Fv = 0;
+            if (Fv > 0) {
+                float featv[kMaxFeat], lp[kMaxAlphaCh];
+                point_features(a.pp, mom, a.logbeta, featv, lp);
+                float feat[NF];
+#pragma unroll
+                for (int q = 0; q < NF; ++q) feat[q] = featv[q];
+                float a1[kAH], a2[kAH], lg[NCH], lse;
+                alpha_forward<NCH, NF>(w, a.L, feat, lp, a1, a2, lg, lse);
+                float lac = lg[0];
+#pragma unroll
+                for (int k = 1; k < NCH; ++k)
+                    if (k == c) lac = lg[k];
+                lac -= lse;
+                v = exp(static_cast<double>(lac - a.logbeta[c] - a.logq[i])) * Fv;
+                if (!isfinite(v)) {
+                    nan_v = true;
+                    v = 0;
+                }
+            }
+            if (a.mom_out)
+                for (int s = 0; s < a.progs[c].n_ext; ++s) {
+                    double *o = a.mom_out + (i * a.progs[c].n_ext + s) * 4;
+                    o[0] = mom[s].e; o[1] = mom[s].x; o[2] = mom[s].y; o[3] = mom[s].z;
+                }
+        }
+        if (a.vout) a.vout[i] = v;
+        const double T = v * static_cast<double>(a.beta[c]);
+        atomicAdd(s_ch + c, 1.0);
+        atomicAdd(s_ch + a.nch + c, T * T);
+    }
+    // block reduction of n, sum, sum2, max, nonzero, nonfinite
+    const double cnt = i < a.n ? 1.0 : 0.0;
+    double q0 = cnt, q1 = v, q2 = v * v, q3 = v, q4 = v != 0 ? 1.0 : 0.0, q5 = nan_v ? 1.0 : 0.0;
+    q0 = warp_sum(q0); q1 = warp_sum(q1); q2 = warp_sum(q2); q3 = warp_max(q3); q4 = warp_sum(q4); q5 = warp_sum(q5);
+    __shared__ double red[kPhysBlock / 32][kPhysFixed];
+    if ((t & 31) == 0) {
+        red[t >> 5][0] = q0; red[t >> 5][1] = q1; red[t >> 5][2] = q2;
+        red[t >> 5][3] = q3; red[t >> 5][4] = q4; red[t >> 5][5] = q5;
+    }
+    __syncthreads();
+    double *out = a.part + static_cast<long long>(blockIdx.x) * (kPhysFixed + 2 * a.nch);
+    if (t < kPhysFixed) {
+        double sr = 0.0;
+        for (int wq = 0; wq < kPhysBlock / 32; ++wq) sr = t == 3 ? fmax(sr, red[wq][3]) : sr + red[wq][t];
+        out[t] = sr;
+    }
+    for (int q = t; q < 2 * a.nch; q += blockDim.x) out[kPhysFixed + q] = s_ch[q];
+}
+
+#ifndef CHILI_FLOW_LAYERS_ONLY
+// Ordered fold of the block partials: out[0..5] = n, sum, sum2, max,
+// nonzero, nonfinite; out[6..] = per channel n_c, sum T_c^2.
+__global__ void k_flow_fold(const double *__restrict__ part, int nblocks, int width, double *__restrict__ out) {
+    const int q = threadIdx.x + blockIdx.x * blockDim.x;
+    if (q >= width) return;
+    double s = 0;
+    for (int b = 0; b < nblocks; ++b) {
+        const double v = part[static_cast<long long>(b) * width + q];
+        s = q == 3 ? fmax(s, v) : s + v;
+    }
+    out[q] = s;
+}
+
+// Ordered sum of the loss partials.
+__global__ void k_loss_fold(const double *__restrict__ part, int nblocks, double scale, double *__restrict__ out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double s = 0;
+    for (int b = 0; b < nblocks; ++b) s += part[b];
+    *out = s * scale;
+}
+
+// Sum and count of positive values of a double array (one block).
+__global__ void k_sum_pos(const double *__restrict__ v, long long n, double *__restrict__ out) {
+    __shared__ double red[256];
+    double s = 0, c = 0;
+    for (long long i = threadIdx.x; i < n; i += 256) {
+        s += v[i];
+        c += v[i] > 0 ? 1.0 : 0.0;
+    }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0;
+        for (int k = 0; k < 256; ++k) tot += red[k];
+        out[0] = tot;
+    }
+    __syncthreads();
+    red[threadIdx.x] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0;
+        for (int k = 0; k < 256; ++k) tot += red[k];
+        out[1] = tot;
+    }
+}
+
+// [n][D] row-major <-> [D][n]
+__global__ void k_transpose_f(const float *__restrict__ in, float *__restrict__ out, long long n, int D, int to_soa) {
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i >= n * D) return;
+    const long long r = i / D;
+    const int d = static_cast<int>(i % D);
+    if (to_soa) out[d * n + r] = in[i];
+    else out[i] = in[d * n + r];
+}
+
+#endif  // CHILI_FLOW_LAYERS_ONLY
+
+}  // namespace chili_flow

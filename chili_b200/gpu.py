@@ -61,6 +61,18 @@ def _declare(lib):
         "chili_gpu_get_training": ([vp, vp, vp], i32),
         "chili_gpu_generate": ([vp, i64, u64, u64, vp, vp, vp], i32),
         "chili_gpu_evaluate_batch": ([vp, i32, vp, vp, i64], i32),
+        "chili_gpu_flow_init": ([vp, P(abi.FlowParams)], i32),
+        "chili_gpu_flow_nparams": ([vp], i64),
+        "chili_gpu_flow_get_params": ([vp, vp], i32),
+        "chili_gpu_flow_set_params": ([vp, vp], i32),
+        "chili_gpu_flow_get_beta": ([vp, vp], i32),
+        "chili_gpu_flow_set_beta": ([vp, vp], i32),
+        "chili_gpu_flow_density": ([vp, vp, vp, i64, vp, vp], i32),
+        "chili_gpu_flow_sample_u": ([vp, vp, vp, i64, vp, vp], i32),
+        "chili_gpu_flow_loss_grad": ([vp, vp, vp, vp, vp, vp, i64, P(dbl), vp], i32),
+        "chili_gpu_flow_train": ([vp, i32, u64, u64, vp], i32),
+        "chili_gpu_flow_iterate": ([vp, u64, u64, u64, i32, P(abi.Stats), P(abi.FlowIterInfo)], i32),
+        "chili_gpu_tc_selftest": ([vp, i32, i32, i32, vp, vp, vp], i32),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(lib, name)
@@ -288,6 +300,84 @@ class Context:
         out = np.empty(u.shape[0])
         self.call("chili_gpu_evaluate_batch", ch, _ptr(u), _ptr(out), u.shape[0])
         return out
+
+    # ------------------------------------------------------ learned proposal
+    def flow_init(self, params=None, **kw):
+        p = params or abi.FlowParams.defaults(**kw)
+        self.call("chili_gpu_flow_init", C.byref(p))
+        self.flow_np = int(self.lib.chili_gpu_flow_nparams(self.h))
+        return self.flow_np
+
+    def flow_get_params(self):
+        out = np.empty(self.flow_np, dtype=np.float32)
+        self.call("chili_gpu_flow_get_params", _ptr(out))
+        return out
+
+    def flow_set_params(self, prm):
+        prm = np.ascontiguousarray(prm, dtype=np.float32)
+        assert prm.size == self.flow_np
+        self.call("chili_gpu_flow_set_params", _ptr(prm))
+
+    def flow_get_beta(self):
+        out = np.empty(self.nch)
+        self.call("chili_gpu_flow_get_beta", _ptr(out))
+        return out
+
+    def flow_set_beta(self, beta):
+        self.call("chili_gpu_flow_set_beta", _ptr(_f64(beta)))
+
+    def _flow_map(self, name, x, ch):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        ch = np.ascontiguousarray(ch, dtype=np.int32)
+        out = np.empty_like(x)
+        lq = np.empty(x.shape[0], dtype=np.float32)
+        self.call(name, _ptr(x), _ptr(ch), x.shape[0], _ptr(out), _ptr(lq))
+        return out, lq
+
+    def flow_density(self, u, ch):
+        """u -> z and log q(u) of each point's channel flow."""
+        return self._flow_map("chili_gpu_flow_density", u, ch)
+
+    def flow_sample_u(self, z, ch):
+        """z -> u and log q(u)."""
+        return self._flow_map("chili_gpu_flow_sample_u", z, ch)
+
+    def flow_loss_grad(self, u, ch, logf, feat, logprior):
+        f32 = lambda a: np.ascontiguousarray(a, dtype=np.float32)
+        u, feat, logprior, logf = f32(u), f32(feat), f32(logprior), f32(logf)
+        ch = np.ascontiguousarray(ch, dtype=np.int32)
+        loss = C.c_double()
+        grad = np.empty(self.flow_np, dtype=np.float32)
+        self.call("chili_gpu_flow_loss_grad", _ptr(u), _ptr(ch), _ptr(logf), _ptr(feat), _ptr(logprior),
+                  u.shape[0], C.byref(loss), _ptr(grad))
+        return loss.value, grad
+
+    def flow_train(self, steps, seed=7, counter=0):
+        loss = np.empty(max(steps, 1))
+        self.call("chili_gpu_flow_train", int(steps), int(seed), int(counter), _ptr(loss))
+        return loss[:steps]
+
+    def flow_iterate(self, ncalls, seed=7, counter=0, adapt_beta=False):
+        st, info = abi.Stats(), abi.FlowIterInfo()
+        self.call("chili_gpu_flow_iterate", int(ncalls), int(seed), int(counter), 1 if adapt_beta else 0,
+                  C.byref(st), C.byref(info))
+        return st, info
+
+    def tc_selftest(self, mode, A, B, N):
+        A = np.ascontiguousarray(A, dtype=np.float32)
+        B = np.ascontiguousarray(B, dtype=np.float32)
+        K = A.shape[1] if mode != 1 else A.shape[0]
+        out = np.empty((128, N), dtype=np.float32)
+        self.call("chili_gpu_tc_selftest", mode, K, N, _ptr(A), _ptr(B), _ptr(out))
+        return out
+
+
+def flow_layout(dims, nch, n_ext, layers=6):
+    """Offsets of the flat parameter vector of the learned proposal (the
+    layout that include/chili_gpu.h documents): a list of (name, offset,
+    shape) with the oracle's parameter names."""
+    from . import flowspec
+    return flowspec.layout(dims, nch, n_ext, layers)
 
 
 def check_channels(cs):

@@ -328,6 +328,74 @@ int chili_gpu_generate(chili_ctx *ctx, int64_t n, uint64_t seed,
 int chili_gpu_evaluate_batch(chili_ctx *ctx, int ch, const double *u,
                              double *out, int64_t n);
 
+/* ------------------------------------------------ learned proposal */
+/* No counterpart in the reference (Chili has no learned proposal): a
+ * channel-conditioned rational-quadratic spline coupling flow on each
+ * channel's VEGAS uniforms and a softmax channel-weight network, trained
+ * online on the GPU (hand-written forward, backward and Adam kernels; bf16
+ * tensor-core products with f32 accumulation; f32 splines; FP64 phase space).
+ * Estimator per point: v = alpha_c(p) f(p) dens_c(p) J / (beta_c q_c(u)) for
+ * the channel c that generated it (c ~ beta, u ~ q_c, x = VEGAS_c(u),
+ * p = FSMapper_c(x)). Requires channels, grids, integrand and channel weights
+ * to be set; beta starts as the current channel weights.
+ *
+ * Flat parameter layout (f32): per coupling layer l: W1 [128][da_l],
+ * E [nch][128], W2 [128][128], W3 [db_l*49][128]; then the channel-weight
+ * network: A1 [64][F], c1 [64], A2 [64][64], c2 [64], A3 [nch][64], c3 [nch],
+ * F = n_out(n_out-1)/2 + n_out. Layer l transforms db_l <= 5 dimensions
+ * (dims <= 10: alternating, half/half and shifted-pair splits and their
+ * complements in turn; dims > 10: dimensions 5l..5l+4 mod dims). */
+typedef struct {
+    int32_t layers;       /* coupling layers (6) */
+    int32_t batch;        /* points per training step (65536) */
+    double lr;            /* Adam step size (1e-3) */
+    uint64_t init_seed;   /* weight initialisation */
+} chili_flow_params;
+
+typedef struct {
+    uint64_t points;       /* points drawn */
+    uint64_t nonzero;      /* points with v != 0 */
+    uint64_t nonfinite;    /* points whose v was not finite (counted as 0) */
+    double weight_max;     /* max v */
+    double unweighting_efficiency;  /* mean v / max v */
+} chili_flow_iter_info;
+
+int chili_gpu_flow_init(chili_ctx *ctx, const chili_flow_params *params);
+int64_t chili_gpu_flow_nparams(const chili_ctx *ctx);
+/* Flat parameters (layout above). Host or device. */
+int chili_gpu_flow_get_params(chili_ctx *ctx, float *prm);
+int chili_gpu_flow_set_params(chili_ctx *ctx, const float *prm);
+/* Channel-selection probabilities beta [nch] of the flow path. */
+int chili_gpu_flow_get_beta(chili_ctx *ctx, double *beta);
+int chili_gpu_flow_set_beta(chili_ctx *ctx, const double *beta);
+/* Density direction u -> z of the flow of each point's channel, and log q(u);
+ * u, z [n][dims] row-major in [0,1]. Host or device. */
+int chili_gpu_flow_density(chili_ctx *ctx, const float *u, const int32_t *ch, int64_t n, float *z,
+                           float *logq);
+/* Sampling direction z -> u, and log q(u). Host or device. */
+int chili_gpu_flow_sample_u(chili_ctx *ctx, const float *z, const int32_t *ch, int64_t n, float *u,
+                            float *logq);
+/* The variance loss mean_i alpha_c^2 F^2 / (beta_c^2 q) on a given batch
+ * (u [n][dims], ch [n], logf [n] = log F, -inf for F = 0, feat [n][F],
+ * logprior [n][nch]) and its gradient with respect to every parameter
+ * (grad [nparams]); no update. Host or device. */
+int chili_gpu_flow_loss_grad(chili_ctx *ctx, const float *u, const int32_t *ch, const float *logf,
+                             const float *feat, const float *logprior, int64_t n, double *loss, float *grad);
+/* `steps` Adam steps, each on a fresh batch drawn from the plain multichannel
+ * proposal (counters counter_base + step*batch ...); loss[steps] (host or
+ * device, may be NULL) receives each step's loss. */
+int chili_gpu_flow_train(chili_ctx *ctx, int steps, uint64_t seed, uint64_t counter_base, double *loss);
+/* One integration pass of ncalls points through the flow path (counters
+ * counter_base ...); StatsData of v. adapt_beta != 0 sets beta_c proportional
+ * to the root mean square of this pass's per-channel terms beta_c v. */
+int chili_gpu_flow_iterate(chili_ctx *ctx, uint64_t ncalls, uint64_t seed, uint64_t counter_base,
+                           int adapt_beta, chili_stats *stats_out, chili_flow_iter_info *info);
+/* Tensor-core check: C[128][N] from f32 A, B rounded to bf16;
+ * mode 0: C = A B^T (A [128][K], B [N][K]); mode 1: C = A^T B (A [K][128],
+ * B [K][N]); mode 2: C = A B (A [128][K], B [K][N]). K and N multiples of 16
+ * in [16, 256]. Host buffers. */
+int chili_gpu_tc_selftest(chili_ctx *ctx, int mode, int K, int N, const float *A, const float *B, float *C);
+
 #ifdef __cplusplus
 }
 #endif

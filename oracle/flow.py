@@ -51,19 +51,27 @@ def bf16(a):
 
 
 def masks(dims, layers):
-    """Conditioning masks: True = identity (conditioning) dimension. The
-    pattern cycles through alternating, half/half and pairwise splits and
-    their complements, so that every dimension is transformed conditioned on
-    every other one within six layers."""
+    """Conditioning masks: True = identity (conditioning) dimension; every
+    layer transforms at most 5 dimensions (5 * 49 spline parameters fit one
+    256-column tensor-core tile). Up to 10 dimensions the pattern cycles
+    through alternating, half/half and shifted-pair splits and their
+    complements; above 10, layer l transforms dimensions 5l .. 5l+4 (mod D)."""
     idx = np.arange(dims)
-    pats = [idx % 2 == 0, idx % 2 == 1, idx < dims // 2, idx >= dims // 2,
-            (idx // 2) % 2 == 0, (idx // 2) % 2 == 1]
     out = []
-    for l in range(layers):
-        m = pats[l % 6]
-        if m.all() or not m.any():
-            m = idx % 2 == (l % 2)
-        out.append(m)
+    if dims <= 10:
+        pats = [idx % 2 == 0, idx % 2 == 1, idx < dims // 2, idx >= dims // 2,
+                ((idx + 1) // 2) % 2 == 0, ((idx + 1) // 2) % 2 == 1]
+        for l in range(layers):
+            m = pats[l % 6]
+            if m.all() or not m.any():
+                m = idx % 2 == (l % 2)
+            out.append(m)
+    else:
+        for l in range(layers):
+            t = (5 * l + np.arange(5)) % dims
+            m = np.ones(dims, dtype=bool)
+            m[t] = False
+            out.append(m)
     return out
 
 
@@ -268,6 +276,7 @@ def flow_forward(spec, p, u, ch, use_bf16=False):
     cache = []
     for l in range(spec.layers):
         ci, ti = spec.cond[l], spec.trans[l]
+        x = np.clip(x, 0.0, 1.0)
         theta, acts = conditioner(spec, p, l, x[:, ci], ch, use_bf16)
         th = theta.reshape(x.shape[0], len(ti), spec.per_dim)
         y, lj = spline_forward(th, x[:, ti], spec.bins)
@@ -283,6 +292,7 @@ def flow_inverse(spec, p, z, ch, use_bf16=False):
     logq = np.zeros(x.shape[0])
     for l in reversed(range(spec.layers)):
         ci, ti = spec.cond[l], spec.trans[l]
+        x = np.clip(x, 0.0, 1.0)
         theta, _ = conditioner(spec, p, l, x[:, ci], ch, use_bf16)
         th = theta.reshape(x.shape[0], len(ti), spec.per_dim)
         xin, lj = spline_inverse(th, x[:, ti], spec.bins)
@@ -318,7 +328,7 @@ def flow_backward(spec, p, cache, ch, g_logq, use_bf16=False):
         gp1q = bf16(gp1) if use_bf16 else gp1
         grads[f"W1_{l}"] = gp1q.T @ (bf16(a0) if use_bf16 else a0)
         gE = np.zeros((spec.nch, H))
-        np.add.at(gE, ch, gp1)
+        np.add.at(gE, ch, gp1q)
         grads[f"E_{l}"] = gE
         ga0 = _mm(gp1, p[f"W1_{l}"], use_bf16)
         gnew = gx.copy()

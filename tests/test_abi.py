@@ -16,7 +16,7 @@ HEADER = os.path.join(ROOT, "include", "chili_gpu.h")
 
 def declared_functions():
     src = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:int|uint64_t|const char \*)\s*(chili_gpu_\w+)\s*\(", src, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|int64_t|uint64_t|const char \*)\s*(chili_gpu_\w+)\s*\(", src, re.M)))
 
 
 def exported_symbols(path):
@@ -50,6 +50,7 @@ def test_struct_layouts_match_the_header(tmp_path):
 int main(void) {
   S(chili_particle_info) S(chili_decay) S(chili_channel_desc) S(chili_idx_value)
   S(chili_pid_pair_value) S(chili_cuts) S(chili_stats) S(chili_multichannel_params) S(chili_mc_iter_info)
+  S(chili_flow_params) S(chili_flow_iter_info) O(chili_flow_params, init_seed) O(chili_flow_iter_info, unweighting_efficiency)
   O(chili_multichannel_params, should_optimize) O(chili_multichannel_params, grid_alpha)
   O(chili_cuts, etamax) O(chili_mc_iter_info, weight_max) O(chili_mc_iter_info, points_weighted)
   return 0;
@@ -60,7 +61,8 @@ int main(void) {
     mirror = {"chili_particle_info": abi.ParticleInfo, "chili_decay": abi.Decay, "chili_channel_desc": abi.ChannelDesc,
               "chili_idx_value": abi.IdxValue, "chili_pid_pair_value": abi.PidPairValue, "chili_cuts": abi.Cuts,
               "chili_stats": abi.Stats, "chili_multichannel_params": abi.MultiChannelParams,
-              "chili_mc_iter_info": abi.MCIterInfo}
+              "chili_mc_iter_info": abi.MCIterInfo, "chili_flow_params": abi.FlowParams,
+              "chili_flow_iter_info": abi.FlowIterInfo}
     for name, cls in mirror.items():
         assert int(got[name]) == C.sizeof(cls), name
     assert int(got["chili_multichannel_params.should_optimize"]) == abi.MultiChannelParams.should_optimize.offset
@@ -68,6 +70,8 @@ int main(void) {
     assert int(got["chili_cuts.etamax"]) == abi.Cuts.etamax.offset
     assert int(got["chili_mc_iter_info.weight_max"]) == abi.MCIterInfo.weight_max.offset
     assert int(got["chili_mc_iter_info.points_weighted"]) == abi.MCIterInfo.points_weighted.offset
+    assert int(got["chili_flow_params.init_seed"]) == abi.FlowParams.init_seed.offset
+    assert int(got["chili_flow_iter_info.unweighting_efficiency"]) == abi.FlowIterInfo.unweighting_efficiency.offset
 
 
 def test_header_limits_match_the_mirror():
