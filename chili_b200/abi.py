@@ -37,6 +37,7 @@ CHILI_FUNC_PROPAGATOR_TOP2 = 3
 
 CHILI_PRE_ACCEPT_ALL = 0
 CHILI_PRE_FINITE = 1
+CHILI_PRE_CUTS = 2
 
 
 class ParticleInfo(C.Structure):

@@ -43,12 +43,17 @@ void launch_channel(chili_ctx *ctx, long long base, long long T, long long mr, i
         rec_dens);
 }
 
-// The phased weight pass (pipeline.cuh) over the n_pre PreProcess-accepted
-// points of a chunk of m counters, in tiles of at most ctx->pipe_tile points
-// so that a tile's buffers stay in L2.
+}  // namespace
 
-int launch_pipeline(chili_ctx *ctx, long long m, long long n_pre, int bins, bool opt, RoundCtl *ctl_pre,
-                    double *rec_val, double *rec_wgt, uint8_t *rec_ok, int32_t *rec_slot, double *rec_dens) {
+// The phased weight pass (pipeline.cuh) over the n_pre listed points of a
+// momenta buffer of m points (list: their indices, ich: their channels,
+// n_list: the device-side count), in tiles of at most ctx->pipe_tile points
+// so that a tile's buffers stay in L2; `combine` launches the last step of
+// each tile (it reads the per-channel densities ctx->dcv, ctx->vwv and the
+// nodes ctx->node_soa of the tile).
+int pipeline_run(chili_ctx *ctx, const double *mom_soa, long long m, const int32_t *list, const int32_t *ich,
+                 const long long *n_list, long long n_pre, int bins, bool opt, int32_t *rec_slot, double *rec_dens,
+                 const TileFn &combine) {
     const PointProgram &P = ctx->pp_host;
     const PointProgram *pp = ctx->point_prog.as<PointProgram>();
     // gridDim.y (point blocks of 128) stays below 65536
@@ -60,15 +65,12 @@ int launch_pipeline(chili_ctx *ctx, long long m, long long n_pre, int bins, bool
     CK(ctx->dcv.ensure(sizeof(double) * ctx->nch * T));
     CK(ctx->ich_tile.ensure(sizeof(int32_t) * T));
     CK(ctx->vwv.ensure(sizeof(double) * ctx->nch * T));
-    const long long *n_list = reinterpret_cast<const long long *>(
-        reinterpret_cast<const char *>(ctl_pre) + offsetof(RoundCtl, n_acc));
     const unsigned gx = static_cast<unsigned>((T + 255) / 256);
     const int n_items = P.n_tents + P.n_dws + P.n_sws;
     const int o = opt ? 1 : 0;
     for (long long base = 0; base < n_pre; base += T) {
         { KTimer kt_(ctx, KT_NODES);
-        k_pp_nodes<<<gx, 256, 0, ctx->stream>>>(pp, ctx->mom_soa.as<double>(), m, ctx->list.as<int32_t>(),
-                                                 ctx->ich.as<int32_t>(), n_list, base, ctx->node_soa.as<double>(),
+        k_pp_nodes<<<gx, 256, 0, ctx->stream>>>(pp, mom_soa, m, list, ich, n_list, base, ctx->node_soa.as<double>(),
                                                  ctx->ich_tile.as<int32_t>(), T); }
         LAUNCHED();
         if (n_items > 0) {
@@ -96,13 +98,33 @@ int launch_pipeline(chili_ctx *ctx, long long m, long long n_pre, int bins, bool
         default: return fail(ctx, CHILI_ERR_STATE, "no phased weight kernel for this dimension");
         }
         LAUNCHED();
-        { KTimer kt_(ctx, KT_COMBINE);
-        k_pp_combine<<<gx, 256, 0, ctx->stream>>>(pp, alpha_ptr(ctx), ctx->dcv.as<double>(), ctx->vwv.as<double>(),
-                                                   ctx->node_soa.as<double>(), n_list, base, T,
-                                                   ctx->f_dev.as<IntegrandDesc>(), rec_val, rec_wgt, rec_ok); }
-        LAUNCHED();
+        if (int rc = combine(base, T)) return rc;
     }
     return CHILI_OK;
+}
+
+namespace {
+
+// The phased weight pass of a multichannel chunk: records of the n_pre
+// PreProcess-accepted points of the chunk of m counters.
+int launch_pipeline(chili_ctx *ctx, long long m, long long n_pre, int bins, bool opt, RoundCtl *ctl_pre,
+                    double *rec_val, double *rec_wgt, uint8_t *rec_ok, int32_t *rec_slot, double *rec_dens) {
+    const PointProgram *pp = ctx->point_prog.as<PointProgram>();
+    const long long *n_list = reinterpret_cast<const long long *>(
+        reinterpret_cast<const char *>(ctl_pre) + offsetof(RoundCtl, n_acc));
+    return pipeline_run(ctx, ctx->mom_soa.as<double>(), m, ctx->list.as<int32_t>(), ctx->ich.as<int32_t>(), n_list,
+                        n_pre, bins, opt, rec_slot, rec_dens, [&](long long base, long long T) -> int {
+                            const unsigned gx = static_cast<unsigned>((T + 255) / 256);
+                            {
+                                KTimer kt_(ctx, KT_COMBINE);
+                                k_pp_combine<<<gx, 256, 0, ctx->stream>>>(
+                                    pp, alpha_ptr(ctx), ctx->dcv.as<double>(), ctx->vwv.as<double>(),
+                                    ctx->node_soa.as<double>(), n_list, base, T, ctx->f_dev.as<IntegrandDesc>(),
+                                    rec_val, rec_wgt, rec_ok);
+                            }
+                            LAUNCHED();
+                            return CHILI_OK;
+                        });
 }
 
 // Hint tables of the grid set (grid.cuh, find_bin_hinted), rebuilt after
@@ -401,10 +423,30 @@ int chili_gpu_set_integrand(chili_ctx *ctx, int kind, const double *params, int 
 int chili_gpu_set_preprocess(chili_ctx *ctx, int kind) {
     if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
     if (kind != CHILI_PRE_ACCEPT_ALL && kind != CHILI_PRE_FINITE)
-        return fail(ctx, CHILI_ERR_INVALID_ARG, "unknown preprocess kind");
+        return fail(ctx, CHILI_ERR_INVALID_ARG,
+                    kind == CHILI_PRE_CUTS ? "CHILI_PRE_CUTS is set with chili_gpu_set_preprocess_cuts"
+                                           : "unknown preprocess kind");
     int rc;
     if ((rc = set_device(ctx))) return rc;
     ctx->f_host.pre = kind;
+    CK(ctx->f_dev.ensure(sizeof(IntegrandDesc)));
+    CK(cudaMemcpyAsync(ctx->f_dev.p, &ctx->f_host, sizeof(IntegrandDesc), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHILI_OK;
+}
+
+int chili_gpu_set_preprocess_cuts(chili_ctx *ctx, double sqrts, double ptmin, double etamax, double delta_r) {
+    if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
+    if (int rc = need_channels(ctx)) return rc;
+    if (!(sqrts > 0) || !(ptmin >= 0) || !(etamax >= 0) || !(delta_r >= 0))
+        return fail(ctx, CHILI_ERR_INVALID_ARG, "cut values must be >= 0 (sqrts > 0)");
+    if (int rc = set_device(ctx)) return rc;
+    ctx->f_host.pre = CHILI_PRE_CUTS;
+    ctx->f_host.n_ext = ctx->n_ext;
+    ctx->f_host.cut[0] = sqrts;
+    ctx->f_host.cut[1] = ptmin;
+    ctx->f_host.cut[2] = etamax;
+    ctx->f_host.cut[3] = delta_r;
     CK(ctx->f_dev.ensure(sizeof(IntegrandDesc)));
     CK(cudaMemcpyAsync(ctx->f_dev.p, &ctx->f_host, sizeof(IntegrandDesc), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));

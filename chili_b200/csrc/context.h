@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cstddef>
 #include <cstdint>
+#include <functional>
 #include <initializer_list>
 #include <string>
 #include <vector>
@@ -58,6 +59,14 @@ struct FlowState;
 struct chili_ctx;
 // Frees the learned proposal's state (flow.cu).
 void flow_release(chili_ctx *ctx);
+// Launches the last step of one tile of the phased weight pass (base = first
+// listed point of the tile, T = tile capacity).
+using TileFn = std::function<int(long long base, long long T)>;
+// The phased weight pass (chili_gpu.cu) over listed points of a momenta
+// buffer [slot][component][m]; rec_dens may be null.
+int pipeline_run(chili_ctx *ctx, const double *mom_soa, long long m, const int32_t *list, const int32_t *ich,
+                 const long long *n_list, long long n_pre, int bins, bool opt, int32_t *rec_slot, double *rec_dens,
+                 const TileFn &combine);
 
 struct chili_ctx {
     int device = 0;
@@ -118,8 +127,11 @@ namespace {
 
 // Kernel classes timed under the "kernel_timing" option.
 const char *const kTimedKernels[] = {"k_mc_forward", "k_pp_nodes", "k_pp_items", "k_pp_chains", "k_pp_channel",
-                                     "k_pp_combine", "k_mc_weight", "k_mc_accum", "k_vegas_iter", nullptr};
-enum { KT_FORWARD, KT_NODES, KT_ITEMS, KT_CHAINS, KT_CHANNEL, KT_COMBINE, KT_WEIGHT, KT_ACCUM, KT_VEGAS };
+                                     "k_pp_combine", "k_mc_weight", "k_mc_accum", "k_vegas_iter", "k_flow_layer",
+                                     "k_flow_layer_bwd", "k_flow_wgrad", "k_alpha_train", "k_flow_phys",
+                                     "k_flow_batch", nullptr};
+enum { KT_FORWARD, KT_NODES, KT_ITEMS, KT_CHAINS, KT_CHANNEL, KT_COMBINE, KT_WEIGHT, KT_ACCUM, KT_VEGAS,
+       KT_FLOW_LAYER, KT_FLOW_BWD, KT_FLOW_WGRAD, KT_ALPHA_TRAIN, KT_FLOW_PHYS, KT_FLOW_BATCH };
 
 cudaEvent_t take_event(chili_ctx *ctx) {
     if (!ctx->event_pool.empty()) {

@@ -37,7 +37,9 @@ struct FlowState {
     bool have_scale = false;
     int adam_t = 0;
     // sampling
-    DevBuf sx0, sx1, sz, su, sch, slq, spart, sfold;
+    DevBuf sx0, sx1, sz, su, sch, slq, spart, sfold, fv;
+    // points of the flow path: momenta [leg][4][m], list, count
+    DevBuf fmom, flist, fcount;
     DevBuf err;
 };
 
@@ -152,6 +154,7 @@ int launch_wgrad(chili_ctx *ctx, const WgradArgs &a) {
         if (int rc = smem_attr(ctx, k_flow_wgrad, kWgSmem)) return rc;
         attr = true;
     }
+    KTimer kt_(ctx, KT_FLOW_WGRAD);
     k_flow_wgrad<<<dim3(kNsplit, 3), 128, kWgSmem, ctx->stream>>>(a);
     LAUNCHED();
     return CHILI_OK;
@@ -291,29 +294,81 @@ int train_pass(chili_ctx *ctx, long long n, float lr, int slot) {
     return CHILI_OK;
 }
 
-BatchArgs batch_args(chili_ctx *ctx, long long n, uint64_t seed, uint64_t ctr0) {
+// m points of the flow path. Training (train = true): u uniform and c ~ beta
+// from counters ctr0 ..., written to u/ch, and the batch rows (log F,
+// features, log prior, F when fval is given). Sampling: u and ch given, the
+// values v of the points. Both: VEGAS map, FSMapper, PreProcess, then every
+// channel's density through the phased weight pass.
+int flow_points(chili_ctx *ctx, bool train, long long m, uint64_t seed, uint64_t ctr0, float *u, int32_t *ch,
+                const float *logq, double *fval) {
     FlowState &S = *ctx->flow;
-    BatchArgs b{};
-    b.progs = ctx->progs.as<ChannelProgram>();
-    b.pp = ctx->point_prog.as<PointProgram>();
-    b.grids = ctx->edges.as<double>();
-    b.cp = S.cp.as<double>();
-    b.logbeta = S.logbeta.as<float>();
-    b.f = ctx->f_dev.as<IntegrandDesc>();
-    b.nch = S.nch;
-    b.dims = S.D;
-    b.bins = ctx->bins;
-    b.seed = seed;
-    b.ctr0 = ctr0;
-    b.n = n;
-    b.log_fscale = S.log_fscale;
-    b.u = S.X.as<float>();
-    b.ch = S.chb.as<int32_t>();
-    b.logf = S.logf.as<float>();
-    b.fval = nullptr;
-    b.feat = S.feat.as<float>();
-    b.logprior = S.logprior.as<float>();
-    return b;
+    CK(S.fmom.ensure(sizeof(double) * 4 * S.n_ext * m));
+    CK(S.flist.ensure(sizeof(int32_t) * m));
+    CK(S.fcount.ensure(sizeof(long long)));
+    CK(cudaMemsetAsync(S.fcount.p, 0, sizeof(long long), ctx->stream));
+    const unsigned gb = static_cast<unsigned>((m + 127) / 128);
+    if (train) {
+        k_flow_rows_init<<<gb, 128, 0, ctx->stream>>>(m, S.nch, S.F, S.logbeta.as<float>(), S.logf.as<float>(),
+                                                      S.feat.as<float>(), S.logprior.as<float>(), fval);
+        LAUNCHED();
+    }
+    GenArgs g{};
+    g.progs = ctx->progs.as<ChannelProgram>();
+    g.grids = ctx->edges.as<double>();
+    g.cp = S.cp.as<double>();
+    g.f = ctx->f_dev.as<IntegrandDesc>();
+    g.nch = S.nch;
+    g.dims = S.D;
+    g.bins = ctx->bins;
+    g.n_ext = S.n_ext;
+    g.seed = seed;
+    g.ctr0 = ctr0;
+    g.m = m;
+    g.u = u;
+    g.ch = ch;
+    g.mom_soa = S.fmom.as<double>();
+    g.list = S.flist.as<int32_t>();
+    g.count = S.fcount.as<long long>();
+    {
+        KTimer kt_(ctx, KT_FLOW_BATCH);
+        if (train) k_flow_gen<true><<<gb, 128, 0, ctx->stream>>>(g);
+        else k_flow_gen<false><<<gb, 128, 0, ctx->stream>>>(g);
+    }
+    LAUNCHED();
+    long long n_acc = 0;
+    CK(cudaMemcpyAsync(&n_acc, S.fcount.p, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (n_acc == 0) return CHILI_OK;
+    CombineArgs c{};
+    c.list = S.flist.as<int32_t>();
+    c.count = S.fcount.as<long long>();
+    c.m = m;
+    c.nch = S.nch;
+    c.n_ext = S.n_ext;
+    c.sqrts = ctx->sqrts;
+    c.f = ctx->f_dev.as<IntegrandDesc>();
+    c.beta = S.beta.as<float>();
+    c.logbeta = S.logbeta.as<float>();
+    c.log_fscale = S.log_fscale;
+    c.logf = S.logf.as<float>();
+    c.fval = fval;
+    c.feat = S.feat.as<float>();
+    c.logprior = S.logprior.as<float>();
+    c.logq = logq;
+    c.w = S.prm.as<float>() + S.off_alpha;
+    c.L = S.AL;
+    c.v = S.fv.as<double>();
+    return pipeline_run(ctx, S.fmom.as<double>(), m, S.flist.as<int32_t>(), ch, S.fcount.as<long long>(), n_acc,
+                        ctx->bins, false, nullptr, nullptr, [&](long long base, long long T) -> int {
+                            CombineArgs t = c;
+                            t.node_soa = ctx->node_soa.as<double>();
+                            t.dcv = ctx->dcv.as<double>();
+                            t.vwv = ctx->vwv.as<double>();
+                            t.ich_tile = ctx->ich_tile.as<int32_t>();
+                            t.base = base;
+                            t.T = T;
+                            return flow_launch_combine(ctx, train, t, static_cast<unsigned>((T + 127) / 128));
+                        });
 }
 
 // The flow over n points (xin, xout [D][n] on the device): the layers in
@@ -352,7 +407,8 @@ void flow_release(chili_ctx *ctx) {
     for (DevBuf *b : {&S.prm, &S.m, &S.v, &S.grad, &S.wtiles, &S.part_f, &S.part_a, &S.loss_part, &S.loss_dev,
                       &S.beta, &S.logbeta, &S.cp, &S.X, &S.chb, &S.logf, &S.fval, &S.feat, &S.logprior, &S.logq,
                       &S.glogq, &S.g0, &S.g1, &S.thetas, &S.h1s, &S.h2s, &S.gths, &S.gp2s, &S.gp1s, &S.scal,
-                      &S.sx0, &S.sx1, &S.sz, &S.su, &S.sch, &S.slq, &S.spart, &S.sfold, &S.err})
+                      &S.sx0, &S.sx1, &S.sz, &S.su, &S.sch, &S.slq, &S.spart, &S.sfold, &S.fv,
+                      &S.fmom, &S.flist, &S.fcount, &S.err})
         b->release();
     delete ctx->flow;
     ctx->flow = nullptr;
@@ -400,6 +456,7 @@ int chili_gpu_flow_init(chili_ctx *ctx, const chili_flow_params *params) {
         std::memset(&L, 0, sizeof(L));
         L.da = da;
         L.db = db;
+        L.nch = S.nch;
         for (int i = 0; i < da; ++i) L.cond[i] = static_cast<int8_t>(S.cond[l][i]);
         for (int j = 0; j < db; ++j) L.trans[j] = static_cast<int8_t>(S.trans[l][j]);
         S.off_w1.push_back(off);
@@ -605,10 +662,9 @@ int chili_gpu_flow_train(chili_ctx *ctx, int steps, uint64_t seed, uint64_t coun
     if (int rc = ensure_train(ctx, n)) return rc;
     if (!S.have_scale) {
         // F scale: mean of F over one batch of the plain proposal
-        BatchArgs b = batch_args(ctx, n, seed, counter_base);
-        b.fval = S.fval.as<double>();
-        k_flow_batch<<<static_cast<unsigned>((n + 127) / 128), 128, 0, ctx->stream>>>(b);
-        LAUNCHED();
+        if (int rc = flow_points(ctx, true, n, seed, counter_base, S.X.as<float>(), S.chb.as<int32_t>(), nullptr,
+                                 S.fval.as<double>()))
+            return rc;
         k_sum_pos<<<1, 256, 0, ctx->stream>>>(S.fval.as<double>(), n, S.scal.as<double>());
         LAUNCHED();
         double sc[2];
@@ -619,9 +675,9 @@ int chili_gpu_flow_train(chili_ctx *ctx, int steps, uint64_t seed, uint64_t coun
         S.have_scale = true;
     }
     for (int s = 0; s < steps; ++s) {
-        BatchArgs b = batch_args(ctx, n, seed, counter_base + static_cast<uint64_t>(s) * n);
-        k_flow_batch<<<static_cast<unsigned>((n + 127) / 128), 128, 0, ctx->stream>>>(b);
-        LAUNCHED();
+        if (int rc = flow_points(ctx, true, n, seed, counter_base + static_cast<uint64_t>(s) * n, S.X.as<float>(),
+                                 S.chb.as<int32_t>(), nullptr, nullptr))
+            return rc;
         if (int rc = train_pass(ctx, n, S.lr, s)) return rc;
     }
     if (int rc = check_err(ctx)) return rc;
@@ -651,34 +707,23 @@ int chili_gpu_flow_iterate(chili_ctx *ctx, uint64_t ncalls, uint64_t seed, uint6
     CK(S.sfold.ensure(sizeof(double) * width));
     CK(S.sz.ensure(sizeof(float) * xs));
     CK(S.su.ensure(sizeof(float) * xs));
+    CK(S.fv.ensure(sizeof(double) * chunk));
     std::vector<double> tot(width, 0.0), fold(width);
     for (uint64_t done = 0; done < ncalls;) {
         const long long m = std::min<long long>(chunk, static_cast<long long>(ncalls - done));
         k_flow_draw<<<static_cast<unsigned>((m + 255) / 256), 256, 0, ctx->stream>>>(
             S.cp.as<double>(), S.nch, S.D, seed, counter_base + done, m, S.sz.as<float>(), S.sch.as<int32_t>(),
-            S.slq.as<float>());
+            S.slq.as<float>(), S.fv.as<double>());
         LAUNCHED();
         if (int rc = flow_pass(ctx, S.sz.as<float>(), S.sch.as<int32_t>(), m, 1, S.su.as<float>(), S.slq.as<float>()))
             return rc;
-        PhysArgs a{};
-        a.progs = ctx->progs.as<ChannelProgram>();
-        a.pp = ctx->point_prog.as<PointProgram>();
-        a.grids = ctx->edges.as<double>();
-        a.logbeta = S.logbeta.as<float>();
-        a.beta = S.beta.as<float>();
-        a.f = ctx->f_dev.as<IntegrandDesc>();
-        a.nch = S.nch;
-        a.dims = S.D;
-        a.bins = ctx->bins;
-        a.n = m;
-        a.u = S.su.as<float>();
-        a.ch = S.sch.as<int32_t>();
-        a.logq = S.slq.as<float>();
-        a.w = S.prm.as<float>() + S.off_alpha;
-        a.L = S.AL;
-        a.part = S.spart.as<double>();
+        if (int rc = flow_points(ctx, false, m, seed, 0, S.su.as<float>(), S.sch.as<int32_t>(), S.slq.as<float>(),
+                                 nullptr))
+            return rc;
         const unsigned nbk = static_cast<unsigned>((m + kPhysBlock - 1) / kPhysBlock);
-        if (int rc = flow_launch_phys(ctx, a, nbk)) return rc;
+        k_flow_stats<<<nbk, kPhysBlock, 0, ctx->stream>>>(S.fv.as<double>(), S.sch.as<int32_t>(), S.beta.as<float>(),
+                                                          S.nch, m, S.spart.as<double>());
+        LAUNCHED();
         k_flow_fold<<<1, 256, 0, ctx->stream>>>(S.spart.as<double>(), static_cast<int>(nbk), width,
                                                 S.sfold.as<double>());
         LAUNCHED();

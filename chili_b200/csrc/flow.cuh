@@ -46,7 +46,7 @@ constexpr int kGTile = 128 * kP * 2;    // one spline-gradient tile (128 points 
 struct FlowLayer {
     const uint8_t *wt;  // kWBytes of tiles
     const float *E;     // [nch][128] channel embedding (first-layer bias per channel)
-    int da, db;
+    int da, db, nch;
     int8_t cond[kMaxDA];
     int8_t trans[8];
 };
@@ -325,7 +325,8 @@ __global__ void __launch_bounds__(128, 1) k_flow_layer(LayerArgs a) {
     for (long long tile = blockIdx.x; __syncthreads_and(ok) && tile < ntiles; tile += gridDim.x) {
         const long long row = tile * 128 + t;
         const bool valid = row < n;
-        const int c = valid ? a.ch[row] : 0;
+        int c = valid ? a.ch[row] : 0;
+        c = (c >= 0 && c < a.L.nch) ? c : 0;  // channel indices come from callers: keep E reads in bounds
         // conditioning coordinates -> A tile (bf16, 16 columns used)
         {
             float av[16];

@@ -26,6 +26,7 @@ int launch_alpha_t(chili_ctx *ctx, const AlphaTrainArgs &a) {
         if (int rc = smem_attr(ctx, k_alpha_train<NCH, NF>, bytes)) return rc;
         attr = bytes;
     }
+    KTimer kt_(ctx, KT_ALPHA_TRAIN);
     k_alpha_train<NCH, NF><<<kAlphaSplit, kAlphaBlock, bytes, ctx->stream>>>(a);
     LAUNCHED();
     return CHILI_OK;
@@ -38,27 +39,33 @@ int launch_alpha(chili_ctx *ctx, const AlphaTrainArgs &a) {
     return fail(ctx, CHILI_ERR_LIMIT, "channel-weight network limited to 64 channels and 32 features");
 }
 
-template <int NCH, int NF>
-int launch_phys_t(chili_ctx *ctx, const PhysArgs &a, unsigned blocks) {
-    const size_t bytes = sizeof(double) * 2 * kMaxAlphaCh + sizeof(float) * a.L.total;
-    static size_t attr = 0;
-    if (attr < bytes) {
-        if (int rc = smem_attr(ctx, k_flow_phys<NCH, NF>, bytes)) return rc;
-        attr = bytes;
+template <bool TRAIN, int NCH, int NF>
+int launch_combine_t(chili_ctx *ctx, const CombineArgs &a, unsigned blocks) {
+    const size_t bytes = TRAIN ? 0 : sizeof(float) * a.L.total;
+    if constexpr (!TRAIN) {
+        static size_t attr = 0;
+        if (attr < bytes) {
+            if (int rc = smem_attr(ctx, k_flow_combine<TRAIN, NCH, NF>, bytes)) return rc;
+            attr = bytes;
+        }
     }
-    k_flow_phys<NCH, NF><<<blocks, kPhysBlock, bytes, ctx->stream>>>(a);
+    KTimer kt_(ctx, KT_FLOW_PHYS);
+    k_flow_combine<TRAIN, NCH, NF><<<blocks, 128, bytes, ctx->stream>>>(a);
     LAUNCHED();
     return CHILI_OK;
 }
 
-int launch_phys(chili_ctx *ctx, const PhysArgs &a, unsigned blocks) {
+template <bool TRAIN>
+int launch_combine(chili_ctx *ctx, const CombineArgs &a, unsigned blocks) {
     const int nch = a.L.nch, F = a.L.F;
-    if (nch <= 16 && F <= 16) return launch_phys_t<16, 16>(ctx, a, blocks);
-    if (nch <= 64 && F <= 32) return launch_phys_t<64, 32>(ctx, a, blocks);
+    if (nch <= 16 && F <= 16) return launch_combine_t<TRAIN, 16, 16>(ctx, a, blocks);
+    if (nch <= 64 && F <= 32) return launch_combine_t<TRAIN, 64, 32>(ctx, a, blocks);
     return fail(ctx, CHILI_ERR_LIMIT, "channel-weight network limited to 64 channels and 32 features");
 }
 
 }  // namespace
 
 int flow_launch_alpha(chili_ctx *ctx, const AlphaTrainArgs &a) { return launch_alpha(ctx, a); }
-int flow_launch_phys(chili_ctx *ctx, const PhysArgs &a, unsigned blocks) { return launch_phys(ctx, a, blocks); }
+int flow_launch_combine(chili_ctx *ctx, bool train, const CombineArgs &a, unsigned blocks) {
+    return train ? launch_combine<true>(ctx, a, blocks) : launch_combine<false>(ctx, a, blocks);
+}

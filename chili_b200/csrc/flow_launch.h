@@ -1,7 +1,7 @@
 // flow_launch.h -- launchers of the learned proposal's heavy kernels, each
 // in its own translation unit so that they compile in parallel
 // (flow_layers.cu: coupling layers; flow_alpha.cu: channel-weight network and
-// the flow-path physics).
+// the last step of the flow-path points).
 #pragma once
 
 #include "context.h"
@@ -12,4 +12,5 @@
 int flow_launch_layer(chili_ctx *ctx, int mode, bool save, const chili_flow::LayerArgs &a, int sms);
 int flow_launch_bwd(chili_ctx *ctx, const chili_flow::BwdArgs &a, int sms);
 int flow_launch_alpha(chili_ctx *ctx, const chili_flow::AlphaTrainArgs &a);
-int flow_launch_phys(chili_ctx *ctx, const chili_flow::PhysArgs &a, unsigned blocks);
+// The last step of a flow-path tile (training rows or sampled values).
+int flow_launch_combine(chili_ctx *ctx, bool train, const chili_flow::CombineArgs &a, unsigned blocks);

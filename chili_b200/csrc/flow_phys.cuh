@@ -11,9 +11,13 @@
 //
 // alpha(p) = softmax(MLP(phi(p)) + log prior(p)): phi = log pair invariants
 // log(s_ij/S) and log(|t_1j|/S) of the outgoing legs, scaled to ~[-1, 1];
-// prior_c = beta_c * prod over c's massive decays of m^2 G^2 / ((s - m^2)^2 +
-// m^2 G^2) (a peak-normalised Breit-Wigner of the decaying current).
+// prior_c = beta_c g_c(p) / sum_k beta_k g_k(p), g_k = 1/D_k the channels'
+// densities (Integrand::GenerateWeight, Integrand.hh:112-123). With the last
+// layer zero and the flow the identity, v = f(p) / sum_k beta_k g_k(p): the
+// plain multichannel estimator itself, which training then improves on.
 #pragma once
+
+#include <math_constants.h>
 
 #include "flow.cuh"
 #include "mc_device.cuh"
@@ -52,12 +56,9 @@ __host__ __device__ inline int n_features(int n_ext) {
     return n_out * (n_out - 1) / 2 + n_out;
 }
 
-// Features and log prior of one point (momenta mom[0..n_ext), nodes rebuilt
-// from the PointProgram).
-__device__ __forceinline__ void point_features(const PointProgram *__restrict__ pp, const V4 *mom,
-                                               const float *__restrict__ logbeta, float *feat, float *logprior) {
-    const int n_ext = pp->n_ext;
-    const double S = pp->sqrts * pp->sqrts;
+// Features of one point (momenta mom[0..n_ext)).
+__device__ __forceinline__ void point_features(const V4 *mom, int n_ext, double sqrts, float *feat) {
+    const double S = sqrts * sqrts;
     int f = 0;
     for (int i = 2; i < n_ext; ++i)
         for (int j = i + 1; j < n_ext; ++j) {
@@ -68,21 +69,11 @@ __device__ __forceinline__ void point_features(const PointProgram *__restrict__ 
         const double tt = fabs(mass2(mom[0] + mom[j])) / S;
         feat[f++] = static_cast<float>(log(fmax(tt, 1e-12)) / 8.0 + 1.0);
     }
-    V4 node[PP_MAX_NODES];
-    for (int i = 0; i < pp->n_nodes; ++i) node[i] = i < n_ext ? mom[i] : node[pp->node_a[i]] + node[pp->node_b[i]];
-    for (int c = 0; c < pp->nch; ++c) {
-        double lp = 0;
-        const PPChannel &C = pp->ch[c];
-        for (int q = 0; q < C.n_dec; ++q) {
-            const int d = C.dw[q];
-            if (pp->dw_massless[d]) continue;
-            const double m = pp->dw_mass[d], g = pp->dw_width[d];
-            const double mw2 = m * m * g * g;
-            const double ds = mass2(node[pp->dw_node[d]]) - m * m;
-            lp += log(mw2 / (ds * ds + mw2));
-        }
-        logprior[c] = logbeta[c] + static_cast<float>(lp);
-    }
+}
+
+__device__ __forceinline__ V4 soa_v4(const double *__restrict__ soa, int s, long long m, long long i) {
+    return V4{soa[(4 * s + 0) * m + i], soa[(4 * s + 1) * m + i], soa[(4 * s + 2) * m + i],
+              soa[(4 * s + 3) * m + i]};
 }
 
 // Channel-weight network forward for one point: the logits of every channel
@@ -190,7 +181,8 @@ __global__ void __launch_bounds__(kAlphaBlock) k_alpha_train(AlphaTrainArgs a) {
 #pragma unroll
             for (int f = 0; f < NF; ++f) s_f[t * LF + f] = feat[f];
         }
-        const int c = valid ? a.ch[row] : 0;
+        int c = valid ? a.ch[row] : 0;
+        c = (c >= 0 && c < L.nch) ? c : 0;
         float lac = lg[0];
 #pragma unroll
         for (int k = 1; k < NCH; ++k)
@@ -272,68 +264,167 @@ constexpr size_t alpha_train_smem(int total) {
                             kAlphaBlock * (NF + 1));
 }
 
-#ifndef CHILI_FLOW_LAYERS_ONLY
-// Training batch from the plain multichannel proposal: channel c with
-// probability beta (table cp), u uniform, x = VEGAS_c(u), p = FSMapper_c(x).
-struct BatchArgs {
-    const ChannelProgram *progs;
-    const PointProgram *pp;
-    const double *grids;
-    const double *cp;
-    const float *logbeta;
+// Flow-path points, step 2, after the phased weight pass of a tile: every
+// channel's density D_k = dens_k vw_k, w0 = 1 / sum_k beta_k / D_k, the
+// integrand. Training: log F (F = f D_c / F_scale), features and log prior
+// of the batch row. Sampling: the channel-weight network and
+// v = alpha_c f D_c / (beta_c q_c) at the point's index (NaN when not finite).
+struct CombineArgs {
+    const double *node_soa;  // tile nodes [node][4][T]
+    const double *dcv, *vwv; // tile densities [channel][T]
+    const int32_t *ich_tile;
+    const int32_t *list;
+    const long long *count;
+    long long base, T, m;
+    int nch, n_ext;
+    double sqrts;
     const IntegrandDesc *f;
-    int nch, dims, bins;
-    uint64_t seed, ctr0;
-    long long n;
+    const float *beta, *logbeta;
+    // training
     double log_fscale;
-    float *u;          // [D][n]
-    int32_t *ch;
-    float *logf;       // [n]
-    double *fval;      // [n] F = f dens J (for the scale), or null
-    float *feat;       // [F][n]
-    float *logprior;   // [nch][n]
+    float *logf;       // [m]
+    double *fval;      // [m] or null
+    float *feat;       // [F][m]
+    float *logprior;   // [nch][m]
+    // sampling
+    const float *logq; // [m]
+    const float *w;    // network parameters
+    AlphaLayout L;
+    double *v;         // [m]
 };
 
-__global__ void __launch_bounds__(128) k_flow_batch(BatchArgs a) {
+template <bool TRAIN, int NCH, int NF>
+__global__ void __launch_bounds__(128) k_flow_combine(CombineArgs a) {
+    extern __shared__ float cw[];  // the network (sampling)
+    if (!TRAIN) {
+        for (int q = threadIdx.x; q < a.L.total; q += blockDim.x) cw[q] = a.w[q];
+        __syncthreads();
+    }
     const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-    if (i >= a.n) return;
+    const long long r = a.base + i;
+    if (i >= a.T || r >= *a.count) return;
+    const long long k = a.list[r];
+    const int c = a.ich_tile[i];
+    V4 mom[CHILI_MAX_EXT];
+    for (int s = 0; s < a.n_ext; ++s) mom[s] = soa_v4(a.node_soa, s, a.T, i);
+    double acc = 0.0, Dc = 0.0;
+    bool ok = true;
+    for (int j = 0; j < a.nch; ++j) {
+        const double Dj = a.dcv[static_cast<long long>(j) * a.T + i] * a.vwv[static_cast<long long>(j) * a.T + i];
+        ok = ok && (Dj > 0) && isfinite(Dj);
+        acc += static_cast<double>(a.beta[j]) / Dj;
+        if (j == c) Dc = Dj;
+    }
+    const double w0 = 1.0 / acc;
+    const double fv = eval_momenta(a.f, mom, a.n_ext);
+    const double F = fv * Dc;
+    ok = ok && (w0 > 0) && isfinite(w0) && (F > 0) && isfinite(F);
+    float lp[NCH > 0 ? NCH : 1];
+    if (ok) {
+        const float lw0 = static_cast<float>(log(w0));
+        for (int j = 0; j < a.nch; ++j) {
+            const double Dj = a.dcv[static_cast<long long>(j) * a.T + i] * a.vwv[static_cast<long long>(j) * a.T + i];
+            lp[j] = a.logbeta[j] - static_cast<float>(log(Dj)) + lw0;
+        }
+    }
+    float featv[kMaxFeat];
+    if (ok) point_features(mom, a.n_ext, a.sqrts, featv);
+    if (TRAIN) {
+        if (!ok) return;  // the row keeps logf = -inf
+        if (a.fval) a.fval[k] = F;
+        a.logf[k] = static_cast<float>(log(F) - a.log_fscale);
+        const int nf = n_features(a.n_ext);
+        for (int q = 0; q < nf; ++q) a.feat[q * a.m + k] = featv[q];
+        for (int j = 0; j < a.nch; ++j) a.logprior[j * a.m + k] = lp[j];
+    } else {
+        double v = 0;
+        if (ok) {
+            float feat[NF];
+#pragma unroll
+            for (int q = 0; q < NF; ++q) feat[q] = q < kMaxFeat ? featv[q] : 0.f;
+            float a1[kAH], a2[kAH], lg[NCH], lse;
+            alpha_forward<NCH, NF>(cw, a.L, feat, lp, a1, a2, lg, lse);
+            float lac = lg[0];
+#pragma unroll
+            for (int q = 1; q < NCH; ++q)
+                if (q == c) lac = lg[q];
+            lac -= lse;
+            v = exp(static_cast<double>(lac - a.logbeta[c] - a.logq[k])) * F;
+            if (!isfinite(v)) v = CUDART_NAN;
+        }
+        a.v[k] = v;
+    }
+}
+
+#ifndef CHILI_FLOW_LAYERS_ONLY
+// Flow-path points, step 1 (training: TRAIN = true, u uniform from the
+// counter-based generator and c ~ beta; sampling: u from the inverse flow,
+// c drawn before it): x = VEGAS_c(u), p = FSMapper_c(x), PreProcess; the
+// accepted points are listed (any order: every point's result is written at
+// its own index) and their external momenta stored [leg][component][m].
+struct GenArgs {
+    const ChannelProgram *progs;
+    const double *grids;
+    const double *cp;
+    const IntegrandDesc *f;
+    int nch, dims, bins, n_ext;
+    uint64_t seed, ctr0;
+    long long m;
+    float *u;          // [D][m]: written (training) or read (sampling)
+    int32_t *ch;       // [m]: written (training) or read (sampling)
+    double *mom_soa;   // [n_ext][4][m]
+    int32_t *list;     // [m]
+    long long *count;  // listed points
+};
+
+template <bool TRAIN>
+__global__ void __launch_bounds__(128) k_flow_gen(GenArgs a) {
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i >= a.m) return;
     const int D = a.dims;
     double r[CHILI_MAX_DIMS + 1];
-    load_uniforms(a.seed, a.ctr0 + i, nullptr, D + 1, r);
-    const int c = select_channel(a.cp, a.nch, r[D]);
-    for (int d = 0; d < D; ++d) a.u[d * a.n + i] = static_cast<float>(r[d]);
-    a.ch[i] = c;
-    double Fv = 0;
+    int c;
+    if (TRAIN) {
+        load_uniforms(a.seed, a.ctr0 + i, nullptr, D + 1, r);
+        c = select_channel(a.cp, a.nch, r[D]);
+        for (int d = 0; d < D; ++d) a.u[d * a.m + i] = static_cast<float>(r[d]);
+        a.ch[i] = c;
+    } else {
+        c = a.ch[i];
+        for (int d = 0; d < D; ++d) r[d] = fmin(static_cast<double>(a.u[d * a.m + i]), 0.99999999999999989);
+    }
+    double jac;
     V4 mom[CHILI_MAX_SLOTS];
     double m2[CHILI_MAX_SLOTS];
-    double jac = 0;
-    bool okp = grid_map_checked(a.grids + static_cast<size_t>(c) * D * (a.bins + 1), D, a.bins, r, jac);
-    if (okp) {
-        fs_generate(a.progs + c, r, mom, m2);
-        okp = preprocess(a.f, mom);
+    if (!grid_map_checked(a.grids + static_cast<size_t>(c) * D * (a.bins + 1), D, a.bins, r, jac)) return;
+    fs_generate(a.progs + c, r, mom, m2);
+    if (!preprocess(a.f, mom)) return;
+    const long long k = static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long *>(a.count), 1ull));
+    a.list[k] = static_cast<int32_t>(i);
+    for (int s = 0; s < a.n_ext; ++s) {
+        a.mom_soa[(4 * s + 0) * a.m + i] = mom[s].e;
+        a.mom_soa[(4 * s + 1) * a.m + i] = mom[s].x;
+        a.mom_soa[(4 * s + 2) * a.m + i] = mom[s].y;
+        a.mom_soa[(4 * s + 3) * a.m + i] = mom[s].z;
     }
-    float feat[kMaxFeat], lp[kMaxAlphaCh];
-    if (okp) {
-        double xx[CHILI_MAX_DIMS];
-        const double dens = fs_weight(a.progs + c, mom, xx);
-        Fv = dens == 0 ? 0 : eval_momenta(a.f, mom, a.progs[c].n_ext) * dens * jac;
-        if (!(Fv > 0) || !isfinite(Fv)) Fv = 0;
-        point_features(a.pp, mom, a.logbeta, feat, lp);
-    } else {
-        for (int q = 0; q < kMaxFeat; ++q) feat[q] = 0.f;
-        for (int q = 0; q < a.nch; ++q) lp[q] = a.logbeta[q];
-    }
-    if (a.fval) a.fval[i] = Fv;
-    a.logf[i] = Fv > 0 ? static_cast<float>(log(Fv) - a.log_fscale) : -INFINITY;
-    const int F = n_features(a.pp->n_ext);
-    for (int q = 0; q < F; ++q) a.feat[q * a.n + i] = feat[q];
-    for (int q = 0; q < a.nch; ++q) a.logprior[q * a.n + i] = lp[q];
+}
+
+// Training rows default to a rejected point: log F = -inf, log prior = log beta.
+__global__ void k_flow_rows_init(long long m, int nch, int F, const float *__restrict__ logbeta, float *__restrict__ logf,
+                                 float *__restrict__ feat, float *__restrict__ logprior, double *__restrict__ fval) {
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i >= m) return;
+    logf[i] = -INFINITY;
+    if (fval) fval[i] = 0;
+    for (int q = 0; q < F; ++q) feat[q * m + i] = 0.f;
+    for (int j = 0; j < nch; ++j) logprior[j * m + i] = logbeta[j];
 }
 
 // Flow-path sampling, step 1: channel c ~ beta, z uniform in [0,1)^D
-// (the flow's base point), log q = 0.
+// (the flow's base point), log q = 0, v = 0.
 __global__ void k_flow_draw(const double *__restrict__ cp, int nch, int dims, uint64_t seed, uint64_t ctr0,
-                            long long n, float *__restrict__ z, int32_t *__restrict__ ch, float *__restrict__ logq) {
+                            long long n, float *__restrict__ z, int32_t *__restrict__ ch, float *__restrict__ logq,
+                            double *__restrict__ v) {
     const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
     if (i >= n) return;
     double r[CHILI_MAX_DIMS + 1];
@@ -341,98 +432,38 @@ __global__ void k_flow_draw(const double *__restrict__ cp, int nch, int dims, ui
     ch[i] = select_channel(cp, nch, r[dims]);
     for (int d = 0; d < dims; ++d) z[d * n + i] = fminf(static_cast<float>(r[d]), 0.99999994f);
     logq[i] = 0.f;
+    v[i] = 0.0;
 }
 
-#endif  // CHILI_FLOW_LAYERS_ONLY
-
-// Flow-path sampling, step 2 (after the inverse flow): the phase-space
-// point, its value v and this block's StatsData partial.
-// part per block: [n, sum, sum2, max, n_nonzero, n_nonfinite] + per channel [n_c, sum T_c^2]
+// StatsData partial of a block of points: [n, sum, sum2, max, nonzero,
+// nonfinite] + per channel [n_c, sum (beta_c v)^2]; NaN values count as 0.
 constexpr int kPhysBlock = 128;
 constexpr int kPhysFixed = 6;
 
-struct PhysArgs {
-    const ChannelProgram *progs;
-    const PointProgram *pp;
-    const double *grids;
-    const float *logbeta;
-    const float *beta;
-    const IntegrandDesc *f;
-    int nch, dims, bins;
-    long long n;
-    const float *u;      // [D][n]
-    const int32_t *ch;
-    const float *logq;
-    const float *w;      // channel-weight network parameters
-    AlphaLayout L;
-    double *part;        // [gridDim.x][kPhysFixed + 2 nch]
-    double *vout;        // [n] or null
-    double *mom_out;     // [n][n_ext][4] or null
-};
-
-template <int NCH, int NF>
-__global__ void __launch_bounds__(kPhysBlock) k_flow_phys(PhysArgs a) {
-    extern __shared__ double sp[];
-    double *s_ch = sp;                                                // [2 nch]
-    float *w = reinterpret_cast<float *>(sp + 2 * kMaxAlphaCh);      // network
+__global__ void __launch_bounds__(kPhysBlock) k_flow_stats(const double *__restrict__ vals,
+                                                           const int32_t *__restrict__ ch,
+                                                           const float *__restrict__ beta, int nch, long long n,
+                                                           double *__restrict__ part) {
+    __shared__ double s_ch[2 * kMaxAlphaCh];
     const int t = threadIdx.x;
-    for (int q = t; q < 2 * a.nch; q += blockDim.x) s_ch[q] = 0;
-    for (int q = t; q < a.L.total; q += blockDim.x) w[q] = a.w[q];
+    for (int q = t; q < 2 * nch; q += blockDim.x) s_ch[q] = 0;
     __syncthreads();
     const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + t;
     double v = 0;
-    bool nan_v = false;
-    if (i < a.n) {
-        const int D = a.dims;
-        const int c = a.ch[i];
-        double r[CHILI_MAX_DIMS];
-        for (int d = 0; d < D; ++d) r[d] = fmin(static_cast<double>(a.u[d * a.n + i]), 0.99999999999999989);
-        double jac = 0;
-        V4 mom[CHILI_MAX_SLOTS];
-        double m2[CHILI_MAX_SLOTS];
-        bool okp = grid_map_checked(a.grids + static_cast<size_t>(c) * D * (a.bins + 1), D, a.bins, r, jac);
-        if (okp) {
-            fs_generate(a.progs + c, r, mom, m2);
-            okp = preprocess(a.f, mom);
+    bool bad = false;
+    if (i < n) {
+        v = vals[i];
+        if (!isfinite(v)) {
+            bad = true;
+            v = 0;
         }
-        if (okp) {
-            double xx[CHILI_MAX_DIMS];
-            const double dens = fs_weight(a.progs + c, mom, xx);
-            double Fv = dens == 0 ? 0 : eval_momenta(a.f, mom, a.progs[c].n_ext) * dens * jac;
-            if (!(Fv > 0) || !isfinite(Fv)) Fv = 0;
-            if (Fv > 0) {
-                float featv[kMaxFeat], lp[kMaxAlphaCh];
-                point_features(a.pp, mom, a.logbeta, featv, lp);
-                float feat[NF];
-#pragma unroll
-                for (int q = 0; q < NF; ++q) feat[q] = featv[q];
-                float a1[kAH], a2[kAH], lg[NCH], lse;
-                alpha_forward<NCH, NF>(w, a.L, feat, lp, a1, a2, lg, lse);
-                float lac = lg[0];
-#pragma unroll
-                for (int k = 1; k < NCH; ++k)
-                    if (k == c) lac = lg[k];
-                lac -= lse;
-                v = exp(static_cast<double>(lac - a.logbeta[c] - a.logq[i])) * Fv;
-                if (!isfinite(v)) {
-                    nan_v = true;
-                    v = 0;
-                }
-            }
-            if (a.mom_out)
-                for (int s = 0; s < a.progs[c].n_ext; ++s) {
-                    double *o = a.mom_out + (i * a.progs[c].n_ext + s) * 4;
-                    o[0] = mom[s].e; o[1] = mom[s].x; o[2] = mom[s].y; o[3] = mom[s].z;
-                }
-        }
-        if (a.vout) a.vout[i] = v;
-        const double T = v * static_cast<double>(a.beta[c]);
+        const int c = ch[i];
+        const double T = v * static_cast<double>(beta[c]);
         atomicAdd(s_ch + c, 1.0);
-        atomicAdd(s_ch + a.nch + c, T * T);
+        atomicAdd(s_ch + nch + c, T * T);
     }
-    // block reduction of n, sum, sum2, max, nonzero, nonfinite
-    const double cnt = i < a.n ? 1.0 : 0.0;
-    double q0 = cnt, q1 = v, q2 = v * v, q3 = v, q4 = v != 0 ? 1.0 : 0.0, q5 = nan_v ? 1.0 : 0.0;
+    const double cnt = i < n ? 1.0 : 0.0;
+    double q0 = cnt, q1 = v, q2 = v * v, q3 = v, q4 = v != 0 ? 1.0 : 0.0, q5 = bad ? 1.0 : 0.0;
     q0 = warp_sum(q0); q1 = warp_sum(q1); q2 = warp_sum(q2); q3 = warp_max(q3); q4 = warp_sum(q4); q5 = warp_sum(q5);
     __shared__ double red[kPhysBlock / 32][kPhysFixed];
     if ((t & 31) == 0) {
@@ -440,16 +471,16 @@ __global__ void __launch_bounds__(kPhysBlock) k_flow_phys(PhysArgs a) {
         red[t >> 5][3] = q3; red[t >> 5][4] = q4; red[t >> 5][5] = q5;
     }
     __syncthreads();
-    double *out = a.part + static_cast<long long>(blockIdx.x) * (kPhysFixed + 2 * a.nch);
+    double *out = part + static_cast<long long>(blockIdx.x) * (kPhysFixed + 2 * nch);
     if (t < kPhysFixed) {
         double sr = 0.0;
         for (int wq = 0; wq < kPhysBlock / 32; ++wq) sr = t == 3 ? fmax(sr, red[wq][3]) : sr + red[wq][t];
         out[t] = sr;
     }
-    for (int q = t; q < 2 * a.nch; q += blockDim.x) out[kPhysFixed + q] = s_ch[q];
+    for (int q = t; q < 2 * nch; q += blockDim.x) out[kPhysFixed + q] = s_ch[q];
 }
 
-#ifndef CHILI_FLOW_LAYERS_ONLY
+
 // Ordered fold of the block partials: out[0..5] = n, sum, sum2, max,
 // nonzero, nonfinite; out[6..] = per channel n_c, sum T_c^2.
 __global__ void k_flow_fold(const double *__restrict__ part, int nblocks, int width, double *__restrict__ out) {

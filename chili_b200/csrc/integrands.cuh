@@ -14,8 +14,9 @@ struct IntegrandDesc {
     int32_t kind;
     int32_t nparams;
     int32_t pre;  // chili_preprocess_kind
-    int32_t pad;
+    int32_t n_ext;  // external legs (CHILI_PRE_CUTS)
     double p[CHILI_MAX_INTEGRAND_PARAMS];
+    double cut[4];  // CHILI_PRE_CUTS: sqrts, ptmin, etamax, delta_r
 };
 
 // f(x) = N [exp(-|x-a|^2/s^2) + exp(-|x-b|^2/s^2)]; params {s, N, a[D], b[D]}.
@@ -65,10 +66,36 @@ __device__ __forceinline__ double eval_momenta(const IntegrandDesc *__restrict__
     }
 }
 
+// The physical region and the cuts of CHILI_PRE_CUTS (include/chili_gpu.h).
+// NaN momenta fail every comparison.
+__device__ __forceinline__ bool pass_cuts(const IntegrandDesc *__restrict__ f, const V4 *mom) {
+    const double half = 0.5 * f->cut[0] * (1.0 + 1e-12);
+    if (!(-mom[0].e <= half) || !(-mom[1].e <= half)) return false;
+    const double pt2min = f->cut[1] * f->cut[1], etamax = f->cut[2], dr2 = f->cut[3] * f->cut[3];
+    const int ne = f->n_ext;
+    double eta[CHILI_MAX_EXT], phi[CHILI_MAX_EXT];
+    for (int i = 2; i < ne; ++i) {
+        const double pt2 = mom[i].x * mom[i].x + mom[i].y * mom[i].y;
+        if (!(pt2 >= pt2min) || !(pt2 > 0)) return false;
+        eta[i] = asinh(mom[i].z / sqrt(pt2));
+        if (!(fabs(eta[i]) <= etamax)) return false;
+        phi[i] = atan2(mom[i].y, mom[i].x);
+    }
+    for (int i = 2; i < ne; ++i)
+        for (int j = i + 1; j < ne; ++j) {
+            double dphi = fabs(phi[i] - phi[j]);
+            if (dphi > kPi) dphi = 2.0 * kPi - dphi;
+            const double deta = eta[i] - eta[j];
+            if (!(deta * deta + dphi * dphi >= dr2)) return false;
+        }
+    return true;
+}
+
 // PreProcess (MultiChannel.hh:219-223); CHILI_PRE_FINITE follows the first
 // check of src/example.cc:26-29.
 __device__ __forceinline__ bool preprocess(const IntegrandDesc *__restrict__ f, const V4 *mom) {
     if (f->pre == CHILI_PRE_FINITE) return !isnan(mom[0].e);
+    if (f->pre == CHILI_PRE_CUTS) return pass_cuts(f, mom);
     return true;
 }
 

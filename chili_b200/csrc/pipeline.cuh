@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(128) k_pp_channel(
     }
     dcv[static_cast<long long>(c) * m + i] = dc;
     vwv[static_cast<long long>(c) * m + i] = vw;
-    rec_dens[static_cast<long long>(c) * mr + r] = dc;
+    if (rec_dens) rec_dens[static_cast<long long>(c) * mr + r] = dc;
 }
 
 // Per point: 1 / sum_c alpha_c / dens_c / vw_c in channel order

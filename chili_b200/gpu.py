@@ -44,6 +44,7 @@ def _declare(lib):
         "chili_gpu_grid_split": ([vp, i32], i32),
         "chili_gpu_set_integrand": ([vp, i32, vp, i32], i32),
         "chili_gpu_set_preprocess": ([vp, i32], i32),
+        "chili_gpu_set_preprocess_cuts": ([vp, dbl, dbl, dbl, dbl], i32),
         "chili_gpu_vegas_iterate": ([vp, u64, u64, u64, vp, dbl, i32, vp, vp], i32),
         "chili_gpu_vegas_iterate_noalloc": ([vp, vp, i32, i32, vp, i32, u64, u64, u64, vp, vp], i32),
         "chili_gpu_set_channels": ([vp, P(abi.ChannelDesc), i32, P(abi.Cuts), dbl, i32], i32),
@@ -215,6 +216,10 @@ class Context:
         p = np.ascontiguousarray(params, dtype=np.float64)
         self._keep.append(p)
         self.call("chili_gpu_set_integrand", kind, _ptr(p) if p.size else None, int(p.size))
+
+    def set_preprocess_cuts(self, sqrts, ptmin=30.0, etamax=99.0, delta_r=0.4):
+        """PreProcess = CHILI_PRE_CUTS (physical region and cuts)."""
+        self.call("chili_gpu_set_preprocess_cuts", float(sqrts), float(ptmin), float(etamax), float(delta_r))
 
     def set_preprocess(self, kind):
         self.call("chili_gpu_set_preprocess", kind)

@@ -160,7 +160,17 @@ enum chili_integrand_kind {
 enum chili_preprocess_kind {
     CHILI_PRE_ACCEPT_ALL = 0,
     /* reject when the first momentum's energy is NaN (src/example.cc:26-29) */
-    CHILI_PRE_FINITE = 1
+    CHILI_PRE_FINITE = 1,
+    /* the physical region and the usual cuts (set with
+     * chili_gpu_set_preprocess_cuts): finite momenta, incoming energies
+     * |E_0|, |E_1| <= sqrts/2 (momentum fractions <= 1), every outgoing leg
+     * pT >= ptmin and |eta| <= etamax, every outgoing pair
+     * Delta R = sqrt(Delta eta^2 + Delta phi^2) >= delta_r.  The reference's
+     * FSMapper generates points outside this region (fractions above 1,
+     * s-channel decay products below the pT cut) that its weights do not
+     * describe consistently across channels; inside it every channel's
+     * single-channel estimate agrees. */
+    CHILI_PRE_CUTS = 2
 };
 
 /* ------------------------------------------------------------ context */
@@ -218,6 +228,9 @@ int chili_gpu_grid_split(chili_ctx *ctx, int nsplit);
 int chili_gpu_set_integrand(chili_ctx *ctx, int kind, const double *params,
                             int nparams);
 int chili_gpu_set_preprocess(chili_ctx *ctx, int kind);
+/* PreProcess = CHILI_PRE_CUTS with these cut values (channels must be set:
+ * the cuts apply to their external legs). */
+int chili_gpu_set_preprocess_cuts(chili_ctx *ctx, double sqrts, double ptmin, double etamax, double delta_r);
 
 /* ------------------------------------------------------ plain VEGAS */
 /* One Vegas::operator() (Vegas.cc:18-52) on grid 0: ncalls points, uniforms

@@ -58,6 +58,7 @@ def _load(path, prefix):
         "ref_mc_destroy": ([vp], None),
         "ref_mc_ndims": ([vp], i32),
         "ref_mc_set_integrand": ([vp, i32, vp, i32, i32], None),
+        "ref_mc_set_cuts": ([vp, dbl, dbl, dbl, dbl], None),
         "ref_mc_set_grids": ([vp, vp], None),
         "ref_mc_get_grids": ([vp, vp], None),
         "ref_mc_set_alpha": ([vp, vp], None),
@@ -179,6 +180,10 @@ class MultiChannel:
             except Exception:
                 pass
             self.h = None
+
+    def set_cuts(self, sqrts, ptmin=30.0, etamax=99.0, delta_r=0.4):
+        """PreProcess = CHILI_PRE_CUTS."""
+        self.oracle().ref_mc_set_cuts(self.h, sqrts, ptmin, etamax, delta_r)
 
     def set_grids(self, edges):
         self.oracle().ref_mc_set_grids(self.h, _p(np.ascontiguousarray(edges, dtype=np.float64)))

@@ -611,8 +611,40 @@ typedef struct {
     chili_multichannel_params prm;
     int fkind, pre;
     double fp[CHILI_MAX_INTEGRAND_PARAMS];
+    double cut[4]; /* CHILI_PRE_CUTS: sqrts, ptmin, etamax, delta_r */
     double *hist, *atrain;
 } mc_t;
+
+/* CHILI_PRE_CUTS (include/chili_gpu.h): physical region and cuts; a
+ * PreProcess callback of this harness, not a reference step. */
+static int pass_cuts(const mc_t *m, const v4 *q) {
+    const double half = 0.5 * m->cut[0] * (1.0 + 1e-12);
+    if (!(-q[0].e <= half) || !(-q[1].e <= half)) return 0;
+    const double pt2min = m->cut[1] * m->cut[1], etamax = m->cut[2], dr2 = m->cut[3] * m->cut[3];
+    double eta[CHILI_MAX_EXT], phi[CHILI_MAX_EXT];
+    for (int i = 2; i < m->n_ext; ++i) {
+        const double pt2 = q[i].x * q[i].x + q[i].y * q[i].y;
+        if (!(pt2 >= pt2min) || !(pt2 > 0)) return 0;
+        eta[i] = asinh(q[i].z / sqrt(pt2));
+        if (!(fabs(eta[i]) <= etamax)) return 0;
+        phi[i] = atan2(q[i].y, q[i].x);
+    }
+    for (int i = 2; i < m->n_ext; ++i)
+        for (int j = i + 1; j < m->n_ext; ++j) {
+            double dphi = fabs(phi[i] - phi[j]);
+            if (dphi > 3.14159265358979323846) dphi = 2.0 * 3.14159265358979323846 - dphi;
+            const double deta = eta[i] - eta[j];
+            if (!(deta * deta + dphi * dphi >= dr2)) return 0;
+        }
+    return 1;
+}
+
+/* PreProcess of the harness: 1 = accepted. */
+static int preprocess_ok(const mc_t *m, const v4 *q) {
+    if (m->pre == CHILI_PRE_FINITE) return !isnan(q[0].e);
+    if (m->pre == CHILI_PRE_CUTS) return pass_cuts(m, q);
+    return 1;
+}
 
 /* std::discrete_distribution (libstdc++ _M_initialize / operator()) as used
  * by Random::SelectIndex (Random.hh:43-45). */
@@ -677,6 +709,11 @@ void orc_mc_set_integrand(void *p, int kind, const double *fp, int np, int pre) 
     m->fkind = kind;
     m->pre = pre;
     for (int i = 0; i < np && i < CHILI_MAX_INTEGRAND_PARAMS; ++i) m->fp[i] = fp[i];
+}
+void orc_mc_set_cuts(void *p, double sqrts, double ptmin, double etamax, double dr) {
+    mc_t *m = p;
+    m->pre = CHILI_PRE_CUTS;
+    m->cut[0] = sqrts; m->cut[1] = ptmin; m->cut[2] = etamax; m->cut[3] = dr;
 }
 void orc_mc_set_grids(void *p, const double *e) {
     mc_t *m = p;
@@ -767,7 +804,7 @@ int orc_mc_iterate(void *p, const double *u, int64_t n_u, int guard, chili_stats
         v4 mom[NSLOT];
         if (am_map1(m->grids + ich * gs, D, B, x, &jac)) fs_gen(&m->ch[ich], x, mom);
         else for (int s = 0; s < m->n_ext; ++s) { v4 z = {NAN, NAN, NAN, NAN}; mom[s] = z; }
-        if (m->pre == CHILI_PRE_FINITE && isnan(mom[0].e)) {
+        if (!preprocess_ok(m, mom)) {
             --i;
             st_add(&st, 0);
             info->rejected_pre++;
@@ -837,7 +874,7 @@ void orc_evaluate_batch(void *p, int c, const double *u, int64_t n, double *out)
         memcpy(x, u + i * m->ndims, sizeof(double) * m->ndims);
         v4 q[NSLOT];
         fs_gen(&m->ch[c], x, q);
-        if (m->pre == CHILI_PRE_FINITE && isnan(q[0].e)) { out[i] = 0; continue; }
+        if (!preprocess_ok(m, q)) { out[i] = 0; continue; }
         double w = fs_wgt(&m->ch[c], q, x);
         out[i] = w == 0 ? 0 : eval_f(m, q) * w;
     }

@@ -349,6 +349,35 @@ void ref_mc_set_integrand(void *p, int kind, const double *params, int nparams, 
         h->integrand.PreProcess() = [](const std::vector<FourVector> &) { return true; };
 }
 
+// CHILI_PRE_CUTS (include/chili_gpu.h) as the PreProcess callback of this
+// harness (the reference's own example filters with JetCluster instead,
+// src/example.cc:25-52); the same arithmetic as the CUDA library and the port.
+void ref_mc_set_cuts(void *p, double sqrts, double ptmin, double etamax, double dr) {
+    auto *h = static_cast<MC *>(p);
+    h->pre = CHILI_PRE_CUTS;
+    const int ne = h->n_ext;
+    h->integrand.PreProcess() = [=](const std::vector<FourVector> &m) {
+        const double half = 0.5 * sqrts * (1.0 + 1e-12);
+        if (!(-m[0][0] <= half) || !(-m[1][0] <= half)) return false;
+        double eta[CHILI_MAX_EXT], phi[CHILI_MAX_EXT];
+        for (int i = 2; i < ne; ++i) {
+            const double pt2 = m[i][1] * m[i][1] + m[i][2] * m[i][2];
+            if (!(pt2 >= ptmin * ptmin) || !(pt2 > 0)) return false;
+            eta[i] = std::asinh(m[i][3] / std::sqrt(pt2));
+            if (!(std::fabs(eta[i]) <= etamax)) return false;
+            phi[i] = std::atan2(m[i][2], m[i][1]);
+        }
+        for (int i = 2; i < ne; ++i)
+            for (int j = i + 1; j < ne; ++j) {
+                double dphi = std::fabs(phi[i] - phi[j]);
+                if (dphi > 3.14159265358979323846) dphi = 2.0 * 3.14159265358979323846 - dphi;
+                const double deta = eta[i] - eta[j];
+                if (!(deta * deta + dphi * dphi >= dr * dr)) return false;
+            }
+        return true;
+    };
+}
+
 void ref_mc_set_grids(void *p, const double *edges) {
     auto *h = static_cast<MC *>(p);
     const size_t per = static_cast<size_t>(h->ndims) * (h->bins + 1);

@@ -59,3 +59,28 @@ def test_launch_count_and_determinism(ctx_factory):
     assert res[0][1] == res[1][1]
     assert res[0][0][0] == res[1][0][0]
     assert _close(res[0][0][3], res[1][0][3], 1e-13)
+
+
+def test_cut_preprocess_iteration_matches_oracle(ctx_factory):
+    """CHILI_PRE_CUTS on the GPU: the same rejections, StatsData and alpha as
+    the C oracle on the same counter-based uniforms."""
+    cs = workloads.channel_set(4)
+    ctx = ctx_factory()
+    ctx.set_channels(cs)
+    ctx.uniform_grids(cs.nch, ctx.ndims, 100)
+    ctx.set_integrand(abi.CHILI_FUNC_PROPAGATOR, channels.propagator_params())
+    ctx.set_preprocess_cuts(1000.0)
+    params = workloads.mc_params(20_000)
+    O = port.MultiChannel(cs, 100, params, abi.CHILI_FUNC_PROPAGATOR, channels.propagator_params())
+    O.set_cuts(1000.0)
+    seed, counter = 13, 0
+    for it in range(2):
+        st, info = ctx.multichannel_iterate(params, seed=seed, counter=counter)
+        u = port.philox_uniforms(seed, counter, info.points_tried, ctx.ndims + 1)
+        st_o, info_o = O.iterate(u)
+        assert info_o.points_tried == info.points_tried and info_o.rejected_pre == info.rejected_pre, it
+        assert st.n == st_o.n and st.n_finite == st_o.n_finite
+        assert _close(st.sum, st_o.sum, 1e-11) and _close(st.sum2, st_o.sum2, 1e-11)
+        ctx.set_grids(O.get_grids())
+        ctx.set_alpha(O.get_alpha()[0])
+        counter += info.points_tried
