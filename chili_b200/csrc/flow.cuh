@@ -52,8 +52,8 @@ struct FlowLayer {
 };
 
 // ------------------------------------------------------------------ spline
-__device__ __forceinline__ float softplus_f(float t) { return t > 20.f ? t : log1pf(expf(t)); }
-__device__ __forceinline__ float sigmoid_f(float t) { return 1.f / (1.f + expf(-t)); }
+__device__ __forceinline__ float softplus_f(float t) { return t > 20.f ? t : log1pf(__expf(t)); }
+__device__ __forceinline__ float sigmoid_f(float t) { return 1.f / (1.f + __expf(-t)); }
 
 // softmax of 16 logits (sm) and the bin sizes min + (1 - 16 min) sm
 __device__ __forceinline__ void bin_sizes(const float *th, float minv, float (&sm)[kBins], float (&sz)[kBins]) {
@@ -63,10 +63,10 @@ __device__ __forceinline__ void bin_sizes(const float *th, float minv, float (&s
     float s = 0.f;
 #pragma unroll
     for (int k = 0; k < kBins; ++k) {
-        sm[k] = expf(th[k] - m);
+        sm[k] = __expf(th[k] - m);
         s += sm[k];
     }
-    const float inv = 1.f / s, sc = 1.f - kBins * minv;
+    const float inv = __frcp_rn(s), sc = 1.f - kBins * minv;
 #pragma unroll
     for (int k = 0; k < kBins; ++k) {
         sm[k] *= inv;
@@ -128,7 +128,7 @@ __device__ __forceinline__ float rqs_forward(const float *th, float x, float &lo
     const float A = s * xi * xi + b.d0 * om;
     const float B = s + (b.d0 + b.d1 - 2.f * s) * om;
     const float C = b.d1 * xi * xi + 2.f * s * om + b.d0 * (1.f - xi) * (1.f - xi);
-    logj = 2.f * logf(s) + logf(C) - 2.f * logf(B);
+    logj = 2.f * __logf(s) + __logf(C) - 2.f * __logf(B);
     return b.y0 + b.hk * A / B;
 }
 
@@ -149,7 +149,7 @@ __device__ __forceinline__ float rqs_inverse(const float *th, float y, float &lo
     const float om = xi * (1.f - xi);
     const float B = s + dl * om;
     const float C = b.d1 * xi * xi + 2.f * s * om + b.d0 * (1.f - xi) * (1.f - xi);
-    logj = 2.f * logf(s) + logf(C) - 2.f * logf(B);
+    logj = 2.f * __logf(s) + __logf(C) - 2.f * __logf(B);
     return b.x0 + xi * b.wk;
 }
 
@@ -284,18 +284,37 @@ struct LayerArgs {
     int *err;
 };
 
-constexpr int kFwdSmem = kWBytes + 128 * 64 * 2 + kHTile + 64 + 1024;
+constexpr int kFwdSmem = kWBytes + 128 * 64 * 2 + kHTile + 512 + 64 + 1024;
+constexpr int kFwdThreads = 256;  // two threads per point (TMEM lanes are shared by warps w and w + 4)
+
+template <int J, int MODE, bool SAVE>
+__device__ __forceinline__ float spline_dim(const LayerArgs &a, uint32_t lane_addr, long long row, bool valid,
+                                            long long n, float &logj) {
+    float th[kPerDim];
+    load_theta<J>(lane_addr, 256, th);
+    if (SAVE && valid) {
+#pragma unroll
+        for (int i = 0; i < kPerDim; ++i) a.theta[(J * kPerDim + i) * n + row] = th[i];
+    }
+    const float x = valid ? fminf(fmaxf(a.xin[a.L.trans[J] * n + row], 0.f), 1.f) : 0.5f;
+    const float y = MODE == 0 ? rqs_forward(th, x, logj) : rqs_inverse(th, x, logj);
+    if (valid) a.xout[a.L.trans[J] * n + row] = y;
+    return y;
+}
 
 template <int DB, int MODE, bool SAVE>
-__global__ void __launch_bounds__(128, 1) k_flow_layer(LayerArgs a) {
+__global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *sm = align1024(smem_raw);
     uint8_t *sW1 = sm, *sW2 = sm + kW1Bytes, *sW3 = sm + kW1Bytes + kW2Bytes;
     uint8_t *sA = sm + kWBytes;
     uint8_t *sH = sA + 128 * 64 * 2;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sH + kHTile);
+    float *sL = reinterpret_cast<float *>(sH + kHTile);  // [128] log-det partials of the second half
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sL + 128);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
     const int t = threadIdx.x, wp = t >> 5;
+    const int half = wp >> 2;               // 0: warps 0-3, 1: warps 4-7
+    const int r = (wp & 3) * 32 + (t & 31);  // the point (TMEM lane) of this thread
     const long long n = a.n;
     const long long ntiles = (n + 127) / 128;
 
@@ -309,7 +328,7 @@ __global__ void __launch_bounds__(128, 1) k_flow_layer(LayerArgs a) {
     __syncthreads();
     tc_fence_after();
     const uint32_t tbase = *tslot;
-    const uint32_t lane_addr = tbase + (static_cast<uint32_t>(wp * 32) << 16);
+    const uint32_t lane_addr = tbase + (static_cast<uint32_t>((wp & 3) * 32) << 16);
     if (t == 0) {
         mbar_expect_tx(bar, kWBytes);
         bulk_g2s(sm, a.L.wt, kWBytes, bar);
@@ -323,12 +342,12 @@ __global__ void __launch_bounds__(128, 1) k_flow_layer(LayerArgs a) {
     const int da = a.L.da;
 
     for (long long tile = blockIdx.x; __syncthreads_and(ok) && tile < ntiles; tile += gridDim.x) {
-        const long long row = tile * 128 + t;
+        const long long row = tile * 128 + r;
         const bool valid = row < n;
         int c = valid ? a.ch[row] : 0;
         c = (c >= 0 && c < a.L.nch) ? c : 0;  // channel indices come from callers: keep E reads in bounds
-        // conditioning coordinates -> A tile (bf16, 16 columns used)
-        {
+        if (half == 0) {
+            // conditioning coordinates -> A tile (bf16, 16 columns used)
             float av[16];
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
@@ -343,12 +362,12 @@ __global__ void __launch_bounds__(128, 1) k_flow_layer(LayerArgs a) {
                 pk.y = pack_bf16x2(av[8 * q + 2], av[8 * q + 3]);
                 pk.z = pack_bf16x2(av[8 * q + 4], av[8 * q + 5]);
                 pk.w = pack_bf16x2(av[8 * q + 6], av[8 * q + 7]);
-                *reinterpret_cast<uint4 *>(sA + sw128_off(t, 8 * q, 128)) = pk;
+                *reinterpret_cast<uint4 *>(sA + sw128_off(r, 8 * q, 128)) = pk;
             }
+        } else if (valid) {
+            // identity coordinates pass through
+            for (int i = 0; i < da; ++i) a.xout[a.L.cond[i] * n + row] = a.xin[a.L.cond[i] * n + row];
         }
-        float xt[DB];
-#pragma unroll
-        for (int j = 0; j < DB; ++j) xt[j] = valid ? fminf(fmaxf(a.xin[a.L.trans[j] * n + row], 0.f), 1.f) : 0.5f;
         fence_async_smem();
         tc_fence_before();
         __syncthreads();
@@ -360,18 +379,19 @@ __global__ void __launch_bounds__(128, 1) k_flow_layer(LayerArgs a) {
         ok = mbar_wait(bar + 1, phase, kWaitLimit) && ok;
         phase ^= 1;
         tc_fence_after();
-        // h1 = lrelu(acc + E[c]); unit 127 = 1
+        // h1 = lrelu(acc + E[c]); unit 127 = 1; this half's 64 columns
         const float *E = a.L.E + static_cast<long long>(c) * kH;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < 2; ++q) {
+            const int c0 = 64 * half + 32 * q;
             float v[32];
-            tmem_ld32(lane_addr + 32 * q, v);
+            tmem_ld32(lane_addr + c0, v);
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
-                v[j] = lrelu(v[j] + __ldg(E + 32 * q + j));
-                if (q == 3 && j == 31) v[j] = 1.f;
+                v[j] = lrelu(v[j] + __ldg(E + c0 + j));
+                if (c0 + j == kH - 1) v[j] = 1.f;
             }
-            store_row32(sH, 128, t, 32 * q, v);
+            store_row32(sH, 128, r, c0, v);
         }
         fence_async_smem();
         tc_fence_before();
@@ -388,15 +408,16 @@ __global__ void __launch_bounds__(128, 1) k_flow_layer(LayerArgs a) {
         tc_fence_after();
         __syncthreads();  // the copy of h1 is complete before h2 overwrites it
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < 2; ++q) {
+            const int c0 = 64 * half + 32 * q;
             float v[32];
-            tmem_ld32(lane_addr + 128 + 32 * q, v);
+            tmem_ld32(lane_addr + 128 + c0, v);
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
                 v[j] = lrelu(v[j]);
-                if (q == 3 && j == 31) v[j] = 1.f;
+                if (c0 + j == kH - 1) v[j] = 1.f;
             }
-            store_row32(sH, 128, t, 32 * q, v);
+            store_row32(sH, 128, r, c0, v);
         }
         fence_async_smem();
         tc_fence_before();
@@ -411,34 +432,20 @@ __global__ void __launch_bounds__(128, 1) k_flow_layer(LayerArgs a) {
         ok = mbar_wait(bar + 1, phase, kWaitLimit) && ok;
         phase ^= 1;
         tc_fence_after();
-        // splines
-        float lsum = 0.f;
-        float xo[DB];
-#pragma unroll
-        for (int j = 0; j < DB; ++j) {
-            float th[kPerDim];
-            switch (j) {
-            case 0: load_theta<0>(lane_addr, 256, th); break;
-            case 1: load_theta<1>(lane_addr, 256, th); break;
-            case 2: load_theta<2>(lane_addr, 256, th); break;
-            case 3: load_theta<3>(lane_addr, 256, th); break;
-            default: load_theta<4>(lane_addr, 256, th); break;
-            }
-            if (SAVE && valid) {
-#pragma unroll
-                for (int i = 0; i < kPerDim; ++i) a.theta[(j * kPerDim + i) * n + row] = th[i];
-            }
-            float lj;
-            xo[j] = MODE == 0 ? rqs_forward(th, xt[j], lj) : rqs_inverse(th, xt[j], lj);
-            lsum += lj;
-        }
-        if (valid) {
-#pragma unroll
-            for (int j = 0; j < DB; ++j) a.xout[a.L.trans[j] * n + row] = xo[j];
-            for (int i = 0; i < da; ++i) a.xout[a.L.cond[i] * n + row] = a.xin[a.L.cond[i] * n + row];
-            a.logq[row] += lsum;
+        // splines: dimensions 0, 2, 4 on the first half, 1, 3 on the second
+        float lsum = 0.f, lj = 0.f;
+        if (half == 0) {
+            if (DB > 0) { spline_dim<0, MODE, SAVE>(a, lane_addr, row, valid, n, lj); lsum += lj; }
+            if (DB > 2) { spline_dim<2, MODE, SAVE>(a, lane_addr, row, valid, n, lj); lsum += lj; }
+            if (DB > 4) { spline_dim<4, MODE, SAVE>(a, lane_addr, row, valid, n, lj); lsum += lj; }
+        } else {
+            if (DB > 1) { spline_dim<1, MODE, SAVE>(a, lane_addr, row, valid, n, lj); lsum += lj; }
+            if (DB > 3) { spline_dim<3, MODE, SAVE>(a, lane_addr, row, valid, n, lj); lsum += lj; }
+            sL[r] = lsum;
         }
         tc_fence_before();
+        __syncthreads();
+        if (half == 0 && valid) a.logq[row] += lsum + sL[r];
     }
     if (!ok && t == 0) atomicExch(a.err, 1);
     // every issued MMA has been waited for (or the wait gave up): release TMEM
@@ -467,18 +474,39 @@ struct BwdArgs {
     int *err;
 };
 
-constexpr int kBwdSmem = kWBytes + kGTile + kHTile + 64 + 1024;
+constexpr int kBwdSmem = kWBytes + kGTile + kHTile + 16 * 128 * 4 + 64 + 1024;
+constexpr int kBwdThreads = 256;  // two threads per point
+
+template <int J>
+__device__ __forceinline__ void spline_dim_bwd(const BwdArgs &a, uint8_t *sG, int r, long long row, bool valid,
+                                               long long n, float gl) {
+    float th[kPerDim], g[kPerDim];
+#pragma unroll
+    for (int i = 0; i < kPerDim; ++i) th[i] = valid ? a.theta[(J * kPerDim + i) * n + row] : 0.f;
+    const float x = valid ? fminf(fmaxf(a.xin[a.L.trans[J] * n + row], 0.f), 1.f) : 0.5f;
+    const float gy = (valid && a.gout) ? a.gout[a.L.trans[J] * n + row] : 0.f;
+    const float gx = rqs_backward(th, x, gy, valid ? gl : 0.f, g);
+    if (valid) a.gin[a.L.trans[J] * n + row] = gx;
+#pragma unroll
+    for (int i = 0; i < kPerDim; ++i) {
+        const uint32_t pk = pack_bf16x2(valid ? g[i] : 0.f, 0.f);
+        *reinterpret_cast<uint16_t *>(sG + sw128_off(r, J * kPerDim + i, 128)) = static_cast<uint16_t>(pk & 0xFFFFu);
+    }
+}
 
 template <int DB>
-__global__ void __launch_bounds__(128, 1) k_flow_layer_bwd(BwdArgs a) {
+__global__ void __launch_bounds__(kBwdThreads, 1) k_flow_layer_bwd(BwdArgs a) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *sm = align1024(smem_raw);
     uint8_t *sW1 = sm, *sW2 = sm + kW1Bytes, *sW3 = sm + kW1Bytes + kW2Bytes;
     uint8_t *sG = sm + kWBytes;
     uint8_t *sP = sG + kGTile;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sP + kHTile);
+    float *sGA = reinterpret_cast<float *>(sP + kHTile);  // [16][128] g_a partials of the second half
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sGA + 16 * 128);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
     const int t = threadIdx.x, wp = t >> 5;
+    const int half = wp >> 2;
+    const int r = (wp & 3) * 32 + (t & 31);
     const long long n = a.n;
     const long long ntiles = (n + 127) / 128;
     if (t == 0) {
@@ -491,7 +519,7 @@ __global__ void __launch_bounds__(128, 1) k_flow_layer_bwd(BwdArgs a) {
     __syncthreads();
     tc_fence_after();
     const uint32_t tbase = *tslot;
-    const uint32_t lane_addr = tbase + (static_cast<uint32_t>(wp * 32) << 16);
+    const uint32_t lane_addr = tbase + (static_cast<uint32_t>((wp & 3) * 32) << 16);
     if (t == 0) {
         mbar_expect_tx(bar, kWBytes);
         bulk_g2s(sm, a.L.wt, kWBytes, bar);
@@ -502,28 +530,20 @@ __global__ void __launch_bounds__(128, 1) k_flow_layer_bwd(BwdArgs a) {
     uint32_t phase = 0;
     const int da = a.L.da;
     for (long long tile = blockIdx.x; __syncthreads_and(ok) && tile < ntiles; tile += gridDim.x) {
-        const long long row = tile * 128 + t;
+        const long long row = tile * 128 + r;
         const bool valid = row < n;
         const float gl = valid ? a.glogq[row] : 0.f;
-        float gxt[DB];
-        // spline backward -> g_theta (bf16 tile, row t)
-#pragma unroll
-        for (int j = 0; j < DB; ++j) {
-            float th[kPerDim], g[kPerDim];
-#pragma unroll
-            for (int i = 0; i < kPerDim; ++i) th[i] = valid ? a.theta[(j * kPerDim + i) * n + row] : 0.f;
-            const float x = valid ? fminf(fmaxf(a.xin[a.L.trans[j] * n + row], 0.f), 1.f) : 0.5f;
-            const float gy = (valid && a.gout) ? a.gout[a.L.trans[j] * n + row] : 0.f;
-            gxt[j] = rqs_backward(th, x, gy, valid ? gl : 0.f, g);
-#pragma unroll
-            for (int i = 0; i < kPerDim; ++i) {
-                const int col = j * kPerDim + i;
-                const uint32_t pk = pack_bf16x2(valid ? g[i] : 0.f, 0.f);
-                *reinterpret_cast<uint16_t *>(sG + sw128_off(t, col, 128)) = static_cast<uint16_t>(pk & 0xFFFFu);
-            }
+        // spline backward -> g_theta (bf16 tile, row r): dims 0, 2, 4 | 1, 3
+        if (half == 0) {
+            if (DB > 0) spline_dim_bwd<0>(a, sG, r, row, valid, n, gl);
+            if (DB > 2) spline_dim_bwd<2>(a, sG, r, row, valid, n, gl);
+            if (DB > 4) spline_dim_bwd<4>(a, sG, r, row, valid, n, gl);
+        } else {
+            if (DB > 1) spline_dim_bwd<1>(a, sG, r, row, valid, n, gl);
+            if (DB > 3) spline_dim_bwd<3>(a, sG, r, row, valid, n, gl);
+            for (int col = DB * kPerDim; col < kP; ++col)
+                *reinterpret_cast<uint16_t *>(sG + sw128_off(r, col, 128)) = 0;
         }
-        for (int col = DB * kPerDim; col < kP; ++col)
-            *reinterpret_cast<uint16_t *>(sG + sw128_off(t, col, 128)) = 0;
         fence_async_smem();
         tc_fence_before();
         __syncthreads();
@@ -538,19 +558,20 @@ __global__ void __launch_bounds__(128, 1) k_flow_layer_bwd(BwdArgs a) {
         ok = mbar_wait(bar + 1, phase, kWaitLimit) && ok;
         phase ^= 1;
         tc_fence_after();
-        // g_p2 = g_h2 * lrelu'(h2), unit 127 -> 0
+        // g_p2 = g_h2 * lrelu'(h2), unit 127 -> 0; this half's 64 columns
         const uint8_t *h2t = a.h2s + tile * kHTile;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < 2; ++q) {
+            const int c0 = 64 * half + 32 * q;
             float v[32], hv[32];
-            tmem_ld32(lane_addr + 32 * q, v);
-            load_row32(h2t, 128, t, 32 * q, hv);
+            tmem_ld32(lane_addr + c0, v);
+            load_row32(h2t, 128, r, c0, hv);
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
                 v[j] *= hv[j] > 0.f ? 1.f : kSlope;
-                if ((q == 3 && j == 31) || !valid) v[j] = 0.f;
+                if (c0 + j == kH - 1 || !valid) v[j] = 0.f;
             }
-            store_row32(sP, 128, t, 32 * q, v);
+            store_row32(sP, 128, r, c0, v);
         }
         fence_async_smem();
         tc_fence_before();
@@ -566,49 +587,52 @@ __global__ void __launch_bounds__(128, 1) k_flow_layer_bwd(BwdArgs a) {
         phase ^= 1;
         tc_fence_after();
         __syncthreads();  // the copy of g_p2 is complete before g_p1 overwrites it
-        // g_p1 = g_h1 * lrelu'(h1); g_a = bf16(g_p1) W1 on the CUDA cores
+        // g_p1 = g_h1 * lrelu'(h1); g_a = bf16(g_p1) W1 on the CUDA cores, this half's units
         const uint8_t *h1t = a.h1s + tile * kHTile;
         float ga[kMaxDA];
 #pragma unroll
         for (int i = 0; i < kMaxDA; ++i) ga[i] = 0.f;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < 2; ++q) {
+            const int c0 = 64 * half + 32 * q;
             float v[32], hv[32];
-            tmem_ld32(lane_addr + 32 * q, v);
-            load_row32(h1t, 128, t, 32 * q, hv);
+            tmem_ld32(lane_addr + c0, v);
+            load_row32(h1t, 128, r, c0, hv);
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
                 v[j] *= hv[j] > 0.f ? 1.f : kSlope;
-                if ((q == 3 && j == 31) || !valid) v[j] = 0.f;
+                if (c0 + j == kH - 1 || !valid) v[j] = 0.f;
             }
-            store_row32(sP, 128, t, 32 * q, v);
+            store_row32(sP, 128, r, c0, v);
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
-                const int hcol = 32 * q + j;
+                const int hcol = c0 + j;
                 const float gq = bf16_hi(pack_bf16x2(0.f, v[j]));
                 // W1[hcol][0..15]: two 16-byte chunks of row hcol of the W1 tile
-                const uint4 c0 = *reinterpret_cast<const uint4 *>(sW1 + sw128_off(hcol, 0, 128));
-                const uint4 c1 = *reinterpret_cast<const uint4 *>(sW1 + sw128_off(hcol, 8, 128));
-                ga[0] += gq * bf16_lo(c0.x); ga[1] += gq * bf16_hi(c0.x);
-                ga[2] += gq * bf16_lo(c0.y); ga[3] += gq * bf16_hi(c0.y);
-                ga[4] += gq * bf16_lo(c0.z); ga[5] += gq * bf16_hi(c0.z);
-                ga[6] += gq * bf16_lo(c0.w); ga[7] += gq * bf16_hi(c0.w);
-                ga[8] += gq * bf16_lo(c1.x); ga[9] += gq * bf16_hi(c1.x);
-                ga[10] += gq * bf16_lo(c1.y); ga[11] += gq * bf16_hi(c1.y);
-                ga[12] += gq * bf16_lo(c1.z); ga[13] += gq * bf16_hi(c1.z);
-                ga[14] += gq * bf16_lo(c1.w); ga[15] += gq * bf16_hi(c1.w);
+                const uint4 w0 = *reinterpret_cast<const uint4 *>(sW1 + sw128_off(hcol, 0, 128));
+                const uint4 w1 = *reinterpret_cast<const uint4 *>(sW1 + sw128_off(hcol, 8, 128));
+                ga[0] += gq * bf16_lo(w0.x); ga[1] += gq * bf16_hi(w0.x);
+                ga[2] += gq * bf16_lo(w0.y); ga[3] += gq * bf16_hi(w0.y);
+                ga[4] += gq * bf16_lo(w0.z); ga[5] += gq * bf16_hi(w0.z);
+                ga[6] += gq * bf16_lo(w0.w); ga[7] += gq * bf16_hi(w0.w);
+                ga[8] += gq * bf16_lo(w1.x); ga[9] += gq * bf16_hi(w1.x);
+                ga[10] += gq * bf16_lo(w1.y); ga[11] += gq * bf16_hi(w1.y);
+                ga[12] += gq * bf16_lo(w1.z); ga[13] += gq * bf16_hi(w1.z);
+                ga[14] += gq * bf16_lo(w1.w); ga[15] += gq * bf16_hi(w1.w);
             }
+        }
+        if (half == 1) {
+#pragma unroll
+            for (int i = 0; i < kMaxDA; ++i) sGA[i * 128 + r] = ga[i];
         }
         __syncthreads();
         copy_block(a.gp1s + tile * kHTile, sP, kHTile);
-        if (valid) {
-#pragma unroll
-            for (int j = 0; j < DB; ++j) a.gin[a.L.trans[j] * n + row] = gxt[j];
+        if (half == 0 && valid) {
 #pragma unroll
             for (int i = 0; i < kMaxDA; ++i)
                 if (i < da) {
                     const int d = a.L.cond[i];
-                    a.gin[d * n + row] = (a.gout ? a.gout[d * n + row] : 0.f) + 2.f * ga[i];
+                    a.gin[d * n + row] = (a.gout ? a.gout[d * n + row] : 0.f) + 2.f * (ga[i] + sGA[i * 128 + r]);
                 }
         }
         tc_fence_before();

@@ -26,7 +26,7 @@ int launch_layer_t(chili_ctx *ctx, const LayerArgs &a, int sms) {
     const long long tiles = (a.n + 127) / 128;
     const unsigned grid = static_cast<unsigned>(std::min<long long>(tiles, sms));
     KTimer kt_(ctx, KT_FLOW_LAYER);
-    k_flow_layer<DB, MODE, SAVE><<<grid, 128, kFwdSmem, ctx->stream>>>(a);
+    k_flow_layer<DB, MODE, SAVE><<<grid, kFwdThreads, kFwdSmem, ctx->stream>>>(a);
     LAUNCHED();
     return CHILI_OK;
 }
@@ -53,7 +53,7 @@ int launch_bwd_t(chili_ctx *ctx, const BwdArgs &a, int sms) {
     const long long tiles = (a.n + 127) / 128;
     const unsigned grid = static_cast<unsigned>(std::min<long long>(tiles, sms));
     KTimer kt_(ctx, KT_FLOW_BWD);
-    k_flow_layer_bwd<DB><<<grid, 128, kBwdSmem, ctx->stream>>>(a);
+    k_flow_layer_bwd<DB><<<grid, kBwdThreads, kBwdSmem, ctx->stream>>>(a);
     LAUNCHED();
     return CHILI_OK;
 }
