@@ -143,9 +143,25 @@ def run_chili(args, rank, world, local_rank):
         if world > 1:
             torch.distributed.barrier()
 
+    # N > 1: the reference's MPI mode (MultiChannel.hh:184-212): every rank
+    # integrates its own counter stream, the training data and StatsData are
+    # summed by one NCCL all-reduce per iteration, every rank adapts alike
+    synced = world > 1
+    if synced:
+        from chili_b200 import parallel
+        rank_obj = parallel.GpuRank(ctx, seed, counter)
+
+    def one_step():
+        if synced:
+            mst, info = parallel.synced_iteration(rank_obj, params, device=dev)
+            return mst, info, (mst[3] / mst[2] if mst[2] > 0 else 0.0) / world
+        st, info = ctx.multichannel_iterate(params, seed=seed, counter=rank_obj_counter[0], guard=True)
+        rank_obj_counter[0] += info.points_tried
+        return st.as_tuple(), info, unweighted_events(st, info)
+
+    rank_obj_counter = [counter]
     for _ in range(args.warmup):
-        st, info = ctx.multichannel_iterate(params, seed=seed, counter=counter, guard=True)
-        counter += info.points_tried
+        one_step()
     torch.cuda.synchronize(dev)
     barrier()
     torch.cuda.synchronize(dev)
@@ -162,12 +178,11 @@ def run_chili(args, rank, world, local_rank):
         ev0.record(stream)
         t_wall0 = time.perf_counter()
         for _ in range(args.steps):
-            st, info = ctx.multichannel_iterate(params, seed=seed, counter=counter, guard=True)
-            counter += info.points_tried
+            st_t, info, u_step = one_step()
             tried += info.points_tried
             weighted += info.points_weighted
-            unw += unweighted_events(st, info)
-            pooled += np.array(st.as_tuple()) * np.array([1, 0, 0, 1, 1, 1])
+            unw += u_step
+            pooled += np.array(st_t) * np.array([1, 0, 0, 1, 1, 1])
             mean, err = gpu.stats_mean_error(pooled)
             history.append((time.perf_counter() - t_wall0, err / abs(mean) if mean else float("inf")))
         ev1.record(stream)
@@ -218,7 +233,9 @@ def run_chili(args, rank, world, local_rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (on-device Philox4x32-10 uniforms)",
-            "config": dict(workload_config(args.ncalls), parallelism=f"replicas x{world}"),
+            "config": dict(workload_config(args.ncalls),
+                           parallelism=f"dp{world}: ranks synchronised by one NCCL all-reduce of the training data "
+                                       f"per iteration" if world > 1 else "single GPU"),
             "points_per_s": acc_tot / (ms_max / 1e3),
             "tried_points_per_s": tried_tot / (ms_max / 1e3),
             "weighted_points_per_step": weighted / args.steps,

@@ -261,6 +261,10 @@ int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value) {
         for (auto &n : ctx->klaunches) n = 0;
         return CHILI_OK;
     }
+    if (std::strcmp(name, "defer_train") == 0) {
+        ctx->defer_train = value != 0;
+        return CHILI_OK;
+    }
     if (std::strcmp(name, "pipeline_tile") == 0) {
         if (value < 1024 || value > (1ll << 24)) return fail(ctx, CHILI_ERR_INVALID_ARG, "pipeline_tile outside [1024, 2^24]");
         ctx->pipe_tile = value;
@@ -819,7 +823,7 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         if (++rounds > 100000) return fail(ctx, CHILI_ERR_TIMEOUT, "no accepted points after 100000 rounds");
     }
     IterAcc acc_h;
-    if (opt) {
+    if (opt && !ctx->defer_train) {
         k_alpha_update<<<1, 32, 0, ctx->stream>>>(alpha_ptr(ctx), best_ptr(ctx), mindiff_ptr(ctx), cp_ptr(ctx),
                                                   acc_train_ptr(ctx), nch, params->beta,
                                                   params->min_alpha, 1);
@@ -838,6 +842,29 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         info->nonfinite_alpha_terms = acc_h.nonfinite;
         info->points_weighted = static_cast<uint64_t>(weighted);
     }
+    return CHILI_OK;
+}
+
+int chili_gpu_multichannel_train(chili_ctx *ctx, const chili_multichannel_params *params, const double *hist,
+                                 const double *alpha_train) {
+    if (!ctx || !params || !hist || !alpha_train) return fail(ctx, CHILI_ERR_INVALID_ARG, "NULL argument");
+    int rc;
+    if ((rc = set_device(ctx))) return rc;
+    if ((rc = need_mc(ctx))) return rc;
+    const int nch = ctx->nch;
+    const size_t hist_n = static_cast<size_t>(nch) * ctx->ndims * ctx->bins;
+    CK(ctx->hist.ensure(sizeof(double) * hist_n));
+    CK(ctx->acc.ensure(sizeof(IterAcc)));
+    Arg ah, aa;
+    if ((rc = resolve(ctx, hist, sizeof(double) * hist_n, 0, true, ah))) return rc;
+    if ((rc = resolve(ctx, alpha_train, sizeof(double) * nch, 1, true, aa))) return rc;
+    CK(cudaMemcpyAsync(ctx->hist.p, ah.dev, sizeof(double) * hist_n, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(acc_train_ptr(ctx), aa.dev, sizeof(double) * nch, cudaMemcpyDeviceToDevice, ctx->stream));
+    k_alpha_update<<<1, 32, 0, ctx->stream>>>(alpha_ptr(ctx), best_ptr(ctx), mindiff_ptr(ctx), cp_ptr(ctx),
+                                              acc_train_ptr(ctx), nch, params->beta, params->min_alpha, 1);
+    LAUNCHED();
+    if ((rc = adapt_grids(ctx, 0, nch, params->grid_alpha, ctx->hist.as<double>(), 1))) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
     return CHILI_OK;
 }
 

@@ -86,6 +86,7 @@ struct chili_ctx {
     bool have_pp = false;      // the set fits the PointProgram limits
     bool use_pp = true;        // option "point_program"
     bool use_pipeline = true;  // option "pipeline": phased weight pass
+    bool defer_train = false;  // option "defer_train": iterations collect training data, Train is the caller's
     long long pipe_tile = 1 << 22;  // option "pipeline_tile": points per tile
     PointProgram pp_host;      // host copy (sizes of the memo buffers)
     DevBuf node_soa, memo, cfail, dcv, vwv;

@@ -129,7 +129,7 @@ int pack_tiles(chili_ctx *ctx) {
     const float *p = S.prm.as<float>();
     for (int l = 0; l < S.L; ++l) {
         k_flow_pack<<<(kP * 128 + 255) / 256, 256, 0, ctx->stream>>>(
-            p + S.off_w1[l], p + S.off_w2[l], p + S.off_w3[l], S.da[l], S.db[l] * kPerDim,
+            p + S.off_w1[l], p + S.off_e[l], p + S.off_w2[l], p + S.off_w3[l], S.da[l], S.nch, S.db[l] * kPerDim,
             S.wtiles.as<uint8_t>() + static_cast<size_t>(l) * kWBytes);
         LAUNCHED();
     }
@@ -428,8 +428,8 @@ int chili_gpu_flow_init(chili_ctx *ctx, const chili_flow_params *params) {
     if (params->layers < 1 || params->layers > 32 || params->batch < 128 || params->batch > (1 << 24))
         return fail(ctx, CHILI_ERR_INVALID_ARG, "layers in [1, 32], batch in [128, 2^24]");
     const int F = n_features(ctx->n_ext);
-    if (ctx->nch > kMaxAlphaCh || F > kMaxFeat)
-        return fail(ctx, CHILI_ERR_LIMIT, "channel-weight network limited to 64 channels and 32 features");
+    if (ctx->nch > kMaxFlowCh || F > kMaxFeat)
+        return fail(ctx, CHILI_ERR_LIMIT, "learned proposal limited to 48 channels and 32 features");
     flow_release(ctx);
     ctx->flow = new FlowState();
     FlowState &S = *ctx->flow;

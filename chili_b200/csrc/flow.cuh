@@ -6,7 +6,8 @@
 // Coupling layer l: the conditioning coordinates a = x[cond] (da <= 16) and
 // the point's channel c give the spline parameters of the transformed
 // coordinates x[trans] (db <= 5):
-//   h1 = lrelu(W1 (2a - 1) + E[c]),  h1[127] = 1
+//   h1 = lrelu(W1 (2a - 1) + E[c]),  h1[127] = 1   (E[c] through a one-hot
+//                                    column c of the same product, K = 64)
 //   h2 = lrelu(W2 h1),               h2[127] = 1      (unit 127 carries the bias)
 //   theta = W3 h2                    (db x 49: 16 widths, 16 heights, 17 slopes)
 // The three products run on the tensor cores (tcgen05, bf16 operands in
@@ -32,11 +33,13 @@ constexpr int kBins = 16;          // spline bins
 constexpr int kPerDim = 3 * kBins + 1;
 constexpr int kMaxDB = 5;          // transformed dimensions per layer
 constexpr int kMaxDA = 16;         // conditioning dimensions per layer
+constexpr int kMaxFlowCh = 48;     // channels (one-hot columns 16..63 of the first product)
 constexpr int kP = 256;            // padded spline-parameter columns (>= 5 * 49)
 constexpr float kMinW = 1e-3f, kMinH = 1e-3f, kMinD = 1e-3f, kSlope = 0.01f;
 constexpr uint32_t kWaitLimit = 1u << 22;
 
-// bf16 weight tiles of one layer, contiguous: W1 [128][64] (da columns used),
+// bf16 weight tiles of one layer, contiguous: W1 [128][64] (columns 0..da-1:
+// W1, columns 16..16+nch-1: the channel embedding E^T, so nch <= 48),
 // W2 [128][128], W3 [256][128] (db*49 rows used), each an SW128 tile.
 constexpr int kW1Bytes = 128 * 64 * 2, kW2Bytes = 128 * 128 * 2, kW3Bytes = kP * 128 * 2;
 constexpr int kWBytes = kW1Bytes + kW2Bytes + kW3Bytes;
@@ -284,23 +287,12 @@ struct LayerArgs {
     int *err;
 };
 
-constexpr int kFwdSmem = kWBytes + 128 * 64 * 2 + kHTile + 512 + 64 + 1024;
+// Shared memory of the forward kernel: weights, A tile, H tile, the second
+// half's log-det partials, and a per-thread staging area for the 64
+// accumulator columns that hold one dimension's spline parameters.
 constexpr int kFwdThreads = 256;  // two threads per point (TMEM lanes are shared by warps w and w + 4)
-
-template <int J, int MODE, bool SAVE>
-__device__ __forceinline__ float spline_dim(const LayerArgs &a, uint32_t lane_addr, long long row, bool valid,
-                                            long long n, float &logj) {
-    float th[kPerDim];
-    load_theta<J>(lane_addr, 256, th);
-    if (SAVE && valid) {
-#pragma unroll
-        for (int i = 0; i < kPerDim; ++i) a.theta[(J * kPerDim + i) * n + row] = th[i];
-    }
-    const float x = valid ? fminf(fmaxf(a.xin[a.L.trans[J] * n + row], 0.f), 1.f) : 0.5f;
-    const float y = MODE == 0 ? rqs_forward(th, x, logj) : rqs_inverse(th, x, logj);
-    if (valid) a.xout[a.L.trans[J] * n + row] = y;
-    return y;
-}
+constexpr int kFwdScratch = 64 * kFwdThreads * 4;
+constexpr int kFwdSmem = kWBytes + 128 * 64 * 2 + kHTile + kFwdScratch + 512 + 64 + 1024;
 
 template <int DB, int MODE, bool SAVE>
 __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
@@ -309,7 +301,8 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
     uint8_t *sW1 = sm, *sW2 = sm + kW1Bytes, *sW3 = sm + kW1Bytes + kW2Bytes;
     uint8_t *sA = sm + kWBytes;
     uint8_t *sH = sA + 128 * 64 * 2;
-    float *sL = reinterpret_cast<float *>(sH + kHTile);  // [128] log-det partials of the second half
+    float *sTh = reinterpret_cast<float *>(sH + kHTile);  // [64][256] spline-parameter staging
+    float *sL = sTh + 64 * kFwdThreads;                    // [128] log-det partials of the second half
     uint64_t *bar = reinterpret_cast<uint64_t *>(sL + 128);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
     const int t = threadIdx.x, wp = t >> 5;
@@ -347,8 +340,9 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
         int c = valid ? a.ch[row] : 0;
         c = (c >= 0 && c < a.L.nch) ? c : 0;  // channel indices come from callers: keep E reads in bounds
         if (half == 0) {
-            // conditioning coordinates -> A tile (bf16, 16 columns used)
-            float av[16];
+            // A tile row: conditioning coordinates (columns 0..15) and the
+            // one-hot of the channel (columns 16..63), bf16
+            float av[32];
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
                 float v = 0.f;
@@ -356,14 +350,11 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
                 av[i] = v;
             }
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                uint4 pk;
-                pk.x = pack_bf16x2(av[8 * q + 0], av[8 * q + 1]);
-                pk.y = pack_bf16x2(av[8 * q + 2], av[8 * q + 3]);
-                pk.z = pack_bf16x2(av[8 * q + 4], av[8 * q + 5]);
-                pk.w = pack_bf16x2(av[8 * q + 6], av[8 * q + 7]);
-                *reinterpret_cast<uint4 *>(sA + sw128_off(r, 8 * q, 128)) = pk;
-            }
+            for (int i = 16; i < 32; ++i) av[i] = (valid && i == 16 + c) ? 1.f : 0.f;
+            store_row32(sA, 128, r, 0, av);
+#pragma unroll
+            for (int i = 0; i < 32; ++i) av[i] = (valid && 32 + i == 16 + c) ? 1.f : 0.f;
+            store_row32(sA, 128, r, 32, av);
         } else if (valid) {
             // identity coordinates pass through
             for (int i = 0; i < da; ++i) a.xout[a.L.cond[i] * n + row] = a.xin[a.L.cond[i] * n + row];
@@ -373,14 +364,15 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
         __syncthreads();
         if (t == 0) {
             tc_fence_after();
-            mma_bf16(tbase, desc_k(aA, 128, 0), desc_k(aW1, 128, 0), id_h, 0);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) mma_bf16(tbase, desc_k(aA, 128, 16 * k), desc_k(aW1, 128, 16 * k), id_h, k > 0);
             mma_commit(bar + 1);
         }
         ok = mbar_wait(bar + 1, phase, kWaitLimit) && ok;
         phase ^= 1;
         tc_fence_after();
-        // h1 = lrelu(acc + E[c]); unit 127 = 1; this half's 64 columns
-        const float *E = a.L.E + static_cast<long long>(c) * kH;
+        // h1 = lrelu(acc) (the product already holds E[c]); unit 127 = 1;
+        // this half's 64 columns
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
             const int c0 = 64 * half + 32 * q;
@@ -388,7 +380,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
             tmem_ld32(lane_addr + c0, v);
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
-                v[j] = lrelu(v[j] + __ldg(E + c0 + j));
+                v[j] = lrelu(v[j]);
                 if (c0 + j == kH - 1) v[j] = 1.f;
             }
             store_row32(sH, 128, r, c0, v);
@@ -432,17 +424,34 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
         ok = mbar_wait(bar + 1, phase, kWaitLimit) && ok;
         phase ^= 1;
         tc_fence_after();
-        // splines: dimensions 0, 2, 4 on the first half, 1, 3 on the second
-        float lsum = 0.f, lj = 0.f;
-        if (half == 0) {
-            if (DB > 0) { spline_dim<0, MODE, SAVE>(a, lane_addr, row, valid, n, lj); lsum += lj; }
-            if (DB > 2) { spline_dim<2, MODE, SAVE>(a, lane_addr, row, valid, n, lj); lsum += lj; }
-            if (DB > 4) { spline_dim<4, MODE, SAVE>(a, lane_addr, row, valid, n, lj); lsum += lj; }
-        } else {
-            if (DB > 1) { spline_dim<1, MODE, SAVE>(a, lane_addr, row, valid, n, lj); lsum += lj; }
-            if (DB > 3) { spline_dim<3, MODE, SAVE>(a, lane_addr, row, valid, n, lj); lsum += lj; }
-            sL[r] = lsum;
+        // splines: dimensions 0, 2, 4 on the first half, 1, 3 on the second;
+        // one copy of the spline code, the dimension a runtime loop
+        float lsum = 0.f;
+#pragma unroll 1
+        for (int j = half; j < DB; j += 2) {
+            const int b0 = j * kPerDim, c0 = b0 & ~15;  // c0 + 64 <= 256
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                float v[16];
+                tmem_ld16(lane_addr + static_cast<uint32_t>(256 + c0 + 16 * q), v);
+#pragma unroll
+                for (int i = 0; i < 16; ++i) sTh[(16 * q + i) * kFwdThreads + t] = v[i];
+            }
+            float th[kPerDim];
+#pragma unroll
+            for (int i = 0; i < kPerDim; ++i) th[i] = sTh[(b0 - c0 + i) * kFwdThreads + t];
+            if (SAVE && valid) {
+#pragma unroll
+                for (int i = 0; i < kPerDim; ++i) a.theta[(b0 + i) * n + row] = th[i];
+            }
+            const int d = a.L.trans[j];
+            const float x = valid ? fminf(fmaxf(a.xin[d * n + row], 0.f), 1.f) : 0.5f;
+            float lj;
+            const float y = MODE == 0 ? rqs_forward(th, x, lj) : rqs_inverse(th, x, lj);
+            if (valid) a.xout[d * n + row] = y;
+            lsum += lj;
         }
+        if (half == 1) sL[r] = lsum;
         tc_fence_before();
         __syncthreads();
         if (half == 0 && valid) a.logq[row] += lsum + sL[r];
@@ -476,23 +485,6 @@ struct BwdArgs {
 
 constexpr int kBwdSmem = kWBytes + kGTile + kHTile + 16 * 128 * 4 + 64 + 1024;
 constexpr int kBwdThreads = 256;  // two threads per point
-
-template <int J>
-__device__ __forceinline__ void spline_dim_bwd(const BwdArgs &a, uint8_t *sG, int r, long long row, bool valid,
-                                               long long n, float gl) {
-    float th[kPerDim], g[kPerDim];
-#pragma unroll
-    for (int i = 0; i < kPerDim; ++i) th[i] = valid ? a.theta[(J * kPerDim + i) * n + row] : 0.f;
-    const float x = valid ? fminf(fmaxf(a.xin[a.L.trans[J] * n + row], 0.f), 1.f) : 0.5f;
-    const float gy = (valid && a.gout) ? a.gout[a.L.trans[J] * n + row] : 0.f;
-    const float gx = rqs_backward(th, x, gy, valid ? gl : 0.f, g);
-    if (valid) a.gin[a.L.trans[J] * n + row] = gx;
-#pragma unroll
-    for (int i = 0; i < kPerDim; ++i) {
-        const uint32_t pk = pack_bf16x2(valid ? g[i] : 0.f, 0.f);
-        *reinterpret_cast<uint16_t *>(sG + sw128_off(r, J * kPerDim + i, 128)) = static_cast<uint16_t>(pk & 0xFFFFu);
-    }
-}
 
 template <int DB>
 __global__ void __launch_bounds__(kBwdThreads, 1) k_flow_layer_bwd(BwdArgs a) {
@@ -533,17 +525,28 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_flow_layer_bwd(BwdArgs a) {
         const long long row = tile * 128 + r;
         const bool valid = row < n;
         const float gl = valid ? a.glogq[row] : 0.f;
-        // spline backward -> g_theta (bf16 tile, row r): dims 0, 2, 4 | 1, 3
-        if (half == 0) {
-            if (DB > 0) spline_dim_bwd<0>(a, sG, r, row, valid, n, gl);
-            if (DB > 2) spline_dim_bwd<2>(a, sG, r, row, valid, n, gl);
-            if (DB > 4) spline_dim_bwd<4>(a, sG, r, row, valid, n, gl);
-        } else {
-            if (DB > 1) spline_dim_bwd<1>(a, sG, r, row, valid, n, gl);
-            if (DB > 3) spline_dim_bwd<3>(a, sG, r, row, valid, n, gl);
+        // spline backward -> g_theta (bf16 tile, row r): dims 0, 2, 4 | 1, 3;
+        // one copy of the spline code, the dimension a runtime loop
+#pragma unroll 1
+        for (int j = half; j < DB; j += 2) {
+            const int b0 = j * kPerDim;
+            float th[kPerDim], g[kPerDim];
+#pragma unroll
+            for (int i = 0; i < kPerDim; ++i) th[i] = valid ? a.theta[(b0 + i) * n + row] : 0.f;
+            const int d = a.L.trans[j];
+            const float x = valid ? fminf(fmaxf(a.xin[d * n + row], 0.f), 1.f) : 0.5f;
+            const float gy = (valid && a.gout) ? a.gout[d * n + row] : 0.f;
+            const float gx = rqs_backward(th, x, gy, valid ? gl : 0.f, g);
+            if (valid) a.gin[d * n + row] = gx;
+#pragma unroll
+            for (int i = 0; i < kPerDim; ++i) {
+                const uint32_t pk = pack_bf16x2(valid ? g[i] : 0.f, 0.f);
+                *reinterpret_cast<uint16_t *>(sG + sw128_off(r, b0 + i, 128)) = static_cast<uint16_t>(pk & 0xFFFFu);
+            }
+        }
+        if (half == 1)
             for (int col = DB * kPerDim; col < kP; ++col)
                 *reinterpret_cast<uint16_t *>(sG + sw128_off(r, col, 128)) = 0;
-        }
         fence_async_smem();
         tc_fence_before();
         __syncthreads();
@@ -604,7 +607,7 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_flow_layer_bwd(BwdArgs a) {
                 if (c0 + j == kH - 1 || !valid) v[j] = 0.f;
             }
             store_row32(sP, 128, r, c0, v);
-#pragma unroll
+#pragma unroll 4
             for (int j = 0; j < 32; ++j) {
                 const int hcol = c0 + j;
                 const float gq = bf16_hi(pack_bf16x2(0.f, v[j]));
@@ -808,13 +811,14 @@ __global__ void k_flow_adam(float *__restrict__ prm, float *__restrict__ m, floa
     prm[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
 }
 
-// f32 master weights of one layer -> its bf16 tiles (zero padding).
-__global__ void k_flow_pack(const float *__restrict__ w1, const float *__restrict__ w2, const float *__restrict__ w3,
-                            int da, int P, uint8_t *__restrict__ wt) {
+// f32 master weights of one layer -> its bf16 tiles (zero padding); the W1
+// tile also carries E^T in columns 16..16+nch-1.
+__global__ void k_flow_pack(const float *__restrict__ w1, const float *__restrict__ E, const float *__restrict__ w2,
+                            const float *__restrict__ w3, int da, int nch, int P, uint8_t *__restrict__ wt) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < 128 * 64) {
         const int r = i / 64, c = i % 64;
-        const float v = c < da ? w1[r * da + c] : 0.f;
+        const float v = c < da ? w1[r * da + c] : ((c >= 16 && c < 16 + nch) ? E[(c - 16) * kH + r] : 0.f);
         *reinterpret_cast<uint16_t *>(wt + sw128_off(r, c, 128)) = static_cast<uint16_t>(pack_bf16x2(v, 0.f) & 0xFFFFu);
     }
     if (i < 128 * 128) {

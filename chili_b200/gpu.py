@@ -60,6 +60,7 @@ def _declare(lib):
         "chili_gpu_multichannel_iterate": ([vp, P(abi.MultiChannelParams), u64, u64, vp, i64, i32,
                                             P(abi.Stats), P(abi.MCIterInfo)], i32),
         "chili_gpu_get_training": ([vp, vp, vp], i32),
+        "chili_gpu_multichannel_train": ([vp, P(abi.MultiChannelParams), vp, vp], i32),
         "chili_gpu_generate": ([vp, i64, u64, u64, vp, vp, vp], i32),
         "chili_gpu_evaluate_batch": ([vp, i32, vp, vp, i64], i32),
         "chili_gpu_flow_init": ([vp, P(abi.FlowParams)], i32),
@@ -292,6 +293,10 @@ class Context:
         a = np.empty(self.nch)
         self.call("chili_gpu_get_training", _ptr(h), _ptr(a))
         return h, a
+
+    def multichannel_train(self, params, hist, alpha_train):
+        """Train from given (e.g. all-reduced) training data."""
+        self.call("chili_gpu_multichannel_train", C.byref(params), _ptr(_f64(hist)), _ptr(_f64(alpha_train)))
 
     def generate(self, n, seed=7, counter=0):
         mom = np.empty((n, self.n_ext, 4))

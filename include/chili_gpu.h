@@ -194,7 +194,11 @@ uint64_t chili_gpu_launch_count(const chili_ctx *ctx);
  * "pipeline_tile": points per tile of that pass (default 4194304).
  * "kernel_timing": 1 brackets the iteration's kernels with CUDA events on the
  * context's stream (totals read by chili_gpu_kernel_time; setting the option
- * resets them), 0 (default) records nothing. */
+ * resets them), 0 (default) records nothing.
+ * "defer_train": 1 makes an optimizing iteration collect its training data
+ * without applying Train, for a caller that sums the data over ranks first
+ * and then calls chili_gpu_multichannel_train (the reference's MPI mode);
+ * 0 (default) trains at the end of the iteration. */
 int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value);
 /* Total device time (ms) and launch count of one kernel class under the
  * "kernel_timing" option: k_mc_forward, k_pp_nodes, k_pp_items, k_pp_chains,
@@ -325,6 +329,16 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx,
 /* Per-channel training histograms [nch*dims*bins] and alpha-training sums
  * [nch] of the last iteration (before adaptation).  Host or device. */
 int chili_gpu_get_training(chili_ctx *ctx, double *hist, double *alpha_train);
+/* MultiChannel::Train (MultiChannel.hh:182-194) from given training data:
+ * channel-weight adaptation (MultiChannel.cc:109-136) from alpha_train [nch],
+ * grid adaptation (Integrand.hh:97-104) from hist [nch*dims*bins], best
+ * weights (MultiChannel.cc:138-154). With an iteration run at
+ * should_optimize = 0 and its own training data this equals the iteration's
+ * own training step; with the training data summed over ranks (one
+ * all-reduce) it is the reference's MPI mode (MultiChannel.hh:184-190), every
+ * rank adapting identically. Host or device. */
+int chili_gpu_multichannel_train(chili_ctx *ctx, const chili_multichannel_params *params, const double *hist,
+                                 const double *alpha_train);
 
 /* Event generation: MultiChannel::GeneratePoint + GenerateWeight
  * (MultiChannel.hh:141-165) for n points in counter order, with no PreProcess
@@ -349,8 +363,8 @@ int chili_gpu_evaluate_batch(chili_ctx *ctx, int ch, const double *u,
  * tensor-core products with f32 accumulation; f32 splines; FP64 phase space).
  * Estimator per point: v = alpha_c(p) f(p) dens_c(p) J / (beta_c q_c(u)) for
  * the channel c that generated it (c ~ beta, u ~ q_c, x = VEGAS_c(u),
- * p = FSMapper_c(x)). Requires channels, grids, integrand and channel weights
- * to be set; beta starts as the current channel weights.
+ * p = FSMapper_c(x)). Requires channels (at most 48), grids, integrand and
+ * channel weights to be set; beta starts as the current channel weights.
  *
  * Flat parameter layout (f32): per coupling layer l: W1 [128][da_l],
  * E [nch][128], W2 [128][128], W3 [db_l*49][128]; then the channel-weight

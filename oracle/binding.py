@@ -69,6 +69,8 @@ def _load(path, prefix):
         "ref_mc_weight": ([vp, vp, vp, i64, vp, vp, vp], None),
         "ref_mc_iterate": ([vp, vp, i64, i32, P(abi.Stats), P(abi.MCIterInfo)], i32),
         "ref_mc_get_training": ([vp, vp, vp], None),
+        "ref_mc_train": ([vp, vp, vp], None),
+        "ref_mc_set_defer": ([vp, i32], None),
         "ref_mc_dropped_dim0": ([vp], C.c_uint64),
         "ref_mc_run_native": ([vp, u32, i32, P(abi.Stats)], None),
         "ref_evaluate_batch": ([vp, i32, vp, i64, vp], None),
@@ -235,6 +237,15 @@ class MultiChannel:
         a = np.empty(self.nch)
         self.oracle().ref_mc_get_training(self.h, _p(h), _p(a))
         return h, a
+
+    def set_defer(self, defer=True):
+        """Collect the training data but leave Train to train() (the C port only)."""
+        self.oracle().ref_mc_set_defer(self.h, 1 if defer else 0)
+
+    def train(self, hist, atrain):
+        """Train from given training data (the C port only)."""
+        self.oracle().ref_mc_train(self.h, _p(np.ascontiguousarray(hist, dtype=np.float64)),
+                                   _p(np.ascontiguousarray(atrain, dtype=np.float64)))
 
     def run_native(self, seed, niter):
         st = abi.Stats()

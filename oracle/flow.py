@@ -258,7 +258,10 @@ def conditioner(spec, p, l, xa, ch, use_bf16=False):
     """theta [N, P] from the conditioning coordinates xa [N, Da] and channels."""
     H = spec.hidden
     a0 = 2 * xa - 1
-    pre1 = _mm(a0, p[f"W1_{l}"].T, use_bf16) + p[f"E_{l}"][ch]
+    # the GPU adds E[c] inside the first tensor-core product (a one-hot column),
+    # so in bf16 mode E is rounded like the other operands
+    E = bf16(p[f"E_{l}"]) if use_bf16 else p[f"E_{l}"]
+    pre1 = _mm(a0, p[f"W1_{l}"].T, use_bf16) + E[ch]
     h1 = lrelu(pre1)
     h1[:, H - 1] = 1.0
     pre2 = _mm(h1, p[f"W2_{l}"].T, use_bf16)

@@ -612,6 +612,7 @@ typedef struct {
     int fkind, pre;
     double fp[CHILI_MAX_INTEGRAND_PARAMS];
     double cut[4]; /* CHILI_PRE_CUTS: sqrts, ptmin, etamax, delta_r */
+    int defer;     /* collect the training data, leave Train to the caller */
     double *hist, *atrain;
 } mc_t;
 
@@ -779,6 +780,36 @@ static double eval_f(const mc_t *m, const v4 *mom) {
     return 1.0;
 }
 
+/* MultiChannel::Train (MultiChannel.hh:182-194): Adapt (MultiChannel.cc:109-136)
+ * from the alpha-training sums, Integrand::Train (Integrand.hh:97-104) from the
+ * per-channel histograms, MaxDifference (MultiChannel.cc:138-154). In the
+ * reference's MPI mode both inputs are the all-reduced sums of the ranks. */
+static void mc_train(mc_t *m, const double *train, const double *hist) {
+    int D = m->ndims, B = m->bins, nch = m->nch;
+    size_t gs = (size_t)D * (B + 1);
+    double nw[CHILI_MAX_CHANNELS], sw = 0, ns = 0;
+    for (int i = 0; i < nch; ++i) { nw[i] = m->alpha[i] * pow(train[i], m->prm.beta); sw += nw[i]; }
+    for (int i = 0; i < nch; ++i) {
+        if (nw[i] == 0) continue;
+        nw[i] /= sw;
+        nw[i] = dmax_(nw[i], m->prm.min_alpha);
+        ns += nw[i];
+    }
+    for (int i = 0; i < nch; ++i) m->alpha[i] = nw[i] / ns;
+    for (int c = 0; c < nch; ++c) {
+        const double *h = hist + (size_t)c * D * B;
+        int nz = 0;
+        for (int q = 0; q < D * B; ++q) nz |= h[q] != 0;
+        if (nz) am_adapt1(m->grids + c * gs, D, B, m->prm.grid_alpha, h);
+    }
+    double mx = 0;
+    for (int i = 0; i + 1 < nch; ++i)
+        for (int j = i + 1; j < nch; ++j) mx = dmax_(mx, fabs(train[i] - train[j]));
+    if (mx < m->min_diff) { memcpy(m->best, m->alpha, sizeof(double) * nch); m->min_diff = mx; }
+}
+void orc_mc_train(void *p, const double *hist, const double *atrain) { mc_train((mc_t *)p, atrain, hist); }
+void orc_mc_set_defer(void *p, int defer) { ((mc_t *)p)->defer = defer; }
+
 /* MultiChannel::operator() (MultiChannel.hh:196-251) on given uniforms, with
  * Train (:182-194) = Adapt (MultiChannel.cc:109-136), Integrand::Train
  * (Integrand.hh:97-104) and MaxDifference (MultiChannel.cc:138-154). */
@@ -835,27 +866,7 @@ int orc_mc_iterate(void *p, const double *u, int64_t n_u, int guard, chili_stats
     info->points_accepted = ncalls;
     info->points_weighted = ncalls + info->rejected_nan;
     memcpy(m->atrain, train, sizeof(double) * nch);
-    if (m->prm.should_optimize) {
-        double nw[CHILI_MAX_CHANNELS], sw = 0, ns = 0;
-        for (int i = 0; i < nch; ++i) { nw[i] = m->alpha[i] * pow(train[i], m->prm.beta); sw += nw[i]; }
-        for (int i = 0; i < nch; ++i) {
-            if (nw[i] == 0) continue;
-            nw[i] /= sw;
-            nw[i] = dmax_(nw[i], m->prm.min_alpha);
-            ns += nw[i];
-        }
-        for (int i = 0; i < nch; ++i) m->alpha[i] = nw[i] / ns;
-        for (int c = 0; c < nch; ++c) {
-            const double *h = m->hist + (size_t)c * D * B;
-            int nz = 0;
-            for (int q = 0; q < D * B; ++q) nz |= h[q] != 0;
-            if (nz) am_adapt1(m->grids + c * gs, D, B, m->prm.grid_alpha, h);
-        }
-        double mx = 0;
-        for (int i = 0; i + 1 < nch; ++i)
-            for (int j = i + 1; j < nch; ++j) mx = dmax_(mx, fabs(train[i] - train[j]));
-        if (mx < m->min_diff) { memcpy(m->best, m->alpha, sizeof(double) * nch); m->min_diff = mx; }
-    }
+    if (m->prm.should_optimize && !m->defer) mc_train(m, train, m->hist);
     free(train);
     st_out(&st, out);
     return 0;

@@ -84,3 +84,31 @@ def test_cut_preprocess_iteration_matches_oracle(ctx_factory):
         ctx.set_grids(O.get_grids())
         ctx.set_alpha(O.get_alpha()[0])
         counter += info.points_tried
+
+
+def test_deferred_train_equals_the_iteration_training(ctx_factory):
+    """defer_train + get_training + multichannel_train (the per-rank steps of
+    the MPI mode, here with one rank) leave the same grids and channel weights
+    as an iteration that trains itself."""
+    cs = workloads.channel_set(4)
+    res = []
+    for defer in (False, True):
+        ctx = ctx_factory()
+        ctx.set_channels(cs)
+        ctx.uniform_grids(cs.nch, ctx.ndims, 100)
+        ctx.set_integrand(abi.CHILI_FUNC_PROPAGATOR, channels.propagator_params())
+        ctx.set_preprocess(abi.CHILI_PRE_FINITE)
+        params = workloads.mc_params(50_000)
+        if defer:
+            ctx.set_option("defer_train", 1)
+        counter = 0
+        for it in range(2):
+            st, info = ctx.multichannel_iterate(params, seed=17, counter=counter)
+            counter += info.points_tried
+            if defer:
+                h, a = ctx.get_training()
+                ctx.multichannel_train(params, h, a)
+        res.append((ctx.get_grids(), ctx.get_alpha()[0], st.as_tuple()))
+    assert np.array_equal(res[0][0], res[1][0])
+    assert np.array_equal(res[0][1], res[1][1])
+    assert res[0][2] == res[1][2]
