@@ -522,6 +522,14 @@ int chili_gpu_set_channels(chili_ctx *ctx, const chili_channel_desc *descs, int 
     ctx->n_ext = n_ext;
     ctx->ndims = progs[0].ndims;
     ctx->sqrts = sqrts;
+    ctx->ch_info.assign(nch, {});
+    ctx->ch_decays.assign(nch, {});
+    ctx->ch_ptmin.assign(nch, {});
+    for (int k = 0; k < nch; ++k) {
+        ctx->ch_info[k].assign(descs[k].info, descs[k].info + descs[k].n_info);
+        ctx->ch_decays[k].assign(descs[k].decays, descs[k].decays + descs[k].n_decays);
+        ctx->ch_ptmin[k].assign(progs[k].info_ptmin, progs[k].info_ptmin + progs[k].n_info);
+    }
     {
         std::vector<PointProgram> pp(1);
         ctx->have_pp = build_point_program(progs, pp[0]);

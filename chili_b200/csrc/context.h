@@ -119,6 +119,13 @@ struct chili_ctx {
     std::vector<cudaEvent_t> event_pool;
     double ktime_ms[16] = {0};
     unsigned long long klaunches[16] = {0};
+    // channel descriptions as given (checkpoint.cu writes them back) and the
+    // FSMapper ptmin list of every channel (Channel.hh:20-26)
+    std::vector<std::vector<chili_particle_info>> ch_info;
+    std::vector<std::vector<chili_decay>> ch_decays;
+    std::vector<std::vector<double>> ch_ptmin;
+    // MultiChannelSummary::best_weights as last loaded (written back unchanged)
+    std::vector<double> summary_best;
     // learned proposal (flow.cu)
     FlowState *flow = nullptr;
 };

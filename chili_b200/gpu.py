@@ -61,6 +61,8 @@ def _declare(lib):
                                             P(abi.Stats), P(abi.MCIterInfo)], i32),
         "chili_gpu_get_training": ([vp, vp, vp], i32),
         "chili_gpu_multichannel_train": ([vp, P(abi.MultiChannelParams), vp, vp], i32),
+        "chili_gpu_save_checkpoint": ([vp, C.c_char_p, P(abi.MultiChannelParams), vp, i64], i32),
+        "chili_gpu_load_checkpoint": ([vp, C.c_char_p, P(abi.MultiChannelParams), vp, i64, P(i64)], i32),
         "chili_gpu_generate": ([vp, i64, u64, u64, vp, vp, vp], i32),
         "chili_gpu_evaluate_batch": ([vp, i32, vp, vp, i64], i32),
         "chili_gpu_flow_init": ([vp, P(abi.FlowParams)], i32),
@@ -297,6 +299,23 @@ class Context:
     def multichannel_train(self, params, hist, alpha_train):
         """Train from given (e.g. all-reduced) training data."""
         self.call("chili_gpu_multichannel_train", C.byref(params), _ptr(_f64(hist)), _ptr(_f64(alpha_train)))
+
+    def save_checkpoint(self, path, params, results=()):
+        """The reference's results.chili (MultiChannel::SaveAs)."""
+        res = (abi.Stats * max(len(results), 1))()
+        for k, s in enumerate(results):
+            res[k] = s if isinstance(s, abi.Stats) else abi.Stats(*s)
+        self.call("chili_gpu_save_checkpoint", str(path).encode(), C.byref(params), C.cast(res, C.c_void_p),
+                  len(results))
+
+    def load_checkpoint(self, path, max_results=4096):
+        """MultiChannel::LoadFrom; returns (params, [Stats])."""
+        p = abi.MultiChannelParams.defaults()
+        res = (abi.Stats * max_results)()
+        n = C.c_int64()
+        self.call("chili_gpu_load_checkpoint", str(path).encode(), C.byref(p), C.cast(res, C.c_void_p), max_results,
+                  C.byref(n))
+        return p, [res[k] for k in range(min(n.value, max_results))]
 
     def generate(self, n, seed=7, counter=0):
         mom = np.empty((n, self.n_ext, 4))

@@ -340,6 +340,22 @@ int chili_gpu_get_training(chili_ctx *ctx, double *hist, double *alpha_train);
 int chili_gpu_multichannel_train(chili_ctx *ctx, const chili_multichannel_params *params, const double *hist,
                                  const double *alpha_train);
 
+/* MultiChannel::SaveAs / LoadFrom (MultiChannel.hh:65-84): the reference's
+ * binary results.chili (Integrand::Serialize, then MultiChannel::Serialize)
+ * written from / read into this context, so that a grid trained by the
+ * reference resumes here and vice versa. Save writes the channel set, grids,
+ * params (the 8 serialised fields), best weights, min_diff and the given
+ * per-iteration StatsData list. Load checks that the file's channels equal
+ * the context's channel set, then sets grids, channel weights = best weights
+ * (as the reference's Deserialize does) and min_diff; params (optional)
+ * receives the file's params (should_optimize = 1, grid_alpha and iteration
+ * kept), results (optional, up to max_results) the StatsData list and
+ * nresults (optional) its length. */
+int chili_gpu_save_checkpoint(chili_ctx *ctx, const char *path, const chili_multichannel_params *params,
+                              const chili_stats *results, int64_t nresults);
+int chili_gpu_load_checkpoint(chili_ctx *ctx, const char *path, chili_multichannel_params *params,
+                              chili_stats *results, int64_t max_results, int64_t *nresults);
+
 /* Event generation: MultiChannel::GeneratePoint + GenerateWeight
  * (MultiChannel.hh:141-165) for n points in counter order, with no PreProcess
  * and no retry.  mom[n*n_ext*4], wgt[n] = f*w (0 if not finite), ch[n];

@@ -71,6 +71,8 @@ def _load(path, prefix):
         "ref_mc_get_training": ([vp, vp, vp], None),
         "ref_mc_train": ([vp, vp, vp], None),
         "ref_mc_set_defer": ([vp, i32], None),
+        "ref_mc_save": ([vp, C.c_char_p], i32),
+        "ref_mc_load": ([vp, C.c_char_p], i32),
         "ref_mc_dropped_dim0": ([vp], C.c_uint64),
         "ref_mc_run_native": ([vp, u32, i32, P(abi.Stats)], None),
         "ref_evaluate_batch": ([vp, i32, vp, i64, vp], None),
@@ -237,6 +239,14 @@ class MultiChannel:
         a = np.empty(self.nch)
         self.oracle().ref_mc_get_training(self.h, _p(h), _p(a))
         return h, a
+
+    def save(self, path):
+        """MultiChannel::SaveAs (the reference build only)."""
+        assert self.oracle().ref_mc_save(self.h, str(path).encode()) == 0
+
+    def load(self, path):
+        """MultiChannel::LoadFrom (the reference build only)."""
+        assert self.oracle().ref_mc_load(self.h, str(path).encode()) == 0
 
     def set_defer(self, defer=True):
         """Collect the training data but leave Train to train() (the C port only)."""

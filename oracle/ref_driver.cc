@@ -378,6 +378,17 @@ void ref_mc_set_cuts(void *p, double sqrts, double ptmin, double etamax, double 
     };
 }
 
+// MultiChannel::SaveAs / LoadFrom (MultiChannel.hh:65-84), the reference's
+// own serialisation.
+int ref_mc_save(void *p, const char *path) {
+    auto *h = static_cast<MC *>(p);
+    return h->mc.SaveAs(h->integrand, std::string(path)) ? 0 : 1;
+}
+int ref_mc_load(void *p, const char *path) {
+    auto *h = static_cast<MC *>(p);
+    return h->mc.LoadFrom(h->integrand, std::string(path)) ? 0 : 1;
+}
+
 void ref_mc_set_grids(void *p, const double *edges) {
     auto *h = static_cast<MC *>(p);
     const size_t per = static_cast<size_t>(h->ndims) * (h->bins + 1);

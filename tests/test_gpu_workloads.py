@@ -109,6 +109,8 @@ def test_deferred_train_equals_the_iteration_training(ctx_factory):
                 h, a = ctx.get_training()
                 ctx.multichannel_train(params, h, a)
         res.append((ctx.get_grids(), ctx.get_alpha()[0], st.as_tuple()))
-    assert np.array_equal(res[0][0], res[1][0])
+    # the histograms are summed with atomics (order varies in the last bits
+    # between runs); the channel weights and StatsData use ordered sums
+    assert np.allclose(res[0][0], res[1][0], rtol=1e-12, atol=1e-15)
     assert np.array_equal(res[0][1], res[1][1])
     assert res[0][2] == res[1][2]
