@@ -132,6 +132,25 @@ class FlowIterInfo(C.Structure):
                 ("weight_max", C.c_double), ("unweighting_efficiency", C.c_double)]
 
 
+CHILI_TASK_CAMEL = 0
+CHILI_TASK_MULTICHANNEL = 1
+
+
+class Task(C.Structure):
+    """chili_task (batched integrands)."""
+    _fields_ = [("kind", C.c_int32), ("dims", C.c_int32), ("bins", C.c_int32), ("ncalls", C.c_uint64),
+                ("grid_alpha", C.c_double), ("beta", C.c_double), ("min_alpha", C.c_double),
+                ("fkind", C.c_int32), ("nparams", C.c_int32), ("params", C.POINTER(C.c_double)),
+                ("pre", C.c_int32), ("nch", C.c_int32), ("descs", C.POINTER(ChannelDesc)),
+                ("cuts", C.POINTER(Cuts)), ("sqrts", C.c_double), ("n_ext", C.c_int32),
+                ("pre_cuts", C.c_double * 4)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("block", C.c_uint32), ("points_per_thread", C.c_uint32), ("ms_per_iteration", C.c_double),
+                ("units", C.c_uint64), ("points", C.c_uint64)]
+
+
 class ChannelSet:
     """Owns ctypes arrays for a list of channel descriptions and one Cuts
     table, keeping them alive while a library call reads them."""

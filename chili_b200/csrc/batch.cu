@@ -1,0 +1,671 @@
+// batch.cu -- many independent integrations in one persistent launch per
+// iteration (include/chili_gpu.h, "batched integrands"; no counterpart in
+// the reference, which integrates one Integrand per MultiChannel/Vegas
+// object).
+//
+// A task is either a camel function integrated by plain VEGAS
+// (Vegas::operator(), Vegas.cc:18-52: ncalls points, f*J, per-bin (f J)^2
+// histogram, AdaptiveMap::Adapt) or a multichannel FSMapper integrand with
+// the combined weight of all its channels (Integrand::GenerateWeight,
+// Integrand.hh:112-123), its channel histograms and alpha training
+// (MultiChannel.hh:167-194), on a fixed budget of ncalls drawn points per
+// iteration (PreProcess rejections count as zero-valued calls; there is no
+// retry loop in the batched mode).
+//
+// Work units are tiles of blockDim * points_per_thread points of one task;
+// a persistent grid (resident blocks of every SM) pulls units from an atomic
+// counter, so tasks of 1e4 and 1e6 points share the machine without one
+// launch per task. Per unit one StatsData partial; per task an ordered fold
+// of its partials (deterministic), then the channel-weight update and a
+// batched grid adaptation over every (task, channel, dimension). The
+// iteration (resets, evaluation, folds, adaptation, iteration counter) is
+// captured once in a CUDA graph and replayed; block size and points per
+// thread are chosen by timing the candidates on the first call.
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "channel_program.h"
+#include "context.h"
+
+using namespace chili_dev;
+
+namespace {
+
+// Channels per multichannel task (the per-thread channel densities live in
+// local memory).
+constexpr int kBatchMaxCh = 64;
+
+struct BatchTask {
+    int32_t kind, dims, bins, nch;
+    long long ncalls;
+    long long unit0, units;    // first work unit, number of units
+    long long grid_off;        // doubles: nch * dims * (bins+1)
+    long long hist_off;        // doubles: nch * dims * bins
+    int32_t ch_off;            // first ChannelProgram / channel-weight slot
+    int32_t desc;              // IntegrandDesc index
+    double grid_alpha, beta, min_alpha;
+    uint64_t key;              // Philox key of the task
+};
+
+struct BatchDev {
+    const BatchTask *tasks;
+    int ntasks;
+    const long long *unit_task;  // first unit of every task (ascending), size ntasks
+    long long nunits;
+    const ChannelProgram *progs;
+    const IntegrandDesc *descs;
+    double *grids, *grids_new, *hist, *atrain;  // atrain per channel slot
+    double *alpha, *best, *mindiff, *cp;        // per channel slot; mindiff per task
+    double *part;                              // [nunits][6]
+    double *stats;                             // [iter slot][ntasks][6]
+    int stat_slots;
+    unsigned long long *next_unit;
+    unsigned long long *iter;
+    int ppt;
+};
+
+__device__ __forceinline__ int unit_to_task(const long long *first, int n, long long u) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (first[mid] <= u) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// One iteration's evaluation: persistent blocks pull units.
+__global__ void __launch_bounds__(256) k_batch_eval(BatchDev B) {
+    __shared__ long long s_unit;
+    __shared__ double ws[8][6];
+    const uint64_t iter = *B.iter;
+    const int t = threadIdx.x;
+    for (;;) {
+        if (t == 0) s_unit = static_cast<long long>(atomicAdd(B.next_unit, 1ull));
+        __syncthreads();
+        const long long u = s_unit;
+        __syncthreads();
+        if (u >= B.nunits) break;
+        const int ti = unit_to_task(B.unit_task, B.ntasks, u);
+        const BatchTask T = B.tasks[ti];
+        const IntegrandDesc *f = B.descs + T.desc;
+        const long long tile = static_cast<long long>(blockDim.x) * B.ppt;
+        const long long p0 = (u - T.unit0) * tile;
+        const int D = T.dims, bins = T.bins;
+        const size_t gsz = static_cast<size_t>(D) * (bins + 1);
+        double cnt = 0, sum = 0, sum2 = 0, mn = 1.7976931348623157e308, mx = 2.2250738585072014e-308, nf = 0;
+        for (int q = 0; q < B.ppt; ++q) {
+            const long long i = p0 + static_cast<long long>(q) * blockDim.x + t;
+            if (i >= T.ncalls) break;
+            const uint64_t ctr = (iter << 32) + static_cast<uint64_t>(i);
+            double r[CHILI_MAX_DIMS + 1];
+            double val;
+            if (T.kind == CHILI_TASK_CAMEL) {
+                load_uniforms(T.key, ctr, nullptr, D, r);
+                const double *g = B.grids + T.grid_off;
+                double jac;
+                if (grid_map_checked(g, D, bins, r, jac)) val = camel(f, r, D) * jac;
+                else val = CUDART_NAN;
+                const double v2 = val * val;
+                double *H = B.hist + T.hist_off;
+                for (int j = 0; j < D; ++j) {
+                    const int bj = find_bin(g + j * (bins + 1), bins, r[j]);
+                    const int s = j * bins + bj;
+                    if (s >= 0) atomicAdd(H + s, v2);
+                }
+            } else {
+                load_uniforms(T.key, ctr, nullptr, D + 1, r);
+                const double *cp = B.cp + T.ch_off;
+                const int c = select_channel(cp, T.nch, r[D]);
+                const double *grids = B.grids + T.grid_off;
+                double jac;
+                val = 0;
+                if (grid_map_checked(grids + c * gsz, D, bins, r, jac)) {
+                    const ChannelProgram *progs = B.progs + T.ch_off;
+                    V4 mom[CHILI_MAX_SLOTS];
+                    double m2[CHILI_MAX_SLOTS];
+                    fs_generate(progs + c, r, mom, m2);
+                    if (preprocess(f, mom)) {
+                        double x[CHILI_MAX_DIMS], xs[CHILI_MAX_DIMS], dens[kBatchMaxCh];
+                        const double w = combined_weight(progs, grids, B.alpha + T.ch_off, T.nch, D, bins, c, mom,
+                                                         x, xs, dens, 1);
+                        const double fv = eval_momenta(f, mom, progs[0].n_ext);
+                        val = w == 0 ? 0 : fv * w;
+                        if (isnan(val)) val = 0;  // a retry in the reference; a zero call here
+                        if (val != 0) {
+                            // AddTrainData (MultiChannel.hh:167-180), non-finite terms dropped
+                            const double v2 = val * val;
+                            double *H = B.hist + T.hist_off + static_cast<size_t>(c) * D * bins;
+                            const double *g = grids + c * gsz;
+                            for (int j = 0; j < D; ++j) {
+                                const int bj = find_bin(g + j * (bins + 1), bins, xs[j]);
+                                if (j * bins + bj >= 0) atomicAdd(H + j * bins + bj, v2);
+                            }
+                            for (int k = 0; k < T.nch; ++k) {
+                                const double tk = v2 * w / dens[k];
+                                if (isfinite(tk)) atomicAdd(B.atrain + T.ch_off + k, tk);
+                            }
+                        }
+                    }
+                }
+            }
+            cnt += 1;
+            sum += val;
+            sum2 += val * val;
+            mn = std_min(mn, val);
+            mx = std_max(mx, val);
+            nf += (val != 0);
+        }
+        cnt = warp_sum(cnt);
+        sum = warp_sum(sum);
+        sum2 = warp_sum(sum2);
+        mn = warp_min(mn);
+        mx = warp_max(mx);
+        nf = warp_sum(nf);
+        const int w = t >> 5, l = t & 31;
+        if (l == 0) {
+            ws[w][0] = cnt; ws[w][1] = mn; ws[w][2] = mx; ws[w][3] = sum; ws[w][4] = sum2; ws[w][5] = nf;
+        }
+        __syncthreads();
+        if (t == 0) {
+            double a[6] = {ws[0][0], ws[0][1], ws[0][2], ws[0][3], ws[0][4], ws[0][5]};
+            for (int k = 1; k < static_cast<int>(blockDim.x >> 5); ++k) {
+                a[0] += ws[k][0]; a[1] = std_min(a[1], ws[k][1]); a[2] = std_max(a[2], ws[k][2]);
+                a[3] += ws[k][3]; a[4] += ws[k][4]; a[5] += ws[k][5];
+            }
+            for (int k = 0; k < 6; ++k) B.part[u * 6 + k] = a[k];
+        }
+        __syncthreads();
+    }
+}
+
+// Per task (one block of kFoldThreads each): fold of its unit partials into
+// the StatsData of this iteration (thread t takes units t, t + kFoldThreads,
+// ... in order, then a fixed tree: deterministic); multichannel tasks then
+// update their channel weights (MultiChannel::Adapt + MaxDifference,
+// MultiChannel.hh:100-140) when adapting.
+constexpr int kFoldThreads = 128;
+
+__global__ void __launch_bounds__(kFoldThreads) k_batch_finalize(BatchDev B, int adapt) {
+    __shared__ double sh[6][kFoldThreads];
+    const int ti = blockIdx.x, t = threadIdx.x;
+    const BatchTask T = B.tasks[ti];
+    double a[6] = {0, 1.7976931348623157e308, 2.2250738585072014e-308, 0, 0, 0};
+    for (long long u = T.unit0 + t; u < T.unit0 + T.units; u += kFoldThreads) {
+        const double *p = B.part + u * 6;
+        a[0] += p[0];
+        a[1] = std_min(a[1], p[1]);
+        a[2] = std_max(a[2], p[2]);
+        a[3] += p[3];
+        a[4] += p[4];
+        a[5] += p[5];
+    }
+    for (int k = 0; k < 6; ++k) sh[k][t] = a[k];
+    __syncthreads();
+    for (int w = kFoldThreads / 2; w > 0; w >>= 1) {
+        if (t < w) {
+            sh[0][t] += sh[0][t + w];
+            sh[1][t] = std_min(sh[1][t], sh[1][t + w]);
+            sh[2][t] = std_max(sh[2][t], sh[2][t + w]);
+            sh[3][t] += sh[3][t + w];
+            sh[4][t] += sh[4][t + w];
+            sh[5][t] += sh[5][t + w];
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        const uint64_t slot = *B.iter % static_cast<uint64_t>(B.stat_slots);
+        double *o = B.stats + (slot * B.ntasks + ti) * 6;
+        for (int k = 0; k < 6; ++k) o[k] = sh[k][0];
+        if (adapt && T.kind == CHILI_TASK_MULTICHANNEL)
+            alpha_update(B.alpha + T.ch_off, B.best + T.ch_off, B.mindiff + ti, B.cp + T.ch_off,
+                         B.atrain + T.ch_off, T.nch, T.beta, T.min_alpha, 1);
+    }
+}
+
+// Grid adaptation of every (task, channel, dimension): one block each.
+struct AdaptJob {
+    int32_t task, ch, dim, pad;
+};
+
+__global__ void k_batch_adapt(BatchDev B, const AdaptJob *__restrict__ jobs, int njobs, int *status) {
+    extern __shared__ double tmp[];
+    const int j = blockIdx.x;
+    if (j >= njobs) return;
+    const AdaptJob J = jobs[j];
+    const BatchTask T = B.tasks[J.task];
+    // plain VEGAS adapts every grid; MultiChannel::Train skips channels
+    // that received no training data
+    grid_adapt_block(B.grids + T.grid_off, B.grids_new + T.grid_off, T.dims, T.bins, T.grid_alpha,
+                     B.hist + T.hist_off, T.kind == CHILI_TASK_MULTICHANNEL ? 1 : 0, status, J.dim, J.ch, tmp);
+}
+
+__global__ void k_batch_commit(BatchDev B, const AdaptJob *__restrict__ jobs, int njobs) {
+    // copy the adapted edges back (grids_new -> grids), one block per job
+    const int j = blockIdx.x;
+    if (j >= njobs) return;
+    const AdaptJob J = jobs[j];
+    const BatchTask T = B.tasks[J.task];
+    const size_t off = T.grid_off + (static_cast<size_t>(J.ch) * T.dims + J.dim) * (T.bins + 1);
+    for (int k = threadIdx.x; k <= T.bins; k += blockDim.x) B.grids[off + k] = B.grids_new[off + k];
+}
+
+__global__ void k_batch_next(BatchDev B) {
+    if (threadIdx.x == 0) {
+        *B.next_unit = 0;
+        *B.iter += 1;
+    }
+}
+
+}  // namespace
+
+struct BatchState {
+    std::vector<BatchTask> tasks;
+    std::vector<long long> unit_first;
+    std::vector<AdaptJob> jobs;
+    int max_bins = 2, nslots = 0;
+    long long total_points = 0, nunits = 0;
+    DevBuf d_tasks, d_first, d_progs, d_descs, d_grids, d_grids_new, d_hist, d_atrain, d_alpha, d_best, d_mindiff,
+        d_cp, d_part, d_stats, d_counters, d_jobs, d_status;
+    int block = 0, ppt = 0, grid_blocks = 0;
+    bool tuned = false;
+    cudaGraphExec_t graph = nullptr;
+    int graph_adapt = -1;
+    double last_ms = 0;
+    size_t hist_doubles = 0;
+    int nslots_alloc = 0;
+};
+
+namespace {
+
+int need_batch(chili_ctx *ctx) {
+    if (!ctx->batch) return fail(ctx, CHILI_ERR_STATE, "no batch set (chili_gpu_batch_set)");
+    return CHILI_OK;
+}
+
+BatchDev batch_dev(chili_ctx *ctx) {
+    BatchState &S = *ctx->batch;
+    BatchDev B{};
+    B.tasks = S.d_tasks.as<BatchTask>();
+    B.ntasks = static_cast<int>(S.tasks.size());
+    B.unit_task = S.d_first.as<long long>();
+    B.nunits = S.nunits;
+    B.progs = S.d_progs.as<ChannelProgram>();
+    B.descs = S.d_descs.as<IntegrandDesc>();
+    B.grids = S.d_grids.as<double>();
+    B.grids_new = S.d_grids_new.as<double>();
+    B.hist = S.d_hist.as<double>();
+    B.atrain = S.d_atrain.as<double>();
+    B.alpha = S.d_alpha.as<double>();
+    B.best = S.d_best.as<double>();
+    B.mindiff = S.d_mindiff.as<double>();
+    B.cp = S.d_cp.as<double>();
+    B.part = S.d_part.as<double>();
+    B.stats = S.d_stats.as<double>();
+    B.stat_slots = S.nslots_alloc;
+    B.next_unit = S.d_counters.as<unsigned long long>();
+    B.iter = S.d_counters.as<unsigned long long>() + 1;
+    B.ppt = S.ppt;
+    return B;
+}
+
+// Work-unit layout for a block size and points per thread.
+int layout_units(chili_ctx *ctx, int block, int ppt) {
+    BatchState &S = *ctx->batch;
+    long long u = 0;
+    S.unit_first.assign(S.tasks.size(), 0);
+    for (size_t k = 0; k < S.tasks.size(); ++k) {
+        const long long tile = static_cast<long long>(block) * ppt;
+        S.tasks[k].unit0 = u;
+        S.tasks[k].units = (S.tasks[k].ncalls + tile - 1) / tile;
+        S.unit_first[k] = u;
+        u += S.tasks[k].units;
+    }
+    S.nunits = u;
+    CK(S.d_tasks.ensure(sizeof(BatchTask) * S.tasks.size()));
+    CK(cudaMemcpyAsync(S.d_tasks.p, S.tasks.data(), sizeof(BatchTask) * S.tasks.size(), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(S.d_first.ensure(sizeof(long long) * S.unit_first.size()));
+    CK(cudaMemcpyAsync(S.d_first.p, S.unit_first.data(), sizeof(long long) * S.unit_first.size(),
+                       cudaMemcpyHostToDevice, ctx->stream));
+    CK(S.d_part.ensure(sizeof(double) * 6 * u));
+    CK(cudaStreamSynchronize(ctx->stream));
+    S.block = block;
+    S.ppt = ppt;
+    int per_sm = 1, sms = 148;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_eval, block, 0);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    S.grid_blocks = std::max(1, per_sm) * sms;
+    return CHILI_OK;
+}
+
+// The iteration as a stream of launches (captured into the graph).
+int enqueue_iteration(chili_ctx *ctx, bool adapt) {
+    BatchState &S = *ctx->batch;
+    CK(cudaMemsetAsync(S.d_hist.p, 0, sizeof(double) * S.hist_doubles, ctx->stream));
+    CK(cudaMemsetAsync(S.d_atrain.p, 0, S.d_atrain.cap, ctx->stream));
+    BatchDev B = batch_dev(ctx);
+    k_batch_eval<<<S.grid_blocks, S.block, 0, ctx->stream>>>(B);
+    LAUNCHED();
+    k_batch_finalize<<<static_cast<unsigned>(S.tasks.size()), kFoldThreads, 0, ctx->stream>>>(B, adapt ? 1 : 0);
+    LAUNCHED();
+    if (adapt && !S.jobs.empty()) {
+        k_batch_adapt<<<static_cast<unsigned>(S.jobs.size()), 32, sizeof(double) * S.max_bins, ctx->stream>>>(
+            B, S.d_jobs.as<AdaptJob>(), static_cast<int>(S.jobs.size()), S.d_status.as<int>());
+        LAUNCHED();
+        k_batch_commit<<<static_cast<unsigned>(S.jobs.size()), 128, 0, ctx->stream>>>(
+            B, S.d_jobs.as<AdaptJob>(), static_cast<int>(S.jobs.size()));
+        LAUNCHED();
+    }
+    k_batch_next<<<1, 32, 0, ctx->stream>>>(B);
+    LAUNCHED();
+    return CHILI_OK;
+}
+
+// Block size and points per thread: the fastest evaluation pass among the
+// candidates (the evaluation accumulates into buffers that every iteration
+// resets; the iteration counter is not advanced).
+int autotune(chili_ctx *ctx) {
+    BatchState &S = *ctx->batch;
+    const int cand[][2] = {{128, 1}, {128, 2}, {256, 1}, {256, 2}, {256, 4}, {128, 4}};
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int bb = 128, bp = 1;
+    for (const auto &c : cand) {
+        if (int rc = layout_units(ctx, c[0], c[1])) return rc;
+        BatchDev B = batch_dev(ctx);
+        for (int rep = 0; rep < 2; ++rep) {  // first pass warms up
+            CK(cudaMemsetAsync(S.d_counters.p, 0, sizeof(unsigned long long), ctx->stream));
+            CK(cudaEventRecord(e0, ctx->stream));
+            k_batch_eval<<<S.grid_blocks, S.block, 0, ctx->stream>>>(B);
+            LAUNCHED();
+            CK(cudaEventRecord(e1, ctx->stream));
+            CK(cudaEventSynchronize(e1));
+        }
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) {
+            best = ms;
+            bb = c[0];
+            bp = c[1];
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CK(cudaMemsetAsync(S.d_counters.p, 0, sizeof(unsigned long long), ctx->stream));
+    return layout_units(ctx, bb, bp);
+}
+
+int capture(chili_ctx *ctx, bool adapt) {
+    BatchState &S = *ctx->batch;
+    if (S.graph) {
+        cudaGraphExecDestroy(S.graph);
+        S.graph = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    const unsigned long long launches = ctx->launches;  // replays are counted, not the capture
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = enqueue_iteration(ctx, adapt);
+    ctx->launches = launches;
+    cudaGraph_t captured = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &captured);
+    if (rc) {
+        if (captured) cudaGraphDestroy(captured);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(ctx, CHILI_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    g = captured;
+    CK(cudaGraphInstantiate(&S.graph, g, 0));
+    cudaGraphDestroy(g);
+    S.graph_adapt = adapt ? 1 : 0;
+    return CHILI_OK;
+}
+
+}  // namespace
+
+void batch_release(chili_ctx *ctx) {
+    if (!ctx || !ctx->batch) return;
+    BatchState &S = *ctx->batch;
+    if (S.graph) cudaGraphExecDestroy(S.graph);
+    for (DevBuf *b : {&S.d_tasks, &S.d_first, &S.d_progs, &S.d_descs, &S.d_grids, &S.d_grids_new, &S.d_hist,
+                      &S.d_atrain, &S.d_alpha, &S.d_best, &S.d_mindiff, &S.d_cp, &S.d_part, &S.d_stats,
+                      &S.d_counters, &S.d_jobs, &S.d_status})
+        b->release();
+    delete ctx->batch;
+    ctx->batch = nullptr;
+}
+
+extern "C" {
+
+int chili_gpu_batch_set(chili_ctx *ctx, const chili_task *tasks, int ntasks) {
+    if (!ctx || !tasks || ntasks < 1 || ntasks > (1 << 20)) return fail(ctx, CHILI_ERR_INVALID_ARG, "1..2^20 tasks");
+    if (int rc = set_device(ctx)) return rc;
+    batch_release(ctx);
+    ctx->batch = new BatchState();
+    BatchState &S = *ctx->batch;
+    std::vector<ChannelProgram> progs;
+    std::vector<IntegrandDesc> descs;
+    std::vector<double> grids, alpha;
+    long long goff = 0, hoff = 0;
+    for (int k = 0; k < ntasks; ++k) {
+        const chili_task &t = tasks[k];
+        BatchTask T{};
+        T.kind = t.kind;
+        T.bins = t.bins;
+        T.ncalls = static_cast<long long>(t.ncalls);
+        T.grid_alpha = t.grid_alpha;
+        T.beta = t.beta;
+        T.min_alpha = t.min_alpha;
+        T.key = 0;
+        IntegrandDesc d{};
+        if (t.bins < 2 || t.bins > CHILI_MAX_BINS || t.ncalls < 1 || t.ncalls >= (1ull << 32)) {
+            batch_release(ctx);
+            return fail(ctx, CHILI_ERR_INVALID_ARG, "task " + std::to_string(k) + ": bins in [2, max], ncalls in [1, 2^32)");
+        }
+        if (t.kind == CHILI_TASK_CAMEL) {
+            if (t.dims < 1 || t.dims > CHILI_MAX_DIMS || t.nparams != 2 + 2 * t.dims || !t.params) {
+                batch_release(ctx);
+                return fail(ctx, CHILI_ERR_INVALID_ARG, "task " + std::to_string(k) + ": camel needs 2 + 2 dims params");
+            }
+            T.dims = t.dims;
+            T.nch = 1;
+            d.kind = CHILI_FUNC_CAMEL;
+            d.nparams = t.nparams;
+            for (int i = 0; i < t.nparams; ++i) d.p[i] = t.params[i];
+            T.ch_off = static_cast<int32_t>(alpha.size());
+            alpha.push_back(1.0);
+        } else if (t.kind == CHILI_TASK_MULTICHANNEL) {
+            std::vector<ChannelProgram> p;
+            const std::string why = build_channel_programs(t.descs, t.nch, t.cuts, t.sqrts, t.n_ext, p);
+            if (!why.empty()) {
+                batch_release(ctx);
+                return fail(ctx, CHILI_ERR_INVALID_ARG, "task " + std::to_string(k) + ": " + why);
+            }
+            const int need = t.fkind == CHILI_FUNC_UNIT ? 0 : 3;
+            const bool fk_ok = t.fkind == CHILI_FUNC_UNIT || t.fkind == CHILI_FUNC_PROPAGATOR ||
+                               t.fkind == CHILI_FUNC_PROPAGATOR_TOP2;
+            const bool pre_ok = t.pre == CHILI_PRE_ACCEPT_ALL || t.pre == CHILI_PRE_FINITE ||
+                                (t.pre == CHILI_PRE_CUTS && t.pre_cuts[0] > 0 && t.pre_cuts[1] >= 0 &&
+                                 t.pre_cuts[2] >= 0 && t.pre_cuts[3] >= 0);
+            if (!fk_ok || !pre_ok || t.nch > kBatchMaxCh || t.nparams < need ||
+                t.nparams > CHILI_MAX_INTEGRAND_PARAMS || (t.nparams > 0 && !t.params)) {
+                batch_release(ctx);
+                return fail(ctx, CHILI_ERR_INVALID_ARG,
+                            "task " + std::to_string(k) +
+                                ": phase-space integrand kind and parameters, preprocess kind and cut values, "
+                                "at most 64 channels");
+            }
+            T.dims = p[0].ndims;
+            T.nch = t.nch;
+            T.ch_off = static_cast<int32_t>(alpha.size());
+            for (int c = 0; c < t.nch; ++c) alpha.push_back(1.0 / t.nch);
+            for (auto &q : p) progs.push_back(q);
+            d.kind = t.fkind;
+            d.nparams = t.nparams;
+            for (int i = 0; i < t.nparams; ++i) d.p[i] = t.params[i];
+            d.pre = t.pre;
+            d.n_ext = t.n_ext;
+            for (int i = 0; i < 4; ++i) d.cut[i] = t.pre == CHILI_PRE_CUTS ? t.pre_cuts[i] : 0.0;
+        } else {
+            batch_release(ctx);
+            return fail(ctx, CHILI_ERR_INVALID_ARG, "task " + std::to_string(k) + ": unknown kind");
+        }
+        if (t.kind == CHILI_TASK_CAMEL) {
+            // an unused program keeps programs and channel slots on one index
+            progs.emplace_back();
+            std::memset(&progs.back(), 0, sizeof(ChannelProgram));
+        }
+        T.desc = static_cast<int32_t>(descs.size());
+        descs.push_back(d);
+        T.grid_off = goff;
+        T.hist_off = hoff;
+        const long long per = static_cast<long long>(T.dims) * (T.bins + 1);
+        for (int c = 0; c < T.nch; ++c)
+            for (int dd = 0; dd < T.dims; ++dd)
+                for (int b = 0; b <= T.bins; ++b) grids.push_back(static_cast<double>(b) / T.bins);
+        goff += per * T.nch;
+        hoff += static_cast<long long>(T.dims) * T.bins * T.nch;
+        S.max_bins = std::max(S.max_bins, T.bins);
+        for (int c = 0; c < T.nch; ++c)
+            for (int dd = 0; dd < T.dims; ++dd) S.jobs.push_back(AdaptJob{k, c, dd, 0});
+        S.tasks.push_back(T);
+        S.total_points += T.ncalls;
+    }
+    const size_t nslot = alpha.size();
+    S.hist_doubles = static_cast<size_t>(hoff);
+    CK(S.d_progs.ensure(sizeof(ChannelProgram) * progs.size()));
+    CK(cudaMemcpyAsync(S.d_progs.p, progs.data(), sizeof(ChannelProgram) * progs.size(), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(S.d_descs.ensure(sizeof(IntegrandDesc) * descs.size()));
+    CK(cudaMemcpyAsync(S.d_descs.p, descs.data(), sizeof(IntegrandDesc) * descs.size(), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(S.d_grids.ensure(sizeof(double) * grids.size()));
+    CK(S.d_grids_new.ensure(sizeof(double) * grids.size()));
+    CK(cudaMemcpyAsync(S.d_grids.p, grids.data(), sizeof(double) * grids.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CK(S.d_hist.ensure(sizeof(double) * std::max<size_t>(S.hist_doubles, 1)));
+    CK(S.d_atrain.ensure(sizeof(double) * nslot));
+    CK(S.d_alpha.ensure(sizeof(double) * nslot));
+    CK(cudaMemcpyAsync(S.d_alpha.p, alpha.data(), sizeof(double) * nslot, cudaMemcpyHostToDevice, ctx->stream));
+    std::vector<double> nanv(nslot, NAN), inf(ntasks, INFINITY);
+    CK(S.d_best.ensure(sizeof(double) * nslot));
+    CK(cudaMemcpyAsync(S.d_best.p, nanv.data(), sizeof(double) * nslot, cudaMemcpyHostToDevice, ctx->stream));
+    CK(S.d_mindiff.ensure(sizeof(double) * ntasks));
+    CK(cudaMemcpyAsync(S.d_mindiff.p, inf.data(), sizeof(double) * ntasks, cudaMemcpyHostToDevice, ctx->stream));
+    CK(S.d_cp.ensure(sizeof(double) * nslot));
+    // the channel-selection table of the initial weights, in the order of
+    // operations of alpha_update
+    std::vector<double> cp(nslot, 1.0);
+    for (const auto &T : S.tasks) {
+        if (T.nch < 2) continue;
+        double sa = 0, c = 0;
+        for (int i = 0; i < T.nch; ++i) sa += alpha[T.ch_off + i];
+        for (int i = 0; i < T.nch; ++i) {
+            const double p = alpha[T.ch_off + i] / sa;
+            c = (i == 0) ? p : c + p;
+            cp[T.ch_off + i] = c;
+        }
+        cp[T.ch_off + T.nch - 1] = 1.0;
+    }
+    CK(cudaMemcpyAsync(S.d_cp.p, cp.data(), sizeof(double) * nslot, cudaMemcpyHostToDevice, ctx->stream));
+    CK(S.d_counters.ensure(sizeof(unsigned long long) * 2));
+    CK(cudaMemsetAsync(S.d_counters.p, 0, sizeof(unsigned long long) * 2, ctx->stream));
+    CK(S.d_jobs.ensure(sizeof(AdaptJob) * std::max<size_t>(S.jobs.size(), 1)));
+    CK(cudaMemcpyAsync(S.d_jobs.p, S.jobs.data(), sizeof(AdaptJob) * S.jobs.size(), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(S.d_status.ensure(sizeof(int)));
+    CK(cudaMemsetAsync(S.d_status.p, 0, sizeof(int), ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return layout_units(ctx, 256, 1);
+}
+
+int chili_gpu_batch_iterate(chili_ctx *ctx, int iterations, uint64_t seed, int adapt, chili_stats *stats,
+                            chili_batch_info *info) {
+    if (!ctx || iterations < 1 || iterations > 100000) return fail(ctx, CHILI_ERR_INVALID_ARG, "iterations in [1, 1e5]");
+    if (int rc = need_batch(ctx)) return rc;
+    if (int rc = set_device(ctx)) return rc;
+    BatchState &S = *ctx->batch;
+    const int nt = static_cast<int>(S.tasks.size());
+    // Philox key of task k: seed + k (the task's own stream)
+    bool keys_changed = false;
+    for (int k = 0; k < nt; ++k) {
+        const uint64_t key = seed + static_cast<uint64_t>(k);
+        keys_changed = keys_changed || S.tasks[k].key != key;
+        S.tasks[k].key = key;
+    }
+    if (keys_changed) {
+        CK(cudaMemcpyAsync(S.d_tasks.p, S.tasks.data(), sizeof(BatchTask) * nt, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    if (!S.tuned) {
+        if (int rc = autotune(ctx)) return rc;
+        S.tuned = true;
+    }
+    if (S.nslots_alloc < iterations) {
+        CK(S.d_stats.ensure(sizeof(double) * 6 * static_cast<size_t>(iterations) * nt));
+        S.nslots_alloc = iterations;
+        if (S.graph) {
+            cudaGraphExecDestroy(S.graph);
+            S.graph = nullptr;
+        }
+    }
+    if (!S.graph || S.graph_adapt != (adapt ? 1 : 0))
+        if (int rc = capture(ctx, adapt != 0)) return rc;
+    unsigned long long iter0 = 0;
+    CK(cudaMemcpyAsync(&iter0, S.d_counters.as<unsigned long long>() + 1, sizeof(iter0), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, ctx->stream));
+    for (int it = 0; it < iterations; ++it) CK(cudaGraphLaunch(S.graph, ctx->stream));
+    CK(cudaEventRecord(e1, ctx->stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ctx->launches += static_cast<unsigned long long>(iterations) * (adapt && !S.jobs.empty() ? 5 : 3);
+    S.last_ms = ms / iterations;
+    if (stats) {
+        std::vector<double> all(6 * static_cast<size_t>(S.nslots_alloc) * nt);
+        CK(cudaMemcpy(all.data(), S.d_stats.p, sizeof(double) * all.size(), cudaMemcpyDeviceToHost));
+        for (int it = 0; it < iterations; ++it) {
+            const uint64_t slot = (iter0 + it) % static_cast<uint64_t>(S.nslots_alloc);
+            for (int k = 0; k < nt; ++k) {
+                const double *o = all.data() + (slot * nt + k) * 6;
+                chili_stats &s = stats[static_cast<size_t>(it) * nt + k];
+                s.n = o[0]; s.min = o[1]; s.max = o[2]; s.sum = o[3]; s.sum2 = o[4]; s.n_finite = o[5];
+            }
+        }
+    }
+    if (info) {
+        info->block = static_cast<uint32_t>(S.block);
+        info->points_per_thread = static_cast<uint32_t>(S.ppt);
+        info->ms_per_iteration = S.last_ms;
+        info->units = static_cast<uint64_t>(S.nunits);
+        info->points = static_cast<uint64_t>(S.total_points);
+    }
+    return CHILI_OK;
+}
+
+int chili_gpu_batch_get_grid(chili_ctx *ctx, int task, double *edges, double *alpha) {
+    if (!ctx) return fail(ctx, CHILI_ERR_INVALID_ARG, "NULL argument");
+    if (int rc = need_batch(ctx)) return rc;
+    BatchState &S = *ctx->batch;
+    if (task < 0 || task >= static_cast<int>(S.tasks.size())) return fail(ctx, CHILI_ERR_INVALID_ARG, "task index");
+    const BatchTask &T = S.tasks[task];
+    const size_t n = static_cast<size_t>(T.nch) * T.dims * (T.bins + 1);
+    if (edges) CK(cudaMemcpy(edges, S.d_grids.as<double>() + T.grid_off, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    if (alpha) CK(cudaMemcpy(alpha, S.d_alpha.as<double>() + T.ch_off, sizeof(double) * T.nch, cudaMemcpyDeviceToHost));
+    return CHILI_OK;
+}
+
+}  // extern "C"

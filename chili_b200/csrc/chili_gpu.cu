@@ -192,6 +192,7 @@ int chili_gpu_destroy(chili_ctx *ctx) {
                       &ctx->v_hist, &ctx->v_train, &ctx->v_out, &ctx->rec, &ctx->ctl3};
     for (DevBuf *b : bufs) b->release();
     flow_release(ctx);
+    batch_release(ctx);
     for (auto &b : ctx->stage) b.release();
     if (ctx->ctl_host) cudaFreeHost(ctx->ctl_host);
     collect_times(ctx);

@@ -56,9 +56,12 @@ constexpr int kStageSlots = 6;
 }  // namespace
 
 struct FlowState;
+struct BatchState;
 struct chili_ctx;
 // Frees the learned proposal's state (flow.cu).
 void flow_release(chili_ctx *ctx);
+// Frees the batched integrands' state (batch.cu).
+void batch_release(chili_ctx *ctx);
 // Launches the last step of one tile of the phased weight pass (base = first
 // listed point of the tile, T = tile capacity).
 using TileFn = std::function<int(long long base, long long T)>;
@@ -128,6 +131,7 @@ struct chili_ctx {
     std::vector<double> summary_best;
     // learned proposal (flow.cu)
     FlowState *flow = nullptr;
+    BatchState *batch = nullptr;
 };
 
 namespace {

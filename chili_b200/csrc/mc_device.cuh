@@ -1,8 +1,11 @@
 // mc_device.cuh -- types and device helpers shared by the kernels of
 // libchili_b200 (kernels.cuh, pipeline.cuh, flow_phys.cuh): iteration
 // accumulator and round records, the channel-selection rule, the checked
-// grid map and the counter-based uniforms.
+// grid map, the counter-based uniforms, the combined channel weight, the
+// channel-weight update and the grid adaptation of one dimension.
 #pragma once
+
+#include <math_constants.h>
 
 #include "channel_program.h"
 #include "common.cuh"
@@ -93,6 +96,143 @@ __device__ __forceinline__ void load_uniforms(uint64_t seed, uint64_t k, const d
             out[2 * q] = a;
             if (2 * q + 1 < n) out[2 * q + 1] = b;
         }
+    }
+}
+
+// ------------------------------------------------- shared by several kernels
+// Integrand::GenerateWeight (Integrand.hh:112-123) for one point.  The
+// uniform buffer x is shared by all channels and not cleared between them,
+// as the reference's _rans; the chosen channel's copy lands in xs.
+__device__ __forceinline__ double combined_weight(const ChannelProgram *__restrict__ progs,
+                                                  const double *__restrict__ grids, const double *__restrict__ alpha,
+                                                  int nch, int dims, int bins, int ich, V4 *mom, double *x,
+                                                  double *xs, double *dens, int dens_stride) {
+    for (int d = 0; d < dims; ++d) x[d] = 0.0;
+    double acc = 0;
+    const size_t gsz = static_cast<size_t>(dims) * (bins + 1);
+    const double before = edge_before_table(dims, bins);
+    for (int c = 0; c < nch; ++c) {
+        const double dc = fs_weight(progs + c, mom, x);
+        if (c == ich)
+            for (int d = 0; d < dims; ++d) xs[d] = x[d];
+        const double vw = grid_weight(grids + c * gsz, dims, bins, x, before);
+        acc += __ldg(alpha + c) / dc / vw;
+        if (dens) dens[static_cast<size_t>(c) * dens_stride] = dc;
+    }
+    return 1.0 / acc;
+}
+
+
+__device__ __forceinline__ void alpha_update(double *__restrict__ alpha, double *__restrict__ best, double *__restrict__ min_diff,
+                               double *__restrict__ cp, const double *__restrict__ train, int nch, double beta,
+                               double min_alpha, int mode) {
+    if (mode == 1) {
+        double nw[CHILI_MAX_CHANNELS];
+        double sum_w = 0;
+        for (int i = 0; i < nch; ++i) {
+            nw[i] = alpha[i] * pow(train[i], beta);
+            sum_w += nw[i];
+        }
+        double new_sum = 0;
+        for (int i = 0; i < nch; ++i) {
+            if (nw[i] == 0) continue;
+            nw[i] /= sum_w;
+            nw[i] = std_max(nw[i], min_alpha);
+            new_sum += nw[i];
+        }
+        for (int i = 0; i < nch; ++i) alpha[i] = nw[i] / new_sum;
+        double mx = 0;
+        for (int i = 0; i + 1 < nch; ++i)
+            for (int j = i + 1; j < nch; ++j) mx = std_max(mx, fabs(train[i] - train[j]));
+        if (mx < *min_diff) {
+            for (int i = 0; i < nch; ++i) best[i] = alpha[i];
+            *min_diff = mx;
+        }
+    }
+    if (nch >= 2) {
+        double s = 0;
+        for (int i = 0; i < nch; ++i) s += alpha[i];
+        double c = 0;
+        for (int i = 0; i < nch; ++i) {
+            const double p = alpha[i] / s;
+            c = (i == 0) ? p : c + p;
+            cp[i] = c;
+        }
+        cp[nch - 1] = 1.0;
+    }
+}
+
+
+// AdaptiveMap::Adapt (AdaptiveMap.cc:67-125) of dimension d of grid c, one
+// block (tmp: bins doubles of shared memory).
+__device__ __forceinline__ void grid_adapt_block(const double *__restrict__ g_old, double *__restrict__ g_new, int dims,
+                                                 int bins, double alpha, const double *__restrict__ train, int skip_zero,
+                                                 int *__restrict__ status, int d, int c, double *tmp) {
+    const double *T = train + static_cast<size_t>(c) * dims * bins;
+    const double *E = g_old + static_cast<size_t>(c) * dims * (bins + 1);
+    double *EN = g_new + static_cast<size_t>(c) * dims * (bins + 1);
+    const double *Ed = E + d * (bins + 1);
+    double *ENd = EN + d * (bins + 1);
+    if (skip_zero) {
+        int nz = 0;
+        for (int k = threadIdx.x; k < dims * bins; k += blockDim.x) nz |= (T[k] != 0);
+        nz = __syncthreads_or(nz);
+        if (!nz) {
+            for (int k = threadIdx.x; k <= bins; k += blockDim.x) ENd[k] = Ed[k];
+            return;
+        }
+    }
+    const double *o = T + d * bins;
+    for (int b = threadIdx.x; b < bins; b += blockDim.x) {
+        double s;
+        if (b == 0) s = (o[0] + o[1]) / 2;
+        else if (b == bins - 1) s = (o[bins - 2] + o[bins - 1]) / 2;
+        else s = ((o[b - 1] + o[b]) + o[b + 1]) / 3;
+        tmp[b] = s;
+    }
+    __syncthreads();
+    __shared__ double norm_s;
+    if (threadIdx.x == 0) {
+        double norm = 0;
+        for (int b = 0; b < bins; ++b) norm = (b == 0) ? tmp[0] : norm + tmp[b];
+        norm_s = norm;
+    }
+    __syncthreads();
+    const double norm = norm_s;
+    if (norm == 0) {  // the reference leaves this dimension of new_hist at zero
+        for (int k = threadIdx.x; k <= bins; k += blockDim.x) ENd[k] = 0.0;
+        return;
+    }
+    for (int b = threadIdx.x; b < bins; b += blockDim.x) {
+        if (tmp[b] != 0) {
+            const double r = tmp[b] / norm;
+            tmp[b] = pow((r - 1.0) / log(r), alpha);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double avg = 0;
+        for (int b = 0; b < bins; ++b) avg += tmp[b];
+        avg /= static_cast<double>(bins);
+        double cbin = 0;
+        int ibin = 0;
+        int bad = 0;
+        const double nan = CUDART_NAN;
+        ENd[0] = 0.0;
+        for (int nb = 1; nb < bins; ++nb) {
+            while (cbin < avg && ibin < bins) cbin += tmp[ibin++];
+            if (cbin < avg) bad = 1;  // the reference would read past the histogram
+            const int flat_prev = d * (bins + 1) + ibin - 1;
+            const double prev = flat_prev >= 0 ? E[flat_prev] : nan;
+            const double curr = Ed[ibin];
+            if (ibin == 0) bad = 1;
+            cbin -= avg;
+            const double delta = (curr - prev) * cbin;
+            const double t = ibin > 0 ? tmp[ibin - 1] : nan;
+            ENd[nb] = curr - delta / t;
+        }
+        ENd[bins] = 1.0;
+        if (bad) atomicOr(status, 1);
     }
 }
 

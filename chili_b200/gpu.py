@@ -77,6 +77,9 @@ def _declare(lib):
         "chili_gpu_flow_train": ([vp, i32, u64, u64, vp], i32),
         "chili_gpu_flow_iterate": ([vp, u64, u64, u64, i32, P(abi.Stats), P(abi.FlowIterInfo)], i32),
         "chili_gpu_tc_selftest": ([vp, i32, i32, i32, vp, vp, vp], i32),
+        "chili_gpu_batch_set": ([vp, P(abi.Task), i32], i32),
+        "chili_gpu_batch_iterate": ([vp, i32, u64, i32, vp, P(abi.BatchInfo)], i32),
+        "chili_gpu_batch_get_grid": ([vp, i32, vp, vp], i32),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(lib, name)
@@ -399,6 +402,67 @@ class Context:
         out = np.empty((128, N), dtype=np.float32)
         self.call("chili_gpu_tc_selftest", mode, K, N, _ptr(A), _ptr(B), _ptr(out))
         return out
+
+
+    # ------------------------------------------------ batched integrands
+    def batch_set(self, tasks):
+        """tasks: list of dicts, {"kind": "camel", "dims", "bins", "ncalls",
+        "params", "grid_alpha"} or {"kind": "multichannel", "channels":
+        ChannelSet, "bins", "ncalls", "fkind", "params", "pre", "pre_cuts",
+        "grid_alpha", "beta", "min_alpha"}."""
+        arr = (abi.Task * len(tasks))()
+        keep = []
+        shapes = []
+        for k, t in enumerate(tasks):
+            T = arr[k]
+            T.bins = int(t.get("bins", 50))
+            T.ncalls = int(t["ncalls"])
+            T.grid_alpha = float(t.get("grid_alpha", 1.5))
+            T.beta = float(t.get("beta", 0.25))
+            T.min_alpha = float(t.get("min_alpha", 1e-5))
+            prm = np.ascontiguousarray(t.get("params", []), dtype=np.float64)
+            keep.append(prm)
+            T.nparams = prm.size
+            T.params = prm.ctypes.data_as(C.POINTER(C.c_double)) if prm.size else None
+            if t["kind"] == "camel":
+                T.kind = abi.CHILI_TASK_CAMEL
+                T.dims = int(t["dims"])
+                shapes.append((1, T.dims, T.bins))
+            else:
+                cs = t["channels"]
+                keep.append(cs)
+                T.kind = abi.CHILI_TASK_MULTICHANNEL
+                T.fkind = int(t.get("fkind", abi.CHILI_FUNC_PROPAGATOR))
+                T.pre = int(t.get("pre", abi.CHILI_PRE_FINITE))
+                for i, v in enumerate(t.get("pre_cuts", (0.0, 0.0, 0.0, 0.0))):
+                    T.pre_cuts[i] = float(v)
+                T.nch = cs.nch
+                T.descs = C.cast(cs.descs, C.POINTER(abi.ChannelDesc))
+                T.cuts = C.pointer(cs.cuts)
+                T.sqrts = cs.sqrts
+                T.n_ext = cs.n_ext
+                shapes.append((cs.nch, cs.ndims, T.bins))
+        self._batch_shapes = []
+        self.call("chili_gpu_batch_set", arr, len(tasks))
+        self._batch_shapes = shapes
+        return shapes
+
+    def batch_iterate(self, iterations=1, seed=42, adapt=True):
+        """-> (stats [iterations, ntasks, 6] as n, min, max, sum, sum2,
+        n_finite; BatchInfo)."""
+        nt = len(getattr(self, "_batch_shapes", []))
+        st = np.empty((iterations, max(nt, 1), 6), dtype=np.float64)
+        info = abi.BatchInfo()
+        self.call("chili_gpu_batch_iterate", int(iterations), int(seed), 1 if adapt else 0, _ptr(st),
+                  C.byref(info))
+        return st, info
+
+    def batch_get_grid(self, task):
+        nch, dims, bins = self._batch_shapes[task]
+        edges = np.empty((nch, dims, bins + 1), dtype=np.float64)
+        alpha = np.empty(nch, dtype=np.float64)
+        self.call("chili_gpu_batch_get_grid", int(task), _ptr(edges), _ptr(alpha))
+        return edges, alpha
 
 
 def flow_layout(dims, nch, n_ext, layers=6):

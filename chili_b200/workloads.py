@@ -3,6 +3,7 @@
 camel_params      the D-dim camel with unit integral (VEGAS workload)
 MC_2TO4           2->4 propagator integrand, 15 channels, 100 bins, 1e6/iter
 MC_2TO6           2->6, 45 channels, 200 bins, 1e7/iter
+batched_tasks     512 uneven integrands for one batched launch
 uniforms53        53-bit uniforms k*2^-53 (exactly representable in the
                   reference's generate_canonical, so both sides see them)
 """
@@ -58,3 +59,34 @@ def uniforms53(rng, shape):
     """Uniforms k * 2^-53 in [0, 1)."""
     k = rng.integers(0, 2 ** 53, size=shape, dtype=np.uint64)
     return k.astype(np.float64) * 2.0 ** -53
+
+
+def batched_tasks(seed=2024, n_camel=256, n_mc=256, camel_bins=50, mc_bins=50):
+    """The batched workload: n_camel camel functions of dimension 2..12
+    (sigma uniform in [0.05, 0.2], centres uniform in [0.2, 0.8], grid alpha
+    1.5) and n_mc 2->n propagator integrands (n = 2..5, sqrt(S) uniform in
+    [200, 2000] GeV, M and Gamma of the Z, channel weights adapted), each with
+    a point count log-uniform in [1e4, 1e6]; task dicts for
+    gpu.Context.batch_set."""
+    rng = np.random.default_rng(seed)
+    tasks = []
+    sets = {}
+    for _ in range(n_camel):
+        dims = int(rng.integers(2, 13))
+        sigma = float(rng.uniform(0.05, 0.2))
+        a, b = rng.uniform(0.2, 0.8, dims), rng.uniform(0.2, 0.8, dims)
+        tasks.append({"kind": "camel", "dims": dims, "bins": camel_bins, "grid_alpha": 1.5,
+                      "ncalls": int(round(10 ** rng.uniform(4, 6))), "params": camel_params(dims, sigma, a, b)})
+    mp = abi.MultiChannelParams.defaults()
+    for _ in range(n_mc):
+        n_out = int(rng.integers(2, 6))
+        sqrts = float(rng.uniform(200.0, 2000.0))
+        key = (n_out, sqrts)
+        if key not in sets:
+            sets[key] = channel_set(n_out, sqrts)
+        tasks.append({"kind": "multichannel", "channels": sets[key], "bins": mc_bins,
+                      "ncalls": int(round(10 ** rng.uniform(4, 6))), "grid_alpha": mp.grid_alpha,
+                      "beta": mp.beta, "min_alpha": mp.min_alpha, "fkind": abi.CHILI_FUNC_PROPAGATOR,
+                      "params": channels.propagator_params(), "pre": abi.CHILI_PRE_FINITE})
+    return tasks
+

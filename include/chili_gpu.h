@@ -439,6 +439,64 @@ int chili_gpu_flow_iterate(chili_ctx *ctx, uint64_t ncalls, uint64_t seed, uint6
  * in [16, 256]. Host buffers. */
 int chili_gpu_tc_selftest(chili_ctx *ctx, int mode, int K, int N, const float *A, const float *B, float *C);
 
+/* ------------------------------------------------------ batched integrands
+ * Many independent integrations advanced together: one persistent launch
+ * evaluates the points of every task per iteration, one graph replays the
+ * whole iteration (evaluation, per-task StatsData folds, channel-weight
+ * updates, grid adaptation).  No counterpart in the reference, which runs one
+ * Vegas or MultiChannel object per integrand (Vegas.cc:18-52,
+ * MultiChannel.hh:184-260); each task follows that object's algorithm with a
+ * fixed budget of ncalls drawn points per iteration: points that PreProcess
+ * rejects, or whose value is NaN, count as calls of value 0 (no retries).
+ * Task k draws its uniforms from the Philox stream of key seed + k, counter
+ * (iteration << 32) + point: a camel task's iteration i equals
+ * chili_gpu_vegas_iterate(seed + k, counter_base = i << 32) on the same grid. */
+enum chili_task_kind {
+    CHILI_TASK_CAMEL = 0,        /* plain VEGAS of the camel (CHILI_FUNC_CAMEL) */
+    CHILI_TASK_MULTICHANNEL = 1  /* FSMapper channels + multichannel weights     */
+};
+
+typedef struct {
+    int32_t kind;           /* chili_task_kind                                  */
+    int32_t dims;           /* camel: dimensions (multichannel: from n_ext)      */
+    int32_t bins;           /* bins of every grid of the task, [2, MAX_BINS]     */
+    uint64_t ncalls;        /* points per iteration, [1, 2^32)                   */
+    double grid_alpha;      /* AdaptiveMap::Adapt exponent (VegasParams::alpha)  */
+    double beta;            /* MultiChannel::Adapt beta (multichannel)           */
+    double min_alpha;       /* MultiChannel::Adapt floor (multichannel)          */
+    int32_t fkind;          /* chili_integrand_kind (multichannel)               */
+    int32_t nparams;
+    const double *params;   /* camel: {s, N, a[dims], b[dims]}                   */
+    int32_t pre;            /* chili_preprocess_kind (multichannel)              */
+    int32_t nch;            /* channels (multichannel)                           */
+    const chili_channel_desc *descs;
+    const chili_cuts *cuts;
+    double sqrts;
+    int32_t n_ext;
+    double pre_cuts[4];     /* CHILI_PRE_CUTS: sqrts, ptmin, etamax, delta_r     */
+} chili_task;
+
+typedef struct {
+    uint32_t block;             /* threads per block of the evaluation launch  */
+    uint32_t points_per_thread; /* points per thread per work unit             */
+    double ms_per_iteration;    /* device time per iteration of the last call  */
+    uint64_t units;             /* work units per iteration                    */
+    uint64_t points;            /* points per iteration, all tasks             */
+} chili_batch_info;
+
+/* Replace the context's batch with ntasks tasks (uniform grids, equal channel
+ * weights).  Host arrays. */
+int chili_gpu_batch_set(chili_ctx *ctx, const chili_task *tasks, int ntasks);
+/* `iterations` iterations of every task (adapt != 0: grids and channel
+ * weights adapt after each); stats[iterations * ntasks] (host, may be NULL)
+ * receives each iteration's StatsData, task-minor.  The first call picks the
+ * block size and points per thread by timing the candidates. */
+int chili_gpu_batch_iterate(chili_ctx *ctx, int iterations, uint64_t seed, int adapt, chili_stats *stats,
+                            chili_batch_info *info);
+/* Task `task`'s grids edges[nch * dims * (bins + 1)] and channel weights
+ * alpha[nch] (host, either may be NULL). */
+int chili_gpu_batch_get_grid(chili_ctx *ctx, int task, double *edges, double *alpha);
+
 #ifdef __cplusplus
 }
 #endif

@@ -71,6 +71,7 @@ def _load(path, prefix):
         "ref_mc_get_training": ([vp, vp, vp], None),
         "ref_mc_train": ([vp, vp, vp], None),
         "ref_mc_set_defer": ([vp, i32], None),
+        "ref_mc_set_fixed_budget": ([vp, i32], None),
         "ref_mc_save": ([vp, C.c_char_p], i32),
         "ref_mc_load": ([vp, C.c_char_p], i32),
         "ref_mc_dropped_dim0": ([vp], C.c_uint64),
@@ -251,6 +252,11 @@ class MultiChannel:
     def set_defer(self, defer=True):
         """Collect the training data but leave Train to train() (the C port only)."""
         self.oracle().ref_mc_set_defer(self.h, 1 if defer else 0)
+
+    def set_fixed_budget(self, on=True):
+        """Every drawn point counts as a call, no retries: the semantics of
+        the CUDA library's batched integrands (the C port only)."""
+        self.oracle().ref_mc_set_fixed_budget(self.h, 1 if on else 0)
 
     def train(self, hist, atrain):
         """Train from given training data (the C port only)."""

@@ -613,6 +613,7 @@ typedef struct {
     double fp[CHILI_MAX_INTEGRAND_PARAMS];
     double cut[4]; /* CHILI_PRE_CUTS: sqrts, ptmin, etamax, delta_r */
     int defer;     /* collect the training data, leave Train to the caller */
+    int fixed;     /* fixed budget: rejected and NaN points are calls of value 0, no retry */
     double *hist, *atrain;
 } mc_t;
 
@@ -809,6 +810,10 @@ static void mc_train(mc_t *m, const double *train, const double *hist) {
 }
 void orc_mc_train(void *p, const double *hist, const double *atrain) { mc_train((mc_t *)p, atrain, hist); }
 void orc_mc_set_defer(void *p, int defer) { ((mc_t *)p)->defer = defer; }
+/* The batched integrands' semantics (not the reference's): every drawn point
+ * is one of the ncalls calls, PreProcess rejections and NaN values included
+ * as calls of value 0; MultiChannel.hh:219-236 otherwise. */
+void orc_mc_set_fixed_budget(void *p, int on) { ((mc_t *)p)->fixed = on; }
 
 /* MultiChannel::operator() (MultiChannel.hh:196-251) on given uniforms, with
  * Train (:182-194) = Adapt (MultiChannel.cc:109-136), Integrand::Train
@@ -836,7 +841,7 @@ int orc_mc_iterate(void *p, const double *u, int64_t n_u, int guard, chili_stats
         if (am_map1(m->grids + ich * gs, D, B, x, &jac)) fs_gen(&m->ch[ich], x, mom);
         else for (int s = 0; s < m->n_ext; ++s) { v4 z = {NAN, NAN, NAN, NAN}; mom[s] = z; }
         if (!preprocess_ok(m, mom)) {
-            --i;
+            if (!m->fixed) --i;
             st_add(&st, 0);
             info->rejected_pre++;
             continue;
@@ -844,7 +849,7 @@ int orc_mc_iterate(void *p, const double *u, int64_t n_u, int guard, chili_stats
         double wgt = combined(m, mom, ich, dens, xs);
         double f = eval_f(m, mom);
         double val = wgt == 0 ? 0 : f * wgt;
-        if (isnan(val)) { val = wgt = 0; --i; info->rejected_nan++; }
+        if (isnan(val)) { val = wgt = 0; if (!m->fixed) --i; info->rejected_nan++; }
         if (m->prm.should_optimize) {
             double v2 = val * val;
             double *h = m->hist + (size_t)ich * D * B;

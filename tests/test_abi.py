@@ -53,6 +53,8 @@ int main(void) {
   S(chili_flow_params) S(chili_flow_iter_info) O(chili_flow_params, init_seed) O(chili_flow_iter_info, unweighting_efficiency)
   O(chili_multichannel_params, should_optimize) O(chili_multichannel_params, grid_alpha)
   O(chili_cuts, etamax) O(chili_mc_iter_info, weight_max) O(chili_mc_iter_info, points_weighted)
+  S(chili_task) S(chili_batch_info) O(chili_task, ncalls) O(chili_task, params) O(chili_task, descs)
+  O(chili_task, sqrts) O(chili_task, n_ext) O(chili_task, pre_cuts) O(chili_batch_info, points)
   return 0;
 }''')
     exe = tmp_path / "layout"
@@ -62,7 +64,7 @@ int main(void) {
               "chili_idx_value": abi.IdxValue, "chili_pid_pair_value": abi.PidPairValue, "chili_cuts": abi.Cuts,
               "chili_stats": abi.Stats, "chili_multichannel_params": abi.MultiChannelParams,
               "chili_mc_iter_info": abi.MCIterInfo, "chili_flow_params": abi.FlowParams,
-              "chili_flow_iter_info": abi.FlowIterInfo}
+              "chili_flow_iter_info": abi.FlowIterInfo, "chili_task": abi.Task, "chili_batch_info": abi.BatchInfo}
     for name, cls in mirror.items():
         assert int(got[name]) == C.sizeof(cls), name
     assert int(got["chili_multichannel_params.should_optimize"]) == abi.MultiChannelParams.should_optimize.offset
@@ -72,6 +74,9 @@ int main(void) {
     assert int(got["chili_mc_iter_info.points_weighted"]) == abi.MCIterInfo.points_weighted.offset
     assert int(got["chili_flow_params.init_seed"]) == abi.FlowParams.init_seed.offset
     assert int(got["chili_flow_iter_info.unweighting_efficiency"]) == abi.FlowIterInfo.unweighting_efficiency.offset
+    for f in ("ncalls", "params", "descs", "sqrts", "n_ext", "pre_cuts"):
+        assert int(got["chili_task." + f]) == getattr(abi.Task, f).offset, f
+    assert int(got["chili_batch_info.points"]) == abi.BatchInfo.points.offset
 
 
 def test_header_limits_match_the_mirror():

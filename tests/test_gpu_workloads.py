@@ -110,7 +110,10 @@ def test_deferred_train_equals_the_iteration_training(ctx_factory):
                 ctx.multichannel_train(params, h, a)
         res.append((ctx.get_grids(), ctx.get_alpha()[0], st.as_tuple()))
     # the histograms are summed with atomics (order varies in the last bits
-    # between runs); the channel weights and StatsData use ordered sums
+    # between runs), so the adapted grids of the first iteration, and with
+    # them the points of the second, agree to rounding only
     assert np.allclose(res[0][0], res[1][0], rtol=1e-12, atol=1e-15)
-    assert np.array_equal(res[0][1], res[1][1])
-    assert res[0][2] == res[1][2]
+    assert np.allclose(res[0][1], res[1][1], rtol=1e-10, atol=0)
+    st0, st1 = res[0][2], res[1][2]
+    assert st0[0] == st1[0] and st0[5] == st1[5]
+    assert _close(st0[3], st1[3], 1e-10) and _close(st0[4], st1[4], 1e-10)
