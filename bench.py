@@ -3,6 +3,7 @@
 implementation of the same workload.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl chili|reference]
+                    [--workload multichannel|batched]
 
 One step = one MultiChannel::operator() iteration: 1e6 accepted points
 (generation, PreProcess, combined weight over all 15 channels, integrand,
@@ -14,6 +15,10 @@ plain path, the learned proposal (spline flow + channel-weight network) is
 trained on the GPU and measured on the same integrand; the line reports both
 paths and selects the one with the lower variance x time per point.  Rank 0
 prints one JSON line.
+
+--workload batched: 512 uneven integrands (camel functions and 2->n
+multichannel integrands) advanced together, one persistent graph-replayed
+launch per iteration; one step = one adapting iteration of every task.
 """
 import argparse
 import json
@@ -52,6 +57,13 @@ def parse():
     ap.add_argument("--no-flow", action="store_true")
     ap.add_argument("--flow-steps", type=int, default=200)
     ap.add_argument("--flow-batch", type=int, default=65536)
+    ap.add_argument("--workload", default="multichannel", choices=["multichannel", "batched"],
+                    help="multichannel: the 2->4 iteration with the learned proposal beside it; batched: 512 "
+                         "uneven integrands in one persistent graph-replayed launch per iteration")
+    ap.add_argument("--batch-scale", type=float, default=1.0,
+                    help="batched: point counts times this factor (small cases for profiling)")
+    ap.add_argument("--no-sequential", action="store_true",
+                    help="batched: skip the one-call-per-task comparison")
     return ap.parse_args()
 
 
@@ -254,7 +266,7 @@ def run_chili(args, rank, world, local_rank):
 
 
 # Per-kernel figures of the committed ncu capture
-# (profiles/multichannel_2to4_kernels.md): FP64 operations (2*DFMA + DADD +
+# (the multichannel 2->4 summary under profiles/): FP64 operations (2*DFMA + DADD +
 # DMUL, executed) and DRAM bytes (read + write), both per weighted point.
 KERNEL_COUNTERS = {
     "k_mc_forward": {
@@ -540,13 +552,271 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------ batched workload
+BATCH_METRIC = "integrand points/s over 512 uneven integrands, one adapting iteration each per step, FP64"
+BATCH_UNIT = "points/s"
+BATCH_SEED = 2024
+
+
+def batched_config(tasks, world):
+    kinds = [t["kind"] for t in tasks]
+    return {"workload": "512 batched integrands: 256 camel functions (dims 2-12, sigma in [0.05, 0.2], centres in "
+                        "[0.2, 0.8], 50 bins, grid alpha 1.5) + 256 multichannel 2->n propagator integrands "
+                        "(n = 2..5, sqrt(S) in [200, 2000] GeV, 50 bins, channel weights adapted); points per "
+                        "integrand log-uniform in [1e4, 1e6]; every drawn point is one call (fixed budget)",
+            "tasks": len(tasks), "camel_tasks": kinds.count("camel"),
+            "multichannel_tasks": kinds.count("multichannel"),
+            "points_per_iteration": int(sum(t["ncalls"] for t in tasks)), "seed": BATCH_SEED,
+            "l2": "L2 flushed (256 MiB write) before every timed iteration",
+            "parallelism": f"{world} ranks, each its own 512 integrands (no collective)" if world > 1
+            else "single GPU"}
+
+
+def sequential_batched_ms(tasks, local_rank):
+    """The same tasks one call each through the single-integrand entry points
+    (chili_gpu_vegas_iterate, chili_gpu_multichannel_iterate), second
+    iteration of each timed by wall clock around the synchronous call."""
+    from chili_b200 import abi, channels, gpu, workloads
+    c = gpu.Context(local_rank)
+    total = 0.0
+    for k, t in enumerate(tasks):
+        if t["kind"] == "camel":
+            c.uniform_grids(1, t["dims"], t["bins"])
+            c.set_integrand(abi.CHILI_FUNC_CAMEL, t["params"])
+            run = lambda ctr: c.vegas_iterate(t["ncalls"], seed=BATCH_SEED + k, counter=ctr,
+                                              alpha=t["grid_alpha"], adapt=True)
+        else:
+            cs = t["channels"]
+            c.set_channels(cs)
+            c.uniform_grids(cs.nch, cs.ndims, t["bins"])
+            c.set_integrand(t["fkind"], t["params"])
+            c.set_preprocess(t["pre"])
+            p = workloads.mc_params(t["ncalls"], grid_alpha=t["grid_alpha"], beta=t["beta"],
+                                    min_alpha=t["min_alpha"])
+            run = lambda ctr: c.multichannel_iterate(p, seed=BATCH_SEED + k, counter=ctr)
+        run(0)
+        c.synchronize()
+        t0 = time.perf_counter()
+        run(1 << 32)
+        c.synchronize()
+        total += time.perf_counter() - t0
+    c.close()
+    return total * 1e3
+
+
+def run_batched(args, rank, world, local_rank):
+    import torch
+
+    from chili_b200 import gpu, workloads
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    tasks = workloads.batched_tasks(seed=BATCH_SEED + rank, scale=args.batch_scale)
+    npts = sum(t["ncalls"] for t in tasks)
+    stream = torch.cuda.Stream(dev)
+    ctx = gpu.Context(local_rank)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.batch_set(tasks)
+    t0 = time.perf_counter()
+    _, info = ctx.batch_iterate(1, seed=BATCH_SEED)  # picks block size and points per thread, captures the graph
+    setup_s = time.perf_counter() - t0
+    for _ in range(max(args.warmup, 3) - 1):
+        ctx.batch_iterate(1, seed=BATCH_SEED)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    ctx.set_option("kernel_timing", 0)
+    torch.cuda.synchronize(dev)
+    barrier()
+    l0 = ctx.launches
+    dev_ms, wall = 0.0, 0.0
+    pooled = np.zeros((len(tasks), 6))
+    with ClockSampler(local_rank) as clk:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            stream.synchronize()
+            w0 = time.perf_counter()
+            st, info = ctx.batch_iterate(1, seed=BATCH_SEED)  # host StatsData read back inside the call
+            wall += time.perf_counter() - w0
+            dev_ms += info.ms_per_iteration
+            pooled += st[0]
+    torch.cuda.synchronize(dev)
+    launches = ctx.launches - l0
+    barrier()
+    t = torch.tensor([dev_ms, wall], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms_max, wall_max = t.tolist()
+    seq_ms = None
+    if not args.no_sequential and rank == 0:
+        seq_ms = sequential_batched_ms(tasks, local_rank)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline_batched()
+    if rank == 0:
+        value = npts * world * args.steps / (ms_max / 1e3)
+        per_iter = ms_max / args.steps
+        kinds = np.array([t["kind"] == "camel" for t in tasks])
+        line = {
+            "metric": BATCH_METRIC, "value": value, "unit": BATCH_UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_iter,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (on-device Philox4x32-10 uniforms, key seed + task)",
+            "config": batched_config(tasks, world),
+            "autotune": {"block": info.block, "points_per_thread": info.points_per_thread,
+                         "units_per_iteration": info.units, "first_call_s": setup_s},
+            "sequential": None if seq_ms is None else {
+                "ms_per_iteration": seq_ms, "points_per_s": npts / (seq_ms / 1e3),
+                "batched_speedup": seq_ms / per_iter,
+                "path": "one chili_gpu_vegas_iterate / chili_gpu_multichannel_iterate call per task "
+                        "(multichannel with the reference's retry loop)"},
+            "nonzero_fraction": {"camel": float(pooled[kinds, 5].sum() / pooled[kinds, 0].sum()),
+                                 "multichannel": float(pooled[~kinds, 5].sum() / pooled[~kinds, 0].sum())},
+            "clocks": clk.summary(),
+            "gpu_launches": launches,
+            "roofline": batched_roofline(per_iter, tasks, dev),
+            "e2e": {"value": npts * world * args.steps / wall_max, "unit": BATCH_UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": int(st.nbytes),
+                    "path": "chili_gpu_batch_iterate (graph replay + host StatsData of every task) by wall clock; "
+                            "the uniforms are counter-based and drawn in the kernel, as the reference draws its "
+                            "own"},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+# k_batch_eval per drawn point, all tasks together (the small case keeps the
+# tasks' mix: every point count scaled by 1/16), from the committed ncu
+# capture (the batched-integrands summary under profiles/): FP64 operations (2*DFMA + DADD +
+# DMUL, executed) and DRAM bytes (read + write; almost all of it the
+# kernel's local-memory stack, not algorithmic traffic).
+BATCH_COUNTERS = {"fp64_ops_per_point": 5683.0, "dram_bytes_per_point": 1702.0,
+                  "source": "profiles/batched_integrands.md"}
+
+
+def batched_roofline(ms_per_iter, tasks, dev):
+    """k_batch_eval (the whole evaluation of an iteration, >97% of its device
+    time) against the FP64 peak measured in this run; its algorithmic HBM
+    traffic is nil (counter-based uniforms, grids and histograms in L2)."""
+    peak = fp64_peak_tflops(dev)
+    npts = sum(t["ncalls"] for t in tasks)
+    c = BATCH_COUNTERS
+    achieved = c["fp64_ops_per_point"] * npts / (ms_per_iter / 1e3) / 1e12
+    return {"kernel": "k_batch_eval", "bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak, "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+            "traffic": c["dram_bytes_per_point"] * npts, "counters_source": c["source"],
+            "note": "ms_per_iter is the whole iteration (evaluation, folds, adaptation)"}
+
+
+def _ref_batch_init():
+    global _WB
+    # the reference's Vegas prints its result to stdout: keep the workers quiet
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    sys.path.insert(0, ROOT)
+    from chili_b200 import abi, workloads
+    from oracle import ref
+    _WB = {"tasks": workloads.batched_tasks(seed=BATCH_SEED), "ref": ref, "abi": abi, "wl": workloads,
+           "rng": np.random.default_rng(os.getpid())}
+
+
+BATCH_SAMPLE_CALLS = 20000
+
+
+def _ref_batch_step(k):
+    """One iteration of task k through the reference's own Vegas or
+    MultiChannel object and its own random numbers (points capped at
+    BATCH_SAMPLE_CALLS); returns (points drawn, seconds)."""
+    t = _WB["tasks"][k]
+    ref, wl = _WB["ref"], _WB["wl"]
+    n = min(t["ncalls"], BATCH_SAMPLE_CALLS)
+    seed = int(_WB["rng"].integers(1, 2 ** 31))
+    if t["kind"] == "camel":
+        t0 = time.perf_counter()
+        ref.vegas_run(t["dims"], t["bins"], t["grid_alpha"], t["params"], seed, n, 1)
+        return n, time.perf_counter() - t0
+    p = wl.mc_params(n, iterations=1, grid_alpha=t["grid_alpha"], beta=t["beta"], min_alpha=t["min_alpha"])
+    R = ref.MultiChannel(t["channels"], t["bins"], p, t["fkind"], t["params"], pre=t["pre"])
+    t0 = time.perf_counter()
+    st = R.run_native(seed, 1)  # StatsData n counts every drawn point (rejections add a 0)
+    return int(st.n), time.perf_counter() - t0
+
+
+def _batch_pool(cores):
+    import multiprocessing as mp
+    return mp.get_context("spawn").Pool(cores, initializer=_ref_batch_init)
+
+
+def cpu_baseline_batched(steps=1):
+    """The reference's own code on the host cores: one iteration of every
+    16th task (32 tasks, points capped at 20000 each), tasks spread over all
+    cores; points/s = points drawn / wall time."""
+    from oracle import ref
+    if not ref.available():
+        return {"value": None, "unavailable": "oracle/_ref not built"}
+    cores = cpu_cores()
+    sample = list(range(0, 512, 16))
+    with _batch_pool(cores) as pool:
+        pool.map(_ref_batch_step, sample[:cores])  # warm-up
+        t0 = time.perf_counter()
+        pts = 0
+        for _ in range(steps):
+            pts += sum(r[0] for r in pool.map(_ref_batch_step, sample))
+        dt = time.perf_counter() - t0
+    return {"value": pts / dt, "unit": BATCH_UNIT, "cores": cores, "kind": "reference",
+            "sample": f"one iteration of every 16th task (32 tasks, at most {BATCH_SAMPLE_CALLS} points each; "
+                      f"multichannel tasks with the reference's retry loop) per step, tasks spread over {cores} "
+                      f"cores"}
+
+
+def run_reference_batched(args, rank, world):
+    if rank != 0:
+        return
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libchili_ref.so not built"}))
+        return
+    from chili_b200 import workloads
+    tasks = workloads.batched_tasks(seed=BATCH_SEED)
+    cores = cpu_cores()
+    sample = list(range(0, 512, 16))
+    pts = 0
+    with _batch_pool(cores) as pool:
+        for _ in range(args.warmup):
+            pool.map(_ref_batch_step, sample)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            pts += sum(r[0] for r in pool.map(_ref_batch_step, sample))
+        dt = time.perf_counter() - t0
+    value = pts / dt
+    line = {
+        "impl": "reference", "metric": BATCH_METRIC, "value": value, "unit": BATCH_UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (host uniforms)", "config": batched_config(tasks, 1),
+        "cpu_baseline": {"value": value, "unit": BATCH_UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"each step: one iteration of every 16th task (32 tasks, at most "
+                                   f"{BATCH_SAMPLE_CALLS} points each), tasks spread over {cores} cores"},
+        "e2e": {"value": value, "unit": BATCH_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
-        run_reference(args, rank, world)
+        if args.workload == "batched":
+            run_reference_batched(args, rank, world)
+        else:
+            run_reference(args, rank, world)
         return
     if world > 1:
         import datetime
@@ -555,7 +825,10 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                              device_id=torch.device("cuda", local_rank))
     try:
-        run_chili(args, rank, world, local_rank)
+        if args.workload == "batched":
+            run_batched(args, rank, world, local_rank)
+        else:
+            run_chili(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch

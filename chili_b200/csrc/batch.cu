@@ -49,20 +49,32 @@ struct BatchTask {
     long long hist_off;        // doubles: nch * dims * bins
     int32_t ch_off;            // first ChannelProgram / channel-weight slot
     int32_t desc;              // IntegrandDesc index
+    int32_t pp;                // PointProgram index, -1: per-channel weights
+    int32_t pad;
     double grid_alpha, beta, min_alpha;
+    double before;             // edge_before_table(dims, bins)
     uint64_t key;              // Philox key of the task
+};
+
+// Work unit u of the iteration: unit `unit` of task `task`.  Units are
+// handed out interleaved over the tasks (ordered by their position within
+// their task), so that the blocks running at one time work on many tasks and
+// their histogram and training adds spread over many addresses.
+struct UnitRef {
+    int32_t task, unit;
 };
 
 struct BatchDev {
     const BatchTask *tasks;
     int ntasks;
-    const long long *unit_task;  // first unit of every task (ascending), size ntasks
+    const UnitRef *umap;  // [nunits]
     long long nunits;
     const ChannelProgram *progs;
+    const PointProgram *pps;
     const IntegrandDesc *descs;
     double *grids, *grids_new, *hist, *atrain;  // atrain per channel slot
     double *alpha, *best, *mindiff, *cp;        // per channel slot; mindiff per task
-    double *part;                              // [nunits][6]
+    double *part;                              // [nunits][6], task-contiguous
     double *stats;                             // [iter slot][ntasks][6]
     int stat_slots;
     unsigned long long *next_unit;
@@ -70,97 +82,109 @@ struct BatchDev {
     int ppt;
 };
 
-__device__ __forceinline__ int unit_to_task(const long long *first, int n, long long u) {
-    int lo = 0, hi = n - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (first[mid] <= u) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
-
-// One iteration's evaluation: persistent blocks pull units.
+// One iteration's evaluation: persistent blocks pull units.  Per unit one
+// StatsData partial; histogram adds go straight to global memory, the
+// channel-training terms are summed per warp, then per block in shared
+// memory, and reach global memory once per unit and channel.
 __global__ void __launch_bounds__(256) k_batch_eval(BatchDev B) {
     __shared__ long long s_unit;
     __shared__ double ws[8][6];
+    __shared__ double s_atr[kBatchMaxCh];
     const uint64_t iter = *B.iter;
-    const int t = threadIdx.x;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    if (t < kBatchMaxCh) s_atr[t] = 0.0;
     for (;;) {
         if (t == 0) s_unit = static_cast<long long>(atomicAdd(B.next_unit, 1ull));
         __syncthreads();
         const long long u = s_unit;
         __syncthreads();
         if (u >= B.nunits) break;
-        const int ti = unit_to_task(B.unit_task, B.ntasks, u);
-        const BatchTask T = B.tasks[ti];
+        const UnitRef ur = B.umap[u];
+        const BatchTask T = B.tasks[ur.task];
         const IntegrandDesc *f = B.descs + T.desc;
         const long long tile = static_cast<long long>(blockDim.x) * B.ppt;
-        const long long p0 = (u - T.unit0) * tile;
+        const long long p0 = ur.unit * tile;
         const int D = T.dims, bins = T.bins;
         const size_t gsz = static_cast<size_t>(D) * (bins + 1);
         double cnt = 0, sum = 0, sum2 = 0, mn = 1.7976931348623157e308, mx = 2.2250738585072014e-308, nf = 0;
         for (int q = 0; q < B.ppt; ++q) {
             const long long i = p0 + static_cast<long long>(q) * blockDim.x + t;
-            if (i >= T.ncalls) break;
+            const bool active = i < T.ncalls;
             const uint64_t ctr = (iter << 32) + static_cast<uint64_t>(i);
-            double r[CHILI_MAX_DIMS + 1];
-            double val;
+            double val = 0;
             if (T.kind == CHILI_TASK_CAMEL) {
-                load_uniforms(T.key, ctr, nullptr, D, r);
-                const double *g = B.grids + T.grid_off;
-                double jac;
-                if (grid_map_checked(g, D, bins, r, jac)) val = camel(f, r, D) * jac;
-                else val = CUDART_NAN;
-                const double v2 = val * val;
-                double *H = B.hist + T.hist_off;
-                for (int j = 0; j < D; ++j) {
-                    const int bj = find_bin(g + j * (bins + 1), bins, r[j]);
-                    const int s = j * bins + bj;
-                    if (s >= 0) atomicAdd(H + s, v2);
+                if (active) {
+                    double r[CHILI_MAX_DIMS];
+                    load_uniforms(T.key, ctr, nullptr, D, r);
+                    const double *g = B.grids + T.grid_off;
+                    double jac;
+                    if (grid_map_checked(g, D, bins, r, jac)) val = camel(f, r, D) * jac;
+                    else val = CUDART_NAN;
+                    const double v2 = val * val;
+                    double *H = B.hist + T.hist_off;
+                    for (int j = 0; j < D; ++j) {
+                        const int s = j * bins + find_bin(g + j * (bins + 1), bins, r[j]);
+                        if (s >= 0) atomicAdd(H + s, v2);
+                    }
                 }
             } else {
-                load_uniforms(T.key, ctr, nullptr, D + 1, r);
-                const double *cp = B.cp + T.ch_off;
-                const int c = select_channel(cp, T.nch, r[D]);
-                const double *grids = B.grids + T.grid_off;
-                double jac;
-                val = 0;
-                if (grid_map_checked(grids + c * gsz, D, bins, r, jac)) {
-                    const ChannelProgram *progs = B.progs + T.ch_off;
-                    V4 mom[CHILI_MAX_SLOTS];
-                    double m2[CHILI_MAX_SLOTS];
-                    fs_generate(progs + c, r, mom, m2);
-                    if (preprocess(f, mom)) {
-                        double x[CHILI_MAX_DIMS], xs[CHILI_MAX_DIMS], dens[kBatchMaxCh];
-                        const double w = combined_weight(progs, grids, B.alpha + T.ch_off, T.nch, D, bins, c, mom,
-                                                         x, xs, dens, 1);
-                        const double fv = eval_momenta(f, mom, progs[0].n_ext);
-                        val = w == 0 ? 0 : fv * w;
-                        if (isnan(val)) val = 0;  // a retry in the reference; a zero call here
-                        if (val != 0) {
-                            // AddTrainData (MultiChannel.hh:167-180), non-finite terms dropped
-                            const double v2 = val * val;
-                            double *H = B.hist + T.hist_off + static_cast<size_t>(c) * D * bins;
-                            const double *g = grids + c * gsz;
-                            for (int j = 0; j < D; ++j) {
-                                const int bj = find_bin(g + j * (bins + 1), bins, xs[j]);
-                                if (j * bins + bj >= 0) atomicAdd(H + j * bins + bj, v2);
-                            }
-                            for (int k = 0; k < T.nch; ++k) {
-                                const double tk = v2 * w / dens[k];
-                                if (isfinite(tk)) atomicAdd(B.atrain + T.ch_off + k, tk);
+                // the task is the block's: every lane reaches the reductions
+                double dens[kBatchMaxCh];
+                double vw = 0;  // val^2 * weight of a point that trains, else 0
+                if (active) {
+                    double r[CHILI_MAX_DIMS + 1];
+                    load_uniforms(T.key, ctr, nullptr, D + 1, r);
+                    const double *cp = B.cp + T.ch_off;
+                    const int c = select_channel(cp, T.nch, r[D]);
+                    const double *grids = B.grids + T.grid_off;
+                    double jac;
+                    if (grid_map_checked(grids + c * gsz, D, bins, r, jac)) {
+                        const ChannelProgram *progs = B.progs + T.ch_off;
+                        V4 mom[CHILI_MAX_SLOTS];
+                        double m2[CHILI_MAX_SLOTS];
+                        fs_generate(progs + c, r, mom, m2);
+                        if (preprocess(f, mom)) {
+                            double x[CHILI_MAX_DIMS], xs[CHILI_MAX_DIMS];
+                            const double *al = B.alpha + T.ch_off;
+                            const double wgt =
+                                T.pp >= 0 ? combined_weight_pp(B.pps + T.pp, grids, al, D, bins, c, mom, x, xs, dens,
+                                                               1, T.before)
+                                          : combined_weight(progs, grids, al, T.nch, D, bins, c, mom, x, xs, dens, 1);
+                            const double fv = eval_momenta(f, mom, progs[0].n_ext);
+                            val = wgt == 0 ? 0 : fv * wgt;
+                            if (isnan(val)) val = 0;  // a retry in the reference; a call of value 0 here
+                            if (val != 0) {
+                                // AddTrainData (MultiChannel.hh:167-180)
+                                const double v2 = val * val;
+                                double *H = B.hist + T.hist_off + static_cast<size_t>(c) * D * bins;
+                                const double *g = grids + c * gsz;
+                                for (int j = 0; j < D; ++j) {
+                                    const int s = j * bins + find_bin(g + j * (bins + 1), bins, xs[j]);
+                                    if (s >= 0) atomicAdd(H + s, v2);
+                                }
+                                vw = v2 * wgt;
                             }
                         }
                     }
                 }
+                const unsigned any = __ballot_sync(0xffffffffu, vw != 0);
+                if (any) {
+                    for (int k = 0; k < T.nch; ++k) {
+                        double term = vw != 0 ? vw / dens[k] : 0.0;
+                        if (!isfinite(term)) term = 0.0;  // non-finite terms dropped
+                        term = warp_sum(term);
+                        if (lane == 0 && term != 0) atomicAdd(s_atr + k, term);
+                    }
+                }
             }
-            cnt += 1;
-            sum += val;
-            sum2 += val * val;
-            mn = std_min(mn, val);
-            mx = std_max(mx, val);
-            nf += (val != 0);
+            if (active) {
+                cnt += 1;
+                sum += val;
+                sum2 += val * val;
+                mn = std_min(mn, val);
+                mx = std_max(mx, val);
+                nf += (val != 0);
+            }
         }
         cnt = warp_sum(cnt);
         sum = warp_sum(sum);
@@ -168,8 +192,7 @@ __global__ void __launch_bounds__(256) k_batch_eval(BatchDev B) {
         mn = warp_min(mn);
         mx = warp_max(mx);
         nf = warp_sum(nf);
-        const int w = t >> 5, l = t & 31;
-        if (l == 0) {
+        if (lane == 0) {
             ws[w][0] = cnt; ws[w][1] = mn; ws[w][2] = mx; ws[w][3] = sum; ws[w][4] = sum2; ws[w][5] = nf;
         }
         __syncthreads();
@@ -179,10 +202,20 @@ __global__ void __launch_bounds__(256) k_batch_eval(BatchDev B) {
                 a[0] += ws[k][0]; a[1] = std_min(a[1], ws[k][1]); a[2] = std_max(a[2], ws[k][2]);
                 a[3] += ws[k][3]; a[4] += ws[k][4]; a[5] += ws[k][5];
             }
-            for (int k = 0; k < 6; ++k) B.part[u * 6 + k] = a[k];
+            double *o = B.part + (T.unit0 + ur.unit) * 6;
+            for (int k = 0; k < 6; ++k) o[k] = a[k];
         }
-        __syncthreads();
+        if (T.kind != CHILI_TASK_CAMEL && t < T.nch) {
+            if (s_atr[t] != 0) atomicAdd(B.atrain + T.ch_off + t, s_atr[t]);
+            s_atr[t] = 0.0;
+        }
     }
+}
+
+// The PointPrograms' (smin, smax) terms.
+__global__ void k_batch_pp_prepare(PointProgram *__restrict__ pps) {
+    PointProgram *pp = pps + blockIdx.x;
+    for (int k = threadIdx.x; k < pp->n_dws; k += blockDim.x) pp_prepare_entry(pp, k);
 }
 
 // Per task (one block of kFoldThreads each): fold of its unit partials into
@@ -267,11 +300,11 @@ __global__ void k_batch_next(BatchDev B) {
 
 struct BatchState {
     std::vector<BatchTask> tasks;
-    std::vector<long long> unit_first;
+    std::vector<UnitRef> umap;
     std::vector<AdaptJob> jobs;
     int max_bins = 2, nslots = 0;
     long long total_points = 0, nunits = 0;
-    DevBuf d_tasks, d_first, d_progs, d_descs, d_grids, d_grids_new, d_hist, d_atrain, d_alpha, d_best, d_mindiff,
+    DevBuf d_tasks, d_umap, d_pps, d_progs, d_descs, d_grids, d_grids_new, d_hist, d_atrain, d_alpha, d_best, d_mindiff,
         d_cp, d_part, d_stats, d_counters, d_jobs, d_status;
     int block = 0, ppt = 0, grid_blocks = 0;
     bool tuned = false;
@@ -294,9 +327,10 @@ BatchDev batch_dev(chili_ctx *ctx) {
     BatchDev B{};
     B.tasks = S.d_tasks.as<BatchTask>();
     B.ntasks = static_cast<int>(S.tasks.size());
-    B.unit_task = S.d_first.as<long long>();
+    B.umap = S.d_umap.as<UnitRef>();
     B.nunits = S.nunits;
     B.progs = S.d_progs.as<ChannelProgram>();
+    B.pps = S.d_pps.as<PointProgram>();
     B.descs = S.d_descs.as<IntegrandDesc>();
     B.grids = S.d_grids.as<double>();
     B.grids_new = S.d_grids_new.as<double>();
@@ -315,25 +349,36 @@ BatchDev batch_dev(chili_ctx *ctx) {
     return B;
 }
 
-// Work-unit layout for a block size and points per thread.
+// Work-unit layout for a block size and points per thread: units of each
+// task, interleaved over the tasks in the order of (unit + 1/2) / units.
 int layout_units(chili_ctx *ctx, int block, int ppt) {
     BatchState &S = *ctx->batch;
     long long u = 0;
-    S.unit_first.assign(S.tasks.size(), 0);
-    for (size_t k = 0; k < S.tasks.size(); ++k) {
-        const long long tile = static_cast<long long>(block) * ppt;
-        S.tasks[k].unit0 = u;
-        S.tasks[k].units = (S.tasks[k].ncalls + tile - 1) / tile;
-        S.unit_first[k] = u;
-        u += S.tasks[k].units;
+    const long long tile = static_cast<long long>(block) * ppt;
+    for (auto &T : S.tasks) {
+        T.unit0 = u;
+        T.units = (T.ncalls + tile - 1) / tile;
+        u += T.units;
     }
     S.nunits = u;
+    S.umap.resize(static_cast<size_t>(u));
+    {
+        std::vector<std::pair<double, UnitRef>> order;
+        order.reserve(static_cast<size_t>(u));
+        for (size_t k = 0; k < S.tasks.size(); ++k)
+            for (long long j = 0; j < S.tasks[k].units; ++j)
+                order.push_back({(j + 0.5) / static_cast<double>(S.tasks[k].units),
+                                 UnitRef{static_cast<int32_t>(k), static_cast<int32_t>(j)}});
+        std::stable_sort(order.begin(), order.end(),
+                         [](const auto &a, const auto &b) { return a.first < b.first; });
+        for (size_t k = 0; k < order.size(); ++k) S.umap[k] = order[k].second;
+    }
     CK(S.d_tasks.ensure(sizeof(BatchTask) * S.tasks.size()));
     CK(cudaMemcpyAsync(S.d_tasks.p, S.tasks.data(), sizeof(BatchTask) * S.tasks.size(), cudaMemcpyHostToDevice,
                        ctx->stream));
-    CK(S.d_first.ensure(sizeof(long long) * S.unit_first.size()));
-    CK(cudaMemcpyAsync(S.d_first.p, S.unit_first.data(), sizeof(long long) * S.unit_first.size(),
-                       cudaMemcpyHostToDevice, ctx->stream));
+    CK(S.d_umap.ensure(sizeof(UnitRef) * S.umap.size()));
+    CK(cudaMemcpyAsync(S.d_umap.p, S.umap.data(), sizeof(UnitRef) * S.umap.size(), cudaMemcpyHostToDevice,
+                       ctx->stream));
     CK(S.d_part.ensure(sizeof(double) * 6 * u));
     CK(cudaStreamSynchronize(ctx->stream));
     S.block = block;
@@ -435,7 +480,7 @@ void batch_release(chili_ctx *ctx) {
     if (!ctx || !ctx->batch) return;
     BatchState &S = *ctx->batch;
     if (S.graph) cudaGraphExecDestroy(S.graph);
-    for (DevBuf *b : {&S.d_tasks, &S.d_first, &S.d_progs, &S.d_descs, &S.d_grids, &S.d_grids_new, &S.d_hist,
+    for (DevBuf *b : {&S.d_tasks, &S.d_umap, &S.d_pps, &S.d_progs, &S.d_descs, &S.d_grids, &S.d_grids_new, &S.d_hist,
                       &S.d_atrain, &S.d_alpha, &S.d_best, &S.d_mindiff, &S.d_cp, &S.d_part, &S.d_stats,
                       &S.d_counters, &S.d_jobs, &S.d_status})
         b->release();
@@ -452,6 +497,7 @@ int chili_gpu_batch_set(chili_ctx *ctx, const chili_task *tasks, int ntasks) {
     ctx->batch = new BatchState();
     BatchState &S = *ctx->batch;
     std::vector<ChannelProgram> progs;
+    std::vector<PointProgram> pps;
     std::vector<IntegrandDesc> descs;
     std::vector<double> grids, alpha;
     long long goff = 0, hoff = 0;
@@ -465,6 +511,7 @@ int chili_gpu_batch_set(chili_ctx *ctx, const chili_task *tasks, int ntasks) {
         T.beta = t.beta;
         T.min_alpha = t.min_alpha;
         T.key = 0;
+        T.pp = -1;
         IntegrandDesc d{};
         if (t.bins < 2 || t.bins > CHILI_MAX_BINS || t.ncalls < 1 || t.ncalls >= (1ull << 32)) {
             batch_release(ctx);
@@ -505,6 +552,10 @@ int chili_gpu_batch_set(chili_ctx *ctx, const chili_task *tasks, int ntasks) {
             }
             T.dims = p[0].ndims;
             T.nch = t.nch;
+            // the shared-entry form of the channel weights when the set fits
+            pps.emplace_back();
+            if (build_point_program(p, pps.back())) T.pp = static_cast<int32_t>(pps.size() - 1);
+            else pps.pop_back();
             T.ch_off = static_cast<int32_t>(alpha.size());
             for (int c = 0; c < t.nch; ++c) alpha.push_back(1.0 / t.nch);
             for (auto &q : p) progs.push_back(q);
@@ -525,6 +576,7 @@ int chili_gpu_batch_set(chili_ctx *ctx, const chili_task *tasks, int ntasks) {
         }
         T.desc = static_cast<int32_t>(descs.size());
         descs.push_back(d);
+        T.before = edge_before_table(T.dims, T.bins);
         T.grid_off = goff;
         T.hist_off = hoff;
         const long long per = static_cast<long long>(T.dims) * (T.bins + 1);
@@ -544,6 +596,14 @@ int chili_gpu_batch_set(chili_ctx *ctx, const chili_task *tasks, int ntasks) {
     CK(S.d_progs.ensure(sizeof(ChannelProgram) * progs.size()));
     CK(cudaMemcpyAsync(S.d_progs.p, progs.data(), sizeof(ChannelProgram) * progs.size(), cudaMemcpyHostToDevice,
                        ctx->stream));
+    if (!pps.empty()) {
+        CK(S.d_pps.ensure(sizeof(PointProgram) * pps.size()));
+        CK(cudaMemcpyAsync(S.d_pps.p, pps.data(), sizeof(PointProgram) * pps.size(), cudaMemcpyHostToDevice,
+                           ctx->stream));
+        k_batch_pp_prepare<<<static_cast<unsigned>(pps.size()), PP_MAX_DWS, 0, ctx->stream>>>(
+            S.d_pps.as<PointProgram>());
+        LAUNCHED();
+    }
     CK(S.d_descs.ensure(sizeof(IntegrandDesc) * descs.size()));
     CK(cudaMemcpyAsync(S.d_descs.p, descs.data(), sizeof(IntegrandDesc) * descs.size(), cudaMemcpyHostToDevice,
                        ctx->stream));

@@ -355,6 +355,24 @@ __device__ __forceinline__ double fs_weight(const ChannelProgram *__restrict__ P
 
 namespace chili_dev {
 
+// The (smin, smax)-only terms of decay weight k of a PointProgram (computed
+// on the device so that they round as the per-point code would):
+// massless: pow(smin, 0.01), pow(smax, 0.01); massive: atan((smin-m2)/mw),
+// atan((smax-m2)/mw) (the PeakedWeight and Breit-Wigner weights,
+// ChannelElements.cc:27-50 and 64-85).
+__device__ __forceinline__ void pp_prepare_entry(PointProgram *__restrict__ pp, int k) {
+    const double smin = pp->dw_smin_c[k], smax = pp->dw_smax[k];
+    if (pp->dw_massless[k]) {
+        const double ce = 1. - 0.99;
+        pp->dw_t1[k] = pow(smin, ce);
+        pp->dw_t2[k] = pow(smax, ce);
+    } else {
+        const double m2 = pp->dw_mass[k] * pp->dw_mass[k], mw = pp->dw_mass[k] * pp->dw_width[k];
+        pp->dw_t1[k] = atan((smin - m2) / mw);  // "ymax" of ChannelElements.cc:94
+        pp->dw_t2[k] = atan((smax - m2) / mw);  // "ymin"
+    }
+}
+
 // Integrand::GenerateWeight (Integrand.hh:112-123) over a PointProgram: the
 // shared parts of all channels are evaluated once per point, then every
 // channel's density is assembled as the reference multiplies it

@@ -129,17 +129,7 @@ __global__ void __launch_bounds__(256) k_pp_items(const PointProgram *__restrict
 // full evaluation bit for bit.
 __global__ void k_pp_prepare(PointProgram *__restrict__ pp) {
     const int k = threadIdx.x + blockIdx.x * blockDim.x;
-    if (k >= pp->n_dws) return;
-    const double smin = pp->dw_smin_c[k], smax = pp->dw_smax[k];
-    if (pp->dw_massless[k]) {
-        const double ce = 1. - 0.99;
-        pp->dw_t1[k] = pow(smin, ce);
-        pp->dw_t2[k] = pow(smax, ce);
-    } else {
-        const double m2 = pp->dw_mass[k] * pp->dw_mass[k], mw = pp->dw_mass[k] * pp->dw_width[k];
-        pp->dw_t1[k] = atan((smin - m2) / mw);  // "ymax" of ChannelElements.cc:94
-        pp->dw_t2[k] = atan((smax - m2) / mw);  // "ymin"
-    }
+    if (k < pp->n_dws) pp_prepare_entry(pp, k);
 }
 
 // One thread per (point, chain): WgtTChan's weight and last uniform

@@ -61,13 +61,13 @@ def uniforms53(rng, shape):
     return k.astype(np.float64) * 2.0 ** -53
 
 
-def batched_tasks(seed=2024, n_camel=256, n_mc=256, camel_bins=50, mc_bins=50):
+def batched_tasks(seed=2024, n_camel=256, n_mc=256, camel_bins=50, mc_bins=50, scale=1.0):
     """The batched workload: n_camel camel functions of dimension 2..12
     (sigma uniform in [0.05, 0.2], centres uniform in [0.2, 0.8], grid alpha
     1.5) and n_mc 2->n propagator integrands (n = 2..5, sqrt(S) uniform in
     [200, 2000] GeV, M and Gamma of the Z, channel weights adapted), each with
-    a point count log-uniform in [1e4, 1e6]; task dicts for
-    gpu.Context.batch_set."""
+    a point count log-uniform in [1e4, 1e6] (times `scale`, at least 100);
+    task dicts for gpu.Context.batch_set."""
     rng = np.random.default_rng(seed)
     tasks = []
     sets = {}
@@ -76,7 +76,8 @@ def batched_tasks(seed=2024, n_camel=256, n_mc=256, camel_bins=50, mc_bins=50):
         sigma = float(rng.uniform(0.05, 0.2))
         a, b = rng.uniform(0.2, 0.8, dims), rng.uniform(0.2, 0.8, dims)
         tasks.append({"kind": "camel", "dims": dims, "bins": camel_bins, "grid_alpha": 1.5,
-                      "ncalls": int(round(10 ** rng.uniform(4, 6))), "params": camel_params(dims, sigma, a, b)})
+                      "ncalls": max(100, int(round(10 ** rng.uniform(4, 6) * scale))),
+                      "params": camel_params(dims, sigma, a, b)})
     mp = abi.MultiChannelParams.defaults()
     for _ in range(n_mc):
         n_out = int(rng.integers(2, 6))
@@ -85,7 +86,7 @@ def batched_tasks(seed=2024, n_camel=256, n_mc=256, camel_bins=50, mc_bins=50):
         if key not in sets:
             sets[key] = channel_set(n_out, sqrts)
         tasks.append({"kind": "multichannel", "channels": sets[key], "bins": mc_bins,
-                      "ncalls": int(round(10 ** rng.uniform(4, 6))), "grid_alpha": mp.grid_alpha,
+                      "ncalls": max(100, int(round(10 ** rng.uniform(4, 6) * scale))), "grid_alpha": mp.grid_alpha,
                       "beta": mp.beta, "min_alpha": mp.min_alpha, "fkind": abi.CHILI_FUNC_PROPAGATOR,
                       "params": channels.propagator_params(), "pre": abi.CHILI_PRE_FINITE})
     return tasks
