@@ -227,6 +227,8 @@ def run_chili(args, rank, world, local_rank):
     if not args.no_flow and world == 1:
         flow = measure_flow(ctx, args, dev, stream, plain)
 
+    unw_out = measure_unweighted_output(ctx, info.weight_max, dev, rank)
+
     e2e = None
     if not args.no_e2e:
         e2e = measure_e2e(ctx, params, args, dev, rank)
@@ -258,6 +260,7 @@ def run_chili(args, rank, world, local_rank):
             "gpu_launches": launches,
             "roofline": roof,
             "paths": {"selected": selected, "plain": plain, "flow": flow},
+            "unweighted_output": unw_out,
             "e2e": e2e,
             "cpu_baseline": cpu,
         }
@@ -424,6 +427,32 @@ def measure_flow(ctx, args, dev, stream, plain):
         "kernel_ms": {k: round(k2[k][0] - k1[k][0], 3) for k in FLOW_KERNELS if k2[k][0] > k1[k][0]},
         "gpu_launches_note": "flow kernels: tcgen05 coupling layers, FP64 phase space, phased weight pass",
     }
+
+
+def measure_unweighted_output(ctx, w_max, dev, rank, n=4_000_000, reps=3):
+    """The unweighting stage end to end: n points drawn, weighted, hit-or-miss
+    against the last iteration's largest weight, and the kept events
+    (momenta, weight, channel) written to pinned host memory."""
+    import torch
+    ne = ctx.n_ext
+    cap = n // 4
+    out = (torch.empty((cap, ne, 4), dtype=torch.float64, pin_memory=True).numpy(),
+           torch.empty(cap, dtype=torch.float64, pin_memory=True).numpy(),
+           torch.empty(cap, dtype=torch.int32, pin_memory=True).numpy())
+    seed = 97 + rank
+    ctx.generate_unweighted(n, w_max, seed=seed, counter=0, max_events=cap, out=out)  # warm-up
+    torch.cuda.synchronize(dev)
+    kept = 0
+    t0 = time.perf_counter()
+    for r in range(reps):
+        _, _, _, info = ctx.generate_unweighted(n, w_max, seed=seed, counter=(r + 1) * n, max_events=cap, out=out)
+        kept += info.kept
+    dt = time.perf_counter() - t0
+    written = min(kept // reps, cap)
+    return {"events_per_s": kept / dt, "points_per_s": n * reps / dt, "efficiency": kept / (n * reps),
+            "w_max": w_max, "overweight_last_call": int(info.overweight), "points_per_call": n,
+            "d2h_bytes_per_call": int(written * (ne * 32 + 12)),
+            "path": "chili_gpu_generate_unweighted with pinned host outputs, wall clock"}
 
 
 def measure_e2e(ctx, params, args, dev, rank):

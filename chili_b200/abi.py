@@ -132,6 +132,12 @@ class FlowIterInfo(C.Structure):
                 ("weight_max", C.c_double), ("unweighting_efficiency", C.c_double)]
 
 
+class UnweightInfo(C.Structure):
+    """chili_unweight_info."""
+    _fields_ = [("points", C.c_uint64), ("rejected_pre", C.c_uint64), ("kept", C.c_uint64),
+                ("overweight", C.c_uint64), ("sum", C.c_double), ("max", C.c_double)]
+
+
 CHILI_TASK_CAMEL = 0
 CHILI_TASK_MULTICHANNEL = 1
 

@@ -916,6 +916,139 @@ int chili_gpu_generate(chili_ctx *ctx, int64_t n, uint64_t seed, uint64_t counte
     return sync_if_host(ctx, {&am, &aw, &ac});
 }
 
+int chili_gpu_generate_unweighted(chili_ctx *ctx, int64_t n, uint64_t seed, uint64_t counter_base, double w_max,
+                                  double *mom, double *wgt, int32_t *ch, int64_t max_events, int64_t *n_events,
+                                  chili_unweight_info *info) {
+    if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
+    int rc;
+    if ((rc = need_mc(ctx))) return rc;
+    if (!ctx->f_set) return fail(ctx, CHILI_ERR_STATE, "no integrand set");
+    if (ctx->f_host.kind == CHILI_FUNC_CAMEL) return fail(ctx, CHILI_ERR_STATE, "the camel is not a phase-space integrand");
+    if (n < 0 || max_events < 0) return fail(ctx, CHILI_ERR_INVALID_ARG, "n and max_events must be >= 0");
+    if (!(w_max > 0) || !std::isfinite(w_max)) return fail(ctx, CHILI_ERR_INVALID_ARG, "w_max must be finite and > 0");
+    const int nch = ctx->nch, D = ctx->ndims, B = ctx->bins, NE = ctx->n_ext;
+    Arg am, aw, ac;
+    if ((rc = resolve(ctx, mom, sizeof(double) * max_events * NE * 4, 0, false, am))) return rc;
+    if ((rc = resolve(ctx, wgt, sizeof(double) * max_events, 1, false, aw))) return rc;
+    if ((rc = resolve(ctx, ch, sizeof(int32_t) * max_events, 2, false, ac))) return rc;
+    const bool pipe = pipeline_dims_ok(D) && ctx->have_pp && ctx->use_pp && ctx->use_pipeline;
+    long long done = 0, kept = 0, n_pre_tot = 0;
+    double sum = 0, over = 0, vmax = -1.7976931348623157e308;
+    while (done < n) {
+        long long m = std::min<long long>(n - done, 1ll << 24);
+        {
+            // keep the per-chunk buffers within ~8 GB, as an iteration does
+            const PointProgram &P = ctx->pp_host;
+            long long per = 8ll * (4 * NE + nch + 4) + 4ll * D + 16;
+            if (pipe) per += 8ll * (4 * P.n_nodes + P.n_memo) + P.n_chains;
+            m = std::min<long long>(m, std::max<long long>(1 << 16, (8ll << 30) / per));
+        }
+        const long long nb_f = (m + kFwdBlock - 1) / kFwdBlock;
+        const long long nb_w = (m + kWgtBlock - 1) / kWgtBlock;
+        CK(ctx->mom_soa.ensure(sizeof(double) * 4 * NE * m));
+        CK(ctx->ich.ensure(sizeof(int32_t) * m));
+        CK(ctx->flag.ensure(m));
+        CK(ctx->list.ensure(sizeof(int32_t) * m));
+        CK(ctx->block_count.ensure(sizeof(int32_t) * nb_f));
+        CK(ctx->block_off.ensure(sizeof(long long) * nb_f));
+        CK(ctx->rec.ensure(m * (2 * sizeof(double) + 1 + sizeof(int32_t) * D + sizeof(double) * nch) + 256));
+        CK(ctx->ctl3.ensure(3 * sizeof(RoundCtl)));
+        // keep flags [m] | kept list [m] | partials [nb_f][3] | sums [3] | control
+        const size_t off_list = (static_cast<size_t>(m) + 15) & ~static_cast<size_t>(15);
+        const size_t off_part = off_list + sizeof(int32_t) * ((static_cast<size_t>(m) + 3) & ~static_cast<size_t>(3));
+        const size_t off_out = off_part + sizeof(double) * 3 * nb_f;
+        const size_t off_ctl = off_out + sizeof(double) * 4;
+        CK(ctx->unw.ensure(off_ctl + sizeof(RoundCtl)));
+        char *ub = ctx->unw.as<char>();
+        uint8_t *keep = reinterpret_cast<uint8_t *>(ub);
+        int32_t *kept_list = reinterpret_cast<int32_t *>(ub + off_list);
+        double *part = reinterpret_cast<double *>(ub + off_part);
+        double *outs = reinterpret_cast<double *>(ub + off_out);
+        RoundCtl *ctl_keep = reinterpret_cast<RoundCtl *>(ub + off_ctl);
+        RoundCtl *ctl_pre = ctx->ctl3.as<RoundCtl>();
+        double *rec_val = ctx->rec.as<double>();
+        double *rec_wgt = rec_val + m;
+        double *rec_dens = rec_wgt + m;
+        int32_t *rec_slot = reinterpret_cast<int32_t *>(rec_dens + static_cast<size_t>(nch) * m);
+        uint8_t *rec_ok = reinterpret_cast<uint8_t *>(rec_slot + static_cast<size_t>(D) * m);
+        const uint64_t ctr0 = counter_base + static_cast<uint64_t>(done);
+        k_mc_forward<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(
+            ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), cp_ptr(ctx), nch, D, B, seed, ctr0, nullptr, m,
+            ctx->f_dev.as<IntegrandDesc>(), NE, ctx->mom_soa.as<double>(), ctx->ich.as<int32_t>(),
+            ctx->flag.as<uint8_t>(), ctx->block_count.as<int32_t>());
+        LAUNCHED();
+        k_mc_scan<<<1, 1024, 0, ctx->stream>>>(ctx->block_count.as<int32_t>(), static_cast<int>(nb_f),
+                                               ctx->flag.as<uint8_t>(), m, m + 1, ctx->block_off.as<long long>(),
+                                               ctl_pre);
+        LAUNCHED();
+        k_mc_compact<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(
+            ctx->flag.as<uint8_t>(), ctx->block_off.as<long long>(), ctl_pre, m, ctx->list.as<int32_t>());
+        LAUNCHED();
+        CK(cudaMemcpyAsync(ctx->ctl_host, ctl_pre, sizeof(RoundCtl), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        const long long n_pre = ctx->ctl_host->n_acc;
+        if (n_pre < 0 || n_pre > m) return fail(ctx, CHILI_ERR_CUDA, "inconsistent point list");
+        n_pre_tot += n_pre;
+        if (pipe) {
+            if ((rc = launch_pipeline(ctx, m, n_pre, B, false, ctl_pre, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens)))
+                return rc;
+        } else {
+            k_mc_weight<<<static_cast<unsigned>(nb_w), kWgtBlock, 0, ctx->stream>>>(
+                ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), alpha_ptr(ctx), nch, D, B, NE,
+                ctx->mom_soa.as<double>(), m, ctx->ich.as<int32_t>(), ctx->list.as<int32_t>(), ctl_pre,
+                ctx->f_dev.as<IntegrandDesc>(), 0, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens, pp_ptr(ctx));
+            LAUNCHED();
+        }
+        k_unw_flag<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(
+            ctx->list.as<int32_t>(), ctl_pre, rec_val, seed, ctr0, w_max, m, keep, part);
+        LAUNCHED();
+        k_unw_reduce<<<1, 256, 0, ctx->stream>>>(part, nb_f, outs);
+        LAUNCHED();
+        k_block_count<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(keep, ctl_pre,
+                                                                                 ctx->block_count.as<int32_t>());
+        LAUNCHED();
+        k_mc_scan<<<1, 1024, 0, ctx->stream>>>(ctx->block_count.as<int32_t>(), static_cast<int>(nb_f), keep, m,
+                                               m + 1, ctx->block_off.as<long long>(), ctl_keep);
+        LAUNCHED();
+        k_mc_compact<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(
+            keep, ctx->block_off.as<long long>(), ctl_keep, m, kept_list);
+        LAUNCHED();
+        k_unw_write<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(
+            kept_list, ctl_keep, ctx->list.as<int32_t>(), ctx->mom_soa.as<double>(), m, NE, ctx->ich.as<int32_t>(),
+            rec_val, w_max, kept, max_events, static_cast<double *>(am.dev), static_cast<double *>(aw.dev),
+            static_cast<int32_t *>(ac.dev));
+        LAUNCHED();
+        double h[3];
+        RoundCtl rk;
+        CK(cudaMemcpyAsync(h, outs, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(&rk, ctl_keep, sizeof(RoundCtl), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (rk.n_acc < 0 || rk.n_acc > n_pre) return fail(ctx, CHILI_ERR_CUDA, "inconsistent kept count");
+        kept += rk.n_acc;
+        sum += h[0];
+        vmax = std::max(vmax, h[1]);
+        over += h[2];
+        done += m;
+    }
+    // copy back only the events written
+    const long long written = std::min<long long>(kept, max_events);
+    if (am.host) am.bytes = sizeof(double) * written * NE * 4;
+    if (aw.host) aw.bytes = sizeof(double) * written;
+    if (ac.host) ac.bytes = sizeof(int32_t) * written;
+    if ((rc = finish_out(ctx, am)) || (rc = finish_out(ctx, aw)) || (rc = finish_out(ctx, ac))) return rc;
+    if ((rc = sync_if_host(ctx, {&am, &aw, &ac}))) return rc;
+    if (n_events) *n_events = kept;
+    if (info) {
+        info->points = static_cast<uint64_t>(n);
+        info->rejected_pre = static_cast<uint64_t>(n - n_pre_tot);
+        info->kept = static_cast<uint64_t>(kept);
+        info->overweight = static_cast<uint64_t>(over);
+        info->sum = sum;
+        info->max = n_pre_tot < n ? std::max(vmax, 0.0) : vmax;  // rejected points have value 0
+    }
+    return CHILI_OK;
+}
+
 int chili_gpu_evaluate_batch(chili_ctx *ctx, int ch, const double *u, double *out, int64_t n) {
     if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
     int rc;

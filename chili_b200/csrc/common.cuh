@@ -92,6 +92,7 @@ __host__ __device__ __forceinline__ void uniform_pair(uint64_t seed, uint64_t k,
 
 // Stream ids keep different consumers of one seed apart.
 constexpr uint32_t kStreamPoints = 0;  // VEGAS / multichannel points
+constexpr uint32_t kStreamAccept = 1;  // hit-or-miss uniforms of the unweighting stage
 
 // ------------------------------------------------------------ reductions
 __device__ __forceinline__ double warp_sum(double v) {

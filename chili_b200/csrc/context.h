@@ -107,6 +107,7 @@ struct chili_ctx {
     RoundCtl *ctl_host = nullptr;  // pinned
     double accept_rate = 0.5, nan_rate = 0.0;
     DevBuf rec, ctl3;
+    DevBuf unw;  // unweighting: keep flags, kept list, partials, round control
     // plain VEGAS scratch
     DevBuf v_part, v_hist, v_train, v_out;
     // staging of host buffers

@@ -724,4 +724,107 @@ __global__ void k_evaluate_batch(const ChannelProgram *__restrict__ prog, const 
     out[i] = w == 0 ? 0 : eval_momenta(f, mom, ne) * w;
 }
 
+// ------------------------------------------------------------- unweighting
+// Hit-or-miss flag of every listed point i < n_pre (point k = list[i], value
+// rec_val[i]): keep when r * w_max < |v|, r the accept-stream uniform of
+// counter ctr0 + k.  keep[i] for all i < m (0 beyond the list); per block:
+// sum of values, largest value, overweight count.
+__global__ void __launch_bounds__(kFwdBlock) k_unw_flag(const int32_t *__restrict__ list,
+                                                         const RoundCtl *__restrict__ ctl_pre,
+                                                         const double *__restrict__ rec_val, uint64_t seed,
+                                                         uint64_t ctr0, double w_max, long long m,
+                                                         uint8_t *__restrict__ keep, double *__restrict__ part) {
+    const long long i = blockIdx.x * static_cast<long long>(kFwdBlock) + threadIdx.x;
+    const long long n_pre = ctl_pre->n_acc;
+    double v = 0.0, mx = -1.7976931348623157e308, over = 0.0;
+    int kp = 0;
+    if (i < m && i < n_pre) {
+        const long long k = list[i];
+        v = rec_val[i];
+        double r, r_unused;
+        uniform_pair(seed, ctr0 + static_cast<uint64_t>(k), kStreamAccept, 0u, r, r_unused);
+        kp = r * w_max < fabs(v) ? 1 : 0;
+        mx = v;
+        over = (kp && fabs(v) > w_max) ? 1.0 : 0.0;
+    }
+    if (i < m) keep[i] = static_cast<uint8_t>(kp);
+    double sum = warp_sum(v);
+    mx = warp_max(mx);
+    over = warp_sum(over);
+    __shared__ double ws[kFwdBlock / 32][3];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) {
+        ws[w][0] = sum;
+        ws[w][1] = mx;
+        ws[w][2] = over;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0, b = -1.7976931348623157e308, c = 0;
+        for (int q = 0; q < kFwdBlock / 32; ++q) {
+            a += ws[q][0];
+            b = std_max(b, ws[q][1]);
+            c += ws[q][2];
+        }
+        part[blockIdx.x * 3 + 0] = a;
+        part[blockIdx.x * 3 + 1] = b;
+        part[blockIdx.x * 3 + 2] = c;
+    }
+}
+
+// Ordered fold of k_unw_flag's partials into out[3] (one block of 256:
+// strided, then a fixed tree).
+__global__ void __launch_bounds__(256) k_unw_reduce(const double *__restrict__ part, long long nb,
+                                                    double *__restrict__ out) {
+    __shared__ double s[3][256];
+    const int t = threadIdx.x;
+    double a = 0, b = -1.7976931348623157e308, c = 0;
+    for (long long q = t; q < nb; q += 256) {
+        a += part[q * 3 + 0];
+        b = std_max(b, part[q * 3 + 1]);
+        c += part[q * 3 + 2];
+    }
+    s[0][t] = a;
+    s[1][t] = b;
+    s[2][t] = c;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (t < w) {
+            s[0][t] += s[0][t + w];
+            s[1][t] = std_max(s[1][t], s[1][t + w]);
+            s[2][t] += s[2][t + w];
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        out[0] = s[0][0];
+        out[1] = s[1][0];
+        out[2] = s[2][0];
+    }
+}
+
+// Kept event j (j < ctl_keep->n_acc) -> output slot base + j (< max_events):
+// momenta [event][leg][E, px, py, pz], weight sign(v) max(|v|, w_max),
+// channel.
+__global__ void __launch_bounds__(kFwdBlock) k_unw_write(
+    const int32_t *__restrict__ kept, const RoundCtl *__restrict__ ctl_keep, const int32_t *__restrict__ list,
+    const double *__restrict__ mom_soa, long long m, int n_ext, const int32_t *__restrict__ ich,
+    const double *__restrict__ rec_val, double w_max, long long base, long long max_events,
+    double *__restrict__ mom_out, double *__restrict__ wgt_out, int32_t *__restrict__ ch_out) {
+    const long long j = blockIdx.x * static_cast<long long>(kFwdBlock) + threadIdx.x;
+    if (j >= ctl_keep->n_acc || j >= m) return;
+    const long long e = base + j;
+    if (e >= max_events) return;
+    const long long i = kept[j];
+    const long long k = list[i];
+    const double v = rec_val[i];
+    if (mom_out)
+        for (int s = 0; s < n_ext; ++s) {
+            double *o = mom_out + (e * n_ext + s) * 4;
+            for (int c = 0; c < 4; ++c) o[c] = mom_soa[(4 * s + c) * m + k];
+        }
+    if (wgt_out) wgt_out[e] = copysign(std_max(fabs(v), w_max), v);
+    if (ch_out) ch_out[e] = ich[k];
+}
+
 }  // namespace chili_dev

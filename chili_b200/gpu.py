@@ -65,6 +65,8 @@ def _declare(lib):
         "chili_gpu_load_checkpoint": ([vp, C.c_char_p, P(abi.MultiChannelParams), vp, i64, P(i64)], i32),
         "chili_gpu_generate": ([vp, i64, u64, u64, vp, vp, vp], i32),
         "chili_gpu_evaluate_batch": ([vp, i32, vp, vp, i64], i32),
+        "chili_gpu_generate_unweighted": ([vp, i64, u64, u64, dbl, vp, vp, vp, i64, P(i64),
+                                           P(abi.UnweightInfo)], i32),
         "chili_gpu_flow_init": ([vp, P(abi.FlowParams)], i32),
         "chili_gpu_flow_nparams": ([vp], i64),
         "chili_gpu_flow_get_params": ([vp, vp], i32),
@@ -326,6 +328,22 @@ class Context:
         ch = np.empty(n, dtype=np.int32)
         self.call("chili_gpu_generate", int(n), int(seed), int(counter), _ptr(mom), _ptr(w), _ptr(ch))
         return mom, w, ch
+
+    def generate_unweighted(self, n, w_max, seed=7, counter=0, max_events=None, out=None):
+        """Unweighted events of n drawn points: (mom [k, n_ext, 4], wgt [k],
+        ch [k], UnweightInfo), k = min(kept, max_events).  out: optional
+        (mom, wgt, ch) buffers (numpy or device tensors) of max_events rows."""
+        if max_events is None:
+            max_events = n
+        if out is None:
+            out = (np.empty((max_events, self.n_ext, 4)), np.empty(max_events), np.empty(max_events, dtype=np.int32))
+        mom, wgt, ch = out
+        ne = C.c_int64()
+        info = abi.UnweightInfo()
+        self.call("chili_gpu_generate_unweighted", int(n), int(seed), int(counter), float(w_max), _ptr(mom),
+                  _ptr(wgt), _ptr(ch), int(max_events), C.byref(ne), C.byref(info))
+        k = min(ne.value, max_events)
+        return mom[:k], wgt[:k], ch[:k], info
 
     def evaluate_batch(self, ch, u):
         u = _f64(u)

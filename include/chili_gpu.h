@@ -364,6 +364,34 @@ int chili_gpu_generate(chili_ctx *ctx, int64_t n, uint64_t seed,
                        uint64_t counter_base, double *mom, double *wgt,
                        int32_t *ch);
 
+/* What one chili_gpu_generate_unweighted call did. */
+typedef struct {
+    uint64_t points;        /* points drawn (= n)                              */
+    uint64_t rejected_pre;  /* PreProcess rejections (value 0, never kept)     */
+    uint64_t kept;          /* unweighted events (also those beyond max_events)*/
+    uint64_t overweight;    /* kept events with |value| > w_max                */
+    double sum;             /* sum of the values of all n points               */
+    double max;             /* largest value                                   */
+} chili_unweight_info;
+
+/* Unweighted events: the unweighting stage the reference leaves to the
+ * PostProcess hook of MultiChannel::operator() (MultiChannel.hh:240-245).
+ * n points are drawn in counter order (counters counter_base ...: the same
+ * points as chili_gpu_multichannel_iterate draws), passed through PreProcess
+ * and given the value v = f * w (the combined multichannel weight; 0 for a
+ * rejected point or a NaN value).  Point k is kept when r_k * w_max < |v_k|,
+ * r_k the uniform of the "accept" stream (Philox4x32-10, key seed, block
+ * {0, lo(k), hi(k), 1}, words 0 and 1).  Kept events are written in counter
+ * order: mom[max_events * n_ext * 4], wgt[max_events] = sign(v) max(|v|,
+ * w_max) (so that sum(wgt) / n estimates the integral), ch[max_events]; any
+ * output may be NULL; n_events (may be NULL) receives the number kept, which
+ * counts the events beyond max_events too (they are not written).
+ * w_max > 0, e.g. the weight_max of an earlier iteration.  Host or device
+ * outputs; no counterpart in the reference's own code. */
+int chili_gpu_generate_unweighted(chili_ctx *ctx, int64_t n, uint64_t seed, uint64_t counter_base, double w_max,
+                                  double *mom, double *wgt, int32_t *ch, int64_t max_events, int64_t *n_events,
+                                  chili_unweight_info *info);
+
 /* Interface::Evaluate (nanobind.hh:23-50) / CallChili (Tensorflow.cc:22-135):
  * uniforms u[n*ndims] through channel ch's FSMapper alone (no VEGAS grid):
  * out[n] = f * FSMapper weight, 0 where PreProcess rejects or the weight is 0.

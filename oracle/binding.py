@@ -78,6 +78,8 @@ def _load(path, prefix):
         "ref_mc_run_native": ([vp, u32, i32, P(abi.Stats)], None),
         "ref_evaluate_batch": ([vp, i32, vp, i64, vp], None),
         "ref_philox_uniforms": ([C.c_uint64, C.c_uint64, i64, i32, vp], None),
+        "ref_philox_stream_uniforms": ([C.c_uint64, C.c_uint64, i64, i32, C.c_uint32, vp], None),
+        "ref_mc_point_values": ([vp, vp, i64, vp, vp, vp], None),
     }
     for name, (args, res) in sigs.items():
         real = prefix + name[4:]
@@ -263,6 +265,14 @@ class MultiChannel:
         self.oracle().ref_mc_train(self.h, _p(np.ascontiguousarray(hist, dtype=np.float64)),
                                    _p(np.ascontiguousarray(atrain, dtype=np.float64)))
 
+    def point_values(self, u):
+        """Value f*w of each point, no retries (the C port only): (val, ich, mom)."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        n = u.shape[0]
+        val, ich, mom = np.empty(n), np.empty(n, dtype=np.int32), np.empty((n, self.n_ext, 4))
+        self.oracle().ref_mc_point_values(self.h, _p(u), n, _p(val), _p(ich), _p(mom))
+        return val, ich, mom
+
     def run_native(self, seed, niter):
         st = abi.Stats()
         self.oracle().ref_mc_run_native(self.h, seed, niter, C.byref(st))
@@ -281,3 +291,12 @@ def philox_uniforms(seed, ctr0, n, d, oracle=None):
     out = np.empty((n, d))
     oracle().ref_philox_uniforms(seed, ctr0, n, d, _p(out))
     return out
+
+
+def philox_stream_uniforms(seed, ctr0, n, d, stream, oracle=None):
+    """Stream `stream` of the CUDA library's counter-based generator (port only)."""
+    oracle = oracle or PORT
+    out = np.empty((n, d))
+    oracle().ref_philox_stream_uniforms(seed, ctr0, n, d, stream, _p(out))
+    return out
+

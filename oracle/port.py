@@ -14,6 +14,7 @@ am_split = partial(binding.am_split, oracle=PORT)
 vegas_iterate = partial(binding.vegas_iterate, oracle=PORT)
 select = partial(binding.select, oracle=PORT)
 philox_uniforms = partial(binding.philox_uniforms, oracle=PORT)
+philox_stream_uniforms = partial(binding.philox_stream_uniforms, oracle=PORT)
 MultiChannel = partial(binding.MultiChannel, oracle=PORT)
 
 

@@ -45,6 +45,19 @@ static void philox(uint32_t c[4], uint32_t k0, uint32_t k1) {
 static double u53(uint32_t hi, uint32_t lo) {
     return (double)(((uint64_t)hi << 21) | (lo >> 11)) * 0x1.0p-53;
 }
+/* Stream s of the same generator: block word 3 = s (0: the points, 1: the
+ * unweighting stage's accept uniforms). */
+void orc_philox_stream_uniforms(uint64_t seed, uint64_t ctr0, int64_t n, int d, uint32_t stream, double *out) {
+    for (int64_t i = 0; i < n; ++i) {
+        uint64_t k = ctr0 + (uint64_t)i;
+        for (int q = 0; 2 * q < d; ++q) {
+            uint32_t c[4] = {(uint32_t)q, (uint32_t)k, (uint32_t)(k >> 32), stream};
+            philox(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+            out[i * d + 2 * q] = u53(c[0], c[1]);
+            if (2 * q + 1 < d) out[i * d + 2 * q + 1] = u53(c[2], c[3]);
+        }
+    }
+}
 void orc_philox_uniforms(uint64_t seed, uint64_t ctr0, int64_t n, int d, double *out) {
     for (int64_t i = 0; i < n; ++i) {
         uint64_t k = ctr0 + (uint64_t)i;
@@ -875,6 +888,35 @@ int orc_mc_iterate(void *p, const double *u, int64_t n_u, int guard, chili_stats
     free(train);
     st_out(&st, out);
     return 0;
+}
+/* The value of each point of MultiChannel::operator() (MultiChannel.hh:
+ * 214-233) without retries: uniforms u[n][D+1] -> channel, momenta, value
+ * f * w (0 for a PreProcess rejection or a NaN value); the input of the
+ * unweighting stage.  mom (n * n_ext * 4) and ich may be NULL. */
+void orc_mc_point_values(void *p, const double *u, int64_t n, double *val, int32_t *ich_out, double *mom_out) {
+    mc_t *m = p;
+    int D = m->ndims, B = m->bins;
+    size_t gs = (size_t)D * (B + 1);
+    double dens[CHILI_MAX_CHANNELS];
+    for (int64_t i = 0; i < n; ++i) {
+        const double *uk = u + i * (D + 1);
+        double x[CHILI_MAX_DIMS], xs[CHILI_MAX_DIMS] = {0}, jac;
+        memcpy(x, uk, sizeof(double) * D);
+        int ich = select1(m->alpha, m->nch, uk[D]);
+        v4 mom[NSLOT];
+        if (am_map1(m->grids + ich * gs, D, B, x, &jac)) fs_gen(&m->ch[ich], x, mom);
+        else for (int s = 0; s < m->n_ext; ++s) { v4 z = {NAN, NAN, NAN, NAN}; mom[s] = z; }
+        double v = 0;
+        if (preprocess_ok(m, mom)) {
+            double wgt = combined(m, mom, ich, dens, xs);
+            double f = eval_f(m, mom);
+            v = wgt == 0 ? 0 : f * wgt;
+            if (isnan(v)) v = 0;
+        }
+        val[i] = v;
+        if (ich_out) ich_out[i] = ich;
+        if (mom_out) memcpy(mom_out + i * m->n_ext * 4, mom, sizeof(double) * 4 * m->n_ext);
+    }
 }
 void orc_mc_get_training(void *p, double *h, double *a) {
     mc_t *m = p;

@@ -190,3 +190,21 @@ def test_port_philox_is_the_published_algorithm():
             if 2 * q + 1 < d:
                 assert got[i, 2 * q + 1] == u1
     assert (got >= 0).all() and (got < 1).all()
+
+
+def test_point_values_and_accept_stream():
+    """The oracle's per-point values (input of the unweighting stage) are the
+    fixed-budget iteration's values: same sum and nonzero count; stream 0 of
+    the stream generator is the points' generator."""
+    cs = workloads.channel_set(4)
+    params = workloads.mc_params(3000)
+    O = port.MultiChannel(cs, 20, params, abi.CHILI_FUNC_PROPAGATOR, channels.propagator_params())
+    O.set_cuts(cs.sqrts)
+    u = port.philox_uniforms(9, 100, 3000, O.ndims + 1)
+    assert np.array_equal(u, port.philox_stream_uniforms(9, 100, 3000, O.ndims + 1, 0))
+    assert not np.array_equal(u[:, :2], port.philox_stream_uniforms(9, 100, 3000, 2, 1))
+    val, ich, mom = O.point_values(u)
+    O.set_fixed_budget(True)
+    st, info = O.iterate(u)
+    assert st.n == 3000 and st.n_finite == np.count_nonzero(val)
+    assert abs(st.sum - val.sum()) <= 1e-13 * abs(val).sum()
