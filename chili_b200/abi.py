@@ -132,6 +132,16 @@ class FlowIterInfo(C.Structure):
                 ("weight_max", C.c_double), ("unweighting_efficiency", C.c_double)]
 
 
+COMBINABLE_FN = C.CFUNCTYPE(C.c_int, C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.c_void_p)
+
+
+class Model(C.Structure):
+    """chili_model: Combinable callback and |pid|-keyed masses and widths."""
+    _fields_ = [("combinable", COMBINABLE_FN), ("user", C.c_void_p),
+                ("n_masses", C.c_int32), ("masses", C.POINTER(IdxValue)),
+                ("n_widths", C.c_int32), ("widths", C.POINTER(IdxValue))]
+
+
 class UnweightInfo(C.Structure):
     """chili_unweight_info."""
     _fields_ = [("points", C.c_uint64), ("rejected_pre", C.c_uint64), ("kept", C.c_uint64),

@@ -14,7 +14,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libchili_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["chili_gpu.cu", "flow.cu", "flow_layers.cu", "flow_alpha.cu", "channel_program.cpp", "checkpoint.cu", "batch.cu"]
+SOURCES = ["chili_gpu.cu", "flow.cu", "flow_layers.cu", "flow_alpha.cu", "channel_program.cpp", "checkpoint.cu", "batch.cu", "construct.cpp"]
 
 
 def nvcc():

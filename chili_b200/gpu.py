@@ -79,6 +79,10 @@ def _declare(lib):
         "chili_gpu_flow_train": ([vp, i32, u64, u64, vp], i32),
         "chili_gpu_flow_iterate": ([vp, u64, u64, u64, i32, P(abi.Stats), P(abi.FlowIterInfo)], i32),
         "chili_gpu_tc_selftest": ([vp, i32, i32, i32, vp, vp, vp], i32),
+        "chili_construct_channels": ([dbl, vp, i32, P(abi.Model), P(abi.Cuts), i32, P(vp), C.c_char_p,
+                                      C.c_size_t], i32),
+        "chili_channel_list_get": ([vp, P(P(abi.ChannelDesc)), P(i32), P(P(abi.Cuts))], i32),
+        "chili_channel_list_free": ([vp], None),
         "chili_gpu_batch_set": ([vp, P(abi.Task), i32], i32),
         "chili_gpu_batch_iterate": ([vp, i32, u64, i32, vp, P(abi.BatchInfo)], i32),
         "chili_gpu_batch_get_grid": ([vp, i32, vp, vp], i32),
@@ -489,6 +493,62 @@ def flow_layout(dims, nch, n_ext, layers=6):
     shape) with the oracle's parameter names."""
     from . import flowspec
     return flowspec.layout(dims, nch, n_ext, layers)
+
+
+def construct_channels(flavs, combinable, masses, widths, sqrts, cuts=None, smax=2):
+    """ConstructChannels (src/Channel/ChannelNode.cc:74-291) in the library:
+    flavs = incoming then outgoing flavours; combinable = callable (f1, f2) ->
+    flavours, or a dict {(f1, f2): [flavours]}; masses / widths = {pid:
+    value} (keyed by |pid|); cuts = None (the reference's default cuts) or a
+    cut dict (channels.default_cuts layout).  Returns an abi.ChannelSet for
+    Context.set_channels."""
+    lib = load()
+    fn = (lambda a, b: combinable.get((a, b), [])) if isinstance(combinable, dict) else combinable
+
+    def cb(f1, f2, out, max_out, user):
+        try:
+            r = [int(v) for v in fn(int(f1), int(f2))]
+        except Exception:
+            return -1
+        if len(r) > max_out:
+            return -1
+        for i, v in enumerate(r):
+            out[i] = v
+        return len(r)
+
+    cfn = abi.COMBINABLE_FN(cb)
+    mt = (abi.IdxValue * max(1, len(masses)))(*[abi.IdxValue(abs(int(k)), float(v)) for k, v in masses.items()])
+    wt = (abi.IdxValue * max(1, len(widths)))(*[abi.IdxValue(abs(int(k)), float(v)) for k, v in widths.items()])
+    model = abi.Model(cfn, None, len(masses), mt, len(widths), wt)
+    fl = (C.c_int32 * len(flavs))(*[int(f) for f in flavs])
+    cin = abi.ChannelSet([], cuts, sqrts, len(flavs)) if cuts is not None else None
+    h = C.c_void_p()
+    err = C.create_string_buffer(512)
+    rc = lib.chili_construct_channels(float(sqrts), fl, len(flavs), C.byref(model),
+                                      C.byref(cin.cuts) if cin else None, int(smax), C.byref(h), err, 512)
+    if rc != 0:
+        raise ChiliError(rc, err.value.decode())
+    try:
+        dp, n, cp = C.POINTER(abi.ChannelDesc)(), C.c_int32(), C.POINTER(abi.Cuts)()
+        lib.chili_channel_list_get(h, C.byref(dp), C.byref(n), C.byref(cp))
+        chans = []
+        for i in range(n.value):
+            d = dp[i]
+            info = [abi.ParticleInfo(d.info[k].idx, d.info[k].pid, d.info[k].mass, d.info[k].width)
+                    for k in range(d.n_info)]
+            dec = [abi.Decay(*[abi.ParticleInfo(q.idx, q.pid, q.mass, q.width)
+                               for q in (d.decays[k].parent, d.decays[k].child1, d.decays[k].child2)])
+                   for k in range(d.n_decays)]
+            chans.append((info, dec))
+        c = cp.contents
+        out_cuts = {"sexternal": [c.sexternal[k] for k in range(c.n_sexternal)],
+                    "deltaR": {(c.deltaR[k].pid1, c.deltaR[k].pid2): c.deltaR[k].value for k in range(c.n_deltaR)},
+                    "smin": {c.smin[k].idx: c.smin[k].value for k in range(c.n_smin)},
+                    "ptmin": {c.ptmin[k].idx: c.ptmin[k].value for k in range(c.n_ptmin)},
+                    "etamax": {c.etamax[k].idx: c.etamax[k].value for k in range(c.n_etamax)}}
+    finally:
+        lib.chili_channel_list_free(h)
+    return abi.ChannelSet(chans, out_cuts, sqrts, len(flavs))
 
 
 def check_channels(cs):

@@ -21,10 +21,13 @@
 
 #include <cmath>
 #include <cstdint>
+#include <functional>
 #include <map>
+#include <memory>
 #include <ostream>
 #include <stdexcept>
 #include <string>
+#include <unordered_map>
 #include <utility>
 #include <vector>
 
@@ -249,6 +252,97 @@ class ChannelSet {
     std::vector<chili_idx_value> smin_, ptmin_, etamax_;
     chili_cuts cuts_{};
 };
+
+// Model (Model.hh:10-29): which flavours two currents combine into, and the
+// masses and widths by |pid|.
+class Model {
+  public:
+    Model(std::function<std::vector<int>(int, int)> func, std::unordered_map<unsigned, double> masses = {})
+        : combinable_(std::move(func)), masses_(std::move(masses)) {}
+    double &Mass(int flav) { return masses_[static_cast<unsigned>(std::abs(flav))]; }
+    double &Width(int flav) { return widths_[static_cast<unsigned>(std::abs(flav))]; }
+    void SetMasses(std::unordered_map<unsigned, double> m) { masses_ = std::move(m); }
+    void SetWidths(std::unordered_map<unsigned, double> w) { widths_ = std::move(w); }
+    std::vector<int> Combinable(int f1, int f2) const { return combinable_(f1, f2); }
+    const std::unordered_map<unsigned, double> &Masses() const { return masses_; }
+    const std::unordered_map<unsigned, double> &Widths() const { return widths_; }
+
+  private:
+    std::function<std::vector<int>(int, int)> combinable_;
+    std::unordered_map<unsigned, double> masses_, widths_;
+};
+
+namespace detail {
+inline int combinable_trampoline(int32_t f1, int32_t f2, int32_t *out, int32_t max_out, void *user) {
+    try {
+        const auto v = static_cast<const Model *>(user)->Combinable(f1, f2);
+        if (static_cast<int32_t>(v.size()) > max_out) return -1;
+        for (size_t i = 0; i < v.size(); ++i) out[i] = v[i];
+        return static_cast<int>(v.size());
+    } catch (...) {
+        return -1;
+    }
+}
+
+inline ParticleInfo from_c(const chili_particle_info &p) { return ParticleInfo{p.idx, p.pid, p.mass, p.width}; }
+
+// The library's ConstructChannels; cuts == nullptr for the default cuts.
+inline std::pair<std::vector<ChannelDescription>, Cuts> construct(double sqrts, const std::vector<int> &flavs,
+                                                                  const Model &model, const Cuts *cuts,
+                                                                  size_t smax) {
+    std::vector<chili_idx_value> mt, wt;
+    for (const auto &kv : model.Masses()) mt.push_back({kv.first, kv.second});
+    for (const auto &kv : model.Widths()) wt.push_back({kv.first, kv.second});
+    chili_model m{&combinable_trampoline, const_cast<Model *>(&model), static_cast<int32_t>(mt.size()), mt.data(),
+                  static_cast<int32_t>(wt.size()), wt.data()};
+    std::vector<int32_t> fl(flavs.begin(), flavs.end());
+    std::unique_ptr<ChannelSet> cin;
+    if (cuts) cin = std::make_unique<ChannelSet>(std::vector<ChannelDescription>{}, *cuts, sqrts, static_cast<int>(flavs.size()));
+    chili_channel_list *list = nullptr;
+    char err[512];
+    const int rc = chili_construct_channels(sqrts, fl.data(), static_cast<int>(fl.size()), &m,
+                                            cin ? cin->cuts() : nullptr, static_cast<int>(smax), &list, err,
+                                            sizeof(err));
+    if (rc != CHILI_OK) throw Error(rc, err);
+    const chili_channel_desc *d = nullptr;
+    const chili_cuts *c = nullptr;
+    int n = 0;
+    chili_channel_list_get(list, &d, &n, &c);
+    std::vector<ChannelDescription> out(static_cast<size_t>(n));
+    for (int i = 0; i < n; ++i) {
+        for (int k = 0; k < d[i].n_info; ++k) out[i].info.push_back(from_c(d[i].info[k]));
+        for (int k = 0; k < d[i].n_decays; ++k)
+            out[i].decays.push_back({from_c(d[i].decays[k].parent),
+                                     {from_c(d[i].decays[k].child1), from_c(d[i].decays[k].child2)}});
+    }
+    Cuts oc;
+    oc.sexternal.assign(c->sexternal, c->sexternal + c->n_sexternal);
+    for (int k = 0; k < c->n_deltaR; ++k) oc.deltaR[{c->deltaR[k].pid1, c->deltaR[k].pid2}] = c->deltaR[k].value;
+    for (int k = 0; k < c->n_smin; ++k) oc.smin[c->smin[k].idx] = c->smin[k].value;
+    for (int k = 0; k < c->n_ptmin; ++k) oc.ptmin[c->ptmin[k].idx] = c->ptmin[k].value;
+    for (int k = 0; k < c->n_etamax; ++k) oc.etamax[c->etamax[k].idx] = c->etamax[k].value;
+    chili_channel_list_free(list);
+    return {std::move(out), std::move(oc)};
+}
+}  // namespace detail
+
+// ConstructChannels (ChannelNode.cc:74-291): the channel set of a process
+// (flavours: the two incoming, then the outgoing) with the default cuts
+// (Delta R 0.4, pT > 30, |eta| < 99).  Where the reference returns one
+// FSMapper per channel, this returns the set a MultiChannel is built on.
+inline ChannelSet ConstructChannels(double sqrts, const std::vector<int> &flavs, const Model &model,
+                                    size_t smax = 2) {
+    auto r = detail::construct(sqrts, flavs, model, nullptr, smax);
+    return ChannelSet(r.first, r.second, sqrts, static_cast<int>(flavs.size()));
+}
+// With given cuts, completed in place with the currents' pT and eta entries
+// (ChannelNode.cc:161-162), as the reference's second overload does.
+inline ChannelSet ConstructChannels(double sqrts, const std::vector<int> &flavs, const Model &model, Cuts &cuts,
+                                    size_t smax = 2) {
+    auto r = detail::construct(sqrts, flavs, model, &cuts, smax);
+    cuts = r.second;
+    return ChannelSet(r.first, r.second, sqrts, static_cast<int>(flavs.size()));
+}
 
 // MultiChannelParams (MultiChannel.hh:29-49).
 struct MultiChannelParams {

@@ -284,6 +284,43 @@ int chili_gpu_set_channels(chili_ctx *ctx, const chili_channel_desc *descs,
  * CHILI_ERR_INVALID_ARG with the reason in err[err_len]. */
 int chili_gpu_check_channels(const chili_channel_desc *descs, int nch, const chili_cuts *cuts, double sqrts,
                              int n_ext, char *err, size_t err_len);
+/* ------------------------------------------------------ channel construction
+ * ConstructChannels (src/Channel/ChannelNode.cc:74-291) on the host: the
+ * FSMapper channel descriptions of a process from a model, to be passed to
+ * chili_gpu_set_channels.  The Model (include/Model/Model.hh:10-29):
+ * Combinable(f1, f2) is a callback that writes the flavours two currents
+ * combine into (at most max_out) to out and returns their number (< 0:
+ * error); masses and widths are keyed by |pid| and must hold every flavour
+ * the enumeration meets (the reference's Model::Mass/Width use .at). */
+typedef int (*chili_combinable_fn)(int32_t f1, int32_t f2, int32_t *out, int32_t max_out, void *user);
+typedef struct {
+    chili_combinable_fn combinable;
+    void *user;
+    int32_t n_masses;
+    const chili_idx_value *masses;
+    int32_t n_widths;
+    const chili_idx_value *widths;
+} chili_model;
+
+typedef struct chili_channel_list chili_channel_list;
+
+/* flavs[n_flavs]: the two incoming then the outgoing flavours (all-outgoing
+ * convention, as the reference's flavs).  cuts == NULL: the first overload
+ * (ChannelNode.cc:74-96: Delta R 0.4 between all flavours, 0 with a top;
+ * pT > 30, |eta| < 99, smin = m^2 on every leg); else the second, which adds
+ * pT 0 / |eta| 99 entries for the internal currents.  smax: the largest
+ * number of s-channel joins (the reference's default is 2).  On success *out
+ * holds the descriptions in the reference's order (its std::set order, with
+ * its rule that descriptions with equal (idx, mass, width) lists are one) and
+ * the completed cuts; free with chili_channel_list_free.  err (may be NULL)
+ * receives the reason of a failure. */
+int chili_construct_channels(double sqrts, const int32_t *flavs, int n_flavs, const chili_model *model,
+                             const chili_cuts *cuts, int smax, chili_channel_list **out, char *err, size_t err_len);
+/* The list's descriptions and cuts (owned by the list). */
+int chili_channel_list_get(const chili_channel_list *list, const chili_channel_desc **descs, int *nch,
+                           const chili_cuts **cuts);
+void chili_channel_list_free(chili_channel_list *list);
+
 /* Phase-space dimensions of the channels, 3*(n_ext-2)-2 (Channel.hh:33). */
 int chili_gpu_ndims(const chili_ctx *ctx);
 /* FSMapper::GeneratePoint (Channel.cc:22-38): x[n*ndims] -> mom[n*n_ext*4]

@@ -80,6 +80,8 @@ def _load(path, prefix):
         "ref_philox_uniforms": ([C.c_uint64, C.c_uint64, i64, i32, vp], None),
         "ref_philox_stream_uniforms": ([C.c_uint64, C.c_uint64, i64, i32, C.c_uint32, vp], None),
         "ref_mc_point_values": ([vp, vp, i64, vp, vp, vp], None),
+        "ref_construct_channels": ([dbl, vp, i32, vp, i32, vp, i32, vp, i32, P(abi.Cuts), i32, vp, i64, P(i64),
+                                    vp, P(i32), vp, P(i32), i32], i32),
     }
     for name, (args, res) in sigs.items():
         real = prefix + name[4:]
@@ -299,4 +301,60 @@ def philox_stream_uniforms(seed, ctr0, n, d, stream, oracle=None):
     out = np.empty((n, d))
     oracle().ref_philox_stream_uniforms(seed, ctr0, n, d, stream, _p(out))
     return out
+
+
+def construct_channels(sqrts, flavs, rules, masses, widths, cuts=None, smax=2, oracle=REF):
+    """The reference's ConstructChannels (the reference build only) with a
+    Model whose Combinable is the table rules {(f1, f2): [flavours]}.
+    Returns (channels, ptmin, etamax): channels = [(info, decays)] with info
+    [(idx, pid, mass, width)] and decays [(parent, child1, child2)] from the
+    mappers' serialized descriptions, in the reference's order; ptmin and
+    etamax the completed cut tables (second overload only, else {})."""
+    import struct
+    rows = []
+    for (f1, f2), out in rules.items():
+        out = list(out)
+        rows.append([f1, f2, len(out)] + out + [0] * (8 - len(out)))
+    rt = np.ascontiguousarray(rows if rows else np.zeros((0, 11)), dtype=np.int32)
+    fl = np.ascontiguousarray(flavs, dtype=np.int32)
+    mt = (abi.IdxValue * max(1, len(masses)))(*[abi.IdxValue(abs(k), v) for k, v in masses.items()])
+    wt = (abi.IdxValue * max(1, len(widths)))(*[abi.IdxValue(abs(k), v) for k, v in widths.items()])
+    cin = abi.ChannelSet([], cuts, sqrts, len(flavs)) if cuts is not None else None
+    cap = 1 << 24
+    buf = C.create_string_buffer(cap)
+    ln = C.c_int64()
+    po, eo = (abi.IdxValue * 1024)(), (abi.IdxValue * 1024)()
+    npo, neo = C.c_int(), C.c_int()
+    n = oracle().ref_construct_channels(float(sqrts), _p(fl), len(flavs), _p(rt), len(rows), mt, len(masses), wt,
+                                        len(widths), C.byref(cin.cuts) if cin else None, int(smax), buf, cap,
+                                        C.byref(ln), po, C.byref(npo), eo, C.byref(neo), 1024)
+    if n < 0:
+        raise RuntimeError("the reference's ConstructChannels threw")
+    data = buf.raw[:ln.value]
+    pos = 0
+
+    def take(fmt):
+        nonlocal pos
+        v = struct.unpack_from(fmt, data, pos)
+        pos += struct.calcsize(fmt)
+        return v
+
+    def pinfo():
+        return take("<Iidd")
+
+    chans = []
+    for _ in range(n):
+        (nl,) = take("<Q")
+        pos += nl  # mapper name
+        (ni,) = take("<Q")
+        info = [pinfo() for _ in range(ni)]
+        (nd,) = take("<Q")
+        dec = [(pinfo(), pinfo(), pinfo()) for _ in range(nd)]
+        take("<ddQQ")
+        (npt,) = take("<Q")
+        take("<%dd" % npt)
+        chans.append((info, dec))
+    ptmin = {po[k].idx: po[k].value for k in range(npo.value)} if cuts is not None else {}
+    etamax = {eo[k].idx: eo[k].value for k in range(neo.value)} if cuts is not None else {}
+    return chans, ptmin, etamax
 

@@ -4,7 +4,7 @@ TEST INFRASTRUCTURE ONLY.
 """
 from functools import partial
 
-from .binding import REF, MultiChannel as _MC, am_adapt, am_map, am_split, am_weight, select, vegas_iterate, vegas_run  # noqa: F401
+from .binding import REF, MultiChannel as _MC, am_adapt, am_map, am_split, am_weight, construct_channels, select, vegas_iterate, vegas_run  # noqa: F401
 
 
 def available():

@@ -20,12 +20,14 @@
 #include <random>
 #include <sstream>
 #include <stdexcept>
+#include <unordered_map>
 #include <vector>
 
 #include "Channel/Channel.hh"
 #include "Channel/ChannelNode.hh"
 #include "Channel/Integrand.hh"
 #include "Channel/MultiChannel.hh"
+#include "Model/Model.hh"
 #include "Integrator/AdaptiveMap.hh"
 #include "Integrator/Statistics.hh"
 #include "Integrator/Vegas.hh"
@@ -621,6 +623,62 @@ void ref_evaluate_batch(void *p, int ch, const double *u, int64_t n, double *out
         double val = weight == 0 ? 0 : h->integrand(point) * weight;
         if (!h->integrand.PostProcess()(point, val)) val = 0;
         out[i] = val;
+    }
+}
+
+// ------------------------------------------------------ ConstructChannels
+// The reference's ConstructChannels (ChannelNode.cc:74-291) with a Model
+// whose Combinable reads a rule table: rows of 11 int32 {f1, f2, n, out[8]}.
+// cuts == NULL: the first overload.  Every mapper's Mapper::Serialize bytes
+// are appended to buf (cap bytes; *len = bytes needed); for the second
+// overload the completed ptmin and etamax tables come back as (idx, value)
+// pairs (capacity max_cut entries each).  Returns the number of channels, or
+// -1 when the reference throws (e.g. a flavour missing from the masses).
+int ref_construct_channels(double sqrts, const int32_t *flavs, int n, const int32_t *rules, int n_rules,
+                           const chili_idx_value *masses, int nm, const chili_idx_value *widths, int nw,
+                           const chili_cuts *cuts, int smax, char *buf, int64_t cap, int64_t *len,
+                           chili_idx_value *ptmin_out, int *n_ptmin, chili_idx_value *etamax_out, int *n_etamax,
+                           int max_cut) {
+    try {
+        std::vector<int32_t> table(rules, rules + 11 * n_rules);
+        auto comb = [table, n_rules](int f1, int f2) {
+            std::vector<int> out;
+            for (int r = 0; r < n_rules; ++r) {
+                const int32_t *row = table.data() + 11 * r;
+                if (row[0] == f1 && row[1] == f2) out.insert(out.end(), row + 3, row + 3 + row[2]);
+            }
+            return out;
+        };
+        std::unordered_map<unsigned int, double> mm, ww;
+        for (int i = 0; i < nm; ++i) mm[masses[i].idx] = masses[i].value;
+        for (int i = 0; i < nw; ++i) ww[widths[i].idx] = widths[i].value;
+        chili::Model model(comb, mm);
+        model.SetWidths(ww);
+        const std::vector<int> fl(flavs, flavs + n);
+        std::vector<std::unique_ptr<chili::FSMapper>> maps;
+        chili::Cuts c;
+        if (cuts) {
+            c = to_cuts(cuts);
+            maps = chili::ConstructChannels(sqrts, fl, model, c, static_cast<size_t>(smax));
+        } else {
+            maps = chili::ConstructChannels(sqrts, fl, model, static_cast<size_t>(smax));
+        }
+        std::ostringstream os;
+        for (const auto &m : maps) chili::Mapper<FourVector>::Serialize(os, *m);
+        const std::string bytes = os.str();
+        *len = static_cast<int64_t>(bytes.size());
+        if (buf && static_cast<int64_t>(bytes.size()) <= cap) std::memcpy(buf, bytes.data(), bytes.size());
+        int k = 0;
+        for (const auto &kv : c.ptmin)
+            if (k < max_cut) ptmin_out[k++] = chili_idx_value{kv.first, kv.second};
+        *n_ptmin = k;
+        k = 0;
+        for (const auto &kv : c.etamax)
+            if (k < max_cut) etamax_out[k++] = chili_idx_value{kv.first, kv.second};
+        *n_etamax = k;
+        return static_cast<int>(maps.size());
+    } catch (...) {
+        return -1;
     }
 }
 

@@ -286,3 +286,22 @@ def test_multichannel_iteration_degenerate_grids(ctx_factory, rng, mc2):
     assert info.points_tried == info_r.points_tried
     assert st.n == st_r.n and st.n_finite == st_r.n_finite
     assert rel(st.sum, st_r.sum) < 1e-11
+
+
+def test_constructed_channels_iterate_like_the_reference(ctx_factory, rng):
+    """A channel set from the library's ConstructChannels (gluon 2->4, smax 2:
+    14 channels with massless s-channel decays) on the GPU against the
+    reference's MultiChannel built from the same descriptions."""
+    from chili_b200 import gpu
+    flavs = [21] * 6
+    cs = gpu.construct_channels(flavs, {(21, 21): [21]}, {21: 0.0}, {21: 0.0}, 1000.0, smax=2)
+    assert cs.nch == 14
+    ncalls = 20_000
+    ctx, R, params = _mc_pair(ctx_factory, cs, 50, ncalls, rng)
+    u = uniforms53(rng, (4 * ncalls, R.ndims + 1))
+    st, info = ctx.multichannel_iterate(params, u=u, guard=True)
+    st_r, info_r = R.iterate(u, guard=True)
+    assert info.points_tried == info_r.points_tried and info.rejected_pre == info_r.rejected_pre
+    assert st.n == st_r.n and st.n_finite == st_r.n_finite
+    assert rel(st.sum, st_r.sum) < 1e-11 and rel(st.sum2, st_r.sum2) < 1e-11
+    assert np.max(rel(ctx.get_alpha()[0], R.get_alpha()[0])) < 1e-11
