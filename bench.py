@@ -40,9 +40,24 @@ FLOW_KERNELS = ["k_flow_layer", "k_flow_layer_bwd", "k_flow_wgrad", "k_alpha_tra
                 "k_pp_nodes", "k_pp_items", "k_pp_chains", "k_pp_channel"]
 METRIC = "time to 0.1% error & unweighted events/s: flow vs plain VEGAS, 1 B200, FP64"
 UNIT = "unweighted events/s"
-NCALLS = 1_000_000
 SEED = 7
-BINS = 100
+
+# The two multichannel workloads: the 2->4 iteration (the headline) and the
+# large 2->6 case. channels(): the channel set; fkind: the integrand.
+WORKLOADS = {
+    "multichannel": {"n_out": 4, "bins": 100, "ncalls": 1_000_000, "fkind": "PROPAGATOR", "flow_layers": 6,
+                     "metric": METRIC, "dims": 10, "channels": 15,
+                     "describe": "multichannel 2->4 propagator integrand, sqrt(S)=1 TeV, 10 dims",
+                     "unweighted_target": None},
+    "large": {"n_out": 6, "bins": 200, "ncalls": 10_000_000, "fkind": "PROPAGATOR_TOP2", "flow_layers": 10,
+              "metric": "time to 0.1% error & unweighting efficiency, 2->6 (45 channels, 200 bins, 1e7 "
+                        "points/iteration): flow vs plain VEGAS, 1 B200, FP64",
+              "dims": 16, "channels": 45,
+              "describe": "multichannel 2->6, product of the two largest pair propagators x t-channel factors, "
+                          "sqrt(S)=1 TeV, 16 dims",
+              "unweighted_target": 1_000_000},
+}
+WL = WORKLOADS["multichannel"]
 
 
 def parse():
@@ -51,15 +66,17 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="chili", choices=["chili", "reference"])
-    ap.add_argument("--ncalls", type=int, default=NCALLS)
+    ap.add_argument("--ncalls", type=int, default=None, help="points per iteration (default: the workload's)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-flow", action="store_true")
     ap.add_argument("--flow-steps", type=int, default=200)
     ap.add_argument("--flow-batch", type=int, default=65536)
-    ap.add_argument("--workload", default="multichannel", choices=["multichannel", "batched"],
-                    help="multichannel: the 2->4 iteration with the learned proposal beside it; batched: 512 "
-                         "uneven integrands in one persistent graph-replayed launch per iteration")
+    ap.add_argument("--workload", default="multichannel", choices=["multichannel", "large", "batched"],
+                    help="multichannel: the 2->4 iteration with the learned proposal beside it; large: the "
+                         "2->6 case (45 channels, 200 bins, 1e7 points per iteration, 10-layer flow, 1e6 "
+                         "unweighted events); batched: 512 uneven integrands in one persistent graph-replayed "
+                         "launch per iteration")
     ap.add_argument("--batch-scale", type=float, default=1.0,
                     help="batched: point counts times this factor (small cases for profiling)")
     ap.add_argument("--no-sequential", action="store_true",
@@ -68,11 +85,12 @@ def parse():
 
 
 def workload_config(ncalls):
-    return {"workload": "multichannel 2->4 propagator integrand, sqrt(S)=1 TeV, 10 dims",
-            "channels": 15, "bins_per_dim": BINS, "points_per_iteration": ncalls,
+    return {"workload": WL["describe"],
+            "channels": WL["channels"], "bins_per_dim": WL["bins"], "points_per_iteration": ncalls,
             "seed": SEED, "alpha_adapted": True, "alpha_guard": True,
             "preprocess": "physical region and cuts: x1, x2 <= 1, pT > 30 GeV, |eta| < 99, dR > 0.4",
-            "l2": "per-step working set > L2 (momenta of ~2e6 tried points, ~380 MB)"}
+            "l2": "per-step working set > L2 (momenta of the tried points: "
+                  f"~{ncalls * 1.7 * 4 * (WL['n_out'] + 2) * 8 / 1e6:.0f} MB)"}
 
 
 # ------------------------------------------------------------------ clocks
@@ -139,13 +157,13 @@ def run_chili(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    cs = channels.multichannel_2_to_4()
+    cs = workloads.channel_set(WL["n_out"])
     ctx = gpu.Context(local_rank)
     stream = torch.cuda.current_stream(dev)
     ctx.set_stream(stream.cuda_stream)
     ctx.set_channels(cs)
-    ctx.uniform_grids(cs.nch, ctx.ndims, BINS)
-    ctx.set_integrand(abi.CHILI_FUNC_PROPAGATOR, channels.propagator_params())
+    ctx.uniform_grids(cs.nch, ctx.ndims, WL["bins"])
+    ctx.set_integrand(getattr(abi, "CHILI_FUNC_" + WL["fkind"]), channels.propagator_params())
     ctx.set_preprocess_cuts(cs.sqrts)
     params = workloads.mc_params(args.ncalls, iterations=args.warmup + args.steps)
     seed = SEED + 1000 * rank  # disjoint streams per rank (weak scaling)
@@ -227,11 +245,21 @@ def run_chili(args, rank, world, local_rank):
     if not args.no_flow and world == 1:
         flow = measure_flow(ctx, args, dev, stream, plain)
 
-    unw_out = measure_unweighted_output(ctx, info.weight_max, dev, rank)
+    if WL["unweighted_target"]:
+        unw_out = measure_unweighted_target(ctx, info.weight_max, dev, rank, WL["unweighted_target"])
+    else:
+        unw_out = measure_unweighted_output(ctx, info.weight_max, dev, rank)
 
     e2e = None
     if not args.no_e2e:
-        e2e = measure_e2e(ctx, params, args, dev, rank)
+        if WL["unweighted_target"]:
+            # 1e7-point iterations: the uniforms would not fit pinned host memory
+            # twice; the end-to-end path is the event output to the host
+            e2e = {"value": unw_out["events_per_s"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": unw_out["d2h_bytes_per_call"], "steps": unw_out["calls"],
+                   "path": unw_out["path"]}
+        else:
+            e2e = measure_e2e(ctx, params, args, dev, rank)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -243,7 +271,7 @@ def run_chili(args, rank, world, local_rank):
             selected = "flow"
         value = flow["value"] if selected == "flow" else unw_tot / (ms_max / 1e3)
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "metric": WL["metric"], "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (on-device Philox4x32-10 uniforms)",
@@ -379,7 +407,7 @@ def measure_flow(ctx, args, dev, stream, plain):
     import torch
     from chili_b200 import abi, gpu
     n = int(round(plain["points_per_step"]))
-    ctx.flow_init(abi.FlowParams.defaults(batch=args.flow_batch, layers=6, lr=1e-3))
+    ctx.flow_init(abi.FlowParams.defaults(batch=args.flow_batch, layers=WL["flow_layers"], lr=1e-3))
     k0 = {k: ctx.kernel_time(k) for k in FLOW_KERNELS}
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -421,7 +449,8 @@ def measure_flow(ctx, args, dev, stream, plain):
         "time_to_0p1pct_s": t01,
         "time_to_0p1pct_with_training_s": (t01 + train_s) if t01 is not None else None,
         "variance_x_time_ratio": ratio, "pull_vs_plain": pull,
-        "training": {"steps": args.flow_steps, "batch": args.flow_batch, "seconds": train_s,
+        "training": {"steps": args.flow_steps, "batch": args.flow_batch, "layers": WL["flow_layers"],
+                     "hidden": "2 x 128 (unit 127 the constant 1)", "seconds": train_s,
                      "loss_first": float(np.mean(loss[:10])), "loss_last": float(np.mean(loss[-10:])),
                      "kernel_ms": {k: round(k1[k][0] - k0[k][0], 3) for k in FLOW_KERNELS if k1[k][0] > k0[k][0]}},
         "kernel_ms": {k: round(k2[k][0] - k1[k][0], 3) for k in FLOW_KERNELS if k2[k][0] > k1[k][0]},
@@ -455,6 +484,37 @@ def measure_unweighted_output(ctx, w_max, dev, rank, n=4_000_000, reps=3):
             "path": "chili_gpu_generate_unweighted with pinned host outputs, wall clock"}
 
 
+def measure_unweighted_target(ctx, w_max, dev, rank, target, chunk=20_000_000, limit_s=60.0):
+    """`target` unweighted events written to pinned host memory, chunk after
+    chunk of drawn points (w_max = the last iteration's largest weight),
+    stopping at the target or after limit_s seconds."""
+    import torch
+    ne = ctx.n_ext
+    cap = target
+    out = (torch.empty((cap, ne, 4), dtype=torch.float64, pin_memory=True).numpy(),
+           torch.empty(cap, dtype=torch.float64, pin_memory=True).numpy(),
+           torch.empty(cap, dtype=torch.int32, pin_memory=True).numpy())
+    seed = 97 + rank
+    ctx.generate_unweighted(1_000_000, w_max, seed=seed, counter=0, max_events=cap, out=out)  # warm-up
+    torch.cuda.synchronize(dev)
+    kept, pts, calls, over = 0, 0, 0, 0
+    t0 = time.perf_counter()
+    while kept < target and time.perf_counter() - t0 < limit_s:
+        view = tuple(b[kept:] for b in out)
+        _, _, _, info = ctx.generate_unweighted(chunk, w_max, seed=seed, counter=(calls + 1) * chunk,
+                                                max_events=cap - kept, out=view)
+        kept += min(info.kept, cap - kept)
+        pts += chunk
+        calls += 1
+        over += info.overweight
+    dt = time.perf_counter() - t0
+    return {"events_per_s": kept / dt, "events": kept, "target": target, "reached": kept >= target,
+            "seconds": dt, "points": pts, "points_per_s": pts / dt, "efficiency": kept / pts, "w_max": w_max,
+            "overweight": over, "calls": calls, "points_per_call": chunk,
+            "d2h_bytes_per_call": int(kept / max(calls, 1) * (ne * 32 + 12)),
+            "path": "chili_gpu_generate_unweighted with pinned host outputs, wall clock"}
+
+
 def measure_e2e(ctx, params, args, dev, rank):
     """Same metric through the C ABI with HOST buffers: each step's uniforms
     come from pinned host memory (copied in inside the call), the StatsData and
@@ -484,25 +544,35 @@ def measure_e2e(ctx, params, args, dev, rank):
 
 
 # ------------------------------------------------------------- reference arm
-def _ref_worker_init(ncalls):
+def _ref_worker_init(ncalls, wl_name):
     global _W
     sys.path.insert(0, ROOT)
     from chili_b200 import abi, channels, workloads
     from oracle import ref
-    cs = channels.multichannel_2_to_4()
+    wl = WORKLOADS[wl_name]
+    cs = workloads.channel_set(wl["n_out"])
     params = workloads.mc_params(ncalls)
-    R = ref.MultiChannel(cs, BINS, params, abi.CHILI_FUNC_PROPAGATOR, channels.propagator_params())
+    R = ref.MultiChannel(cs, wl["bins"], params, getattr(abi, "CHILI_FUNC_" + wl["fkind"]),
+                         channels.propagator_params())
     R.set_cuts(cs.sqrts)
     _W = {"R": R, "cs": cs, "ncalls": ncalls, "rng": np.random.default_rng(os.getpid()), "wl": workloads}
 
 
 def _ref_worker_step(_):
     R = _W["R"]
-    # with uniform grids the cuts keep ~13% of the points; adapted grids ~60%
-    u = _W["wl"].uniforms53(_W["rng"], (int(_W["ncalls"] * 12) + 256, R.ndims + 1))
-    t0 = time.perf_counter()
-    st, info = R.iterate(u, guard=True)
-    dt = time.perf_counter() - t0
+    # the cuts keep ~13% (2->4) or ~0.6% (2->6) of the points on uniform
+    # grids, more on adapted ones: the uniform buffer grows until it suffices
+    while True:
+        f = _W.setdefault("factor", 12)
+        u = _W["wl"].uniforms53(_W["rng"], (int(_W["ncalls"] * f) + 256, R.ndims + 1))
+        t0 = time.perf_counter()
+        try:
+            st, info = R.iterate(u, guard=True)
+        except RuntimeError:
+            _W["factor"] = f * 4
+            continue
+        dt = time.perf_counter() - t0
+        break
     return (st.sum / info.weight_max if info.weight_max > 0 else 0.0, _W["ncalls"], info.points_tried, dt,
             st.as_tuple())
 
@@ -510,7 +580,8 @@ def _ref_worker_step(_):
 def _pool(cores, ncalls):
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
-    return ctx.Pool(cores, initializer=_ref_worker_init, initargs=(ncalls,))
+    name = next(k for k, v in WORKLOADS.items() if v is WL)
+    return ctx.Pool(cores, initializer=_ref_worker_init, initargs=(ncalls, name))
 
 
 def cpu_cores():
@@ -528,7 +599,7 @@ def cpu_baseline(args, kind="reference"):
     if not ref.available():
         return {"value": None, "unavailable": "oracle/_ref not built"}
     cores = cpu_cores()
-    ncalls = 20000
+    ncalls = 20000 if WL["n_out"] <= 4 else 4000
     with _pool(cores, ncalls) as pool:
         pool.map(_ref_worker_step, range(cores))  # warm-up: one adapted iteration each
         t0 = time.perf_counter()
@@ -549,7 +620,7 @@ def run_reference(args, rank, world):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libchili_ref.so not built"}))
         return
     cores = cpu_cores()
-    ncalls = 10000
+    ncalls = 10000 if WL["n_out"] <= 4 else 2000
     unw = 0.0
     acc = 0
     pooled = np.zeros(6)
@@ -568,7 +639,7 @@ def run_reference(args, rank, world):
     from chili_b200.gpu import stats_mean_error
     mean, err = stats_mean_error(pooled)
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "impl": "reference", "metric": WL["metric"], "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (host uniforms)", "config": workload_config(ncalls * cores),
@@ -837,7 +908,12 @@ def run_reference_batched(args, rank, world):
 
 
 def main():
+    global WL
     args = parse()
+    if args.workload in WORKLOADS:
+        WL = WORKLOADS[args.workload]
+    if args.ncalls is None:
+        args.ncalls = WL["ncalls"]
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))

@@ -25,12 +25,21 @@ __device__ __forceinline__ V4 v4(double e, double x, double y, double z) { retur
 __device__ __forceinline__ V4 operator+(V4 a, V4 b) { return V4{a.e + b.e, a.x + b.x, a.y + b.y, a.z + b.z}; }
 __device__ __forceinline__ V4 operator-(V4 a, V4 b) { return V4{a.e - b.e, a.x - b.x, a.y - b.y, a.z - b.z}; }
 __device__ __forceinline__ V4 scale(V4 a, double s) { return V4{a.e * s, a.x * s, a.y * s, a.z * s}; }
-// Minkowski product E E' - (p.p'), FourVector.cc operator*
-__device__ __forceinline__ double dot4(V4 a, V4 b) { return a.e * b.e - (a.x * b.x + a.y * b.y + a.z * b.z); }
+// Products of momenta round every product and sum separately, in the
+// reference's order (FourVector.cc operator*, FourVector.hh Pt2/P2), as its
+// x86-64 build does: a contracted multiply-add would round differently, and
+// the cancellation in the invariant mass of nearly collinear momenta (the
+// compound currents of nested decays) amplifies that to ~1e-9.
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+// Minkowski product E E' - ((px px' + py py') + pz pz')
+__device__ __forceinline__ double dot4(V4 a, V4 b) {
+    return __dsub_rn(dmul(a.e, b.e), dadd(dadd(dmul(a.x, b.x), dmul(a.y, b.y)), dmul(a.z, b.z)));
+}
 __device__ __forceinline__ double mass2(V4 a) { return dot4(a, a); }
-__device__ __forceinline__ double pt2(V4 a) { return a.x * a.x + a.y * a.y; }
-__device__ __forceinline__ double p2(V4 a) { return pt2(a) + a.z * a.z; }
-__device__ __forceinline__ double dot3(V4 a, V4 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ double pt2(V4 a) { return dadd(dmul(a.x, a.x), dmul(a.y, a.y)); }
+__device__ __forceinline__ double p2(V4 a) { return dadd(pt2(a), dmul(a.z, a.z)); }
+__device__ __forceinline__ double dot3(V4 a, V4 b) { return dadd(dadd(dmul(a.x, b.x), dmul(a.y, b.y)), dmul(a.z, b.z)); }
 __device__ __forceinline__ double rapidity(V4 a) {
     if (a.e == 0) return 99;
     return log((a.e + a.z) / (a.e - a.z)) / 2;
