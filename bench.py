@@ -72,6 +72,9 @@ def parse():
     ap.add_argument("--no-flow", action="store_true")
     ap.add_argument("--flow-steps", type=int, default=200)
     ap.add_argument("--flow-batch", type=int, default=65536)
+    ap.add_argument("--flow-long-steps", type=int, default=600,
+                    help="also train a second flow this many steps and report it beside the 200-step one "
+                         "(0: skip)")
     ap.add_argument("--workload", default="multichannel", choices=["multichannel", "large", "batched"],
                     help="multichannel: the 2->4 iteration with the learned proposal beside it; large: the "
                          "2->6 case (45 channels, 200 bins, 1e7 points per iteration, 10-layer flow, 1e6 "
@@ -241,9 +244,11 @@ def run_chili(args, rank, world, local_rank):
              "points_per_step": tried_tot / args.steps, "integral": mean, "rel_error": err / abs(mean),
              "rel_var_per_point": (err / abs(mean)) ** 2 * tried_tot, "time_to_0p1pct_s": t01,
              "unweighting_efficiency": unw_tot / tried_tot if tried_tot else None}
-    flow = None
+    flow = flow_long = None
     if not args.no_flow and world == 1:
         flow = measure_flow(ctx, args, dev, stream, plain)
+        if args.flow_long_steps > 0:
+            flow_long = measure_flow(ctx, args, dev, stream, plain, train_steps=args.flow_long_steps)
 
     if WL["unweighted_target"]:
         unw_out = measure_unweighted_target(ctx, info.weight_max, dev, rank, WL["unweighted_target"])
@@ -287,7 +292,7 @@ def run_chili(args, rank, world, local_rank):
             "clocks": clk.summary(),
             "gpu_launches": launches,
             "roofline": roof,
-            "paths": {"selected": selected, "plain": plain, "flow": flow},
+            "paths": {"selected": selected, "plain": plain, "flow": flow, "flow_long_training": flow_long},
             "unweighted_output": unw_out,
             "e2e": e2e,
             "cpu_baseline": cpu,
@@ -399,7 +404,7 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 
 
-def measure_flow(ctx, args, dev, stream, plain):
+def measure_flow(ctx, args, dev, stream, plain, train_steps=None):
     """The learned proposal on the same context (grids and channel weights as
     the plain path left them): online training on the GPU, one beta
     adaptation pass, then `steps` timed passes of as many points as a plain
@@ -407,11 +412,12 @@ def measure_flow(ctx, args, dev, stream, plain):
     import torch
     from chili_b200 import abi, gpu
     n = int(round(plain["points_per_step"]))
+    train_steps = args.flow_steps if train_steps is None else train_steps
     ctx.flow_init(abi.FlowParams.defaults(batch=args.flow_batch, layers=WL["flow_layers"], lr=1e-3))
     k0 = {k: ctx.kernel_time(k) for k in FLOW_KERNELS}
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    loss = ctx.flow_train(args.flow_steps, seed=SEED + 77, counter=0)
+    loss = ctx.flow_train(train_steps, seed=SEED + 77, counter=0)
     ctx.flow_iterate(n, seed=SEED + 78, counter=0, adapt_beta=True)
     e1.record(stream)
     torch.cuda.synchronize(dev)
@@ -449,7 +455,7 @@ def measure_flow(ctx, args, dev, stream, plain):
         "time_to_0p1pct_s": t01,
         "time_to_0p1pct_with_training_s": (t01 + train_s) if t01 is not None else None,
         "variance_x_time_ratio": ratio, "pull_vs_plain": pull,
-        "training": {"steps": args.flow_steps, "batch": args.flow_batch, "layers": WL["flow_layers"],
+        "training": {"steps": train_steps, "batch": args.flow_batch, "layers": WL["flow_layers"],
                      "hidden": "2 x 128 (unit 127 the constant 1)", "seconds": train_s,
                      "loss_first": float(np.mean(loss[:10])), "loss_last": float(np.mean(loss[-10:])),
                      "kernel_ms": {k: round(k1[k][0] - k0[k][0], 3) for k in FLOW_KERNELS if k1[k][0] > k0[k][0]}},

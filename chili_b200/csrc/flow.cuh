@@ -287,12 +287,39 @@ struct LayerArgs {
     int *err;
 };
 
-// Shared memory of the forward kernel: weights, A tile, H tile, the second
-// half's log-det partials, and a per-thread staging area for the 64
-// accumulator columns that hold one dimension's spline parameters.
-constexpr int kFwdThreads = 256;  // two threads per point (TMEM lanes are shared by warps w and w + 4)
-constexpr int kFwdScratch = 64 * kFwdThreads * 4;
-constexpr int kFwdSmem = kWBytes + 128 * 64 * 2 + kHTile + kFwdScratch + 512 + 64 + 1024;
+// Shared memory of the forward kernel: weights, A tile, H tile, and the
+// log-det partials of the three other thread groups of a point.
+constexpr int kFwdThreads = 512;  // four threads per point (TMEM lanes are shared by warps w, w+4, w+8, w+12)
+constexpr int kFwdSmem = kWBytes + 128 * 64 * 2 + kHTile + 3 * 128 * 4 + 64 + 1024;
+
+// theta of dimension j from the accumulator columns 256 + [c0, c0 + 64),
+// c0 = 49 j rounded down to 16 (c0 + 64 <= 256 for j < 5): two loads in
+// flight, then a shift by off = 49 j - c0 (0..4) in three conditional steps
+// so that every register index stays a compile-time constant.
+__device__ __forceinline__ void theta_window(uint32_t lane_addr, int j, float (&v)[64]) {
+    const int b0 = j * kPerDim, c0 = b0 & ~15, off = b0 - c0;
+    uint32_t r0[32], r1[32];
+    tmem_ld32_async(lane_addr + static_cast<uint32_t>(256 + c0), r0);
+    tmem_ld32_async(lane_addr + static_cast<uint32_t>(256 + c0 + 32), r1);
+    tmem_wait_ld();
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+        v[i] = __uint_as_float(r0[i]);
+        v[32 + i] = __uint_as_float(r1[i]);
+    }
+    if (off & 1) {
+#pragma unroll
+        for (int i = 0; i < 63; ++i) v[i] = v[i + 1];
+    }
+    if (off & 2) {
+#pragma unroll
+        for (int i = 0; i < 62; ++i) v[i] = v[i + 2];
+    }
+    if (off & 4) {
+#pragma unroll
+        for (int i = 0; i < 60; ++i) v[i] = v[i + 4];
+    }
+}
 
 template <int DB, int MODE, bool SAVE>
 __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
@@ -301,12 +328,11 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
     uint8_t *sW1 = sm, *sW2 = sm + kW1Bytes, *sW3 = sm + kW1Bytes + kW2Bytes;
     uint8_t *sA = sm + kWBytes;
     uint8_t *sH = sA + 128 * 64 * 2;
-    float *sTh = reinterpret_cast<float *>(sH + kHTile);  // [64][256] spline-parameter staging
-    float *sL = sTh + 64 * kFwdThreads;                    // [128] log-det partials of the second half
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sL + 128);
+    float *sL = reinterpret_cast<float *>(sH + kHTile);  // [3][128] log-det partials of groups 1..3
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sL + 3 * 128);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
     const int t = threadIdx.x, wp = t >> 5;
-    const int half = wp >> 2;               // 0: warps 0-3, 1: warps 4-7
+    const int grp = wp >> 2;                 // 0..3: the thread group of this warp
     const int r = (wp & 3) * 32 + (t & 31);  // the point (TMEM lane) of this thread
     const long long n = a.n;
     const long long ntiles = (n + 127) / 128;
@@ -337,25 +363,27 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
     for (long long tile = blockIdx.x; __syncthreads_and(ok) && tile < ntiles; tile += gridDim.x) {
         const long long row = tile * 128 + r;
         const bool valid = row < n;
-        int c = valid ? a.ch[row] : 0;
-        c = (c >= 0 && c < a.L.nch) ? c : 0;  // channel indices come from callers: keep E reads in bounds
-        if (half == 0) {
-            // A tile row: conditioning coordinates (columns 0..15) and the
-            // one-hot of the channel (columns 16..63), bf16
+        if (grp < 2) {
+            // A tile row, bf16: group 0 the conditioning coordinates (columns
+            // 0..15) and one-hot columns 16..31, group 1 one-hot columns 32..63
+            int c = valid ? a.ch[row] : 0;
+            c = (c >= 0 && c < a.L.nch) ? c : 0;  // channel indices come from callers: keep E reads in bounds
             float av[32];
+            if (grp == 0) {
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                float v = 0.f;
-                if (i < da && valid) v = 2.f * fminf(fmaxf(a.xin[a.L.cond[i] * n + row], 0.f), 1.f) - 1.f;
-                av[i] = v;
+                for (int i = 0; i < 16; ++i) {
+                    float v = 0.f;
+                    if (i < da && valid) v = 2.f * fminf(fmaxf(a.xin[a.L.cond[i] * n + row], 0.f), 1.f) - 1.f;
+                    av[i] = v;
+                }
+#pragma unroll
+                for (int i = 16; i < 32; ++i) av[i] = (valid && i == 16 + c) ? 1.f : 0.f;
+            } else {
+#pragma unroll
+                for (int i = 0; i < 32; ++i) av[i] = (valid && 32 + i == 16 + c) ? 1.f : 0.f;
             }
-#pragma unroll
-            for (int i = 16; i < 32; ++i) av[i] = (valid && i == 16 + c) ? 1.f : 0.f;
-            store_row32(sA, 128, r, 0, av);
-#pragma unroll
-            for (int i = 0; i < 32; ++i) av[i] = (valid && 32 + i == 16 + c) ? 1.f : 0.f;
-            store_row32(sA, 128, r, 32, av);
-        } else if (valid) {
+            store_row32(sA, 128, r, 32 * grp, av);
+        } else if (grp == 2 && valid) {
             // identity coordinates pass through
             for (int i = 0; i < da; ++i) a.xout[a.L.cond[i] * n + row] = a.xin[a.L.cond[i] * n + row];
         }
@@ -372,10 +400,9 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
         phase ^= 1;
         tc_fence_after();
         // h1 = lrelu(acc) (the product already holds E[c]); unit 127 = 1;
-        // this half's 64 columns
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int c0 = 64 * half + 32 * q;
+        // this group's 32 columns
+        {
+            const int c0 = 32 * grp;
             float v[32];
             tmem_ld32(lane_addr + c0, v);
 #pragma unroll
@@ -399,9 +426,8 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
         phase ^= 1;
         tc_fence_after();
         __syncthreads();  // the copy of h1 is complete before h2 overwrites it
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int c0 = 64 * half + 32 * q;
+        {
+            const int c0 = 32 * grp;
             float v[32];
             tmem_ld32(lane_addr + 128 + c0, v);
 #pragma unroll
@@ -424,22 +450,14 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
         ok = mbar_wait(bar + 1, phase, kWaitLimit) && ok;
         phase ^= 1;
         tc_fence_after();
-        // splines: dimensions 0, 2, 4 on the first half, 1, 3 on the second;
+        // splines: dimension j on group j % 4 (group 0 also takes dimension 4);
         // one copy of the spline code, the dimension a runtime loop
         float lsum = 0.f;
 #pragma unroll 1
-        for (int j = half; j < DB; j += 2) {
-            const int b0 = j * kPerDim, c0 = b0 & ~15;  // c0 + 64 <= 256
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                float v[16];
-                tmem_ld16(lane_addr + static_cast<uint32_t>(256 + c0 + 16 * q), v);
-#pragma unroll
-                for (int i = 0; i < 16; ++i) sTh[(16 * q + i) * kFwdThreads + t] = v[i];
-            }
-            float th[kPerDim];
-#pragma unroll
-            for (int i = 0; i < kPerDim; ++i) th[i] = sTh[(b0 - c0 + i) * kFwdThreads + t];
+        for (int j = grp; j < DB; j += 4) {
+            float th[64];
+            theta_window(lane_addr, j, th);
+            const int b0 = j * kPerDim;
             if (SAVE && valid) {
 #pragma unroll
                 for (int i = 0; i < kPerDim; ++i) a.theta[(b0 + i) * n + row] = th[i];
@@ -451,10 +469,10 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
             if (valid) a.xout[d * n + row] = y;
             lsum += lj;
         }
-        if (half == 1) sL[r] = lsum;
+        if (grp > 0) sL[(grp - 1) * 128 + r] = lsum;
         tc_fence_before();
         __syncthreads();
-        if (half == 0 && valid) a.logq[row] += lsum + sL[r];
+        if (grp == 0 && valid) a.logq[row] += lsum + sL[r] + sL[128 + r] + sL[256 + r];
     }
     if (!ok && t == 0) atomicExch(a.err, 1);
     // every issued MMA has been waited for (or the wait gave up): release TMEM
