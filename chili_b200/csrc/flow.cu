@@ -128,9 +128,10 @@ int pack_tiles(chili_ctx *ctx) {
     FlowState &S = *ctx->flow;
     const float *p = S.prm.as<float>();
     for (int l = 0; l < S.L; ++l) {
-        k_flow_pack<<<(kP * 128 + 255) / 256, 256, 0, ctx->stream>>>(
-            p + S.off_w1[l], p + S.off_e[l], p + S.off_w2[l], p + S.off_w3[l], S.da[l], S.nch, S.db[l] * kPerDim,
-            S.wtiles.as<uint8_t>() + static_cast<size_t>(l) * kWBytes);
+        uint8_t *wt = S.wtiles.as<uint8_t>() + static_cast<size_t>(l) * kWLayerBytes;
+        k_flow_pack<<<(kPF * 128 + 255) / 256, 256, 0, ctx->stream>>>(
+            p + S.off_w1[l], p + S.off_e[l], p + S.off_w2[l], p + S.off_w3[l], S.da[l], S.nch, S.db[l] * kPerDim, wt,
+            wt + kWBytes);
         LAUNCHED();
     }
     return CHILI_OK;
@@ -188,7 +189,8 @@ int ensure_train(chili_ctx *ctx, long long n) {
 
 FlowLayer layer_dev(FlowState &S, int l) {
     FlowLayer L = S.layers[l];
-    L.wt = S.wtiles.as<uint8_t>() + static_cast<size_t>(l) * kWBytes;
+    L.wt = S.wtiles.as<uint8_t>() + static_cast<size_t>(l) * kWLayerBytes;
+    L.wtf = L.wt + kWBytes;
     L.E = S.prm.as<float>() + S.off_e[l];
     return L;
 }
@@ -496,8 +498,8 @@ int chili_gpu_flow_init(chili_ctx *ctx, const chili_flow_params *params) {
     CK(cudaMemcpyAsync(S.prm.p, p.data(), sizeof(float) * S.np, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemsetAsync(S.m.p, 0, sizeof(float) * S.np, ctx->stream));
     CK(cudaMemsetAsync(S.v.p, 0, sizeof(float) * S.np, ctx->stream));
-    CK(S.wtiles.ensure(static_cast<size_t>(S.L) * kWBytes));
-    CK(cudaMemsetAsync(S.wtiles.p, 0, static_cast<size_t>(S.L) * kWBytes, ctx->stream));
+    CK(S.wtiles.ensure(static_cast<size_t>(S.L) * kWLayerBytes));
+    CK(cudaMemsetAsync(S.wtiles.p, 0, static_cast<size_t>(S.L) * kWLayerBytes, ctx->stream));
     CK(S.part_f.ensure(sizeof(float) * kNsplit * S.np_flow));
     CK(S.part_a.ensure(sizeof(float) * kAlphaSplit * S.AL.total));
     CK(S.loss_part.ensure(sizeof(double) * kAlphaSplit));

@@ -43,11 +43,19 @@ constexpr uint32_t kWaitLimit = 1u << 22;
 // W2 [128][128], W3 [256][128] (db*49 rows used), each an SW128 tile.
 constexpr int kW1Bytes = 128 * 64 * 2, kW2Bytes = 128 * 128 * 2, kW3Bytes = kP * 128 * 2;
 constexpr int kWBytes = kW1Bytes + kW2Bytes + kW3Bytes;
+// The forward kernel's copy of W3 with every dimension's 49 rows at a
+// 64-row boundary (rows 64 j .. 64 j + 48 for dimension j; the rest zero), so
+// that each dimension's spline parameters land at an aligned block of 64
+// accumulator columns. Stored per layer after the kWBytes of tiles.
+constexpr int kPF = 64 * kMaxDB;
+constexpr int kW3FBytes = kPF * 128 * 2;
+constexpr int kWLayerBytes = kWBytes + kW3FBytes;
 constexpr int kHTile = 128 * 128 * 2;   // one activation tile (128 points x 128 units)
 constexpr int kGTile = 128 * kP * 2;    // one spline-gradient tile (128 points x 256)
 
 struct FlowLayer {
-    const uint8_t *wt;  // kWBytes of tiles
+    const uint8_t *wt;   // kWBytes of tiles (W1, W2, W3)
+    const uint8_t *wtf;  // kW3FBytes: W3 in the forward kernel's padded row order
     const float *E;     // [nch][128] channel embedding (first-layer bias per channel)
     int da, db, nch;
     int8_t cond[kMaxDA];
@@ -287,37 +295,22 @@ struct LayerArgs {
     int *err;
 };
 
-// Shared memory of the forward kernel: weights, A tile, H tile, and the
-// log-det partials of the three other thread groups of a point.
+// Shared memory of the forward kernel: W1, W2, the padded W3, A tile, H tile,
+// and the log-det partials of the three other thread groups of a point.
 constexpr int kFwdThreads = 512;  // four threads per point (TMEM lanes are shared by warps w, w+4, w+8, w+12)
-constexpr int kFwdSmem = kWBytes + 128 * 64 * 2 + kHTile + 3 * 128 * 4 + 64 + 1024;
+constexpr int kFwdSmem = kW1Bytes + kW2Bytes + kW3FBytes + 128 * 64 * 2 + kHTile + 3 * 128 * 4 + 64 + 1024;
 
-// theta of dimension j from the accumulator columns 256 + [c0, c0 + 64),
-// c0 = 49 j rounded down to 16 (c0 + 64 <= 256 for j < 5): two loads in
-// flight, then a shift by off = 49 j - c0 (0..4) in three conditional steps
-// so that every register index stays a compile-time constant.
+// theta of dimension j: the 64 accumulator columns 128 + 64 j .. (the first
+// 49 used), two loads in flight.
 __device__ __forceinline__ void theta_window(uint32_t lane_addr, int j, float (&v)[64]) {
-    const int b0 = j * kPerDim, c0 = b0 & ~15, off = b0 - c0;
     uint32_t r0[32], r1[32];
-    tmem_ld32_async(lane_addr + static_cast<uint32_t>(256 + c0), r0);
-    tmem_ld32_async(lane_addr + static_cast<uint32_t>(256 + c0 + 32), r1);
+    tmem_ld32_async(lane_addr + static_cast<uint32_t>(128 + 64 * j), r0);
+    tmem_ld32_async(lane_addr + static_cast<uint32_t>(128 + 64 * j + 32), r1);
     tmem_wait_ld();
 #pragma unroll
     for (int i = 0; i < 32; ++i) {
         v[i] = __uint_as_float(r0[i]);
         v[32 + i] = __uint_as_float(r1[i]);
-    }
-    if (off & 1) {
-#pragma unroll
-        for (int i = 0; i < 63; ++i) v[i] = v[i + 1];
-    }
-    if (off & 2) {
-#pragma unroll
-        for (int i = 0; i < 62; ++i) v[i] = v[i + 2];
-    }
-    if (off & 4) {
-#pragma unroll
-        for (int i = 0; i < 60; ++i) v[i] = v[i + 4];
     }
 }
 
@@ -325,8 +318,8 @@ template <int DB, int MODE, bool SAVE>
 __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *sm = align1024(smem_raw);
-    uint8_t *sW1 = sm, *sW2 = sm + kW1Bytes, *sW3 = sm + kW1Bytes + kW2Bytes;
-    uint8_t *sA = sm + kWBytes;
+    uint8_t *sW1 = sm, *sW2 = sm + kW1Bytes, *sW3 = sm + kW1Bytes + kW2Bytes;  // sW3: kPF padded rows
+    uint8_t *sA = sW3 + kW3FBytes;
     uint8_t *sH = sA + 128 * 64 * 2;
     float *sL = reinterpret_cast<float *>(sH + kHTile);  // [3][128] log-det partials of groups 1..3
     uint64_t *bar = reinterpret_cast<uint64_t *>(sL + 3 * 128);
@@ -349,14 +342,19 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
     const uint32_t tbase = *tslot;
     const uint32_t lane_addr = tbase + (static_cast<uint32_t>((wp & 3) * 32) << 16);
     if (t == 0) {
-        mbar_expect_tx(bar, kWBytes);
-        bulk_g2s(sm, a.L.wt, kWBytes, bar);
+        mbar_expect_tx(bar, kW1Bytes + kW2Bytes + kW3FBytes);
+        bulk_g2s(sm, a.L.wt, kW1Bytes + kW2Bytes, bar);
+        bulk_g2s(sW3, a.L.wtf, kW3FBytes, bar);
     }
     bool ok = mbar_wait(bar, 0, kWaitLimit);
     const uint32_t aW1 = smem_u32(sW1), aW2 = smem_u32(sW2), aW3 = smem_u32(sW3);
     const uint32_t aA = smem_u32(sA), aH = smem_u32(sH);
     constexpr uint32_t id_h = idesc_bf16(128, 128, false, false);
-    constexpr uint32_t id_p = idesc_bf16(128, kP, false, false);
+    // theta: dimensions 0 .. min(DB, 4) - 1 in one product (columns 128 ..),
+    // dimension 4 in a second one (columns 384 .. 447)
+    constexpr int kN1 = 64 * (DB < 4 ? DB : 4);
+    constexpr uint32_t id_p1 = idesc_bf16(128, kN1, false, false);
+    constexpr uint32_t id_p2 = idesc_bf16(128, 64, false, false);
     uint32_t phase = 0;
     const int da = a.L.da;
 
@@ -418,7 +416,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
         if (t == 0) {
             tc_fence_after();
 #pragma unroll
-            for (int k = 0; k < 8; ++k) mma_bf16(tbase + 128, desc_k(aH, 128, 16 * k), desc_k(aW2, 128, 16 * k), id_h, k > 0);
+            for (int k = 0; k < 8; ++k) mma_bf16(tbase, desc_k(aH, 128, 16 * k), desc_k(aW2, 128, 16 * k), id_h, k > 0);
             mma_commit(bar + 1);
         }
         if (SAVE) copy_block(a.h1s + tile * kHTile, sH, kHTile);
@@ -429,7 +427,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
         {
             const int c0 = 32 * grp;
             float v[32];
-            tmem_ld32(lane_addr + 128 + c0, v);
+            tmem_ld32(lane_addr + c0, v);  // h2's accumulator reuses h1's columns
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
                 v[j] = lrelu(v[j]);
@@ -443,7 +441,12 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
         if (t == 0) {
             tc_fence_after();
 #pragma unroll
-            for (int k = 0; k < 8; ++k) mma_bf16(tbase + 256, desc_k(aH, 128, 16 * k), desc_k(aW3, kP, 16 * k), id_p, k > 0);
+            for (int k = 0; k < 8; ++k) {
+                mma_bf16(tbase + 128, desc_k(aH, 128, 16 * k), desc_k(aW3, kPF, 16 * k), id_p1, k > 0);
+                if (DB == 5)  // rows 256 .. 319 of the padded tile: 32 KB into each 64-column chunk
+                    mma_bf16(tbase + 384, desc_k(aH, 128, 16 * k), desc_k(aW3 + 256 / 8 * 1024, kPF, 16 * k), id_p2,
+                             k > 0);
+            }
             mma_commit(bar + 1);
         }
         if (SAVE) copy_block(a.h2s + tile * kHTile, sH, kHTile);
@@ -456,7 +459,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
 #pragma unroll 1
         for (int j = grp; j < DB; j += 4) {
             float th[64];
-            theta_window(lane_addr, j, th);
+            theta_window(lane_addr, j, th);  // th[0 .. 48]: this dimension's parameters
             const int b0 = j * kPerDim;
             if (SAVE && valid) {
 #pragma unroll
@@ -832,7 +835,8 @@ __global__ void k_flow_adam(float *__restrict__ prm, float *__restrict__ m, floa
 // f32 master weights of one layer -> its bf16 tiles (zero padding); the W1
 // tile also carries E^T in columns 16..16+nch-1.
 __global__ void k_flow_pack(const float *__restrict__ w1, const float *__restrict__ E, const float *__restrict__ w2,
-                            const float *__restrict__ w3, int da, int nch, int P, uint8_t *__restrict__ wt) {
+                            const float *__restrict__ w3, int da, int nch, int P, uint8_t *__restrict__ wt,
+                            uint8_t *__restrict__ wtf) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < 128 * 64) {
         const int r = i / 64, c = i % 64;
@@ -849,6 +853,13 @@ __global__ void k_flow_pack(const float *__restrict__ w1, const float *__restric
         const float v = r < P ? w3[r * 128 + c] : 0.f;
         *reinterpret_cast<uint16_t *>(wt + kW1Bytes + kW2Bytes + sw128_off(r, c, kP)) =
             static_cast<uint16_t>(pack_bf16x2(v, 0.f) & 0xFFFFu);
+    }
+    if (i < kPF * 128) {
+        // padded copy: dimension j's parameter q at row 64 j + q
+        const int r = i / 128, c = i % 128, j = r / 64, q = r % 64;
+        const int src = j * kPerDim + q;
+        const float v = (q < kPerDim && src < P) ? w3[src * 128 + c] : 0.f;
+        *reinterpret_cast<uint16_t *>(wtf + sw128_off(r, c, kPF)) = static_cast<uint16_t>(pack_bf16x2(v, 0.f) & 0xFFFFu);
     }
 }
 
