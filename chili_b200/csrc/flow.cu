@@ -769,8 +769,8 @@ int chili_gpu_flow_iterate(chili_ctx *ctx, uint64_t ncalls, uint64_t seed, uint6
 
 int chili_gpu_tc_selftest(chili_ctx *ctx, int mode, int K, int N, const float *A, const float *B, float *C) {
     if (!ctx || !A || !B || !C) return fail(ctx, CHILI_ERR_INVALID_ARG, "null argument");
-    if (mode < 0 || mode > 2 || K < 16 || K > 256 || K % 16 || N < 16 || N > 256 || N % 16)
-        return fail(ctx, CHILI_ERR_INVALID_ARG, "mode 0..2, K and N multiples of 16 in [16, 256]");
+    if (mode < 0 || mode > 3 || K < 16 || K > 256 || K % 16 || N < 16 || N > 256 || N % 16)
+        return fail(ctx, CHILI_ERR_INVALID_ARG, "mode 0..3, K and N multiples of 16 in [16, 256]");
     if (int rc = set_device(ctx)) return rc;
     const size_t na = 128 * static_cast<size_t>(K), nbb = static_cast<size_t>(N) * K, nc = 128 * static_cast<size_t>(N);
     DevBuf &da = ctx->stage[0], &db = ctx->stage[1], &dc = ctx->stage[2], &de = ctx->stage[3];

@@ -41,7 +41,7 @@ int launch_alpha(chili_ctx *ctx, const AlphaTrainArgs &a) {
 
 template <bool TRAIN, int NCH, int NF>
 int launch_combine_t(chili_ctx *ctx, const CombineArgs &a, unsigned blocks) {
-    const size_t bytes = TRAIN ? 0 : sizeof(float) * a.L.total;
+    const size_t bytes = TRAIN ? 0 : sizeof(float) * AlphaSmem<NCH, NF>::kTotal;
     if constexpr (!TRAIN) {
         static size_t attr = 0;
         if (attr < bytes) {

@@ -269,6 +269,94 @@ constexpr size_t alpha_train_smem(int total) {
 // integrand. Training: log F (F = f D_c / F_scale), features and log prior
 // of the batch row. Sampling: the channel-weight network and
 // v = alpha_c f D_c / (beta_c q_c) at the point's index (NaN when not finite).
+// The channel-weight network as the sampling pass keeps it in shared memory:
+// every block 16-byte aligned and W1's rows padded to NF columns, so that the
+// products read four weights per shared load.
+template <int NCH, int NF>
+struct AlphaSmem {
+    static constexpr int kC1 = 0, kA1 = kAH, kC2 = kA1 + kAH * NF, kA2 = kC2 + kAH, kC3 = kA2 + kAH * kAH,
+                         kA3 = kC3 + NCH, kTotal = kA3 + NCH * kAH;
+};
+
+template <int NCH, int NF>
+__device__ __forceinline__ void alpha_to_smem(const float *__restrict__ w, const AlphaLayout &L, float *s) {
+    using S = AlphaSmem<NCH, NF>;
+    for (int q = threadIdx.x; q < S::kTotal; q += blockDim.x) {
+        float v = 0.f;
+        if (q < S::kA1) v = w[L.c1 + q];
+        else if (q < S::kC2) {
+            const int i = (q - S::kA1) / NF, f = (q - S::kA1) % NF;
+            v = f < L.F ? w[L.a1 + i * L.F + f] : 0.f;
+        } else if (q < S::kA2) v = w[L.c2 + q - S::kC2];
+        else if (q < S::kC3) v = w[L.a2 + q - S::kA2];
+        else if (q < S::kA3) v = (q - S::kC3) < L.nch ? w[L.c3 + q - S::kC3] : 0.f;
+        else {
+            const int k = (q - S::kA3) / kAH, j = (q - S::kA3) % kAH;
+            v = k < L.nch ? w[L.a3 + k * kAH + j] : 0.f;
+        }
+        s[q] = v;
+    }
+}
+
+// alpha_forward on the shared-memory copy (float4 weight reads).
+template <int NCH, int NF>
+__device__ __forceinline__ void alpha_forward_smem(const float *__restrict__ s, int nch, const float (&feat)[NF],
+                                                   const float *logprior, float (&lg)[NCH], float &lse) {
+    using S = AlphaSmem<NCH, NF>;
+    float a1[kAH], a2[kAH];
+#pragma unroll
+    for (int i = 0; i < kAH; ++i) {
+        float acc = s[S::kC1 + i];
+        const float4 *wr = reinterpret_cast<const float4 *>(s + S::kA1 + i * NF);
+#pragma unroll
+        for (int q = 0; q < NF / 4; ++q) {
+            const float4 w4 = wr[q];
+            acc += w4.x * feat[4 * q] + w4.y * feat[4 * q + 1] + w4.z * feat[4 * q + 2] + w4.w * feat[4 * q + 3];
+        }
+        a1[i] = lrelu(acc);
+    }
+#pragma unroll
+    for (int j = 0; j < kAH; ++j) {
+        float acc = s[S::kC2 + j];
+        const float4 *wr = reinterpret_cast<const float4 *>(s + S::kA2 + j * kAH);
+#pragma unroll
+        for (int q = 0; q < kAH / 4; ++q) {
+            const float4 w4 = wr[q];
+            acc += w4.x * a1[4 * q] + w4.y * a1[4 * q + 1] + w4.z * a1[4 * q + 2] + w4.w * a1[4 * q + 3];
+        }
+        a2[j] = lrelu(acc);
+    }
+    float mx = -INFINITY;
+#pragma unroll
+    for (int k = 0; k < NCH; ++k) {
+        float acc = -INFINITY;
+        if (k < nch) {
+            acc = s[S::kC3 + k] + logprior[k];
+            const float4 *wr = reinterpret_cast<const float4 *>(s + S::kA3 + k * kAH);
+#pragma unroll
+            for (int q = 0; q < kAH / 4; ++q) {
+                const float4 w4 = wr[q];
+                acc += w4.x * a2[4 * q] + w4.y * a2[4 * q + 1] + w4.z * a2[4 * q + 2] + w4.w * a2[4 * q + 3];
+            }
+        }
+        lg[k] = acc;
+        mx = fmaxf(mx, acc);
+    }
+    float se = 0.f;
+#pragma unroll
+    for (int k = 0; k < NCH; ++k)
+        if (k < nch) se += expf(lg[k] - mx);
+    lse = mx + logf(se);
+}
+
+// log(x) of a positive double to float precision: exponent exactly, the
+// mantissa's log in f32 (the log priors are f32 values).
+__device__ __forceinline__ float log_d2f(double x) {
+    int e;
+    const double mnt = frexp(x, &e);
+    return __logf(static_cast<float>(mnt)) + static_cast<float>(e) * 0.69314718055994531f;
+}
+
 struct CombineArgs {
     const double *node_soa;  // tile nodes [node][4][T]
     const double *dcv, *vwv; // tile densities [channel][T]
@@ -295,9 +383,9 @@ struct CombineArgs {
 
 template <bool TRAIN, int NCH, int NF>
 __global__ void __launch_bounds__(128) k_flow_combine(CombineArgs a) {
-    extern __shared__ float cw[];  // the network (sampling)
+    extern __shared__ __align__(16) float cw[];  // the network (sampling), AlphaSmem layout
     if (!TRAIN) {
-        for (int q = threadIdx.x; q < a.L.total; q += blockDim.x) cw[q] = a.w[q];
+        alpha_to_smem<NCH, NF>(a.w, a.L, cw);
         __syncthreads();
     }
     const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
@@ -321,10 +409,10 @@ __global__ void __launch_bounds__(128) k_flow_combine(CombineArgs a) {
     ok = ok && (w0 > 0) && isfinite(w0) && (F > 0) && isfinite(F);
     float lp[NCH > 0 ? NCH : 1];
     if (ok) {
-        const float lw0 = static_cast<float>(log(w0));
+        const float lw0 = log_d2f(w0);
         for (int j = 0; j < a.nch; ++j) {
             const double Dj = a.dcv[static_cast<long long>(j) * a.T + i] * a.vwv[static_cast<long long>(j) * a.T + i];
-            lp[j] = a.logbeta[j] - static_cast<float>(log(Dj)) + lw0;
+            lp[j] = a.logbeta[j] - log_d2f(Dj) + lw0;
         }
     }
     float featv[kMaxFeat];
@@ -342,8 +430,8 @@ __global__ void __launch_bounds__(128) k_flow_combine(CombineArgs a) {
             float feat[NF];
 #pragma unroll
             for (int q = 0; q < NF; ++q) feat[q] = q < kMaxFeat ? featv[q] : 0.f;
-            float a1[kAH], a2[kAH], lg[NCH], lse;
-            alpha_forward<NCH, NF>(cw, a.L, feat, lp, a1, a2, lg, lse);
+            float lg[NCH], lse;
+            alpha_forward_smem<NCH, NF>(cw, a.L.nch, feat, lp, lg, lse);
             float lac = lg[0];
 #pragma unroll
             for (int q = 1; q < NCH; ++q)

@@ -501,7 +501,10 @@ int chili_gpu_flow_iterate(chili_ctx *ctx, uint64_t ncalls, uint64_t seed, uint6
 /* Tensor-core check: C[128][N] from f32 A, B rounded to bf16;
  * mode 0: C = A B^T (A [128][K], B [N][K]); mode 1: C = A^T B (A [K][128],
  * B [K][N]); mode 2: C = A B (A [128][K], B [K][N]). K and N multiples of 16
- * in [16, 256]. Host buffers. */
+ * in [16, 256]. Host buffers.  Mode 3 checks the failure path: no product is
+ * issued, the kernel's bounded wait on its mbarrier gives up (2^16 polls),
+ * releases its tensor memory and the call returns CHILI_ERR_TIMEOUT; the
+ * context stays usable. */
 int chili_gpu_tc_selftest(chili_ctx *ctx, int mode, int K, int N, const float *A, const float *B, float *C);
 
 /* ------------------------------------------------------ batched integrands

@@ -35,6 +35,22 @@ def test_tensor_core_products(ctx_factory, mode, K, N):
     assert np.abs(C - ref).max() <= 1e-4 * max(1.0, np.abs(ref).max())
 
 
+def test_bounded_wait_gives_up_and_the_context_survives(ctx_factory):
+    """Failure detection without a fault: a tensor-core wait on an mbarrier
+    that nothing arrives on gives up after its bounded number of polls, the
+    kernel releases its tensor memory and the call reports CHILI_ERR_TIMEOUT;
+    the same context then runs a product normally."""
+    from chili_b200.gpu import ChiliError
+    ctx = ctx_factory()
+    rng = np.random.default_rng(4)
+    A, B = rng.normal(size=(128, 64)), rng.normal(size=(64, 64))
+    with pytest.raises(ChiliError) as e:
+        ctx.tc_selftest(3, A, B, 64)
+    assert e.value.code == abi.CHILI_ERR_TIMEOUT
+    C = ctx.tc_selftest(0, A, B, 64)
+    assert np.abs(C - bf16(A) @ bf16(B).T).max() <= 1e-4 * max(1.0, np.abs(bf16(A) @ bf16(B).T).max())
+
+
 def _setup(ctx_factory, batch=4096, plain_iters=0, cuts=False):
     cs = workloads.channel_set(4)
     ctx = ctx_factory()
