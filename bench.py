@@ -250,6 +250,7 @@ def run_chili(args, rank, world, local_rank):
         if args.flow_long_steps > 0:
             flow_long = measure_flow(ctx, args, dev, stream, plain, train_steps=args.flow_long_steps)
 
+    ctx.set_option("kernel_timing", 0)  # no per-kernel events around the event-output calls
     if WL["unweighted_target"]:
         unw_out = measure_unweighted_target(ctx, info.weight_max, dev, rank, WL["unweighted_target"])
     else:
@@ -464,7 +465,7 @@ def measure_flow(ctx, args, dev, stream, plain, train_steps=None):
     }
 
 
-def measure_unweighted_output(ctx, w_max, dev, rank, n=4_000_000, reps=3):
+def measure_unweighted_output(ctx, w_max, dev, rank, n=4_000_000, reps=8):
     """The unweighting stage end to end: n points drawn, weighted, hit-or-miss
     against the last iteration's largest weight, and the kept events
     (momenta, weight, channel) written to pinned host memory."""

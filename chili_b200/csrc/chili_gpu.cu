@@ -262,6 +262,11 @@ int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value) {
         for (auto &n : ctx->klaunches) n = 0;
         return CHILI_OK;
     }
+    if (std::strcmp(name, "max_rounds") == 0) {
+        if (value < 1) return fail(ctx, CHILI_ERR_INVALID_ARG, "max_rounds must be >= 1");
+        ctx->max_rounds = value;
+        return CHILI_OK;
+    }
     if (std::strcmp(name, "defer_train") == 0) {
         ctx->defer_train = value != 0;
         return CHILI_OK;
@@ -829,7 +834,8 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         needed -= (r.n_acc - r.nan_round);
         if (r.cut > 0) ctx->accept_rate = std::max(0.02, static_cast<double>(r.n_acc) / static_cast<double>(r.cut));
         if (r.n_acc > 0) ctx->nan_rate = std::min(0.5, static_cast<double>(r.nan_round) / static_cast<double>(r.n_acc));
-        if (++rounds > 100000) return fail(ctx, CHILI_ERR_TIMEOUT, "no accepted points after 100000 rounds");
+        if (++rounds > static_cast<unsigned long long>(ctx->max_rounds))
+            return fail(ctx, CHILI_ERR_TIMEOUT, "ncalls not reached after max_rounds rounds (every point rejected or NaN?)");
     }
     IterAcc acc_h;
     if (opt && !ctx->defer_train) {

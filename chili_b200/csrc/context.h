@@ -91,6 +91,7 @@ struct chili_ctx {
     bool use_pipeline = true;  // option "pipeline": phased weight pass
     bool defer_train = false;  // option "defer_train": iterations collect training data, Train is the caller's
     long long pipe_tile = 1 << 22;  // option "pipeline_tile": points per tile
+    long long max_rounds = 100000;  // option "max_rounds": chunks an iteration may take before CHILI_ERR_TIMEOUT
     PointProgram pp_host;      // host copy (sizes of the memo buffers)
     DevBuf node_soa, memo, cfail, dcv, vwv;
     DevBuf hints, sorted, widths;  // hinted bin search tables and bin widths of the grids

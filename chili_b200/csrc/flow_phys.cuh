@@ -395,24 +395,28 @@ __global__ void __launch_bounds__(128) k_flow_combine(CombineArgs a) {
     const int c = a.ich_tile[i];
     V4 mom[CHILI_MAX_EXT];
     for (int s = 0; s < a.n_ext; ++s) mom[s] = soa_v4(a.node_soa, s, a.T, i);
+    // g_j = 1 / D_j; a channel whose D_j is +inf contributes nothing to the
+    // mixture (g_j = 0, its prior and weight 0), as its term alpha_j / D_j
+    // does in the plain combined weight; the sampled channel's D_c must be
+    // finite and positive
     double acc = 0.0, Dc = 0.0;
     bool ok = true;
     for (int j = 0; j < a.nch; ++j) {
         const double Dj = a.dcv[static_cast<long long>(j) * a.T + i] * a.vwv[static_cast<long long>(j) * a.T + i];
-        ok = ok && (Dj > 0) && isfinite(Dj);
+        ok = ok && (Dj > 0);  // NaN and non-positive densities: no value
         acc += static_cast<double>(a.beta[j]) / Dj;
         if (j == c) Dc = Dj;
     }
     const double w0 = 1.0 / acc;
     const double fv = eval_momenta(a.f, mom, a.n_ext);
     const double F = fv * Dc;
-    ok = ok && (w0 > 0) && isfinite(w0) && (F > 0) && isfinite(F);
+    ok = ok && isfinite(Dc) && (w0 > 0) && isfinite(w0) && (F > 0) && isfinite(F);
     float lp[NCH > 0 ? NCH : 1];
     if (ok) {
         const float lw0 = log_d2f(w0);
         for (int j = 0; j < a.nch; ++j) {
             const double Dj = a.dcv[static_cast<long long>(j) * a.T + i] * a.vwv[static_cast<long long>(j) * a.T + i];
-            lp[j] = a.logbeta[j] - log_d2f(Dj) + lw0;
+            lp[j] = isinf(Dj) ? -INFINITY : a.logbeta[j] - log_d2f(Dj) + lw0;
         }
     }
     float featv[kMaxFeat];
@@ -427,9 +431,13 @@ __global__ void __launch_bounds__(128) k_flow_combine(CombineArgs a) {
     } else {
         double v = 0;
         if (ok) {
+            // the network's padded input columns must read 0, not whatever
+            // the local memory beyond this point's nf features holds (0 x
+            // inf would be NaN)
+            const int nf = n_features(a.n_ext);
             float feat[NF];
 #pragma unroll
-            for (int q = 0; q < NF; ++q) feat[q] = q < kMaxFeat ? featv[q] : 0.f;
+            for (int q = 0; q < NF; ++q) feat[q] = (q < nf && q < kMaxFeat) ? featv[q] : 0.f;
             float lg[NCH], lse;
             alpha_forward_smem<NCH, NF>(cw, a.L.nch, feat, lp, lg, lse);
             float lac = lg[0];

@@ -565,3 +565,40 @@ def stats_mean_error(st):
     mean = s / n
     var = (s2 / n - mean * mean) / (n - 1)
     return mean, float(np.sqrt(var)) if var > 0 else 0.0
+
+
+def optimize(ctx, params, seed=7, counter=0, log=None):
+    """MultiChannel::Optimize (MultiChannel.hh:253-270) on a context with
+    channels, grids and integrand set: iterations until the pooled relative
+    error reaches params.rtol or params.niterations iterations ran.  With
+    `log` (a text file object) one JSON line per iteration: iteration,
+    estimate and error of the iteration and pooled, points tried, calls,
+    nonzero values, largest weight, unweighting efficiency (sum / w_max / n),
+    seconds.  Returns (pooled mean, pooled error, the per-iteration
+    records)."""
+    import json
+    import time
+    pooled = np.zeros(6)
+    records = []
+    it = 0
+    while it < params.niterations:
+        t0 = time.perf_counter()
+        st, info = ctx.multichannel_iterate(params, seed=seed, counter=counter)
+        dt = time.perf_counter() - t0
+        counter += info.points_tried
+        t = st.as_tuple()
+        pooled += np.array(t) * np.array([1, 0, 0, 1, 1, 1])
+        m_it, e_it = stats_mean_error(t)
+        mean, err = stats_mean_error(pooled)
+        rec = {"iteration": it, "estimate": m_it, "error": e_it, "pooled": mean, "pooled_error": err,
+               "points_tried": int(info.points_tried), "n": t[0], "n_nonzero": t[5], "w_max": info.weight_max,
+               "unweighting_efficiency": (t[3] / info.weight_max / t[0]) if info.weight_max > 0 else 0.0,
+               "seconds": dt}
+        records.append(rec)
+        if log is not None:
+            log.write(json.dumps(rec) + "\n")
+        it += 1
+        if mean != 0 and err / abs(mean) <= params.rtol:
+            break
+    mean, err = stats_mean_error(pooled)
+    return mean, err, records

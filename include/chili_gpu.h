@@ -198,7 +198,10 @@ uint64_t chili_gpu_launch_count(const chili_ctx *ctx);
  * "defer_train": 1 makes an optimizing iteration collect its training data
  * without applying Train, for a caller that sums the data over ranks first
  * and then calls chili_gpu_multichannel_train (the reference's MPI mode);
- * 0 (default) trains at the end of the iteration. */
+ * 0 (default) trains at the end of the iteration.
+ * "max_rounds": chunks of points a multichannel iteration may draw before it
+ * gives up with CHILI_ERR_TIMEOUT (default 100000; the reference's loop has
+ * no such bound and never ends when every point is rejected or NaN). */
 int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value);
 /* Total device time (ms) and launch count of one kernel class under the
  * "kernel_timing" option: k_mc_forward, k_pp_nodes, k_pp_items, k_pp_chains,

@@ -117,3 +117,23 @@ def test_deferred_train_equals_the_iteration_training(ctx_factory):
     st0, st1 = res[0][2], res[1][2]
     assert st0[0] == st1[0] and st0[5] == st1[5]
     assert _close(st0[3], st1[3], 1e-10) and _close(st0[4], st1[4], 1e-10)
+
+
+def test_optimize_writes_one_json_line_per_iteration(ctx_factory):
+    """gpu.optimize: MultiChannel::Optimize's loop with a JSON-lines log of
+    every iteration; stops at niterations (rtol 0) and pools the iterations."""
+    import io
+    import json
+    from chili_b200 import gpu
+    cs = workloads.channel_set(4)
+    ctx = ctx_factory()
+    ctx.set_channels(cs)
+    ctx.uniform_grids(cs.nch, ctx.ndims, 50)
+    ctx.set_integrand(abi.CHILI_FUNC_PROPAGATOR, channels.propagator_params())
+    ctx.set_preprocess_cuts(cs.sqrts)
+    buf = io.StringIO()
+    mean, err, recs = gpu.optimize(ctx, workloads.mc_params(20_000, iterations=3), seed=5, log=buf)
+    lines = [json.loads(x) for x in buf.getvalue().splitlines()]
+    assert [r["iteration"] for r in lines] == [0, 1, 2] and len(recs) == 3
+    assert all(r["n"] >= 20_000 and r["w_max"] > 0 and 0 < r["unweighting_efficiency"] < 1 for r in lines)
+    assert lines[-1]["pooled"] == mean and mean > 0 and 0 < err < mean
