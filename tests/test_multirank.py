@@ -90,3 +90,43 @@ def test_two_ranks_match_one_process(tmp_path):
     a1, _, _ = one.get_alpha()
     assert np.allclose(a1, r0["alpha"], rtol=1e-10, atol=0)
     assert np.allclose(one.get_grids(), r0["grids"], rtol=1e-10, atol=1e-14)
+
+
+def _worker_dies(rank, world, port, out_dir):
+    """Rank 1 leaves after its first synchronized iteration, before the
+    second one's collective (between steps, with nothing in flight); rank 0
+    must learn of it from the process group (an error from its next
+    all-reduce within the group's timeout), not hang."""
+    import datetime
+    import time
+    import torch.distributed as dist
+    from chili_b200 import parallel
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=10))
+    r = _PortRank(rank)
+    parallel.synced_iteration(r, r.params)
+    if rank == 1:
+        os._exit(0)  # leaves without destroying the group
+    t0 = time.monotonic()
+    outcome = "completed"
+    try:
+        parallel.synced_iteration(r, r.params)
+    except Exception as e:  # gloo reports the lost peer or the timeout
+        outcome = type(e).__name__
+    with open(os.path.join(out_dir, "rank0.txt"), "w") as f:
+        f.write(f"{outcome} {time.monotonic() - t0:.1f}")
+    os._exit(0)
+
+
+def test_a_rank_that_leaves_is_detected(tmp_path):
+    import torch.multiprocessing as mp
+    from oracle import port
+    if not port.available():
+        pytest.skip("C oracle not built")
+    ctx = mp.start_processes(_worker_dies, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=False,
+                             start_method="spawn")
+    for p in ctx.processes:
+        p.join(120)
+    assert all(not p.is_alive() for p in ctx.processes)
+    outcome, secs = (tmp_path / "rank0.txt").read_text().split()
+    assert outcome != "completed" and float(secs) < 60
