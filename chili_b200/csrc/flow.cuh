@@ -296,9 +296,14 @@ struct LayerArgs {
 };
 
 // Shared memory of the forward kernel: W1, W2, the padded W3, A tile, H tile,
-// and the log-det partials of the three other thread groups of a point.
-constexpr int kFwdThreads = 512;  // four threads per point (TMEM lanes are shared by warps w, w+4, w+8, w+12)
-constexpr int kFwdSmem = kW1Bytes + kW2Bytes + kW3FBytes + 128 * 64 * 2 + kHTile + 3 * 128 * 4 + 64 + 1024;
+// and the log-det partials of the four other thread groups of a point.
+// Five thread groups of 128 (one thread per point each; TMEM lanes are shared
+// by warps w, w+4, ..., w+16): groups 0-3 split the 128 hidden columns of the
+// epilogues, group j evaluates the spline of dimension j.
+constexpr int kFwdGroups = 5;
+constexpr int kFwdThreads = 128 * kFwdGroups;
+constexpr int kFwdSmem = kW1Bytes + kW2Bytes + kW3FBytes + 128 * 64 * 2 + kHTile + (kFwdGroups - 1) * 128 * 4 + 64 +
+                         1024;
 
 // theta of dimension j: the 64 accumulator columns 128 + 64 j .. (the first
 // 49 used), two loads in flight.
@@ -321,11 +326,11 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
     uint8_t *sW1 = sm, *sW2 = sm + kW1Bytes, *sW3 = sm + kW1Bytes + kW2Bytes;  // sW3: kPF padded rows
     uint8_t *sA = sW3 + kW3FBytes;
     uint8_t *sH = sA + 128 * 64 * 2;
-    float *sL = reinterpret_cast<float *>(sH + kHTile);  // [3][128] log-det partials of groups 1..3
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sL + 3 * 128);
+    float *sL = reinterpret_cast<float *>(sH + kHTile);  // [4][128] log-det partials of groups 1..4
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sL + (kFwdGroups - 1) * 128);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
     const int t = threadIdx.x, wp = t >> 5;
-    const int grp = wp >> 2;                 // 0..3: the thread group of this warp
+    const int grp = wp >> 2;                 // 0..4: the thread group of this warp
     const int r = (wp & 3) * 32 + (t & 31);  // the point (TMEM lane) of this thread
     const long long n = a.n;
     const long long ntiles = (n + 127) / 128;
@@ -398,8 +403,8 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
         phase ^= 1;
         tc_fence_after();
         // h1 = lrelu(acc) (the product already holds E[c]); unit 127 = 1;
-        // this group's 32 columns
-        {
+        // this group's 32 columns (groups 0-3)
+        if (grp < 4) {
             const int c0 = 32 * grp;
             float v[32];
             tmem_ld32(lane_addr + c0, v);
@@ -424,7 +429,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
         phase ^= 1;
         tc_fence_after();
         __syncthreads();  // the copy of h1 is complete before h2 overwrites it
-        {
+        if (grp < 4) {
             const int c0 = 32 * grp;
             float v[32];
             tmem_ld32(lane_addr + c0, v);  // h2's accumulator reuses h1's columns
@@ -453,11 +458,11 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
         ok = mbar_wait(bar + 1, phase, kWaitLimit) && ok;
         phase ^= 1;
         tc_fence_after();
-        // splines: dimension j on group j % 4 (group 0 also takes dimension 4);
-        // one copy of the spline code, the dimension a runtime loop
+        // splines: dimension j on group j; one copy of the spline code, the
+        // dimension a runtime value
         float lsum = 0.f;
 #pragma unroll 1
-        for (int j = grp; j < DB; j += 4) {
+        for (int j = grp; j < DB; j += kFwdGroups) {
             float th[64];
             theta_window(lane_addr, j, th);  // th[0 .. 48]: this dimension's parameters
             const int b0 = j * kPerDim;
@@ -475,7 +480,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
         if (grp > 0) sL[(grp - 1) * 128 + r] = lsum;
         tc_fence_before();
         __syncthreads();
-        if (grp == 0 && valid) a.logq[row] += lsum + sL[r] + sL[128 + r] + sL[256 + r];
+        if (grp == 0 && valid) a.logq[row] += lsum + sL[r] + sL[128 + r] + sL[256 + r] + sL[384 + r];
     }
     if (!ok && t == 0) atomicExch(a.err, 1);
     // every issued MMA has been waited for (or the wait gave up): release TMEM
