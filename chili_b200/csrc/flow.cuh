@@ -260,25 +260,6 @@ __device__ __forceinline__ void copy_block(void *dst, const void *src, int bytes
     for (int i = threadIdx.x; i < bytes / 16; i += blockDim.x) d[i] = s[i];
 }
 
-// The 49 spline parameters of transformed dimension J from the f32
-// accumulator columns col0 + 49 J ... (aligned 16-column loads).
-template <int J>
-__device__ __forceinline__ void load_theta(uint32_t lane_addr, int col0, float (&th)[kPerDim]) {
-    constexpr int b = J * kPerDim;
-    constexpr int c0 = b & ~15;
-    constexpr int c1 = (b + kPerDim - 1) & ~15;
-    float buf[64];
-#pragma unroll
-    for (int c = c0; c <= c1; c += 16) {
-        float v[16];
-        tmem_ld16(lane_addr + static_cast<uint32_t>(col0 + c), v);
-#pragma unroll
-        for (int i = 0; i < 16; ++i) buf[c - c0 + i] = v[i];
-    }
-#pragma unroll
-    for (int i = 0; i < kPerDim; ++i) th[i] = buf[b - c0 + i];
-}
-
 // ------------------------------------------------- coupling layer, forward
 // MODE 0: density direction x -> y = RQS(x) (training and log q of given
 // points); MODE 1: sampling direction y -> x = RQS^-1(y). SAVE keeps the
