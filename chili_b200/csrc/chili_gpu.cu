@@ -107,6 +107,47 @@ namespace {
 
 // The phased weight pass of a multichannel chunk: records of the n_pre
 // PreProcess-accepted points of the chunk of m counters.
+// The forward pass of a chunk of m points whose uniforms u[m][D+1] are in
+// host memory: slices of kUploadSlice rows are copied into the staging
+// buffer on the context's copy stream, and the forward launch of each slice
+// waits (on the device) for its own copy only.
+constexpr long long kUploadSlice = 1ll << 18;  // rows per slice, a multiple of kFwdBlock
+
+int forward_from_host(chili_ctx *ctx, const double *u, long long m, uint64_t seed, uint64_t ctr0) {
+    const int D = ctx->ndims;
+    const size_t row = sizeof(double) * (D + 1);
+    CK(ctx->stage[0].ensure(row * static_cast<size_t>(m)));
+    if (!ctx->copy_stream) CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+    const long long nslices = (m + kUploadSlice - 1) / kUploadSlice;
+    while (static_cast<long long>(ctx->copy_events.size()) < nslices + 1) {
+        cudaEvent_t e;
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ctx->copy_events.push_back(e);
+    }
+    // the staging buffer is free once the work queued before on the
+    // context's stream (earlier readers of it) is done
+    CK(cudaEventRecord(ctx->copy_events[nslices], ctx->stream));
+    CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->copy_events[nslices], 0));
+    double *dst = ctx->stage[0].as<double>();
+    for (long long s = 0; s < nslices; ++s) {
+        const long long s0 = s * kUploadSlice, len = std::min(kUploadSlice, m - s0);
+        CK(cudaMemcpyAsync(dst + s0 * (D + 1), u + s0 * (D + 1), row * static_cast<size_t>(len),
+                           cudaMemcpyHostToDevice, ctx->copy_stream));
+        CK(cudaEventRecord(ctx->copy_events[s], ctx->copy_stream));
+    }
+    KTimer kt_(ctx, KT_FORWARD);
+    for (long long s = 0; s < nslices; ++s) {
+        const long long s0 = s * kUploadSlice, len = std::min(kUploadSlice, m - s0);
+        CK(cudaStreamWaitEvent(ctx->stream, ctx->copy_events[s], 0));
+        k_mc_forward<<<static_cast<unsigned>((len + kFwdBlock - 1) / kFwdBlock), kFwdBlock, 0, ctx->stream>>>(
+            ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), cp_ptr(ctx), ctx->nch, D, ctx->bins, seed, ctr0,
+            dst, m, ctx->f_dev.as<IntegrandDesc>(), ctx->n_ext, ctx->mom_soa.as<double>(), ctx->ich.as<int32_t>(),
+            ctx->flag.as<uint8_t>(), ctx->block_count.as<int32_t>(), s0);
+        LAUNCHED();
+    }
+    return CHILI_OK;
+}
+
 int launch_pipeline(chili_ctx *ctx, long long m, long long n_pre, int bins, bool opt, RoundCtl *ctl_pre,
                     double *rec_val, double *rec_wgt, uint8_t *rec_ok, int32_t *rec_slot, double *rec_dens) {
     const PointProgram *pp = ctx->point_prog.as<PointProgram>();
@@ -189,7 +230,7 @@ int chili_gpu_destroy(chili_ctx *ctx) {
     DevBuf *bufs[] = {&ctx->edges, &ctx->edges_tmp, &ctx->progs, &ctx->point_prog, &ctx->node_soa, &ctx->memo, &ctx->cfail, &ctx->dcv, &ctx->vwv, &ctx->hints, &ctx->sorted, &ctx->widths, &ctx->ich_tile, &ctx->alpha_buf, &ctx->f_dev, &ctx->mom_soa,
                       &ctx->ich, &ctx->flag, &ctx->list, &ctx->block_count, &ctx->block_off, &ctx->part,
                       &ctx->hist, &ctx->round_res, &ctx->acc, &ctx->ctl, &ctx->status, &ctx->v_part,
-                      &ctx->v_hist, &ctx->v_train, &ctx->v_out, &ctx->rec, &ctx->ctl3};
+                      &ctx->v_hist, &ctx->v_train, &ctx->v_out, &ctx->rec, &ctx->ctl3, &ctx->unw};
     for (DevBuf *b : bufs) b->release();
     flow_release(ctx);
     batch_release(ctx);
@@ -197,6 +238,11 @@ int chili_gpu_destroy(chili_ctx *ctx) {
     if (ctx->ctl_host) cudaFreeHost(ctx->ctl_host);
     collect_times(ctx);
     for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
+    for (cudaEvent_t e : ctx->copy_events) cudaEventDestroy(e);
+    if (ctx->copy_stream) {
+        cudaStreamSynchronize(ctx->copy_stream);
+        cudaStreamDestroy(ctx->copy_stream);
+    }
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return CHILI_OK;
@@ -712,12 +758,11 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
     if (ncalls < 1) return fail(ctx, CHILI_ERR_INVALID_ARG, "ncalls must be positive");
     const int nch = ctx->nch, D = ctx->ndims, B = ctx->bins, NE = ctx->n_ext;
     const bool opt = params->should_optimize != 0;
+    // uniforms in device memory are read in place; host uniforms are staged
+    // chunk by chunk, only the rows the chunk consumes
     const double *ud = nullptr;
-    Arg au;
-    if (u) {
-        if ((rc = resolve(ctx, u, sizeof(double) * n_u * (D + 1), 0, true, au))) return rc;
-        ud = static_cast<const double *>(au.dev);
-    }
+    const bool u_host = u && !is_device_ptr(u);
+    if (u && !u_host) ud = u;
     const size_t hist_n = static_cast<size_t>(nch) * D * B;
     CK(ctx->hist.ensure(sizeof(double) * hist_n));
     CK(ctx->acc.ensure(sizeof(IterAcc)));
@@ -769,14 +814,20 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         double *rec_dens = rec_wgt + m;
         int32_t *rec_slot = reinterpret_cast<int32_t *>(rec_dens + static_cast<size_t>(nch) * m);
         uint8_t *rec_ok = reinterpret_cast<uint8_t *>(rec_slot + static_cast<size_t>(D) * m);
-        {
-        KTimer kt_(ctx, KT_FORWARD);
-        k_mc_forward<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(
-            ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), cp_ptr(ctx), nch, D, B, seed,
-            counter_base + tried, ud ? ud + tried * (D + 1) : nullptr, m, ctx->f_dev.as<IntegrandDesc>(), NE,
-            ctx->mom_soa.as<double>(), ctx->ich.as<int32_t>(), ctx->flag.as<uint8_t>(), ctx->block_count.as<int32_t>());
+        if (u_host) {
+            // host uniforms: slices copied on the copy stream, each slice's
+            // forward launch waiting for its own copy, so that the copy of
+            // the next slice overlaps the mapping of this one
+            if ((rc = forward_from_host(ctx, u + tried * (D + 1), m, seed, counter_base + tried))) return rc;
+        } else {
+            KTimer kt_(ctx, KT_FORWARD);
+            k_mc_forward<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(
+                ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), cp_ptr(ctx), nch, D, B, seed,
+                counter_base + tried, ud ? ud + tried * (D + 1) : nullptr, m, ctx->f_dev.as<IntegrandDesc>(), NE,
+                ctx->mom_soa.as<double>(), ctx->ich.as<int32_t>(), ctx->flag.as<uint8_t>(),
+                ctx->block_count.as<int32_t>(), 0);
+            LAUNCHED();
         }
-        LAUNCHED();
         // offsets of every PreProcess-accepted point (no cut at this stage)
         k_mc_scan<<<1, 1024, 0, ctx->stream>>>(ctx->block_count.as<int32_t>(), static_cast<int>(nb_f),
                                                ctx->flag.as<uint8_t>(), m, m + 1, ctx->block_off.as<long long>(),
@@ -981,7 +1032,7 @@ int chili_gpu_generate_unweighted(chili_ctx *ctx, int64_t n, uint64_t seed, uint
         k_mc_forward<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(
             ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), cp_ptr(ctx), nch, D, B, seed, ctr0, nullptr, m,
             ctx->f_dev.as<IntegrandDesc>(), NE, ctx->mom_soa.as<double>(), ctx->ich.as<int32_t>(),
-            ctx->flag.as<uint8_t>(), ctx->block_count.as<int32_t>());
+            ctx->flag.as<uint8_t>(), ctx->block_count.as<int32_t>(), 0);
         LAUNCHED();
         k_mc_scan<<<1, 1024, 0, ctx->stream>>>(ctx->block_count.as<int32_t>(), static_cast<int>(nb_f),
                                                ctx->flag.as<uint8_t>(), m, m + 1, ctx->block_off.as<long long>(),

@@ -74,6 +74,8 @@ int pipeline_run(chili_ctx *ctx, const double *mom_soa, long long m, const int32
 struct chili_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;      // uploads of host uniforms, overlapped with the forward pass
+    std::vector<cudaEvent_t> copy_events;
     bool own_stream = false;
     std::string err;
     unsigned long long launches = 0;

@@ -356,7 +356,10 @@ int chili_gpu_multichannel_weight(chili_ctx *ctx, const double *mom,
  * zero-valued calls.  Uniforms come from the generator (seed, counter_base+k)
  * or, when u is not NULL, from u[k*(ndims+1)...] (ndims uniforms then the
  * channel uniform, MultiChannel.hh:145-147) for k < n_u; running out of u is
- * CHILI_ERR_LIMIT.  With should_optimize the channel grids, alpha and best
+ * CHILI_ERR_LIMIT.  Device-resident u is read in place; host u (pinned for
+ * asynchronous copies) is uploaded as the iteration consumes it, in slices
+ * on a second stream that overlap the mapping of the previous slice, so only
+ * the rows tried cross PCIe.  With should_optimize the channel grids, alpha and best
  * weights are adapted on the device (MultiChannel.hh:182-194).
  * guard_alpha != 0 drops non-finite alpha-training terms, a documented
  * deviation from the reference (which propagates them). */
