@@ -150,3 +150,30 @@ def test_batch_rejects_bad_tasks(ctx_factory):
         ctx.batch_set([t])
     with pytest.raises(ChiliError):
         ctx.batch_iterate(1)
+
+
+def test_graph_recapture_on_changed_calls(ctx_factory):
+    """Calls that change the iteration count (more stats slots) or switch
+    adaptation off and on re-capture the iteration graph: the same results
+    as one call per iteration on a second context."""
+    rng = np.random.default_rng(12)
+    tasks = [camel_task(rng, 4, 20000, 30), mc_task(3, 700.0, 8000, 20)]
+    a, b = ctx_factory(), ctx_factory()
+    a.batch_set(tasks)
+    b.batch_set(tasks)
+    plan = [(1, True), (2, False), (3, True), (1, False)]
+    got, want = [], []
+    for n, adapt in plan:
+        st, _ = a.batch_iterate(n, seed=3, adapt=adapt)
+        got += list(st)
+        for _ in range(n):
+            s1, _ = b.batch_iterate(1, seed=3, adapt=adapt)
+            want.append(s1[0])
+    assert len(got) == len(want) == 7
+    for g, w in zip(got, want):
+        assert np.array_equal(g[:, 0], w[:, 0]) and np.array_equal(g[:, 5], w[:, 5])
+        assert np.max(rel(g[:, 3], w[:, 3])) < 1e-9
+    for k in range(len(tasks)):
+        ea, aa = a.batch_get_grid(k)
+        eb, ab = b.batch_get_grid(k)
+        assert np.max(rel(ea, eb)) < 1e-7 and np.max(rel(aa, ab)) < 1e-7
