@@ -548,8 +548,22 @@ def measure_e2e(ctx, params, args, dev, rank):
         unw += unweighted_events(st, info)
         rows += info.points_tried
     dt = time.perf_counter() - t0
-    return {"value": unw / dt, "unit": UNIT, "h2d_bytes_per_step": int(rows / steps * (D + 1) * 8),
-            "d2h_bytes_per_step": int(2 * 48 + 32), "steps": steps,
+    # the PCIe floor: the same bytes as one pinned host-to-device copy
+    nb = int(rows / steps)
+    src = torch.from_numpy(bufs[0][:nb])
+    dst = torch.empty(src.shape, dtype=torch.float64, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dst.copy_(src, non_blocking=True)
+    e0.record()
+    for _ in range(3):
+        dst.copy_(src, non_blocking=True)
+    e1.record()
+    e1.synchronize()
+    copy_ms = e0.elapsed_time(e1) / 3
+    del dst
+    return {"value": unw / dt, "unit": UNIT, "h2d_bytes_per_step": int(nb * (D + 1) * 8),
+            "d2h_bytes_per_step": int(2 * 48 + 32), "steps": steps, "ms_per_step": dt / steps * 1e3,
+            "h2d_copy_ms": copy_ms, "h2d_gbs": nb * (D + 1) * 8 / copy_ms / 1e6,
             "path": "chili_gpu_multichannel_iterate with host uniforms (pinned) and host StatsData"}
 
 

@@ -105,15 +105,14 @@ int pipeline_run(chili_ctx *ctx, const double *mom_soa, long long m, const int32
 
 namespace {
 
-// The phased weight pass of a multichannel chunk: records of the n_pre
-// PreProcess-accepted points of the chunk of m counters.
-// The forward pass of a chunk of m points whose uniforms u[m][D+1] are in
-// host memory: slices of kUploadSlice rows are copied into the staging
-// buffer on the context's copy stream, and the forward launch of each slice
-// waits (on the device) for its own copy only.
+// Host uniforms u[m][D+1]: rows [0, m) are copied into the staging buffer
+// in slices of kUploadSlice rows on the context's copy stream, slice s
+// followed by copy_events[s].  The rounds of the iteration then take one
+// slice (or the rest of one) each, so that the upload of the next slices
+// overlaps the whole weight pass of this one.
 constexpr long long kUploadSlice = 1ll << 18;  // rows per slice, a multiple of kFwdBlock
 
-int forward_from_host(chili_ctx *ctx, const double *u, long long m, uint64_t seed, uint64_t ctr0) {
+int upload_host(chili_ctx *ctx, const double *u, long long m) {
     const int D = ctx->ndims;
     const size_t row = sizeof(double) * (D + 1);
     CK(ctx->stage[0].ensure(row * static_cast<size_t>(m)));
@@ -135,19 +134,11 @@ int forward_from_host(chili_ctx *ctx, const double *u, long long m, uint64_t see
                            cudaMemcpyHostToDevice, ctx->copy_stream));
         CK(cudaEventRecord(ctx->copy_events[s], ctx->copy_stream));
     }
-    KTimer kt_(ctx, KT_FORWARD);
-    for (long long s = 0; s < nslices; ++s) {
-        const long long s0 = s * kUploadSlice, len = std::min(kUploadSlice, m - s0);
-        CK(cudaStreamWaitEvent(ctx->stream, ctx->copy_events[s], 0));
-        k_mc_forward<<<static_cast<unsigned>((len + kFwdBlock - 1) / kFwdBlock), kFwdBlock, 0, ctx->stream>>>(
-            ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), cp_ptr(ctx), ctx->nch, D, ctx->bins, seed, ctr0,
-            dst, m, ctx->f_dev.as<IntegrandDesc>(), ctx->n_ext, ctx->mom_soa.as<double>(), ctx->ich.as<int32_t>(),
-            ctx->flag.as<uint8_t>(), ctx->block_count.as<int32_t>(), s0);
-        LAUNCHED();
-    }
     return CHILI_OK;
 }
 
+// The phased weight pass of a multichannel chunk: records of the n_pre
+// PreProcess-accepted points of the chunk of m counters.
 int launch_pipeline(chili_ctx *ctx, long long m, long long n_pre, int bins, bool opt, RoundCtl *ctl_pre,
                     double *rec_val, double *rec_wgt, uint8_t *rec_ok, int32_t *rec_slot, double *rec_dens) {
     const PointProgram *pp = ctx->point_prog.as<PointProgram>();
@@ -209,7 +200,7 @@ int chili_gpu_create(int device, chili_ctx **out) {
         return fail(nullptr, CHILI_ERR_CUDA, "cudaStreamCreate failed");
     }
     ctx->own_stream = true;
-    if (cudaMallocHost(reinterpret_cast<void **>(&ctx->ctl_host), sizeof(RoundCtl)) != cudaSuccess) {
+    if (cudaMallocHost(reinterpret_cast<void **>(&ctx->ctl_host), 2 * sizeof(RoundCtl)) != cudaSuccess) {
         cudaStreamDestroy(ctx->stream);
         delete ctx;
         return fail(nullptr, CHILI_ERR_CUDA, "cudaMallocHost failed");
@@ -778,6 +769,7 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
     const size_t acc_smem = sizeof(double) * (kWgtBlock / 32) * nch;
 
     long long needed = ncalls, tried = 0, weighted = 0;
+    long long staged_begin = 0, staged_end = 0;  // rows of host u in the staging buffer
     unsigned long long rounds = 0;
     while (needed > 0) {
         // chunk: enough counters for `needed` accepted, non-NaN points at the
@@ -797,6 +789,19 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
             m = std::min<long long>(m, n_u - tried);
             if (m <= 0) return fail(ctx, CHILI_ERR_LIMIT, "the given uniforms ran out before ncalls points were accepted");
         }
+        int slice = -1;
+        if (u_host) {
+            // host uniforms: the rows the rates predict are uploaded once, in
+            // slices; this round takes (the rest of) one slice
+            if (tried >= staged_end) {
+                if ((rc = upload_host(ctx, u + tried * (D + 1), m))) return rc;
+                staged_begin = tried;
+                staged_end = tried + m;
+            }
+            const long long off = tried - staged_begin;
+            slice = static_cast<int>(off / kUploadSlice);
+            m = std::min(m, std::min((slice + 1) * kUploadSlice, staged_end - staged_begin) - off);
+        }
         const long long nb_f = (m + kFwdBlock - 1) / kFwdBlock;
         const long long nb_w = (m + kWgtBlock - 1) / kWgtBlock;
         CK(ctx->mom_soa.ensure(sizeof(double) * 4 * NE * m));
@@ -814,18 +819,18 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         double *rec_dens = rec_wgt + m;
         int32_t *rec_slot = reinterpret_cast<int32_t *>(rec_dens + static_cast<size_t>(nch) * m);
         uint8_t *rec_ok = reinterpret_cast<uint8_t *>(rec_slot + static_cast<size_t>(D) * m);
-        if (u_host) {
-            // host uniforms: slices copied on the copy stream, each slice's
-            // forward launch waiting for its own copy, so that the copy of
-            // the next slice overlaps the mapping of this one
-            if ((rc = forward_from_host(ctx, u + tried * (D + 1), m, seed, counter_base + tried))) return rc;
-        } else {
+        {
+            const double *u_in = ud ? ud + tried * (D + 1) : nullptr;
+            if (u_host) {
+                // the forward launch waits (on the device) for its slice's copy only
+                CK(cudaStreamWaitEvent(ctx->stream, ctx->copy_events[slice], 0));
+                u_in = ctx->stage[0].as<double>() + (tried - staged_begin) * (D + 1);
+            }
             KTimer kt_(ctx, KT_FORWARD);
             k_mc_forward<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(
                 ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), cp_ptr(ctx), nch, D, B, seed,
-                counter_base + tried, ud ? ud + tried * (D + 1) : nullptr, m, ctx->f_dev.as<IntegrandDesc>(), NE,
-                ctx->mom_soa.as<double>(), ctx->ich.as<int32_t>(), ctx->flag.as<uint8_t>(),
-                ctx->block_count.as<int32_t>(), 0);
+                counter_base + tried, u_in, m, ctx->f_dev.as<IntegrandDesc>(), NE, ctx->mom_soa.as<double>(),
+                ctx->ich.as<int32_t>(), ctx->flag.as<uint8_t>(), ctx->block_count.as<int32_t>());
             LAUNCHED();
         }
         // offsets of every PreProcess-accepted point (no cut at this stage)
@@ -837,10 +842,16 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
             ctx->flag.as<uint8_t>(), ctx->block_off.as<long long>(), ctl_pre, m, ctx->list.as<int32_t>());
         LAUNCHED();
         if (pipe) {
-            CK(cudaMemcpyAsync(ctx->ctl_host, ctl_pre, sizeof(RoundCtl), cudaMemcpyDeviceToHost, ctx->stream));
-            CK(cudaStreamSynchronize(ctx->stream));
-            const long long n_pre = ctx->ctl_host->n_acc;
-            weighted += n_pre;
+            // the launches are sized by the accepted count, read back here;
+            // a host-uniform round (one slice) does not wait for it: its
+            // launches cover all m points and the threads past the
+            // device-side count return at once
+            long long n_pre = m;
+            if (!u_host || m > ctx->pipe_tile) {
+                CK(cudaMemcpyAsync(ctx->ctl_host, ctl_pre, sizeof(RoundCtl), cudaMemcpyDeviceToHost, ctx->stream));
+                CK(cudaStreamSynchronize(ctx->stream));
+                n_pre = ctx->ctl_host->n_acc;
+            }
             int rc2 = launch_pipeline(ctx, m, n_pre, B, opt, ctl_pre, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens);
             if (rc2) return rc2;
         } else {
@@ -876,9 +887,11 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
                                                     ctx->acc.as<IterAcc>());
         LAUNCHED();
         CK(cudaMemcpyAsync(ctx->ctl_host, ctx->ctl.p, sizeof(RoundCtl), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->ctl_host + 1, ctl_pre, sizeof(RoundCtl), cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
         if (ctx->timing) collect_times(ctx);
-        const RoundCtl r = *ctx->ctl_host;
+        const RoundCtl r = ctx->ctl_host[0];
+        weighted += ctx->ctl_host[1].n_acc;
         if (r.cut <= 0 || r.cut > m || r.n_acc < 0 || r.nan_round < 0 || r.nan_round > r.n_acc)
             return fail(ctx, CHILI_ERR_CUDA, "inconsistent round record");
         tried += r.cut;
@@ -1032,7 +1045,7 @@ int chili_gpu_generate_unweighted(chili_ctx *ctx, int64_t n, uint64_t seed, uint
         k_mc_forward<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(
             ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), cp_ptr(ctx), nch, D, B, seed, ctr0, nullptr, m,
             ctx->f_dev.as<IntegrandDesc>(), NE, ctx->mom_soa.as<double>(), ctx->ich.as<int32_t>(),
-            ctx->flag.as<uint8_t>(), ctx->block_count.as<int32_t>(), 0);
+            ctx->flag.as<uint8_t>(), ctx->block_count.as<int32_t>());
         LAUNCHED();
         k_mc_scan<<<1, 1024, 0, ctx->stream>>>(ctx->block_count.as<int32_t>(), static_cast<int>(nb_f),
                                                ctx->flag.as<uint8_t>(), m, m + 1, ctx->block_off.as<long long>(),

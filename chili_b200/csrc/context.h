@@ -107,7 +107,7 @@ struct chili_ctx {
     bool f_set = false;
     // multichannel iteration scratch
     DevBuf mom_soa, ich, flag, list, block_count, block_off, part, hist, round_res, acc, ctl, status;
-    RoundCtl *ctl_host = nullptr;  // pinned
+    RoundCtl *ctl_host = nullptr;  // pinned, two records: the round, the PreProcess count
     double accept_rate = 0.5, nan_rate = 0.0;
     DevBuf rec, ctl3;
     DevBuf unw;  // unweighting: keep flags, kept list, partials, round control

@@ -305,10 +305,8 @@ __global__ void __launch_bounds__(kFwdBlock) k_mc_forward(
     const ChannelProgram *__restrict__ progs, const double *__restrict__ grids, const double *__restrict__ cp,
     int nch, int dims, int bins, uint64_t seed, uint64_t ctr0, const double *__restrict__ u_in, long long m,
     const IntegrandDesc *__restrict__ f, int n_ext, double *__restrict__ mom_soa, int32_t *__restrict__ ich_out,
-    uint8_t *__restrict__ flag, int32_t *__restrict__ block_count, long long k0) {
-    // k0: first point of this launch (a multiple of kFwdBlock; the points
-    // before it belong to earlier launches over the same chunk)
-    const long long k = k0 + blockIdx.x * static_cast<long long>(kFwdBlock) + threadIdx.x;
+    uint8_t *__restrict__ flag, int32_t *__restrict__ block_count) {
+    const long long k = blockIdx.x * static_cast<long long>(kFwdBlock) + threadIdx.x;
     int acc = 0;
     if (k < m) {
         double r[CHILI_MAX_DIMS + 1];
@@ -340,7 +338,7 @@ __global__ void __launch_bounds__(kFwdBlock) k_mc_forward(
         flag[k] = static_cast<uint8_t>(acc);
     }
     const int cnt = __syncthreads_count(acc);
-    if (threadIdx.x == 0) block_count[k0 / kFwdBlock + blockIdx.x] = cnt;
+    if (threadIdx.x == 0) block_count[blockIdx.x] = cnt;
 }
 
 // One block of 1024 threads: exclusive scan of the per-block accepted counts

@@ -137,3 +137,42 @@ def test_optimize_writes_one_json_line_per_iteration(ctx_factory):
     assert [r["iteration"] for r in lines] == [0, 1, 2] and len(recs) == 3
     assert all(r["n"] >= 20_000 and r["w_max"] > 0 and 0 < r["unweighting_efficiency"] < 1 for r in lines)
     assert lines[-1]["pooled"] == mean and mean > 0 and 0 < err < mean
+
+
+def test_host_uniforms_in_slices_match_device_uniforms(ctx_factory):
+    """Host uniforms (pinned) are uploaded in slices of 2^18 rows and each
+    slice is mapped and weighted as its own round; the same uniforms in
+    device memory are read in place in one round.  Both take the same points
+    (counts exact) and agree to the rounding of the partial-sum folds, over
+    two adapting iterations with the physical-region cuts (the first one on
+    uniform grids outgrows its predicted upload and needs a second one).
+    The first iteration's largest weight agrees bit for bit."""
+    import torch
+    cs = workloads.channel_set(4)
+    ctxs = []
+    for _ in range(2):
+        ctx = ctx_factory()
+        ctx.set_channels(cs)
+        ctx.uniform_grids(cs.nch, ctx.ndims, 100)
+        ctx.set_integrand(abi.CHILI_FUNC_PROPAGATOR, channels.propagator_params())
+        ctx.set_preprocess_cuts(1000.0)
+        ctxs.append(ctx)
+    params = workloads.mc_params(200_000)
+    rng = np.random.default_rng(29)
+    for it in range(2):
+        n_u = 2_500_000
+        host = torch.empty((n_u, ctxs[0].ndims + 1), dtype=torch.float64, pin_memory=True)
+        host.numpy()[:] = workloads.uniforms53(rng, tuple(host.shape))
+        dev = host.to("cuda")
+        st_h, info_h = ctxs[0].multichannel_iterate(params, u=host.numpy(), guard=True)
+        st_d, info_d = ctxs[1].multichannel_iterate(params, u=dev, guard=True)
+        assert info_h.points_tried == info_d.points_tried > (1 << 18), it
+        assert info_h.rejected_pre == info_d.rejected_pre
+        assert st_h.n == st_d.n and st_h.n_finite == st_d.n_finite
+        assert _close(st_h.sum, st_d.sum, 1e-12) and _close(st_h.sum2, st_d.sum2, 1e-12)
+        # the first iteration runs on identical grids (largest weight bit for
+        # bit); the second on grids adapted from atomically summed histograms
+        tol = 0 if it == 0 else 1e-12
+        assert _close(st_h.min, st_d.min, tol) and _close(st_h.max, st_d.max, tol), it
+        assert np.allclose(ctxs[0].get_alpha()[0], ctxs[1].get_alpha()[0], rtol=1e-10, atol=0)
+        assert np.allclose(ctxs[0].get_grids(), ctxs[1].get_grids(), rtol=1e-10, atol=1e-15)
