@@ -200,7 +200,9 @@ int chili_gpu_create(int device, chili_ctx **out) {
         return fail(nullptr, CHILI_ERR_CUDA, "cudaStreamCreate failed");
     }
     ctx->own_stream = true;
-    if (cudaMallocHost(reinterpret_cast<void **>(&ctx->ctl_host), 2 * sizeof(RoundCtl)) != cudaSuccess) {
+    if (cudaMallocHost(reinterpret_cast<void **>(&ctx->ctl_host), 2 * sizeof(RoundCtl)) != cudaSuccess ||
+        cudaMallocHost(reinterpret_cast<void **>(&ctx->iter_host), sizeof(long long) * kIterCtl) != cudaSuccess) {
+        if (ctx->ctl_host) cudaFreeHost(ctx->ctl_host);
         cudaStreamDestroy(ctx->stream);
         delete ctx;
         return fail(nullptr, CHILI_ERR_CUDA, "cudaMallocHost failed");
@@ -221,12 +223,13 @@ int chili_gpu_destroy(chili_ctx *ctx) {
     DevBuf *bufs[] = {&ctx->edges, &ctx->edges_tmp, &ctx->progs, &ctx->point_prog, &ctx->node_soa, &ctx->memo, &ctx->cfail, &ctx->dcv, &ctx->vwv, &ctx->hints, &ctx->sorted, &ctx->widths, &ctx->ich_tile, &ctx->alpha_buf, &ctx->f_dev, &ctx->mom_soa,
                       &ctx->ich, &ctx->flag, &ctx->list, &ctx->block_count, &ctx->block_off, &ctx->part,
                       &ctx->hist, &ctx->round_res, &ctx->acc, &ctx->ctl, &ctx->status, &ctx->v_part,
-                      &ctx->v_hist, &ctx->v_train, &ctx->v_out, &ctx->rec, &ctx->ctl3, &ctx->unw};
+                      &ctx->v_hist, &ctx->v_train, &ctx->v_out, &ctx->rec, &ctx->ctl3, &ctx->unw, &ctx->iter_ctl};
     for (DevBuf *b : bufs) b->release();
     flow_release(ctx);
     batch_release(ctx);
     for (auto &b : ctx->stage) b.release();
     if (ctx->ctl_host) cudaFreeHost(ctx->ctl_host);
+    if (ctx->iter_host) cudaFreeHost(ctx->iter_host);
     collect_times(ctx);
     for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : ctx->copy_events) cudaEventDestroy(e);
@@ -769,15 +772,16 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
     const size_t acc_smem = sizeof(double) * (kWgtBlock / 32) * nch;
 
     long long needed = ncalls, tried = 0, weighted = 0;
-    long long staged_begin = 0, staged_end = 0;  // rows of host u in the staging buffer
     unsigned long long rounds = 0;
+    const bool pipe = pipeline_dims_ok(D) && ctx->have_pp && ctx->use_pp && ctx->use_pipeline;
+    if (u_host) CK(ctx->iter_ctl.ensure(sizeof(long long) * kIterCtl));
+    long long *iter = ctx->iter_ctl.as<long long>();
     while (needed > 0) {
         // chunk: enough counters for `needed` accepted, non-NaN points at the
         // rates of the previous iteration, with a 2% margin
         const double rate = std::max(ctx->accept_rate * (1.0 - ctx->nan_rate), 0.02);
         long long m = static_cast<long long>(static_cast<double>(needed) / rate * 1.02) + 2048;
         m = std::min<long long>(m, 1ll << 24);
-        const bool pipe = pipeline_dims_ok(D) && ctx->have_pp && ctx->use_pp && ctx->use_pipeline;
         {
             // keep the per-chunk buffers within ~8 GB
             const PointProgram &P = ctx->pp_host;
@@ -789,116 +793,144 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
             m = std::min<long long>(m, n_u - tried);
             if (m <= 0) return fail(ctx, CHILI_ERR_LIMIT, "the given uniforms ran out before ncalls points were accepted");
         }
-        int slice = -1;
+        // Host uniforms: the chunk's rows are uploaded in slices and every
+        // slice is queued as one round without a host round trip; the device
+        // keeps the count still needed and the chunk's totals (iter), and the
+        // rounds after the one that completes the iteration do no work.
+        // Otherwise the chunk is one round, its record read back at its end.
+        const long long S = u_host ? std::min(m, kUploadSlice) : m;
+        const long long n_rounds = (m + S - 1) / S;
         if (u_host) {
-            // host uniforms: the rows the rates predict are uploaded once, in
-            // slices; this round takes (the rest of) one slice
-            if (tried >= staged_end) {
-                if ((rc = upload_host(ctx, u + tried * (D + 1), m))) return rc;
-                staged_begin = tried;
-                staged_end = tried + m;
-            }
-            const long long off = tried - staged_begin;
-            slice = static_cast<int>(off / kUploadSlice);
-            m = std::min(m, std::min((slice + 1) * kUploadSlice, staged_end - staged_begin) - off);
+            if ((rc = upload_host(ctx, u + tried * (D + 1), m))) return rc;
+            k_iter_init<<<1, 1, 0, ctx->stream>>>(iter, needed);
+            LAUNCHED();
         }
-        const long long nb_f = (m + kFwdBlock - 1) / kFwdBlock;
-        const long long nb_w = (m + kWgtBlock - 1) / kWgtBlock;
-        CK(ctx->mom_soa.ensure(sizeof(double) * 4 * NE * m));
-        CK(ctx->ich.ensure(sizeof(int32_t) * m));
-        CK(ctx->flag.ensure(m));
-        CK(ctx->list.ensure(sizeof(int32_t) * m));
+        const long long nb_f = (S + kFwdBlock - 1) / kFwdBlock;
+        const long long nb_w = (S + kWgtBlock - 1) / kWgtBlock;
+        CK(ctx->mom_soa.ensure(sizeof(double) * 4 * NE * S));
+        CK(ctx->ich.ensure(sizeof(int32_t) * S));
+        CK(ctx->flag.ensure(S));
+        CK(ctx->list.ensure(sizeof(int32_t) * S));
         CK(ctx->block_count.ensure(sizeof(int32_t) * nb_f));
         CK(ctx->block_off.ensure(sizeof(long long) * nb_f));
         CK(ctx->part.ensure(sizeof(double) * (kPartFixed + nch) * nb_w));
-        CK(ctx->rec.ensure(m * (2 * sizeof(double) + 1 + sizeof(int32_t) * D + sizeof(double) * nch) + 256));
+        CK(ctx->rec.ensure(S * (2 * sizeof(double) + 1 + sizeof(int32_t) * D + sizeof(double) * nch) + 256));
         CK(ctx->ctl3.ensure(3 * sizeof(RoundCtl)));
         RoundCtl *ctl_pre = ctx->ctl3.as<RoundCtl>(), *ctl_list = ctl_pre + 1;
-        double *rec_val = ctx->rec.as<double>();
-        double *rec_wgt = rec_val + m;
-        double *rec_dens = rec_wgt + m;
-        int32_t *rec_slot = reinterpret_cast<int32_t *>(rec_dens + static_cast<size_t>(nch) * m);
-        uint8_t *rec_ok = reinterpret_cast<uint8_t *>(rec_slot + static_cast<size_t>(D) * m);
-        {
-            const double *u_in = ud ? ud + tried * (D + 1) : nullptr;
-            if (u_host) {
-                // the forward launch waits (on the device) for its slice's copy only
-                CK(cudaStreamWaitEvent(ctx->stream, ctx->copy_events[slice], 0));
-                u_in = ctx->stage[0].as<double>() + (tried - staged_begin) * (D + 1);
+        for (long long q = 0; q < n_rounds; ++q) {
+            const long long r0 = q * S, mm = std::min(S, m - r0);  // this round's rows of the chunk
+            const long long nbf = (mm + kFwdBlock - 1) / kFwdBlock, nbw = (mm + kWgtBlock - 1) / kWgtBlock;
+            const long long *gate = u_host ? iter : nullptr;
+            // records with stride mm
+            double *rec_val = ctx->rec.as<double>();
+            double *rec_wgt = rec_val + mm;
+            double *rec_dens = rec_wgt + mm;
+            int32_t *rec_slot = reinterpret_cast<int32_t *>(rec_dens + static_cast<size_t>(nch) * mm);
+            uint8_t *rec_ok = reinterpret_cast<uint8_t *>(rec_slot + static_cast<size_t>(D) * mm);
+            {
+                const double *u_in = ud ? ud + (tried + r0) * (D + 1) : nullptr;
+                if (u_host) {
+                    // the forward launch waits (on the device) for its slice's copy only
+                    CK(cudaStreamWaitEvent(ctx->stream, ctx->copy_events[q], 0));
+                    u_in = ctx->stage[0].as<double>() + r0 * (D + 1);
+                }
+                KTimer kt_(ctx, KT_FORWARD);
+                k_mc_forward<<<static_cast<unsigned>(nbf), kFwdBlock, 0, ctx->stream>>>(
+                    ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), cp_ptr(ctx), nch, D, B, seed,
+                    counter_base + tried + r0, u_in, mm, ctx->f_dev.as<IntegrandDesc>(), NE,
+                    ctx->mom_soa.as<double>(), ctx->ich.as<int32_t>(), ctx->flag.as<uint8_t>(),
+                    ctx->block_count.as<int32_t>(), gate);
+                LAUNCHED();
             }
-            KTimer kt_(ctx, KT_FORWARD);
-            k_mc_forward<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(
-                ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), cp_ptr(ctx), nch, D, B, seed,
-                counter_base + tried, u_in, m, ctx->f_dev.as<IntegrandDesc>(), NE, ctx->mom_soa.as<double>(),
-                ctx->ich.as<int32_t>(), ctx->flag.as<uint8_t>(), ctx->block_count.as<int32_t>());
+            // offsets of every PreProcess-accepted point (no cut at this stage)
+            k_mc_scan<<<1, 1024, 0, ctx->stream>>>(ctx->block_count.as<int32_t>(), static_cast<int>(nbf),
+                                                   ctx->flag.as<uint8_t>(), mm, mm + 1, gate, 0,
+                                                   ctx->block_off.as<long long>(), ctl_pre);
             LAUNCHED();
-        }
-        // offsets of every PreProcess-accepted point (no cut at this stage)
-        k_mc_scan<<<1, 1024, 0, ctx->stream>>>(ctx->block_count.as<int32_t>(), static_cast<int>(nb_f),
-                                               ctx->flag.as<uint8_t>(), m, m + 1, ctx->block_off.as<long long>(),
-                                               ctl_pre);
-        LAUNCHED();
-        k_mc_compact<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(
-            ctx->flag.as<uint8_t>(), ctx->block_off.as<long long>(), ctl_pre, m, ctx->list.as<int32_t>());
-        LAUNCHED();
-        if (pipe) {
-            // the launches are sized by the accepted count, read back here;
-            // a host-uniform round (one slice) does not wait for it: its
-            // launches cover all m points and the threads past the
-            // device-side count return at once
-            long long n_pre = m;
-            if (!u_host || m > ctx->pipe_tile) {
-                CK(cudaMemcpyAsync(ctx->ctl_host, ctl_pre, sizeof(RoundCtl), cudaMemcpyDeviceToHost, ctx->stream));
-                CK(cudaStreamSynchronize(ctx->stream));
-                n_pre = ctx->ctl_host->n_acc;
+            k_mc_compact<<<static_cast<unsigned>(nbf), kFwdBlock, 0, ctx->stream>>>(
+                ctx->flag.as<uint8_t>(), ctx->block_off.as<long long>(), ctl_pre, mm, ctx->list.as<int32_t>());
+            LAUNCHED();
+            if (pipe) {
+                // the launches are sized by the accepted count, read back here;
+                // a queued host-uniform round does not wait for it: its
+                // launches cover all mm points and the threads past the
+                // device-side count return at once
+                long long n_pre = mm;
+                if (!u_host || mm > ctx->pipe_tile) {
+                    CK(cudaMemcpyAsync(ctx->ctl_host, ctl_pre, sizeof(RoundCtl), cudaMemcpyDeviceToHost,
+                                       ctx->stream));
+                    CK(cudaStreamSynchronize(ctx->stream));
+                    n_pre = ctx->ctl_host->n_acc;
+                }
+                int rc2 = launch_pipeline(ctx, mm, n_pre, B, opt, ctl_pre, rec_val, rec_wgt, rec_ok, rec_slot,
+                                          rec_dens);
+                if (rc2) return rc2;
+            } else {
+                KTimer kt_(ctx, KT_WEIGHT);
+                k_mc_weight<<<static_cast<unsigned>(nbw), kWgtBlock, 0, ctx->stream>>>(
+                    ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), alpha_ptr(ctx), nch, D, B, NE,
+                    ctx->mom_soa.as<double>(), mm, ctx->ich.as<int32_t>(), ctx->list.as<int32_t>(), ctl_pre,
+                    ctx->f_dev.as<IntegrandDesc>(), opt ? 1 : 0, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens,
+                    pp_ptr(ctx));
+                LAUNCHED();
             }
-            int rc2 = launch_pipeline(ctx, m, n_pre, B, opt, ctl_pre, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens);
-            if (rc2) return rc2;
-        } else {
-            KTimer kt_(ctx, KT_WEIGHT);
-            k_mc_weight<<<static_cast<unsigned>(nb_w), kWgtBlock, 0, ctx->stream>>>(
-                ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), alpha_ptr(ctx), nch, D, B, NE,
-                ctx->mom_soa.as<double>(), m, ctx->ich.as<int32_t>(), ctx->list.as<int32_t>(), ctl_pre,
-                ctx->f_dev.as<IntegrandDesc>(), opt ? 1 : 0, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens,
-                pp_ptr(ctx));
+            // the cut: the needed-th record whose value is not NaN (the
+            // device's count when the rounds are queued)
+            k_block_count<<<static_cast<unsigned>(nbf), kFwdBlock, 0, ctx->stream>>>(rec_ok, ctl_pre,
+                                                                                    ctx->block_count.as<int32_t>());
             LAUNCHED();
+            k_mc_scan<<<1, 1024, 0, ctx->stream>>>(ctx->block_count.as<int32_t>(), static_cast<int>(nbf), rec_ok,
+                                                   mm, needed, gate, 1, ctx->block_off.as<long long>(), ctl_list);
+            LAUNCHED();
+            k_cut_finalize<<<1, 1, 0, ctx->stream>>>(ctl_list, ctl_pre, ctx->list.as<int32_t>(), mm, needed,
+                                                     u_host ? iter : nullptr, ctx->ctl.as<RoundCtl>());
+            LAUNCHED();
+            {
+                KTimer kt_(ctx, KT_ACCUM);
+                k_mc_accum<<<static_cast<unsigned>(nbw), kWgtBlock, acc_smem, ctx->stream>>>(
+                    ctx->ctl.as<RoundCtl>(), mm, nch, D, static_cast<int>(hist_n), rec_val, rec_wgt, rec_ok, rec_slot,
+                    rec_dens, opt ? 1 : 0, guard_alpha ? 1 : 0, ctx->hist.as<double>(), ctx->part.as<double>());
+            }
+            LAUNCHED();
+            k_mc_reduce<<<kPartFixed + nch, 256, 0, ctx->stream>>>(ctx->part.as<double>(), nch,
+                                                                   ctx->ctl.as<RoundCtl>(),
+                                                                   ctx->round_res.as<double>());
+            LAUNCHED();
+            k_mc_accumulate<<<1, 256, 0, ctx->stream>>>(ctx->round_res.as<double>(), nch, ctx->ctl.as<RoundCtl>(),
+                                                        ctx->acc.as<IterAcc>());
+            LAUNCHED();
+            if (u_host) continue;
+            CK(cudaMemcpyAsync(ctx->ctl_host, ctx->ctl.p, sizeof(RoundCtl), cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaMemcpyAsync(ctx->ctl_host + 1, ctl_pre, sizeof(RoundCtl), cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            if (ctx->timing) collect_times(ctx);
+            const RoundCtl r = ctx->ctl_host[0];
+            if (r.cut <= 0 || r.cut > mm || r.n_acc < 0 || r.nan_round < 0 || r.nan_round > r.n_acc)
+                return fail(ctx, CHILI_ERR_CUDA, "inconsistent round record");
+            tried += r.cut;
+            needed -= (r.n_acc - r.nan_round);
+            weighted += ctx->ctl_host[1].n_acc;
+            ctx->accept_rate = std::max(0.02, static_cast<double>(r.n_acc) / static_cast<double>(r.cut));
+            if (r.n_acc > 0) ctx->nan_rate = std::min(0.5, static_cast<double>(r.nan_round) / static_cast<double>(r.n_acc));
         }
-        // the cut: the needed-th record whose value is not NaN
-        k_block_count<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(rec_ok, ctl_pre,
-                                                                                 ctx->block_count.as<int32_t>());
-        LAUNCHED();
-        k_mc_scan<<<1, 1024, 0, ctx->stream>>>(ctx->block_count.as<int32_t>(), static_cast<int>(nb_f), rec_ok, m,
-                                               needed, ctx->block_off.as<long long>(), ctl_list);
-        LAUNCHED();
-        k_cut_finalize<<<1, 1, 0, ctx->stream>>>(ctl_list, ctl_pre, ctx->list.as<int32_t>(), m, needed,
-                                                 ctx->ctl.as<RoundCtl>());
-        LAUNCHED();
-        {
-        KTimer kt_(ctx, KT_ACCUM);
-        k_mc_accum<<<static_cast<unsigned>(nb_w), kWgtBlock, acc_smem, ctx->stream>>>(
-            ctx->ctl.as<RoundCtl>(), m, nch, D, static_cast<int>(hist_n), rec_val, rec_wgt, rec_ok, rec_slot, rec_dens, opt ? 1 : 0,
-            guard_alpha ? 1 : 0, ctx->hist.as<double>(), ctx->part.as<double>());
+        if (u_host) {
+            // the queued rounds' totals
+            CK(cudaMemcpyAsync(ctx->iter_host, iter, sizeof(long long) * kIterCtl, cudaMemcpyDeviceToHost,
+                               ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            if (ctx->timing) collect_times(ctx);
+            const long long *t = ctx->iter_host;  // remaining, tried, accepted, NaN, weighted
+            if (t[1] <= 0 || t[1] > m || t[2] < 0 || t[3] < 0 || t[3] > t[2] || t[0] > needed ||
+                needed - t[0] != t[2] - t[3])
+                return fail(ctx, CHILI_ERR_CUDA, "inconsistent round record");
+            tried += t[1];
+            needed = t[0];
+            weighted += t[4];
+            ctx->accept_rate = std::max(0.02, static_cast<double>(t[2]) / static_cast<double>(t[1]));
+            if (t[2] > 0) ctx->nan_rate = std::min(0.5, static_cast<double>(t[3]) / static_cast<double>(t[2]));
         }
-        LAUNCHED();
-        k_mc_reduce<<<kPartFixed + nch, 256, 0, ctx->stream>>>(ctx->part.as<double>(), nch, ctx->ctl.as<RoundCtl>(),
-                                                               ctx->round_res.as<double>());
-        LAUNCHED();
-        k_mc_accumulate<<<1, 256, 0, ctx->stream>>>(ctx->round_res.as<double>(), nch, ctx->ctl.as<RoundCtl>(),
-                                                    ctx->acc.as<IterAcc>());
-        LAUNCHED();
-        CK(cudaMemcpyAsync(ctx->ctl_host, ctx->ctl.p, sizeof(RoundCtl), cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaMemcpyAsync(ctx->ctl_host + 1, ctl_pre, sizeof(RoundCtl), cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
-        if (ctx->timing) collect_times(ctx);
-        const RoundCtl r = ctx->ctl_host[0];
-        weighted += ctx->ctl_host[1].n_acc;
-        if (r.cut <= 0 || r.cut > m || r.n_acc < 0 || r.nan_round < 0 || r.nan_round > r.n_acc)
-            return fail(ctx, CHILI_ERR_CUDA, "inconsistent round record");
-        tried += r.cut;
-        needed -= (r.n_acc - r.nan_round);
-        if (r.cut > 0) ctx->accept_rate = std::max(0.02, static_cast<double>(r.n_acc) / static_cast<double>(r.cut));
-        if (r.n_acc > 0) ctx->nan_rate = std::min(0.5, static_cast<double>(r.nan_round) / static_cast<double>(r.n_acc));
-        if (++rounds > static_cast<unsigned long long>(ctx->max_rounds))
+        rounds += static_cast<unsigned long long>(n_rounds);
+        if (rounds > static_cast<unsigned long long>(ctx->max_rounds))
             return fail(ctx, CHILI_ERR_TIMEOUT, "ncalls not reached after max_rounds rounds (every point rejected or NaN?)");
     }
     IterAcc acc_h;
@@ -1045,11 +1077,11 @@ int chili_gpu_generate_unweighted(chili_ctx *ctx, int64_t n, uint64_t seed, uint
         k_mc_forward<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(
             ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), cp_ptr(ctx), nch, D, B, seed, ctr0, nullptr, m,
             ctx->f_dev.as<IntegrandDesc>(), NE, ctx->mom_soa.as<double>(), ctx->ich.as<int32_t>(),
-            ctx->flag.as<uint8_t>(), ctx->block_count.as<int32_t>());
+            ctx->flag.as<uint8_t>(), ctx->block_count.as<int32_t>(), nullptr);
         LAUNCHED();
         k_mc_scan<<<1, 1024, 0, ctx->stream>>>(ctx->block_count.as<int32_t>(), static_cast<int>(nb_f),
-                                               ctx->flag.as<uint8_t>(), m, m + 1, ctx->block_off.as<long long>(),
-                                               ctl_pre);
+                                               ctx->flag.as<uint8_t>(), m, m + 1, nullptr, 0,
+                                               ctx->block_off.as<long long>(), ctl_pre);
         LAUNCHED();
         k_mc_compact<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(
             ctx->flag.as<uint8_t>(), ctx->block_off.as<long long>(), ctl_pre, m, ctx->list.as<int32_t>());
@@ -1078,7 +1110,7 @@ int chili_gpu_generate_unweighted(chili_ctx *ctx, int64_t n, uint64_t seed, uint
                                                                                  ctx->block_count.as<int32_t>());
         LAUNCHED();
         k_mc_scan<<<1, 1024, 0, ctx->stream>>>(ctx->block_count.as<int32_t>(), static_cast<int>(nb_f), keep, m,
-                                               m + 1, ctx->block_off.as<long long>(), ctl_keep);
+                                               m + 1, nullptr, 0, ctx->block_off.as<long long>(), ctl_keep);
         LAUNCHED();
         k_mc_compact<<<static_cast<unsigned>(nb_f), kFwdBlock, 0, ctx->stream>>>(
             keep, ctx->block_off.as<long long>(), ctl_keep, m, kept_list);

@@ -108,6 +108,8 @@ struct chili_ctx {
     // multichannel iteration scratch
     DevBuf mom_soa, ich, flag, list, block_count, block_off, part, hist, round_res, acc, ctl, status;
     RoundCtl *ctl_host = nullptr;  // pinned, two records: the round, the PreProcess count
+    long long *iter_host = nullptr;  // pinned, the queued rounds' state (k_iter_init)
+    DevBuf iter_ctl;                 // device copy of that state
     double accept_rate = 0.5, nan_rate = 0.0;
     DevBuf rec, ctl3;
     DevBuf unw;  // unweighting: keep flags, kept list, partials, round control

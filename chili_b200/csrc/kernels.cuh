@@ -305,7 +305,12 @@ __global__ void __launch_bounds__(kFwdBlock) k_mc_forward(
     const ChannelProgram *__restrict__ progs, const double *__restrict__ grids, const double *__restrict__ cp,
     int nch, int dims, int bins, uint64_t seed, uint64_t ctr0, const double *__restrict__ u_in, long long m,
     const IntegrandDesc *__restrict__ f, int n_ext, double *__restrict__ mom_soa, int32_t *__restrict__ ich_out,
-    uint8_t *__restrict__ flag, int32_t *__restrict__ block_count) {
+    uint8_t *__restrict__ flag, int32_t *__restrict__ block_count, const long long *__restrict__ gate) {
+    // gate (queued rounds): the count still needed; nothing to do once it is 0
+    if (gate && *gate <= 0) {
+        if (threadIdx.x == 0) block_count[blockIdx.x] = 0;
+        return;
+    }
     const long long k = blockIdx.x * static_cast<long long>(kFwdBlock) + threadIdx.x;
     int acc = 0;
     if (k < m) {
@@ -342,10 +347,25 @@ __global__ void __launch_bounds__(kFwdBlock) k_mc_forward(
 }
 
 // One block of 1024 threads: exclusive scan of the per-block accepted counts
-// and the cut at the `needed`-th accepted point.
+// and the cut at the `needed`-th accepted point.  remaining (queued rounds,
+// may be NULL): the device's count still needed; when it is 0 the round is
+// empty (cut 0, nothing accepted), and with cut_at_remaining it replaces
+// `needed`.
 __global__ void __launch_bounds__(1024) k_mc_scan(const int32_t *__restrict__ block_count, int nb,
                                                   const uint8_t *__restrict__ flag, long long m, long long needed,
+                                                  const long long *__restrict__ remaining, int cut_at_remaining,
                                                   long long *__restrict__ block_off, RoundCtl *__restrict__ ctl) {
+    if (remaining) {
+        const long long rem = *remaining;
+        if (rem <= 0) {
+            if (threadIdx.x == 0) {
+                ctl->cut = 0;
+                ctl->n_acc = 0;
+            }
+            return;
+        }
+        if (cut_at_remaining) needed = rem;
+    }
     __shared__ long long wsum[32];
     __shared__ long long running_s;
     __shared__ int cut_block_s;
@@ -509,9 +529,19 @@ __global__ void __launch_bounds__(kFwdBlock) k_block_count(const uint8_t *__rest
 // Turns the cut over the record list (ctl_list: cut = records included,
 // n_acc = non-NaN among them) into the round record: counters consumed,
 // PreProcess-accepted points among them, NaN retries among those.
+// iter (queued rounds, may be NULL; k_iter_init): the count still needed
+// replaces `needed` and is brought down by this round, which also adds to
+// the chunk's totals; a round queued after the count reached 0 is empty.
 __global__ void k_cut_finalize(const RoundCtl *__restrict__ ctl_list, const RoundCtl *__restrict__ ctl_pre,
                                const int32_t *__restrict__ list, long long m, long long needed,
-                               RoundCtl *__restrict__ ctl) {
+                               long long *__restrict__ iter, RoundCtl *__restrict__ ctl) {
+    if (iter) {
+        needed = iter[0];
+        if (needed <= 0) {
+            *ctl = RoundCtl{0, 0, 0, 0};
+            return;
+        }
+    }
     const long long n_pre = ctl_pre->n_acc;
     const long long ok = n_pre > 0 ? ctl_list->n_acc : 0;
     const bool enough = ok >= needed;
@@ -522,6 +552,21 @@ __global__ void k_cut_finalize(const RoundCtl *__restrict__ ctl_list, const Roun
     r.nan_round = L - ok;
     r.pad = 0;
     *ctl = r;
+    if (iter) {
+        iter[0] = needed - (r.n_acc - r.nan_round);
+        iter[1] += r.cut;
+        iter[2] += r.n_acc;
+        iter[3] += r.nan_round;
+        iter[4] += n_pre;
+    }
+}
+
+// Queued rounds' state: the count still needed, then the totals of counters
+// consumed, PreProcess-accepted points, NaN retries and weighted points.
+constexpr int kIterCtl = 5;
+__global__ void k_iter_init(long long *__restrict__ iter, long long needed) {
+    iter[0] = needed;
+    for (int j = 1; j < kIterCtl; ++j) iter[j] = 0;
 }
 
 // Ordered-prefix accumulation of the records [0, ctl->n_acc): StatsData
