@@ -251,6 +251,7 @@ def run_chili(args, rank, world, local_rank):
             flow_long = measure_flow(ctx, args, dev, stream, plain, train_steps=args.flow_long_steps)
 
     ctx.set_option("kernel_timing", 0)  # no per-kernel events around the event-output calls
+    unw_q = quantile_unweighting(ctx, seed=4242 + rank)
     if WL["unweighted_target"]:
         unw_out = measure_unweighted_target(ctx, info.weight_max, dev, rank, WL["unweighted_target"])
     else:
@@ -295,6 +296,7 @@ def run_chili(args, rank, world, local_rank):
             "roofline": roof,
             "paths": {"selected": selected, "plain": plain, "flow": flow, "flow_long_training": flow_long},
             "unweighted_output": unw_out,
+            "unweighting_quantile": unw_q,
             "e2e": e2e,
             "cpu_baseline": cpu,
         }
@@ -489,6 +491,27 @@ def measure_unweighted_output(ctx, w_max, dev, rank, n=4_000_000, reps=8):
             "w_max": w_max, "overweight_last_call": int(info.overweight), "points_per_call": n,
             "d2h_bytes_per_call": int(written * (ne * 32 + 12)),
             "path": "chili_gpu_generate_unweighted with pinned host outputs, wall clock"}
+
+
+def quantile_unweighting(ctx, seed, n=2_000_000, q=0.999):
+    """Unweighting efficiency <v> / w_q with w_q the q-quantile of the
+    nonzero values |v| of n drawn points instead of their maximum, in the
+    reference's Percentile convention (Statistics.hh:22-59: the
+    (floor(k q) + 1)-th smallest of k values); <v> is over all n points
+    (zeros of rejected points included, as in StatsData).  The values come
+    from chili_gpu_generate_unweighted with a vanishing w_max, which keeps
+    every nonzero value and returns it unchanged."""
+    wgt = np.empty(n)
+    _, v, _, _ = ctx.generate_unweighted(n, 1e-300, seed=seed, counter=0, max_events=n, out=(None, wgt, None))
+    mean = float(np.sum(v)) / n
+    nz = np.sort(np.abs(v))
+    if len(nz) == 0:
+        return {"quantile": q, "points": n, "nonzero": 0}
+    w_q = float(nz[int(len(nz) * q)])
+    return {"quantile": q, "w_max_quantile": w_q, "w_max_sample": float(nz[-1]),
+            "efficiency": mean / w_q, "efficiency_with_max": mean / float(nz[-1]),
+            "overweight_fraction": float(np.mean(nz > w_q)), "points": n, "nonzero": int(len(nz)),
+            "path": "chili_gpu_generate_unweighted values on the adapted channels, host sort"}
 
 
 def measure_unweighted_target(ctx, w_max, dev, rank, target, chunk=20_000_000, limit_s=60.0):

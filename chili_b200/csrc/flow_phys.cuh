@@ -303,7 +303,7 @@ template <int NCH, int NF>
 __device__ __forceinline__ void alpha_forward_smem(const float *__restrict__ s, int nch, const float (&feat)[NF],
                                                    const float *logprior, float (&lg)[NCH], float &lse) {
     using S = AlphaSmem<NCH, NF>;
-    float a1[kAH], a2[kAH];
+    float a1[kAH];
 #pragma unroll
     for (int i = 0; i < kAH; ++i) {
         float acc = s[S::kC1 + i];
@@ -316,32 +316,37 @@ __device__ __forceinline__ void alpha_forward_smem(const float *__restrict__ s, 
         a1[i] = lrelu(acc);
     }
 #pragma unroll
-    for (int j = 0; j < kAH; ++j) {
-        float acc = s[S::kC2 + j];
-        const float4 *wr = reinterpret_cast<const float4 *>(s + S::kA2 + j * kAH);
+    for (int k = 0; k < NCH; ++k) lg[k] = k < nch ? s[S::kC3 + k] + logprior[k] : -INFINITY;
+    // the second hidden layer four units at a time, each group added into
+    // the logits at once (the same order of additions as a whole second
+    // layer followed by the last one, without holding all of it; a rolled
+    // loop, so that the registers hold the first layer and one group)
+#pragma unroll 1
+    for (int q = 0; q < kAH / 4; ++q) {
+        float h[4];
 #pragma unroll
-        for (int q = 0; q < kAH / 4; ++q) {
-            const float4 w4 = wr[q];
-            acc += w4.x * a1[4 * q] + w4.y * a1[4 * q + 1] + w4.z * a1[4 * q + 2] + w4.w * a1[4 * q + 3];
+        for (int jj = 0; jj < 4; ++jj) {
+            const int j = 4 * q + jj;
+            float acc = s[S::kC2 + j];
+            const float4 *wr = reinterpret_cast<const float4 *>(s + S::kA2 + j * kAH);
+#pragma unroll
+            for (int r = 0; r < kAH / 4; ++r) {
+                const float4 w4 = wr[r];
+                acc += w4.x * a1[4 * r] + w4.y * a1[4 * r + 1] + w4.z * a1[4 * r + 2] + w4.w * a1[4 * r + 3];
+            }
+            h[jj] = lrelu(acc);
         }
-        a2[j] = lrelu(acc);
+#pragma unroll
+        for (int k = 0; k < NCH; ++k) {
+            if (k < nch) {
+                const float4 w4 = reinterpret_cast<const float4 *>(s + S::kA3 + k * kAH)[q];
+                lg[k] += w4.x * h[0] + w4.y * h[1] + w4.z * h[2] + w4.w * h[3];
+            }
+        }
     }
     float mx = -INFINITY;
 #pragma unroll
-    for (int k = 0; k < NCH; ++k) {
-        float acc = -INFINITY;
-        if (k < nch) {
-            acc = s[S::kC3 + k] + logprior[k];
-            const float4 *wr = reinterpret_cast<const float4 *>(s + S::kA3 + k * kAH);
-#pragma unroll
-            for (int q = 0; q < kAH / 4; ++q) {
-                const float4 w4 = wr[q];
-                acc += w4.x * a2[4 * q] + w4.y * a2[4 * q + 1] + w4.z * a2[4 * q + 2] + w4.w * a2[4 * q + 3];
-            }
-        }
-        lg[k] = acc;
-        mx = fmaxf(mx, acc);
-    }
+    for (int k = 0; k < NCH; ++k) mx = fmaxf(mx, lg[k]);
     float se = 0.f;
 #pragma unroll
     for (int k = 0; k < NCH; ++k)
@@ -382,7 +387,7 @@ struct CombineArgs {
 };
 
 template <bool TRAIN, int NCH, int NF>
-__global__ void __launch_bounds__(128) k_flow_combine(CombineArgs a) {
+__global__ void __launch_bounds__(128, TRAIN ? 1 : 4) k_flow_combine(CombineArgs a) {
     extern __shared__ __align__(16) float cw[];  // the network (sampling), AlphaSmem layout
     if (!TRAIN) {
         alpha_to_smem<NCH, NF>(a.w, a.L, cw);

@@ -347,7 +347,7 @@ class Context:
         self.call("chili_gpu_generate_unweighted", int(n), int(seed), int(counter), float(w_max), _ptr(mom),
                   _ptr(wgt), _ptr(ch), int(max_events), C.byref(ne), C.byref(info))
         k = min(ne.value, max_events)
-        return mom[:k], wgt[:k], ch[:k], info
+        return tuple(None if a is None else a[:k] for a in (mom, wgt, ch)) + (info,)
 
     def evaluate_batch(self, ch, u):
         u = _f64(u)
