@@ -106,18 +106,25 @@ int pipeline_run(chili_ctx *ctx, const double *mom_soa, long long m, const int32
 namespace {
 
 // Host uniforms u[m][D+1]: rows [0, m) are copied into the staging buffer
-// in slices of kUploadSlice rows on the context's copy stream, slice s
-// followed by copy_events[s].  The rounds of the iteration then take one
-// slice (or the rest of one) each, so that the upload of the next slices
-// overlaps the whole weight pass of this one.
-constexpr long long kUploadSlice = 1ll << 18;  // rows per slice, a multiple of kFwdBlock
+// in slices on the context's copy stream, slice s followed by
+// copy_events[s]: a first slice of kFirstSlice rows (the only copy nothing
+// overlaps), then slices of kUploadSlice rows.  The rounds of the iteration
+// take one slice each, so that the upload of the next slices overlaps the
+// whole weight pass of this one.
+constexpr long long kFirstSlice = 1ll << 16;   // rows; both multiples of kFwdBlock
+constexpr long long kUploadSlice = 1ll << 18;
+
+long long slice_begin(long long s) { return s == 0 ? 0 : kFirstSlice + (s - 1) * kUploadSlice; }
+long long slice_count(long long m) {
+    return m <= kFirstSlice ? 1 : 1 + (m - kFirstSlice + kUploadSlice - 1) / kUploadSlice;
+}
 
 int upload_host(chili_ctx *ctx, const double *u, long long m) {
     const int D = ctx->ndims;
     const size_t row = sizeof(double) * (D + 1);
     CK(ctx->stage[0].ensure(row * static_cast<size_t>(m)));
     if (!ctx->copy_stream) CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
-    const long long nslices = (m + kUploadSlice - 1) / kUploadSlice;
+    const long long nslices = slice_count(m);
     while (static_cast<long long>(ctx->copy_events.size()) < nslices + 1) {
         cudaEvent_t e;
         CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -129,7 +136,7 @@ int upload_host(chili_ctx *ctx, const double *u, long long m) {
     CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->copy_events[nslices], 0));
     double *dst = ctx->stage[0].as<double>();
     for (long long s = 0; s < nslices; ++s) {
-        const long long s0 = s * kUploadSlice, len = std::min(kUploadSlice, m - s0);
+        const long long s0 = slice_begin(s), len = std::min(slice_begin(s + 1), m) - s0;
         CK(cudaMemcpyAsync(dst + s0 * (D + 1), u + s0 * (D + 1), row * static_cast<size_t>(len),
                            cudaMemcpyHostToDevice, ctx->copy_stream));
         CK(cudaEventRecord(ctx->copy_events[s], ctx->copy_stream));
@@ -798,8 +805,8 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         // keeps the count still needed and the chunk's totals (iter), and the
         // rounds after the one that completes the iteration do no work.
         // Otherwise the chunk is one round, its record read back at its end.
-        const long long S = u_host ? std::min(m, kUploadSlice) : m;
-        const long long n_rounds = (m + S - 1) / S;
+        const long long S = u_host ? std::min(m, kUploadSlice) : m;  // rows of the largest round
+        const long long n_rounds = u_host ? slice_count(m) : 1;
         if (u_host) {
             if ((rc = upload_host(ctx, u + tried * (D + 1), m))) return rc;
             k_iter_init<<<1, 1, 0, ctx->stream>>>(iter, needed);
@@ -818,7 +825,9 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         CK(ctx->ctl3.ensure(3 * sizeof(RoundCtl)));
         RoundCtl *ctl_pre = ctx->ctl3.as<RoundCtl>(), *ctl_list = ctl_pre + 1;
         for (long long q = 0; q < n_rounds; ++q) {
-            const long long r0 = q * S, mm = std::min(S, m - r0);  // this round's rows of the chunk
+            // this round's rows of the chunk: [r0, r0 + mm)
+            const long long r0 = u_host ? slice_begin(q) : 0;
+            const long long mm = u_host ? std::min(slice_begin(q + 1), m) - r0 : m;
             const long long nbf = (mm + kFwdBlock - 1) / kFwdBlock, nbw = (mm + kWgtBlock - 1) / kWgtBlock;
             const long long *gate = u_host ? iter : nullptr;
             // records with stride mm
