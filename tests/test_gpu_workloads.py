@@ -139,14 +139,16 @@ def test_optimize_writes_one_json_line_per_iteration(ctx_factory):
     assert lines[-1]["pooled"] == mean and mean > 0 and 0 < err < mean
 
 
-def test_host_uniforms_in_slices_match_device_uniforms(ctx_factory):
-    """Host uniforms (pinned) are uploaded in slices of 2^18 rows and each
-    slice is mapped and weighted as its own round; the same uniforms in
+@pytest.mark.parametrize("pipeline", [1, 0])
+def test_host_uniforms_in_slices_match_device_uniforms(ctx_factory, pipeline):
+    """Host uniforms (pinned) are uploaded in slices (2^16 rows, then 2^18)
+    and each slice is mapped and weighted as its own queued round; the same uniforms in
     device memory are read in place in one round.  Both take the same points
     (counts exact) and agree to the rounding of the partial-sum folds, over
     two adapting iterations with the physical-region cuts (the first one on
     uniform grids outgrows its predicted upload and needs a second one).
-    The first iteration's largest weight agrees bit for bit."""
+    The first iteration's largest weight agrees bit for bit.  Both weight
+    passes: the phased one and the fused per-point one (pipeline 0)."""
     import torch
     cs = workloads.channel_set(4)
     ctxs = []
@@ -156,6 +158,7 @@ def test_host_uniforms_in_slices_match_device_uniforms(ctx_factory):
         ctx.uniform_grids(cs.nch, ctx.ndims, 100)
         ctx.set_integrand(abi.CHILI_FUNC_PROPAGATOR, channels.propagator_params())
         ctx.set_preprocess_cuts(1000.0)
+        ctx.set_option("pipeline", pipeline)
         ctxs.append(ctx)
     params = workloads.mc_params(200_000)
     rng = np.random.default_rng(29)
