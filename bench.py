@@ -416,7 +416,13 @@ def measure_flow(ctx, args, dev, stream, plain, train_steps=None):
     from chili_b200 import abi, gpu
     n = int(round(plain["points_per_step"]))
     train_steps = args.flow_steps if train_steps is None else train_steps
-    ctx.flow_init(abi.FlowParams.defaults(batch=args.flow_batch, layers=WL["flow_layers"], lr=1e-3))
+    fp = abi.FlowParams.defaults(batch=args.flow_batch, layers=WL["flow_layers"], lr=1e-3)
+    # one-time costs (first launch of each kernel, first allocations) outside
+    # the timed training: three steps on a throwaway network, then a fresh one
+    ctx.flow_init(fp)
+    ctx.flow_train(3, seed=SEED + 76, counter=0)
+    torch.cuda.synchronize(dev)
+    ctx.flow_init(fp)
     k0 = {k: ctx.kernel_time(k) for k in FLOW_KERNELS}
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)

@@ -50,7 +50,7 @@ struct BatchTask {
     int32_t ch_off;            // first ChannelProgram / channel-weight slot
     int32_t desc;              // IntegrandDesc index
     int32_t pp;                // PointProgram index, -1: per-channel weights
-    int32_t pad;
+    int32_t phased;            // 1: weighted by the phased pass, outside k_batch_eval
     double grid_alpha, beta, min_alpha;
     double before;             // edge_before_table(dims, bins)
     uint64_t key;              // Philox key of the task
@@ -212,6 +212,131 @@ __global__ void __launch_bounds__(256) k_batch_eval(BatchDev B) {
     }
 }
 
+// Phased multichannel tasks (the shared-entry weight pass of the single
+// iterations, pipeline.cuh, one tile of up to ph_tile points of one task at a
+// time): step 1, the points p0 .. p0+mm-1 of task ti as k_batch_eval draws
+// them (Philox key of the task, counters (iteration << 32) + point), the
+// channel, VEGAS map, FSMapper and PreProcess; accepted points' external
+// momenta to mom_soa [slot][component][ms], per block of kFwdBlock points
+// the accepted count.
+__global__ void __launch_bounds__(kFwdBlock) k_bt_forward(BatchDev B, int ti, long long p0, long long mm,
+                                                          double *__restrict__ mom_soa, long long ms,
+                                                          int32_t *__restrict__ ich_out, uint8_t *__restrict__ flag,
+                                                          int32_t *__restrict__ block_count) {
+    const BatchTask T = B.tasks[ti];
+    const long long k = blockIdx.x * static_cast<long long>(kFwdBlock) + threadIdx.x;
+    int acc = 0;
+    if (k < mm) {
+        const int D = T.dims, bins = T.bins;
+        const uint64_t ctr = (*B.iter << 32) + static_cast<uint64_t>(p0 + k);
+        double r[CHILI_MAX_DIMS + 1];
+        load_uniforms(T.key, ctr, nullptr, D + 1, r);
+        const int c = select_channel(B.cp + T.ch_off, T.nch, r[D]);
+        const double *g = B.grids + T.grid_off + static_cast<size_t>(c) * D * (bins + 1);
+        double jac;
+        if (grid_map_checked(g, D, bins, r, jac)) {
+            V4 mom[CHILI_MAX_SLOTS];
+            double m2[CHILI_MAX_SLOTS];
+            const ChannelProgram *prog = B.progs + T.ch_off + c;
+            fs_generate(prog, r, mom, m2);
+            if (preprocess(B.descs + T.desc, mom)) {
+                acc = 1;
+                for (int s = 0; s < prog->n_ext; ++s) {
+                    mom_soa[(4 * s + 0) * ms + k] = mom[s].e;
+                    mom_soa[(4 * s + 1) * ms + k] = mom[s].x;
+                    mom_soa[(4 * s + 2) * ms + k] = mom[s].y;
+                    mom_soa[(4 * s + 3) * ms + k] = mom[s].z;
+                }
+            }
+        }
+        ich_out[k] = c;
+        flag[k] = static_cast<uint8_t>(acc);
+    }
+    const int cnt = __syncthreads_count(acc);
+    if (threadIdx.x == 0) block_count[blockIdx.x] = cnt;
+}
+
+// Step 3 (after compact_launch and pp_pass_launch): block b of the tile is
+// work unit p0/kFwdBlock + b of the task; its accepted points are the records
+// block_off[b] .. + block_count[b] (the list keeps point order), the others
+// are calls of value 0.  StatsData partial of the unit, AddTrainData
+// (MultiChannel.hh:167-180) histogram adds and channel-training terms, as
+// k_batch_eval does per point (NaN values count as 0).
+__global__ void __launch_bounds__(kFwdBlock) k_bt_accum(BatchDev B, int ti, long long p0, long long mm,
+                                                        const int32_t *__restrict__ block_count,
+                                                        const long long *__restrict__ block_off,
+                                                        const double *__restrict__ rec_val,
+                                                        const double *__restrict__ rec_wgt,
+                                                        const uint8_t *__restrict__ rec_ok,
+                                                        const int32_t *__restrict__ rec_slot,
+                                                        const double *__restrict__ rec_dens, long long mr) {
+    __shared__ double ws[kFwdBlock / 32][6];
+    __shared__ double s_atr[kBatchMaxCh];
+    const BatchTask T = B.tasks[ti];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    if (t < kBatchMaxCh) s_atr[t] = 0.0;
+    __syncthreads();
+    const long long k0 = blockIdx.x * static_cast<long long>(kFwdBlock);
+    const long long active = mm - k0 < kFwdBlock ? mm - k0 : kFwdBlock;
+    const int nrec = block_count[blockIdx.x];
+    const long long r = block_off[blockIdx.x] + t;
+    double val = 0, vw = 0;
+    if (t < nrec) {
+        val = rec_ok[r] ? rec_val[r] : 0.0;
+        if (isnan(val)) val = 0;
+        if (val != 0) {
+            const double v2 = val * val;
+            double *H = B.hist + T.hist_off;
+            for (int j = 0; j < T.dims; ++j) {
+                const int s = rec_slot[j * mr + r];
+                if (s >= 0) atomicAdd(H + s, v2);
+            }
+            vw = v2 * rec_wgt[r];
+        }
+    }
+    const unsigned any = __ballot_sync(0xffffffffu, vw != 0);
+    if (any) {
+        for (int c = 0; c < T.nch; ++c) {
+            double term = 0.0;
+            if (vw != 0) {  // only the records' own lanes read their densities
+                term = vw / rec_dens[c * mr + r];
+                if (!isfinite(term)) term = 0.0;  // non-finite terms dropped
+            }
+            term = warp_sum(term);
+            if (lane == 0 && term != 0) atomicAdd(s_atr + c, term);
+        }
+    }
+    // StatsData over the unit's active points: the records, and value-0
+    // calls for the rest (they enter min and max as 0)
+    double cnt = t < nrec ? 1 : 0, sum = val, sum2 = val * val, nf = val != 0 ? 1 : 0;
+    double mn = t < nrec ? val : 1.7976931348623157e308, mx = t < nrec ? val : 2.2250738585072014e-308;
+    cnt = warp_sum(cnt);
+    sum = warp_sum(sum);
+    sum2 = warp_sum(sum2);
+    nf = warp_sum(nf);
+    mn = warp_min(mn);
+    mx = warp_max(mx);
+    if (lane == 0) {
+        ws[w][0] = cnt; ws[w][1] = mn; ws[w][2] = mx; ws[w][3] = sum; ws[w][4] = sum2; ws[w][5] = nf;
+    }
+    __syncthreads();
+    if (t == 0) {
+        double a[6] = {ws[0][0], ws[0][1], ws[0][2], ws[0][3], ws[0][4], ws[0][5]};
+        for (int q = 1; q < kFwdBlock / 32; ++q) {
+            a[0] += ws[q][0]; a[1] = std_min(a[1], ws[q][1]); a[2] = std_max(a[2], ws[q][2]);
+            a[3] += ws[q][3]; a[4] += ws[q][4]; a[5] += ws[q][5];
+        }
+        if (nrec < active) {  // rejected points: calls of value 0
+            a[0] += static_cast<double>(active - nrec);
+            a[1] = std_min(a[1], 0.0);
+            a[2] = std_max(a[2], 0.0);
+        }
+        double *o = B.part + (T.unit0 + p0 / kFwdBlock + blockIdx.x) * 6;
+        for (int q = 0; q < 6; ++q) o[q] = a[q];
+    }
+    if (t < T.nch && s_atr[t] != 0) atomicAdd(B.atrain + T.ch_off + t, s_atr[t]);
+}
+
 // The PointPrograms' (smin, smax) terms.
 __global__ void k_batch_pp_prepare(PointProgram *__restrict__ pps) {
     PointProgram *pp = pps + blockIdx.x;
@@ -307,8 +432,16 @@ struct BatchState {
     DevBuf d_tasks, d_umap, d_pps, d_progs, d_descs, d_grids, d_grids_new, d_hist, d_atrain, d_alpha, d_best, d_mindiff,
         d_cp, d_part, d_stats, d_counters, d_jobs, d_status;
     int block = 0, ppt = 0, grid_blocks = 0;
+    long long n_pulled = 0;  // units k_batch_eval pulls (the tasks that are not phased)
+    // phased multichannel tasks: host copies of the point programs (launch
+    // sizes) and one tile's buffers (ph_tile points)
+    std::vector<PointProgram> pps_host;
+    long long ph_tile = 0;
+    DevBuf ph_mom, ph_ich, ph_flag, ph_list, ph_bcount, ph_boff, ph_ctl, ph_node, ph_memo, ph_cfail, ph_dcv, ph_vwv,
+        ph_ich_tile, ph_val, ph_wgt, ph_ok, ph_slot, ph_dens;
     bool tuned = false;
     cudaGraphExec_t graph = nullptr;
+    unsigned long long graph_launches = 0;  // kernels of one replay
     int graph_adapt = -1;
     double last_ms = 0;
     size_t hist_doubles = 0;
@@ -328,7 +461,7 @@ BatchDev batch_dev(chili_ctx *ctx) {
     B.tasks = S.d_tasks.as<BatchTask>();
     B.ntasks = static_cast<int>(S.tasks.size());
     B.umap = S.d_umap.as<UnitRef>();
-    B.nunits = S.nunits;
+    B.nunits = S.n_pulled;
     B.progs = S.d_progs.as<ChannelProgram>();
     B.pps = S.d_pps.as<PointProgram>();
     B.descs = S.d_descs.as<IntegrandDesc>();
@@ -356,19 +489,22 @@ int layout_units(chili_ctx *ctx, int block, int ppt) {
     long long u = 0;
     const long long tile = static_cast<long long>(block) * ppt;
     for (auto &T : S.tasks) {
+        // a phased task's units are the kFwdBlock-point blocks of its tiles
+        const long long tt = T.phased ? kFwdBlock : tile;
         T.unit0 = u;
-        T.units = (T.ncalls + tile - 1) / tile;
+        T.units = (T.ncalls + tt - 1) / tt;
         u += T.units;
     }
     S.nunits = u;
-    S.umap.resize(static_cast<size_t>(u));
     {
         std::vector<std::pair<double, UnitRef>> order;
         order.reserve(static_cast<size_t>(u));
         for (size_t k = 0; k < S.tasks.size(); ++k)
-            for (long long j = 0; j < S.tasks[k].units; ++j)
+            for (long long j = 0; j < S.tasks[k].units && !S.tasks[k].phased; ++j)
                 order.push_back({(j + 0.5) / static_cast<double>(S.tasks[k].units),
                                  UnitRef{static_cast<int32_t>(k), static_cast<int32_t>(j)}});
+        S.umap.resize(order.size());
+        S.n_pulled = static_cast<long long>(order.size());
         std::stable_sort(order.begin(), order.end(),
                          [](const auto &a, const auto &b) { return a.first < b.first; });
         for (size_t k = 0; k < order.size(); ++k) S.umap[k] = order[k].second;
@@ -376,7 +512,7 @@ int layout_units(chili_ctx *ctx, int block, int ppt) {
     CK(S.d_tasks.ensure(sizeof(BatchTask) * S.tasks.size()));
     CK(cudaMemcpyAsync(S.d_tasks.p, S.tasks.data(), sizeof(BatchTask) * S.tasks.size(), cudaMemcpyHostToDevice,
                        ctx->stream));
-    CK(S.d_umap.ensure(sizeof(UnitRef) * S.umap.size()));
+    CK(S.d_umap.ensure(sizeof(UnitRef) * std::max<size_t>(S.umap.size(), 1)));
     CK(cudaMemcpyAsync(S.d_umap.p, S.umap.data(), sizeof(UnitRef) * S.umap.size(), cudaMemcpyHostToDevice,
                        ctx->stream));
     CK(S.d_part.ensure(sizeof(double) * 6 * u));
@@ -398,6 +534,56 @@ int enqueue_iteration(chili_ctx *ctx, bool adapt) {
     BatchDev B = batch_dev(ctx);
     k_batch_eval<<<S.grid_blocks, S.block, 0, ctx->stream>>>(B);
     LAUNCHED();
+    for (size_t ti = 0; ti < S.tasks.size(); ++ti) {
+        const BatchTask &T = S.tasks[ti];
+        if (!T.phased) continue;
+        const long long ms = S.ph_tile;
+        RoundCtl *ctl = S.ph_ctl.as<RoundCtl>();
+        const long long *n_list =
+            reinterpret_cast<const long long *>(reinterpret_cast<const char *>(ctl) + offsetof(RoundCtl, n_acc));
+        for (long long p0 = 0; p0 < T.ncalls; p0 += ms) {
+            const long long mm = std::min(ms, T.ncalls - p0);
+            const unsigned nb = static_cast<unsigned>((mm + kFwdBlock - 1) / kFwdBlock);
+            k_bt_forward<<<nb, kFwdBlock, 0, ctx->stream>>>(B, static_cast<int>(ti), p0, mm, S.ph_mom.as<double>(), ms,
+                                                           S.ph_ich.as<int32_t>(), S.ph_flag.as<uint8_t>(),
+                                                           S.ph_bcount.as<int32_t>());
+            LAUNCHED();
+            if (int rc = compact_launch(ctx, S.ph_bcount.as<int32_t>(), static_cast<int>(nb), S.ph_flag.as<uint8_t>(),
+                                        mm, S.ph_boff.as<long long>(), ctl, S.ph_list.as<int32_t>()))
+                return rc;
+            PPPass a{};
+            a.pp = S.d_pps.as<PointProgram>() + T.pp;
+            a.pp_host = &S.pps_host[static_cast<size_t>(T.pp)];
+            a.mom_soa = S.ph_mom.as<double>();
+            a.mc = ms;
+            a.list = S.ph_list.as<int32_t>();
+            a.ich = S.ph_ich.as<int32_t>();
+            a.n_list = n_list;
+            a.T = mm;
+            a.mr = ms;
+            a.bins = T.bins;
+            a.grids = B.grids + T.grid_off;
+            a.node_soa = S.ph_node.as<double>();
+            a.memo = S.ph_memo.as<double>();
+            a.dcv = S.ph_dcv.as<double>();
+            a.vwv = S.ph_vwv.as<double>();
+            a.cfail = S.ph_cfail.as<uint8_t>();
+            a.ich_tile = S.ph_ich_tile.as<int32_t>();
+            a.rec_slot = S.ph_slot.as<int32_t>();
+            a.rec_dens = S.ph_dens.as<double>();
+            a.alpha = B.alpha + T.ch_off;
+            a.f = B.descs + T.desc;
+            a.rec_val = S.ph_val.as<double>();
+            a.rec_wgt = S.ph_wgt.as<double>();
+            a.rec_ok = S.ph_ok.as<uint8_t>();
+            if (int rc = pp_pass_launch(ctx, a)) return rc;
+            k_bt_accum<<<nb, kFwdBlock, 0, ctx->stream>>>(B, static_cast<int>(ti), p0, mm, S.ph_bcount.as<int32_t>(),
+                                                         S.ph_boff.as<long long>(), S.ph_val.as<double>(),
+                                                         S.ph_wgt.as<double>(), S.ph_ok.as<uint8_t>(),
+                                                         S.ph_slot.as<int32_t>(), S.ph_dens.as<double>(), ms);
+            LAUNCHED();
+        }
+    }
     k_batch_finalize<<<static_cast<unsigned>(S.tasks.size()), kFoldThreads, 0, ctx->stream>>>(B, adapt ? 1 : 0);
     LAUNCHED();
     if (adapt && !S.jobs.empty()) {
@@ -459,6 +645,7 @@ int capture(chili_ctx *ctx, bool adapt) {
     const unsigned long long launches = ctx->launches;  // replays are counted, not the capture
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     const int rc = enqueue_iteration(ctx, adapt);
+    S.graph_launches = ctx->launches - launches;
     ctx->launches = launches;
     cudaGraph_t captured = nullptr;
     const cudaError_t e = cudaStreamEndCapture(ctx->stream, &captured);
@@ -482,7 +669,9 @@ void batch_release(chili_ctx *ctx) {
     if (S.graph) cudaGraphExecDestroy(S.graph);
     for (DevBuf *b : {&S.d_tasks, &S.d_umap, &S.d_pps, &S.d_progs, &S.d_descs, &S.d_grids, &S.d_grids_new, &S.d_hist,
                       &S.d_atrain, &S.d_alpha, &S.d_best, &S.d_mindiff, &S.d_cp, &S.d_part, &S.d_stats,
-                      &S.d_counters, &S.d_jobs, &S.d_status})
+                      &S.d_counters, &S.d_jobs, &S.d_status, &S.ph_mom, &S.ph_ich, &S.ph_flag, &S.ph_list,
+                      &S.ph_bcount, &S.ph_boff, &S.ph_ctl, &S.ph_node, &S.ph_memo, &S.ph_cfail, &S.ph_dcv, &S.ph_vwv,
+                      &S.ph_ich_tile, &S.ph_val, &S.ph_wgt, &S.ph_ok, &S.ph_slot, &S.ph_dens})
         b->release();
     delete ctx->batch;
     ctx->batch = nullptr;
@@ -556,6 +745,8 @@ int chili_gpu_batch_set(chili_ctx *ctx, const chili_task *tasks, int ntasks) {
             pps.emplace_back();
             if (build_point_program(p, pps.back())) T.pp = static_cast<int32_t>(pps.size() - 1);
             else pps.pop_back();
+            // weighted by the phased pass when its kernels cover the set
+            T.phased = (T.pp >= 0 && ctx->batch_phased && pipeline_dims_ok(T.dims)) ? 1 : 0;
             T.ch_off = static_cast<int32_t>(alpha.size());
             for (int c = 0; c < t.nch; ++c) alpha.push_back(1.0 / t.nch);
             for (auto &q : p) progs.push_back(q);
@@ -593,6 +784,47 @@ int chili_gpu_batch_set(chili_ctx *ctx, const chili_task *tasks, int ntasks) {
     }
     const size_t nslot = alpha.size();
     S.hist_doubles = static_cast<size_t>(hoff);
+    {
+        // one tile of the phased tasks: up to 2^19 points, buffers for the
+        // largest point program among them
+        long long tile = 0;
+        int ne = 1, nn = 1, nmemo = 1, nchain = 1, nch = 1, dims = 1;
+        for (const auto &T : S.tasks) {
+            if (!T.phased) continue;
+            const PointProgram &P = pps[static_cast<size_t>(T.pp)];
+            tile = std::max(tile, (T.ncalls + kFwdBlock - 1) / kFwdBlock * kFwdBlock);
+            ne = std::max(ne, P.n_ext);
+            nn = std::max(nn, P.n_nodes);
+            nmemo = std::max(nmemo, P.n_memo);
+            nchain = std::max(nchain, P.n_chains);
+            nch = std::max(nch, P.nch);
+            dims = std::max(dims, P.ndims);
+        }
+        S.ph_tile = std::min<long long>(tile, 1ll << 19);
+        const size_t T = static_cast<size_t>(std::max<long long>(S.ph_tile, kFwdBlock));
+        const size_t nb = T / kFwdBlock;
+        if (S.ph_tile > 0) {
+            CK(S.ph_mom.ensure(sizeof(double) * 4 * ne * T));
+            CK(S.ph_ich.ensure(sizeof(int32_t) * T));
+            CK(S.ph_flag.ensure(T));
+            CK(S.ph_list.ensure(sizeof(int32_t) * T));
+            CK(S.ph_bcount.ensure(sizeof(int32_t) * nb));
+            CK(S.ph_boff.ensure(sizeof(long long) * nb));
+            CK(S.ph_ctl.ensure(sizeof(RoundCtl)));
+            CK(S.ph_node.ensure(sizeof(double) * 4 * nn * T));
+            CK(S.ph_memo.ensure(sizeof(double) * nmemo * T));
+            CK(S.ph_cfail.ensure(static_cast<size_t>(nchain) * T));
+            CK(S.ph_dcv.ensure(sizeof(double) * nch * T));
+            CK(S.ph_vwv.ensure(sizeof(double) * nch * T));
+            CK(S.ph_ich_tile.ensure(sizeof(int32_t) * T));
+            CK(S.ph_val.ensure(sizeof(double) * T));
+            CK(S.ph_wgt.ensure(sizeof(double) * T));
+            CK(S.ph_ok.ensure(T));
+            CK(S.ph_slot.ensure(sizeof(int32_t) * dims * T));
+            CK(S.ph_dens.ensure(sizeof(double) * nch * T));
+        }
+    }
+    S.pps_host = pps;
     CK(S.d_progs.ensure(sizeof(ChannelProgram) * progs.size()));
     CK(cudaMemcpyAsync(S.d_progs.p, progs.data(), sizeof(ChannelProgram) * progs.size(), cudaMemcpyHostToDevice,
                        ctx->stream));
@@ -692,7 +924,7 @@ int chili_gpu_batch_iterate(chili_ctx *ctx, int iterations, uint64_t seed, int a
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    ctx->launches += static_cast<unsigned long long>(iterations) * (adapt && !S.jobs.empty() ? 5 : 3);
+    ctx->launches += static_cast<unsigned long long>(iterations) * S.graph_launches;
     S.last_ms = ms / iterations;
     if (stats) {
         std::vector<double> all(6 * static_cast<size_t>(S.nslots_alloc) * nt);

@@ -24,14 +24,14 @@
 
 using namespace chili_dev;
 
-namespace {
-
 bool pipeline_dims_ok(int d) {
     switch (d) {
     case 1: case 4: case 7: case 10: case 13: case 16: case 19: case 22: return true;
     default: return false;
     }
 }
+
+namespace {
 
 template <int D>
 void launch_channel(chili_ctx *ctx, long long base, long long T, long long mr, int bins, int opt,
@@ -75,16 +75,21 @@ int pipeline_run(chili_ctx *ctx, const double *mom_soa, long long m, const int32
         LAUNCHED();
         if (n_items > 0) {
             KTimer kt_(ctx, KT_ITEMS);
-            if (P.n_tents > 0)
+            if (P.n_tents > 0) {
                 k_pp_items<0><<<dim3(P.n_tents, gx), 256, 0, ctx->stream>>>(pp, ctx->node_soa.as<double>(), n_list,
                                                                              base, T, ctx->memo.as<double>());
-            if (P.n_dws > 0)
+                LAUNCHED();
+            }
+            if (P.n_dws > 0) {
                 k_pp_items<1><<<dim3(P.n_dws, gx), 256, 0, ctx->stream>>>(pp, ctx->node_soa.as<double>(), n_list,
                                                                            base, T, ctx->memo.as<double>());
-            if (P.n_sws > 0)
+                LAUNCHED();
+            }
+            if (P.n_sws > 0) {
                 k_pp_items<2><<<dim3(P.n_sws, gx), 256, 0, ctx->stream>>>(pp, ctx->node_soa.as<double>(), n_list,
                                                                            base, T, ctx->memo.as<double>());
-            LAUNCHED();
+                LAUNCHED();
+            }
         }
         { KTimer kt_(ctx, KT_CHAINS);
         k_pp_chains<<<dim3(P.n_chains, gx), 256, 0, ctx->stream>>>(pp, ctx->node_soa.as<double>(), n_list, base, T,
@@ -100,6 +105,58 @@ int pipeline_run(chili_ctx *ctx, const double *mom_soa, long long m, const int32
         LAUNCHED();
         if (int rc = combine(base, T)) return rc;
     }
+    return CHILI_OK;
+}
+
+int pp_pass_launch(chili_ctx *ctx, const PPPass &a) {
+    const PointProgram &P = *a.pp_host;
+    const long long T = a.T;
+    if (T < 1 || T > 65535ll * 128) return fail(ctx, CHILI_ERR_LIMIT, "phased pass of 1 .. 65535*128 points");
+    const unsigned gx = static_cast<unsigned>((T + 255) / 256);
+    k_pp_nodes<<<gx, 256, 0, ctx->stream>>>(a.pp, a.mom_soa, a.mc, a.list, a.ich, a.n_list, 0, a.node_soa, a.ich_tile,
+                                             T);
+    LAUNCHED();
+    if (P.n_tents > 0) {
+        k_pp_items<0><<<dim3(P.n_tents, gx), 256, 0, ctx->stream>>>(a.pp, a.node_soa, a.n_list, 0, T, a.memo);
+        LAUNCHED();
+    }
+    if (P.n_dws > 0) {
+        k_pp_items<1><<<dim3(P.n_dws, gx), 256, 0, ctx->stream>>>(a.pp, a.node_soa, a.n_list, 0, T, a.memo);
+        LAUNCHED();
+    }
+    if (P.n_sws > 0) {
+        k_pp_items<2><<<dim3(P.n_sws, gx), 256, 0, ctx->stream>>>(a.pp, a.node_soa, a.n_list, 0, T, a.memo);
+        LAUNCHED();
+    }
+    if (P.n_chains > 0) {
+        k_pp_chains<<<dim3(P.n_chains, gx), 256, 0, ctx->stream>>>(a.pp, a.node_soa, a.n_list, 0, T, a.memo, a.cfail);
+        LAUNCHED();
+    }
+    const dim3 gc(static_cast<unsigned>(P.nch), static_cast<unsigned>((T + 127) / 128));
+    switch (P.ndims) {
+#define CHILI_CH(D)                                                                                              \
+    case D:                                                                                                      \
+        k_pp_channel<D><<<gc, 128, 0, ctx->stream>>>(a.pp, a.grids, a.hints, a.sorted, a.widths, a.bins, a.memo, \
+                                                     a.cfail, a.ich_tile, a.n_list, 0, T, a.mr, 1, a.dcv, a.vwv, \
+                                                     a.rec_slot, a.rec_dens);                                    \
+        break;
+        CHILI_CH(1) CHILI_CH(4) CHILI_CH(7) CHILI_CH(10) CHILI_CH(13) CHILI_CH(16) CHILI_CH(19) CHILI_CH(22)
+#undef CHILI_CH
+    default: return fail(ctx, CHILI_ERR_STATE, "no phased weight kernel for this dimension");
+    }
+    LAUNCHED();
+    k_pp_combine<<<gx, 256, 0, ctx->stream>>>(a.pp, a.alpha, a.dcv, a.vwv, a.node_soa, a.n_list, 0, T, a.f,
+                                               a.rec_val, a.rec_wgt, a.rec_ok);
+    LAUNCHED();
+    return CHILI_OK;
+}
+
+int compact_launch(chili_ctx *ctx, const int32_t *block_count, int nb, const uint8_t *flag, long long m,
+                   long long *block_off, RoundCtl *ctl, int32_t *list) {
+    k_mc_scan<<<1, 1024, 0, ctx->stream>>>(block_count, nb, flag, m, m + 1, nullptr, 0, block_off, ctl);
+    LAUNCHED();
+    k_mc_compact<<<static_cast<unsigned>(nb), kFwdBlock, 0, ctx->stream>>>(flag, block_off, ctl, m, list);
+    LAUNCHED();
     return CHILI_OK;
 }
 
@@ -316,6 +373,10 @@ int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value) {
     }
     if (std::strcmp(name, "defer_train") == 0) {
         ctx->defer_train = value != 0;
+        return CHILI_OK;
+    }
+    if (std::strcmp(name, "batch_phased") == 0) {
+        ctx->batch_phased = value != 0;
         return CHILI_OK;
     }
     if (std::strcmp(name, "pipeline_tile") == 0) {

@@ -71,6 +71,40 @@ int pipeline_run(chili_ctx *ctx, const double *mom_soa, long long m, const int32
                  const long long *n_list, long long n_pre, int bins, bool opt, int32_t *rec_slot, double *rec_dens,
                  const TileFn &combine);
 
+// One phased weight pass with explicit buffers and no host round trip (so
+// that a graph can capture it; chili_gpu.cu): T launch points, of which the
+// first *n_list are listed; tile-local buffers with stride T, records with
+// stride mr; hints, sorted and widths may be null (plain bin search).
+struct PPPass {
+    const PointProgram *pp;       // device
+    const PointProgram *pp_host;  // host copy: launch sizes
+    const double *mom_soa;        // [slot][component][mc]
+    long long mc;
+    const int32_t *list, *ich;
+    const long long *n_list;
+    long long T, mr;
+    int bins;
+    const double *grids;
+    const uint32_t *hints;
+    const uint8_t *sorted;
+    const double *widths;
+    double *node_soa, *memo, *dcv, *vwv;
+    uint8_t *cfail;
+    int32_t *ich_tile, *rec_slot;
+    double *rec_dens;
+    const double *alpha;
+    const IntegrandDesc *f;
+    double *rec_val, *rec_wgt;
+    uint8_t *rec_ok;
+};
+int pp_pass_launch(chili_ctx *ctx, const PPPass &a);
+// The ordered list of flagged points of m (per-block counts of kFwdBlock
+// points in block_count): offsets, ctl->n_acc and list (chili_gpu.cu).
+int compact_launch(chili_ctx *ctx, const int32_t *block_count, int nb, const uint8_t *flag, long long m,
+                   long long *block_off, RoundCtl *ctl, int32_t *list);
+// Whether the phased weight kernels are built for this many dimensions.
+bool pipeline_dims_ok(int d);
+
 struct chili_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -92,6 +126,7 @@ struct chili_ctx {
     bool use_pp = true;        // option "point_program"
     bool use_pipeline = true;  // option "pipeline": phased weight pass
     bool defer_train = false;  // option "defer_train": iterations collect training data, Train is the caller's
+    bool batch_phased = true;  // option "batch_phased": batched multichannel tasks by the phased weight pass
     long long pipe_tile = 1 << 22;  // option "pipeline_tile": points per tile
     long long max_rounds = 100000;  // option "max_rounds": chunks an iteration may take before CHILI_ERR_TIMEOUT
     PointProgram pp_host;      // host copy (sizes of the memo buffers)

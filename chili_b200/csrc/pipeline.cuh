@@ -258,15 +258,18 @@ __global__ void __launch_bounds__(128) k_pp_channel(
     const double fb = static_cast<double>(bins);
     const double before = edge_before_table(DIMS, bins);
     const double *g = grids + static_cast<size_t>(c) * DIMS * (bins + 1);
-    const uint32_t *hc = hints + static_cast<size_t>(c) * DIMS * H;
-    const double *wc = widths + static_cast<size_t>(c) * DIMS * bins;
-    const uint8_t *sc = sorted + c * DIMS;
+    const uint32_t *hc = hints ? hints + static_cast<size_t>(c) * DIMS * H : nullptr;
+    const double *wc = widths ? widths + static_cast<size_t>(c) * DIMS * bins : nullptr;
+    const uint8_t *sc = sorted ? sorted + c * DIMS : nullptr;
     const bool chosen = should_opt && c == ich_tile[i];
     double vw = 1.0;
 #pragma unroll
     for (int p = 0; p < DIMS; ++p) {
-        const int b = find_bin_hinted(g + p * (bins + 1), hc + p * H, __ldg(sc + p) != 0, bins, H, x[p]);
-        vw = __dmul_rn(vw, __dmul_rn(bin_width_t(g, wc, bins, p, b, before), fb));
+        // without hint tables (batched tasks): the plain search and widths
+        const int b = hints ? find_bin_hinted(g + p * (bins + 1), hc + p * H, __ldg(sc + p) != 0, bins, H, x[p])
+                            : find_bin(g + p * (bins + 1), bins, x[p]);
+        const double wdt = hints ? bin_width_t(g, wc, bins, p, b, before) : bin_width(g, bins, p, b, before);
+        vw = __dmul_rn(vw, __dmul_rn(wdt, fb));
         if (chosen) {
             const int s = p * bins + b;
             rec_slot[p * mr + r] = s >= 0 ? c * DIMS * bins + s : -1;
