@@ -843,24 +843,26 @@ def run_batched(args, rank, world, local_rank):
     ctx.close()
 
 
-# k_batch_eval per drawn point, all tasks together (the small case keeps the
-# tasks' mix: every point count scaled by 1/16), from the committed ncu
-# capture (the batched-integrands summary under profiles/): FP64 operations (2*DFMA + DADD +
-# DMUL, executed) and DRAM bytes (read + write; almost all of it the
-# kernel's local-memory stack, not algorithmic traffic).
-BATCH_COUNTERS = {"fp64_ops_per_point": 5683.0, "dram_bytes_per_point": 1702.0,
+# One iteration's kernels per drawn point, all tasks together (the small case
+# keeps the tasks' mix: every point count scaled by 1/16), from the committed
+# ncu capture (the batched-integrands summary under profiles/): FP64
+# operations (2*DFMA + DADD + DMUL, executed) and DRAM bytes (read + write).
+BATCH_COUNTERS = {"fp64_ops_per_point": 3623.3, "dram_bytes_per_point": 651.0,
                   "source": "profiles/batched_integrands.md"}
 
 
 def batched_roofline(ms_per_iter, tasks, dev):
-    """k_batch_eval (the whole evaluation of an iteration, >97% of its device
-    time) against the FP64 peak measured in this run; its algorithmic HBM
-    traffic is nil (counter-based uniforms, grids and histograms in L2)."""
+    """The iteration's kernels together (k_batch_eval for the camel tasks;
+    k_bt_forward, the phased k_pp_* weight pass and k_bt_accum for the
+    multichannel ones) against the FP64 peak measured in this run; the
+    algorithmic HBM traffic is nil (counter-based uniforms, grids and
+    histograms in L2; the phased buffers of one task tile)."""
     peak = fp64_peak_tflops(dev)
     npts = sum(t["ncalls"] for t in tasks)
     c = BATCH_COUNTERS
     achieved = c["fp64_ops_per_point"] * npts / (ms_per_iter / 1e3) / 1e12
-    return {"kernel": "k_batch_eval", "bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+    return {"kernel": "k_batch_eval + k_bt_forward + k_pp_* + k_bt_accum (one iteration)", "bound": "fp64",
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak, "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
             "traffic": c["dram_bytes_per_point"] * npts, "counters_source": c["source"],
             "note": "ms_per_iter is the whole iteration (evaluation, folds, adaptation)"}
