@@ -40,6 +40,8 @@ namespace {
 // Channels per multichannel task (the per-thread channel densities live in
 // local memory).
 constexpr int kBatchMaxCh = 64;
+// Parallel branches of the phased multichannel task chains in the graph.
+constexpr int kPhBranches = 8;
 
 struct BatchTask {
     int32_t kind, dims, bins, nch;
@@ -437,8 +439,14 @@ struct BatchState {
     // sizes) and one tile's buffers (ph_tile points)
     std::vector<PointProgram> pps_host;
     long long ph_tile = 0;
-    DevBuf ph_mom, ph_ich, ph_flag, ph_list, ph_bcount, ph_boff, ph_ctl, ph_node, ph_memo, ph_cfail, ph_dcv, ph_vwv,
-        ph_ich_tile, ph_val, ph_wgt, ph_ok, ph_slot, ph_dens;
+    struct PhBufs {
+        DevBuf mom, ich, flag, list, bcount, boff, ctl, node, memo, cfail, dcv, vwv, ich_tile, val, wgt, ok, slot, dens;
+    };
+    // the task chains run as kPhBranches parallel branches of the graph,
+    // each with its own stream (at capture) and tile buffers
+    std::vector<PhBufs> ph;
+    std::vector<cudaStream_t> ph_streams;
+    std::vector<cudaEvent_t> ph_events;
     bool tuned = false;
     cudaGraphExec_t graph = nullptr;
     unsigned long long graph_launches = 0;  // kernels of one replay
@@ -526,62 +534,95 @@ int layout_units(chili_ctx *ctx, int block, int ppt) {
     return CHILI_OK;
 }
 
+// The kernels of one phased task, tile by tile, on ctx->stream with the
+// buffers b.
+int enqueue_phased_task(chili_ctx *ctx, const BatchDev &B, int ti, BatchState::PhBufs &b) {
+    BatchState &S = *ctx->batch;
+    const BatchTask &T = S.tasks[static_cast<size_t>(ti)];
+    const long long ms = S.ph_tile;
+    RoundCtl *ctl = b.ctl.as<RoundCtl>();
+    const long long *n_list =
+        reinterpret_cast<const long long *>(reinterpret_cast<const char *>(ctl) + offsetof(RoundCtl, n_acc));
+    for (long long p0 = 0; p0 < T.ncalls; p0 += ms) {
+        const long long mm = std::min(ms, T.ncalls - p0);
+        const unsigned nb = static_cast<unsigned>((mm + kFwdBlock - 1) / kFwdBlock);
+        k_bt_forward<<<nb, kFwdBlock, 0, ctx->stream>>>(B, ti, p0, mm, b.mom.as<double>(), ms, b.ich.as<int32_t>(),
+                                                       b.flag.as<uint8_t>(), b.bcount.as<int32_t>());
+        LAUNCHED();
+        if (int rc = compact_launch(ctx, b.bcount.as<int32_t>(), static_cast<int>(nb), b.flag.as<uint8_t>(), mm,
+                                    b.boff.as<long long>(), ctl, b.list.as<int32_t>()))
+            return rc;
+        PPPass a{};
+        a.pp = S.d_pps.as<PointProgram>() + T.pp;
+        a.pp_host = &S.pps_host[static_cast<size_t>(T.pp)];
+        a.mom_soa = b.mom.as<double>();
+        a.mc = ms;
+        a.list = b.list.as<int32_t>();
+        a.ich = b.ich.as<int32_t>();
+        a.n_list = n_list;
+        a.T = mm;
+        a.mr = ms;
+        a.bins = T.bins;
+        a.grids = B.grids + T.grid_off;
+        a.node_soa = b.node.as<double>();
+        a.memo = b.memo.as<double>();
+        a.dcv = b.dcv.as<double>();
+        a.vwv = b.vwv.as<double>();
+        a.cfail = b.cfail.as<uint8_t>();
+        a.ich_tile = b.ich_tile.as<int32_t>();
+        a.rec_slot = b.slot.as<int32_t>();
+        a.rec_dens = b.dens.as<double>();
+        a.alpha = B.alpha + T.ch_off;
+        a.f = B.descs + T.desc;
+        a.rec_val = b.val.as<double>();
+        a.rec_wgt = b.wgt.as<double>();
+        a.rec_ok = b.ok.as<uint8_t>();
+        if (int rc = pp_pass_launch(ctx, a)) return rc;
+        k_bt_accum<<<nb, kFwdBlock, 0, ctx->stream>>>(B, ti, p0, mm, b.bcount.as<int32_t>(), b.boff.as<long long>(),
+                                                     b.val.as<double>(), b.wgt.as<double>(), b.ok.as<uint8_t>(),
+                                                     b.slot.as<int32_t>(), b.dens.as<double>(), ms);
+        LAUNCHED();
+    }
+    return CHILI_OK;
+}
+
 // The iteration as a stream of launches (captured into the graph).
 int enqueue_iteration(chili_ctx *ctx, bool adapt) {
     BatchState &S = *ctx->batch;
     CK(cudaMemsetAsync(S.d_hist.p, 0, sizeof(double) * S.hist_doubles, ctx->stream));
     CK(cudaMemsetAsync(S.d_atrain.p, 0, S.d_atrain.cap, ctx->stream));
     BatchDev B = batch_dev(ctx);
+    const cudaStream_t main = ctx->stream;
+    if (!S.ph.empty()) CK(cudaEventRecord(S.ph_events[kPhBranches], main));
     k_batch_eval<<<S.grid_blocks, S.block, 0, ctx->stream>>>(B);
     LAUNCHED();
-    for (size_t ti = 0; ti < S.tasks.size(); ++ti) {
-        const BatchTask &T = S.tasks[ti];
-        if (!T.phased) continue;
-        const long long ms = S.ph_tile;
-        RoundCtl *ctl = S.ph_ctl.as<RoundCtl>();
-        const long long *n_list =
-            reinterpret_cast<const long long *>(reinterpret_cast<const char *>(ctl) + offsetof(RoundCtl, n_acc));
-        for (long long p0 = 0; p0 < T.ncalls; p0 += ms) {
-            const long long mm = std::min(ms, T.ncalls - p0);
-            const unsigned nb = static_cast<unsigned>((mm + kFwdBlock - 1) / kFwdBlock);
-            k_bt_forward<<<nb, kFwdBlock, 0, ctx->stream>>>(B, static_cast<int>(ti), p0, mm, S.ph_mom.as<double>(), ms,
-                                                           S.ph_ich.as<int32_t>(), S.ph_flag.as<uint8_t>(),
-                                                           S.ph_bcount.as<int32_t>());
-            LAUNCHED();
-            if (int rc = compact_launch(ctx, S.ph_bcount.as<int32_t>(), static_cast<int>(nb), S.ph_flag.as<uint8_t>(),
-                                        mm, S.ph_boff.as<long long>(), ctl, S.ph_list.as<int32_t>()))
-                return rc;
-            PPPass a{};
-            a.pp = S.d_pps.as<PointProgram>() + T.pp;
-            a.pp_host = &S.pps_host[static_cast<size_t>(T.pp)];
-            a.mom_soa = S.ph_mom.as<double>();
-            a.mc = ms;
-            a.list = S.ph_list.as<int32_t>();
-            a.ich = S.ph_ich.as<int32_t>();
-            a.n_list = n_list;
-            a.T = mm;
-            a.mr = ms;
-            a.bins = T.bins;
-            a.grids = B.grids + T.grid_off;
-            a.node_soa = S.ph_node.as<double>();
-            a.memo = S.ph_memo.as<double>();
-            a.dcv = S.ph_dcv.as<double>();
-            a.vwv = S.ph_vwv.as<double>();
-            a.cfail = S.ph_cfail.as<uint8_t>();
-            a.ich_tile = S.ph_ich_tile.as<int32_t>();
-            a.rec_slot = S.ph_slot.as<int32_t>();
-            a.rec_dens = S.ph_dens.as<double>();
-            a.alpha = B.alpha + T.ch_off;
-            a.f = B.descs + T.desc;
-            a.rec_val = S.ph_val.as<double>();
-            a.rec_wgt = S.ph_wgt.as<double>();
-            a.rec_ok = S.ph_ok.as<uint8_t>();
-            if (int rc = pp_pass_launch(ctx, a)) return rc;
-            k_bt_accum<<<nb, kFwdBlock, 0, ctx->stream>>>(B, static_cast<int>(ti), p0, mm, S.ph_bcount.as<int32_t>(),
-                                                         S.ph_boff.as<long long>(), S.ph_val.as<double>(),
-                                                         S.ph_wgt.as<double>(), S.ph_ok.as<uint8_t>(),
-                                                         S.ph_slot.as<int32_t>(), S.ph_dens.as<double>(), ms);
-            LAUNCHED();
+    if (!S.ph.empty()) {
+        // fork (before the camel tasks' evaluation, which runs beside the
+        // branches): each branch runs its phased tasks on its own stream and
+        // buffers; join before the folds
+        // tasks by decreasing points, each to the branch with the fewest
+        // points so far (longest-processing-time order)
+        std::vector<int> order;
+        for (size_t ti = 0; ti < S.tasks.size(); ++ti)
+            if (S.tasks[ti].phased) order.push_back(static_cast<int>(ti));
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int a, int b) { return S.tasks[a].ncalls > S.tasks[b].ncalls; });
+        std::vector<long long> load(kPhBranches, 0);
+        std::vector<bool> used(kPhBranches, false);
+        for (int ti : order) {
+            const int br = static_cast<int>(std::min_element(load.begin(), load.end()) - load.begin());
+            load[br] += S.tasks[ti].ncalls;
+            if (!used[br]) CK(cudaStreamWaitEvent(S.ph_streams[br], S.ph_events[kPhBranches], 0));
+            used[br] = true;
+            ctx->stream = S.ph_streams[br];  // the launchers below enqueue on ctx->stream
+            const int rc = enqueue_phased_task(ctx, B, ti, S.ph[br]);
+            ctx->stream = main;
+            if (rc) return rc;
+        }
+        for (int br = 0; br < kPhBranches; ++br) {
+            if (!used[br]) continue;
+            CK(cudaEventRecord(S.ph_events[br], S.ph_streams[br]));
+            CK(cudaStreamWaitEvent(main, S.ph_events[br], 0));
         }
     }
     k_batch_finalize<<<static_cast<unsigned>(S.tasks.size()), kFoldThreads, 0, ctx->stream>>>(B, adapt ? 1 : 0);
@@ -669,10 +710,14 @@ void batch_release(chili_ctx *ctx) {
     if (S.graph) cudaGraphExecDestroy(S.graph);
     for (DevBuf *b : {&S.d_tasks, &S.d_umap, &S.d_pps, &S.d_progs, &S.d_descs, &S.d_grids, &S.d_grids_new, &S.d_hist,
                       &S.d_atrain, &S.d_alpha, &S.d_best, &S.d_mindiff, &S.d_cp, &S.d_part, &S.d_stats,
-                      &S.d_counters, &S.d_jobs, &S.d_status, &S.ph_mom, &S.ph_ich, &S.ph_flag, &S.ph_list,
-                      &S.ph_bcount, &S.ph_boff, &S.ph_ctl, &S.ph_node, &S.ph_memo, &S.ph_cfail, &S.ph_dcv, &S.ph_vwv,
-                      &S.ph_ich_tile, &S.ph_val, &S.ph_wgt, &S.ph_ok, &S.ph_slot, &S.ph_dens})
+                      &S.d_counters, &S.d_jobs, &S.d_status})
         b->release();
+    for (auto &b : S.ph)
+        for (DevBuf *d : {&b.mom, &b.ich, &b.flag, &b.list, &b.bcount, &b.boff, &b.ctl, &b.node, &b.memo, &b.cfail,
+                          &b.dcv, &b.vwv, &b.ich_tile, &b.val, &b.wgt, &b.ok, &b.slot, &b.dens})
+            d->release();
+    for (cudaStream_t st : S.ph_streams) cudaStreamDestroy(st);
+    for (cudaEvent_t e : S.ph_events) cudaEventDestroy(e);
     delete ctx->batch;
     ctx->batch = nullptr;
 }
@@ -800,28 +845,41 @@ int chili_gpu_batch_set(chili_ctx *ctx, const chili_task *tasks, int ntasks) {
             nch = std::max(nch, P.nch);
             dims = std::max(dims, P.ndims);
         }
-        S.ph_tile = std::min<long long>(tile, 1ll << 19);
+        S.ph_tile = std::min<long long>(tile, 1ll << 18);
         const size_t T = static_cast<size_t>(std::max<long long>(S.ph_tile, kFwdBlock));
         const size_t nb = T / kFwdBlock;
         if (S.ph_tile > 0) {
-            CK(S.ph_mom.ensure(sizeof(double) * 4 * ne * T));
-            CK(S.ph_ich.ensure(sizeof(int32_t) * T));
-            CK(S.ph_flag.ensure(T));
-            CK(S.ph_list.ensure(sizeof(int32_t) * T));
-            CK(S.ph_bcount.ensure(sizeof(int32_t) * nb));
-            CK(S.ph_boff.ensure(sizeof(long long) * nb));
-            CK(S.ph_ctl.ensure(sizeof(RoundCtl)));
-            CK(S.ph_node.ensure(sizeof(double) * 4 * nn * T));
-            CK(S.ph_memo.ensure(sizeof(double) * nmemo * T));
-            CK(S.ph_cfail.ensure(static_cast<size_t>(nchain) * T));
-            CK(S.ph_dcv.ensure(sizeof(double) * nch * T));
-            CK(S.ph_vwv.ensure(sizeof(double) * nch * T));
-            CK(S.ph_ich_tile.ensure(sizeof(int32_t) * T));
-            CK(S.ph_val.ensure(sizeof(double) * T));
-            CK(S.ph_wgt.ensure(sizeof(double) * T));
-            CK(S.ph_ok.ensure(T));
-            CK(S.ph_slot.ensure(sizeof(int32_t) * dims * T));
-            CK(S.ph_dens.ensure(sizeof(double) * nch * T));
+            S.ph.resize(kPhBranches);
+            for (auto &b : S.ph) {
+                CK(b.mom.ensure(sizeof(double) * 4 * ne * T));
+                CK(b.ich.ensure(sizeof(int32_t) * T));
+                CK(b.flag.ensure(T));
+                CK(b.list.ensure(sizeof(int32_t) * T));
+                CK(b.bcount.ensure(sizeof(int32_t) * nb));
+                CK(b.boff.ensure(sizeof(long long) * nb));
+                CK(b.ctl.ensure(sizeof(RoundCtl)));
+                CK(b.node.ensure(sizeof(double) * 4 * nn * T));
+                CK(b.memo.ensure(sizeof(double) * nmemo * T));
+                CK(b.cfail.ensure(static_cast<size_t>(nchain) * T));
+                CK(b.dcv.ensure(sizeof(double) * nch * T));
+                CK(b.vwv.ensure(sizeof(double) * nch * T));
+                CK(b.ich_tile.ensure(sizeof(int32_t) * T));
+                CK(b.val.ensure(sizeof(double) * T));
+                CK(b.wgt.ensure(sizeof(double) * T));
+                CK(b.ok.ensure(T));
+                CK(b.slot.ensure(sizeof(int32_t) * dims * T));
+                CK(b.dens.ensure(sizeof(double) * nch * T));
+            }
+            for (int k = 0; k < kPhBranches; ++k) {
+                cudaStream_t st;
+                CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+                S.ph_streams.push_back(st);
+            }
+            for (int k = 0; k <= kPhBranches; ++k) {
+                cudaEvent_t e;
+                CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+                S.ph_events.push_back(e);
+            }
         }
     }
     S.pps_host = pps;
