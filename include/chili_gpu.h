@@ -201,7 +201,11 @@ uint64_t chili_gpu_launch_count(const chili_ctx *ctx);
  * 0 (default) trains at the end of the iteration.
  * "max_rounds": chunks of points a multichannel iteration may draw before it
  * gives up with CHILI_ERR_TIMEOUT (default 100000; the reference's loop has
- * no such bound and never ends when every point is rejected or NaN). */
+ * no such bound and never ends when every point is rejected or NaN).
+ * "batch_phased": 1 (default) weights the batched multichannel tasks whose
+ * channel set has a shared-entry program with the phased weight pass (task
+ * chains as parallel graph branches); 0 evaluates every point in one thread
+ * of the persistent batch kernel.  Read by chili_gpu_batch_set. */
 int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value);
 /* Total device time (ms) and launch count of one kernel class under the
  * "kernel_timing" option: k_mc_forward, k_pp_nodes, k_pp_items, k_pp_chains,

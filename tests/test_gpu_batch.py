@@ -109,9 +109,17 @@ def test_camel_tasks_match_the_oracle(ctx_factory):
     assert info.block in (128, 256) and info.points_per_thread in (1, 2, 4)
 
 
-def test_multichannel_tasks_match_the_oracle(ctx_factory):
-    tasks = [mc_task(2, 500.0, 20000, 20), mc_task(3, 1500.0, 5000, 30), mc_task(4, 1000.0, 30000, 25, cuts=True)]
-    run_and_check(ctx_factory(), tasks, seed=11, iterations=2)
+@pytest.mark.parametrize("phased", [1, 0])
+def test_multichannel_tasks_match_the_oracle(ctx_factory, phased):
+    """Both weight passes of the batched multichannel tasks: the phased one
+    (task chains of the shared-entry kernels, the default) and every point
+    in one thread of the persistent kernel (option batch_phased 0)."""
+    # the 2->4 task spans two phased tiles (2^18 points each)
+    tasks = [mc_task(2, 500.0, 20000, 20), mc_task(3, 1500.0, 5000, 30), mc_task(4, 1000.0, 265000, 25, cuts=True),
+             mc_task(5, 800.0, 20000, 15)]
+    ctx = ctx_factory()
+    ctx.set_option("batch_phased", phased)
+    run_and_check(ctx, tasks, seed=11, iterations=2)
 
 
 def test_mixed_batch_matches_the_oracle(ctx_factory):
