@@ -59,12 +59,16 @@ int pipeline_run(chili_ctx *ctx, const double *mom_soa, long long m, const int32
     // gridDim.y (point blocks of 128) stays below 65536
     const long long T = std::min<long long>(std::min<long long>(ctx->pipe_tile, 65535ll * 128),
                                             std::max<long long>(n_pre, 1));
-    CK(ctx->node_soa.ensure(sizeof(double) * 4 * P.n_nodes * T));
-    CK(ctx->memo.ensure(sizeof(double) * std::max(1, P.n_memo) * T));
-    CK(ctx->cfail.ensure(static_cast<size_t>(std::max(1, P.n_chains)) * T));
-    CK(ctx->dcv.ensure(sizeof(double) * ctx->nch * T));
-    CK(ctx->ich_tile.ensure(sizeof(int32_t) * T));
-    CK(ctx->vwv.ensure(sizeof(double) * ctx->nch * T));
+    // buffers for a whole number of 2^16 points: the accepted count of a
+    // chunk varies from call to call, and a buffer that grew by a few points
+    // each time would be reallocated (a device synchronisation) each time
+    const long long Ta = (T + 65535) / 65536 * 65536;
+    CK(ctx->node_soa.ensure(sizeof(double) * 4 * P.n_nodes * Ta));
+    CK(ctx->memo.ensure(sizeof(double) * std::max(1, P.n_memo) * Ta));
+    CK(ctx->cfail.ensure(static_cast<size_t>(std::max(1, P.n_chains)) * Ta));
+    CK(ctx->dcv.ensure(sizeof(double) * ctx->nch * Ta));
+    CK(ctx->ich_tile.ensure(sizeof(int32_t) * Ta));
+    CK(ctx->vwv.ensure(sizeof(double) * ctx->nch * Ta));
     const unsigned gx = static_cast<unsigned>((T + 255) / 256);
     const int n_items = P.n_tents + P.n_dws + P.n_sws;
     const int o = opt ? 1 : 0;
@@ -134,11 +138,16 @@ int pp_pass_launch(chili_ctx *ctx, const PPPass &a) {
     }
     const dim3 gc(static_cast<unsigned>(P.nch), static_cast<unsigned>((T + 127) / 128));
     switch (P.ndims) {
-#define CHILI_CH(D)                                                                                              \
-    case D:                                                                                                      \
-        k_pp_channel<D><<<gc, 128, 0, ctx->stream>>>(a.pp, a.grids, a.hints, a.sorted, a.widths, a.bins, a.memo, \
-                                                     a.cfail, a.ich_tile, a.n_list, 0, T, a.mr, 1, a.dcv, a.vwv, \
-                                                     a.rec_slot, a.rec_dens);                                    \
+#define CHILI_CH(D)                                                                                          \
+    case D:                                                                                                  \
+        if (a.hints)                                                                                         \
+            k_pp_channel<D, true><<<gc, 128, 0, ctx->stream>>>(                                              \
+                a.pp, a.grids, a.hints, a.sorted, a.widths, a.bins, a.memo, a.cfail, a.ich_tile, a.n_list, 0, T, \
+                a.mr, 1, a.dcv, a.vwv, a.rec_slot, a.rec_dens);                                              \
+        else                                                                                                 \
+            k_pp_channel<D, false><<<gc, 128, 0, ctx->stream>>>(                                             \
+                a.pp, a.grids, a.hints, a.sorted, a.widths, a.bins, a.memo, a.cfail, a.ich_tile, a.n_list, 0, T, \
+                a.mr, 1, a.dcv, a.vwv, a.rec_slot, a.rec_dens);                                              \
         break;
         CHILI_CH(1) CHILI_CH(4) CHILI_CH(7) CHILI_CH(10) CHILI_CH(13) CHILI_CH(16) CHILI_CH(19) CHILI_CH(22)
 #undef CHILI_CH

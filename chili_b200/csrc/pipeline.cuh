@@ -214,7 +214,9 @@ __device__ __forceinline__ double eval_momenta_soa(const IntegrandDesc *__restri
 // uniform of the latest earlier channel whose chain did not fail (zero if
 // none).  Writes dcv/vwv (tile-local, stride m), the density record and, for
 // the point's own channel, the histogram slots.
-template <int DIMS>
+// HINTS false (batched tasks): the plain bin search and widths from the
+// edges, no hint tables.
+template <int DIMS, bool HINTS = true>
 __global__ void __launch_bounds__(128) k_pp_channel(
     const PointProgram *__restrict__ pp, const double *__restrict__ grids, const uint32_t *__restrict__ hints,
     const uint8_t *__restrict__ sorted, const double *__restrict__ widths, int bins, const double *__restrict__ memo,
@@ -258,17 +260,22 @@ __global__ void __launch_bounds__(128) k_pp_channel(
     const double fb = static_cast<double>(bins);
     const double before = edge_before_table(DIMS, bins);
     const double *g = grids + static_cast<size_t>(c) * DIMS * (bins + 1);
-    const uint32_t *hc = hints ? hints + static_cast<size_t>(c) * DIMS * H : nullptr;
-    const double *wc = widths ? widths + static_cast<size_t>(c) * DIMS * bins : nullptr;
-    const uint8_t *sc = sorted ? sorted + c * DIMS : nullptr;
+    const uint32_t *hc = HINTS ? hints + static_cast<size_t>(c) * DIMS * H : nullptr;
+    const double *wc = HINTS ? widths + static_cast<size_t>(c) * DIMS * bins : nullptr;
+    const uint8_t *sc = HINTS ? sorted + c * DIMS : nullptr;
     const bool chosen = should_opt && c == ich_tile[i];
     double vw = 1.0;
 #pragma unroll
     for (int p = 0; p < DIMS; ++p) {
-        // without hint tables (batched tasks): the plain search and widths
-        const int b = hints ? find_bin_hinted(g + p * (bins + 1), hc + p * H, __ldg(sc + p) != 0, bins, H, x[p])
-                            : find_bin(g + p * (bins + 1), bins, x[p]);
-        const double wdt = hints ? bin_width_t(g, wc, bins, p, b, before) : bin_width(g, bins, p, b, before);
+        int b;
+        double wdt;
+        if constexpr (HINTS) {
+            b = find_bin_hinted(g + p * (bins + 1), hc + p * H, __ldg(sc + p) != 0, bins, H, x[p]);
+            wdt = bin_width_t(g, wc, bins, p, b, before);
+        } else {
+            b = find_bin(g + p * (bins + 1), bins, x[p]);
+            wdt = bin_width(g, bins, p, b, before);
+        }
         vw = __dmul_rn(vw, __dmul_rn(wdt, fb));
         if (chosen) {
             const int s = p * bins + b;
