@@ -882,16 +882,20 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
             k_iter_init<<<1, 1, 0, ctx->stream>>>(iter, needed);
             LAUNCHED();
         }
-        const long long nb_f = (S + kFwdBlock - 1) / kFwdBlock;
-        const long long nb_w = (S + kWgtBlock - 1) / kWgtBlock;
-        CK(ctx->mom_soa.ensure(sizeof(double) * 4 * NE * S));
-        CK(ctx->ich.ensure(sizeof(int32_t) * S));
-        CK(ctx->flag.ensure(S));
-        CK(ctx->list.ensure(sizeof(int32_t) * S));
+        // buffers for a whole number of 2^16 points (the chunk size follows
+        // the acceptance rate and would otherwise reallocate, synchronising
+        // the device, whenever it grows a little)
+        const long long Sa = (S + 65535) / 65536 * 65536;
+        const long long nb_f = (Sa + kFwdBlock - 1) / kFwdBlock;
+        const long long nb_w = (Sa + kWgtBlock - 1) / kWgtBlock;
+        CK(ctx->mom_soa.ensure(sizeof(double) * 4 * NE * Sa));
+        CK(ctx->ich.ensure(sizeof(int32_t) * Sa));
+        CK(ctx->flag.ensure(Sa));
+        CK(ctx->list.ensure(sizeof(int32_t) * Sa));
         CK(ctx->block_count.ensure(sizeof(int32_t) * nb_f));
         CK(ctx->block_off.ensure(sizeof(long long) * nb_f));
         CK(ctx->part.ensure(sizeof(double) * (kPartFixed + nch) * nb_w));
-        CK(ctx->rec.ensure(S * (2 * sizeof(double) + 1 + sizeof(int32_t) * D + sizeof(double) * nch) + 256));
+        CK(ctx->rec.ensure(Sa * (2 * sizeof(double) + 1 + sizeof(int32_t) * D + sizeof(double) * nch) + 256));
         CK(ctx->ctl3.ensure(3 * sizeof(RoundCtl)));
         RoundCtl *ctl_pre = ctx->ctl3.as<RoundCtl>(), *ctl_list = ctl_pre + 1;
         for (long long q = 0; q < n_rounds; ++q) {
