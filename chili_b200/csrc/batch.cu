@@ -436,7 +436,7 @@ struct BatchState {
     int block = 0, ppt = 0, grid_blocks = 0;
     long long n_pulled = 0;  // units k_batch_eval pulls (the tasks that are not phased)
     // phased multichannel tasks: host copies of the point programs (launch
-    // sizes) and one tile's buffers (ph_tile points)
+    // sizes) and the tile size (ph_tile points)
     std::vector<PointProgram> pps_host;
     long long ph_tile = 0;
     struct PhBufs {
@@ -830,8 +830,8 @@ int chili_gpu_batch_set(chili_ctx *ctx, const chili_task *tasks, int ntasks) {
     const size_t nslot = alpha.size();
     S.hist_doubles = static_cast<size_t>(hoff);
     {
-        // one tile of the phased tasks: up to 2^19 points, buffers for the
-        // largest point program among them
+        // one tile of the phased tasks: up to 2^18 points; per branch,
+        // buffers for the largest point program among them
         long long tile = 0;
         int ne = 1, nn = 1, nmemo = 1, nchain = 1, nch = 1, dims = 1;
         for (const auto &T : S.tasks) {
