@@ -212,12 +212,13 @@ int upload_host(chili_ctx *ctx, const double *u, long long m) {
 
 // The phased weight pass of a multichannel chunk: records of the n_pre
 // PreProcess-accepted points of the chunk of m counters.
-int launch_pipeline(chili_ctx *ctx, long long m, long long n_pre, int bins, bool opt, RoundCtl *ctl_pre,
-                    double *rec_val, double *rec_wgt, uint8_t *rec_ok, int32_t *rec_slot, double *rec_dens) {
+int launch_pipeline(chili_ctx *ctx, const double *mom_soa, const int32_t *ich, long long m, long long n_pre, int bins,
+                    bool opt, RoundCtl *ctl_pre, double *rec_val, double *rec_wgt, uint8_t *rec_ok, int32_t *rec_slot,
+                    double *rec_dens) {
     const PointProgram *pp = ctx->point_prog.as<PointProgram>();
     const long long *n_list = reinterpret_cast<const long long *>(
         reinterpret_cast<const char *>(ctl_pre) + offsetof(RoundCtl, n_acc));
-    return pipeline_run(ctx, ctx->mom_soa.as<double>(), m, ctx->list.as<int32_t>(), ctx->ich.as<int32_t>(), n_list,
+    return pipeline_run(ctx, mom_soa, m, ctx->list.as<int32_t>(), ich, n_list,
                         n_pre, bins, opt, rec_slot, rec_dens, [&](long long base, long long T) -> int {
                             const unsigned gx = static_cast<unsigned>((T + 255) / 256);
                             {
@@ -296,7 +297,8 @@ int chili_gpu_destroy(chili_ctx *ctx) {
     DevBuf *bufs[] = {&ctx->edges, &ctx->edges_tmp, &ctx->progs, &ctx->point_prog, &ctx->node_soa, &ctx->memo, &ctx->cfail, &ctx->dcv, &ctx->vwv, &ctx->hints, &ctx->sorted, &ctx->widths, &ctx->ich_tile, &ctx->alpha_buf, &ctx->f_dev, &ctx->mom_soa,
                       &ctx->ich, &ctx->flag, &ctx->list, &ctx->block_count, &ctx->block_off, &ctx->part,
                       &ctx->hist, &ctx->round_res, &ctx->acc, &ctx->ctl, &ctx->status, &ctx->v_part,
-                      &ctx->v_hist, &ctx->v_train, &ctx->v_out, &ctx->rec, &ctx->ctl3, &ctx->unw, &ctx->iter_ctl};
+                      &ctx->v_hist, &ctx->v_train, &ctx->v_out, &ctx->rec, &ctx->ctl3, &ctx->unw, &ctx->iter_ctl,
+                      &ctx->mom_soa_alt, &ctx->ich_alt, &ctx->flag_alt, &ctx->block_count_alt};
     for (DevBuf *b : bufs) b->release();
     flow_release(ctx);
     batch_release(ctx);
@@ -306,6 +308,14 @@ int chili_gpu_destroy(chili_ctx *ctx) {
     collect_times(ctx);
     for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : ctx->copy_events) cudaEventDestroy(e);
+    for (int k = 0; k < 2; ++k) {
+        if (ctx->fwd_done[k]) cudaEventDestroy(ctx->fwd_done[k]);
+        if (ctx->round_done[k]) cudaEventDestroy(ctx->round_done[k]);
+    }
+    if (ctx->fwd_stream) {
+        cudaStreamSynchronize(ctx->fwd_stream);
+        cudaStreamDestroy(ctx->fwd_stream);
+    }
     if (ctx->copy_stream) {
         cudaStreamSynchronize(ctx->copy_stream);
         cudaStreamDestroy(ctx->copy_stream);
@@ -898,6 +908,20 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         CK(ctx->rec.ensure(Sa * (2 * sizeof(double) + 1 + sizeof(int32_t) * D + sizeof(double) * nch) + 256));
         CK(ctx->ctl3.ensure(3 * sizeof(RoundCtl)));
         RoundCtl *ctl_pre = ctx->ctl3.as<RoundCtl>(), *ctl_list = ctl_pre + 1;
+        if (u_host) {
+            // the second set of forward buffers and the forward stream
+            CK(ctx->mom_soa_alt.ensure(sizeof(double) * 4 * NE * Sa));
+            CK(ctx->ich_alt.ensure(sizeof(int32_t) * Sa));
+            CK(ctx->flag_alt.ensure(Sa));
+            CK(ctx->block_count_alt.ensure(sizeof(int32_t) * nb_f));
+            if (!ctx->fwd_stream) {
+                CK(cudaStreamCreateWithFlags(&ctx->fwd_stream, cudaStreamNonBlocking));
+                for (int k = 0; k < 2; ++k) {
+                    CK(cudaEventCreateWithFlags(&ctx->fwd_done[k], cudaEventDisableTiming));
+                    CK(cudaEventCreateWithFlags(&ctx->round_done[k], cudaEventDisableTiming));
+                }
+            }
+        }
         for (long long q = 0; q < n_rounds; ++q) {
             // this round's rows of the chunk: [r0, r0 + mm)
             const long long r0 = u_host ? slice_begin(q) : 0;
@@ -910,28 +934,45 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
             double *rec_dens = rec_wgt + mm;
             int32_t *rec_slot = reinterpret_cast<int32_t *>(rec_dens + static_cast<size_t>(nch) * mm);
             uint8_t *rec_ok = reinterpret_cast<uint8_t *>(rec_slot + static_cast<size_t>(D) * mm);
+            // host-uniform rounds alternate between two sets of forward
+            // buffers, so that the forward pass of round q + 1 (on the
+            // forward stream) runs beside the weight pass of round q
+            const int par = u_host ? static_cast<int>(q & 1) : 0;
+            double *mom = (par ? ctx->mom_soa_alt : ctx->mom_soa).as<double>();
+            int32_t *ich = (par ? ctx->ich_alt : ctx->ich).as<int32_t>();
+            uint8_t *flag = (par ? ctx->flag_alt : ctx->flag).as<uint8_t>();
+            int32_t *bcount = (par ? ctx->block_count_alt : ctx->block_count).as<int32_t>();
             {
                 const double *u_in = ud ? ud + (tried + r0) * (D + 1) : nullptr;
+                const cudaStream_t main = ctx->stream;
                 if (u_host) {
-                    // the forward launch waits (on the device) for its slice's copy only
-                    CK(cudaStreamWaitEvent(ctx->stream, ctx->copy_events[q], 0));
+                    // the forward launch waits (on the device) for its slice's
+                    // copy and for the round that last used its buffers
+                    CK(cudaStreamWaitEvent(ctx->fwd_stream, ctx->copy_events[q], 0));
+                    if (q >= 2) CK(cudaStreamWaitEvent(ctx->fwd_stream, ctx->round_done[par], 0));
                     u_in = ctx->stage[0].as<double>() + r0 * (D + 1);
+                    ctx->stream = ctx->fwd_stream;
                 }
-                KTimer kt_(ctx, KT_FORWARD);
-                k_mc_forward<<<static_cast<unsigned>(nbf), kFwdBlock, 0, ctx->stream>>>(
-                    ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), cp_ptr(ctx), nch, D, B, seed,
-                    counter_base + tried + r0, u_in, mm, ctx->f_dev.as<IntegrandDesc>(), NE,
-                    ctx->mom_soa.as<double>(), ctx->ich.as<int32_t>(), ctx->flag.as<uint8_t>(),
-                    ctx->block_count.as<int32_t>(), gate);
+                {
+                    KTimer kt_(ctx, KT_FORWARD);
+                    k_mc_forward<<<static_cast<unsigned>(nbf), kFwdBlock, 0, ctx->stream>>>(
+                        ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), cp_ptr(ctx), nch, D, B, seed,
+                        counter_base + tried + r0, u_in, mm, ctx->f_dev.as<IntegrandDesc>(), NE, mom, ich, flag,
+                        bcount, gate);
+                }
+                ctx->stream = main;
                 LAUNCHED();
+                if (u_host) {
+                    CK(cudaEventRecord(ctx->fwd_done[par], ctx->fwd_stream));
+                    CK(cudaStreamWaitEvent(main, ctx->fwd_done[par], 0));
+                }
             }
             // offsets of every PreProcess-accepted point (no cut at this stage)
-            k_mc_scan<<<1, 1024, 0, ctx->stream>>>(ctx->block_count.as<int32_t>(), static_cast<int>(nbf),
-                                                   ctx->flag.as<uint8_t>(), mm, mm + 1, gate, 0,
+            k_mc_scan<<<1, 1024, 0, ctx->stream>>>(bcount, static_cast<int>(nbf), flag, mm, mm + 1, gate, 0,
                                                    ctx->block_off.as<long long>(), ctl_pre);
             LAUNCHED();
             k_mc_compact<<<static_cast<unsigned>(nbf), kFwdBlock, 0, ctx->stream>>>(
-                ctx->flag.as<uint8_t>(), ctx->block_off.as<long long>(), ctl_pre, mm, ctx->list.as<int32_t>());
+                flag, ctx->block_off.as<long long>(), ctl_pre, mm, ctx->list.as<int32_t>());
             LAUNCHED();
             if (pipe) {
                 // the launches are sized by the accepted count, read back here;
@@ -945,25 +986,23 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
                     CK(cudaStreamSynchronize(ctx->stream));
                     n_pre = ctx->ctl_host->n_acc;
                 }
-                int rc2 = launch_pipeline(ctx, mm, n_pre, B, opt, ctl_pre, rec_val, rec_wgt, rec_ok, rec_slot,
-                                          rec_dens);
+                int rc2 = launch_pipeline(ctx, mom, ich, mm, n_pre, B, opt, ctl_pre, rec_val, rec_wgt, rec_ok,
+                                          rec_slot, rec_dens);
                 if (rc2) return rc2;
             } else {
                 KTimer kt_(ctx, KT_WEIGHT);
                 k_mc_weight<<<static_cast<unsigned>(nbw), kWgtBlock, 0, ctx->stream>>>(
                     ctx->progs.as<ChannelProgram>(), ctx->edges.as<double>(), alpha_ptr(ctx), nch, D, B, NE,
-                    ctx->mom_soa.as<double>(), mm, ctx->ich.as<int32_t>(), ctx->list.as<int32_t>(), ctl_pre,
-                    ctx->f_dev.as<IntegrandDesc>(), opt ? 1 : 0, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens,
-                    pp_ptr(ctx));
+                    mom, mm, ich, ctx->list.as<int32_t>(), ctl_pre, ctx->f_dev.as<IntegrandDesc>(), opt ? 1 : 0,
+                    rec_val, rec_wgt, rec_ok, rec_slot, rec_dens, pp_ptr(ctx));
                 LAUNCHED();
             }
             // the cut: the needed-th record whose value is not NaN (the
             // device's count when the rounds are queued)
-            k_block_count<<<static_cast<unsigned>(nbf), kFwdBlock, 0, ctx->stream>>>(rec_ok, ctl_pre,
-                                                                                    ctx->block_count.as<int32_t>());
+            k_block_count<<<static_cast<unsigned>(nbf), kFwdBlock, 0, ctx->stream>>>(rec_ok, ctl_pre, bcount);
             LAUNCHED();
-            k_mc_scan<<<1, 1024, 0, ctx->stream>>>(ctx->block_count.as<int32_t>(), static_cast<int>(nbf), rec_ok,
-                                                   mm, needed, gate, 1, ctx->block_off.as<long long>(), ctl_list);
+            k_mc_scan<<<1, 1024, 0, ctx->stream>>>(bcount, static_cast<int>(nbf), rec_ok, mm, needed, gate, 1,
+                                                   ctx->block_off.as<long long>(), ctl_list);
             LAUNCHED();
             k_cut_finalize<<<1, 1, 0, ctx->stream>>>(ctl_list, ctl_pre, ctx->list.as<int32_t>(), mm, needed,
                                                      u_host ? iter : nullptr, ctx->ctl.as<RoundCtl>());
@@ -982,7 +1021,10 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
             k_mc_accumulate<<<1, 256, 0, ctx->stream>>>(ctx->round_res.as<double>(), nch, ctx->ctl.as<RoundCtl>(),
                                                         ctx->acc.as<IterAcc>());
             LAUNCHED();
-            if (u_host) continue;
+            if (u_host) {
+                CK(cudaEventRecord(ctx->round_done[par], ctx->stream));
+                continue;
+            }
             CK(cudaMemcpyAsync(ctx->ctl_host, ctx->ctl.p, sizeof(RoundCtl), cudaMemcpyDeviceToHost, ctx->stream));
             CK(cudaMemcpyAsync(ctx->ctl_host + 1, ctl_pre, sizeof(RoundCtl), cudaMemcpyDeviceToHost, ctx->stream));
             CK(cudaStreamSynchronize(ctx->stream));
@@ -1175,7 +1217,8 @@ int chili_gpu_generate_unweighted(chili_ctx *ctx, int64_t n, uint64_t seed, uint
         if (n_pre < 0 || n_pre > m) return fail(ctx, CHILI_ERR_CUDA, "inconsistent point list");
         n_pre_tot += n_pre;
         if (pipe) {
-            if ((rc = launch_pipeline(ctx, m, n_pre, B, false, ctl_pre, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens)))
+            if ((rc = launch_pipeline(ctx, ctx->mom_soa.as<double>(), ctx->ich.as<int32_t>(), m, n_pre, B, false,
+                                      ctl_pre, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens)))
                 return rc;
         } else {
             k_mc_weight<<<static_cast<unsigned>(nb_w), kWgtBlock, 0, ctx->stream>>>(

@@ -142,6 +142,11 @@ struct chili_ctx {
     bool f_set = false;
     // multichannel iteration scratch
     DevBuf mom_soa, ich, flag, list, block_count, block_off, part, hist, round_res, acc, ctl, status;
+    // host-uniform rounds: the forward pass of the next round runs on its own
+    // stream beside this round's weight pass, into the other set of buffers
+    DevBuf mom_soa_alt, ich_alt, flag_alt, block_count_alt;
+    cudaStream_t fwd_stream = nullptr;
+    cudaEvent_t fwd_done[2] = {nullptr, nullptr}, round_done[2] = {nullptr, nullptr};
     RoundCtl *ctl_host = nullptr;  // pinned, two records: the round, the PreProcess count
     long long *iter_host = nullptr;  // pinned, the queued rounds' state (k_iter_init)
     DevBuf iter_ctl;                 // device copy of that state
