@@ -361,7 +361,7 @@ int chili_gpu_multichannel_weight(chili_ctx *ctx, const double *mom,
  * or, when u is not NULL, from u[k*(ndims+1)...] (ndims uniforms then the
  * channel uniform, MultiChannel.hh:145-147) for k < n_u; running out of u is
  * CHILI_ERR_LIMIT.  Device-resident u is read in place; host u (pinned for
- * asynchronous copies) is uploaded in slices of 2^18 rows on a second stream,
+ * asynchronous copies) is uploaded in slices (2^16, 2^18, then 2^19 rows) on a second stream,
  * the rows the last iteration's acceptance rate predicts; each slice is
  * mapped and weighted while the next ones cross PCIe, and rows past the
  * point that completes ncalls are not copied beyond the predicted ones.

@@ -141,7 +141,7 @@ def test_optimize_writes_one_json_line_per_iteration(ctx_factory):
 
 @pytest.mark.parametrize("pipeline", [1, 0])
 def test_host_uniforms_in_slices_match_device_uniforms(ctx_factory, pipeline):
-    """Host uniforms (pinned) are uploaded in slices (2^16 rows, then 2^18)
+    """Host uniforms (pinned) are uploaded in slices (2^16, 2^18, then 2^19 rows)
     and each slice is mapped and weighted as its own queued round; the same uniforms in
     device memory are read in place in one round.  Both take the same points
     (counts exact) and agree to the rounding of the partial-sum folds, over
