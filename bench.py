@@ -75,15 +75,19 @@ def parse():
     ap.add_argument("--flow-long-steps", type=int, default=600,
                     help="also train a second flow this many steps and report it beside the 200-step one "
                          "(0: skip)")
-    ap.add_argument("--workload", default="multichannel", choices=["multichannel", "large", "batched"],
+    ap.add_argument("--workload", default="multichannel", choices=["multichannel", "large", "batched", "vegas"],
                     help="multichannel: the 2->4 iteration with the learned proposal beside it; large: the "
                          "2->6 case (45 channels, 200 bins, 1e7 points per iteration, 10-layer flow, 1e6 "
                          "unweighted events); batched: 512 uneven integrands in one persistent graph-replayed "
-                         "launch per iteration")
+                         "launch per iteration; vegas: plain VEGAS on the 4-d camel (50 bins, 1e5 points per "
+                         "iteration) and its materialised points")
     ap.add_argument("--batch-scale", type=float, default=1.0,
                     help="batched: point counts times this factor (small cases for profiling)")
     ap.add_argument("--no-sequential", action="store_true",
                     help="batched: skip the one-call-per-task comparison")
+    ap.add_argument("--gen-points", type=int, default=100_000_000,
+                    help="vegas: points per launch of the materialised generation")
+    ap.add_argument("--no-t01", action="store_true", help="vegas: skip the time-to-0.1%% run")
     return ap.parse_args()
 
 
@@ -182,7 +186,7 @@ def run_chili(args, rank, world, local_rank):
     synced = world > 1
     if synced:
         from chili_b200 import parallel
-        rank_obj = parallel.GpuRank(ctx, seed, counter)
+        rank_obj = parallel.GpuRank(ctx, seed, counter, shared_stream=True)
 
     def one_step():
         if synced:
@@ -238,7 +242,7 @@ def run_chili(args, rank, world, local_rank):
 
     kernel_ms = {k: ctx.kernel_time(k) for k in TIMED_KERNELS}
     kernel_ms = {k: v for k, v in kernel_ms.items() if v[1] > 0}
-    roof = roofline(kernel_ms, weighted, dev)
+    roof = roofline(kernel_ms, weighted, args.ncalls * args.steps, ms, dev)
 
     plain = {"value": unw_tot / (ms_max / 1e3), "ms_per_step": ms_max / args.steps,
              "points_per_step": tried_tot / args.steps, "integral": mean, "rel_error": err / abs(mean),
@@ -282,9 +286,9 @@ def run_chili(args, rank, world, local_rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (on-device Philox4x32-10 uniforms)",
-            "config": dict(workload_config(args.ncalls),
-                           parallelism=f"dp{world}: ranks synchronised by one NCCL all-reduce of the training data "
-                                       f"per iteration" if world > 1 else "single GPU"),
+            "config": workload_config(args.ncalls),
+            "parallelism": f"dp{world}: ranks synchronised by one NCCL all-reduce of the training data per "
+                           f"iteration" if world > 1 else "single GPU",
             "points_per_s": acc_tot / (ms_max / 1e3),
             "tried_points_per_s": tried_tot / (ms_max / 1e3),
             "weighted_points_per_step": weighted / args.steps,
@@ -365,37 +369,47 @@ def fp64_peak_tflops(dev):
     return 2.0 * n ** 3 / best / 1e12
 
 
-def roofline(kernel_ms, weighted, dev):
-    """The dominant kernel of the timed region (by CUDA-event time) against
-    both of its possible bounds: executed FP64 operations against the FP64
-    peak measured in this run (cuBLAS DGEMM), and DRAM bytes against the
-    measured HBM copy bandwidth. `bound` names the resource that the kernel
-    uses the larger fraction of; the other view is reported beside it."""
+def roofline(kernel_ms, weighted, accepted, step_ms, dev):
+    """The FP64 roofline of the multichannel step (the binding resource:
+    every point evaluates every channel's inverse map, mostly
+    transcendental-function expansions).  For the dominant kernel of the
+    timed region (by CUDA-event time): achieved = its FP64 operations per
+    weighted point (2 DFMA + DADD + DMUL, the committed ncu counters; a
+    property of the per-point work, not of the batch size) x the weighted
+    points of one launch / the launch's average CUDA-event duration, against
+    the cuBLAS DGEMM peak measured in this run.  traffic = its measured DRAM
+    bytes per launch (the phased pass keeps intermediates in HBM: the ratio
+    to its zero algorithmic bytes is the waste).  `step` gives the same view
+    for all kernels of the step, and the HBM view of the materialised event
+    record (204 B per accepted point)."""
     dom = max(kernel_ms, key=lambda k: kernel_ms[k][0])
     ms, launches = kernel_ms[dom]
     peak = fp64_peak_tflops(dev)
     hbm = measured_peaks().get("hbm_gbs")
     c = KERNEL_COUNTERS.get(dom)
-    out = {"kernel": dom, "launches": launches, "ms_per_launch": ms / max(launches, 1),
-           "share_of_kernel_time": ms / sum(v[0] for v in kernel_ms.values()),
+    per_launch = weighted / max(launches, 1)
+    out = {"kernel": dom, "bound": "fp64", "launches": launches, "ms_per_launch": ms / max(launches, 1),
+           "weighted_points_per_launch": per_launch, "share_of_kernel_time": ms / sum(v[0] for v in kernel_ms.values()),
+           "peak": peak, "unit": "TFLOP/s", "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
            "kernel_ms": {k: round(v[0], 4) for k, v in kernel_ms.items()}}
-    if not c:
-        out.update(bound="fp64", achieved=None, peak=peak, unit="TFLOP/s", frac=None, traffic=None)
-        return out
-    sec = ms / 1e3
-    fp64 = {"achieved": c["fp64_ops_per_point"] * weighted / sec / 1e12, "peak": peak, "unit": "TFLOP/s",
-            "peak_source": "cuBLAS DGEMM 8192^3 measured in this run"}
-    fp64["frac"] = fp64["achieved"] / peak
-    mem = {"achieved": c["dram_bytes_per_point"] * weighted / sec / 1e9, "peak": hbm, "unit": "GB/s",
-           "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured copy bandwidth)"}
-    mem["frac"] = mem["achieved"] / hbm if hbm else None
-    if mem["frac"] is not None and mem["frac"] > fp64["frac"]:
-        out.update(bound="hbm", **mem)
-        out["fp64_view"] = fp64
+    if c:
+        ach = c["fp64_ops_per_point"] * per_launch / (ms / max(launches, 1) / 1e3) / 1e12
+        out.update(achieved=ach, frac=ach / peak, fp64_ops_per_point=c["fp64_ops_per_point"],
+                   traffic=c["dram_bytes_per_point"] * per_launch, algorithmic_bytes=0,
+                   counters_source=c["source"])
     else:
-        out.update(bound="fp64", **fp64)
-        out["hbm_view"] = mem
-    out.update(traffic=c["dram_bytes_per_point"] * weighted / max(launches, 1), counters_source=c["source"])
+        out.update(achieved=None, frac=None, traffic=None)
+    ops = sum(KERNEL_COUNTERS[k]["fp64_ops_per_point"] for k in kernel_ms if k in KERNEL_COUNTERS)
+    dram = sum(KERNEL_COUNTERS[k]["dram_bytes_per_point"] for k in kernel_ms if k in KERNEL_COUNTERS)
+    sec = step_ms / 1e3
+    out["step"] = {
+        "fp64": {"ops_per_weighted_point": ops, "achieved": ops * weighted / sec / 1e12, "unit": "TFLOP/s",
+                 "frac": ops * weighted / sec / 1e12 / peak},
+        "hbm_event_record": {"bytes_per_accepted_point": 204, "achieved": 204 * accepted / sec / 1e9, "unit": "GB/s",
+                             "peak": hbm, "frac": 204 * accepted / sec / 1e9 / hbm if hbm else None},
+        "dram_bytes_per_weighted_point": dram,
+        "seconds": sec, "weighted_points": weighted, "accepted_points": accepted,
+    }
     return out
 
 
@@ -597,46 +611,6 @@ def measure_e2e(ctx, params, args, dev, rank):
 
 
 # ------------------------------------------------------------- reference arm
-def _ref_worker_init(ncalls, wl_name):
-    global _W
-    sys.path.insert(0, ROOT)
-    from chili_b200 import abi, channels, workloads
-    from oracle import ref
-    wl = WORKLOADS[wl_name]
-    cs = workloads.channel_set(wl["n_out"])
-    params = workloads.mc_params(ncalls)
-    R = ref.MultiChannel(cs, wl["bins"], params, getattr(abi, "CHILI_FUNC_" + wl["fkind"]),
-                         channels.propagator_params())
-    R.set_cuts(cs.sqrts)
-    _W = {"R": R, "cs": cs, "ncalls": ncalls, "rng": np.random.default_rng(os.getpid()), "wl": workloads}
-
-
-def _ref_worker_step(_):
-    R = _W["R"]
-    # the cuts keep ~13% (2->4) or ~0.6% (2->6) of the points on uniform
-    # grids, more on adapted ones: the uniform buffer grows until it suffices
-    while True:
-        f = _W.setdefault("factor", 12)
-        u = _W["wl"].uniforms53(_W["rng"], (int(_W["ncalls"] * f) + 256, R.ndims + 1))
-        t0 = time.perf_counter()
-        try:
-            st, info = R.iterate(u, guard=True)
-        except RuntimeError:
-            _W["factor"] = f * 4
-            continue
-        dt = time.perf_counter() - t0
-        break
-    return (st.sum / info.weight_max if info.weight_max > 0 else 0.0, _W["ncalls"], info.points_tried, dt,
-            st.as_tuple())
-
-
-def _pool(cores, ncalls):
-    import multiprocessing as mp
-    ctx = mp.get_context("spawn")
-    name = next(k for k, v in WORKLOADS.items() if v is WL)
-    return ctx.Pool(cores, initializer=_ref_worker_init, initargs=(ncalls, name))
-
-
 def cpu_cores():
     try:
         return len(os.sched_getaffinity(0))
@@ -644,63 +618,384 @@ def cpu_cores():
         return os.cpu_count() or 1
 
 
+def reference_ncalls():
+    """Points per reference iteration: the workload's own 1e6 for the 2->4
+    workload (like for like with the GPU step); the 2->6 workload's 1e7
+    points would take minutes per iteration on the host, so a bounded sample
+    of 2000 points per core."""
+    return WL["ncalls"] if WL["n_out"] <= 4 else 2000 * cpu_cores()
+
+
+def _ref_mpi(ncalls):
+    from oracle.mpi_ranks import RefMPI
+    return RefMPI(cpu_cores(), n_out=WL["n_out"], bins=WL["bins"], ncalls=ncalls, fkind=WL["fkind"], seed=SEED,
+                  cuts=True)
+
+
 def cpu_baseline(args, kind="reference"):
-    """The reference (oracle/_ref) timed on the host: one iteration of a
-    bounded sample per core, all cores in parallel (replica stand-in for the
-    reference's MPI mode)."""
+    """The reference (oracle/_ref) timed on the host in its MPI mode
+    (MultiChannel.hh:184-212) over one process per core: one iteration of
+    the workload's points after one warm-up iteration."""
     from oracle import ref
     if not ref.available():
         return {"value": None, "unavailable": "oracle/_ref not built"}
-    cores = cpu_cores()
-    ncalls = 20000 if WL["n_out"] <= 4 else 4000
-    with _pool(cores, ncalls) as pool:
-        pool.map(_ref_worker_step, range(cores))  # warm-up: one adapted iteration each
-        t0 = time.perf_counter()
-        res = pool.map(_ref_worker_step, range(cores))
-        dt = time.perf_counter() - t0
-    unw = sum(r[0] for r in res)
-    return {"value": unw / dt, "unit": UNIT, "cores": cores, "kind": kind,
-            "points_per_s": sum(r[1] for r in res) / dt,
-            "sample": f"one guarded MultiChannel iteration of {ncalls} accepted points per core on {cores} "
-                      f"cores in parallel, after one warm-up iteration"}
+    ncalls = reference_ncalls()
+    with _ref_mpi(ncalls) as M:
+        M.iterate()  # warm-up: the iteration on uniform grids
+        st, w_max, tried, sec = M.iterate()
+    cores = M.nranks
+    return {"value": (st[3] / w_max if w_max > 0 else 0.0) / sec, "unit": UNIT, "cores": cores, "kind": kind,
+            "points_per_s": M.ncalls_rank * cores / sec, "seconds": sec,
+            "sample": f"one MultiChannel iteration of {M.ncalls_rank * cores} accepted points in the reference's "
+                      f"MPI mode ({cores} host processes of {M.ncalls_rank} points, training data summed, every "
+                      f"rank adapting alike), after one warm-up iteration; time = the slowest rank"}
 
 
 def run_reference(args, rank, world):
+    """The reference's own CPU implementation of the step: one
+    MultiChannel::operator() iteration of the workload's points with the
+    alpha and grid adaptation, in the reference's MPI mode over one process
+    per host core (ncalls / size points per rank, training data and StatsData
+    summed, Train on every rank; MultiChannel.hh:184-212).  Each step's time
+    is the slowest rank's iteration plus its Train (the uniforms are drawn
+    before the clock starts); the unweighted events of a step are its summed
+    values over the largest weight of all its points, as on the GPU."""
     if rank != 0:
         return
     from oracle import ref
     if not ref.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libchili_ref.so not built"}))
         return
-    cores = cpu_cores()
-    ncalls = 10000 if WL["n_out"] <= 4 else 2000
-    unw = 0.0
-    acc = 0
+    ncalls = reference_ncalls()
+    unw, secs = 0.0, 0.0
     pooled = np.zeros(6)
-    with _pool(cores, ncalls) as pool:
-        for _ in range(args.warmup):
-            pool.map(_ref_worker_step, range(cores))
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            res = pool.map(_ref_worker_step, range(cores))
-            unw += sum(r[0] for r in res)
-            acc += sum(r[1] for r in res)
-            for r in res:
-                pooled += np.array(r[4]) * np.array([1, 0, 0, 1, 1, 1])
-        dt = time.perf_counter() - t0
-    value = unw / dt
+    history = []
     from chili_b200.gpu import stats_mean_error
+    with _ref_mpi(ncalls) as M:
+        for _ in range(args.warmup):
+            M.iterate()
+        for _ in range(args.steps):
+            st, w_max, tried, sec = M.iterate()
+            unw += st[3] / w_max if w_max > 0 else 0.0
+            secs += sec
+            pooled += np.array(st) * np.array([1, 0, 0, 1, 1, 1])
+            m_, e_ = stats_mean_error(pooled)
+            history.append((secs, e_ / abs(m_) if m_ else float("inf")))
+    cores = M.nranks
+    value = unw / secs
     mean, err = stats_mean_error(pooled)
     line = {
         "impl": "reference", "metric": WL["metric"], "value": value, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (host uniforms)", "config": workload_config(ncalls * cores),
-        "points_per_s": acc / dt, "integral": mean, "rel_error": err / abs(mean),
+        "data": "synthetic (host uniforms)", "config": workload_config(M.ncalls_rank * cores),
+        "parallelism": f"the reference's MPI mode over {cores} host processes",
+        "points_per_s": M.ncalls_rank * cores * args.steps / secs, "integral": mean, "rel_error": err / abs(mean),
+        "time_to_0p1pct_s": next((h[0] for h in history if h[1] <= 1e-3), None),
+        "unweighting_efficiency": unw / (M.ncalls_rank * cores * args.steps),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                         "sample": f"each step: one guarded MultiChannel iteration of {ncalls} accepted points "
-                                   f"per core, {cores} cores in parallel (independent replicas)"},
+                         "sample": f"each step: one MultiChannel iteration of {M.ncalls_rank * cores} accepted "
+                                   f"points in the reference's MPI mode ({cores} processes of {M.ncalls_rank}), "
+                                   f"time = the slowest rank's iteration and Train"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------- plain VEGAS workload
+VEGAS_METRIC = "VEGAS points/s and time to 0.1% error, 4-d camel (50 bins, alpha 1.5, 1e5 points/iteration), FP64"
+VEGAS_UNIT = "points/s"
+# FP64 operations (2*DFMA + DADD + DMUL, executed) per point of the fused
+# iteration kernel, from the committed ncu capture of the 1e5-point
+# iteration (profiles/vegas_camel_kernels.md)
+VEGAS_COUNTERS = {"k_vegas_iter": None}
+
+
+def vegas_config(cfg):
+    return {"workload": f"plain VEGAS, {cfg['dims']}-d camel (sigma 0.1, centres 1/3 and 2/3, unit integral)",
+            "bins_per_dim": cfg["bins"], "grid_alpha": cfg["alpha"], "points_per_iteration": cfg["ncalls"],
+            "seed": cfg["seed"], "refine": "none",
+            "l2": "flushed between timed iterations (256 MB write outside the timed events); the uniforms are "
+                  "generated on the device"}
+
+
+def run_vegas(args, rank, world, local_rank):
+    """Config 1 of the benchmark definition: plain VEGAS (Vegas::operator(),
+    Vegas.cc:18-52) on the 4-d camel.  One step = one iteration of 1e5
+    points with the grid adaptation, fused in one kernel (on-device
+    uniforms, map, camel, StatsData and histogram in shared memory) plus the
+    fold and the adaptation.  Beside it: the materialised points
+    (chili_gpu_vegas_generate: x and f*J written to HBM, 40 B per point),
+    the HBM-bound form of the same map, and the time to 0.1% pooled error."""
+    import ctypes as C
+
+    import torch
+
+    from chili_b200 import abi, gpu, workloads
+    cfg = dict(workloads.VEGAS_CAMEL)
+    n = args.ncalls if args.ncalls else cfg["ncalls"]
+    cfg["ncalls"] = n
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.current_stream(dev)
+    ctx = gpu.Context(local_rank)
+    ctx.set_stream(stream.cuda_stream)
+    params = workloads.camel_params(cfg["dims"])
+    ctx.uniform_grids(1, cfg["dims"], cfg["bins"])
+    ctx.set_integrand(abi.CHILI_FUNC_CAMEL, params)
+    seed = cfg["seed"] + 1000 * rank
+    stats_dev = torch.zeros((args.warmup + args.steps, 6), dtype=torch.float64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step(k, counter):
+        ctx.call("chili_gpu_vegas_iterate", n, seed, counter, None, float(cfg["alpha"]), 1,
+                 C.c_void_p(stats_dev[k].data_ptr()), None)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    counter = 0
+    for k in range(args.warmup):
+        step(k, counter)
+        counter += n
+    torch.cuda.synchronize(dev)
+    barrier()
+    torch.cuda.synchronize(dev)
+    ctx.set_option("kernel_timing", 1)
+    l0 = ctx.launches
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local_rank) as clk:
+        for k in range(args.steps):
+            flush.fill_(k & 0xff)  # L2 flushed between the timed iterations, outside their events
+            evs[k][0].record(stream)
+            step(args.warmup + k, counter)
+            evs[k][1].record(stream)
+            counter += n
+        torch.cuda.synchronize(dev)
+    launches = ctx.launches - l0
+    ctx.set_option("kernel_timing", 0)
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = t.item()
+    st = stats_dev[args.warmup:].cpu().numpy()
+    pooled = (st * np.array([1, 0, 0, 1, 1, 1])).sum(axis=0)
+    mean, err = gpu.stats_mean_error(pooled)
+    kms, kl = ctx.kernel_time("k_vegas_iter")
+    c = VEGAS_COUNTERS.get("k_vegas_iter")
+    peak = fp64_peak_tflops(dev)
+    roof = {"kernel": "k_vegas_iter", "bound": "fp64", "launches": kl, "ms_per_launch": kms / max(kl, 1),
+            "share_of_step": kms / ms, "peak": peak, "unit": "TFLOP/s",
+            "peak_source": "cuBLAS DGEMM 8192^3 measured in this run"}
+    if c:
+        roof.update(achieved=c["fp64_ops_per_point"] * n * kl / (kms / 1e3) / 1e12,
+                    fp64_ops_per_point=c["fp64_ops_per_point"], counters_source=c["source"],
+                    traffic=c.get("dram_bytes_per_launch"))
+        roof["frac"] = roof["achieved"] / peak
+    else:
+        roof.update(achieved=None, frac=None, traffic=None)
+
+    mat = vegas_materialised(ctx, dev, stream, cfg, n=args.gen_points)
+    t01 = None if args.no_t01 else vegas_time_to_target(ctx, cfg, params, seed + 17, dev)
+    e2e = None if args.no_e2e else vegas_e2e(ctx, cfg, args, dev, rank)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline_vegas(cfg)
+    if rank == 0:
+        line = {
+            "metric": VEGAS_METRIC, "value": n * args.steps * world / (ms_max / 1e3), "unit": VEGAS_UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (on-device Philox4x32-10 uniforms)", "config": vegas_config(cfg),
+            "parallelism": f"dp{world}: independent replicas" if world > 1 else "single GPU",
+            "integral": mean, "rel_error": err / abs(mean), "time_to_0p1pct": t01,
+            "clocks": clk.summary(), "gpu_launches": launches, "roofline": roof, "materialised": mat,
+            "e2e": e2e, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def vegas_materialised(ctx, dev, stream, cfg, n=100_000_000, reps=10):
+    """chili_gpu_vegas_generate on the adapted grid: n points, x (8 dims B)
+    and f*J (8 B) written per point; outputs (4 GB) far larger than L2."""
+    import torch
+    D = cfg["dims"]
+    x = torch.empty((n, D), dtype=torch.float64, device=dev)
+    w = torch.empty(n, dtype=torch.float64, device=dev)
+    for r in range(3):
+        ctx.vegas_generate(n, seed=cfg["seed"], counter=r * n, out=(x, w))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for r in range(reps):
+        ctx.vegas_generate(n, seed=cfg["seed"], counter=(3 + r) * n, out=(x, w))
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / reps
+    hbm = measured_peaks().get("hbm_gbs")
+    b = 8 * (D + 1)
+    achieved = b * n / (ms / 1e3) / 1e9
+    mean = float(w.mean().item())
+    del x, w
+    return {"points_per_s": n / (ms / 1e3), "points_per_launch": n, "ms_per_launch": ms,
+            "mean_weight": mean,
+            "roofline": {"kernel": "k_vegas_generate", "bound": "hbm", "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": achieved / hbm if hbm else None,
+                         "algorithmic_bytes_per_point": b,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured copy bandwidth)",
+                         "traffic": VEGAS_GEN_TRAFFIC}}
+
+
+# DRAM bytes (read + write) per point of k_vegas_generate from the committed
+# ncu capture (profiles/vegas_camel_kernels.md), or None
+VEGAS_GEN_TRAFFIC = None
+
+
+def vegas_time_to_target(ctx, cfg, params, seed, dev, target=1e-3, max_iter=4000):
+    """Wall time of Vegas iterations from a uniform grid until the pooled
+    relative error is at most `target` (each iteration's StatsData read back
+    to decide, as Vegas::Optimize does, Vegas.cc:56-61)."""
+    import torch
+
+    from chili_b200 import gpu
+    ctx.uniform_grids(1, cfg["dims"], cfg["bins"])
+    torch.cuda.synchronize(dev)
+    pooled = np.zeros(6)
+    t0 = time.perf_counter()
+    it = 0
+    rel = float("inf")
+    while it < max_iter:
+        st = ctx.vegas_iterate(cfg["ncalls"], seed=seed, counter=it * cfg["ncalls"], alpha=cfg["alpha"])
+        pooled += np.array(st.as_tuple()) * np.array([1, 0, 0, 1, 1, 1])
+        it += 1
+        m, e = gpu.stats_mean_error(pooled)
+        rel = e / abs(m)
+        if rel <= target:
+            break
+    dt = time.perf_counter() - t0
+    return {"seconds": dt if rel <= target else None, "iterations": it, "points": it * cfg["ncalls"],
+            "rel_error": rel, "integral": float(gpu.stats_mean_error(pooled)[0]),
+            "path": "chili_gpu_vegas_iterate per iteration with host StatsData, wall clock"}
+
+
+def vegas_e2e(ctx, cfg, args, dev, rank):
+    """The iteration through the C ABI with HOST buffers: the step's uniforms
+    from pinned host memory (copied inside the call) and StatsData back."""
+    import torch
+
+    from chili_b200 import workloads
+    n, D = cfg["ncalls"], cfg["dims"]
+    rng = np.random.default_rng(4321 + rank)
+    bufs = []
+    for _ in range(2):
+        t = torch.empty((n, D), dtype=torch.float64, pin_memory=True)
+        t.numpy()[:] = workloads.uniforms53(rng, (n, D))
+        bufs.append(t.numpy())
+    ctx.vegas_iterate(n, u=bufs[0], alpha=cfg["alpha"])
+    torch.cuda.synchronize(dev)
+    steps = max(5, args.steps)
+    t0 = time.perf_counter()
+    for s in range(steps):
+        ctx.vegas_iterate(n, u=bufs[s % 2], alpha=cfg["alpha"])
+    dt = time.perf_counter() - t0
+    return {"value": n * steps / dt, "unit": VEGAS_UNIT, "h2d_bytes_per_step": n * D * 8,
+            "d2h_bytes_per_step": 48, "steps": steps, "ms_per_step": dt / steps * 1e3,
+            "path": "chili_gpu_vegas_iterate with host uniforms (pinned) and host StatsData, wall clock"}
+
+
+def _vegas_ref_run(cfg, warmup, steps, target=None, max_iter=4000):
+    from chili_b200.gpu import stats_mean_error
+    from oracle.mpi_ranks import RefVegasMPI
+    with RefVegasMPI(cpu_cores(), dims=cfg["dims"], bins=cfg["bins"], alpha=cfg["alpha"], ncalls=cfg["ncalls"],
+                     seed=cfg["seed"]) as M:
+        for _ in range(warmup):
+            M.iterate()
+        secs, pooled = 0.0, np.zeros(6)
+        for _ in range(steps):
+            st, sec = M.iterate()
+            secs += sec
+            pooled += np.array(st) * np.array([1, 0, 0, 1, 1, 1])
+        t01 = None
+        if target:
+            M.edges = np.tile(np.arange(cfg["bins"] + 1, dtype=np.float64) / cfg["bins"], (cfg["dims"], 1))
+            acc, tot, it = np.zeros(6), 0.0, 0
+            while it < max_iter:
+                st, sec = M.iterate()
+                tot += sec
+                it += 1
+                acc += np.array(st) * np.array([1, 0, 0, 1, 1, 1])
+                m, e = stats_mean_error(acc)
+                if e / abs(m) <= target:
+                    t01 = {"seconds": tot, "iterations": it, "points": it * M.ncalls_rank * M.nranks,
+                           "rel_error": e / abs(m), "integral": m}
+                    break
+    return secs, pooled, M
+
+
+def cpu_baseline_vegas(cfg, steps=20):
+    from oracle import ref
+    if not ref.available():
+        return {"value": None, "unavailable": "oracle/_ref not built"}
+    secs, pooled, M = _vegas_ref_run(cfg, 1, steps)
+    pts = M.ncalls_rank * M.nranks * steps
+    return {"value": pts / secs, "unit": VEGAS_UNIT, "cores": M.nranks, "kind": "reference",
+            "sample": f"{steps} Vegas iterations of {M.ncalls_rank * M.nranks} points in the reference's MPI mode "
+                      f"({M.nranks} processes of {M.ncalls_rank}), after one warm-up; time = the slowest rank "
+                      f"plus the adaptation"}
+
+
+def run_reference_vegas(args, rank, world):
+    if rank != 0:
+        return
+    from oracle import ref
+    from chili_b200 import workloads
+    from chili_b200.gpu import stats_mean_error
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libchili_ref.so not built"}))
+        return
+    cfg = dict(workloads.VEGAS_CAMEL)
+    if args.ncalls:
+        cfg["ncalls"] = args.ncalls
+    from oracle.mpi_ranks import RefVegasMPI
+    with RefVegasMPI(cpu_cores(), dims=cfg["dims"], bins=cfg["bins"], alpha=cfg["alpha"], ncalls=cfg["ncalls"],
+                     seed=cfg["seed"]) as M:
+        for _ in range(args.warmup):
+            M.iterate()
+        secs, pooled = 0.0, np.zeros(6)
+        for _ in range(args.steps):
+            st, sec = M.iterate()
+            secs += sec
+            pooled += np.array(st) * np.array([1, 0, 0, 1, 1, 1])
+        # time to 0.1% pooled error from a uniform grid
+        M.edges = np.tile(np.arange(cfg["bins"] + 1, dtype=np.float64) / cfg["bins"], (cfg["dims"], 1))
+        acc, tot, it, t01 = np.zeros(6), 0.0, 0, None
+        while it < 4000:
+            st, sec = M.iterate()
+            tot += sec
+            it += 1
+            acc += np.array(st) * np.array([1, 0, 0, 1, 1, 1])
+            m_, e_ = stats_mean_error(acc)
+            if e_ / abs(m_) <= 1e-3:
+                t01 = {"seconds": tot, "iterations": it, "rel_error": e_ / abs(m_), "integral": m_}
+                break
+    pts = M.ncalls_rank * M.nranks
+    mean, err = stats_mean_error(pooled)
+    value = pts * args.steps / secs
+    cfg["ncalls"] = pts
+    line = {
+        "impl": "reference", "metric": VEGAS_METRIC, "value": value, "unit": VEGAS_UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (host uniforms)", "config": vegas_config(cfg),
+        "parallelism": f"the reference's MPI mode over {M.nranks} host processes",
+        "integral": mean, "rel_error": err / abs(mean), "time_to_0p1pct": t01,
+        "cpu_baseline": {"value": value, "unit": VEGAS_UNIT, "cores": M.nranks, "kind": "reference",
+                         "sample": f"each step: one Vegas iteration of {pts} points in the reference's MPI mode "
+                                   f"({M.nranks} processes of {M.ncalls_rank}), time = the slowest rank plus the "
+                                   f"adaptation"},
+        "e2e": {"value": value, "unit": VEGAS_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
@@ -967,7 +1262,7 @@ def main():
     args = parse()
     if args.workload in WORKLOADS:
         WL = WORKLOADS[args.workload]
-    if args.ncalls is None:
+    if args.ncalls is None and args.workload in WORKLOADS:
         args.ncalls = WL["ncalls"]
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -975,6 +1270,8 @@ def main():
     if args.impl == "reference":
         if args.workload == "batched":
             run_reference_batched(args, rank, world)
+        elif args.workload == "vegas":
+            run_reference_vegas(args, rank, world)
         else:
             run_reference(args, rank, world)
         return
@@ -987,6 +1284,8 @@ def main():
     try:
         if args.workload == "batched":
             run_batched(args, rank, world, local_rank)
+        elif args.workload == "vegas":
+            run_vegas(args, rank, world, local_rank)
         else:
             run_chili(args, rank, world, local_rank)
     finally:

@@ -645,6 +645,44 @@ int chili_gpu_vegas_iterate(chili_ctx *ctx, uint64_t ncalls, uint64_t seed, uint
     return sync_if_host(ctx, {&au, &ast, &atr});
 }
 
+int chili_gpu_vegas_generate(chili_ctx *ctx, uint64_t n, uint64_t seed, uint64_t counter_base, double *x_out,
+                             double *w_out) {
+    if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
+    int rc;
+    if ((rc = need_grids(ctx))) return rc;
+    if (!ctx->f_set || ctx->f_host.kind != CHILI_FUNC_CAMEL)
+        return fail(ctx, CHILI_ERR_STATE, "plain VEGAS needs the camel integrand");
+    if (ctx->f_host.nparams < 2 + 2 * ctx->dims)
+        return fail(ctx, CHILI_ERR_INVALID_ARG, "camel needs 2 + 2*dims parameters");
+    if (!x_out || !w_out) return fail(ctx, CHILI_ERR_INVALID_ARG, "x_out and w_out are required");
+    if (n == 0) return CHILI_OK;
+    if (n > (1ull << 40)) return fail(ctx, CHILI_ERR_LIMIT, "n must be at most 2^40");
+    const int D = ctx->dims, B = ctx->bins;
+    const size_t smem = sizeof(double) * ((static_cast<size_t>(D) * (B + 1) + 1) / 2 * 2 + kGenTile * (D + 1));
+    if (smem > 200 * 1024) return fail(ctx, CHILI_ERR_LIMIT, "grid too large for the shared-memory staging");
+    const long long nn = static_cast<long long>(n);
+    Arg ax, aw;
+    if ((rc = resolve(ctx, x_out, sizeof(double) * nn * D, 0, false, ax))) return rc;
+    if ((rc = resolve(ctx, w_out, sizeof(double) * nn, 1, false, aw))) return rc;
+    if (smem > 48 * 1024)
+        CK(cudaFuncSetAttribute(k_vegas_generate, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem)));
+    int sms = 148, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_vegas_generate, kGenTile, smem));
+    const long long tiles = (nn + kGenTile - 1) / kGenTile;
+    const long long nblocks = std::min<long long>(tiles, static_cast<long long>(sms) * std::max(per_sm, 1));
+    {
+        KTimer kt_(ctx, KT_VEGAS_GEN);
+        k_vegas_generate<<<static_cast<unsigned>(nblocks), kGenTile, smem, ctx->stream>>>(
+            ctx->edges.as<double>(), D, B, seed, counter_base, nn, ctx->f_dev.as<IntegrandDesc>(),
+            static_cast<double *>(ax.dev), static_cast<double *>(aw.dev));
+    }
+    LAUNCHED();
+    if ((rc = finish_out(ctx, ax)) || (rc = finish_out(ctx, aw))) return rc;
+    return sync_if_host(ctx, {&ax, &aw});
+}
+
 // ------------------------------------------------------------------ channels
 int chili_gpu_set_channels(chili_ctx *ctx, const chili_channel_desc *descs, int nch, const chili_cuts *cuts,
                            double sqrts, int n_ext) {
@@ -736,23 +774,34 @@ int chili_gpu_fsmapper_generate(chili_ctx *ctx, int ch, const double *x, double 
     return sync_if_host(ctx, {&ax, &am});
 }
 
-int chili_gpu_fsmapper_weight(chili_ctx *ctx, int ch, const double *mom, double *x_out, double *w, int64_t n) {
+namespace {
+int fsmapper_weight(chili_ctx *ctx, int ch, const double *mom, double *x, double *w, int64_t n, bool x_in) {
     if (!ctx) return fail(nullptr, CHILI_ERR_INVALID_ARG, "ctx is NULL");
     int rc;
     if ((rc = need_channels(ctx))) return rc;
-    if (ch < 0 || ch >= ctx->nch || !mom || !w || n < 0) return fail(ctx, CHILI_ERR_INVALID_ARG, "bad argument");
+    if (ch < 0 || ch >= ctx->nch || !mom || !w || n < 0 || (x_in && !x))
+        return fail(ctx, CHILI_ERR_INVALID_ARG, "bad argument");
     if (n == 0) return CHILI_OK;
     Arg am, ax, aw;
     if ((rc = resolve(ctx, mom, sizeof(double) * n * ctx->n_ext * 4, 0, true, am))) return rc;
-    if ((rc = resolve(ctx, x_out, sizeof(double) * n * ctx->ndims, 1, false, ax))) return rc;
+    if ((rc = resolve(ctx, x, sizeof(double) * n * ctx->ndims, 1, x_in, ax))) return rc;
     if ((rc = resolve(ctx, w, sizeof(double) * n, 2, false, aw))) return rc;
     k_fs_weight<<<grid_for(n, 128), 128, 0, ctx->stream>>>(ctx->progs.as<ChannelProgram>() + ch,
                                                            static_cast<const double *>(am.dev),
                                                            static_cast<double *>(ax.dev),
-                                                           static_cast<double *>(aw.dev), n);
+                                                           static_cast<double *>(aw.dev), n, x_in ? 1 : 0);
     LAUNCHED();
     if ((rc = finish_out(ctx, ax)) || (rc = finish_out(ctx, aw))) return rc;
     return sync_if_host(ctx, {&am, &ax, &aw});
+}
+}  // namespace
+
+int chili_gpu_fsmapper_weight(chili_ctx *ctx, int ch, const double *mom, double *x_out, double *w, int64_t n) {
+    return fsmapper_weight(ctx, ch, mom, x_out, w, n, false);
+}
+
+int chili_gpu_fsmapper_weight_inout(chili_ctx *ctx, int ch, const double *mom, double *x, double *w, int64_t n) {
+    return fsmapper_weight(ctx, ch, mom, x, w, n, true);
 }
 
 // -------------------------------------------------------------- multichannel
@@ -895,9 +944,12 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         const long long S = u_host ? std::min(m, kUploadSlice) : m;  // rows of the largest round
         const long long n_rounds = u_host ? slice_count(m) : 1;
         if (u_host) {
-            if ((rc = upload_host(ctx, u + tried * (D + 1), m))) return rc;
+            // the gate is set before upload_host records the event the
+            // slice copies (and so every forward launch of the chunk, on
+            // the forward stream) wait on
             k_iter_init<<<1, 1, 0, ctx->stream>>>(iter, needed);
             LAUNCHED();
+            if ((rc = upload_host(ctx, u + tried * (D + 1), m))) return rc;
         }
         // buffers for a whole number of 2^16 points (the chunk size follows
         // the acceptance rate and would otherwise reallocate, synchronising
@@ -1107,8 +1159,8 @@ int chili_gpu_multichannel_train(chili_ctx *ctx, const chili_multichannel_params
                                               acc_train_ptr(ctx), nch, params->beta, params->min_alpha, 1);
     LAUNCHED();
     if ((rc = adapt_grids(ctx, 0, nch, params->grid_alpha, ctx->hist.as<double>(), 1))) return rc;
-    CK(cudaStreamSynchronize(ctx->stream));
-    return CHILI_OK;
+    // host inputs were staged: their buffers are free once the copies ran
+    return sync_if_host(ctx, {&ah, &aa});
 }
 
 int chili_gpu_get_training(chili_ctx *ctx, double *hist, double *alpha_train) {
@@ -1127,6 +1179,44 @@ int chili_gpu_get_training(chili_ctx *ctx, double *hist, double *alpha_train) {
     if ((rc = finish_out(ctx, ah)) || (rc = finish_out(ctx, aa))) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     return CHILI_OK;
+}
+
+namespace {
+// [hist | atrain | n, sum, sum2, n_finite | max, -min] of the last iteration
+__global__ void k_pack_training(const double *__restrict__ hist, long long hist_n, const IterAcc *__restrict__ acc,
+                                int nch, double *__restrict__ buf) {
+    const long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (t < hist_n) buf[t] = hist[t];
+    if (t < nch) buf[hist_n + t] = acc->atrain[t];
+    if (t == 0) {
+        double *s = buf + hist_n + nch;
+        s[0] = acc->st[0];
+        s[1] = acc->st[3];
+        s[2] = acc->st[4];
+        s[3] = acc->st[5];
+        s[4] = acc->st[2];
+        s[5] = -acc->st[1];
+    }
+}
+}  // namespace
+
+int chili_gpu_pack_training(chili_ctx *ctx, double *buf, int64_t len) {
+    if (!ctx || !buf) return fail(ctx, CHILI_ERR_INVALID_ARG, "NULL argument");
+    int rc;
+    if ((rc = need_mc(ctx))) return rc;
+    if (!ctx->hist.p || !ctx->acc.p) return fail(ctx, CHILI_ERR_STATE, "no iteration has run");
+    const long long hist_n = static_cast<long long>(ctx->nch) * ctx->ndims * ctx->bins;
+    const long long need = hist_n + ctx->nch + 6;
+    if (len < need) return fail(ctx, CHILI_ERR_INVALID_ARG, "buffer shorter than nch*dims*bins + nch + 6");
+    Arg ab;
+    if ((rc = resolve(ctx, buf, sizeof(double) * need, 0, false, ab))) return rc;
+    const long long nt = std::max<long long>(hist_n, ctx->nch);
+    k_pack_training<<<grid_for(nt, 256), 256, 0, ctx->stream>>>(ctx->hist.as<double>(), hist_n,
+                                                                ctx->acc.as<IterAcc>(), ctx->nch,
+                                                                static_cast<double *>(ab.dev));
+    LAUNCHED();
+    if ((rc = finish_out(ctx, ab))) return rc;
+    return sync_if_host(ctx, {&ab});
 }
 
 int chili_gpu_generate(chili_ctx *ctx, int64_t n, uint64_t seed, uint64_t counter_base, double *mom, double *wgt,
@@ -1334,6 +1424,13 @@ cudaError_t noalloc_scratch(int dev, double **out) {
     return cudaSuccess;
 }
 
+// Writes the integrand descriptor into the scratch array.  The descriptor
+// travels as a kernel argument (copied at launch), so no host memory is
+// read after the call returns.
+__global__ void k_noalloc_store_desc(IntegrandDesc *dst, const IntegrandDesc src) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *dst = src;
+}
+
 bool on_device(const void *p, int dev) {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -1371,9 +1468,8 @@ extern "C" int chili_gpu_vegas_iterate_noalloc(void *stream, const double *edges
     for (int i = 0; i < nparams; ++i) desc.p[i] = camel_params[i];
     IntegrandDesc *desc_dev = reinterpret_cast<IntegrandDesc *>(scratch);
     double *part = scratch + kNoAllocDescDoubles;
-    // the descriptor comes from pageable host memory: the copy has left it
-    // when cudaMemcpyAsync returns
-    CK(cudaMemcpyAsync(desc_dev, &desc, sizeof(IntegrandDesc), cudaMemcpyHostToDevice, st));
+    k_noalloc_store_desc<<<1, 1, 0, st>>>(desc_dev, desc);
+    CK(cudaGetLastError());
     const int nh = dims * bins;
     CK(cudaMemsetAsync(train_out, 0, sizeof(double) * nh, st));  // the histogram starts at zero
     int sms = 148;

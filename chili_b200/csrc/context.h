@@ -166,8 +166,8 @@ struct chili_ctx {
     };
     std::vector<Pending> pending;
     std::vector<cudaEvent_t> event_pool;
-    double ktime_ms[16] = {0};
-    unsigned long long klaunches[16] = {0};
+    double ktime_ms[32] = {0};
+    unsigned long long klaunches[32] = {0};
     // channel descriptions as given (checkpoint.cu writes them back) and the
     // FSMapper ptmin list of every channel (Channel.hh:20-26)
     std::vector<std::vector<chili_particle_info>> ch_info;
@@ -187,9 +187,9 @@ namespace {
 const char *const kTimedKernels[] = {"k_mc_forward", "k_pp_nodes", "k_pp_items", "k_pp_chains", "k_pp_channel",
                                      "k_pp_combine", "k_mc_weight", "k_mc_accum", "k_vegas_iter", "k_flow_layer",
                                      "k_flow_layer_bwd", "k_flow_wgrad", "k_alpha_train", "k_flow_phys",
-                                     "k_flow_batch", nullptr};
+                                     "k_flow_batch", "k_vegas_generate", nullptr};
 enum { KT_FORWARD, KT_NODES, KT_ITEMS, KT_CHAINS, KT_CHANNEL, KT_COMBINE, KT_WEIGHT, KT_ACCUM, KT_VEGAS,
-       KT_FLOW_LAYER, KT_FLOW_BWD, KT_FLOW_WGRAD, KT_ALPHA_TRAIN, KT_FLOW_PHYS, KT_FLOW_BATCH };
+       KT_FLOW_LAYER, KT_FLOW_BWD, KT_FLOW_WGRAD, KT_ALPHA_TRAIN, KT_FLOW_PHYS, KT_FLOW_BATCH, KT_VEGAS_GEN };
 
 cudaEvent_t take_event(chili_ctx *ctx) {
     if (!ctx->event_pool.empty()) {

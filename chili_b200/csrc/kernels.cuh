@@ -201,6 +201,72 @@ __global__ void k_vegas_iter(const double *__restrict__ g, int dims, int bins, u
     }
 }
 
+// Materialised VEGAS points on the camel: point i's uniforms (the counter
+// stream of k_vegas_iter, ctr0 + i) through the grid, x_out[i][dims] and the
+// point's weight f(x) J(u) to w_out[i].  The grid (dims x (bins+1) edges) is
+// staged in shared memory; a block's points are assembled in shared memory
+// and leave as contiguous 16-byte stores, so the only HBM traffic is the
+// 8 (dims + 1) bytes written per point.  Persistent grid-stride over tiles
+// of kGenTile points.
+constexpr int kGenTile = 256;
+__global__ void __launch_bounds__(kGenTile) k_vegas_generate(const double *__restrict__ g, int dims, int bins,
+                                                             uint64_t seed, uint64_t ctr0, long long n,
+                                                             const IntegrandDesc *__restrict__ f,
+                                                             double *__restrict__ x_out, double *__restrict__ w_out) {
+    extern __shared__ __align__(16) double gsh[];
+    const int ne = dims * (bins + 1);
+    double *xt = gsh + ((ne + 1) & ~1);  // kGenTile * dims x values, 16-byte aligned
+    double *wt = xt + kGenTile * dims;   // kGenTile weights
+    for (int k = threadIdx.x; k < ne; k += blockDim.x) gsh[k] = g[k];
+    __syncthreads();
+    const double fb = static_cast<double>(bins);
+    const long long ntiles = (n + kGenTile - 1) / kGenTile;
+    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const long long i0 = t * kGenTile, i = i0 + threadIdx.x;
+        const int cnt = static_cast<int>(n - i0 < kGenTile ? n - i0 : kGenTile);
+        if (i < n) {
+            double r[CHILI_MAX_DIMS];
+            load_uniforms(seed, ctr0 + i, nullptr, dims, r);
+            // AdaptiveMap::operator() (AdaptiveMap.cc:40-56) on the staged
+            // edges, rounded as grid_map_checked
+            double jac = 1.0;
+            bool ok = true;
+            for (int d = 0; d < dims; ++d) {
+                const double pos = __dmul_rn(r[d], fb);
+                if (!(pos >= 0.0 && pos < fb)) {
+                    ok = false;
+                    break;
+                }
+                const int idx = static_cast<int>(pos);
+                const double loc = __dsub_rn(pos, static_cast<double>(idx));
+                const double *e = gsh + d * (bins + 1);
+                const double left = e[idx];
+                const double size = __dsub_rn(e[idx + 1], left);
+                r[d] = __dadd_rn(left, __dmul_rn(loc, size));
+                jac = __dmul_rn(jac, __dmul_rn(size, fb));
+            }
+            const double w = ok ? camel(f, r, dims) * jac : CUDART_NAN;
+            for (int d = 0; d < dims; ++d) xt[threadIdx.x * dims + d] = ok ? r[d] : CUDART_NAN;
+            wt[threadIdx.x] = w;
+        }
+        __syncthreads();
+        // the tile's rows are contiguous in x_out: cnt * dims doubles from
+        // i0 * dims, written as double2 where both ends allow it
+        double *xo = x_out + i0 * dims;
+        const int nx = cnt * dims;
+        const bool vec = ((reinterpret_cast<uintptr_t>(xo) & 15) == 0) && ((nx & 1) == 0);
+        if (vec) {
+            const double2 *src = reinterpret_cast<const double2 *>(xt);
+            double2 *dst = reinterpret_cast<double2 *>(xo);
+            for (int k = threadIdx.x; k < (nx >> 1); k += blockDim.x) dst[k] = src[k];
+        } else {
+            for (int k = threadIdx.x; k < nx; k += blockDim.x) xo[k] = xt[k];
+        }
+        if (threadIdx.x < cnt) w_out[i0 + threadIdx.x] = wt[threadIdx.x];
+        __syncthreads();
+    }
+}
+
 // Ordered fold of k_vegas_iter's partials: stats into out6, histogram
 // partials (when per block) into train[dims*bins].
 __global__ void k_vegas_finalize(const double *__restrict__ part, int nblocks, const double *__restrict__ hist_part,
@@ -250,8 +316,11 @@ __global__ void k_fs_generate(const ChannelProgram *__restrict__ prog, const dou
     }
 }
 
+// x_out is also read first when x_in != 0: the uniform buffer then starts
+// from the caller's contents (FSMapper::GenerateWeight writes only the
+// entries its chain consumes, Channel.cc:40-61), else from zeros.
 __global__ void k_fs_weight(const ChannelProgram *__restrict__ prog, const double *__restrict__ mom,
-                            double *__restrict__ x_out, double *__restrict__ w, long long n) {
+                            double *x_out, double *__restrict__ w, long long n, int x_in) {
     const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
     if (i >= n) return;
     const int nd = prog->ndims, ne = prog->n_ext;
@@ -261,7 +330,7 @@ __global__ void k_fs_weight(const ChannelProgram *__restrict__ prog, const doubl
         m[k] = V4{q[0], q[1], q[2], q[3]};
     }
     double r[CHILI_MAX_DIMS];
-    for (int d = 0; d < nd; ++d) r[d] = 0.0;  // the reference's rans start zeroed
+    for (int d = 0; d < nd; ++d) r[d] = x_in ? x_out[i * nd + d] : 0.0;
     const double wt = fs_weight(prog, m, r);
     w[i] = wt;
     if (x_out)

@@ -47,6 +47,9 @@ def _declare(lib):
         "chili_gpu_set_preprocess_cuts": ([vp, dbl, dbl, dbl, dbl], i32),
         "chili_gpu_vegas_iterate": ([vp, u64, u64, u64, vp, dbl, i32, vp, vp], i32),
         "chili_gpu_vegas_iterate_noalloc": ([vp, vp, i32, i32, vp, i32, u64, u64, u64, vp, vp], i32),
+        "chili_gpu_vegas_generate": ([vp, u64, u64, u64, vp, vp], i32),
+        "chili_gpu_fsmapper_weight_inout": ([vp, i32, vp, vp, vp, i64], i32),
+        "chili_gpu_pack_training": ([vp, vp, i64], i32),
         "chili_gpu_set_channels": ([vp, P(abi.ChannelDesc), i32, P(abi.Cuts), dbl, i32], i32),
         "chili_gpu_ndims": ([vp], i32),
         "chili_gpu_check_channels": ([P(abi.ChannelDesc), i32, P(abi.Cuts), dbl, i32, C.c_char_p,
@@ -245,6 +248,15 @@ class Context:
                   float(alpha), 1 if adapt else 0, C.byref(st), _ptr(tr))
         return (st, tr) if train else st
 
+    def vegas_generate(self, n, seed=42, counter=0, out=None):
+        """n materialised VEGAS points of grid 0 on the camel: (x[n, dims],
+        w[n]).  out = (x, w) may be given (numpy or CUDA tensors)."""
+        if out is None:
+            out = (np.empty((n, self.dims)), np.empty(n))
+        x, w = out
+        self.call("chili_gpu_vegas_generate", int(n), int(seed), int(counter), _ptr(x), _ptr(w))
+        return x, w
+
     # -------------------------------------------------------------- channels
     def set_channels(self, cs):
         self._keep.append(cs)
@@ -304,6 +316,15 @@ class Context:
         a = np.empty(self.nch)
         self.call("chili_gpu_get_training", _ptr(h), _ptr(a))
         return h, a
+
+    def packed_training_len(self):
+        return self.nch * self.ndims * self.bins + self.nch + 6
+
+    def pack_training(self, buf):
+        """[hist | alpha_train | n, sum, sum2, n_finite | max, -min] of the last
+        iteration into buf (a CUDA tensor stays on the device)."""
+        self.call("chili_gpu_pack_training", _ptr(buf), int(buf.shape[0]))
+        return buf
 
     def multichannel_train(self, params, hist, alpha_train):
         """Train from given (e.g. all-reduced) training data."""

@@ -39,9 +39,24 @@ def synced_iteration(integrator, params, group=None, device=None):
     """One iteration of the MPI mode on this rank: local points, one
     all-reduce of the training data and StatsData, identical training on
     every rank. Returns the merged StatsData tuple (n, min, max, sum, sum2,
-    n_finite) and this rank's iteration record."""
+    n_finite) and this rank's iteration record.
+
+    A rank that packs its training data on the device (GpuRank with a CUDA
+    device) exchanges it in place: the library writes the packed buffer on
+    the device, the all-reduce runs on it (NCCL over NVLink), and the
+    library trains from device pointers into the summed buffer; only the six
+    merged StatsData values come back to the host."""
     import torch
     import torch.distributed as dist
+    if device is not None and torch.device(device).type == "cuda" and hasattr(integrator, "pack_training"):
+        st, info = integrator.run(params)
+        buf = integrator.pack_training(device)
+        nh = buf.shape[0] - 6 - integrator.nch
+        dist.all_reduce(buf[:-2], group=group)
+        dist.all_reduce(buf[-2:], op=dist.ReduceOp.MAX, group=group)
+        integrator.train(params, buf[:nh], buf[nh:nh + integrator.nch])
+        s = buf[-6:].cpu().numpy()
+        return (s[0], -float(s[5]), float(s[4]), s[1], s[2], s[3]), info
     st, info = integrator.run(params)
     hist, atrain = integrator.training()
     hist = np.asarray(hist, dtype=np.float64)
@@ -60,10 +75,15 @@ def synced_iteration(integrator, params, group=None, device=None):
 
 
 class GpuRank:
-    """A chili_b200 context as one rank (its own seed or counter range)."""
+    """A chili_b200 context as one rank (its own seed or counter range).
+    shared_stream: the context runs on torch's current stream (set with
+    Context.set_stream), so the collectives and the library's kernels are
+    ordered by the stream alone; otherwise the two streams are synchronised
+    around the collective."""
 
-    def __init__(self, ctx, seed, counter):
+    def __init__(self, ctx, seed, counter, shared_stream=False):
         self.ctx, self.seed, self.counter = ctx, seed, counter
+        self.shared_stream = shared_stream
         ctx.set_option("defer_train", 1)
 
     def run(self, params):
@@ -71,8 +91,26 @@ class GpuRank:
         self.counter += info.points_tried
         return st.as_tuple(), info
 
+    @property
+    def nch(self):
+        return self.ctx.nch
+
     def training(self):
         return self.ctx.get_training()
 
+    def pack_training(self, device):
+        """The packed training buffer in device memory (chili_gpu_pack_training)."""
+        import torch
+        buf = torch.empty(self.ctx.packed_training_len(), dtype=torch.float64, device=device)
+        if not self.shared_stream:
+            torch.cuda.current_stream(device).synchronize()  # buf's allocation, on torch's stream
+        self.ctx.pack_training(buf)
+        if not self.shared_stream:
+            self.ctx.synchronize()
+        return buf
+
     def train(self, params, hist, atrain):
+        if not self.shared_stream and hasattr(hist, "device") and hist.device.type == "cuda":
+            import torch
+            torch.cuda.current_stream(hist.device).synchronize()  # the collective's result
         self.ctx.multichannel_train(params, hist, atrain)

@@ -129,10 +129,22 @@ class Vegas {
                                       static_cast<int>(camel_params.size())),
               ctx_.get());
     }
+    // Uniforms from the caller instead of the device generator: before each
+    // iteration source(n, out) writes the next n = ncalls * dims uniforms to
+    // out, point after point (the order Vegas::operator() draws them from
+    // Random::Generate, Vegas.cc:32), for instance a replay of a reference
+    // run's stream.  An empty function restores the device generator.
+    void SetUniformSource(std::function<void(size_t, double *)> source) { source_ = std::move(source); }
     // Vegas::operator() (Vegas.cc:18-52): one iteration, then Adapt.
     void operator()() {
         chili_stats st;
-        check(chili_gpu_vegas_iterate(ctx_.get(), params_.ncalls, seed_, counter_, nullptr, params_.alpha, 1, &st,
+        const double *u = nullptr;
+        if (source_) {
+            uniforms_.resize(params_.ncalls * grid_.Dims());
+            source_(uniforms_.size(), uniforms_.data());
+            u = uniforms_.data();
+        }
+        check(chili_gpu_vegas_iterate(ctx_.get(), params_.ncalls, seed_, counter_, u, params_.alpha, 1, &st,
                                       nullptr),
               ctx_.get());
         counter_ += params_.ncalls;
@@ -154,12 +166,15 @@ class Vegas {
             }
         }
     }
-    // Vegas::Refine (Vegas.cc:79-82).
+    // Vegas::Refine (Vegas.cc:79-82): the device grid split in two
+    // (AdaptiveMap::Split), ncalls doubled.  The host copy only takes the
+    // new shape here; Grid() fills it from the device.
     void Refine() {
         check(chili_gpu_grid_split(ctx_.get(), 2), ctx_.get());
         params_.ncalls *= 2;
         grid_ = AdaptiveMap(grid_.Dims(), grid_.Bins() * 2);
     }
+    const VegasParams &Params() const { return params_; }
     // Vegas::Grid (Vegas.hh:67-68): the device grid copied back.
     const AdaptiveMap &Grid() {
         check(chili_gpu_get_grids(ctx_.get(), grid_.Hist().data(), 1, static_cast<int>(grid_.Dims()),
@@ -182,6 +197,8 @@ class Vegas {
     VegasParams params_;
     uint64_t seed_, counter_ = 0;
     VegasSummary summary_;
+    std::function<void(size_t, double *)> source_;
+    std::vector<double> uniforms_;
 };
 
 // ParticleInfo / ChannelDescription (ChannelNode.hh:26-51) and Cuts

@@ -254,6 +254,17 @@ int chili_gpu_vegas_iterate(chili_ctx *ctx, uint64_t ncalls, uint64_t seed,
                             double alpha, int adapt, chili_stats *stats_out,
                             double *train_out);
 
+/* Materialised VEGAS points (the events of a Vegas integration of the camel,
+ * Vegas.cc:29-36 without the accumulation): point i takes the uniforms of
+ * counter counter_base + i (the stream chili_gpu_vegas_iterate draws), maps
+ * them through grid 0 (AdaptiveMap::operator(), AdaptiveMap.cc:40-56) and
+ * writes x_out[i*dims + d] and its weight w_out[i] = f(x) J (NaN where a
+ * uniform lies outside [0, 1)).  Host or device buffers.  The grid must fit
+ * the kernel's shared-memory staging (8 dims (bins+1) + 8 * 256 (dims+1)
+ * bytes <= 200 KB, else CHILI_ERR_LIMIT). */
+int chili_gpu_vegas_generate(chili_ctx *ctx, uint64_t n, uint64_t seed, uint64_t counter_base, double *x_out,
+                             double *w_out);
+
 /* Plain VEGAS without any device allocation.  This entry point has no
  * counterpart in the reference.  It is for callers that cannot call
  * cudaMalloc: code running inside another framework whose device memory that
@@ -338,6 +349,12 @@ int chili_gpu_fsmapper_generate(chili_ctx *ctx, int ch, const double *x,
  * (optional), w[n].  Host or device. */
 int chili_gpu_fsmapper_weight(chili_ctx *ctx, int ch, const double *mom,
                               double *x_out, double *w, int64_t n);
+/* FSMapper::GenerateWeight with the reference's in/out uniform buffer
+ * (Channel.cc:40-61, the rans argument): x[n*ndims] is read first and only
+ * the entries the channel's inverse map consumes are overwritten, as the
+ * reference leaves the rest of its buffer (a t-chain that fails leaves its
+ * last entry alone).  Host or device. */
+int chili_gpu_fsmapper_weight_inout(chili_ctx *ctx, int ch, const double *mom, double *x, double *w, int64_t n);
 
 /* -------------------------------------------------------- multichannel */
 /* Channel weights alpha (MultiChannel.cc:62-67 initialises them to 1/nch). */
@@ -388,6 +405,16 @@ int chili_gpu_get_training(chili_ctx *ctx, double *hist, double *alpha_train);
  * rank adapting identically. Host or device. */
 int chili_gpu_multichannel_train(chili_ctx *ctx, const chili_multichannel_params *params, const double *hist,
                                  const double *alpha_train);
+/* The last iteration's training data and StatsData packed for the MPI
+ * mode's exchange (MultiChannel.hh:184-190, MultiChannel.cc:69-77) in one
+ * FP64 buffer of len >= nch*dims*bins + nch + 6:
+ *   [hist (nch*dims*bins) | alpha_train (nch) | n, sum, sum2, n_finite | max, -min]
+ * The first nch*dims*bins + nch + 4 values are summed over the ranks, the
+ * last two reduced by maximum; hist and alpha_train of the sums then go to
+ * chili_gpu_multichannel_train as device pointers into the same buffer.
+ * With a device buffer the copy stays on the device in stream order (no
+ * host round trip); host buffers are filled before the call returns. */
+int chili_gpu_pack_training(chili_ctx *ctx, double *buf, int64_t len);
 
 /* MultiChannel::SaveAs / LoadFrom (MultiChannel.hh:65-84): the reference's
  * binary results.chili (Integrand::Serialize, then MultiChannel::Serialize)

@@ -76,6 +76,9 @@ def _load(path, prefix):
         "ref_mc_load": ([vp, C.c_char_p], i32),
         "ref_mc_dropped_dim0": ([vp], C.c_uint64),
         "ref_mc_run_native": ([vp, u32, i32, P(abi.Stats)], None),
+        "ref_random_uniforms": ([u32, i64, vp], None),
+        "ref_vegas_optimize": ([i32, i32, dbl, vp, i32, u32, i64, i64, dbl, dbl, i64, i32, vp, P(i64), P(i64),
+                                P(abi.Stats), vp, i64], i32),
         "ref_evaluate_batch": ([vp, i32, vp, i64, vp], None),
         "ref_philox_uniforms": ([C.c_uint64, C.c_uint64, i64, i32, vp], None),
         "ref_philox_stream_uniforms": ([C.c_uint64, C.c_uint64, i64, i32, C.c_uint32, vp], None),
@@ -152,6 +155,35 @@ def vegas_run(dims, bins, alpha, params, seed, ncalls, niter, oracle=REF):
     st = abi.Stats()
     oracle().ref_vegas_run(dims, bins, alpha, _p(p), p.size, seed, ncalls, niter, C.byref(st))
     return st
+
+
+def random_uniforms(seed, n, oracle=REF):
+    """The reference's own uniform stream (Random::Instance() seeded with
+    `seed`, n draws; the reference build only)."""
+    out = np.empty(n)
+    oracle().ref_random_uniforms(seed, n, _p(out))
+    return out
+
+
+def vegas_optimize(dims, bins, alpha, params, seed, ncalls, nrefine, atol, rtol, nitn, max_iter=256,
+                   oracle=REF):
+    """The reference's Vegas::Optimize on the camel with its own generator
+    seeded by `seed` (the reference build only).  Returns a dict: iterations
+    (StatsData tuples), bins, ncalls (after the last Refine), pooled
+    StatsData, edges [dims, bins + 1]."""
+    p = np.ascontiguousarray(params, dtype=np.float64)
+    iters = (abi.Stats * max_iter)()
+    b_out, n_out = C.c_int64(), C.c_int64()
+    pooled = abi.Stats()
+    cap = dims * (bins * 2 ** 12 + 1)
+    edges = np.empty(cap)
+    n_it = oracle().ref_vegas_optimize(dims, bins, alpha, _p(p), p.size, seed, ncalls, nrefine, atol, rtol, nitn,
+                                       max_iter, iters, C.byref(b_out), C.byref(n_out), C.byref(pooled),
+                                       _p(edges), cap)
+    B = b_out.value
+    return {"iterations": [iters[i].as_tuple() for i in range(min(n_it, max_iter))], "n_iterations": n_it,
+            "bins": B, "ncalls": n_out.value, "pooled": pooled.as_tuple(),
+            "edges": edges[:dims * (B + 1)].reshape(dims, B + 1).copy()}
 
 
 def select(alpha, v, oracle=REF):
@@ -254,7 +286,7 @@ class MultiChannel:
         assert self.oracle().ref_mc_load(self.h, str(path).encode()) == 0
 
     def set_defer(self, defer=True):
-        """Collect the training data but leave Train to train() (the C port only)."""
+        """Collect the training data but leave Train to train()."""
         self.oracle().ref_mc_set_defer(self.h, 1 if defer else 0)
 
     def set_fixed_budget(self, on=True):
@@ -263,7 +295,8 @@ class MultiChannel:
         self.oracle().ref_mc_set_fixed_budget(self.h, 1 if on else 0)
 
     def train(self, hist, atrain):
-        """Train from given training data (the C port only)."""
+        """MultiChannel::Train on given training data (the MPI mode's step
+        after the all-reduce)."""
         self.oracle().ref_mc_train(self.h, _p(np.ascontiguousarray(hist, dtype=np.float64)),
                                    _p(np.ascontiguousarray(atrain, dtype=np.float64)))
 

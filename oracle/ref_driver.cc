@@ -176,6 +176,10 @@ struct MC {
     // last-iteration training data, copied out before Train() clears it
     std::vector<double> last_hist, last_atrain;
     uint64_t dropped_dim0 = 0;
+    // the reference's MPI mode with the all-reduce done by the caller: an
+    // iteration collects its training data and leaves MultiChannel::Train
+    // to ref_mc_train, which runs it on the ranks' summed data
+    int defer = 0;
 };
 
 }  // namespace
@@ -574,10 +578,82 @@ int ref_mc_iterate(void *p, const double *u, int64_t n_u, int guard, chili_stats
         std::memcpy(h->last_hist.data() + c * ndims * h->bins, td.data(), sizeof(double) * td.size());
     }
     h->last_atrain = train_data;
-    if (h->params.should_optimize) mc.Train(func, train_data);
+    if (h->params.should_optimize && !h->defer) mc.Train(func, train_data);
     mc.UpdateResults(results);
     fill_stats(results, stats);
     return 0;
+}
+
+void ref_mc_set_defer(void *p, int defer) { static_cast<MC *>(p)->defer = defer; }
+
+// MultiChannel::Train (MultiChannel.hh:182-194) on given training data: the
+// step that follows the MPI all-reduce of the alpha-training sums and of
+// every channel's histogram (MultiChannel.hh:184-190), with the sums of all
+// ranks in place of the all-reduce.  The reference's own Train runs: Adapt,
+// Integrand::Train, MaxDifference.
+void ref_mc_train(void *p, const double *hist, const double *atrain) {
+    auto *h = static_cast<MC *>(p);
+    Quiet quiet;
+    auto &func = h->integrand;
+    const size_t nch = func.NChannels(), per = static_cast<size_t>(h->ndims) * h->bins;
+    for (size_t c = 0; c < nch; ++c) {
+        auto &td = func.GetChannel(c).train_data;
+        td.assign(hist + c * per, hist + (c + 1) * per);
+    }
+    std::vector<double> train_data(atrain, atrain + nch);
+    h->mc.Train(func, train_data);
+}
+
+// The reference's own uniform stream: Random::Instance() seeded with `seed`
+// (Random.hh:15-21), then n draws of Generate, in the order Vegas::operator()
+// consumes them (Vegas.cc:32).
+void ref_random_uniforms(unsigned seed, int64_t n, double *out) {
+    chili::Random::Instance().Seed(seed);
+    std::vector<double> v(static_cast<size_t>(n));
+    chili::Random::Instance().Generate(v);
+    std::memcpy(out, v.data(), sizeof(double) * v.size());
+}
+
+// The reference's own Vegas::Optimize (Vegas.cc:54-69) on the camel, with its
+// global generator seeded by `seed`: iterations until the pooled error meets
+// atol or rtol and at least nitn iterations ran, Refine (grid split in two,
+// ncalls doubled, Vegas.cc:79-82) every nrefine iterations.  Outputs: the
+// number of iterations, each iteration's StatsData (at most max_iter), the
+// final bins per dimension and ncalls, the pooled StatsData and the final
+// grid edges (dims * (bins_out + 1), at most max_edges values).
+int ref_vegas_optimize(int dims, int bins, double alpha, const double *params, int nparams, unsigned seed,
+                       int64_t ncalls, int64_t nrefine, double atol, double rtol, int64_t nitn, int max_iter,
+                       chili_stats *iters, int64_t *bins_out, int64_t *ncalls_out, chili_stats *pooled,
+                       double *edges_out, int64_t max_edges) {
+    Quiet quiet;
+    std::streambuf *saved = std::cout.rdbuf(nullptr);  // PrintIteration (Vegas.cc:63)
+    chili::Random::Instance().Seed(seed);
+    chili::VegasParams vp;
+    vp.ncalls = static_cast<size_t>(ncalls);
+    vp.nrefine = static_cast<size_t>(nrefine);
+    vp.atol = atol;
+    vp.rtol = rtol;
+    vp.alpha = alpha;
+    vp.ninterations = static_cast<size_t>(nitn);
+    chili::Vegas vegas(chili::AdaptiveMap(static_cast<size_t>(dims), static_cast<size_t>(bins)), vp);
+    vegas.SetVerbosity(0);
+    std::vector<double> p(params, params + nparams);
+    chili::Func<double> f = [p](const std::vector<double> &x) { return camel(x, p); };
+    vegas.Optimize(f);
+    const auto grid = vegas.Grid();
+    *bins_out = static_cast<int64_t>(grid.Bins());
+    // ncalls after the last Refine: the reference keeps it in its private
+    // params; every Refine doubles it
+    const auto summary = vegas.Summary();  // prints "Final integral" (Vegas.cc:84-90)
+    std::cout.rdbuf(saved);
+    const int n_it = static_cast<int>(summary.results.size());
+    const int64_t nref = nrefine > 0 ? n_it / nrefine : 0;
+    *ncalls_out = ncalls << nref;
+    for (int i = 0; i < n_it && i < max_iter; ++i) fill_stats(summary.results[i], iters + i);
+    fill_stats(summary.sum_results, pooled);
+    const int64_t ne = static_cast<int64_t>(grid.Dims()) * (*bins_out + 1);
+    if (ne <= max_edges) std::memcpy(edges_out, grid.Hist().data(), sizeof(double) * ne);
+    return n_it;
 }
 
 void ref_mc_get_training(void *p, double *hist, double *atrain) {

@@ -137,7 +137,10 @@ def test_loss_gradients_match_oracle(ctx_factory):
     batch["logf"][::17] = -np.inf
     loss, grad = ctx.flow_loss_grad(batch["u"], batch["ch"], batch["logf"], batch["feat"], batch["logprior"])
     Lo, go, _ = F.loss_and_grads(spec, p, batch, use_bf16=True)
-    assert abs(loss - Lo) <= 2e-3 * Lo, (loss, Lo)
+    # the oracle rounds the tensor-core operands to bf16 as the GPU does; the
+    # rest is f32 accumulation order and the spline's f32 arithmetic (seen on
+    # B200: loss within 6e-5, each parameter block within 4e-3, median 7e-4)
+    assert abs(loss - Lo) <= 2e-4 * Lo, (loss, Lo)
     g = flowspec.unflatten(grad, lay)
     worst = {}
     for k in go:
@@ -147,8 +150,9 @@ def test_loss_gradients_match_oracle(ctx_factory):
             assert np.abs(g[k]).max() < 1e-6, k
             continue
         worst[k] = np.linalg.norm(g[k] - ref) / nrm
-    bad = {k: v for k, v in worst.items() if v > 3e-2}
+    bad = {k: v for k, v in worst.items() if v > 1e-2}
     assert not bad, bad
+    assert np.median(list(worst.values())) < 2e-3, worst
 
 
 def _rel_var(st):

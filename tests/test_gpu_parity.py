@@ -109,6 +109,30 @@ def test_vegas_iteration_matches_reference(ctx_factory, rng):
     assert np.max(rel(ctx.get_grids()[0], e_r)) < 1e-11
 
 
+@pytest.mark.parametrize("dims,bins,n", [(4, 50, 200_003), (7, 100, 4_097), (1, 2, 5)])
+def test_vegas_generate_matches_reference(ctx_factory, rng, dims, bins, n):
+    """Materialised VEGAS points: the device generator's uniforms (counter
+    stream regenerated by the C port) through the reference's own
+    AdaptiveMap::operator() give x bit for bit; the weight f(x) J within
+    1e-12 (CUDA's exp against numpy's).  Sizes that are not a multiple of
+    the 256-point tile, odd row lengths and a one-bin-pair grid."""
+    from oracle import port
+    ctx = ctx_factory()
+    p = workloads.camel_params(dims)
+    edges = random_grid(rng, dims, bins)
+    ctx.set_grids(edges[None])
+    ctx.set_integrand(abi.CHILI_FUNC_CAMEL, p)
+    seed, ctr = 42, 12345
+    x, w = ctx.vegas_generate(n, seed=seed, counter=ctr)
+    u = port.philox_uniforms(seed, ctr, n, dims)
+    x_r, jac_r = ref.am_map(edges, u)
+    assert np.array_equal(x, x_r)
+    a, b = np.asarray(p[2:2 + dims]), np.asarray(p[2 + dims:2 + 2 * dims])
+    s2 = p[0] * p[0]
+    f = p[1] * (np.exp(-np.sum((x_r - a) ** 2, axis=1) / s2) + np.exp(-np.sum((x_r - b) ** 2, axis=1) / s2))
+    assert np.max(rel(w, f * jac_r)) < 1e-12
+
+
 def test_vegas_camel_converges(ctx_factory):
     ctx = ctx_factory()
     cfg = workloads.VEGAS_CAMEL
@@ -232,6 +256,12 @@ def test_multichannel_iteration_matches_reference(ctx_factory, rng, mc2, path):
         a, b, md = ctx.get_alpha()
         a_r, b_r, md_r = R.get_alpha()
         assert np.max(rel(a, a_r)) < 1e-11
+        # MaxDifference (MultiChannel.cc:138-154): the largest pairwise gap of
+        # the alpha-training sums, and the adapted weights saved whenever it
+        # is the smallest so far
+        assert np.isfinite(md) and md_r < 1.7e308, (md, md_r)
+        assert rel(md, md_r)[0] < 1e-10, (md, md_r)
+        assert np.max(rel(b, b_r)) < 1e-11, (b, b_r)
         g, g_r = ctx.get_grids(), R.get_grids()
         assert np.max(np.abs(g - g_r)) < 1e-10
         # continue both from identical state so later iterations stay comparable
