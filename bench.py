@@ -88,6 +88,8 @@ def parse():
     ap.add_argument("--gen-points", type=int, default=100_000_000,
                     help="vegas: points per launch of the materialised generation")
     ap.add_argument("--no-t01", action="store_true", help="vegas: skip the time-to-0.1%% run")
+    ap.add_argument("--no-others", action="store_true",
+                    help="multichannel: skip the compact runs of the other workloads")
     return ap.parse_args()
 
 
@@ -107,10 +109,10 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        import tempfile
+        self.path = os.path.join(tempfile.gettempdir(), f"chili_bench_clocks_{os.getpid()}_{index}.csv")
 
     def __enter__(self):
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -166,7 +168,11 @@ def run_chili(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     cs = workloads.channel_set(WL["n_out"])
     ctx = gpu.Context(local_rank)
-    stream = torch.cuda.current_stream(dev)
+    # a stream of our own, current for torch too: the library's kernels, the
+    # collectives and the timing events share it (torch's default stream is
+    # the legacy NULL stream, which does not order the library's own stream)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
     ctx.set_channels(cs)
     ctx.uniform_grids(cs.nch, ctx.ndims, WL["bins"])
@@ -275,6 +281,9 @@ def run_chili(args, rank, world, local_rank):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(args)
+    others = None
+    if world == 1 and WL is WORKLOADS["multichannel"] and not args.no_others:
+        others = compact_other_workloads(args, dev, rank)
 
     if rank == 0:
         selected = "plain"
@@ -303,9 +312,107 @@ def run_chili(args, rank, world, local_rank):
             "unweighting_quantile": unw_q,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "other_workloads": others,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
+
+
+# ------------------------------------------- the other workloads, compactly
+def compact_other_workloads(args, dev, rank):
+    """Short, time-bounded runs of the other benchmark configurations beside
+    the headline, so that one default run records them all: the plain VEGAS
+    camel (4-d, 50 bins, 1e5 points per iteration) with its materialised
+    points, the 512-integrand batch and the 2->6 / 45-channel / 200-bin
+    workload (1e7 points per iteration, plain path).  Device time by CUDA
+    events on a stream of their own."""
+    import torch
+
+    from chili_b200 import abi, channels, gpu, workloads
+    out = {}
+    stream = torch.cuda.Stream(dev)
+    prev = torch.cuda.current_stream(dev)
+    torch.cuda.set_stream(stream)
+    try:
+        # plain VEGAS
+        cfg = dict(workloads.VEGAS_CAMEL)
+        ctx = gpu.Context(dev.index)
+        ctx.set_stream(stream.cuda_stream)
+        ctx.uniform_grids(1, cfg["dims"], cfg["bins"])
+        ctx.set_integrand(abi.CHILI_FUNC_CAMEL, workloads.camel_params(cfg["dims"]))
+        sd = torch.zeros(6, dtype=torch.float64, device=dev)
+        import ctypes as C
+
+        def vstep(k):
+            ctx.call("chili_gpu_vegas_iterate", cfg["ncalls"], cfg["seed"], k * cfg["ncalls"], None,
+                     float(cfg["alpha"]), 1, C.c_void_p(sd.data_ptr()), None)
+        for k in range(5):
+            vstep(k)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in range(50):
+            vstep(5 + k)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / 50
+        mat = vegas_materialised(ctx, dev, stream, cfg, n=50_000_000, reps=5)
+        out["vegas"] = {"workload": "plain VEGAS, 4-d camel, 50 bins, alpha 1.5, 1e5 points per iteration",
+                        "ms_per_iteration": ms, "points_per_s": cfg["ncalls"] / (ms / 1e3),
+                        "materialised_points_per_s": mat["points_per_s"],
+                        "materialised_hbm_frac": mat["roofline"]["frac"],
+                        "full_line": "python bench.py --workload vegas"}
+        ctx.close()
+        # the 512 batched integrands
+        tasks = workloads.batched_tasks(seed=BATCH_SEED + rank)
+        npts = sum(t["ncalls"] for t in tasks)
+        ctx = gpu.Context(dev.index)
+        ctx.set_stream(stream.cuda_stream)
+        ctx.batch_set(tasks)
+        ctx.batch_iterate(1, seed=BATCH_SEED)
+        ctx.batch_iterate(1, seed=BATCH_SEED)
+        l0 = ctx.launches
+        bms = 0.0
+        for _ in range(3):
+            _, info = ctx.batch_iterate(1, seed=BATCH_SEED)
+            bms += info.ms_per_iteration
+        out["batched"] = {"workload": "512 integrands (256 camels D 2-12, 256 multichannel 2->n), one adapting "
+                                      "iteration each per step", "ms_per_iteration": bms / 3,
+                          "points_per_s": npts / (bms / 3 / 1e3), "launches_per_iteration": (ctx.launches - l0) / 3,
+                          "full_line": "python bench.py --workload batched"}
+        ctx.close()
+        # 2->6, 45 channels, 200 bins, 1e7 points per iteration
+        wl = WORKLOADS["large"]
+        cs = workloads.channel_set(6)
+        ctx = gpu.Context(dev.index)
+        ctx.set_stream(stream.cuda_stream)
+        ctx.set_channels(cs)
+        ctx.uniform_grids(cs.nch, ctx.ndims, wl["bins"])
+        ctx.set_integrand(abi.CHILI_FUNC_PROPAGATOR_TOP2, channels.propagator_params())
+        ctx.set_preprocess_cuts(cs.sqrts)
+        params = workloads.mc_params(wl["ncalls"], iterations=6)
+        c = 0
+        for _ in range(3):
+            st, info = ctx.multichannel_iterate(params, seed=SEED, counter=c, guard=True)
+            c += info.points_tried
+        e0.record(stream)
+        unw, tried = 0.0, 0
+        for _ in range(3):
+            st, info = ctx.multichannel_iterate(params, seed=SEED, counter=c, guard=True)
+            c += info.points_tried
+            unw += unweighted_events(st, info)
+            tried += info.points_tried
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / 3
+        out["large"] = {"workload": wl["describe"] + ", 45 channels, 200 bins, 1e7 accepted points per iteration, "
+                                                     "plain path", "ms_per_iteration": ms,
+                        "unweighted_events_per_s": unw / (3 * ms / 1e3),
+                        "tried_points_per_s": tried / (3 * ms / 1e3),
+                        "full_line": "python bench.py --workload large"}
+        ctx.close()
+    finally:
+        torch.cuda.set_stream(prev)
+    return out
 
 
 # Per-kernel figures of the committed ncu capture
@@ -737,7 +844,8 @@ def run_vegas(args, rank, world, local_rank):
     cfg["ncalls"] = n
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)  # current for torch too (the flush and the events share it)
+    torch.cuda.set_stream(stream)
     ctx = gpu.Context(local_rank)
     ctx.set_stream(stream.cuda_stream)
     params = workloads.camel_params(cfg["dims"])
@@ -774,6 +882,7 @@ def run_vegas(args, rank, world, local_rank):
             counter += n
         torch.cuda.synchronize(dev)
     launches = ctx.launches - l0
+    kms, kl = ctx.kernel_time("k_vegas_iter")
     ctx.set_option("kernel_timing", 0)
     ms = sum(a.elapsed_time(b) for a, b in evs)
     t = torch.tensor([ms], dtype=torch.float64, device=dev)
@@ -783,7 +892,6 @@ def run_vegas(args, rank, world, local_rank):
     st = stats_dev[args.warmup:].cpu().numpy()
     pooled = (st * np.array([1, 0, 0, 1, 1, 1])).sum(axis=0)
     mean, err = gpu.stats_mean_error(pooled)
-    kms, kl = ctx.kernel_time("k_vegas_iter")
     c = VEGAS_COUNTERS.get("k_vegas_iter")
     peak = fp64_peak_tflops(dev)
     roof = {"kernel": "k_vegas_iter", "bound": "fp64", "launches": kl, "ms_per_launch": kms / max(kl, 1),

@@ -25,6 +25,7 @@
 #include <math_constants.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -32,6 +33,7 @@
 
 #include "channel_program.h"
 #include "context.h"
+#include "phase_dev.cuh"
 
 using namespace chili_dev;
 
@@ -221,12 +223,12 @@ __global__ void __launch_bounds__(256) k_batch_eval(BatchDev B) {
 // channel, VEGAS map, FSMapper and PreProcess; accepted points' external
 // momenta to mom_soa [slot][component][ms], per block of kFwdBlock points
 // the accepted count.
-__global__ void __launch_bounds__(kFwdBlock) k_bt_forward(BatchDev B, int ti, long long p0, long long mm,
-                                                          double *__restrict__ mom_soa, long long ms,
-                                                          int32_t *__restrict__ ich_out, uint8_t *__restrict__ flag,
-                                                          int32_t *__restrict__ block_count) {
+__device__ __forceinline__ void bt_forward_block(const BatchDev &B, int ti, long long p0, long long mm,
+                                                 double *__restrict__ mom_soa, long long ms,
+                                                 int32_t *__restrict__ ich_out, uint8_t *__restrict__ flag,
+                                                 int32_t *__restrict__ block_count, long long bx) {
     const BatchTask T = B.tasks[ti];
-    const long long k = blockIdx.x * static_cast<long long>(kFwdBlock) + threadIdx.x;
+    const long long k = bx * static_cast<long long>(kFwdBlock) + threadIdx.x;
     int acc = 0;
     if (k < mm) {
         const int D = T.dims, bins = T.bins;
@@ -255,7 +257,14 @@ __global__ void __launch_bounds__(kFwdBlock) k_bt_forward(BatchDev B, int ti, lo
         flag[k] = static_cast<uint8_t>(acc);
     }
     const int cnt = __syncthreads_count(acc);
-    if (threadIdx.x == 0) block_count[blockIdx.x] = cnt;
+    if (threadIdx.x == 0) block_count[bx] = cnt;
+}
+
+__global__ void __launch_bounds__(kFwdBlock) k_bt_forward(BatchDev B, int ti, long long p0, long long mm,
+                                                          double *__restrict__ mom_soa, long long ms,
+                                                          int32_t *__restrict__ ich_out, uint8_t *__restrict__ flag,
+                                                          int32_t *__restrict__ block_count) {
+    bt_forward_block(B, ti, p0, mm, mom_soa, ms, ich_out, flag, block_count, blockIdx.x);
 }
 
 // Step 3 (after compact_launch and pp_pass_launch): block b of the tile is
@@ -264,24 +273,24 @@ __global__ void __launch_bounds__(kFwdBlock) k_bt_forward(BatchDev B, int ti, lo
 // are calls of value 0.  StatsData partial of the unit, AddTrainData
 // (MultiChannel.hh:167-180) histogram adds and channel-training terms, as
 // k_batch_eval does per point (NaN values count as 0).
-__global__ void __launch_bounds__(kFwdBlock) k_bt_accum(BatchDev B, int ti, long long p0, long long mm,
-                                                        const int32_t *__restrict__ block_count,
-                                                        const long long *__restrict__ block_off,
-                                                        const double *__restrict__ rec_val,
-                                                        const double *__restrict__ rec_wgt,
-                                                        const uint8_t *__restrict__ rec_ok,
-                                                        const int32_t *__restrict__ rec_slot,
-                                                        const double *__restrict__ rec_dens, long long mr) {
+__device__ __forceinline__ void bt_accum_block(const BatchDev &B, int ti, long long p0, long long mm,
+                                               const int32_t *__restrict__ block_count,
+                                               const long long *__restrict__ block_off,
+                                               const double *__restrict__ rec_val,
+                                               const double *__restrict__ rec_wgt,
+                                               const uint8_t *__restrict__ rec_ok,
+                                               const int32_t *__restrict__ rec_slot,
+                                               const double *__restrict__ rec_dens, long long mr, long long bx) {
     __shared__ double ws[kFwdBlock / 32][6];
     __shared__ double s_atr[kBatchMaxCh];
     const BatchTask T = B.tasks[ti];
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     if (t < kBatchMaxCh) s_atr[t] = 0.0;
     __syncthreads();
-    const long long k0 = blockIdx.x * static_cast<long long>(kFwdBlock);
+    const long long k0 = bx * static_cast<long long>(kFwdBlock);
     const long long active = mm - k0 < kFwdBlock ? mm - k0 : kFwdBlock;
-    const int nrec = block_count[blockIdx.x];
-    const long long r = block_off[blockIdx.x] + t;
+    const int nrec = block_count[bx];
+    const long long r = block_off[bx] + t;
     double val = 0, vw = 0;
     if (t < nrec) {
         val = rec_ok[r] ? rec_val[r] : 0.0;
@@ -333,11 +342,138 @@ __global__ void __launch_bounds__(kFwdBlock) k_bt_accum(BatchDev B, int ti, long
             a[1] = std_min(a[1], 0.0);
             a[2] = std_max(a[2], 0.0);
         }
-        double *o = B.part + (T.unit0 + p0 / kFwdBlock + blockIdx.x) * 6;
+        double *o = B.part + (T.unit0 + p0 / kFwdBlock + bx) * 6;
         for (int q = 0; q < 6; ++q) o[q] = a[q];
     }
     if (t < T.nch && s_atr[t] != 0) atomicAdd(B.atrain + T.ch_off + t, s_atr[t]);
 }
+
+__global__ void __launch_bounds__(kFwdBlock) k_bt_accum(BatchDev B, int ti, long long p0, long long mm,
+                                                        const int32_t *__restrict__ block_count,
+                                                        const long long *__restrict__ block_off,
+                                                        const double *__restrict__ rec_val,
+                                                        const double *__restrict__ rec_wgt,
+                                                        const uint8_t *__restrict__ rec_ok,
+                                                        const int32_t *__restrict__ rec_slot,
+                                                        const double *__restrict__ rec_dens, long long mr) {
+    bt_accum_block(B, ti, p0, mm, block_count, block_off, rec_val, rec_wgt, rec_ok, rec_slot, rec_dens, mr,
+                   blockIdx.x);
+}
+
+// ----------------------------------------------- grouped phased weight pass
+// The phased multichannel tasks of an iteration run in waves: a wave is a
+// list of pieces (points [p0, p0 + mm) of one task, with buffers of their
+// own carved out of one arena, stride ms = mm rounded up to kFwdBlock), and
+// each step of the pass is ONE launch over all pieces of the wave: the
+// blocks of a step are numbered piece after piece (prefix[step][k] is the
+// first block of piece k) and each block finds its piece by binary search.
+// The per-piece work is exactly the per-task chain's (the same device
+// functions), so the results do not depend on the grouping.
+struct Piece {
+    int32_t ti, nb;                    // task; blocks of kFwdBlock points
+    int32_t n_items[3], n_chains, nch, dims, bins;
+    long long p0, mm, ms;
+    const PointProgram *pp;
+    const double *grids, *alpha;
+    const IntegrandDesc *f;
+    double *mom;
+    int32_t *ich;
+    uint8_t *flag;
+    int32_t *bcount;
+    long long *boff;
+    RoundCtl *ctl;
+    int32_t *list;
+    double *node, *memo, *dcv, *vwv;
+    uint8_t *cfail;
+    int32_t *ich_tile;
+    double *val, *wgt;
+    uint8_t *ok;
+    int32_t *slot;
+    double *dens;
+};
+enum { GS_FWD, GS_COMPACT, GS_NODES, GS_ITEM0, GS_ITEM1, GS_ITEM2, GS_CHAINS, GS_CHANNEL, GS_COMBINE, GS_ACCUM,
+       kGroupSteps };
+
+struct WaveDev {
+    const Piece *pieces;
+    int n;
+    const long long *prefix;  // [kGroupSteps][n + 1]
+};
+
+// The piece k in [lo, hi) of a step whose blocks [prefix[k], prefix[k+1])
+// hold block b.
+__device__ __forceinline__ int find_piece(const long long *__restrict__ pre, int lo, int hi, long long b) {
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(pre + mid) <= b) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+#define CHILI_PIECE(step)                                                        \
+    const long long *pre_ = W.prefix + static_cast<size_t>(step) * (W.n + 1);    \
+    const long long b_ = blockIdx.x + blk0;                                      \
+    const int k_ = find_piece(pre_, lo, hi, b_);                                 \
+    const Piece &P = W.pieces[k_];                                               \
+    const long long lb = b_ - pre_[k_];
+
+__global__ void __launch_bounds__(kFwdBlock) k_g_forward(BatchDev B, WaveDev W, int lo, int hi, long long blk0) {
+    CHILI_PIECE(GS_FWD)
+    bt_forward_block(B, P.ti, P.p0, P.mm, P.mom, P.ms, P.ich, P.flag, P.bcount, lb);
+}
+
+__global__ void __launch_bounds__(1024) k_g_scan(WaveDev W) {
+    const Piece &P = W.pieces[blockIdx.x];
+    mc_scan_body(P.bcount, P.nb, P.flag, P.mm, P.mm + 1, nullptr, 0, P.boff, P.ctl);
+}
+
+__global__ void __launch_bounds__(kFwdBlock) k_g_compact(WaveDev W, int lo, int hi, long long blk0) {
+    CHILI_PIECE(GS_COMPACT)
+    mc_compact_block(P.flag, P.boff, P.ctl, P.mm, P.list, lb);
+}
+
+__global__ void __launch_bounds__(256) k_g_nodes(WaveDev W, int lo, int hi, long long blk0) {
+    CHILI_PIECE(GS_NODES)
+    pp_nodes_block(P.pp, P.mom, P.ms, P.list, P.ich, &P.ctl->n_acc, 0, P.node, P.ich_tile, P.ms, lb);
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(256, KIND == 2 ? 4 : 1) k_g_items(WaveDev W, int lo, int hi, long long blk0) {
+    CHILI_PIECE(GS_ITEM0 + KIND)
+    const int ni = P.n_items[KIND];
+    pp_items_block<KIND>(P.pp, P.node, &P.ctl->n_acc, 0, P.ms, P.memo, static_cast<int>(lb % ni), lb / ni);
+}
+
+__global__ void __launch_bounds__(256) k_g_chains(WaveDev W, int lo, int hi, long long blk0) {
+    CHILI_PIECE(GS_CHAINS)
+    pp_chains_block(P.pp, P.node, &P.ctl->n_acc, 0, P.ms, P.memo, P.cfail, static_cast<int>(lb % P.n_chains),
+                    lb / P.n_chains);
+}
+
+// Pieces [lo, hi) of the wave have DIMS dimensions.
+template <int DIMS>
+__global__ void __launch_bounds__(128) k_g_channel(WaveDev W, int lo, int hi, long long blk0) {
+    CHILI_PIECE(GS_CHANNEL)
+    const int c = static_cast<int>(lb % P.nch);
+    const long long i = (lb / P.nch) * 128 + threadIdx.x;
+    if (i < P.ms && i < P.ctl->n_acc)
+        pp_channel_point<DIMS, false>(P.pp, P.grids, nullptr, nullptr, nullptr, P.bins, P.memo, P.cfail, P.ich_tile,
+                                      P.ms, P.ms, 1, P.dcv, P.vwv, P.slot, P.dens, i, i, c);
+}
+
+__global__ void __launch_bounds__(256) k_g_combine(WaveDev W, int lo, int hi, long long blk0) {
+    CHILI_PIECE(GS_COMBINE)
+    const long long i = lb * 256 + threadIdx.x;
+    if (i < P.ms && i < P.ctl->n_acc)
+        pp_combine_point(P.pp, P.alpha, P.dcv, P.vwv, P.node, P.ms, i, i, P.f, P.val, P.wgt, P.ok, false);
+}
+
+__global__ void __launch_bounds__(kFwdBlock) k_g_accum(BatchDev B, WaveDev W, int lo, int hi, long long blk0) {
+    CHILI_PIECE(GS_ACCUM)
+    bt_accum_block(B, P.ti, P.p0, P.mm, P.bcount, P.boff, P.val, P.wgt, P.ok, P.slot, P.dens, P.ms, lb);
+}
+#undef CHILI_PIECE
 
 // The PointPrograms' (smin, smax) terms.
 __global__ void k_batch_pp_prepare(PointProgram *__restrict__ pps) {
@@ -447,6 +583,19 @@ struct BatchState {
     std::vector<PhBufs> ph;
     std::vector<cudaStream_t> ph_streams;
     std::vector<cudaEvent_t> ph_events;
+    // grouped mode (option "batch_grouped", the default): the phased tasks in
+    // waves of pieces, one launch per step and wave (see Piece)
+    bool grouped = false;
+    struct WaveHost {
+        int first = 0, n = 0;                        // pieces [first, first + n)
+        long long prefix_off = 0;                    // into d_prefix
+        std::vector<long long> blocks;               // per step: total blocks
+        std::vector<std::array<int, 3>> dgroups;     // (dims, k0, k1): pieces [k0, k1) of one dimension
+    };
+    std::vector<Piece> pieces;
+    std::vector<WaveHost> waves;
+    std::vector<long long> prefix_host;
+    DevBuf d_pieces, d_prefix, d_arena;
     bool tuned = false;
     cudaGraphExec_t graph = nullptr;
     unsigned long long graph_launches = 0;  // kernels of one replay
@@ -586,6 +735,62 @@ int enqueue_phased_task(chili_ctx *ctx, const BatchDev &B, int ti, BatchState::P
     return CHILI_OK;
 }
 
+// The phased tasks' waves, one after another on ctx->stream: one launch per
+// step and wave.
+int enqueue_waves(chili_ctx *ctx, const BatchDev &B) {
+    BatchState &S = *ctx->batch;
+    for (const auto &w : S.waves) {
+        const WaveDev W{S.d_pieces.as<Piece>() + w.first, w.n, S.d_prefix.as<long long>() + w.prefix_off};
+        const long long *pre = S.prefix_host.data() + w.prefix_off;
+        auto blocks = [&](int step) { return static_cast<unsigned>(w.blocks[static_cast<size_t>(step)]); };
+        k_g_forward<<<blocks(GS_FWD), kFwdBlock, 0, ctx->stream>>>(B, W, 0, w.n, 0);
+        LAUNCHED();
+        k_g_scan<<<static_cast<unsigned>(w.n), 1024, 0, ctx->stream>>>(W);
+        LAUNCHED();
+        k_g_compact<<<blocks(GS_COMPACT), kFwdBlock, 0, ctx->stream>>>(W, 0, w.n, 0);
+        LAUNCHED();
+        k_g_nodes<<<blocks(GS_NODES), 256, 0, ctx->stream>>>(W, 0, w.n, 0);
+        LAUNCHED();
+        if (blocks(GS_ITEM0)) {
+            k_g_items<0><<<blocks(GS_ITEM0), 256, 0, ctx->stream>>>(W, 0, w.n, 0);
+            LAUNCHED();
+        }
+        if (blocks(GS_ITEM1)) {
+            k_g_items<1><<<blocks(GS_ITEM1), 256, 0, ctx->stream>>>(W, 0, w.n, 0);
+            LAUNCHED();
+        }
+        if (blocks(GS_ITEM2)) {
+            k_g_items<2><<<blocks(GS_ITEM2), 256, 0, ctx->stream>>>(W, 0, w.n, 0);
+            LAUNCHED();
+        }
+        if (blocks(GS_CHAINS)) {
+            k_g_chains<<<blocks(GS_CHAINS), 256, 0, ctx->stream>>>(W, 0, w.n, 0);
+            LAUNCHED();
+        }
+        const long long *pc = pre + static_cast<size_t>(GS_CHANNEL) * (w.n + 1);
+        for (const auto &g : w.dgroups) {
+            const long long b0 = pc[g[1]], nbk = pc[g[2]] - b0;
+            if (nbk <= 0) continue;
+            switch (g[0]) {
+#define CHILI_GCH(D)                                                                                        \
+    case D:                                                                                                 \
+        k_g_channel<D><<<static_cast<unsigned>(nbk), 128, 0, ctx->stream>>>(W, g[1], g[2], b0);            \
+        break;
+                CHILI_GCH(1) CHILI_GCH(4) CHILI_GCH(7) CHILI_GCH(10) CHILI_GCH(13) CHILI_GCH(16) CHILI_GCH(19)
+                CHILI_GCH(22)
+#undef CHILI_GCH
+                default: return fail(ctx, CHILI_ERR_STATE, "no phased weight kernel for this dimension");
+            }
+            LAUNCHED();
+        }
+        k_g_combine<<<blocks(GS_COMBINE), 256, 0, ctx->stream>>>(W, 0, w.n, 0);
+        LAUNCHED();
+        k_g_accum<<<blocks(GS_ACCUM), kFwdBlock, 0, ctx->stream>>>(B, W, 0, w.n, 0);
+        LAUNCHED();
+    }
+    return CHILI_OK;
+}
+
 // The iteration as a stream of launches (captured into the graph).
 int enqueue_iteration(chili_ctx *ctx, bool adapt) {
     BatchState &S = *ctx->batch;
@@ -593,10 +798,24 @@ int enqueue_iteration(chili_ctx *ctx, bool adapt) {
     CK(cudaMemsetAsync(S.d_atrain.p, 0, S.d_atrain.cap, ctx->stream));
     BatchDev B = batch_dev(ctx);
     const cudaStream_t main = ctx->stream;
+    if (S.grouped && !S.waves.empty()) {
+        // the waves on a second stream beside the camel tasks' evaluation
+        CK(cudaEventRecord(S.ph_events[1], main));
+        CK(cudaStreamWaitEvent(S.ph_streams[0], S.ph_events[1], 0));
+        k_batch_eval<<<S.grid_blocks, S.block, 0, ctx->stream>>>(B);
+        LAUNCHED();
+        ctx->stream = S.ph_streams[0];
+        const int rc = enqueue_waves(ctx, B);
+        ctx->stream = main;
+        if (rc) return rc;
+        CK(cudaEventRecord(S.ph_events[0], S.ph_streams[0]));
+        CK(cudaStreamWaitEvent(main, S.ph_events[0], 0));
+    } else {
     if (!S.ph.empty()) CK(cudaEventRecord(S.ph_events[kPhBranches], main));
     k_batch_eval<<<S.grid_blocks, S.block, 0, ctx->stream>>>(B);
     LAUNCHED();
-    if (!S.ph.empty()) {
+    }
+    if (!S.grouped && !S.ph.empty()) {
         // fork (before the camel tasks' evaluation, which runs beside the
         // branches): each branch runs its phased tasks on its own stream and
         // buffers; join before the folds
@@ -702,6 +921,161 @@ int capture(chili_ctx *ctx, bool adapt) {
     return CHILI_OK;
 }
 
+// Grouped mode: the phased tasks cut into pieces of at most kPieceMax
+// points, packed into waves of at most ctx->batch_wave points (pieces of one
+// dimension together within a wave), each piece's buffers carved out of one
+// arena that every wave reuses (the waves run one after another).
+constexpr long long kPieceMax = 1ll << 20;
+
+int plan_waves(chili_ctx *ctx, const std::vector<PointProgram> &pps) {
+    BatchState &S = *ctx->batch;
+    // a piece never exceeds a wave (small waves, for tests, cut the tasks finer)
+    const long long wave_max = std::max<long long>(ctx->batch_wave / kFwdBlock * kFwdBlock, kFwdBlock);
+    const long long piece_max = std::min(kPieceMax, wave_max);
+    // pieces, task by task (largest tasks first, so that waves fill evenly)
+    std::vector<int> order;
+    for (size_t ti = 0; ti < S.tasks.size(); ++ti)
+        if (S.tasks[ti].phased) order.push_back(static_cast<int>(ti));
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return S.tasks[a].ncalls > S.tasks[b].ncalls; });
+    std::vector<Piece> pcs;
+    for (int ti : order) {
+        const BatchTask &T = S.tasks[static_cast<size_t>(ti)];
+        for (long long p0 = 0; p0 < T.ncalls; p0 += piece_max) {
+            Piece P{};
+            P.ti = ti;
+            P.p0 = p0;
+            P.mm = std::min(piece_max, T.ncalls - p0);
+            P.ms = (P.mm + kFwdBlock - 1) / kFwdBlock * kFwdBlock;
+            P.nb = static_cast<int32_t>(P.ms / kFwdBlock);
+            pcs.push_back(P);
+        }
+    }
+    // waves: first fit in that order
+    std::vector<std::vector<Piece>> waves;
+    std::vector<long long> load;
+    for (const Piece &P : pcs) {
+        size_t w = 0;
+        while (w < waves.size() && load[w] + P.ms > wave_max) ++w;
+        if (w == waves.size()) {
+            waves.emplace_back();
+            load.push_back(0);
+        }
+        waves[w].push_back(P);
+        load[w] += P.ms;
+    }
+    // per piece: constants and buffer sizes
+    auto sizes = [&](const Piece &P, const PointProgram &PP, size_t *out) {
+        const size_t ms = static_cast<size_t>(P.ms), nb = static_cast<size_t>(P.nb);
+        const size_t v[] = {sizeof(double) * 4 * PP.n_ext * ms, sizeof(int32_t) * ms, ms, sizeof(int32_t) * nb,
+                            sizeof(long long) * nb, sizeof(RoundCtl), sizeof(int32_t) * ms,
+                            sizeof(double) * 4 * PP.n_nodes * ms, sizeof(double) * std::max(1, PP.n_memo) * ms,
+                            static_cast<size_t>(std::max(1, PP.n_chains)) * ms, sizeof(double) * PP.nch * ms,
+                            sizeof(double) * PP.nch * ms, sizeof(int32_t) * ms, sizeof(double) * ms,
+                            sizeof(double) * ms, ms, sizeof(int32_t) * PP.ndims * ms, sizeof(double) * PP.nch * ms};
+        for (int q = 0; q < 18; ++q) out[q] = (v[q] + 255) / 256 * 256;
+    };
+    size_t arena = 256;
+    for (auto &w : waves) {
+        size_t tot = 0;
+        for (const Piece &P : w) {
+            size_t sz[18];
+            sizes(P, pps[static_cast<size_t>(S.tasks[static_cast<size_t>(P.ti)].pp)], sz);
+            for (size_t q : sz) tot += q;
+        }
+        arena = std::max(arena, tot);
+    }
+    CK(S.d_arena.ensure(arena));
+    S.pieces.clear();
+    S.waves.clear();
+    S.prefix_host.clear();
+    for (auto &w : waves) {
+        // pieces of one dimension together
+        std::stable_sort(w.begin(), w.end(), [&](const Piece &a, const Piece &b) {
+            return S.tasks[static_cast<size_t>(a.ti)].dims < S.tasks[static_cast<size_t>(b.ti)].dims;
+        });
+        BatchState::WaveHost wh;
+        wh.first = static_cast<int>(S.pieces.size());
+        wh.n = static_cast<int>(w.size());
+        wh.prefix_off = static_cast<long long>(S.prefix_host.size());
+        std::vector<std::vector<long long>> pre(kGroupSteps, std::vector<long long>(w.size() + 1, 0));
+        uint8_t *base = S.d_arena.as<uint8_t>();
+        size_t off = 0;
+        for (size_t k = 0; k < w.size(); ++k) {
+            Piece &P = w[k];
+            const BatchTask &T = S.tasks[static_cast<size_t>(P.ti)];
+            const PointProgram &PP = pps[static_cast<size_t>(T.pp)];
+            P.n_items[0] = PP.n_tents;
+            P.n_items[1] = PP.n_dws;
+            P.n_items[2] = PP.n_sws;
+            P.n_chains = PP.n_chains;
+            P.nch = PP.nch;
+            P.dims = T.dims;
+            P.bins = T.bins;
+            P.pp = S.d_pps.as<PointProgram>() + T.pp;
+            P.grids = S.d_grids.as<double>() + T.grid_off;
+            P.alpha = S.d_alpha.as<double>() + T.ch_off;
+            P.f = S.d_descs.as<IntegrandDesc>() + T.desc;
+            size_t sz[18];
+            sizes(P, PP, sz);
+            void *ptr[18];
+            for (int q = 0; q < 18; ++q) {
+                ptr[q] = base + off;
+                off += sz[q];
+            }
+            P.mom = static_cast<double *>(ptr[0]);
+            P.ich = static_cast<int32_t *>(ptr[1]);
+            P.flag = static_cast<uint8_t *>(ptr[2]);
+            P.bcount = static_cast<int32_t *>(ptr[3]);
+            P.boff = static_cast<long long *>(ptr[4]);
+            P.ctl = static_cast<RoundCtl *>(ptr[5]);
+            P.list = static_cast<int32_t *>(ptr[6]);
+            P.node = static_cast<double *>(ptr[7]);
+            P.memo = static_cast<double *>(ptr[8]);
+            P.cfail = static_cast<uint8_t *>(ptr[9]);
+            P.dcv = static_cast<double *>(ptr[10]);
+            P.vwv = static_cast<double *>(ptr[11]);
+            P.ich_tile = static_cast<int32_t *>(ptr[12]);
+            P.val = static_cast<double *>(ptr[13]);
+            P.wgt = static_cast<double *>(ptr[14]);
+            P.ok = static_cast<uint8_t *>(ptr[15]);
+            P.slot = static_cast<int32_t *>(ptr[16]);
+            P.dens = static_cast<double *>(ptr[17]);
+            const long long gx = (P.ms + 255) / 256, gy = (P.ms + 127) / 128;
+            const long long nblk[kGroupSteps] = {P.nb, P.nb, gx, P.n_items[0] * gx, P.n_items[1] * gx,
+                                                 P.n_items[2] * gx, P.n_chains * gx, P.nch * gy, gx, P.nb};
+            for (int st = 0; st < kGroupSteps; ++st) pre[static_cast<size_t>(st)][k + 1] = pre[st][k] + nblk[st];
+            if (wh.dgroups.empty() || wh.dgroups.back()[0] != P.dims)
+                wh.dgroups.push_back({P.dims, static_cast<int>(k), static_cast<int>(k) + 1});
+            else
+                wh.dgroups.back()[2] = static_cast<int>(k) + 1;
+        }
+        for (int st = 0; st < kGroupSteps; ++st) {
+            wh.blocks.push_back(pre[static_cast<size_t>(st)][w.size()]);
+            if (wh.blocks.back() > 0x7fffffffll) return fail(ctx, CHILI_ERR_LIMIT, "wave too large for one launch");
+            S.prefix_host.insert(S.prefix_host.end(), pre[static_cast<size_t>(st)].begin(),
+                                 pre[static_cast<size_t>(st)].end());
+        }
+        for (const Piece &P : w) S.pieces.push_back(P);
+        S.waves.push_back(wh);
+    }
+    CK(S.d_pieces.ensure(sizeof(Piece) * std::max<size_t>(1, S.pieces.size())));
+    CK(cudaMemcpyAsync(S.d_pieces.p, S.pieces.data(), sizeof(Piece) * S.pieces.size(), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(S.d_prefix.ensure(sizeof(long long) * std::max<size_t>(1, S.prefix_host.size())));
+    CK(cudaMemcpyAsync(S.d_prefix.p, S.prefix_host.data(), sizeof(long long) * S.prefix_host.size(),
+                       cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));  // the host vectors are the copies' sources
+    cudaStream_t st;
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    S.ph_streams.push_back(st);
+    for (int k = 0; k < 2; ++k) {
+        cudaEvent_t e;
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        S.ph_events.push_back(e);
+    }
+    return CHILI_OK;
+}
+
 }  // namespace
 
 void batch_release(chili_ctx *ctx) {
@@ -710,7 +1084,7 @@ void batch_release(chili_ctx *ctx) {
     if (S.graph) cudaGraphExecDestroy(S.graph);
     for (DevBuf *b : {&S.d_tasks, &S.d_umap, &S.d_pps, &S.d_progs, &S.d_descs, &S.d_grids, &S.d_grids_new, &S.d_hist,
                       &S.d_atrain, &S.d_alpha, &S.d_best, &S.d_mindiff, &S.d_cp, &S.d_part, &S.d_stats,
-                      &S.d_counters, &S.d_jobs, &S.d_status})
+                      &S.d_counters, &S.d_jobs, &S.d_status, &S.d_pieces, &S.d_prefix, &S.d_arena})
         b->release();
     for (auto &b : S.ph)
         for (DevBuf *d : {&b.mom, &b.ich, &b.flag, &b.list, &b.bcount, &b.boff, &b.ctl, &b.node, &b.memo, &b.cfail,
@@ -848,7 +1222,8 @@ int chili_gpu_batch_set(chili_ctx *ctx, const chili_task *tasks, int ntasks) {
         S.ph_tile = std::min<long long>(tile, 1ll << 18);
         const size_t T = static_cast<size_t>(std::max<long long>(S.ph_tile, kFwdBlock));
         const size_t nb = T / kFwdBlock;
-        if (S.ph_tile > 0) {
+        S.grouped = ctx->batch_grouped && S.ph_tile > 0;  // waves planned once the device tables exist
+        if (!S.grouped && S.ph_tile > 0) {
             S.ph.resize(kPhBranches);
             for (auto &b : S.ph) {
                 CK(b.mom.ensure(sizeof(double) * 4 * ne * T));
@@ -933,6 +1308,8 @@ int chili_gpu_batch_set(chili_ctx *ctx, const chili_task *tasks, int ntasks) {
     CK(S.d_status.ensure(sizeof(int)));
     CK(cudaMemsetAsync(S.d_status.p, 0, sizeof(int), ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    if (S.grouped)
+        if (int rc = plan_waves(ctx, pps)) return rc;
     return layout_units(ctx, 256, 1);
 }
 

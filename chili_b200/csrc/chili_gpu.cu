@@ -35,8 +35,17 @@ namespace {
 
 template <int D>
 void launch_channel(chili_ctx *ctx, long long base, long long T, long long mr, int bins, int opt,
-                    const long long *n_list, int32_t *rec_slot, double *rec_dens) {
-    k_pp_channel<D><<<dim3(ctx->nch, static_cast<unsigned>((T + 127) / 128)), 128, 0, ctx->stream>>>(
+                    const long long *n_list, int32_t *rec_slot, double *rec_dens, const PPCombine *fuse) {
+    const dim3 grid(ctx->nch, static_cast<unsigned>((T + 127) / 128));
+    if (fuse) {
+        k_pp_channel<D, true, true><<<grid, 128, 0, ctx->stream>>>(
+            ctx->point_prog.as<PointProgram>(), ctx->edges.as<double>(), ctx->hints.as<uint32_t>(),
+            ctx->sorted.as<uint8_t>(), ctx->widths.as<double>(), bins, ctx->memo.as<double>(),
+            ctx->cfail.as<uint8_t>(), ctx->ich_tile.as<int32_t>(), n_list, base, T, mr, opt, ctx->dcv.as<double>(),
+            ctx->vwv.as<double>(), rec_slot, rec_dens, *fuse);
+        return;
+    }
+    k_pp_channel<D><<<grid, 128, 0, ctx->stream>>>(
         ctx->point_prog.as<PointProgram>(), ctx->edges.as<double>(), ctx->hints.as<uint32_t>(),
         ctx->sorted.as<uint8_t>(), ctx->widths.as<double>(), bins, ctx->memo.as<double>(), ctx->cfail.as<uint8_t>(),
         ctx->ich_tile.as<int32_t>(), n_list, base, T, mr, opt, ctx->dcv.as<double>(), ctx->vwv.as<double>(), rec_slot,
@@ -53,7 +62,7 @@ void launch_channel(chili_ctx *ctx, long long base, long long T, long long mr, i
 // nodes ctx->node_soa of the tile).
 int pipeline_run(chili_ctx *ctx, const double *mom_soa, long long m, const int32_t *list, const int32_t *ich,
                  const long long *n_list, long long n_pre, int bins, bool opt, int32_t *rec_slot, double *rec_dens,
-                 const TileFn &combine) {
+                 const TileFn &combine, const PPFusedOut *fused) {
     const PointProgram &P = ctx->pp_host;
     const PointProgram *pp = ctx->point_prog.as<PointProgram>();
     // gridDim.y (point blocks of 128) stays below 65536
@@ -69,6 +78,17 @@ int pipeline_run(chili_ctx *ctx, const double *mom_soa, long long m, const int32
     CK(ctx->dcv.ensure(sizeof(double) * ctx->nch * Ta));
     CK(ctx->ich_tile.ensure(sizeof(int32_t) * Ta));
     CK(ctx->vwv.ensure(sizeof(double) * ctx->nch * Ta));
+    PPCombine comb{};
+    const bool fuse = fused && ctx->fuse_combine;
+    if (fuse) {
+        const size_t nblk = static_cast<size_t>((Ta + 127) / 128);
+        if (ctx->arrivals.cap < sizeof(unsigned) * nblk) {
+            CK(ctx->arrivals.ensure(sizeof(unsigned) * nblk));
+            CK(cudaMemsetAsync(ctx->arrivals.p, 0, ctx->arrivals.cap, ctx->stream));
+        }
+        comb = PPCombine{alpha_ptr(ctx), ctx->node_soa.as<double>(), ctx->f_dev.as<IntegrandDesc>(), fused->rec_val,
+                         fused->rec_wgt, fused->rec_ok, ctx->arrivals.as<unsigned>()};
+    }
     const unsigned gx = static_cast<unsigned>((T + 255) / 256);
     const int n_items = P.n_tents + P.n_dws + P.n_sws;
     const int o = opt ? 1 : 0;
@@ -101,13 +121,14 @@ int pipeline_run(chili_ctx *ctx, const double *mom_soa, long long m, const int32
         LAUNCHED();
         switch (P.ndims) {
 #define CHILI_CH(D) \
-    case D: { KTimer kt_(ctx, KT_CHANNEL); launch_channel<D>(ctx, base, T, m, bins, o, n_list, rec_slot, rec_dens); } break;
+    case D: { KTimer kt_(ctx, KT_CHANNEL); launch_channel<D>(ctx, base, T, m, bins, o, n_list, rec_slot, rec_dens, fuse ? &comb : nullptr); } break;
             CHILI_CH(1) CHILI_CH(4) CHILI_CH(7) CHILI_CH(10) CHILI_CH(13) CHILI_CH(16) CHILI_CH(19) CHILI_CH(22)
 #undef CHILI_CH
         default: return fail(ctx, CHILI_ERR_STATE, "no phased weight kernel for this dimension");
         }
         LAUNCHED();
-        if (int rc = combine(base, T)) return rc;
+        if (!fuse)
+            if (int rc = combine(base, T)) return rc;
     }
     return CHILI_OK;
 }
@@ -225,6 +246,7 @@ int launch_pipeline(chili_ctx *ctx, const double *mom_soa, const int32_t *ich, l
     const PointProgram *pp = ctx->point_prog.as<PointProgram>();
     const long long *n_list = reinterpret_cast<const long long *>(
         reinterpret_cast<const char *>(ctl_pre) + offsetof(RoundCtl, n_acc));
+    const PPFusedOut fused{rec_val, rec_wgt, rec_ok};
     return pipeline_run(ctx, mom_soa, m, ctx->list.as<int32_t>(), ich, n_list,
                         n_pre, bins, opt, rec_slot, rec_dens, [&](long long base, long long T) -> int {
                             const unsigned gx = static_cast<unsigned>((T + 255) / 256);
@@ -237,7 +259,7 @@ int launch_pipeline(chili_ctx *ctx, const double *mom_soa, const int32_t *ich, l
                             }
                             LAUNCHED();
                             return CHILI_OK;
-                        });
+                        }, &fused);
 }
 
 // Hint tables of the grid set (grid.cuh, find_bin_hinted), rebuilt after
@@ -290,7 +312,7 @@ int chili_gpu_create(int device, chili_ctx **out) {
     }
     cudaDeviceGetAttribute(&ctx->max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     cudaFuncSetAttribute(k_mc_accum, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->max_smem_optin);
-    cudaFuncSetAttribute(k_vegas_iter, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->max_smem_optin);
+    cudaFuncSetAttribute(k_vegas_iter<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->max_smem_optin);
     cudaFuncSetAttribute(k_grid_adapt, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->max_smem_optin);
     cudaGetLastError();
     *out = ctx;
@@ -305,7 +327,7 @@ int chili_gpu_destroy(chili_ctx *ctx) {
                       &ctx->ich, &ctx->flag, &ctx->list, &ctx->block_count, &ctx->block_off, &ctx->part,
                       &ctx->hist, &ctx->round_res, &ctx->acc, &ctx->ctl, &ctx->status, &ctx->v_part,
                       &ctx->v_hist, &ctx->v_train, &ctx->v_out, &ctx->rec, &ctx->ctl3, &ctx->unw, &ctx->iter_ctl,
-                      &ctx->mom_soa_alt, &ctx->ich_alt, &ctx->flag_alt, &ctx->block_count_alt};
+                      &ctx->mom_soa_alt, &ctx->ich_alt, &ctx->flag_alt, &ctx->block_count_alt, &ctx->arrivals};
     for (DevBuf *b : bufs) b->release();
     flow_release(ctx);
     batch_release(ctx);
@@ -380,6 +402,15 @@ int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value) {
         ctx->use_pp = value != 0;
         return CHILI_OK;
     }
+    if (std::strcmp(name, "vegas_gen_ppt") == 0) {
+        if (value != 1 && value != 2 && value != 4) return fail(ctx, CHILI_ERR_INVALID_ARG, "vegas_gen_ppt: 1, 2 or 4");
+        ctx->gen_ppt = value;
+        return CHILI_OK;
+    }
+    if (std::strcmp(name, "pipeline_fuse") == 0) {
+        ctx->fuse_combine = value != 0;
+        return CHILI_OK;
+    }
     if (std::strcmp(name, "pipeline") == 0) {
         ctx->use_pipeline = value != 0;
         return CHILI_OK;
@@ -399,6 +430,15 @@ int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value) {
     }
     if (std::strcmp(name, "defer_train") == 0) {
         ctx->defer_train = value != 0;
+        return CHILI_OK;
+    }
+    if (std::strcmp(name, "batch_grouped") == 0) {
+        ctx->batch_grouped = value != 0;
+        return CHILI_OK;
+    }
+    if (std::strcmp(name, "batch_wave_points") == 0) {
+        if (value < 1 || value > (1ll << 30)) return fail(ctx, CHILI_ERR_INVALID_ARG, "batch_wave_points in [1, 2^30]");
+        ctx->batch_wave = value;
         return CHILI_OK;
     }
     if (std::strcmp(name, "batch_phased") == 0) {
@@ -625,8 +665,19 @@ int chili_gpu_vegas_iterate(chili_ctx *ctx, uint64_t ncalls, uint64_t seed, uint
     CK(ctx->v_out.ensure(sizeof(double) * 6));
     if (!smem) CK(cudaMemsetAsync(ctx->v_hist.p, 0, hist_bytes, ctx->stream));
     {
+    using IterKernel = void (*)(const double *, int, int, uint64_t, uint64_t, const double *, long long,
+                                const IntegrandDesc *, double *, double *, int);
+    IterKernel kern = k_vegas_iter<0>;  // the histogram stays below 48 KB of shared memory here
+    switch (D) {
+#define CHILI_IT(d) \
+    case d: kern = k_vegas_iter<d>; break;
+        CHILI_IT(1) CHILI_IT(2) CHILI_IT(3) CHILI_IT(4) CHILI_IT(5) CHILI_IT(6) CHILI_IT(7) CHILI_IT(8)
+        CHILI_IT(10) CHILI_IT(12) CHILI_IT(16)
+#undef CHILI_IT
+        default: break;
+    }
     KTimer kt_(ctx, KT_VEGAS);
-    k_vegas_iter<<<static_cast<unsigned>(nblocks), kVegasBlock, smem ? hist_bytes : 0, ctx->stream>>>(
+    kern<<<static_cast<unsigned>(nblocks), kVegasBlock, smem ? hist_bytes : 0, ctx->stream>>>(
         ctx->edges.as<double>(), D, B, seed, counter_base, static_cast<const double *>(au.dev), n,
         ctx->f_dev.as<IntegrandDesc>(), ctx->v_part.as<double>(), ctx->v_hist.as<double>(), smem ? 1 : 0);
     }
@@ -658,23 +709,39 @@ int chili_gpu_vegas_generate(chili_ctx *ctx, uint64_t n, uint64_t seed, uint64_t
     if (n == 0) return CHILI_OK;
     if (n > (1ull << 40)) return fail(ctx, CHILI_ERR_LIMIT, "n must be at most 2^40");
     const int D = ctx->dims, B = ctx->bins;
-    const size_t smem = sizeof(double) * ((static_cast<size_t>(D) * (B + 1) + 1) / 2 * 2 + kGenTile * (D + 1));
+    // points per thread: 4 where the staged tile stays small, else 1
+    const size_t grid_doubles = (static_cast<size_t>(D) * (B + 1) + 1) / 2 * 2;
+    int ppt = static_cast<int>(ctx->gen_ppt);
+    if (sizeof(double) * (grid_doubles + static_cast<size_t>(kGenTile) * ppt * (D + 1)) > 64 * 1024) ppt = 1;
+    const size_t smem = sizeof(double) * (grid_doubles + static_cast<size_t>(kGenTile) * ppt * (D + 1));
     if (smem > 200 * 1024) return fail(ctx, CHILI_ERR_LIMIT, "grid too large for the shared-memory staging");
     const long long nn = static_cast<long long>(n);
     Arg ax, aw;
     if ((rc = resolve(ctx, x_out, sizeof(double) * nn * D, 0, false, ax))) return rc;
     if ((rc = resolve(ctx, w_out, sizeof(double) * nn, 1, false, aw))) return rc;
+    using GenKernel = void (*)(const double *, int, int, uint64_t, uint64_t, long long, const IntegrandDesc *,
+                               double *, double *);
+    GenKernel kern = k_vegas_generate<0, 1>;
+    switch (D * 8 + ppt) {
+#define CHILI_GEN(d)                                             \
+    case d * 8 + 1: kern = k_vegas_generate<d, 1>; break;       \
+    case d * 8 + 2: kern = k_vegas_generate<d, 2>; break;       \
+    case d * 8 + 4: kern = k_vegas_generate<d, 4>; break;
+        CHILI_GEN(1) CHILI_GEN(2) CHILI_GEN(3) CHILI_GEN(4) CHILI_GEN(5) CHILI_GEN(6) CHILI_GEN(7) CHILI_GEN(8)
+        CHILI_GEN(10) CHILI_GEN(12) CHILI_GEN(16)
+#undef CHILI_GEN
+        default: ppt = 1; break;
+    }
     if (smem > 48 * 1024)
-        CK(cudaFuncSetAttribute(k_vegas_generate, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(smem)));
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     int sms = 148, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_vegas_generate, kGenTile, smem));
-    const long long tiles = (nn + kGenTile - 1) / kGenTile;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kGenTile, smem));
+    const long long tiles = (nn + static_cast<long long>(kGenTile) * ppt - 1) / (static_cast<long long>(kGenTile) * ppt);
     const long long nblocks = std::min<long long>(tiles, static_cast<long long>(sms) * std::max(per_sm, 1));
     {
         KTimer kt_(ctx, KT_VEGAS_GEN);
-        k_vegas_generate<<<static_cast<unsigned>(nblocks), kGenTile, smem, ctx->stream>>>(
+        kern<<<static_cast<unsigned>(nblocks), kGenTile, smem, ctx->stream>>>(
             ctx->edges.as<double>(), D, B, seed, counter_base, nn, ctx->f_dev.as<IntegrandDesc>(),
             static_cast<double *>(ax.dev), static_cast<double *>(aw.dev));
     }
@@ -1477,7 +1544,7 @@ extern "C" int chili_gpu_vegas_iterate_noalloc(void *stream, const double *edges
     const long long n = static_cast<long long>(ncalls);
     const long long nblocks = std::min<long long>(std::min<long long>(grid_for(n, kVegasBlock), sms * 4ll),
                                                   kNoAllocMaxBlocks);
-    k_vegas_iter<<<static_cast<unsigned>(nblocks), kVegasBlock, 0, st>>>(edges, dims, bins, seed, counter_base,
+    k_vegas_iter<0><<<static_cast<unsigned>(nblocks), kVegasBlock, 0, st>>>(edges, dims, bins, seed, counter_base,
                                                                           nullptr, n, desc_dev, part, train_out, 0);
     CK(cudaGetLastError());
     k_vegas_finalize<<<1, 256, 0, st>>>(part, static_cast<int>(nblocks), nullptr, 0, nh, train_out, stats_out);

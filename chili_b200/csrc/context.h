@@ -67,9 +67,16 @@ void batch_release(chili_ctx *ctx);
 using TileFn = std::function<int(long long base, long long T)>;
 // The phased weight pass (chili_gpu.cu) over listed points of a momenta
 // buffer [slot][component][m]; rec_dens may be null.
+// fused (optional): the standard combine step's outputs; when given (and the
+// "pipeline_fuse" option is on) the combine runs inside the channel kernel
+// and `combine` is not called.
+struct PPFusedOut {
+    double *rec_val, *rec_wgt;
+    uint8_t *rec_ok;
+};
 int pipeline_run(chili_ctx *ctx, const double *mom_soa, long long m, const int32_t *list, const int32_t *ich,
                  const long long *n_list, long long n_pre, int bins, bool opt, int32_t *rec_slot, double *rec_dens,
-                 const TileFn &combine);
+                 const TileFn &combine, const PPFusedOut *fused = nullptr);
 
 // One phased weight pass with explicit buffers and no host round trip (so
 // that a graph can capture it; chili_gpu.cu): T launch points, of which the
@@ -125,12 +132,17 @@ struct chili_ctx {
     bool have_pp = false;      // the set fits the PointProgram limits
     bool use_pp = true;        // option "point_program"
     bool use_pipeline = true;  // option "pipeline": phased weight pass
+    bool fuse_combine = false;  // option "pipeline_fuse": combine step inside the channel kernel (slower: off)
+    long long gen_ppt = 2;       // option "vegas_gen_ppt": points per thread of chili_gpu_vegas_generate
     bool defer_train = false;  // option "defer_train": iterations collect training data, Train is the caller's
     bool batch_phased = true;  // option "batch_phased": batched multichannel tasks by the phased weight pass
+    bool batch_grouped = true;  // option "batch_grouped": the phased tasks in waves, one launch per step and wave
+    long long batch_wave = 1ll << 22;  // option "batch_wave_points": points per wave of the grouped mode
     long long pipe_tile = 1 << 22;  // option "pipeline_tile": points per tile
     long long max_rounds = 100000;  // option "max_rounds": chunks an iteration may take before CHILI_ERR_TIMEOUT
     PointProgram pp_host;      // host copy (sizes of the memo buffers)
     DevBuf node_soa, memo, cfail, dcv, vwv;
+    DevBuf arrivals;  // per point block of a tile: the fused combine's arrival counters (zero between launches)
     DevBuf hints, sorted, widths;  // hinted bin search tables and bin widths of the grids
     DevBuf ich_tile;
     // channel weights: alpha[CH], best[CH], cp[CH], min_diff

@@ -27,6 +27,7 @@
 #pragma once
 
 #include "mc_device.cuh"
+#include "phase_dev.cuh"
 
 namespace chili_dev {
 
@@ -140,10 +141,14 @@ __global__ void k_grid_split(const double *__restrict__ g_old, double *__restric
 // ------------------------------------------------------------- plain VEGAS
 // One Vegas::operator() over n points (grid-stride).  Histogram in shared
 // memory when it fits (smem_hist), else global atomics into hist.
-__global__ void k_vegas_iter(const double *__restrict__ g, int dims, int bins, uint64_t seed, uint64_t ctr0,
+// DIMS > 0: the dimension fixed at compile time (coordinates in registers);
+// DIMS == 0: `dims` at run time (a local array).
+template <int DIMS>
+__global__ void k_vegas_iter(const double *__restrict__ g, int dims_rt, int bins, uint64_t seed, uint64_t ctr0,
                              const double *__restrict__ u_in, long long n, const IntegrandDesc *__restrict__ f,
                              double *__restrict__ part, double *__restrict__ hist, int smem_hist) {
     extern __shared__ double sh[];
+    const int dims = DIMS > 0 ? DIMS : dims_rt;
     const int nh = dims * bins;
     if (smem_hist)
         for (int k = threadIdx.x; k < nh; k += blockDim.x) sh[k] = 0.0;
@@ -152,8 +157,9 @@ __global__ void k_vegas_iter(const double *__restrict__ g, int dims, int bins, u
     double cnt = 0, sum = 0, sum2 = 0, mn = 1.7976931348623157e308, mx = 2.2250738585072014e-308, nf = 0;
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<long long>(gridDim.x) * blockDim.x) {
-        double r[CHILI_MAX_DIMS];
+        double r[DIMS > 0 ? DIMS : CHILI_MAX_DIMS];
         if (u_in) {
+#pragma unroll
             for (int d = 0; d < dims; ++d) r[d] = __ldg(u_in + i * dims + d);
         } else {
             load_uniforms(seed, ctr0 + i, nullptr, dims, r);
@@ -169,6 +175,7 @@ __global__ void k_vegas_iter(const double *__restrict__ g, int dims, int bins, u
         mn = std_min(mn, val);
         mx = std_max(mx, val);
         nf += (val != 0);
+#pragma unroll
         for (int j = 0; j < dims; ++j) {
             const int b = find_bin(g + j * (bins + 1), bins, r[j]);
             const int s = j * bins + b;
@@ -208,46 +215,59 @@ __global__ void k_vegas_iter(const double *__restrict__ g, int dims, int bins, u
 // and leave as contiguous 16-byte stores, so the only HBM traffic is the
 // 8 (dims + 1) bytes written per point.  Persistent grid-stride over tiles
 // of kGenTile points.
+// DIMS > 0 fixes the dimension at compile time (the point's coordinates stay
+// in registers); DIMS == 0 takes `dims` at run time (a local array).  PPT
+// points per thread (independent dependency chains the scheduler overlaps):
+// a tile is kGenTile * PPT points.
 constexpr int kGenTile = 256;
-__global__ void __launch_bounds__(kGenTile) k_vegas_generate(const double *__restrict__ g, int dims, int bins,
+template <int DIMS, int PPT>
+__global__ void __launch_bounds__(kGenTile) k_vegas_generate(const double *__restrict__ g, int dims_rt, int bins,
                                                              uint64_t seed, uint64_t ctr0, long long n,
                                                              const IntegrandDesc *__restrict__ f,
                                                              double *__restrict__ x_out, double *__restrict__ w_out) {
     extern __shared__ __align__(16) double gsh[];
+    constexpr int kTile = kGenTile * PPT;
+    const int dims = DIMS > 0 ? DIMS : dims_rt;
     const int ne = dims * (bins + 1);
-    double *xt = gsh + ((ne + 1) & ~1);  // kGenTile * dims x values, 16-byte aligned
-    double *wt = xt + kGenTile * dims;   // kGenTile weights
+    double *xt = gsh + ((ne + 1) & ~1);  // kTile * dims x values, 16-byte aligned
+    double *wt = xt + kTile * dims;      // kTile weights
     for (int k = threadIdx.x; k < ne; k += blockDim.x) gsh[k] = g[k];
     __syncthreads();
     const double fb = static_cast<double>(bins);
-    const long long ntiles = (n + kGenTile - 1) / kGenTile;
+    const long long ntiles = (n + kTile - 1) / kTile;
     for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const long long i0 = t * kGenTile, i = i0 + threadIdx.x;
-        const int cnt = static_cast<int>(n - i0 < kGenTile ? n - i0 : kGenTile);
-        if (i < n) {
-            double r[CHILI_MAX_DIMS];
-            load_uniforms(seed, ctr0 + i, nullptr, dims, r);
-            // AdaptiveMap::operator() (AdaptiveMap.cc:40-56) on the staged
-            // edges, rounded as grid_map_checked
-            double jac = 1.0;
-            bool ok = true;
-            for (int d = 0; d < dims; ++d) {
-                const double pos = __dmul_rn(r[d], fb);
-                if (!(pos >= 0.0 && pos < fb)) {
-                    ok = false;
-                    break;
+        const long long i0 = t * kTile;
+        const int cnt = static_cast<int>(n - i0 < kTile ? n - i0 : kTile);
+#pragma unroll
+        for (int q = 0; q < PPT; ++q) {
+            const int l = q * kGenTile + threadIdx.x;  // point of the tile
+            if (l < cnt) {
+                double r[DIMS > 0 ? DIMS : CHILI_MAX_DIMS];
+                load_uniforms(seed, ctr0 + i0 + l, nullptr, dims, r);
+                // AdaptiveMap::operator() (AdaptiveMap.cc:40-56) on the staged
+                // edges, rounded as grid_map_checked
+                double jac = 1.0;
+                bool ok = true;
+#pragma unroll
+                for (int d = 0; d < dims; ++d) {
+                    const double pos = __dmul_rn(r[d], fb);
+                    if (!(pos >= 0.0 && pos < fb)) {
+                        ok = false;
+                        break;
+                    }
+                    const int idx = static_cast<int>(pos);
+                    const double loc = __dsub_rn(pos, static_cast<double>(idx));
+                    const double *e = gsh + d * (bins + 1);
+                    const double left = e[idx];
+                    const double size = __dsub_rn(e[idx + 1], left);
+                    r[d] = __dadd_rn(left, __dmul_rn(loc, size));
+                    jac = __dmul_rn(jac, __dmul_rn(size, fb));
                 }
-                const int idx = static_cast<int>(pos);
-                const double loc = __dsub_rn(pos, static_cast<double>(idx));
-                const double *e = gsh + d * (bins + 1);
-                const double left = e[idx];
-                const double size = __dsub_rn(e[idx + 1], left);
-                r[d] = __dadd_rn(left, __dmul_rn(loc, size));
-                jac = __dmul_rn(jac, __dmul_rn(size, fb));
+                const double w = ok ? camel(f, r, dims) * jac : CUDART_NAN;
+#pragma unroll
+                for (int d = 0; d < dims; ++d) xt[l * dims + d] = ok ? r[d] : CUDART_NAN;
+                wt[l] = w;
             }
-            const double w = ok ? camel(f, r, dims) * jac : CUDART_NAN;
-            for (int d = 0; d < dims; ++d) xt[threadIdx.x * dims + d] = ok ? r[d] : CUDART_NAN;
-            wt[threadIdx.x] = w;
         }
         __syncthreads();
         // the tile's rows are contiguous in x_out: cnt * dims doubles from
@@ -262,7 +282,7 @@ __global__ void __launch_bounds__(kGenTile) k_vegas_generate(const double *__res
         } else {
             for (int k = threadIdx.x; k < nx; k += blockDim.x) xo[k] = xt[k];
         }
-        if (threadIdx.x < cnt) w_out[i0 + threadIdx.x] = wt[threadIdx.x];
+        for (int k = threadIdx.x; k < cnt; k += blockDim.x) w_out[i0 + k] = wt[k];
         __syncthreads();
     }
 }
@@ -420,115 +440,20 @@ __global__ void __launch_bounds__(kFwdBlock) k_mc_forward(
 // may be NULL): the device's count still needed; when it is 0 the round is
 // empty (cut 0, nothing accepted), and with cut_at_remaining it replaces
 // `needed`.
+
 __global__ void __launch_bounds__(1024) k_mc_scan(const int32_t *__restrict__ block_count, int nb,
                                                   const uint8_t *__restrict__ flag, long long m, long long needed,
                                                   const long long *__restrict__ remaining, int cut_at_remaining,
                                                   long long *__restrict__ block_off, RoundCtl *__restrict__ ctl) {
-    if (remaining) {
-        const long long rem = *remaining;
-        if (rem <= 0) {
-            if (threadIdx.x == 0) {
-                ctl->cut = 0;
-                ctl->n_acc = 0;
-            }
-            return;
-        }
-        if (cut_at_remaining) needed = rem;
-    }
-    __shared__ long long wsum[32];
-    __shared__ long long running_s;
-    __shared__ int cut_block_s;
-    __shared__ long long cut_off_s;
-    if (threadIdx.x == 0) {
-        running_s = 0;
-        cut_block_s = -1;
-        cut_off_s = 0;
-    }
-    __syncthreads();
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int base = 0; base < nb; base += 1024) {
-        const int i = base + threadIdx.x;
-        const long long c = i < nb ? block_count[i] : 0;
-        long long incl = c;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const long long t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
-        }
-        if (lane == 31) wsum[w] = incl;
-        __syncthreads();
-        if (w == 0) {
-            long long v = wsum[lane];
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const long long t = __shfl_up_sync(0xffffffffu, v, o);
-                if (lane >= o) v += t;
-            }
-            wsum[lane] = v;  // inclusive warp totals
-        }
-        __syncthreads();
-        const long long warp_excl = w > 0 ? wsum[w - 1] : 0;
-        const long long off = running_s + warp_excl + incl - c;
-        if (i < nb) {
-            block_off[i] = off;
-            if (off < needed && needed <= off + c) {
-                cut_block_s = i;
-                cut_off_s = off;
-            }
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) running_s += wsum[31];
-        __syncthreads();
-    }
-    const long long total = running_s;
-    if (cut_block_s < 0) {
-        if (threadIdx.x == 0) {
-            ctl->cut = m;
-            ctl->n_acc = total;
-        }
-        return;
-    }
-    // position of the r-th accepted point inside the cut block
-    const long long r = needed - cut_off_s;
-    const long long k = static_cast<long long>(cut_block_s) * kFwdBlock + threadIdx.x;
-    int f = 0;
-    if (threadIdx.x < kFwdBlock && k < m) f = flag[k] ? 1 : 0;
-    long long incl = f;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const long long t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-    }
-    __syncthreads();
-    if (lane == 31) wsum[w] = incl;
-    __syncthreads();
-    long long pre = 0;
-    for (int q = 0; q < w; ++q) pre += wsum[q];
-    incl += pre;
-    if (threadIdx.x < kFwdBlock && f && incl == r) {
-        ctl->cut = k + 1;
-        ctl->n_acc = needed;
-    }
+    mc_scan_body(block_count, nb, flag, m, needed, remaining, cut_at_remaining, block_off, ctl);
 }
+
 
 __global__ void __launch_bounds__(kFwdBlock) k_mc_compact(const uint8_t *__restrict__ flag,
                                                           const long long *__restrict__ block_off,
                                                           const RoundCtl *__restrict__ ctl, long long m,
                                                           int32_t *__restrict__ list) {
-    const long long k = blockIdx.x * static_cast<long long>(kFwdBlock) + threadIdx.x;
-    const long long cut = ctl->cut;
-    const int a = (k < m && k < cut) ? flag[k] : 0;
-    const unsigned ballot = __ballot_sync(0xffffffffu, a);
-    __shared__ int wc[kFwdBlock / 32];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    if (lane == 0) wc[w] = __popc(ballot);
-    __syncthreads();
-    int pre = 0;
-    for (int q = 0; q < w; ++q) pre += wc[q];
-    if (a) {
-        const long long pos = block_off[blockIdx.x] + pre + __popc(ballot & ((1u << lane) - 1u));
-        list[pos] = static_cast<int32_t>(k);
-    }
+    mc_compact_block(flag, block_off, ctl, m, list, blockIdx.x);
 }
 
 // The expensive pass: combined weight and integrand of every PreProcess-

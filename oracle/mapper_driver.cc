@@ -12,8 +12,9 @@
 //
 // Output lines:
 //   MAP ch npts gen_max gen_p99 wgt_max wgt_p99 rans_max nan_mismatch
-//       relative differences GPU vs FSMapper per channel: momenta of
-//       GeneratePoint, weights and in/out uniform buffers of GenerateWeight
+//       differences GPU vs FSMapper per channel: GeneratePoint momenta
+//       (relative to each leg's energy), GenerateWeight weights (relative)
+//       and its in/out uniform buffers (relative)
 //   ITER k n mean_stock mean_gpu var_stock var_gpu
 //       one MultiChannel::operator() each (same seed, no adaptation)
 //   SAVE ok            the GPU mappers' MultiChannel::SaveAs loads back
@@ -160,11 +161,16 @@ int main(int argc, char **argv) {
                 std::vector<FourVector> ms, mg;
                 stock.GeneratePoint(ms, x);
                 gpu.GeneratePoint(mg, x);
-                for (size_t k = 0; k < ms.size(); ++k)
+                // component differences relative to the leg's energy (a
+                // component near zero has no relative precision of its own)
+                for (size_t k = 0; k < ms.size(); ++k) {
+                    const bool e_ok = !std::isnan(ms[k][0]);
+                    const double scale = e_ok ? std::max(std::abs(ms[k][0]), 1e-300) : 1.0;
                     for (size_t q = 0; q < 4; ++q) {
                         if (std::isnan(ms[k][q]) != std::isnan(mg[k][q])) ++nan_mismatch;
-                        else dg.push_back(rel(mg[k][q], ms[k][q]));
+                        else if (e_ok && !std::isnan(ms[k][q])) dg.push_back(std::abs(mg[k][q] - ms[k][q]) / scale);
                     }
+                }
                 if (std::isnan(ms[0][0])) continue;
                 // in/out uniform buffers that start alike with values the map may leave
                 std::vector<double> rs(stock.NDims()), rg;

@@ -109,17 +109,29 @@ def test_camel_tasks_match_the_oracle(ctx_factory):
     assert info.block in (128, 256) and info.points_per_thread in (1, 2, 4)
 
 
-@pytest.mark.parametrize("phased", [1, 0])
-def test_multichannel_tasks_match_the_oracle(ctx_factory, phased):
-    """Both weight passes of the batched multichannel tasks: the phased one
-    (task chains of the shared-entry kernels, the default) and every point
-    in one thread of the persistent kernel (option batch_phased 0)."""
+@pytest.mark.parametrize("mode", ["grouped", "grouped_small_waves", "task_chains", "one_kernel"])
+def test_multichannel_tasks_match_the_oracle(ctx_factory, mode):
+    """Every weight pass of the batched multichannel tasks: the phased pass
+    in waves of pieces, one launch per step and wave (the default; with
+    waves of 2^16 points the tasks are cut into several pieces and the
+    pieces spread over several waves), the phased pass as one chain of
+    launches per task tile (option batch_grouped 0), and every point in one
+    thread of the persistent kernel (option batch_phased 0)."""
     # the 2->4 task spans two phased tiles (2^18 points each)
     tasks = [mc_task(2, 500.0, 20000, 20), mc_task(3, 1500.0, 5000, 30), mc_task(4, 1000.0, 265000, 25, cuts=True),
              mc_task(5, 800.0, 20000, 15)]
     ctx = ctx_factory()
-    ctx.set_option("batch_phased", phased)
+    if mode == "grouped_small_waves":
+        ctx.set_option("batch_wave_points", 1 << 16)
+    ctx.set_option("batch_grouped", 0 if mode == "task_chains" else 1)
+    ctx.set_option("batch_phased", 0 if mode == "one_kernel" else 1)
     run_and_check(ctx, tasks, seed=11, iterations=2)
+    l0 = ctx.launches
+    ctx.batch_iterate(1, seed=11, adapt=True)
+    launches = ctx.launches - l0
+    if mode.startswith("grouped"):
+        # a handful of launches per wave, not a chain per task tile
+        assert launches < (30 if mode == "grouped" else 200), launches
 
 
 def test_mixed_batch_matches_the_oracle(ctx_factory):

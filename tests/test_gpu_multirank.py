@@ -10,8 +10,9 @@ in the host-side collective between iterations.
 
 After every iteration both ranks hold identical grids and channel weights,
 and they equal one process that ran both counter ranges on one context
-(training deferred), summed the two packed buffers and trained once:
-bit for bit, since a sum of two values does not depend on the order."""
+(training deferred), summed the two packed buffers and trained once: counts
+exactly, sums, grids and channel weights to the rounding of the partial-sum
+folds (each context chunks its points after its own acceptance history)."""
 import os
 import socket
 
@@ -102,8 +103,12 @@ def test_two_library_ranks_equal_one_process(tmp_path):
         ctx.synchronize()
         s = tot.cpu().numpy()
         m = r0["merged"][k]
-        assert m[0] == s[nh + ctx.nch] and m[3] == s[nh + ctx.nch + 1] and m[4] == s[nh + ctx.nch + 2]
+        # counts exact; the sums agree to the order of the partial-sum folds
+        # (the chunking follows each context's own acceptance history)
+        assert m[0] == s[nh + ctx.nch]
+        assert abs(m[3] - s[nh + ctx.nch + 1]) <= 1e-12 * abs(m[3])
+        assert abs(m[4] - s[nh + ctx.nch + 2]) <= 1e-12 * abs(m[4])
     a, b, md = ctx.get_alpha()
-    assert np.array_equal(a, r0["alpha"]) and np.array_equal(b, r0["best"])
-    assert np.array_equal(ctx.get_grids(), r0["grids"])
+    assert np.allclose(a, r0["alpha"], rtol=1e-10, atol=0) and np.allclose(b, r0["best"], rtol=1e-10, atol=0)
+    assert np.allclose(ctx.get_grids(), r0["grids"], rtol=1e-10, atol=1e-14)
     ctx.close()
