@@ -812,10 +812,13 @@ def run_reference(args, rank, world):
 # --------------------------------------------------------- plain VEGAS workload
 VEGAS_METRIC = "VEGAS points/s and time to 0.1% error, 4-d camel (50 bins, alpha 1.5, 1e5 points/iteration), FP64"
 VEGAS_UNIT = "points/s"
-# FP64 operations (2*DFMA + DADD + DMUL, executed) per point of the fused
-# iteration kernel, from the committed ncu capture of the 1e5-point
-# iteration (profiles/vegas_camel_kernels.md)
-VEGAS_COUNTERS = {"k_vegas_iter": None}
+# FP64 operations (2*DFMA + DADD + DMUL, executed) per point of the point
+# loop the iteration kernels share (k_vegas_iter, and k_vegas_step, which
+# adds the last block's fold and adaptation: O(dims * bins) once per
+# iteration), and DRAM bytes per launch, from the committed ncu capture of
+# the 1e5-point iteration (profiles/vegas_camel_kernels.md)
+VEGAS_COUNTERS = {"fp64_ops_per_point": 180.1, "dram_bytes_per_launch": 32.5e3,
+                  "source": "profiles/vegas_camel_kernels.md"}
 
 
 def vegas_config(cfg):
@@ -882,7 +885,11 @@ def run_vegas(args, rank, world, local_rank):
             counter += n
         torch.cuda.synchronize(dev)
     launches = ctx.launches - l0
-    kms, kl = ctx.kernel_time("k_vegas_iter")
+    kname = "k_vegas_step"
+    kms, kl = ctx.kernel_time(kname)
+    if kl == 0:  # the iteration ran as separate point, fold and adaptation kernels
+        kname = "k_vegas_iter"
+        kms, kl = ctx.kernel_time(kname)
     ctx.set_option("kernel_timing", 0)
     ms = sum(a.elapsed_time(b) for a, b in evs)
     t = torch.tensor([ms], dtype=torch.float64, device=dev)
@@ -892,18 +899,17 @@ def run_vegas(args, rank, world, local_rank):
     st = stats_dev[args.warmup:].cpu().numpy()
     pooled = (st * np.array([1, 0, 0, 1, 1, 1])).sum(axis=0)
     mean, err = gpu.stats_mean_error(pooled)
-    c = VEGAS_COUNTERS.get("k_vegas_iter")
+    c = VEGAS_COUNTERS
     peak = fp64_peak_tflops(dev)
-    roof = {"kernel": "k_vegas_iter", "bound": "fp64", "launches": kl, "ms_per_launch": kms / max(kl, 1),
+    roof = {"kernel": kname, "bound": "fp64", "launches": kl, "ms_per_launch": kms / max(kl, 1),
             "share_of_step": kms / ms, "peak": peak, "unit": "TFLOP/s",
-            "peak_source": "cuBLAS DGEMM 8192^3 measured in this run"}
-    if c:
-        roof.update(achieved=c["fp64_ops_per_point"] * n * kl / (kms / 1e3) / 1e12,
-                    fp64_ops_per_point=c["fp64_ops_per_point"], counters_source=c["source"],
-                    traffic=c.get("dram_bytes_per_launch"))
-        roof["frac"] = roof["achieved"] / peak
-    else:
-        roof.update(achieved=None, frac=None, traffic=None)
+            "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+            "achieved": c["fp64_ops_per_point"] * n * kl / (kms / 1e3) / 1e12 if kl else None,
+            "fp64_ops_per_point": c["fp64_ops_per_point"], "counters_source": c["source"],
+            "traffic": c["dram_bytes_per_launch"], "algorithmic_bytes": 0,
+            "note": "fused mode: uniforms drawn in the kernel, grid and histogram in L1/shared memory; "
+                    "a 1e5-point launch is latency-bound (see materialised for the HBM-bound form)"}
+    roof["frac"] = roof["achieved"] / peak if roof["achieved"] else None
 
     mat = vegas_materialised(ctx, dev, stream, cfg, n=args.gen_points)
     t01 = None if args.no_t01 else vegas_time_to_target(ctx, cfg, params, seed + 17, dev)
@@ -953,12 +959,17 @@ def vegas_materialised(ctx, dev, stream, cfg, n=100_000_000, reps=10):
                          "unit": "GB/s", "frac": achieved / hbm if hbm else None,
                          "algorithmic_bytes_per_point": b,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured copy bandwidth)",
-                         "traffic": VEGAS_GEN_TRAFFIC}}
+                         "traffic": vegas_gen_traffic(n),
+                         "traffic_source": "profiles/vegas_camel_kernels.md (40 B/point less the L2-resident "
+                                           "tail, from captures at 4e6 and 2.5e7 points)"}}
 
 
-# DRAM bytes (read + write) per point of k_vegas_generate from the committed
-# ncu capture (profiles/vegas_camel_kernels.md), or None
-VEGAS_GEN_TRAFFIC = None
+# DRAM bytes of a k_vegas_generate launch of n points, from the committed
+# ncu captures at 4e6 and 2.5e7 points (profiles/vegas_camel_kernels.md):
+# 40 B per point written, less the ~60 MB of the output still in L2 when
+# the kernel ends (99.9 MB and 939.5 MB measured)
+def vegas_gen_traffic(n):
+    return 40.0 * n - 60.1e6
 
 
 def vegas_time_to_target(ctx, cfg, params, seed, dev, target=1e-3, max_iter=4000):

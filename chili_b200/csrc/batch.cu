@@ -44,6 +44,9 @@ namespace {
 constexpr int kBatchMaxCh = 64;
 // Parallel branches of the phased multichannel task chains in the graph.
 constexpr int kPhBranches = 8;
+// Grouped mode: waves on two streams, so that one wave's tail overlaps the
+// next one's start.
+constexpr int kWaveStreams = 2;
 
 struct BatchTask {
     int32_t kind, dims, bins, nch;
@@ -458,7 +461,8 @@ __global__ void __launch_bounds__(128) k_g_channel(WaveDev W, int lo, int hi, lo
     const int c = static_cast<int>(lb % P.nch);
     const long long i = (lb / P.nch) * 128 + threadIdx.x;
     if (i < P.ms && i < P.ctl->n_acc)
-        pp_channel_point<DIMS, false>(P.pp, P.grids, nullptr, nullptr, nullptr, P.bins, P.memo, P.cfail, P.ich_tile,
+        pp_channel_point<DIMS, false>(P.pp, P.grids, nullptr, nullptr, nullptr, P.bins, P.memo, P.cfail,
+                                      P.ich_tile,
                                       P.ms, P.ms, 1, P.dcv, P.vwv, P.slot, P.dens, i, i, c);
 }
 
@@ -595,7 +599,8 @@ struct BatchState {
     std::vector<Piece> pieces;
     std::vector<WaveHost> waves;
     std::vector<long long> prefix_host;
-    DevBuf d_pieces, d_prefix, d_arena;
+    DevBuf d_pieces, d_prefix;
+    DevBuf d_arena[2];  // wave w uses arena w % 2 and stream w % 2
     bool tuned = false;
     cudaGraphExec_t graph = nullptr;
     unsigned long long graph_launches = 0;  // kernels of one replay
@@ -739,7 +744,10 @@ int enqueue_phased_task(chili_ctx *ctx, const BatchDev &B, int ti, BatchState::P
 // step and wave.
 int enqueue_waves(chili_ctx *ctx, const BatchDev &B) {
     BatchState &S = *ctx->batch;
-    for (const auto &w : S.waves) {
+    const cudaStream_t caller = ctx->stream;
+    for (size_t wi = 0; wi < S.waves.size(); ++wi) {
+        const auto &w = S.waves[wi];
+        ctx->stream = S.ph_streams[wi % kWaveStreams];  // the wave's arena belongs to this stream
         const WaveDev W{S.d_pieces.as<Piece>() + w.first, w.n, S.d_prefix.as<long long>() + w.prefix_off};
         const long long *pre = S.prefix_host.data() + w.prefix_off;
         auto blocks = [&](int step) { return static_cast<unsigned>(w.blocks[static_cast<size_t>(step)]); };
@@ -788,6 +796,7 @@ int enqueue_waves(chili_ctx *ctx, const BatchDev &B) {
         k_g_accum<<<blocks(GS_ACCUM), kFwdBlock, 0, ctx->stream>>>(B, W, 0, w.n, 0);
         LAUNCHED();
     }
+    ctx->stream = caller;
     return CHILI_OK;
 }
 
@@ -799,17 +808,18 @@ int enqueue_iteration(chili_ctx *ctx, bool adapt) {
     BatchDev B = batch_dev(ctx);
     const cudaStream_t main = ctx->stream;
     if (S.grouped && !S.waves.empty()) {
-        // the waves on a second stream beside the camel tasks' evaluation
-        CK(cudaEventRecord(S.ph_events[1], main));
-        CK(cudaStreamWaitEvent(S.ph_streams[0], S.ph_events[1], 0));
+        // the waves on their streams beside the camel tasks' evaluation
+        CK(cudaEventRecord(S.ph_events[kWaveStreams], main));
+        for (int j = 0; j < kWaveStreams; ++j) CK(cudaStreamWaitEvent(S.ph_streams[j], S.ph_events[kWaveStreams], 0));
         k_batch_eval<<<S.grid_blocks, S.block, 0, ctx->stream>>>(B);
         LAUNCHED();
-        ctx->stream = S.ph_streams[0];
         const int rc = enqueue_waves(ctx, B);
         ctx->stream = main;
         if (rc) return rc;
-        CK(cudaEventRecord(S.ph_events[0], S.ph_streams[0]));
-        CK(cudaStreamWaitEvent(main, S.ph_events[0], 0));
+        for (int j = 0; j < kWaveStreams; ++j) {
+            CK(cudaEventRecord(S.ph_events[j], S.ph_streams[j]));
+            CK(cudaStreamWaitEvent(main, S.ph_events[j], 0));
+        }
     } else {
     if (!S.ph.empty()) CK(cudaEventRecord(S.ph_events[kPhBranches], main));
     k_batch_eval<<<S.grid_blocks, S.block, 0, ctx->stream>>>(B);
@@ -974,21 +984,22 @@ int plan_waves(chili_ctx *ctx, const std::vector<PointProgram> &pps) {
                             sizeof(double) * ms, ms, sizeof(int32_t) * PP.ndims * ms, sizeof(double) * PP.nch * ms};
         for (int q = 0; q < 18; ++q) out[q] = (v[q] + 255) / 256 * 256;
     };
-    size_t arena = 256;
-    for (auto &w : waves) {
+    size_t arena[kWaveStreams] = {256, 256};
+    for (size_t wi = 0; wi < waves.size(); ++wi) {
         size_t tot = 0;
-        for (const Piece &P : w) {
+        for (const Piece &P : waves[wi]) {
             size_t sz[18];
             sizes(P, pps[static_cast<size_t>(S.tasks[static_cast<size_t>(P.ti)].pp)], sz);
             for (size_t q : sz) tot += q;
         }
-        arena = std::max(arena, tot);
+        arena[wi % kWaveStreams] = std::max(arena[wi % kWaveStreams], tot);
     }
-    CK(S.d_arena.ensure(arena));
+    for (int j = 0; j < kWaveStreams; ++j) CK(S.d_arena[j].ensure(arena[j]));
     S.pieces.clear();
     S.waves.clear();
     S.prefix_host.clear();
-    for (auto &w : waves) {
+    for (size_t wi = 0; wi < waves.size(); ++wi) {
+        auto &w = waves[wi];
         // pieces of one dimension together
         std::stable_sort(w.begin(), w.end(), [&](const Piece &a, const Piece &b) {
             return S.tasks[static_cast<size_t>(a.ti)].dims < S.tasks[static_cast<size_t>(b.ti)].dims;
@@ -998,7 +1009,7 @@ int plan_waves(chili_ctx *ctx, const std::vector<PointProgram> &pps) {
         wh.n = static_cast<int>(w.size());
         wh.prefix_off = static_cast<long long>(S.prefix_host.size());
         std::vector<std::vector<long long>> pre(kGroupSteps, std::vector<long long>(w.size() + 1, 0));
-        uint8_t *base = S.d_arena.as<uint8_t>();
+        uint8_t *base = S.d_arena[wi % kWaveStreams].as<uint8_t>();
         size_t off = 0;
         for (size_t k = 0; k < w.size(); ++k) {
             Piece &P = w[k];
@@ -1065,10 +1076,12 @@ int plan_waves(chili_ctx *ctx, const std::vector<PointProgram> &pps) {
     CK(cudaMemcpyAsync(S.d_prefix.p, S.prefix_host.data(), sizeof(long long) * S.prefix_host.size(),
                        cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));  // the host vectors are the copies' sources
-    cudaStream_t st;
-    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    S.ph_streams.push_back(st);
-    for (int k = 0; k < 2; ++k) {
+    for (int j = 0; j < kWaveStreams; ++j) {
+        cudaStream_t st;
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        S.ph_streams.push_back(st);
+    }
+    for (int k = 0; k <= kWaveStreams; ++k) {
         cudaEvent_t e;
         CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         S.ph_events.push_back(e);
@@ -1084,7 +1097,8 @@ void batch_release(chili_ctx *ctx) {
     if (S.graph) cudaGraphExecDestroy(S.graph);
     for (DevBuf *b : {&S.d_tasks, &S.d_umap, &S.d_pps, &S.d_progs, &S.d_descs, &S.d_grids, &S.d_grids_new, &S.d_hist,
                       &S.d_atrain, &S.d_alpha, &S.d_best, &S.d_mindiff, &S.d_cp, &S.d_part, &S.d_stats,
-                      &S.d_counters, &S.d_jobs, &S.d_status, &S.d_pieces, &S.d_prefix, &S.d_arena})
+                      &S.d_counters, &S.d_jobs, &S.d_status, &S.d_pieces, &S.d_prefix, &S.d_arena[0],
+                      &S.d_arena[1]})
         b->release();
     for (auto &b : S.ph)
         for (DevBuf *d : {&b.mom, &b.ich, &b.flag, &b.list, &b.bcount, &b.boff, &b.ctl, &b.node, &b.memo, &b.cfail,

@@ -33,6 +33,8 @@ bool pipeline_dims_ok(int d) {
 
 namespace {
 
+int rebuild_hints(chili_ctx *ctx);
+
 template <int D>
 void launch_channel(chili_ctx *ctx, long long base, long long T, long long mr, int bins, int opt,
                     const long long *n_list, int32_t *rec_slot, double *rec_dens, const PPCombine *fuse) {
@@ -47,9 +49,9 @@ void launch_channel(chili_ctx *ctx, long long base, long long T, long long mr, i
     }
     k_pp_channel<D><<<grid, 128, 0, ctx->stream>>>(
         ctx->point_prog.as<PointProgram>(), ctx->edges.as<double>(), ctx->hints.as<uint32_t>(),
-        ctx->sorted.as<uint8_t>(), ctx->widths.as<double>(), bins, ctx->memo.as<double>(), ctx->cfail.as<uint8_t>(),
-        ctx->ich_tile.as<int32_t>(), n_list, base, T, mr, opt, ctx->dcv.as<double>(), ctx->vwv.as<double>(), rec_slot,
-        rec_dens);
+        ctx->sorted.as<uint8_t>(), ctx->widths.as<double>(), bins, ctx->memo.as<double>(),
+        ctx->cfail.as<uint8_t>(), ctx->ich_tile.as<int32_t>(), n_list, base, T, mr, opt, ctx->dcv.as<double>(),
+        ctx->vwv.as<double>(), rec_slot, rec_dens);
 }
 
 }  // namespace
@@ -63,6 +65,8 @@ void launch_channel(chili_ctx *ctx, long long base, long long T, long long mr, i
 int pipeline_run(chili_ctx *ctx, const double *mom_soa, long long m, const int32_t *list, const int32_t *ich,
                  const long long *n_list, long long n_pre, int bins, bool opt, int32_t *rec_slot, double *rec_dens,
                  const TileFn &combine, const PPFusedOut *fused) {
+    if (ctx->hints_stale)
+        if (int rc = rebuild_hints(ctx)) return rc;
     const PointProgram &P = ctx->pp_host;
     const PointProgram *pp = ctx->point_prog.as<PointProgram>();
     // gridDim.y (point blocks of 128) stays below 65536
@@ -163,12 +167,12 @@ int pp_pass_launch(chili_ctx *ctx, const PPPass &a) {
     case D:                                                                                                  \
         if (a.hints)                                                                                         \
             k_pp_channel<D, true><<<gc, 128, 0, ctx->stream>>>(                                              \
-                a.pp, a.grids, a.hints, a.sorted, a.widths, a.bins, a.memo, a.cfail, a.ich_tile, a.n_list, 0, T, \
-                a.mr, 1, a.dcv, a.vwv, a.rec_slot, a.rec_dens);                                              \
+                a.pp, a.grids, a.hints, a.sorted, a.widths, a.bins, a.memo, a.cfail, a.ich_tile, a.n_list,        \
+                0, T, a.mr, 1, a.dcv, a.vwv, a.rec_slot, a.rec_dens);                                        \
         else                                                                                                 \
             k_pp_channel<D, false><<<gc, 128, 0, ctx->stream>>>(                                             \
-                a.pp, a.grids, a.hints, a.sorted, a.widths, a.bins, a.memo, a.cfail, a.ich_tile, a.n_list, 0, T, \
-                a.mr, 1, a.dcv, a.vwv, a.rec_slot, a.rec_dens);                                              \
+                a.pp, a.grids, a.hints, a.sorted, a.widths, a.bins, a.memo, a.cfail, a.ich_tile,              \
+                a.n_list, 0, T, a.mr, 1, a.dcv, a.vwv, a.rec_slot, a.rec_dens);                              \
         break;
         CHILI_CH(1) CHILI_CH(4) CHILI_CH(7) CHILI_CH(10) CHILI_CH(13) CHILI_CH(16) CHILI_CH(19) CHILI_CH(22)
 #undef CHILI_CH
@@ -265,6 +269,7 @@ int launch_pipeline(chili_ctx *ctx, const double *mom_soa, const int32_t *ich, l
 // Hint tables of the grid set (grid.cuh, find_bin_hinted), rebuilt after
 // every change of the edges.
 int rebuild_hints(chili_ctx *ctx) {
+    ctx->hints_stale = false;
     const int H = kHintPerBin * ctx->bins;
     CK(ctx->hints.ensure(sizeof(uint32_t) * static_cast<size_t>(ctx->g_nch) * ctx->dims * H));
     CK(ctx->sorted.ensure(static_cast<size_t>(ctx->g_nch) * ctx->dims));
@@ -327,7 +332,8 @@ int chili_gpu_destroy(chili_ctx *ctx) {
                       &ctx->ich, &ctx->flag, &ctx->list, &ctx->block_count, &ctx->block_off, &ctx->part,
                       &ctx->hist, &ctx->round_res, &ctx->acc, &ctx->ctl, &ctx->status, &ctx->v_part,
                       &ctx->v_hist, &ctx->v_train, &ctx->v_out, &ctx->rec, &ctx->ctl3, &ctx->unw, &ctx->iter_ctl,
-                      &ctx->mom_soa_alt, &ctx->ich_alt, &ctx->flag_alt, &ctx->block_count_alt, &ctx->arrivals};
+                      &ctx->mom_soa_alt, &ctx->ich_alt, &ctx->flag_alt, &ctx->block_count_alt, &ctx->arrivals,
+                      &ctx->v_arrive};
     for (DevBuf *b : bufs) b->release();
     flow_release(ctx);
     batch_release(ctx);
@@ -400,6 +406,10 @@ int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value) {
     if (!ctx || !name) return fail(ctx, CHILI_ERR_INVALID_ARG, "NULL argument");
     if (std::strcmp(name, "point_program") == 0) {
         ctx->use_pp = value != 0;
+        return CHILI_OK;
+    }
+    if (std::strcmp(name, "vegas_fused") == 0) {
+        ctx->vegas_fused = value != 0;
         return CHILI_OK;
     }
     if (std::strcmp(name, "vegas_gen_ppt") == 0) {
@@ -523,6 +533,8 @@ int chili_gpu_grid_weight(chili_ctx *ctx, int ch, const double *x, double *w, in
     if ((rc = resolve(ctx, x, sizeof(double) * n * D, 0, true, ax))) return rc;
     if ((rc = resolve(ctx, w, sizeof(double) * n, 1, false, aw))) return rc;
     if ((rc = resolve(ctx, bin, sizeof(int32_t) * n * D, 2, false, ab))) return rc;
+    if (ctx->hints_stale)
+        if ((rc = rebuild_hints(ctx))) return rc;
     const double *g = ctx->edges.as<double>() + static_cast<size_t>(ch) * D * (B + 1);
     const uint32_t *hg = ctx->hints.as<uint32_t>() + static_cast<size_t>(ch) * D * (kHintPerBin * B);
     const uint8_t *sg = ctx->sorted.as<uint8_t>() + static_cast<size_t>(ch) * D;
@@ -658,6 +670,52 @@ int chili_gpu_vegas_iterate(chili_ctx *ctx, uint64_t ncalls, uint64_t seed, uint
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
     const size_t hist_bytes = sizeof(double) * nh;
     const bool smem = hist_bytes <= 48 * 1024;
+    if (smem && adapt && ctx->vegas_fused && ctx->g_nch == 1 &&
+        sizeof(double) * B * (kVegasBlock / 32) <= 48 * 1024) {
+        // the whole iteration in one launch (k_vegas_step): points, a
+        // two-level ordered fold and the adaptation
+        const long long nb = std::min<long long>(grid_for(n, kVegasBlock), static_cast<long long>(sms) * 4);
+        const long long ngrp = (nb + kStepGroup - 1) / kStepGroup;
+        CK(ctx->v_part.ensure(sizeof(double) * 6 * (nb + ngrp)));
+        CK(ctx->v_hist.ensure(hist_bytes * (nb + ngrp)));
+        CK(ctx->v_train.ensure(hist_bytes));
+        CK(ctx->v_out.ensure(sizeof(double) * 6));
+        CK(ctx->status.ensure(sizeof(int)));
+        const size_t arrive_bytes = sizeof(unsigned) * (1 + ngrp);
+        if (ctx->v_arrive.cap < arrive_bytes) {
+            CK(ctx->v_arrive.ensure(arrive_bytes));
+            CK(cudaMemsetAsync(ctx->v_arrive.p, 0, ctx->v_arrive.cap, ctx->stream));
+        }
+        CK(ctx->edges_tmp.ensure(sizeof(double) * D * (B + 1)));
+        using StepKernel = void (*)(const double *, double *, int, int, uint64_t, uint64_t, const double *, long long,
+                                    const IntegrandDesc *, double *, double *, double *, double *, double *, double *,
+                                    double, int, unsigned *, int *);
+        StepKernel kern = k_vegas_step<0>;
+        switch (D) {
+#define CHILI_ST(d) \
+    case d: kern = k_vegas_step<d>; break;
+            CHILI_ST(1) CHILI_ST(2) CHILI_ST(3) CHILI_ST(4) CHILI_ST(5) CHILI_ST(6) CHILI_ST(7) CHILI_ST(8)
+            CHILI_ST(10) CHILI_ST(12) CHILI_ST(16)
+#undef CHILI_ST
+            default: break;
+        }
+        double *train_dev = train_out ? static_cast<double *>(atr.dev) : ctx->v_train.as<double>();
+        double *out_dev = stats_out ? static_cast<double *>(ast.dev) : ctx->v_out.as<double>();
+        {
+            KTimer kt_(ctx, KT_VEGAS_STEP);
+            kern<<<static_cast<unsigned>(nb), kVegasBlock,
+                   std::max(hist_bytes, sizeof(double) * B * (kVegasBlock / 32)), ctx->stream>>>(
+                ctx->edges.as<double>(), ctx->edges_tmp.as<double>(), D, B, seed, counter_base,
+                static_cast<const double *>(au.dev), n, ctx->f_dev.as<IntegrandDesc>(), ctx->v_part.as<double>(),
+                ctx->v_hist.as<double>(), ctx->v_part.as<double>() + 6 * nb, ctx->v_hist.as<double>() + nh * nb,
+                train_dev, out_dev, alpha, 1, ctx->v_arrive.as<unsigned>(), ctx->status.as<int>());
+        }
+        LAUNCHED();
+        std::swap(ctx->edges, ctx->edges_tmp);
+        ctx->hints_stale = true;  // rebuilt where a bin search uses them
+        if ((rc = finish_out(ctx, ast)) || (rc = finish_out(ctx, atr))) return rc;
+        return sync_if_host(ctx, {&au, &ast, &atr});
+    }
     long long nblocks = std::min<long long>(grid_for(n, kVegasBlock), static_cast<long long>(sms) * 4);
     CK(ctx->v_part.ensure(sizeof(double) * 6 * nblocks));
     CK(ctx->v_hist.ensure(smem ? hist_bytes * nblocks : hist_bytes));

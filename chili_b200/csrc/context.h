@@ -134,6 +134,8 @@ struct chili_ctx {
     bool use_pipeline = true;  // option "pipeline": phased weight pass
     bool fuse_combine = false;  // option "pipeline_fuse": combine step inside the channel kernel (slower: off)
     long long gen_ppt = 2;       // option "vegas_gen_ppt": points per thread of chili_gpu_vegas_generate
+    bool vegas_fused = true;     // option "vegas_fused": a whole adapting Vegas iteration in one launch
+    bool hints_stale = false;    // the grids changed since the hint tables were built
     bool defer_train = false;  // option "defer_train": iterations collect training data, Train is the caller's
     bool batch_phased = true;  // option "batch_phased": batched multichannel tasks by the phased weight pass
     bool batch_grouped = true;  // option "batch_grouped": the phased tasks in waves, one launch per step and wave
@@ -143,6 +145,7 @@ struct chili_ctx {
     PointProgram pp_host;      // host copy (sizes of the memo buffers)
     DevBuf node_soa, memo, cfail, dcv, vwv;
     DevBuf arrivals;  // per point block of a tile: the fused combine's arrival counters (zero between launches)
+    DevBuf v_arrive;  // the fused Vegas iteration's arrival counter (zero between launches)
     DevBuf hints, sorted, widths;  // hinted bin search tables and bin widths of the grids
     DevBuf ich_tile;
     // channel weights: alpha[CH], best[CH], cp[CH], min_diff
@@ -199,9 +202,10 @@ namespace {
 const char *const kTimedKernels[] = {"k_mc_forward", "k_pp_nodes", "k_pp_items", "k_pp_chains", "k_pp_channel",
                                      "k_pp_combine", "k_mc_weight", "k_mc_accum", "k_vegas_iter", "k_flow_layer",
                                      "k_flow_layer_bwd", "k_flow_wgrad", "k_alpha_train", "k_flow_phys",
-                                     "k_flow_batch", "k_vegas_generate", nullptr};
+                                     "k_flow_batch", "k_vegas_generate", "k_vegas_step", nullptr};
 enum { KT_FORWARD, KT_NODES, KT_ITEMS, KT_CHAINS, KT_CHANNEL, KT_COMBINE, KT_WEIGHT, KT_ACCUM, KT_VEGAS,
-       KT_FLOW_LAYER, KT_FLOW_BWD, KT_FLOW_WGRAD, KT_ALPHA_TRAIN, KT_FLOW_PHYS, KT_FLOW_BATCH, KT_VEGAS_GEN };
+       KT_FLOW_LAYER, KT_FLOW_BWD, KT_FLOW_WGRAD, KT_ALPHA_TRAIN, KT_FLOW_PHYS, KT_FLOW_BATCH, KT_VEGAS_GEN,
+       KT_VEGAS_STEP };
 
 cudaEvent_t take_event(chili_ctx *ctx) {
     if (!ctx->event_pool.empty()) {

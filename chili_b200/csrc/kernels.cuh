@@ -144,9 +144,10 @@ __global__ void k_grid_split(const double *__restrict__ g_old, double *__restric
 // DIMS > 0: the dimension fixed at compile time (coordinates in registers);
 // DIMS == 0: `dims` at run time (a local array).
 template <int DIMS>
-__global__ void k_vegas_iter(const double *__restrict__ g, int dims_rt, int bins, uint64_t seed, uint64_t ctr0,
-                             const double *__restrict__ u_in, long long n, const IntegrandDesc *__restrict__ f,
-                             double *__restrict__ part, double *__restrict__ hist, int smem_hist) {
+__device__ __forceinline__ void vegas_points(const double *__restrict__ g, int dims_rt, int bins, uint64_t seed,
+                                             uint64_t ctr0, const double *__restrict__ u_in, long long n,
+                                             const IntegrandDesc *__restrict__ f, double *__restrict__ part,
+                                             double *__restrict__ hist, int smem_hist) {
     extern __shared__ double sh[];
     const int dims = DIMS > 0 ? DIMS : dims_rt;
     const int nh = dims * bins;
@@ -206,6 +207,13 @@ __global__ void k_vegas_iter(const double *__restrict__ g, int dims_rt, int bins
         double *dst = hist + static_cast<size_t>(blockIdx.x) * nh;
         for (int k = threadIdx.x; k < nh; k += blockDim.x) dst[k] = sh[k];
     }
+}
+
+template <int DIMS>
+__global__ void k_vegas_iter(const double *__restrict__ g, int dims_rt, int bins, uint64_t seed, uint64_t ctr0,
+                             const double *__restrict__ u_in, long long n, const IntegrandDesc *__restrict__ f,
+                             double *__restrict__ part, double *__restrict__ hist, int smem_hist) {
+    vegas_points<DIMS>(g, dims_rt, bins, seed, ctr0, u_in, n, f, part, hist, smem_hist);
 }
 
 // Materialised VEGAS points on the camel: point i's uniforms (the counter
@@ -288,13 +296,16 @@ __global__ void __launch_bounds__(kGenTile) k_vegas_generate(const double *__res
 }
 
 // Ordered fold of k_vegas_iter's partials: stats into out6, histogram
-// partials (when per block) into train[dims*bins].
-__global__ void k_vegas_finalize(const double *__restrict__ part, int nblocks, const double *__restrict__ hist_part,
-                                 int per_block_hist, int nh, double *__restrict__ train, double *__restrict__ out6) {
+// partials (when per block) into train[dims*bins].  The partials are read
+// from L2 (__ldcg): in k_vegas_step other blocks of the same launch wrote
+// them.
+__device__ __forceinline__ void vegas_fold(const double *part, int nblocks, const double *hist_part,
+                                           int per_block_hist, int nh, double *__restrict__ train,
+                                           double *__restrict__ out6) {
     if (per_block_hist) {
         for (int k = threadIdx.x; k < nh; k += blockDim.x) {
             double s = 0;
-            for (int b = 0; b < nblocks; ++b) s += hist_part[static_cast<size_t>(b) * nh + k];
+            for (int b = 0; b < nblocks; ++b) s += __ldcg(hist_part + static_cast<size_t>(b) * nh + k);
             train[k] = s;
         }
     }
@@ -303,20 +314,109 @@ __global__ void k_vegas_finalize(const double *__restrict__ part, int nblocks, c
                csum2 = 0, nf = 0;
         for (int b = 0; b < nblocks; ++b) {
             const double *p = part + b * 6;
-            n += p[0];
-            mn = std_min(mn, p[1]);
-            mx = std_max(mx, p[2]);
-            double y = p[3] - csum, t = sum + y;  // Kahan
+            n += __ldcg(p);
+            mn = std_min(mn, __ldcg(p + 1));
+            mx = std_max(mx, __ldcg(p + 2));
+            double y = __ldcg(p + 3) - csum, t = sum + y;  // Kahan
             csum = (t - sum) - y;
             sum = t;
-            y = p[4] - csum2;
+            y = __ldcg(p + 4) - csum2;
             t = sum2 + y;
             csum2 = (t - sum2) - y;
             sum2 = t;
-            nf += p[5];
+            nf += __ldcg(p + 5);
         }
         out6[0] = n; out6[1] = mn; out6[2] = mx; out6[3] = sum; out6[4] = sum2; out6[5] = nf;
     }
+}
+
+__global__ void k_vegas_finalize(const double *__restrict__ part, int nblocks, const double *__restrict__ hist_part,
+                                 int per_block_hist, int nh, double *__restrict__ train, double *__restrict__ out6) {
+    vegas_fold(part, nblocks, hist_part, per_block_hist, nh, train, out6);
+}
+
+// Ordered fold of the partials of blocks [b0, b1) (StatsData with Kahan sums,
+// histogram bin by bin) into one partial: out6 and out_hist[nh].  The
+// partials were written by other blocks of the same launch: read from L2.
+__device__ __forceinline__ void vegas_fold_range(const double *part, const double *hist_part, int b0, int b1, int nh,
+                                                 double *__restrict__ out_hist, double *__restrict__ out6) {
+    for (int k = threadIdx.x; k < nh; k += blockDim.x) {
+        double s = 0;
+        for (int b = b0; b < b1; ++b) s += __ldcg(hist_part + static_cast<size_t>(b) * nh + k);
+        out_hist[k] = s;
+    }
+    if (threadIdx.x == 0) {
+        double n = 0, mn = 1.7976931348623157e308, mx = 2.2250738585072014e-308, sum = 0, csum = 0, sum2 = 0,
+               csum2 = 0, nf = 0;
+        for (int b = b0; b < b1; ++b) {
+            const double *p = part + b * 6;
+            n += __ldcg(p);
+            mn = std_min(mn, __ldcg(p + 1));
+            mx = std_max(mx, __ldcg(p + 2));
+            double y = __ldcg(p + 3) - csum, t = sum + y;  // Kahan
+            csum = (t - sum) - y;
+            sum = t;
+            y = __ldcg(p + 4) - csum2;
+            t = sum2 + y;
+            csum2 = (t - sum2) - y;
+            sum2 = t;
+            nf += __ldcg(p + 5);
+        }
+        out6[0] = n; out6[1] = mn; out6[2] = mx; out6[3] = sum; out6[4] = sum2; out6[5] = nf;
+    }
+}
+
+// One whole Vegas::operator() (Vegas.cc:18-52) in one launch: the points of
+// k_vegas_iter (histogram in shared memory, one partial per block); then,
+// per group of kStepGroup consecutive blocks, the last of them to finish
+// folds the group's partials in block order into a group partial; the last
+// group to be folded folds the group partials in group order, writes the
+// StatsData to out6 and the histogram to train, and runs
+// AdaptiveMap::Adapt (AdaptiveMap.cc:67-125) dimension by dimension from g
+// into g_new.  Arrival counters (arrive[0] for the groups, arrive[1 + group]
+// within a group) are zero between launches and reset by the block that
+// completes them; no block waits for another.  The fixed grouping keeps the
+// sums deterministic.
+constexpr int kStepGroup = 16;
+template <int DIMS>
+__global__ void k_vegas_step(const double *__restrict__ g, double *__restrict__ g_new, int dims_rt, int bins,
+                             uint64_t seed, uint64_t ctr0, const double *__restrict__ u_in, long long n,
+                             const IntegrandDesc *__restrict__ f, double *part, double *hist_part, double *gpart,
+                             double *ghist, double *__restrict__ train, double *__restrict__ out6, double alpha,
+                             int adapt, unsigned *__restrict__ arrive, int *__restrict__ status) {
+    extern __shared__ double sh[];
+    vegas_points<DIMS>(g, dims_rt, bins, seed, ctr0, u_in, n, f, part, hist_part, 1);
+    const int dims = DIMS > 0 ? DIMS : dims_rt;
+    const int nh = dims * bins;
+    const int grp = blockIdx.x / kStepGroup, ngrp = (gridDim.x + kStepGroup - 1) / kStepGroup;
+    const int b0 = grp * kStepGroup, b1 = min(b0 + kStepGroup, static_cast<int>(gridDim.x));
+    __shared__ bool last;
+    __threadfence();  // this block's partials visible before its arrival
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(arrive + 1 + grp, 1u) == static_cast<unsigned>(b1 - b0 - 1);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    vegas_fold_range(part, hist_part, b0, b1, nh, ghist + static_cast<size_t>(grp) * nh, gpart + grp * 6);
+    if (threadIdx.x == 0) arrive[1 + grp] = 0u;
+    __threadfence();  // the group partial visible before the group's arrival
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(arrive, 1u) == static_cast<unsigned>(ngrp - 1);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    vegas_fold_range(gpart, ghist, 0, ngrp, nh, train, out6);
+    __syncthreads();  // train complete (and the points' shared histogram no longer needed)
+    if (adapt) {
+        // one warp per dimension (each with its own bins doubles of shared
+        // memory), the dimensions in rounds of the block's warps
+        if (threadIdx.x == 0) *status = 0;
+        __syncthreads();
+        const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        for (int d = w; d < dims; d += nw) grid_adapt_impl<true>(g, g_new, dims, bins, alpha, train, 0, status, d, 0,
+                                                                 sh + static_cast<size_t>(w) * bins);
+    }
+    if (threadIdx.x == 0) *arrive = 0u;
 }
 
 // ------------------------------------------------------------- channels

@@ -163,11 +163,21 @@ __device__ __forceinline__ void alpha_update(double *__restrict__ alpha, double 
 }
 
 
-// AdaptiveMap::Adapt (AdaptiveMap.cc:67-125) of dimension d of grid c, one
-// block (tmp: bins doubles of shared memory).
-__device__ __forceinline__ void grid_adapt_block(const double *__restrict__ g_old, double *__restrict__ g_new, int dims,
-                                                 int bins, double alpha, const double *__restrict__ train, int skip_zero,
-                                                 int *__restrict__ status, int d, int c, double *tmp) {
+// AdaptiveMap::Adapt (AdaptiveMap.cc:67-125) of dimension d of grid c by one
+// block (WARP false; tmp: bins doubles of shared memory) or by one warp
+// (WARP true: the lanes of the calling warp, tmp its own bins doubles).  The
+// order-dependent sums and the rebinning run serially in thread (lane) 0 in
+// the reference's order; smoothing and the importance factors in parallel.
+template <bool WARP>
+__device__ __forceinline__ void grid_adapt_impl(const double *__restrict__ g_old, double *__restrict__ g_new, int dims,
+                                                int bins, double alpha, const double *__restrict__ train,
+                                                int skip_zero, int *__restrict__ status, int d, int c, double *tmp) {
+    const int tid = WARP ? static_cast<int>(threadIdx.x & 31) : static_cast<int>(threadIdx.x);
+    const int nthr = WARP ? 32 : static_cast<int>(blockDim.x);
+    auto sync = [] {
+        if (WARP) __syncwarp();
+        else __syncthreads();
+    };
     const double *T = train + static_cast<size_t>(c) * dims * bins;
     const double *E = g_old + static_cast<size_t>(c) * dims * (bins + 1);
     double *EN = g_new + static_cast<size_t>(c) * dims * (bins + 1);
@@ -175,42 +185,49 @@ __device__ __forceinline__ void grid_adapt_block(const double *__restrict__ g_ol
     double *ENd = EN + d * (bins + 1);
     if (skip_zero) {
         int nz = 0;
-        for (int k = threadIdx.x; k < dims * bins; k += blockDim.x) nz |= (T[k] != 0);
-        nz = __syncthreads_or(nz);
+        for (int k = tid; k < dims * bins; k += nthr) nz |= (T[k] != 0);
+        nz = WARP ? __any_sync(0xffffffffu, nz) : __syncthreads_or(nz);
         if (!nz) {
-            for (int k = threadIdx.x; k <= bins; k += blockDim.x) ENd[k] = Ed[k];
+            for (int k = tid; k <= bins; k += nthr) ENd[k] = Ed[k];
             return;
         }
     }
     const double *o = T + d * bins;
-    for (int b = threadIdx.x; b < bins; b += blockDim.x) {
+    for (int b = tid; b < bins; b += nthr) {
         double s;
         if (b == 0) s = (o[0] + o[1]) / 2;
         else if (b == bins - 1) s = (o[bins - 2] + o[bins - 1]) / 2;
         else s = ((o[b - 1] + o[b]) + o[b + 1]) / 3;
         tmp[b] = s;
     }
-    __syncthreads();
-    __shared__ double norm_s;
-    if (threadIdx.x == 0) {
-        double norm = 0;
-        for (int b = 0; b < bins; ++b) norm = (b == 0) ? tmp[0] : norm + tmp[b];
-        norm_s = norm;
+    sync();
+    double norm = 0;
+    if (WARP) {
+        if (tid == 0)
+            for (int b = 0; b < bins; ++b) norm = (b == 0) ? tmp[0] : norm + tmp[b];
+        norm = __shfl_sync(0xffffffffu, norm, 0);
+    } else {
+        __shared__ double norm_s;
+        if (tid == 0) {
+            double nm = 0;
+            for (int b = 0; b < bins; ++b) nm = (b == 0) ? tmp[0] : nm + tmp[b];
+            norm_s = nm;
+        }
+        __syncthreads();
+        norm = norm_s;
     }
-    __syncthreads();
-    const double norm = norm_s;
     if (norm == 0) {  // the reference leaves this dimension of new_hist at zero
-        for (int k = threadIdx.x; k <= bins; k += blockDim.x) ENd[k] = 0.0;
+        for (int k = tid; k <= bins; k += nthr) ENd[k] = 0.0;
         return;
     }
-    for (int b = threadIdx.x; b < bins; b += blockDim.x) {
+    for (int b = tid; b < bins; b += nthr) {
         if (tmp[b] != 0) {
             const double r = tmp[b] / norm;
             tmp[b] = pow((r - 1.0) / log(r), alpha);
         }
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    sync();
+    if (tid == 0) {
         double avg = 0;
         for (int b = 0; b < bins; ++b) avg += tmp[b];
         avg /= static_cast<double>(bins);
@@ -234,6 +251,13 @@ __device__ __forceinline__ void grid_adapt_block(const double *__restrict__ g_ol
         ENd[bins] = 1.0;
         if (bad) atomicOr(status, 1);
     }
+    sync();
+}
+
+__device__ __forceinline__ void grid_adapt_block(const double *__restrict__ g_old, double *__restrict__ g_new, int dims,
+                                                 int bins, double alpha, const double *__restrict__ train, int skip_zero,
+                                                 int *__restrict__ status, int d, int c, double *tmp) {
+    grid_adapt_impl<false>(g_old, g_new, dims, bins, alpha, train, skip_zero, status, d, c, tmp);
 }
 
 }  // namespace chili_dev
