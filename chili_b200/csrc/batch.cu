@@ -44,9 +44,9 @@ namespace {
 constexpr int kBatchMaxCh = 64;
 // Parallel branches of the phased multichannel task chains in the graph.
 constexpr int kPhBranches = 8;
-// Grouped mode: waves on two streams, so that one wave's tail overlaps the
-// next one's start.
-constexpr int kWaveStreams = 2;
+// Grouped mode: waves on up to this many streams (option
+// "batch_wave_streams"), so that one wave's tail overlaps the next one's start.
+constexpr int kMaxWaveStreams = 4;
 
 struct BatchTask {
     int32_t kind, dims, bins, nch;
@@ -600,7 +600,8 @@ struct BatchState {
     std::vector<WaveHost> waves;
     std::vector<long long> prefix_host;
     DevBuf d_pieces, d_prefix;
-    DevBuf d_arena[2];  // wave w uses arena w % 2 and stream w % 2
+    DevBuf d_arena[kMaxWaveStreams];  // wave w uses arena w % nstreams and stream w % nstreams
+    int wave_streams = 2;
     bool tuned = false;
     cudaGraphExec_t graph = nullptr;
     unsigned long long graph_launches = 0;  // kernels of one replay
@@ -747,7 +748,7 @@ int enqueue_waves(chili_ctx *ctx, const BatchDev &B) {
     const cudaStream_t caller = ctx->stream;
     for (size_t wi = 0; wi < S.waves.size(); ++wi) {
         const auto &w = S.waves[wi];
-        ctx->stream = S.ph_streams[wi % kWaveStreams];  // the wave's arena belongs to this stream
+        ctx->stream = S.ph_streams[wi % S.wave_streams];  // the wave's arena belongs to this stream
         const WaveDev W{S.d_pieces.as<Piece>() + w.first, w.n, S.d_prefix.as<long long>() + w.prefix_off};
         const long long *pre = S.prefix_host.data() + w.prefix_off;
         auto blocks = [&](int step) { return static_cast<unsigned>(w.blocks[static_cast<size_t>(step)]); };
@@ -809,14 +810,15 @@ int enqueue_iteration(chili_ctx *ctx, bool adapt) {
     const cudaStream_t main = ctx->stream;
     if (S.grouped && !S.waves.empty()) {
         // the waves on their streams beside the camel tasks' evaluation
-        CK(cudaEventRecord(S.ph_events[kWaveStreams], main));
-        for (int j = 0; j < kWaveStreams; ++j) CK(cudaStreamWaitEvent(S.ph_streams[j], S.ph_events[kWaveStreams], 0));
+        const int ns = S.wave_streams;
+        CK(cudaEventRecord(S.ph_events[ns], main));
+        for (int j = 0; j < ns; ++j) CK(cudaStreamWaitEvent(S.ph_streams[j], S.ph_events[ns], 0));
         k_batch_eval<<<S.grid_blocks, S.block, 0, ctx->stream>>>(B);
         LAUNCHED();
         const int rc = enqueue_waves(ctx, B);
         ctx->stream = main;
         if (rc) return rc;
-        for (int j = 0; j < kWaveStreams; ++j) {
+        for (int j = 0; j < ns; ++j) {
             CK(cudaEventRecord(S.ph_events[j], S.ph_streams[j]));
             CK(cudaStreamWaitEvent(main, S.ph_events[j], 0));
         }
@@ -984,7 +986,10 @@ int plan_waves(chili_ctx *ctx, const std::vector<PointProgram> &pps) {
                             sizeof(double) * ms, ms, sizeof(int32_t) * PP.ndims * ms, sizeof(double) * PP.nch * ms};
         for (int q = 0; q < 18; ++q) out[q] = (v[q] + 255) / 256 * 256;
     };
-    size_t arena[kWaveStreams] = {256, 256};
+    S.wave_streams = static_cast<int>(std::min<long long>(std::max<long long>(ctx->batch_wave_streams, 1),
+                                                          kMaxWaveStreams));
+    const int ns = S.wave_streams;
+    size_t arena[kMaxWaveStreams] = {256, 256, 256, 256};
     for (size_t wi = 0; wi < waves.size(); ++wi) {
         size_t tot = 0;
         for (const Piece &P : waves[wi]) {
@@ -992,9 +997,9 @@ int plan_waves(chili_ctx *ctx, const std::vector<PointProgram> &pps) {
             sizes(P, pps[static_cast<size_t>(S.tasks[static_cast<size_t>(P.ti)].pp)], sz);
             for (size_t q : sz) tot += q;
         }
-        arena[wi % kWaveStreams] = std::max(arena[wi % kWaveStreams], tot);
+        arena[wi % ns] = std::max(arena[wi % ns], tot);
     }
-    for (int j = 0; j < kWaveStreams; ++j) CK(S.d_arena[j].ensure(arena[j]));
+    for (int j = 0; j < ns; ++j) CK(S.d_arena[j].ensure(arena[j]));
     S.pieces.clear();
     S.waves.clear();
     S.prefix_host.clear();
@@ -1009,7 +1014,7 @@ int plan_waves(chili_ctx *ctx, const std::vector<PointProgram> &pps) {
         wh.n = static_cast<int>(w.size());
         wh.prefix_off = static_cast<long long>(S.prefix_host.size());
         std::vector<std::vector<long long>> pre(kGroupSteps, std::vector<long long>(w.size() + 1, 0));
-        uint8_t *base = S.d_arena[wi % kWaveStreams].as<uint8_t>();
+        uint8_t *base = S.d_arena[wi % ns].as<uint8_t>();
         size_t off = 0;
         for (size_t k = 0; k < w.size(); ++k) {
             Piece &P = w[k];
@@ -1076,12 +1081,12 @@ int plan_waves(chili_ctx *ctx, const std::vector<PointProgram> &pps) {
     CK(cudaMemcpyAsync(S.d_prefix.p, S.prefix_host.data(), sizeof(long long) * S.prefix_host.size(),
                        cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));  // the host vectors are the copies' sources
-    for (int j = 0; j < kWaveStreams; ++j) {
+    for (int j = 0; j < ns; ++j) {
         cudaStream_t st;
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         S.ph_streams.push_back(st);
     }
-    for (int k = 0; k <= kWaveStreams; ++k) {
+    for (int k = 0; k <= ns; ++k) {
         cudaEvent_t e;
         CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         S.ph_events.push_back(e);
@@ -1098,7 +1103,7 @@ void batch_release(chili_ctx *ctx) {
     for (DevBuf *b : {&S.d_tasks, &S.d_umap, &S.d_pps, &S.d_progs, &S.d_descs, &S.d_grids, &S.d_grids_new, &S.d_hist,
                       &S.d_atrain, &S.d_alpha, &S.d_best, &S.d_mindiff, &S.d_cp, &S.d_part, &S.d_stats,
                       &S.d_counters, &S.d_jobs, &S.d_status, &S.d_pieces, &S.d_prefix, &S.d_arena[0],
-                      &S.d_arena[1]})
+                      &S.d_arena[1], &S.d_arena[2], &S.d_arena[3]})
         b->release();
     for (auto &b : S.ph)
         for (DevBuf *d : {&b.mom, &b.ich, &b.flag, &b.list, &b.bcount, &b.boff, &b.ctl, &b.node, &b.memo, &b.cfail,

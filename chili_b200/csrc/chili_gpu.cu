@@ -446,6 +446,11 @@ int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value) {
         ctx->batch_grouped = value != 0;
         return CHILI_OK;
     }
+    if (std::strcmp(name, "batch_wave_streams") == 0) {
+        if (value < 1 || value > 4) return fail(ctx, CHILI_ERR_INVALID_ARG, "batch_wave_streams in [1, 4]");
+        ctx->batch_wave_streams = value;
+        return CHILI_OK;
+    }
     if (std::strcmp(name, "batch_wave_points") == 0) {
         if (value < 1 || value > (1ll << 30)) return fail(ctx, CHILI_ERR_INVALID_ARG, "batch_wave_points in [1, 2^30]");
         ctx->batch_wave = value;
