@@ -90,6 +90,11 @@ def parse():
     ap.add_argument("--no-t01", action="store_true", help="vegas: skip the time-to-0.1%% run")
     ap.add_argument("--no-others", action="store_true",
                     help="multichannel: skip the compact runs of the other workloads")
+    ap.add_argument("--no-unweighting", action="store_true",
+                    help="multichannel: skip the unweighting-quantile and event-output measurements")
+    ap.add_argument("--log-iterations", action="store_true",
+                    help="multichannel: one line per iteration on stderr (points tried, weighted, accepted), "
+                         "to normalise per-launch profiler counters")
     return ap.parse_args()
 
 
@@ -203,8 +208,18 @@ def run_chili(args, rank, world, local_rank):
         return st.as_tuple(), info, unweighted_events(st, info)
 
     rank_obj_counter = [counter]
+    n_iter = [0]
+
+    def logged(out):
+        if args.log_iterations:
+            info = out[1]
+            print(f"iteration {n_iter[0]}: tried {info.points_tried} weighted {info.points_weighted} "
+                  f"accepted {info.points_accepted}", file=sys.stderr, flush=True)
+        n_iter[0] += 1
+        return out
+
     for _ in range(args.warmup):
-        one_step()
+        logged(one_step())
     torch.cuda.synchronize(dev)
     barrier()
     torch.cuda.synchronize(dev)
@@ -221,7 +236,7 @@ def run_chili(args, rank, world, local_rank):
         ev0.record(stream)
         t_wall0 = time.perf_counter()
         for _ in range(args.steps):
-            st_t, info, u_step = one_step()
+            st_t, info, u_step = logged(one_step())
             tried += info.points_tried
             weighted += info.points_weighted
             unw += u_step
@@ -261,15 +276,19 @@ def run_chili(args, rank, world, local_rank):
             flow_long = measure_flow(ctx, args, dev, stream, plain, train_steps=args.flow_long_steps)
 
     ctx.set_option("kernel_timing", 0)  # no per-kernel events around the event-output calls
-    unw_q = quantile_unweighting(ctx, seed=4242 + rank)
-    if WL["unweighted_target"]:
-        unw_out = measure_unweighted_target(ctx, info.weight_max, dev, rank, WL["unweighted_target"])
-    else:
-        unw_out = measure_unweighted_output(ctx, info.weight_max, dev, rank)
+    unw_q = unw_out = None
+    if not args.no_unweighting:
+        unw_q = quantile_unweighting(ctx, seed=4242 + rank)
+        if WL["unweighted_target"]:
+            unw_out = measure_unweighted_target(ctx, info.weight_max, dev, rank, WL["unweighted_target"])
+        else:
+            unw_out = measure_unweighted_output(ctx, info.weight_max, dev, rank)
 
     e2e = None
     if not args.no_e2e:
         if WL["unweighted_target"]:
+            if unw_out is None:
+                raise SystemExit("bench.py: the large workload's e2e is its event output (drop --no-unweighting)")
             # 1e7-point iterations: the uniforms would not fit pinned host memory
             # twice; the end-to-end path is the event output to the host
             e2e = {"value": unw_out["events_per_s"], "unit": UNIT, "h2d_bytes_per_step": 0,
