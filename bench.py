@@ -214,7 +214,8 @@ def run_chili(args, rank, world, local_rank):
         if args.log_iterations:
             info = out[1]
             print(f"iteration {n_iter[0]}: tried {info.points_tried} weighted {info.points_weighted} "
-                  f"accepted {info.points_accepted}", file=sys.stderr, flush=True)
+                  f"accepted {info.points_accepted} drawn {info.points_drawn} chunks {info.chunks}",
+                  file=sys.stderr, flush=True)
         n_iter[0] += 1
         return out
 
@@ -228,6 +229,7 @@ def run_chili(args, rank, world, local_rank):
     ctx.set_option("kernel_timing", 1)  # CUDA events around each kernel of the timed region
     l0 = ctx.launches
     weighted = 0
+    drawn = 0
     pooled = np.zeros(6)
     history = []
     unw = 0.0
@@ -239,6 +241,7 @@ def run_chili(args, rank, world, local_rank):
             st_t, info, u_step = logged(one_step())
             tried += info.points_tried
             weighted += info.points_weighted
+            drawn += info.points_drawn
             unw += u_step
             pooled += np.array(st_t) * np.array([1, 0, 0, 1, 1, 1])
             mean, err = gpu.stats_mean_error(pooled)
@@ -263,7 +266,7 @@ def run_chili(args, rank, world, local_rank):
 
     kernel_ms = {k: ctx.kernel_time(k) for k in TIMED_KERNELS}
     kernel_ms = {k: v for k, v in kernel_ms.items() if v[1] > 0}
-    roof = roofline(kernel_ms, weighted, args.ncalls * args.steps, ms, dev)
+    roof = roofline(kernel_ms, weighted, args.ncalls * args.steps, ms, dev, drawn=drawn)
 
     plain = {"value": unw_tot / (ms_max / 1e3), "ms_per_step": ms_max / args.steps,
              "points_per_step": tried_tot / args.steps, "integral": mean, "rel_error": err / abs(mean),
@@ -495,7 +498,7 @@ def fp64_peak_tflops(dev):
     return 2.0 * n ** 3 / best / 1e12
 
 
-def roofline(kernel_ms, weighted, accepted, step_ms, dev):
+def roofline(kernel_ms, weighted, accepted, step_ms, dev, drawn=None):
     """The FP64 roofline of the multichannel step (the binding resource:
     every point evaluates every channel's inverse map, mostly
     transcendental-function expansions).  For the dominant kernel of the
@@ -513,9 +516,14 @@ def roofline(kernel_ms, weighted, accepted, step_ms, dev):
     peak = fp64_peak_tflops(dev)
     hbm = measured_peaks().get("hbm_gbs")
     c = KERNEL_COUNTERS.get(dom)
-    per_launch = weighted / max(launches, 1)
+    drawn = drawn or weighted
+
+    def points(k):  # the points a kernel class processes: drawn (forward) or weighted
+        return drawn if KERNEL_COUNTERS.get(k, {}).get("basis") == "drawn" else weighted
+    per_launch = points(dom) / max(launches, 1)
     out = {"kernel": dom, "bound": "fp64", "launches": launches, "ms_per_launch": ms / max(launches, 1),
-           "weighted_points_per_launch": per_launch, "share_of_kernel_time": ms / sum(v[0] for v in kernel_ms.values()),
+           "points_per_launch": per_launch, "points_basis": KERNEL_COUNTERS.get(dom, {}).get("basis", "weighted"),
+           "share_of_kernel_time": ms / sum(v[0] for v in kernel_ms.values()),
            "peak": peak, "unit": "TFLOP/s", "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
            "kernel_ms": {k: round(v[0], 4) for k, v in kernel_ms.items()}}
     if c:
@@ -525,16 +533,18 @@ def roofline(kernel_ms, weighted, accepted, step_ms, dev):
                    counters_source=c["source"])
     else:
         out.update(achieved=None, frac=None, traffic=None)
-    ops = sum(KERNEL_COUNTERS[k]["fp64_ops_per_point"] for k in kernel_ms if k in KERNEL_COUNTERS)
-    dram = sum(KERNEL_COUNTERS[k]["dram_bytes_per_point"] for k in kernel_ms if k in KERNEL_COUNTERS)
+    # the whole step: each kernel class's count times the points it processed
+    ops_tot = sum(KERNEL_COUNTERS[k]["fp64_ops_per_point"] * points(k) for k in kernel_ms if k in KERNEL_COUNTERS)
+    dram_tot = sum(KERNEL_COUNTERS[k]["dram_bytes_per_point"] * points(k) for k in kernel_ms if k in KERNEL_COUNTERS)
+    ops, dram = ops_tot / weighted, dram_tot / weighted
     sec = step_ms / 1e3
     out["step"] = {
-        "fp64": {"ops_per_weighted_point": ops, "achieved": ops * weighted / sec / 1e12, "unit": "TFLOP/s",
-                 "frac": ops * weighted / sec / 1e12 / peak},
+        "fp64": {"ops_per_weighted_point": ops, "achieved": ops_tot / sec / 1e12, "unit": "TFLOP/s",
+                 "frac": ops_tot / sec / 1e12 / peak},
         "hbm_event_record": {"bytes_per_accepted_point": 204, "achieved": 204 * accepted / sec / 1e9, "unit": "GB/s",
                              "peak": hbm, "frac": 204 * accepted / sec / 1e9 / hbm if hbm else None},
         "dram_bytes_per_weighted_point": dram,
-        "seconds": sec, "weighted_points": weighted, "accepted_points": accepted,
+        "seconds": sec, "weighted_points": weighted, "drawn_points": drawn, "accepted_points": accepted,
     }
     return out
 

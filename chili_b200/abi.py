@@ -112,16 +112,17 @@ class MCIterInfo(C.Structure):
     _fields_ = [("points_tried", C.c_uint64), ("points_accepted", C.c_uint64),
                 ("rejected_pre", C.c_uint64), ("rejected_nan", C.c_uint64),
                 ("weight_max", C.c_double), ("nonfinite_alpha_terms", C.c_double),
-                ("points_weighted", C.c_uint64)]
+                ("points_weighted", C.c_uint64), ("points_drawn", C.c_uint64), ("chunks", C.c_uint64)]
 
 
 class FlowParams(C.Structure):
     """chili_flow_params (learned proposal)."""
-    _fields_ = [("layers", C.c_int32), ("batch", C.c_int32), ("lr", C.c_double), ("init_seed", C.c_uint64)]
+    _fields_ = [("layers", C.c_int32), ("batch", C.c_int32), ("lr", C.c_double), ("init_seed", C.c_uint64),
+                ("hidden", C.c_int32), ("depth", C.c_int32)]
 
     @classmethod
     def defaults(cls, **kw):
-        p = cls(layers=6, batch=65536, lr=1e-3, init_seed=1)
+        p = cls(layers=6, batch=65536, lr=1e-3, init_seed=1, hidden=128, depth=2)
         for k, v in kw.items():
             setattr(p, k, v)
         return p

@@ -20,7 +20,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # different rounding of a fused multiply-add to ~1e-9). The tensor-core flow
 # layers and the channel-weight network keep contraction.
 NO_CONTRACT = {"chili_gpu.cu", "batch.cu", "flow.cu"}
-SOURCES = ["chili_gpu.cu", "flow.cu", "flow_layers.cu", "flow_alpha.cu", "channel_program.cpp", "checkpoint.cu", "batch.cu", "construct.cpp"]
+SOURCES = ["chili_gpu.cu", "flow.cu", "flow_layers.cu", "flow_wide.cu", "flow_alpha.cu", "channel_program.cpp", "checkpoint.cu", "batch.cu", "construct.cpp"]
 
 
 def nvcc():

@@ -460,6 +460,10 @@ int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value) {
         ctx->batch_phased = value != 0;
         return CHILI_OK;
     }
+    if (std::strcmp(name, "flow_streamed") == 0) {
+        ctx->flow_streamed = value != 0;
+        return CHILI_OK;
+    }
     if (std::strcmp(name, "pipeline_tile") == 0) {
         if (value < 1024 || value > (1ll << 24)) return fail(ctx, CHILI_ERR_INVALID_ARG, "pipeline_tile outside [1024, 2^24]");
         ctx->pipe_tile = value;
@@ -1044,7 +1048,7 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
     }
     const size_t acc_smem = sizeof(double) * (kWgtBlock / 32) * nch;
 
-    long long needed = ncalls, tried = 0, weighted = 0;
+    long long needed = ncalls, tried = 0, weighted = 0, drawn = 0, chunks = 0;
     unsigned long long rounds = 0;
     const bool pipe = pipeline_dims_ok(D) && ctx->have_pp && ctx->use_pp && ctx->use_pipeline;
     if (u_host) CK(ctx->iter_ctl.ensure(sizeof(long long) * kIterCtl));
@@ -1073,6 +1077,8 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         // Otherwise the chunk is one round, its record read back at its end.
         const long long S = u_host ? std::min(m, kUploadSlice) : m;  // rows of the largest round
         const long long n_rounds = u_host ? slice_count(m) : 1;
+        drawn += m;
+        ++chunks;
         if (u_host) {
             // the gate is set before upload_host records the event the
             // slice copies (and so every forward launch of the chunk, on
@@ -1266,6 +1272,8 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         info->weight_max = acc_h.wmax;
         info->nonfinite_alpha_terms = acc_h.nonfinite;
         info->points_weighted = static_cast<uint64_t>(weighted);
+        info->points_drawn = static_cast<uint64_t>(drawn);
+        info->chunks = static_cast<uint64_t>(chunks);
     }
     return CHILI_OK;
 }

@@ -25,6 +25,13 @@ struct FlowState {
     std::vector<int> da, db;
     std::vector<std::vector<int>> cond, trans;
     std::vector<long long> off_w1, off_e, off_w2, off_w3;
+    // conditioner: H hidden units, NH hidden layers; streamed: the
+    // streamed-weight kernels (flow_wide.cuh) instead of the resident ones
+    int H = kH, NH = 2;
+    bool streamed = false;
+    std::vector<std::vector<long long>> off_w2x;  // per layer: the NH - 1 square matrices
+    std::vector<WideLayer> wlayers;
+    DevBuf hsw, gpsw, gthsw;  // streamed kernels: saved activations, g_p tiles, g_theta tiles
     long long np_flow = 0, np = 0, off_alpha = 0;
     AlphaLayout AL{};
     DevBuf prm, m, v, grad, wtiles, part_f, part_a, loss_part, loss_dev;
@@ -127,6 +134,24 @@ int upload_beta(chili_ctx *ctx) {
 int pack_tiles(chili_ctx *ctx) {
     FlowState &S = *ctx->flow;
     const float *p = S.prm.as<float>();
+    if (S.streamed) {
+        for (int l = 0; l < S.L; ++l) {
+            WidePackArgs a{};
+            a.prm = p;
+            a.off_w1 = S.off_w1[l];
+            a.off_e = S.off_e[l];
+            a.off_w3 = S.off_w3[l];
+            for (int k = 0; k < S.NH - 1; ++k) a.off_w2[k] = S.off_w2x[l][k];
+            a.H = S.H;
+            a.nh = S.NH;
+            a.da = S.da[l];
+            a.nch = S.nch;
+            a.db = S.db[l];
+            a.w = S.wtiles.as<uint8_t>() + static_cast<size_t>(l) * wide_layer_bytes(S.H, S.NH);
+            if (int rc = flow_launch_pack_wide(ctx, a)) return rc;
+        }
+        return CHILI_OK;
+    }
     for (int l = 0; l < S.L; ++l) {
         uint8_t *wt = S.wtiles.as<uint8_t>() + static_cast<size_t>(l) * kWLayerBytes;
         k_flow_pack<<<(kPF * 128 + 255) / 256, 256, 0, ctx->stream>>>(
@@ -178,6 +203,14 @@ int ensure_train(chili_ctx *ctx, long long n) {
     CK(S.g0.ensure(fN * S.D));
     CK(S.g1.ensure(fN * S.D));
     CK(S.thetas.ensure(fN * static_cast<size_t>(kMaxDB * kPerDim) * S.L));
+    if (S.streamed) {
+        const size_t act = static_cast<size_t>(wide_act_bytes(S.H)) * tiles;
+        CK(S.hsw.ensure(act * S.NH * S.L));
+        CK(S.gpsw.ensure(act * S.NH));
+        CK(S.gthsw.ensure(static_cast<size_t>(tiles) * kGTileW));
+        S.nb = n;
+        return CHILI_OK;
+    }
     CK(S.h1s.ensure(static_cast<size_t>(tiles) * kHTile * S.L));
     CK(S.h2s.ensure(static_cast<size_t>(tiles) * kHTile * S.L));
     CK(S.gths.ensure(static_cast<size_t>(tiles) * kGTile));
@@ -195,6 +228,96 @@ FlowLayer layer_dev(FlowState &S, int l) {
     return L;
 }
 
+// One coupling layer forward on the kernels of the configured kind (theta
+// and the activations saved for the backward pass when save).
+int layer_forward(chili_ctx *ctx, int l, int mode, bool save, long long n, const float *xin, float *xout,
+                  const int32_t *ch, float *logq, float *theta) {
+    FlowState &S = *ctx->flow;
+    const long long tiles = (n + 127) / 128;
+    if (S.streamed) {
+        WideFwdArgs a{};
+        a.L = S.wlayers[l];
+        a.n = n;
+        a.xin = xin;
+        a.xout = xout;
+        a.ch = ch;
+        a.logq = logq;
+        if (save) a.hs = S.hsw.as<uint8_t>() + static_cast<size_t>(l) * S.NH * tiles * wide_act_bytes(S.H);
+        a.theta = theta;
+        a.err = S.err.as<int>();
+        return flow_launch_layer_wide(ctx, mode, save, a, S.sms);
+    }
+    LayerArgs a{};
+    a.L = layer_dev(S, l);
+    a.n = n;
+    a.xin = xin;
+    a.xout = xout;
+    a.ch = ch;
+    a.logq = logq;
+    if (save) {
+        a.h1s = S.h1s.as<uint8_t>() + static_cast<size_t>(l) * tiles * kHTile;
+        a.h2s = S.h2s.as<uint8_t>() + static_cast<size_t>(l) * tiles * kHTile;
+    }
+    a.theta = theta;
+    a.err = S.err.as<int>();
+    return flow_launch_layer(ctx, mode, save, a, S.sms);
+}
+
+// Backward and weight gradients of coupling layer l on the streamed-weight
+// kernels.
+int layer_backward_streamed(chili_ctx *ctx, int l, long long n, const float *xin, const float *theta,
+                            const float *gout, float *gin) {
+    FlowState &S = *ctx->flow;
+    const long long tiles = (n + 127) / 128;
+    const uint8_t *hs = S.hsw.as<uint8_t>() + static_cast<size_t>(l) * S.NH * tiles * wide_act_bytes(S.H);
+    WideBwdArgs b{};
+    b.L = S.wlayers[l];
+    b.n = n;
+    b.xin = xin;
+    b.theta = theta;
+    b.hs = hs;
+    b.gout = gout;
+    b.glogq = S.glogq.as<float>();
+    b.gin = gin;
+    b.gths = S.gthsw.as<uint8_t>();
+    b.gps = S.gpsw.as<uint8_t>();
+    b.err = S.err.as<int>();
+    if (int rc = flow_launch_bwd_wide(ctx, b, S.sms)) return rc;
+    WideWgradArgs w{};
+    w.n = n;
+    w.H = S.H;
+    w.nh = S.NH;
+    w.da = S.da[l];
+    w.db = S.db[l];
+    w.nch = S.nch;
+    w.ncol2 = ((16 + S.nch) + 63) & ~63;
+    for (int i = 0; i < S.da[l]; ++i) w.cond[i] = static_cast<int8_t>(S.cond[l][i]);
+    w.xin = xin;
+    w.ch = S.chb.as<int32_t>();
+    w.hs = hs;
+    w.gps = b.gps;
+    w.gths = b.gths;
+    w.part = S.part_f.as<float>();
+    w.nparam = S.np_flow;
+    w.off_w1 = S.off_w1[l];
+    w.off_e = S.off_e[l];
+    w.off_w3 = S.off_w3[l];
+    for (int k = 0; k < S.NH - 1; ++k) w.off_w2[k] = S.off_w2x[l][k];
+    w.err = S.err.as<int>();
+    const int halves = S.H / 128;
+    auto add = [&](int kind, int m, int mh, int np) {
+        w.item[w.nitems++] = WideWgradItem{static_cast<int8_t>(kind), static_cast<int8_t>(m),
+                                           static_cast<int8_t>(mh), static_cast<int8_t>(np)};
+    };
+    for (int mh = 0; mh < halves; ++mh) {
+        add(0, 0, mh, 0);
+        if (S.db[l] == 5) add(0, 0, mh, 1);
+        for (int m = 0; m < S.NH - 1; ++m) add(1, m, mh, 0);
+        add(2, 0, mh, 0);
+    }
+    return flow_launch_wgrad_wide(ctx, w, kNsplit);
+}
+
 // Flow forward (density direction, saving), channel-weight network + loss,
 // flow backward and weight gradients, Adam (lr = 0: gradients only, into
 // S.grad), the step's loss into loss_dev[slot]. Inputs already in the
@@ -206,20 +329,10 @@ int train_pass(chili_ctx *ctx, long long n, float lr, int slot) {
     const size_t xs = static_cast<size_t>(S.D) * n;
     const size_t thn = static_cast<size_t>(kMaxDB * kPerDim) * n;
     CK(cudaMemsetAsync(S.logq.p, 0, sizeof(float) * n, ctx->stream));
-    for (int l = 0; l < S.L; ++l) {
-        LayerArgs a{};
-        a.L = layer_dev(S, l);
-        a.n = n;
-        a.xin = X + xs * l;
-        a.xout = X + xs * (l + 1);
-        a.ch = S.chb.as<int32_t>();
-        a.logq = S.logq.as<float>();
-        a.h1s = S.h1s.as<uint8_t>() + static_cast<size_t>(l) * tiles * kHTile;
-        a.h2s = S.h2s.as<uint8_t>() + static_cast<size_t>(l) * tiles * kHTile;
-        a.theta = S.thetas.as<float>() + thn * l;
-        a.err = S.err.as<int>();
-        if (int rc = flow_launch_layer(ctx, 0, true, a, S.sms)) return rc;
-    }
+    for (int l = 0; l < S.L; ++l)
+        if (int rc = layer_forward(ctx, l, 0, true, n, X + xs * l, X + xs * (l + 1), S.chb.as<int32_t>(),
+                                   S.logq.as<float>(), S.thetas.as<float>() + thn * l))
+            return rc;
     AlphaTrainArgs aa{};
     aa.n = n;
     aa.L = S.AL;
@@ -236,6 +349,13 @@ int train_pass(chili_ctx *ctx, long long n, float lr, int slot) {
     if (int rc = flow_launch_alpha(ctx, aa)) return rc;
     float *gcur = S.g0.as<float>(), *gnext = S.g1.as<float>();
     for (int l = S.L - 1; l >= 0; --l) {
+        if (S.streamed) {
+            if (int rc = layer_backward_streamed(ctx, l, n, X + xs * l, S.thetas.as<float>() + thn * l,
+                                                 l == S.L - 1 ? nullptr : gcur, gnext))
+                return rc;
+            std::swap(gcur, gnext);
+            continue;
+        }
         BwdArgs b{};
         b.L = layer_dev(S, l);
         b.n = n;
@@ -386,17 +506,9 @@ int flow_pass(chili_ctx *ctx, const float *xin_dev, const int32_t *ch_dev, long 
     float *bufs[2] = {S.sx0.as<float>(), S.sx1.as<float>()};
     for (int k = 0; k < S.L; ++k) {
         const int l = mode == 0 ? k : S.L - 1 - k;
-        LayerArgs a{};
-        a.L = layer_dev(S, l);
-        a.n = n;
-        a.xin = cur;
-        a.xout = k == S.L - 1 ? xout_dev : bufs[k & 1];
-        a.ch = ch_dev;
-        a.logq = logq_dev;
-        a.err = S.err.as<int>();
-        const int rc = flow_launch_layer(ctx, mode, false, a, S.sms);
-        if (rc) return rc;
-        cur = a.xout;
+        float *out = k == S.L - 1 ? xout_dev : bufs[k & 1];
+        if (int rc = layer_forward(ctx, l, mode, false, n, cur, out, ch_dev, logq_dev, nullptr)) return rc;
+        cur = out;
     }
     return CHILI_OK;
 }
@@ -409,6 +521,7 @@ void flow_release(chili_ctx *ctx) {
     for (DevBuf *b : {&S.prm, &S.m, &S.v, &S.grad, &S.wtiles, &S.part_f, &S.part_a, &S.loss_part, &S.loss_dev,
                       &S.beta, &S.logbeta, &S.cp, &S.X, &S.chb, &S.logf, &S.fval, &S.feat, &S.logprior, &S.logq,
                       &S.glogq, &S.g0, &S.g1, &S.thetas, &S.h1s, &S.h2s, &S.gths, &S.gp2s, &S.gp1s, &S.scal,
+                      &S.hsw, &S.gpsw, &S.gthsw,
                       &S.sx0, &S.sx1, &S.sz, &S.su, &S.sch, &S.slq, &S.spart, &S.sfold, &S.fv,
                       &S.fmom, &S.flist, &S.fcount, &S.err})
         b->release();
@@ -442,6 +555,13 @@ int chili_gpu_flow_init(chili_ctx *ctx, const chili_flow_params *params) {
     S.n_ext = ctx->n_ext;
     S.batch = params->batch;
     S.lr = static_cast<float>(params->lr);
+    S.H = params->hidden ? params->hidden : kH;
+    S.NH = params->depth ? params->depth : 2;
+    if ((S.H != 128 && S.H != 256) || S.NH < 2 || S.NH > kWMaxNH) {
+        flow_release(ctx);
+        return fail(ctx, CHILI_ERR_INVALID_ARG, "conditioner: hidden 128 or 256, depth 2..4");
+    }
+    S.streamed = S.H != kH || S.NH != 2 || ctx->flow_streamed;
     cudaDeviceGetAttribute(&S.sms, cudaDevAttrMultiProcessorCount, ctx->device);
     flow_masks(S.D, S.L, S.cond, S.trans);
     long long off = 0;
@@ -461,14 +581,28 @@ int chili_gpu_flow_init(chili_ctx *ctx, const chili_flow_params *params) {
         L.nch = S.nch;
         for (int i = 0; i < da; ++i) L.cond[i] = static_cast<int8_t>(S.cond[l][i]);
         for (int j = 0; j < db; ++j) L.trans[j] = static_cast<int8_t>(S.trans[l][j]);
+        const long long H = S.H;
         S.off_w1.push_back(off);
-        off += static_cast<long long>(kH) * da;
+        off += H * da;
         S.off_e.push_back(off);
-        off += static_cast<long long>(S.nch) * kH;
+        off += S.nch * H;
         S.off_w2.push_back(off);
-        off += static_cast<long long>(kH) * kH;
+        S.off_w2x.emplace_back();
+        for (int k = 0; k < S.NH - 1; ++k) {
+            S.off_w2x.back().push_back(off);
+            off += H * H;
+        }
         S.off_w3.push_back(off);
-        off += static_cast<long long>(db) * kPerDim * kH;
+        off += db * kPerDim * H;
+        WideLayer W{};
+        W.H = S.H;
+        W.nh = S.NH;
+        W.da = da;
+        W.db = db;
+        W.nch = S.nch;
+        for (int i = 0; i < da; ++i) W.cond[i] = L.cond[i];
+        for (int j = 0; j < db; ++j) W.trans[j] = L.trans[j];
+        S.wlayers.push_back(W);
     }
     S.np_flow = off;
     S.off_alpha = off;
@@ -479,12 +613,14 @@ int chili_gpu_flow_init(chili_ctx *ctx, const chili_flow_params *params) {
     uint64_t rs = params->init_seed;
     for (int l = 0; l < S.L; ++l) {
         const int da = S.da[l], db = S.db[l];
-        const double b1 = std::sqrt(6.0 / da), b2 = std::sqrt(6.0 / kH);
-        for (int i = 0; i < kH * da; ++i) p[S.off_w1[l] + i] = static_cast<float>(b1 * unif_pm1(rs));
-        for (int i = 0; i < kH * kH; ++i) p[S.off_w2[l] + i] = static_cast<float>(b2 * unif_pm1(rs));
+        const int H = S.H;
+        const double b1 = std::sqrt(6.0 / da), b2 = std::sqrt(6.0 / H);
+        for (int i = 0; i < H * da; ++i) p[S.off_w1[l] + i] = static_cast<float>(b1 * unif_pm1(rs));
+        for (int k = 0; k < S.NH - 1; ++k)
+            for (int i = 0; i < H * H; ++i) p[S.off_w2x[l][k] + i] = static_cast<float>(b2 * unif_pm1(rs));
         const float did = static_cast<float>(std::log(std::expm1(1.0 - 1e-3)));
         for (int j = 0; j < db; ++j)
-            for (int k = 0; k <= kBins; ++k) p[S.off_w3[l] + (j * kPerDim + 2 * kBins + k) * kH + (kH - 1)] = did;
+            for (int k = 0; k <= kBins; ++k) p[S.off_w3[l] + (j * kPerDim + 2 * kBins + k) * H + (H - 1)] = did;
     }
     {
         const double ba1 = std::sqrt(6.0 / F), ba2 = std::sqrt(6.0 / kAH);
@@ -498,8 +634,11 @@ int chili_gpu_flow_init(chili_ctx *ctx, const chili_flow_params *params) {
     CK(cudaMemcpyAsync(S.prm.p, p.data(), sizeof(float) * S.np, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemsetAsync(S.m.p, 0, sizeof(float) * S.np, ctx->stream));
     CK(cudaMemsetAsync(S.v.p, 0, sizeof(float) * S.np, ctx->stream));
-    CK(S.wtiles.ensure(static_cast<size_t>(S.L) * kWLayerBytes));
-    CK(cudaMemsetAsync(S.wtiles.p, 0, static_cast<size_t>(S.L) * kWLayerBytes, ctx->stream));
+    const size_t wbytes = static_cast<size_t>(S.L) * (S.streamed ? wide_layer_bytes(S.H, S.NH) : kWLayerBytes);
+    CK(S.wtiles.ensure(wbytes));
+    CK(cudaMemsetAsync(S.wtiles.p, 0, wbytes, ctx->stream));
+    for (int l = 0; l < S.L; ++l)
+        S.wlayers[l].w = S.wtiles.as<uint8_t>() + static_cast<size_t>(l) * wide_layer_bytes(S.H, S.NH);
     CK(S.part_f.ensure(sizeof(float) * kNsplit * S.np_flow));
     CK(S.part_a.ensure(sizeof(float) * kAlphaSplit * S.AL.total));
     CK(S.loss_part.ensure(sizeof(double) * kAlphaSplit));

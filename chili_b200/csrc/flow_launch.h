@@ -6,6 +6,7 @@
 
 #include "context.h"
 #include "flow_phys.cuh"
+#include "flow_wide.cuh"
 
 // Coupling-layer forward (mode 0: density direction, 1: sampling), one block
 // per SM at most.
@@ -14,3 +15,9 @@ int flow_launch_bwd(chili_ctx *ctx, const chili_flow::BwdArgs &a, int sms);
 int flow_launch_alpha(chili_ctx *ctx, const chili_flow::AlphaTrainArgs &a);
 // The last step of a flow-path tile (training rows or sampled values).
 int flow_launch_combine(chili_ctx *ctx, bool train, const chili_flow::CombineArgs &a, unsigned blocks);
+
+// The wide-conditioner kernels (flow_wide.cuh; flow_wide.cu).
+int flow_launch_layer_wide(chili_ctx *ctx, int mode, bool save, const chili_flow::WideFwdArgs &a, int sms);
+int flow_launch_bwd_wide(chili_ctx *ctx, const chili_flow::WideBwdArgs &a, int sms);
+int flow_launch_wgrad_wide(chili_ctx *ctx, const chili_flow::WideWgradArgs &a, int nsplit);
+int flow_launch_pack_wide(chili_ctx *ctx, const chili_flow::WidePackArgs &a);

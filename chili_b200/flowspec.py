@@ -36,13 +36,23 @@ def n_features(n_ext):
     return n_out * (n_out - 1) // 2 + n_out
 
 
-def layout(dims, nch, n_ext, layers=6):
-    """[(name, offset, shape)] in the library's order."""
+def w2_name(l, k):
+    """The k-th square hidden matrix of coupling layer l."""
+    return f"W2_{l}" if k == 0 else f"W2_{l}_{k}"
+
+
+def layout(dims, nch, n_ext, layers=6, hidden=HIDDEN, depth=2):
+    """[(name, offset, shape)] in the library's order: per coupling layer
+    W1 [hidden][da], E [nch][hidden], depth - 1 square matrices
+    [hidden][hidden], W3 [db*49][hidden]; then the channel-weight network."""
     out, off = [], 0
+    H = hidden
     for l, m in enumerate(masks(dims, layers)):
         da, db = int(m.sum()), int((~m).sum())
-        for name, shape in ((f"W1_{l}", (HIDDEN, da)), (f"E_{l}", (nch, HIDDEN)), (f"W2_{l}", (HIDDEN, HIDDEN)),
-                            (f"W3_{l}", (db * PER_DIM, HIDDEN))):
+        items = [(f"W1_{l}", (H, da)), (f"E_{l}", (nch, H))]
+        items += [(w2_name(l, k), (H, H)) for k in range(depth - 1)]
+        items.append((f"W3_{l}", (db * PER_DIM, H)))
+        for name, shape in items:
             out.append((name, off, shape))
             off += int(np.prod(shape))
     F, A = n_features(n_ext), ALPHA_HIDDEN

@@ -508,12 +508,12 @@ class Context:
         return edges, alpha
 
 
-def flow_layout(dims, nch, n_ext, layers=6):
+def flow_layout(dims, nch, n_ext, layers=6, hidden=128, depth=2):
     """Offsets of the flat parameter vector of the learned proposal (the
     layout that include/chili_gpu.h documents): a list of (name, offset,
     shape) with the oracle's parameter names."""
     from . import flowspec
-    return flowspec.layout(dims, nch, n_ext, layers)
+    return flowspec.layout(dims, nch, n_ext, layers, hidden, depth)
 
 
 def construct_channels(flavs, combinable, masses, widths, sqrts, cuts=None, smax=2):

@@ -138,6 +138,10 @@ typedef struct {
     uint64_t points_weighted; /* points whose combined weight was computed
                                  (PreProcess-accepted points of the chunks,
                                  including those beyond the cut)           */
+    uint64_t points_drawn;    /* counters the chunks' forward launches
+                                 covered (each chunk is drawn whole,
+                                 including points beyond the cut)          */
+    uint64_t chunks;          /* chunks of points the iteration drew       */
 } chili_mc_iter_info;
 
 /* ------------------------------------------------------------ integrands */
@@ -205,7 +209,12 @@ uint64_t chili_gpu_launch_count(const chili_ctx *ctx);
  * "batch_phased": 1 (default) weights the batched multichannel tasks whose
  * channel set has a shared-entry program with the phased weight pass (task
  * chains as parallel graph branches); 0 evaluates every point in one thread
- * of the persistent batch kernel.  Read by chili_gpu_batch_set. */
+ * of the persistent batch kernel.  Read by chili_gpu_batch_set.
+ * "flow_streamed": 1 runs a learned proposal of 2 x 128 hidden units on the
+ * streamed-weight coupling kernels that wider or deeper conditioners always
+ * use (the same function; a cross-check of the two kernel families), 0
+ * (default) on the kernels that keep the weights in shared memory.  Read by
+ * chili_gpu_flow_init. */
 int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value);
 /* Total device time (ms) and launch count of one kernel class under the
  * "kernel_timing" option: k_mc_forward, k_pp_nodes, k_pp_items, k_pp_chains,
@@ -486,17 +495,24 @@ int chili_gpu_evaluate_batch(chili_ctx *ctx, int ch, const double *u,
  * p = FSMapper_c(x)). Requires channels (at most 48), grids, integrand and
  * channel weights to be set; beta starts as the current channel weights.
  *
- * Flat parameter layout (f32): per coupling layer l: W1 [128][da_l],
- * E [nch][128], W2 [128][128], W3 [db_l*49][128]; then the channel-weight
- * network: A1 [64][F], c1 [64], A2 [64][64], c2 [64], A3 [nch][64], c3 [nch],
- * F = n_out(n_out-1)/2 + n_out. Layer l transforms db_l <= 5 dimensions
- * (dims <= 10: alternating, half/half and shifted-pair splits and their
- * complements in turn; dims > 10: dimensions 5l..5l+4 mod dims). */
+ * Conditioner of layer l, H = hidden units, depth hidden layers:
+ * h_1 = lrelu(W1 (2a - 1) + E[c]), h_k = lrelu(W2_{k-2} h_{k-1}) for
+ * k = 2..depth, theta = W3 h_depth; unit H-1 of every hidden layer is the
+ * constant 1 (it carries the biases).
+ * Flat parameter layout (f32): per coupling layer l: W1 [H][da_l],
+ * E [nch][H], W2_0 .. W2_{depth-2} [H][H] each, W3 [db_l*49][H]; then the
+ * channel-weight network: A1 [64][F], c1 [64], A2 [64][64], c2 [64],
+ * A3 [nch][64], c3 [nch], F = n_out(n_out-1)/2 + n_out. Layer l transforms
+ * db_l <= 5 dimensions (dims <= 10: alternating, half/half and shifted-pair
+ * splits and their complements in turn; dims > 10: dimensions 5l..5l+4 mod
+ * dims). */
 typedef struct {
     int32_t layers;       /* coupling layers (6) */
     int32_t batch;        /* points per training step (65536) */
     double lr;            /* Adam step size (1e-3) */
     uint64_t init_seed;   /* weight initialisation */
+    int32_t hidden;       /* hidden units H of a conditioner: 128 or 256 (0: 128) */
+    int32_t depth;        /* hidden layers of a conditioner: 2..4 (0: 2) */
 } chili_flow_params;
 
 typedef struct {

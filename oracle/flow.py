@@ -78,9 +78,10 @@ def masks(dims, layers):
 class Spec:
     """Sizes of the flow and the channel-weight network."""
 
-    def __init__(self, dims, nch, nfeat, layers=6, hidden=128, bins=K_BINS, alpha_hidden=64):
+    def __init__(self, dims, nch, nfeat, layers=6, hidden=128, bins=K_BINS, alpha_hidden=64, depth=2):
         self.dims, self.nch, self.nfeat = dims, nch, nfeat
         self.layers, self.hidden, self.bins, self.alpha_hidden = layers, hidden, bins, alpha_hidden
+        self.depth = depth  # hidden layers of a conditioner (W1, then depth - 1 square matrices)
         self.masks = masks(dims, layers)
         self.cond = [np.where(m)[0] for m in self.masks]
         self.trans = [np.where(~m)[0] for m in self.masks]
@@ -97,7 +98,8 @@ class Spec:
             da, P = len(self.cond[l]), self.nparams[l]
             p[f"W1_{l}"] = rng.uniform(-1, 1, (H, da)) * math.sqrt(6.0 / da)
             p[f"E_{l}"] = np.zeros((self.nch, H))
-            p[f"W2_{l}"] = rng.uniform(-1, 1, (H, H)) * math.sqrt(6.0 / H)
+            for k in range(self.depth - 1):
+                p[w2_name(l, k)] = rng.uniform(-1, 1, (H, H)) * math.sqrt(6.0 / H)
             w3 = np.zeros((P, H))
             for j in range(len(self.trans[l])):
                 o = j * self.per_dim + 2 * self.bins
@@ -111,6 +113,12 @@ class Spec:
         p["A3"] = np.zeros((self.nch, A))
         p["c3"] = np.zeros(self.nch)
         return p
+
+
+def w2_name(l, k):
+    """Name of the k-th square hidden matrix of coupling layer l (W2_l for
+    the first, W2_l_k for the further ones of deeper conditioners)."""
+    return f"W2_{l}" if k == 0 else f"W2_{l}_{k}"
 
 
 def lrelu(x):
@@ -261,14 +269,15 @@ def conditioner(spec, p, l, xa, ch, use_bf16=False):
     # the GPU adds E[c] inside the first tensor-core product (a one-hot column),
     # so in bf16 mode E is rounded like the other operands
     E = bf16(p[f"E_{l}"]) if use_bf16 else p[f"E_{l}"]
-    pre1 = _mm(a0, p[f"W1_{l}"].T, use_bf16) + E[ch]
-    h1 = lrelu(pre1)
-    h1[:, H - 1] = 1.0
-    pre2 = _mm(h1, p[f"W2_{l}"].T, use_bf16)
-    h2 = lrelu(pre2)
-    h2[:, H - 1] = 1.0
-    theta = _mm(h2, p[f"W3_{l}"].T, use_bf16)
-    return theta, (a0, h1, h2)
+    h = lrelu(_mm(a0, p[f"W1_{l}"].T, use_bf16) + E[ch])
+    h[:, H - 1] = 1.0
+    hs = [h]
+    for k in range(spec.depth - 1):
+        h = lrelu(_mm(h, p[w2_name(l, k)].T, use_bf16))
+        h[:, H - 1] = 1.0
+        hs.append(h)
+    theta = _mm(h, p[f"W3_{l}"].T, use_bf16)
+    return theta, (a0, *hs)
 
 
 def flow_forward(spec, p, u, ch, use_bf16=False):
@@ -313,27 +322,26 @@ def flow_backward(spec, p, cache, ch, g_logq, use_bf16=False):
     gx = np.zeros((n, spec.dims))
     for l in reversed(range(spec.layers)):
         ci, ti = spec.cond[l], spec.trans[l]
-        x_in, th, (a0, h1, h2) = cache[l]
+        x_in, th, (a0, *hs) = cache[l]
+        q = bf16 if use_bf16 else (lambda v: v)
         gy = gx[:, ti]
         gj = np.repeat(g_logq[:, None], len(ti), axis=1)
         gth, gxt = spline_backward(th, x_in[:, ti], gy, gj, spec.bins)
         gtheta = gth.reshape(n, -1)
-        gq = bf16(gtheta) if use_bf16 else gtheta
-        grads[f"W3_{l}"] = gq.T @ (bf16(h2) if use_bf16 else h2)
-        gh2 = _mm(gtheta, p[f"W3_{l}"], use_bf16)
-        gh2[:, H - 1] = 0.0
-        gp2 = gh2 * dlrelu(h2)
-        gp2q = bf16(gp2) if use_bf16 else gp2
-        grads[f"W2_{l}"] = gp2q.T @ (bf16(h1) if use_bf16 else h1)
-        gh1 = _mm(gp2, p[f"W2_{l}"], use_bf16)
-        gh1[:, H - 1] = 0.0
-        gp1 = gh1 * dlrelu(h1)
-        gp1q = bf16(gp1) if use_bf16 else gp1
-        grads[f"W1_{l}"] = gp1q.T @ (bf16(a0) if use_bf16 else a0)
+        grads[f"W3_{l}"] = q(gtheta).T @ q(hs[-1])
+        g = _mm(gtheta, p[f"W3_{l}"], use_bf16)  # gradient of the last hidden layer
+        for k in reversed(range(spec.depth)):
+            g[:, H - 1] = 0.0
+            gp = g * dlrelu(hs[k])  # gradient of layer k's pre-activation
+            if k > 0:
+                grads[w2_name(l, k - 1)] = q(gp).T @ q(hs[k - 1])
+                g = _mm(gp, p[w2_name(l, k - 1)], use_bf16)
+        gp1q = q(gp)
+        grads[f"W1_{l}"] = gp1q.T @ q(a0)
         gE = np.zeros((spec.nch, H))
         np.add.at(gE, ch, gp1q)
         grads[f"E_{l}"] = gE
-        ga0 = _mm(gp1, p[f"W1_{l}"], use_bf16)
+        ga0 = _mm(gp, p[f"W1_{l}"], use_bf16)
         gnew = gx.copy()
         gnew[:, ti] = gxt
         gnew[:, ci] += 2 * ga0

@@ -50,9 +50,9 @@ def test_struct_layouts_match_the_header(tmp_path):
 int main(void) {
   S(chili_particle_info) S(chili_decay) S(chili_channel_desc) S(chili_idx_value)
   S(chili_pid_pair_value) S(chili_cuts) S(chili_stats) S(chili_multichannel_params) S(chili_mc_iter_info)
-  S(chili_flow_params) S(chili_flow_iter_info) O(chili_flow_params, init_seed) O(chili_flow_iter_info, unweighting_efficiency)
+  S(chili_flow_params) S(chili_flow_iter_info) O(chili_flow_params, init_seed) O(chili_flow_params, depth) O(chili_flow_iter_info, unweighting_efficiency)
   O(chili_multichannel_params, should_optimize) O(chili_multichannel_params, grid_alpha)
-  O(chili_cuts, etamax) O(chili_mc_iter_info, weight_max) O(chili_mc_iter_info, points_weighted)
+  O(chili_cuts, etamax) O(chili_mc_iter_info, weight_max) O(chili_mc_iter_info, points_weighted) O(chili_mc_iter_info, chunks)
   S(chili_task) S(chili_batch_info) O(chili_task, ncalls) O(chili_task, params) O(chili_task, descs)
   O(chili_task, sqrts) O(chili_task, n_ext) O(chili_task, pre_cuts) O(chili_batch_info, points)
   return 0;
@@ -72,7 +72,9 @@ int main(void) {
     assert int(got["chili_cuts.etamax"]) == abi.Cuts.etamax.offset
     assert int(got["chili_mc_iter_info.weight_max"]) == abi.MCIterInfo.weight_max.offset
     assert int(got["chili_mc_iter_info.points_weighted"]) == abi.MCIterInfo.points_weighted.offset
+    assert int(got["chili_mc_iter_info.chunks"]) == abi.MCIterInfo.chunks.offset
     assert int(got["chili_flow_params.init_seed"]) == abi.FlowParams.init_seed.offset
+    assert int(got["chili_flow_params.depth"]) == abi.FlowParams.depth.offset
     assert int(got["chili_flow_iter_info.unweighting_efficiency"]) == abi.FlowIterInfo.unweighting_efficiency.offset
     for f in ("ncalls", "params", "descs", "sqrts", "n_ext", "pre_cuts"):
         assert int(got["chili_task." + f]) == getattr(abi.Task, f).offset, f

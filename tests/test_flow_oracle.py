@@ -25,9 +25,10 @@ def _batch(rng, n, dims, nch, nfeat):
     return b
 
 
-def test_gradients_match_central_differences():
+@pytest.mark.parametrize("depth", [2, 3])
+def test_gradients_match_central_differences(depth):
     rng = np.random.default_rng(0)
-    spec = F.Spec(10, 3, 10, layers=6, hidden=16)
+    spec = F.Spec(10, 3, 10, layers=6 if depth == 2 else 3, hidden=16, depth=depth)
     p = _perturbed(spec, rng)
     batch = _batch(rng, 40, 10, 3, 10)
     L, g, _ = F.loss_and_grads(spec, p, batch)
@@ -82,13 +83,14 @@ def test_initial_flow_is_the_identity():
     assert np.abs(lq).max() < 1e-12
 
 
-@pytest.mark.parametrize("dims,layers", [(4, 6), (7, 6), (10, 6), (16, 10)])
-def test_host_layout_mirror_matches_the_oracle(dims, layers):
+@pytest.mark.parametrize("dims,layers,hidden,depth", [(4, 6, 128, 2), (7, 6, 128, 2), (10, 6, 128, 2),
+                                                      (16, 10, 128, 2), (10, 10, 256, 3), (7, 4, 128, 4)])
+def test_host_layout_mirror_matches_the_oracle(dims, layers, hidden, depth):
     for a, b in zip(flowspec.masks(dims, layers), F.masks(dims, layers)):
         assert (a == b).all()
-    spec = F.Spec(dims, 15, flowspec.n_features(6), layers=layers)
+    spec = F.Spec(dims, 15, flowspec.n_features(6), layers=layers, hidden=hidden, depth=depth)
     p = spec.init(np.random.default_rng(3))
-    lay = flowspec.layout(dims, 15, 6, layers)
+    lay = flowspec.layout(dims, 15, 6, layers, hidden, depth)
     assert [n for n, _, _ in lay] == list(p.keys())
     for name, _, shape in lay:
         assert tuple(shape) == p[name].shape, name
@@ -104,3 +106,15 @@ def test_bf16_rounding_is_round_to_nearest_even():
     r = F.bf16(x)
     assert r[0] == 1.0 and r[1] == 1.0 and r[2] == 1.0 + 2 ** -6 and r[3] == -2.5 and r[4] == 0.0
     assert abs(r[5] - 3.140625) < 1e-12
+
+
+def test_deeper_conditioner_at_identity_init():
+    """A 3 x 256 conditioner starts as the identity flow like the 2 x 128 one:
+    the last layer is zero apart from the slope bias on the constant unit."""
+    rng = np.random.default_rng(5)
+    spec = F.Spec(10, 15, 10, layers=10, hidden=256, depth=3)
+    p = spec.init(rng)
+    u = rng.random((200, 10))
+    z, lq, _ = F.flow_forward(spec, p, u, rng.integers(0, 15, 200))
+    assert np.abs(z - u).max() < 1e-12
+    assert np.abs(lq).max() < 1e-12
