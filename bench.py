@@ -46,10 +46,12 @@ SEED = 7
 # large 2->6 case. channels(): the channel set; fkind: the integrand.
 WORKLOADS = {
     "multichannel": {"n_out": 4, "bins": 100, "ncalls": 1_000_000, "fkind": "PROPAGATOR", "flow_layers": 6,
+                     "flow_hidden": 128, "flow_depth": 2,
                      "metric": METRIC, "dims": 10, "channels": 15,
                      "describe": "multichannel 2->4 propagator integrand, sqrt(S)=1 TeV, 10 dims",
                      "unweighted_target": None},
     "large": {"n_out": 6, "bins": 200, "ncalls": 10_000_000, "fkind": "PROPAGATOR_TOP2", "flow_layers": 10,
+              "flow_hidden": 256, "flow_depth": 3,
               "metric": "time to 0.1% error & unweighting efficiency, 2->6 (45 channels, 200 bins, 1e7 "
                         "points/iteration): flow vs plain VEGAS, 1 B200, FP64",
               "dims": 16, "channels": 45,
@@ -437,45 +439,26 @@ def compact_other_workloads(args, dev, rank):
     return out
 
 
-# Per-kernel figures of the committed ncu capture
-# (the multichannel 2->4 summary under profiles/): FP64 operations (2*DFMA + DADD +
-# DMUL, executed) and DRAM bytes (read + write), both per weighted point.
+# Per-kernel figures of the committed ncu capture (the multichannel 2->4
+# summary under profiles/): FP64 operations (2*DFMA + DADD + DMUL, executed)
+# and DRAM bytes (read + write) per point of the kernel's basis: drawn
+# counters for the forward kernel (it runs over every drawn point of a
+# chunk), weighted points for the rest.
 KERNEL_COUNTERS = {
-    "k_mc_forward": {
-        "fp64_ops_per_point": 2081.0,
-        "dram_bytes_per_point": 690.5,
-        "source": "profiles/multichannel_2to4_kernels.md"
-    },
-    "k_pp_nodes": {
-        "fp64_ops_per_point": 24.0,
-        "dram_bytes_per_point": 473.3,
-        "source": "profiles/multichannel_2to4_kernels.md"
-    },
-    "k_pp_items": {
-        "fp64_ops_per_point": 9095.2,
-        "dram_bytes_per_point": 1054.4,
-        "source": "profiles/multichannel_2to4_kernels.md"
-    },
-    "k_pp_chains": {
-        "fp64_ops_per_point": 3709.5,
-        "dram_bytes_per_point": 554.6,
-        "source": "profiles/multichannel_2to4_kernels.md"
-    },
-    "k_pp_channel": {
-        "fp64_ops_per_point": 683.9,
-        "dram_bytes_per_point": 1010.0,
-        "source": "profiles/multichannel_2to4_kernels.md"
-    },
-    "k_pp_combine": {
-        "fp64_ops_per_point": 730.5,
-        "dram_bytes_per_point": 411.0,
-        "source": "profiles/multichannel_2to4_kernels.md"
-    },
-    "k_mc_accum": {
-        "fp64_ops_per_point": 336.0,
-        "dram_bytes_per_point": 117.2,
-        "source": "profiles/multichannel_2to4_kernels.md"
-    }
+    "k_mc_forward": {"fp64_ops_per_point": 1868.7, "dram_bytes_per_point": 424.4, "basis": "drawn",
+                     "source": "profiles/multichannel_2to4_kernels.md"},
+    "k_pp_nodes": {"fp64_ops_per_point": 24.0, "dram_bytes_per_point": 838.1, "basis": "weighted",
+                     "source": "profiles/multichannel_2to4_kernels.md"},
+    "k_pp_items": {"fp64_ops_per_point": 9343.5, "dram_bytes_per_point": 1316.3, "basis": "weighted",
+                     "source": "profiles/multichannel_2to4_kernels.md"},
+    "k_pp_chains": {"fp64_ops_per_point": 3684.0, "dram_bytes_per_point": 597.0, "basis": "weighted",
+                     "source": "profiles/multichannel_2to4_kernels.md"},
+    "k_pp_channel": {"fp64_ops_per_point": 684.0, "dram_bytes_per_point": 1077.4, "basis": "weighted",
+                     "source": "profiles/multichannel_2to4_kernels.md"},
+    "k_pp_combine": {"fp64_ops_per_point": 724.0, "dram_bytes_per_point": 416.2, "basis": "weighted",
+                     "source": "profiles/multichannel_2to4_kernels.md"},
+    "k_mc_accum": {"fp64_ops_per_point": 300.0, "dram_bytes_per_point": 32.3, "basis": "weighted",
+                     "source": "profiles/multichannel_2to4_kernels.md"}
 }
 
 
@@ -566,7 +549,8 @@ def measure_flow(ctx, args, dev, stream, plain, train_steps=None):
     from chili_b200 import abi, gpu
     n = int(round(plain["points_per_step"]))
     train_steps = args.flow_steps if train_steps is None else train_steps
-    fp = abi.FlowParams.defaults(batch=args.flow_batch, layers=WL["flow_layers"], lr=1e-3)
+    fp = abi.FlowParams.defaults(batch=args.flow_batch, layers=WL["flow_layers"], lr=1e-3,
+                                 hidden=WL["flow_hidden"], depth=WL["flow_depth"])
     # one-time costs (first launch of each kernel, first allocations) outside
     # the timed training: three steps on a throwaway network, then a fresh one
     ctx.flow_init(fp)
@@ -605,6 +589,23 @@ def measure_flow(ctx, args, dev, stream, plain, train_steps=None):
     ratio = (rv * t_step / n) / (plain["rel_var_per_point"] * t_plain / plain["points_per_step"])
     t01 = next((h[0] for h in history if h[1] <= 1e-3), None)
     pull = (mean - plain["integral"]) / np.hypot(err, plain["rel_error"] * abs(plain["integral"]))
+    # tensor-core roofline of the coupling layers: the conditioners' useful
+    # products (FLOPs from the layer shapes) over the layer kernels' CUDA-event
+    # time, against the sustained cuBLAS bf16 figure (the kernels run inside
+    # long passes); training runs the forward products, the two data-gradient
+    # products of the same shapes and the weight-gradient products (3x)
+    f_pt = flow_flops_per_point(ctx.ndims, WL["flow_layers"], WL["flow_hidden"], WL["flow_depth"])
+    peak_bf16 = measured_peaks().get("bf16_tflops_sustained") or measured_peaks().get("bf16_tflops")
+    lay_ms = k2["k_flow_layer"][0] - k1["k_flow_layer"][0]
+    tr_ms = sum(k1[k][0] - k0[k][0] for k in ("k_flow_layer", "k_flow_layer_bwd", "k_flow_wgrad"))
+    tensor = {"flops_per_point_per_pass": f_pt, "peak": peak_bf16, "unit": "TFLOP/s",
+              "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (cuBLAS bf16, seconds-long loop)"}
+    if lay_ms > 0:
+        a = f_pt * n * args.steps / (lay_ms / 1e3) / 1e12
+        tensor["pass"] = {"achieved": a, "frac": a / peak_bf16 if peak_bf16 else None, "kernel_ms": lay_ms}
+    if tr_ms > 0:
+        a = 3 * f_pt * args.flow_batch * train_steps / (tr_ms / 1e3) / 1e12
+        tensor["training"] = {"achieved": a, "frac": a / peak_bf16 if peak_bf16 else None, "kernel_ms": tr_ms}
     return {
         "value": unw / (ms / 1e3), "unit": UNIT, "ms_per_step": t_step * 1e3, "points_per_step": n,
         "integral": mean, "rel_error": err / abs(mean), "rel_var_per_point": rv,
@@ -615,12 +616,28 @@ def measure_flow(ctx, args, dev, stream, plain, train_steps=None):
         "time_to_0p1pct_with_training_s": (t01 + train_s) if t01 is not None else None,
         "variance_x_time_ratio": ratio, "pull_vs_plain": pull,
         "training": {"steps": train_steps, "batch": args.flow_batch, "layers": WL["flow_layers"],
-                     "hidden": "2 x 128 (unit 127 the constant 1)", "seconds": train_s,
+                     "hidden": f"{WL['flow_depth']} x {WL['flow_hidden']} (unit {WL['flow_hidden'] - 1} the "
+                               f"constant 1; " + ("weights resident in shared memory" if WL["flow_hidden"] == 128
+                                                   and WL["flow_depth"] == 2 else "weights streamed per tile") + ")",
+                     "seconds": train_s,
                      "loss_first": float(np.mean(loss[:10])), "loss_last": float(np.mean(loss[-10:])),
                      "kernel_ms": {k: round(k1[k][0] - k0[k][0], 3) for k in FLOW_KERNELS if k1[k][0] > k0[k][0]}},
         "kernel_ms": {k: round(k2[k][0] - k1[k][0], 3) for k in FLOW_KERNELS if k2[k][0] > k1[k][0]},
         "gpu_launches_note": "flow kernels: tcgen05 coupling layers, FP64 phase space, phased weight pass",
+        "tensor_roofline": tensor,
     }
+
+
+def flow_flops_per_point(dims, layers, hidden, depth):
+    """Useful tensor-core FLOPs of one flow pass per point: per coupling layer
+    2 H da (first product; the channel embedding is a one-hot lookup),
+    2 (depth - 1) H^2 (hidden products) and 2 (49 db) H (spline parameters)."""
+    from chili_b200 import flowspec
+    tot = 0
+    for m in flowspec.masks(dims, layers):
+        da, db = int(m.sum()), int((~m).sum())
+        tot += 2 * hidden * da + 2 * (depth - 1) * hidden * hidden + 2 * flowspec.PER_DIM * db * hidden
+    return tot
 
 
 def measure_unweighted_output(ctx, w_max, dev, rank, n=4_000_000, reps=8):
