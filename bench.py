@@ -269,6 +269,15 @@ def run_chili(args, rank, world, local_rank):
     kernel_ms = {k: ctx.kernel_time(k) for k in TIMED_KERNELS}
     kernel_ms = {k: v for k, v in kernel_ms.items() if v[1] > 0}
     roof = roofline(kernel_ms, weighted, args.ncalls * args.steps, ms, dev, drawn=drawn)
+    # where the step's device time goes: the timed kernel classes, the small
+    # per-round kernels, the end-of-iteration adaptation, and the rest (the
+    # device idle while the host reads a round's counts back and launches)
+    main_ms = sum(v[0] for v in kernel_ms.values())
+    other_ms = ctx.kernel_time("round_other")[0]
+    end_ms = ctx.kernel_time("iteration_end")[0]
+    time_split = {"kernels_ms_per_step": main_ms / args.steps, "round_other_ms_per_step": other_ms / args.steps,
+                  "iteration_end_ms_per_step": end_ms / args.steps,
+                  "rest_ms_per_step": (ms - main_ms - other_ms - end_ms) / args.steps}
 
     plain = {"value": unw_tot / (ms_max / 1e3), "ms_per_step": ms_max / args.steps,
              "points_per_step": tried_tot / args.steps, "integral": mean, "rel_error": err / abs(mean),
@@ -331,6 +340,7 @@ def run_chili(args, rank, world, local_rank):
             "clocks": clk.summary(),
             "gpu_launches": launches,
             "roofline": roof,
+            "time_split": time_split,
             "paths": {"selected": selected, "plain": plain, "flow": flow, "flow_long_training": flow_long},
             "unweighted_output": unw_out,
             "unweighting_quantile": unw_q,

@@ -1163,12 +1163,15 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
                 }
             }
             // offsets of every PreProcess-accepted point (no cut at this stage)
-            k_mc_scan<<<1, 1024, 0, ctx->stream>>>(bcount, static_cast<int>(nbf), flag, mm, mm + 1, gate, 0,
-                                                   ctx->block_off.as<long long>(), ctl_pre);
-            LAUNCHED();
-            k_mc_compact<<<static_cast<unsigned>(nbf), kFwdBlock, 0, ctx->stream>>>(
-                flag, ctx->block_off.as<long long>(), ctl_pre, mm, ctx->list.as<int32_t>());
-            LAUNCHED();
+            {
+                KTimer kt_(ctx, KT_ROUND_OTHER);
+                k_mc_scan<<<1, 1024, 0, ctx->stream>>>(bcount, static_cast<int>(nbf), flag, mm, mm + 1, gate, 0,
+                                                       ctx->block_off.as<long long>(), ctl_pre);
+                LAUNCHED();
+                k_mc_compact<<<static_cast<unsigned>(nbf), kFwdBlock, 0, ctx->stream>>>(
+                    flag, ctx->block_off.as<long long>(), ctl_pre, mm, ctx->list.as<int32_t>());
+                LAUNCHED();
+            }
             if (pipe) {
                 // the launches are sized by the accepted count, read back here;
                 // a queued host-uniform round does not wait for it: its
@@ -1194,14 +1197,17 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
             }
             // the cut: the needed-th record whose value is not NaN (the
             // device's count when the rounds are queued)
-            k_block_count<<<static_cast<unsigned>(nbf), kFwdBlock, 0, ctx->stream>>>(rec_ok, ctl_pre, bcount);
-            LAUNCHED();
-            k_mc_scan<<<1, 1024, 0, ctx->stream>>>(bcount, static_cast<int>(nbf), rec_ok, mm, needed, gate, 1,
-                                                   ctx->block_off.as<long long>(), ctl_list);
-            LAUNCHED();
-            k_cut_finalize<<<1, 1, 0, ctx->stream>>>(ctl_list, ctl_pre, ctx->list.as<int32_t>(), mm, needed,
-                                                     u_host ? iter : nullptr, ctx->ctl.as<RoundCtl>());
-            LAUNCHED();
+            {
+                KTimer kt_(ctx, KT_ROUND_OTHER);
+                k_block_count<<<static_cast<unsigned>(nbf), kFwdBlock, 0, ctx->stream>>>(rec_ok, ctl_pre, bcount);
+                LAUNCHED();
+                k_mc_scan<<<1, 1024, 0, ctx->stream>>>(bcount, static_cast<int>(nbf), rec_ok, mm, needed, gate, 1,
+                                                       ctx->block_off.as<long long>(), ctl_list);
+                LAUNCHED();
+                k_cut_finalize<<<1, 1, 0, ctx->stream>>>(ctl_list, ctl_pre, ctx->list.as<int32_t>(), mm, needed,
+                                                         u_host ? iter : nullptr, ctx->ctl.as<RoundCtl>());
+                LAUNCHED();
+            }
             {
                 KTimer kt_(ctx, KT_ACCUM);
                 k_mc_accum<<<static_cast<unsigned>(nbw), kWgtBlock, acc_smem, ctx->stream>>>(
@@ -1209,13 +1215,16 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
                     rec_dens, opt ? 1 : 0, guard_alpha ? 1 : 0, ctx->hist.as<double>(), ctx->part.as<double>());
             }
             LAUNCHED();
-            k_mc_reduce<<<kPartFixed + nch, 256, 0, ctx->stream>>>(ctx->part.as<double>(), nch,
-                                                                   ctx->ctl.as<RoundCtl>(),
-                                                                   ctx->round_res.as<double>());
-            LAUNCHED();
-            k_mc_accumulate<<<1, 256, 0, ctx->stream>>>(ctx->round_res.as<double>(), nch, ctx->ctl.as<RoundCtl>(),
-                                                        ctx->acc.as<IterAcc>());
-            LAUNCHED();
+            {
+                KTimer kt_(ctx, KT_ROUND_OTHER);
+                k_mc_reduce<<<kPartFixed + nch, 256, 0, ctx->stream>>>(ctx->part.as<double>(), nch,
+                                                                       ctx->ctl.as<RoundCtl>(),
+                                                                       ctx->round_res.as<double>());
+                LAUNCHED();
+                k_mc_accumulate<<<1, 256, 0, ctx->stream>>>(ctx->round_res.as<double>(), nch,
+                                                            ctx->ctl.as<RoundCtl>(), ctx->acc.as<IterAcc>());
+                LAUNCHED();
+            }
             if (u_host) {
                 CK(cudaEventRecord(ctx->round_done[par], ctx->stream));
                 continue;
@@ -1255,6 +1264,7 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
     }
     IterAcc acc_h;
     if (opt && !ctx->defer_train) {
+        KTimer kt_(ctx, KT_ITER_END);
         k_alpha_update<<<1, 32, 0, ctx->stream>>>(alpha_ptr(ctx), best_ptr(ctx), mindiff_ptr(ctx), cp_ptr(ctx),
                                                   acc_train_ptr(ctx), nch, params->beta,
                                                   params->min_alpha, 1);

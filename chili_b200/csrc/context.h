@@ -204,10 +204,14 @@ namespace {
 const char *const kTimedKernels[] = {"k_mc_forward", "k_pp_nodes", "k_pp_items", "k_pp_chains", "k_pp_channel",
                                      "k_pp_combine", "k_mc_weight", "k_mc_accum", "k_vegas_iter", "k_flow_layer",
                                      "k_flow_layer_bwd", "k_flow_wgrad", "k_alpha_train", "k_flow_phys",
-                                     "k_flow_batch", "k_vegas_generate", "k_vegas_step", nullptr};
+                                     "k_flow_batch", "k_vegas_generate", "k_vegas_step", "round_other",
+                                     "iteration_end", nullptr};
+// round_other: the small kernels of a multichannel round (offsets, compaction,
+// the cut, the per-round folds); iteration_end: the channel-weight and grid
+// adaptation after the last round.
 enum { KT_FORWARD, KT_NODES, KT_ITEMS, KT_CHAINS, KT_CHANNEL, KT_COMBINE, KT_WEIGHT, KT_ACCUM, KT_VEGAS,
        KT_FLOW_LAYER, KT_FLOW_BWD, KT_FLOW_WGRAD, KT_ALPHA_TRAIN, KT_FLOW_PHYS, KT_FLOW_BATCH, KT_VEGAS_GEN,
-       KT_VEGAS_STEP };
+       KT_VEGAS_STEP, KT_ROUND_OTHER, KT_ITER_END };
 
 cudaEvent_t take_event(chili_ctx *ctx) {
     if (!ctx->event_pool.empty()) {
