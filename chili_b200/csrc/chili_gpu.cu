@@ -35,6 +35,10 @@ namespace {
 
 int rebuild_hints(chili_ctx *ctx);
 
+// Largest table (one channel's edges, widths, hints) staged in shared memory
+// by k_pp_channel_tab; larger channel tables take k_pp_channel.
+constexpr size_t kMaxChannelTab = 112 * 1024;
+
 template <int D>
 void launch_channel(chili_ctx *ctx, long long base, long long T, long long mr, int bins, int opt,
                     const long long *n_list, int32_t *rec_slot, double *rec_dens, const PPCombine *fuse) {
@@ -45,6 +49,22 @@ void launch_channel(chili_ctx *ctx, long long base, long long T, long long mr, i
             ctx->sorted.as<uint8_t>(), ctx->widths.as<double>(), bins, ctx->memo.as<double>(),
             ctx->cfail.as<uint8_t>(), ctx->ich_tile.as<int32_t>(), n_list, base, T, mr, opt, ctx->dcv.as<double>(),
             ctx->vwv.as<double>(), rec_slot, rec_dens, *fuse);
+        return;
+    }
+    const size_t tab = channel_tab_bytes(D, bins);
+    if (ctx->channel_tables && tab <= kMaxChannelTab) {
+        static size_t attr = 0;  // dynamic shared memory granted so far
+        if (tab > attr) {
+            cudaFuncSetAttribute(k_pp_channel_tab<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(kMaxChannelTab));
+            attr = kMaxChannelTab;
+        }
+        const dim3 gt(ctx->nch, static_cast<unsigned>((T + kTabPoints - 1) / kTabPoints));
+        k_pp_channel_tab<D><<<gt, kTabThreads, tab, ctx->stream>>>(
+            ctx->point_prog.as<PointProgram>(), ctx->edges.as<double>(), ctx->hints.as<uint32_t>(),
+            ctx->sorted.as<uint8_t>(), ctx->widths.as<double>(), bins, ctx->memo.as<double>(),
+            ctx->cfail.as<uint8_t>(), ctx->ich_tile.as<int32_t>(), n_list, base, T, mr, opt, ctx->dcv.as<double>(),
+            ctx->vwv.as<double>(), rec_slot, rec_dens);
         return;
     }
     k_pp_channel<D><<<grid, 128, 0, ctx->stream>>>(
@@ -458,6 +478,10 @@ int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value) {
     }
     if (std::strcmp(name, "batch_phased") == 0) {
         ctx->batch_phased = value != 0;
+        return CHILI_OK;
+    }
+    if (std::strcmp(name, "channel_tables") == 0) {
+        ctx->channel_tables = value != 0;
         return CHILI_OK;
     }
     if (std::strcmp(name, "flow_streamed") == 0) {

@@ -140,6 +140,7 @@ struct chili_ctx {
     bool batch_phased = true;  // option "batch_phased": batched multichannel tasks by the phased weight pass
     bool batch_grouped = true;  // option "batch_grouped": the phased tasks in waves, one launch per step and wave
     long long batch_wave = 1ll << 22;  // option "batch_wave_points": points per wave of the grouped mode
+    bool channel_tables = true;  // option "channel_tables": k_pp_channel with the channel's tables in shared memory
     bool flow_streamed = false;  // option "flow_streamed": streamed-weight coupling kernels even at 2 x 128
     long long batch_wave_streams = 3;  // option "batch_wave_streams": streams the waves alternate over (1..4)
     long long pipe_tile = 1 << 22;  // option "pipeline_tile": points per tile

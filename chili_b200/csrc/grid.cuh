@@ -11,15 +11,24 @@
 
 namespace chili_dev {
 
+// Table reads: through the read-only path (global tables, NC = true) or
+// plain loads (tables staged in shared memory, NC = false).
+template <bool NC, class T>
+__device__ __forceinline__ T tab_ld(const T *p) {
+    if constexpr (NC) return __ldg(p);
+    else return *p;
+}
+
 // std::lower_bound over edges[0..bins) with libstdc++'s probe sequence, then
 // "- 1" as in AdaptiveMap::FindBin (AdaptiveMap.cc:34-38).  Returns -1 where
 // the reference returns SIZE_MAX (x <= edges[0] or x NaN).
+template <bool NC = true>
 __device__ __forceinline__ int find_bin(const double *__restrict__ e, int bins, double x) {
     int first = 0, len = bins;
     while (len > 0) {
         const int half = len >> 1;
         const int mid = first + half;
-        if (__ldg(e + mid) < x) {
+        if (tab_ld<NC>(e + mid) < x) {
             first = mid + 1;
             len = len - half - 1;
         } else {
@@ -55,12 +64,13 @@ __host__ __device__ inline double edge_before_table(int dims, int bins) {
 // width(dim, bin) of the flat edge table, including the reference's reading
 // of bin == SIZE_MAX: lower_edge at flat index dim*(bins+1) - 1 (the previous
 // dimension's last edge, or the word before the table for dim 0).
+template <bool NC = true>
 __device__ __forceinline__ double bin_width(const double *__restrict__ g, int bins, int dim, int bin,
                                             double before) {
     const int base = dim * (bins + 1);
-    if (bin >= 0) return __dsub_rn(__ldg(g + base + bin + 1), __ldg(g + base + bin));
-    const double lower = dim > 0 ? __ldg(g + base - 1) : before;
-    return __dsub_rn(__ldg(g + base), lower);
+    if (bin >= 0) return __dsub_rn(tab_ld<NC>(g + base + bin + 1), tab_ld<NC>(g + base + bin));
+    const double lower = dim > 0 ? tab_ld<NC>(g + base - 1) : before;
+    return __dsub_rn(tab_ld<NC>(g + base), lower);
 }
 
 // AdaptiveMap::operator() (AdaptiveMap.cc:40-56) on one point: x in place,
@@ -118,17 +128,18 @@ __device__ __forceinline__ int edge_cell(double v, int H) {
     return p >= static_cast<double>(H) ? H : static_cast<int>(p);
 }
 
+template <bool NC = true>
 __device__ __forceinline__ int find_bin_hinted(const double *__restrict__ e, const uint32_t *__restrict__ hint,
                                                bool sorted, int bins, int H, double x) {
-    if (!sorted || !(x >= 0.0 && x < 1.0)) return find_bin(e, bins, x);
+    if (!sorted || !(x >= 0.0 && x < 1.0)) return find_bin<NC>(e, bins, x);
     const int c = static_cast<int>(x * static_cast<double>(H));  // < H for x < 1
-    const uint32_t hp = __ldg(hint + c);  // hint[c] | hint[c+1] << 16
+    const uint32_t hp = tab_ld<NC>(hint + c);  // hint[c] | hint[c+1] << 16
     int first = static_cast<int>(hp & 0xffffu);
     int len = static_cast<int>(hp >> 16) - first;
     while (len > 0) {  // lower_bound inside the bracket
         const int half = len >> 1;
         const int mid = first + half;
-        if (__ldg(e + mid) < x) {
+        if (tab_ld<NC>(e + mid) < x) {
             first = mid + 1;
             len = len - half - 1;
         } else {
@@ -141,10 +152,11 @@ __device__ __forceinline__ int find_bin_hinted(const double *__restrict__ e, con
 // width(dim, bin) from the precomputed table wt[dim*bins + bin] (the same
 // subtraction as bin_width, done once per grid), the reference's reading of
 // bin == SIZE_MAX from the edges.
+template <bool NC = true>
 __device__ __forceinline__ double bin_width_t(const double *__restrict__ g, const double *__restrict__ wt, int bins,
                                               int dim, int bin, double before) {
-    if (bin >= 0) return __ldg(wt + dim * bins + bin);
-    return bin_width(g, bins, dim, bin, before);
+    if (bin >= 0) return tab_ld<NC>(wt + dim * bins + bin);
+    return bin_width<NC>(g, bins, dim, bin, before);
 }
 
 }  // namespace chili_dev

@@ -216,7 +216,10 @@ __device__ __forceinline__ void pp_combine_point(const PointProgram *__restrict_
 }
 
 // Channel c's density and VEGAS weight at tile point i (record r).
-template <int DIMS, bool HINTS>
+// TAB: grids / hints / sorted / widths are channel c's own tables staged in
+// shared memory (plain loads), instead of the tables of every channel in
+// global memory.
+template <int DIMS, bool HINTS, bool TAB = false>
 __device__ __forceinline__ void pp_channel_point(
     const PointProgram *__restrict__ pp, const double *__restrict__ grids, const uint32_t *__restrict__ hints,
     const uint8_t *__restrict__ sorted, const double *__restrict__ widths, int bins, const double *__restrict__ memo,
@@ -255,10 +258,10 @@ __device__ __forceinline__ void pp_channel_point(
     const int H = kHintPerBin * bins;
     const double fb = static_cast<double>(bins);
     const double before = edge_before_table(DIMS, bins);
-    const double *g = grids + static_cast<size_t>(c) * DIMS * (bins + 1);
-    const uint32_t *hc = HINTS ? hints + static_cast<size_t>(c) * DIMS * H : nullptr;
-    const double *wc = HINTS ? widths + static_cast<size_t>(c) * DIMS * bins : nullptr;
-    const uint8_t *sc = HINTS ? sorted + c * DIMS : nullptr;
+    const double *g = TAB ? grids : grids + static_cast<size_t>(c) * DIMS * (bins + 1);
+    const uint32_t *hc = HINTS ? (TAB ? hints : hints + static_cast<size_t>(c) * DIMS * H) : nullptr;
+    const double *wc = HINTS ? (TAB ? widths : widths + static_cast<size_t>(c) * DIMS * bins) : nullptr;
+    const uint8_t *sc = HINTS ? (TAB ? sorted : sorted + c * DIMS) : nullptr;
     const bool chosen = should_opt && c == ich_tile[i];
     double vw = 1.0;
 #pragma unroll
@@ -266,11 +269,11 @@ __device__ __forceinline__ void pp_channel_point(
         int b;
         double wdt;
         if constexpr (HINTS) {
-            b = find_bin_hinted(g + p * (bins + 1), hc + p * H, __ldg(sc + p) != 0, bins, H, x[p]);
-            wdt = bin_width_t(g, wc, bins, p, b, before);
+            b = find_bin_hinted<!TAB>(g + p * (bins + 1), hc + p * H, tab_ld<!TAB>(sc + p) != 0, bins, H, x[p]);
+            wdt = bin_width_t<!TAB>(g, wc, bins, p, b, before);
         } else {
-            b = find_bin(g + p * (bins + 1), bins, x[p]);
-            wdt = bin_width(g, bins, p, b, before);
+            b = find_bin<!TAB>(g + p * (bins + 1), bins, x[p]);
+            wdt = bin_width<!TAB>(g, bins, p, b, before);
         }
         vw = __dmul_rn(vw, __dmul_rn(wdt, fb));
         if (chosen) {

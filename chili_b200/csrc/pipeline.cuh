@@ -61,6 +61,54 @@ __global__ void __launch_bounds__(256) k_pp_chains(const PointProgram *__restric
 }
 
 
+// k_pp_channel with channel c's edge, hint, width and monotone tables staged
+// in shared memory (blockIdx.x = c, kTabPoints points per block): the bin
+// searches' scattered reads hit shared memory instead of L1, where the tables
+// of all channels do not fit. The same per-point function and arithmetic as
+// k_pp_channel.
+constexpr int kTabPoints = 1024;
+constexpr int kTabThreads = 256;
+
+// Shared-memory bytes of one channel's tables.
+__host__ __device__ inline size_t channel_tab_bytes(int dims, int bins) {
+    const size_t H = static_cast<size_t>(kHintPerBin) * bins;
+    return 8 * static_cast<size_t>(dims) * (2 * bins + 1) + 4 * dims * H + dims;
+}
+
+template <int DIMS>
+__global__ void __launch_bounds__(kTabThreads) k_pp_channel_tab(
+    const PointProgram *__restrict__ pp, const double *__restrict__ grids, const uint32_t *__restrict__ hints,
+    const uint8_t *__restrict__ sorted, const double *__restrict__ widths, int bins, const double *__restrict__ memo,
+    const uint8_t *__restrict__ cfail, const int32_t *__restrict__ ich_tile, const long long *__restrict__ n_list,
+    long long base, long long m, long long mr, int should_opt, double *__restrict__ dcv, double *__restrict__ vwv,
+    int32_t *__restrict__ rec_slot, double *__restrict__ rec_dens) {
+    extern __shared__ double tab[];
+    const int c = blockIdx.x;
+    const int H = kHintPerBin * bins;
+    const int ne = DIMS * (bins + 1), nw = DIMS * bins, nh = DIMS * H;
+    double *se = tab;
+    double *sw = se + ne;
+    uint32_t *sh = reinterpret_cast<uint32_t *>(sw + nw);
+    uint8_t *ss = reinterpret_cast<uint8_t *>(sh + nh);
+    const double *ge = grids + static_cast<size_t>(c) * ne;
+    const double *gw = widths + static_cast<size_t>(c) * nw;
+    const uint32_t *gh = hints + static_cast<size_t>(c) * nh;
+    for (int k = threadIdx.x; k < ne; k += kTabThreads) se[k] = __ldg(ge + k);
+    for (int k = threadIdx.x; k < nw; k += kTabThreads) sw[k] = __ldg(gw + k);
+    for (int k = threadIdx.x; k < nh; k += kTabThreads) sh[k] = __ldg(gh + k);
+    if (threadIdx.x < DIMS) ss[threadIdx.x] = __ldg(sorted + c * DIMS + threadIdx.x);
+    __syncthreads();
+    const long long n = *n_list;
+#pragma unroll 1
+    for (int j = 0; j < kTabPoints / kTabThreads; ++j) {
+        const long long i = blockIdx.y * static_cast<long long>(kTabPoints) + j * kTabThreads + threadIdx.x;
+        const long long r = base + i;
+        if (i < m && r < n)
+            pp_channel_point<DIMS, true, true>(pp, se, sh, ss, sw, bins, memo, cfail, ich_tile, m, mr, should_opt,
+                                               dcv, vwv, rec_slot, rec_dens, i, r, c);
+    }
+}
+
 // The combine step fused into k_pp_channel: the last of a point block's
 // nch channel blocks to finish (an arrival counter per point block, reset by
 // that block for the next launch) runs k_pp_combine's per-point work on the

@@ -210,6 +210,9 @@ uint64_t chili_gpu_launch_count(const chili_ctx *ctx);
  * channel set has a shared-entry program with the phased weight pass (task
  * chains as parallel graph branches); 0 evaluates every point in one thread
  * of the persistent batch kernel.  Read by chili_gpu_batch_set.
+ * "channel_tables": 1 (default) stages each channel's edge, hint and width
+ * tables in shared memory for the bin searches of the phased weight pass
+ * (tables up to 112 KB), 0 reads them from global memory; the same numbers.
  * "flow_streamed": 1 runs a learned proposal of 2 x 128 hidden units on the
  * streamed-weight coupling kernels that wider or deeper conditioners always
  * use (the same function; a cross-check of the two kernel families), 0

@@ -239,6 +239,7 @@ def test_combined_weight(ctx_factory, rng, mc2, point_program):
 
 WEIGHT_PATHS = {"pipeline": dict(point_program=1, pipeline=1),
                 "pipeline_fused_combine": dict(point_program=1, pipeline=1, pipeline_fuse=1),
+                "pipeline_global_tables": dict(point_program=1, pipeline=1, channel_tables=0),
                 "fused_point_program": dict(point_program=1, pipeline=0),
                 "per_channel": dict(point_program=0, pipeline=0)}
 
@@ -361,3 +362,29 @@ def test_constructed_channels_iterate_like_the_reference(ctx_factory, rng):
     # ~1e-7 per point (seen on B200 over random grids: 5e-11 .. 1e-9)
     assert rel(st.sum, st_r.sum) < 5e-9 and rel(st.sum2, st_r.sum2) < 2e-8
     assert np.max(rel(ctx.get_alpha()[0], R.get_alpha()[0])) < 1e-8
+
+
+def test_channel_tables_in_shared_memory_are_bit_identical(ctx_factory, rng):
+    """The phased weight pass with each channel's bin-search tables staged in
+    shared memory gives the same bits as with the tables read from global
+    memory: StatsData, channel weights and adapted grids over adapting
+    iterations of the 2->4 workload on the device's own uniforms."""
+    cs = workloads.channel_set(4)
+    out = []
+    for tables in (1, 0):
+        ctx = ctx_factory()
+        ctx.set_option("channel_tables", tables)
+        ctx.set_channels(cs)
+        ctx.uniform_grids(cs.nch, ctx.ndims, 100)
+        ctx.set_integrand(abi.CHILI_FUNC_PROPAGATOR, channels.propagator_params())
+        ctx.set_preprocess_cuts(cs.sqrts)
+        params = workloads.mc_params(100_000)
+        c, sts = 0, []
+        for _ in range(4):
+            st, info = ctx.multichannel_iterate(params, seed=3, counter=c, guard=True)
+            c += info.points_tried
+            sts.append(st.as_tuple())
+        out.append((sts, ctx.get_alpha()[0], ctx.get_grids()))
+    assert out[0][0] == out[1][0]
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][2], out[1][2])
