@@ -367,8 +367,10 @@ def test_constructed_channels_iterate_like_the_reference(ctx_factory, rng):
 def test_channel_tables_in_shared_memory_are_bit_identical(ctx_factory, rng):
     """The phased weight pass with each channel's bin-search tables staged in
     shared memory gives the same bits as with the tables read from global
-    memory: StatsData, channel weights and adapted grids over adapting
-    iterations of the 2->4 workload on the device's own uniforms."""
+    memory: the first iteration's StatsData of the 2->4 workload on the
+    device's own uniforms. Later iterations start from grids adapted on
+    histograms summed with FP64 atomics, whose order varies from run to run,
+    so they agree to rounding."""
     cs = workloads.channel_set(4)
     out = []
     for tables in (1, 0):
@@ -385,6 +387,9 @@ def test_channel_tables_in_shared_memory_are_bit_identical(ctx_factory, rng):
             c += info.points_tried
             sts.append(st.as_tuple())
         out.append((sts, ctx.get_alpha()[0], ctx.get_grids()))
-    assert out[0][0] == out[1][0]
-    assert np.array_equal(out[0][1], out[1][1])
-    assert np.array_equal(out[0][2], out[1][2])
+    assert out[0][0][0] == out[1][0][0]
+    for a, b in zip(out[0][0][1:], out[1][0][1:]):
+        assert a[0] == b[0] and a[5] == b[5]
+        assert all(rel(x, y) < 1e-11 for x, y in zip(a[2:5], b[2:5]))
+    assert np.allclose(out[0][1], out[1][1], rtol=1e-10, atol=0)
+    assert np.allclose(out[0][2], out[1][2], rtol=1e-10, atol=0)
