@@ -218,23 +218,25 @@ namespace {
 
 // Host uniforms u[m][D+1]: rows [0, m) are copied into the staging buffer
 // in slices on the context's copy stream, slice s followed by
-// copy_events[s]: a first slice of kFirstSlice rows (the only copy nothing
-// overlaps), a second of kSecondSlice, then slices of kUploadSlice rows
-// (the copy of a slice takes a little less than its weight pass, so the
-// copies stay ahead).  The rounds of the iteration take one slice each, so
-// that the upload of the next slices overlaps the whole weight pass of
-// this one.
+// copy_events[s]: slices that double from kFirstSlice rows (the only copy
+// nothing overlaps) up to kUploadSlice rows, so that the weight passes start
+// early and the copies, a little faster per row than the weight pass, stay
+// ahead.  The rounds of the iteration take one slice each, so that the
+// upload of the next slices overlaps the whole weight pass of this one.
 constexpr long long kFirstSlice = 1ll << 16;   // rows; both multiples of kFwdBlock
 constexpr long long kUploadSlice = 1ll << 19;
-constexpr long long kSecondSlice = 1ll << 18;
 
+long long slice_rows(long long s) { return s >= 3 ? kUploadSlice : std::min(kUploadSlice, kFirstSlice << s); }
 long long slice_begin(long long s) {
-    return s == 0 ? 0 : s == 1 ? kFirstSlice : kFirstSlice + kSecondSlice + (s - 2) * kUploadSlice;
+    long long b = 0;
+    for (long long j = 0; j < s && j < 3; ++j) b += slice_rows(j);
+    if (s > 3) b += (s - 3) * kUploadSlice;
+    return b;
 }
 long long slice_count(long long m) {
-    if (m <= kFirstSlice) return 1;
-    if (m <= kFirstSlice + kSecondSlice) return 2;
-    return 2 + (m - kFirstSlice - kSecondSlice + kUploadSlice - 1) / kUploadSlice;
+    long long n = 0;
+    while (slice_begin(n) < m) ++n;
+    return std::max(n, 1ll);
 }
 
 int upload_host(chili_ctx *ctx, const double *u, long long m) {
