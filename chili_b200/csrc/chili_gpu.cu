@@ -79,7 +79,10 @@ void launch_channel(chili_ctx *ctx, long long base, long long T, long long mr, i
 // The phased weight pass (pipeline.cuh) over the n_pre listed points of a
 // momenta buffer of m points (list: their indices, ich: their channels,
 // n_list: the device-side count), in tiles of at most ctx->pipe_tile points
-// so that a tile's buffers stay in L2; `combine` launches the last step of
+// (option "pipeline_tile"; the default 2^22 makes one tile of a chunk, whose
+// intermediates go through HBM: tiles small enough for their buffers to stay
+// in L2 were measured slower, every launch's tail growing with the launch
+// count); `combine` launches the last step of
 // each tile (it reads the per-channel densities ctx->dcv, ctx->vwv and the
 // nodes ctx->node_soa of the tile).
 int pipeline_run(chili_ctx *ctx, const double *mom_soa, long long m, const int32_t *list, const int32_t *ich,
