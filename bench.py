@@ -36,8 +36,8 @@ sys.path.insert(0, ROOT)
 
 TIMED_KERNELS = ["k_mc_forward", "k_pp_nodes", "k_pp_items", "k_pp_chains", "k_pp_channel", "k_pp_combine",
                  "k_mc_weight", "k_mc_accum"]
-FLOW_KERNELS = ["k_flow_layer", "k_flow_layer_bwd", "k_flow_wgrad", "k_alpha_train", "k_flow_phys", "k_flow_batch",
-                "k_pp_nodes", "k_pp_items", "k_pp_chains", "k_pp_channel"]
+FLOW_KERNELS = ["k_flow_layer", "k_flow_layer_bwd", "k_flow_wgrad", "k_alpha_train", "k_alpha_eval", "k_flow_phys",
+                "k_flow_batch", "k_pp_nodes", "k_pp_items", "k_pp_chains", "k_pp_channel"]
 METRIC = "time to 0.1% error & unweighted events/s: flow vs plain VEGAS, 1 B200, FP64"
 UNIT = "unweighted events/s"
 SEED = 7
@@ -562,9 +562,11 @@ def measure_flow(ctx, args, dev, stream, plain, train_steps=None):
     fp = abi.FlowParams.defaults(batch=args.flow_batch, layers=WL["flow_layers"], lr=1e-3,
                                  hidden=WL["flow_hidden"], depth=WL["flow_depth"])
     # one-time costs (first launch of each kernel, first allocations) outside
-    # the timed training: three steps on a throwaway network, then a fresh one
+    # the timed training: three steps and one sampling pass on a throwaway
+    # network, then a fresh one
     ctx.flow_init(fp)
     ctx.flow_train(3, seed=SEED + 76, counter=0)
+    ctx.flow_iterate(n, seed=SEED + 75, counter=0)
     torch.cuda.synchronize(dev)
     ctx.flow_init(fp)
     k0 = {k: ctx.kernel_time(k) for k in FLOW_KERNELS}

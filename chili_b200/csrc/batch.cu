@@ -454,16 +454,27 @@ __global__ void __launch_bounds__(256) k_g_chains(WaveDev W, int lo, int hi, lon
                     lb / P.n_chains);
 }
 
-// Pieces [lo, hi) of the wave have DIMS dimensions.
-template <int DIMS>
+// Pieces [lo, hi) of the wave have DIMS dimensions. A block works on one
+// channel c of one piece; TAB: the block first stages channel c's edges
+// (DIMS x (bins + 1) doubles, dynamic shared memory) and its bin searches
+// read them there instead of through L1 from global memory.
+template <int DIMS, bool TAB>
 __global__ void __launch_bounds__(128) k_g_channel(WaveDev W, int lo, int hi, long long blk0) {
     CHILI_PIECE(GS_CHANNEL)
     const int c = static_cast<int>(lb % P.nch);
     const long long i = (lb / P.nch) * 128 + threadIdx.x;
+    const double *g = P.grids;
+    if constexpr (TAB) {
+        extern __shared__ double se[];
+        const int ne = DIMS * (P.bins + 1);
+        const double *ge = P.grids + static_cast<size_t>(c) * ne;
+        for (int k = threadIdx.x; k < ne; k += 128) se[k] = __ldg(ge + k);
+        __syncthreads();
+        g = se;
+    }
     if (i < P.ms && i < P.ctl->n_acc)
-        pp_channel_point<DIMS, false>(P.pp, P.grids, nullptr, nullptr, nullptr, P.bins, P.memo, P.cfail,
-                                      P.ich_tile,
-                                      P.ms, P.ms, 1, P.dcv, P.vwv, P.slot, P.dens, i, i, c);
+        pp_channel_point<DIMS, false, TAB>(P.pp, g, nullptr, nullptr, nullptr, P.bins, P.memo, P.cfail, P.ich_tile,
+                                           P.ms, P.ms, 1, P.dcv, P.vwv, P.slot, P.dens, i, i, c);
 }
 
 __global__ void __launch_bounds__(256) k_g_combine(WaveDev W, int lo, int hi, long long blk0) {
@@ -594,7 +605,7 @@ struct BatchState {
         int first = 0, n = 0;                        // pieces [first, first + n)
         long long prefix_off = 0;                    // into d_prefix
         std::vector<long long> blocks;               // per step: total blocks
-        std::vector<std::array<int, 3>> dgroups;     // (dims, k0, k1): pieces [k0, k1) of one dimension
+        std::vector<std::array<int, 4>> dgroups;     // (dims, k0, k1, bins): pieces [k0, k1) of one dimension, their most bins
     };
     std::vector<Piece> pieces;
     std::vector<WaveHost> waves;
@@ -780,10 +791,16 @@ int enqueue_waves(chili_ctx *ctx, const BatchDev &B) {
         for (const auto &g : w.dgroups) {
             const long long b0 = pc[g[1]], nbk = pc[g[2]] - b0;
             if (nbk <= 0) continue;
+            // one channel's edges in shared memory when they fit the default 48 KB
+            const size_t tab = sizeof(double) * static_cast<size_t>(g[0]) * (g[3] + 1);
+            const bool use_tab = ctx->channel_tables && tab <= 48 * 1024;
             switch (g[0]) {
 #define CHILI_GCH(D)                                                                                        \
     case D:                                                                                                 \
-        k_g_channel<D><<<static_cast<unsigned>(nbk), 128, 0, ctx->stream>>>(W, g[1], g[2], b0);            \
+        if (use_tab)                                                                                        \
+            k_g_channel<D, true><<<static_cast<unsigned>(nbk), 128, tab, ctx->stream>>>(W, g[1], g[2], b0); \
+        else                                                                                                \
+            k_g_channel<D, false><<<static_cast<unsigned>(nbk), 128, 0, ctx->stream>>>(W, g[1], g[2], b0);  \
         break;
                 CHILI_GCH(1) CHILI_GCH(4) CHILI_GCH(7) CHILI_GCH(10) CHILI_GCH(13) CHILI_GCH(16) CHILI_GCH(19)
                 CHILI_GCH(22)
@@ -1060,10 +1077,12 @@ int plan_waves(chili_ctx *ctx, const std::vector<PointProgram> &pps) {
             const long long nblk[kGroupSteps] = {P.nb, P.nb, gx, P.n_items[0] * gx, P.n_items[1] * gx,
                                                  P.n_items[2] * gx, P.n_chains * gx, P.nch * gy, gx, P.nb};
             for (int st = 0; st < kGroupSteps; ++st) pre[static_cast<size_t>(st)][k + 1] = pre[st][k] + nblk[st];
-            if (wh.dgroups.empty() || wh.dgroups.back()[0] != P.dims)
-                wh.dgroups.push_back({P.dims, static_cast<int>(k), static_cast<int>(k) + 1});
-            else
+            if (wh.dgroups.empty() || wh.dgroups.back()[0] != P.dims) {
+                wh.dgroups.push_back({P.dims, static_cast<int>(k), static_cast<int>(k) + 1, P.bins});
+            } else {
                 wh.dgroups.back()[2] = static_cast<int>(k) + 1;
+                wh.dgroups.back()[3] = std::max(wh.dgroups.back()[3], P.bins);
+            }
         }
         for (int st = 0; st < kGroupSteps; ++st) {
             wh.blocks.push_back(pre[static_cast<size_t>(st)][w.size()]);

@@ -341,7 +341,9 @@ int chili_gpu_create(int device, chili_ctx **out) {
         return fail(nullptr, CHILI_ERR_CUDA, "cudaMallocHost failed");
     }
     cudaDeviceGetAttribute(&ctx->max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
     cudaFuncSetAttribute(k_mc_accum, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->max_smem_optin);
+    cudaFuncSetAttribute(k_mc_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->max_smem_optin);
     cudaFuncSetAttribute(k_vegas_iter<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->max_smem_optin);
     cudaFuncSetAttribute(k_grid_adapt, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->max_smem_optin);
     cudaGetLastError();
@@ -483,6 +485,10 @@ int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value) {
     }
     if (std::strcmp(name, "batch_phased") == 0) {
         ctx->batch_phased = value != 0;
+        return CHILI_OK;
+    }
+    if (std::strcmp(name, "hist_shared") == 0) {
+        ctx->hist_shared = value != 0;
         return CHILI_OK;
     }
     if (std::strcmp(name, "channel_tables") == 0) {
@@ -1076,6 +1082,9 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         CK(cudaMemcpyAsync(ctx->acc.p, &a0, sizeof(IterAcc), cudaMemcpyHostToDevice, ctx->stream));
     }
     const size_t acc_smem = sizeof(double) * (kWgtBlock / 32) * nch;
+    // the histogram adds staged in shared memory when one block can hold the
+    // whole histogram (option "hist_shared")
+    const bool hist_smem = ctx->hist_shared && sizeof(double) * hist_n <= static_cast<size_t>(ctx->max_smem_optin);
 
     long long needed = ncalls, tried = 0, weighted = 0, drawn = 0, chunks = 0;
     unsigned long long rounds = 0;
@@ -1241,9 +1250,17 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
                 KTimer kt_(ctx, KT_ACCUM);
                 k_mc_accum<<<static_cast<unsigned>(nbw), kWgtBlock, acc_smem, ctx->stream>>>(
                     ctx->ctl.as<RoundCtl>(), mm, nch, D, static_cast<int>(hist_n), rec_val, rec_wgt, rec_ok, rec_slot,
-                    rec_dens, opt ? 1 : 0, guard_alpha ? 1 : 0, ctx->hist.as<double>(), ctx->part.as<double>());
+                    rec_dens, opt ? 1 : 0, guard_alpha ? 1 : 0, hist_smem ? nullptr : ctx->hist.as<double>(),
+                    ctx->part.as<double>());
+                LAUNCHED();
+                if (hist_smem && opt) {
+                    k_mc_hist<<<static_cast<unsigned>(std::min<long long>(nbw, ctx->sms)), 1024,
+                                sizeof(double) * hist_n, ctx->stream>>>(ctx->ctl.as<RoundCtl>(), mm, D,
+                                                                        static_cast<int>(hist_n), rec_val, rec_slot,
+                                                                        ctx->hist.as<double>());
+                    LAUNCHED();
+                }
             }
-            LAUNCHED();
             {
                 KTimer kt_(ctx, KT_ROUND_OTHER);
                 k_mc_reduce<<<kPartFixed + nch, 256, 0, ctx->stream>>>(ctx->part.as<double>(), nch,

@@ -140,7 +140,9 @@ struct chili_ctx {
     bool batch_phased = true;  // option "batch_phased": batched multichannel tasks by the phased weight pass
     bool batch_grouped = true;  // option "batch_grouped": the phased tasks in waves, one launch per step and wave
     long long batch_wave = 1ll << 22;  // option "batch_wave_points": points per wave of the grouped mode
-    bool channel_tables = true;  // option "channel_tables": k_pp_channel with the channel's tables in shared memory
+    bool hist_shared = true;     // option "hist_shared": the iteration's histogram adds staged in shared memory
+    bool channel_tables = true;  // option "channel_tables": k_pp_channel (and the batch's k_g_channel) with the
+                                 // channel's tables in shared memory
     bool flow_streamed = false;  // option "flow_streamed": streamed-weight coupling kernels even at 2 x 128
     long long batch_wave_streams = 3;  // option "batch_wave_streams": streams the waves alternate over (1..4)
     long long pipe_tile = 1 << 22;  // option "pipeline_tile": points per tile
@@ -176,6 +178,7 @@ struct chili_ctx {
     // staging of host buffers
     DevBuf stage[kStageSlots];
     int max_smem_optin = 0;
+    int sms = 148;  // streaming multiprocessors of the device
     // option "kernel_timing": CUDA events around the iteration's kernels
     bool timing = false;
     struct Pending {
@@ -206,13 +209,13 @@ const char *const kTimedKernels[] = {"k_mc_forward", "k_pp_nodes", "k_pp_items",
                                      "k_pp_combine", "k_mc_weight", "k_mc_accum", "k_vegas_iter", "k_flow_layer",
                                      "k_flow_layer_bwd", "k_flow_wgrad", "k_alpha_train", "k_flow_phys",
                                      "k_flow_batch", "k_vegas_generate", "k_vegas_step", "round_other",
-                                     "iteration_end", nullptr};
+                                     "iteration_end", "k_alpha_eval", nullptr};
 // round_other: the small kernels of a multichannel round (offsets, compaction,
 // the cut, the per-round folds); iteration_end: the channel-weight and grid
 // adaptation after the last round.
 enum { KT_FORWARD, KT_NODES, KT_ITEMS, KT_CHAINS, KT_CHANNEL, KT_COMBINE, KT_WEIGHT, KT_ACCUM, KT_VEGAS,
        KT_FLOW_LAYER, KT_FLOW_BWD, KT_FLOW_WGRAD, KT_ALPHA_TRAIN, KT_FLOW_PHYS, KT_FLOW_BATCH, KT_VEGAS_GEN,
-       KT_VEGAS_STEP, KT_ROUND_OTHER, KT_ITER_END };
+       KT_VEGAS_STEP, KT_ROUND_OTHER, KT_ITER_END, KT_ALPHA_EVAL };
 
 cudaEvent_t take_event(chili_ctx *ctx) {
     if (!ctx->event_pool.empty()) {

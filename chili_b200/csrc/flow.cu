@@ -34,7 +34,7 @@ struct FlowState {
     DevBuf hsw, gpsw, gthsw;  // streamed kernels: saved activations, g_p tiles, g_theta tiles
     long long np_flow = 0, np = 0, off_alpha = 0;
     AlphaLayout AL{};
-    DevBuf prm, m, v, grad, wtiles, part_f, part_a, loss_part, loss_dev;
+    DevBuf prm, m, v, grad, wtiles, atiles, part_f, part_a, loss_part, loss_dev;
     DevBuf beta, logbeta, cp;  // f32 beta, f32 log beta, f64 selection table
     std::vector<double> beta_host;
     // training
@@ -43,8 +43,9 @@ struct FlowState {
     double log_fscale = 0;
     bool have_scale = false;
     int adam_t = 0;
-    // sampling
+    // sampling; the channel-weight network's rows of a sampling chunk
     DevBuf sx0, sx1, sz, su, sch, slq, spart, sfold, fv;
+    DevBuf slogf, sfeat, slogprior, sfval;
     // points of the flow path: momenta [leg][4][m], list, count
     DevBuf fmom, flist, fcount;
     DevBuf err;
@@ -134,6 +135,7 @@ int upload_beta(chili_ctx *ctx) {
 int pack_tiles(chili_ctx *ctx) {
     FlowState &S = *ctx->flow;
     const float *p = S.prm.as<float>();
+    if (int rc = flow_launch_alpha_pack(ctx, p + S.off_alpha, S.AL, S.atiles.as<uint8_t>())) return rc;
     if (S.streamed) {
         for (int l = 0; l < S.L; ++l) {
             WidePackArgs a{};
@@ -333,9 +335,10 @@ int train_pass(chili_ctx *ctx, long long n, float lr, int slot) {
         if (int rc = layer_forward(ctx, l, 0, true, n, X + xs * l, X + xs * (l + 1), S.chb.as<int32_t>(),
                                    S.logq.as<float>(), S.thetas.as<float>() + thn * l))
             return rc;
-    AlphaTrainArgs aa{};
+    AlphaTcArgs aa{};
     aa.n = n;
     aa.L = S.AL;
+    aa.tiles = S.atiles.as<uint8_t>();
     aa.w = S.prm.as<float>() + S.off_alpha;
     aa.feat = S.feat.as<float>();
     aa.logprior = S.logprior.as<float>();
@@ -346,6 +349,7 @@ int train_pass(chili_ctx *ctx, long long n, float lr, int slot) {
     aa.glogq = S.glogq.as<float>();
     aa.part = S.part_a.as<float>();
     aa.loss_part = S.loss_part.as<double>();
+    aa.err = S.err.as<int>();
     if (int rc = flow_launch_alpha(ctx, aa)) return rc;
     float *gcur = S.g0.as<float>(), *gnext = S.g1.as<float>();
     for (int l = S.L - 1; l >= 0; --l) {
@@ -419,21 +423,30 @@ int train_pass(chili_ctx *ctx, long long n, float lr, int slot) {
 // m points of the flow path. Training (train = true): u uniform and c ~ beta
 // from counters ctr0 ..., written to u/ch, and the batch rows (log F,
 // features, log prior, F when fval is given). Sampling: u and ch given, the
-// values v of the points. Both: VEGAS map, FSMapper, PreProcess, then every
-// channel's density through the phased weight pass.
+// rows of the chunk, then the values v of the points (the channel-weight
+// network on the tensor cores). Both: VEGAS map, FSMapper, PreProcess, then
+// every channel's density through the phased weight pass.
 int flow_points(chili_ctx *ctx, bool train, long long m, uint64_t seed, uint64_t ctr0, float *u, int32_t *ch,
                 const float *logq, double *fval) {
     FlowState &S = *ctx->flow;
     CK(S.fmom.ensure(sizeof(double) * 4 * S.n_ext * m));
     CK(S.flist.ensure(sizeof(int32_t) * m));
     CK(S.fcount.ensure(sizeof(long long)));
+    float *logf = S.logf.as<float>(), *feat = S.feat.as<float>(), *logprior = S.logprior.as<float>();
+    if (!train) {
+        CK(S.slogf.ensure(sizeof(float) * m));
+        CK(S.sfeat.ensure(sizeof(float) * std::max(S.F, 1) * m));
+        CK(S.slogprior.ensure(sizeof(float) * S.nch * m));
+        CK(S.sfval.ensure(sizeof(double) * m));
+        logf = S.slogf.as<float>();
+        feat = S.sfeat.as<float>();
+        logprior = S.slogprior.as<float>();
+        fval = S.sfval.as<double>();
+    }
     CK(cudaMemsetAsync(S.fcount.p, 0, sizeof(long long), ctx->stream));
     const unsigned gb = static_cast<unsigned>((m + 127) / 128);
-    if (train) {
-        k_flow_rows_init<<<gb, 128, 0, ctx->stream>>>(m, S.nch, S.F, S.logbeta.as<float>(), S.logf.as<float>(),
-                                                      S.feat.as<float>(), S.logprior.as<float>(), fval);
-        LAUNCHED();
-    }
+    k_flow_rows_init<<<gb, 128, 0, ctx->stream>>>(m, S.nch, S.F, S.logbeta.as<float>(), logf, feat, logprior, fval);
+    LAUNCHED();
     GenArgs g{};
     g.progs = ctx->progs.as<ChannelProgram>();
     g.grids = ctx->edges.as<double>();
@@ -460,37 +473,52 @@ int flow_points(chili_ctx *ctx, bool train, long long m, uint64_t seed, uint64_t
     long long n_acc = 0;
     CK(cudaMemcpyAsync(&n_acc, S.fcount.p, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    if (n_acc == 0) return CHILI_OK;
-    CombineArgs c{};
-    c.list = S.flist.as<int32_t>();
-    c.count = S.fcount.as<long long>();
-    c.m = m;
-    c.nch = S.nch;
-    c.n_ext = S.n_ext;
-    c.sqrts = ctx->sqrts;
-    c.f = ctx->f_dev.as<IntegrandDesc>();
-    c.beta = S.beta.as<float>();
-    c.logbeta = S.logbeta.as<float>();
-    c.log_fscale = S.log_fscale;
-    c.logf = S.logf.as<float>();
-    c.fval = fval;
-    c.feat = S.feat.as<float>();
-    c.logprior = S.logprior.as<float>();
-    c.logq = logq;
-    c.w = S.prm.as<float>() + S.off_alpha;
-    c.L = S.AL;
-    c.v = S.fv.as<double>();
-    return pipeline_run(ctx, S.fmom.as<double>(), m, S.flist.as<int32_t>(), ch, S.fcount.as<long long>(), n_acc,
-                        ctx->bins, false, nullptr, nullptr, [&](long long base, long long T) -> int {
-                            CombineArgs t = c;
-                            t.node_soa = ctx->node_soa.as<double>();
-                            t.dcv = ctx->dcv.as<double>();
-                            t.vwv = ctx->vwv.as<double>();
-                            t.ich_tile = ctx->ich_tile.as<int32_t>();
-                            t.base = base;
-                            t.T = T;
-                            return flow_launch_combine(ctx, train, t, static_cast<unsigned>((T + 127) / 128));
-                        });
+    if (n_acc > 0) {
+        CombineArgs c{};
+        c.list = S.flist.as<int32_t>();
+        c.count = S.fcount.as<long long>();
+        c.m = m;
+        c.nch = S.nch;
+        c.n_ext = S.n_ext;
+        c.sqrts = ctx->sqrts;
+        c.f = ctx->f_dev.as<IntegrandDesc>();
+        c.beta = S.beta.as<float>();
+        c.logbeta = S.logbeta.as<float>();
+        c.log_fscale = S.log_fscale;
+        c.logf = logf;
+        c.fval = fval;
+        c.feat = feat;
+        c.logprior = logprior;
+        if (int rc = pipeline_run(ctx, S.fmom.as<double>(), m, S.flist.as<int32_t>(), ch, S.fcount.as<long long>(),
+                                  n_acc, ctx->bins, false, nullptr, nullptr, [&](long long base, long long T) -> int {
+                                      CombineArgs t = c;
+                                      t.node_soa = ctx->node_soa.as<double>();
+                                      t.dcv = ctx->dcv.as<double>();
+                                      t.vwv = ctx->vwv.as<double>();
+                                      t.ich_tile = ctx->ich_tile.as<int32_t>();
+                                      t.base = base;
+                                      t.T = T;
+                                      return flow_launch_combine(ctx, t, static_cast<unsigned>((T + 127) / 128));
+                                  }))
+            return rc;
+    }
+    if (train) return CHILI_OK;
+    // the values: alpha_c F / (beta_c q) of every row, 0 for rows without one
+    AlphaTcArgs e{};
+    e.n = m;
+    e.L = S.AL;
+    e.tiles = S.atiles.as<uint8_t>();
+    e.w = S.prm.as<float>() + S.off_alpha;
+    e.feat = feat;
+    e.logprior = logprior;
+    e.ch = ch;
+    e.logf = logf;
+    e.logbeta = S.logbeta.as<float>();
+    e.logq = logq;
+    e.fval = fval;
+    e.v = S.fv.as<double>();
+    e.err = S.err.as<int>();
+    return flow_launch_alpha_eval(ctx, e, S.sms);
 }
 
 // The flow over n points (xin, xout [D][n] on the device): the layers in
@@ -518,7 +546,8 @@ int flow_pass(chili_ctx *ctx, const float *xin_dev, const int32_t *ch_dev, long 
 void flow_release(chili_ctx *ctx) {
     if (!ctx || !ctx->flow) return;
     FlowState &S = *ctx->flow;
-    for (DevBuf *b : {&S.prm, &S.m, &S.v, &S.grad, &S.wtiles, &S.part_f, &S.part_a, &S.loss_part, &S.loss_dev,
+    for (DevBuf *b : {&S.prm, &S.m, &S.v, &S.grad, &S.wtiles, &S.atiles, &S.slogf, &S.sfeat, &S.slogprior, &S.sfval,
+                      &S.part_f, &S.part_a, &S.loss_part, &S.loss_dev,
                       &S.beta, &S.logbeta, &S.cp, &S.X, &S.chb, &S.logf, &S.fval, &S.feat, &S.logprior, &S.logq,
                       &S.glogq, &S.g0, &S.g1, &S.thetas, &S.h1s, &S.h2s, &S.gths, &S.gp2s, &S.gp1s, &S.scal,
                       &S.hsw, &S.gpsw, &S.gthsw,
@@ -543,8 +572,8 @@ int chili_gpu_flow_init(chili_ctx *ctx, const chili_flow_params *params) {
     if (params->layers < 1 || params->layers > 32 || params->batch < 128 || params->batch > (1 << 24))
         return fail(ctx, CHILI_ERR_INVALID_ARG, "layers in [1, 32], batch in [128, 2^24]");
     const int F = n_features(ctx->n_ext);
-    if (ctx->nch > kMaxFlowCh || F > kMaxFeat)
-        return fail(ctx, CHILI_ERR_LIMIT, "learned proposal limited to 48 channels and 32 features");
+    if (ctx->nch > kMaxFlowCh || F > kMaxFeat - 1)
+        return fail(ctx, CHILI_ERR_LIMIT, "learned proposal limited to 48 channels and 31 features");
     flow_release(ctx);
     ctx->flow = new FlowState();
     FlowState &S = *ctx->flow;
@@ -637,6 +666,7 @@ int chili_gpu_flow_init(chili_ctx *ctx, const chili_flow_params *params) {
     const size_t wbytes = static_cast<size_t>(S.L) * (S.streamed ? wide_layer_bytes(S.H, S.NH) : kWLayerBytes);
     CK(S.wtiles.ensure(wbytes));
     CK(cudaMemsetAsync(S.wtiles.p, 0, wbytes, ctx->stream));
+    CK(S.atiles.ensure(kAWBytes));
     for (int l = 0; l < S.L; ++l)
         S.wlayers[l].w = S.wtiles.as<uint8_t>() + static_cast<size_t>(l) * wide_layer_bytes(S.H, S.NH);
     CK(S.part_f.ensure(sizeof(float) * kNsplit * S.np_flow));

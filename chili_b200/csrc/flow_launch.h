@@ -12,9 +12,14 @@
 // per SM at most.
 int flow_launch_layer(chili_ctx *ctx, int mode, bool save, const chili_flow::LayerArgs &a, int sms);
 int flow_launch_bwd(chili_ctx *ctx, const chili_flow::BwdArgs &a, int sms);
-int flow_launch_alpha(chili_ctx *ctx, const chili_flow::AlphaTrainArgs &a);
-// The last step of a flow-path tile (training rows or sampled values).
-int flow_launch_combine(chili_ctx *ctx, bool train, const chili_flow::CombineArgs &a, unsigned blocks);
+// The channel-weight network on the tensor cores (flow_alpha_tc.cuh):
+// training (forward, loss, backward, weight-gradient partials of kAlphaSplit
+// CTAs), sampling (the values of the rows), and the packing of its bf16 tiles.
+int flow_launch_alpha(chili_ctx *ctx, const chili_flow::AlphaTcArgs &a);
+int flow_launch_alpha_eval(chili_ctx *ctx, const chili_flow::AlphaTcArgs &a, int sms);
+int flow_launch_alpha_pack(chili_ctx *ctx, const float *w, const chili_flow::AlphaLayout &L, uint8_t *tiles);
+// The last step of a flow-path tile: the rows of the channel-weight network.
+int flow_launch_combine(chili_ctx *ctx, const chili_flow::CombineArgs &a, unsigned blocks);
 
 // The wide-conditioner kernels (flow_wide.cuh; flow_wide.cu).
 int flow_launch_layer_wide(chili_ctx *ctx, int mode, bool save, const chili_flow::WideFwdArgs &a, int sms);

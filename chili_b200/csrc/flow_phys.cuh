@@ -29,7 +29,6 @@ using namespace chili_dev;
 constexpr int kAH = 64;        // hidden units of the channel-weight network
 constexpr int kMaxFeat = 32;
 constexpr int kMaxAlphaCh = 64;
-constexpr int kAlphaBlock = 64;
 
 // Offsets of the channel-weight network's parameters in its flat f32 block.
 struct AlphaLayout {
@@ -50,6 +49,34 @@ __host__ __device__ inline AlphaLayout alpha_layout(int F, int nch) {
     L.total = L.c3 + nch;
     return L;
 }
+
+// The channel-weight network's bf16 weight tiles (flow_alpha_tc.cuh): A1
+// (hidden x feature), A2 (out x in), A3 (channel x hidden), 64 x 64 each.
+constexpr int kATile = 64 * 64 * 2;
+constexpr int kAWBytes = 3 * kATile;
+
+// Arguments of the channel-weight network's tensor-core kernel (one row per
+// point: features, log prior, channel, log F, log q).
+struct AlphaTcArgs {
+    long long n;          // rows
+    AlphaLayout L;
+    const uint8_t *tiles; // kAWBytes (k_alpha_pack)
+    const float *w;       // f32 parameters (the biases are read from here)
+    const float *feat;    // [F][n]
+    const float *logprior;// [nch][n]
+    const int32_t *ch;    // [n]
+    const float *logf;    // [n]: training log F (-inf: no value); sampling: -inf marks a row without value
+    const float *logbeta; // [nch]
+    const float *logq;    // [n]
+    // training
+    float *glogq;         // [n]
+    float *part;          // [gridDim.x][L.total]
+    double *loss_part;    // [gridDim.x]
+    // sampling
+    const double *fval;   // [n] F of the row
+    double *v;            // [n] the value alpha_c F / (beta_c q)
+    int *err;
+};
 
 __host__ __device__ inline int n_features(int n_ext) {
     const int n_out = n_ext - 2;
@@ -76,284 +103,11 @@ __device__ __forceinline__ V4 soa_v4(const double *__restrict__ soa, int s, long
               soa[(4 * s + 3) * m + i]};
 }
 
-// Channel-weight network forward for one point: the logits of every channel
-// and their log-sum-exp.
-template <int NCH, int NF>
-__device__ __forceinline__ void alpha_forward(const float *__restrict__ w, const AlphaLayout &L, const float (&feat)[NF],
-                                              const float *logprior, float (&a1)[kAH], float (&a2)[kAH],
-                                              float (&lg)[NCH], float &lse) {
-#pragma unroll 4
-    for (int i = 0; i < kAH; ++i) {
-        float s = w[L.c1 + i];
-#pragma unroll
-        for (int f = 0; f < NF; ++f)
-            if (f < L.F) s += w[L.a1 + i * L.F + f] * feat[f];
-        a1[i] = lrelu(s);
-    }
-#pragma unroll 4
-    for (int j = 0; j < kAH; ++j) {
-        float s = w[L.c2 + j];
-#pragma unroll
-        for (int i = 0; i < kAH; ++i) s += w[L.a2 + j * kAH + i] * a1[i];
-        a2[j] = lrelu(s);
-    }
-    float mx = -INFINITY;
-#pragma unroll
-    for (int k = 0; k < NCH; ++k) {
-        float s = -INFINITY;
-        if (k < L.nch) {
-            s = w[L.c3 + k] + logprior[k];
-#pragma unroll
-            for (int j = 0; j < kAH; ++j) s += w[L.a3 + k * kAH + j] * a2[j];
-        }
-        lg[k] = s;
-        mx = fmaxf(mx, s);
-    }
-    float se = 0.f;
-#pragma unroll
-    for (int k = 0; k < NCH; ++k)
-        if (k < L.nch) se += expf(lg[k] - mx);
-    lse = mx + logf(se);
-}
-
-// Channel-weight network: forward, variance-loss terms, backward, weight
-// gradients (this block's partial), for one training batch. Also writes
-// d loss / d log q for the flow's backward pass.
-//   l_i = alpha_c^2 F^2 / (beta_c^2 q)  (F = f dens J / F_scale), loss = mean l_i
-struct AlphaTrainArgs {
-    long long n;
-    AlphaLayout L;
-    const float *w;         // parameters (flat)
-    const float *feat;      // [F][n]
-    const float *logprior;  // [nch][n]
-    const int32_t *ch;
-    const float *logf;      // [n], -inf for a zero / invalid point
-    const float *logbeta;   // [nch]
-    const float *logq;      // [n]
-    float *glogq;           // [n]
-    float *part;            // [gridDim.x][L.total]
-    double *loss_part;      // [gridDim.x]
-};
-
-template <int NCH, int NF>
-__global__ void __launch_bounds__(kAlphaBlock) k_alpha_train(AlphaTrainArgs a) {
-    constexpr int R = kAlphaBlock, LD = kAH + 1, LF = NF + 1, LC = NCH + 1;
-    extern __shared__ float sa[];
-    const AlphaLayout L = a.L;
-    float *w = sa;                        // L.total
-    float *s_a1 = w + ((L.total + 3) & ~3);
-    float *s_a2 = s_a1 + R * LD;
-    float *s_g1 = s_a2 + R * LD;
-    float *s_g2 = s_g1 + R * LD;
-    float *s_gl = s_g2 + R * LD;          // [R][NCH+1]
-    float *s_f = s_gl + R * LC;           // [R][NF+1]
-    const int t = threadIdx.x;
-    for (int i = t; i < L.total; i += R) w[i] = a.w[i];
-    __syncthreads();
-    float acc2[kAH], acc3[NCH], acc1[NF];
-#pragma unroll
-    for (int i = 0; i < kAH; ++i) acc2[i] = 0.f;
-#pragma unroll
-    for (int k = 0; k < NCH; ++k) acc3[k] = 0.f;
-#pragma unroll
-    for (int f = 0; f < NF; ++f) acc1[f] = 0.f;
-    float gc1 = 0.f, gc2 = 0.f, gc3 = 0.f;
-    double lsum = 0.0;
-    const long long ntiles = (a.n + R - 1) / R;
-    const float invn = 1.f / static_cast<float>(a.n);
-    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const long long row = tile * R + t;
-        const bool valid = row < a.n;
-        float lg[NCH], lse;
-        {
-            float feat[NF], lp[NCH];
-#pragma unroll
-            for (int f = 0; f < NF; ++f) feat[f] = (valid && f < L.F) ? a.feat[f * a.n + row] : 0.f;
-#pragma unroll
-            for (int k = 0; k < NCH; ++k) lp[k] = (valid && k < L.nch) ? a.logprior[k * a.n + row] : 0.f;
-            float a1[kAH], a2[kAH];
-            alpha_forward<NCH, NF>(w, L, feat, lp, a1, a2, lg, lse);
-#pragma unroll
-            for (int i = 0; i < kAH; ++i) {
-                s_a1[t * LD + i] = a1[i];
-                s_a2[t * LD + i] = a2[i];
-            }
-#pragma unroll
-            for (int f = 0; f < NF; ++f) s_f[t * LF + f] = feat[f];
-        }
-        int c = valid ? a.ch[row] : 0;
-        c = (c >= 0 && c < L.nch) ? c : 0;
-        float lac = lg[0];
-#pragma unroll
-        for (int k = 1; k < NCH; ++k)
-            if (k == c) lac = lg[k];
-        lac -= lse;
-        float ell = 0.f;
-        if (valid) {
-            const float e = 2.f * lac + 2.f * a.logf[row] - 2.f * a.logbeta[c] - a.logq[row];
-            ell = isfinite(e) ? expf(e) : 0.f;
-            if (!isfinite(ell)) ell = 0.f;
-            a.glogq[row] = -ell * invn;
-        }
-        lsum += ell;
-        const float gsel = 2.f * ell * invn;
-        // g_logits = gsel (delta_kc - alpha_k)
-#pragma unroll
-        for (int k = 0; k < NCH; ++k) {
-            const float al = k < L.nch ? expf(lg[k] - lse) : 0.f;
-            lg[k] = gsel * ((k == c ? 1.f : 0.f) - al);
-            s_gl[t * LC + k] = lg[k];
-        }
-#pragma unroll 4
-        for (int j = 0; j < kAH; ++j) {
-            float sg = 0.f;
-#pragma unroll
-            for (int k = 0; k < NCH; ++k)
-                if (k < L.nch) sg += w[L.a3 + k * kAH + j] * lg[k];
-            s_g2[t * LD + j] = sg * (s_a2[t * LD + j] > 0.f ? 1.f : kSlope);
-        }
-#pragma unroll 4
-        for (int i = 0; i < kAH; ++i) {
-            float sg = 0.f;
-#pragma unroll 8
-            for (int j = 0; j < kAH; ++j) sg += w[L.a2 + j * kAH + i] * s_g2[t * LD + j];
-            s_g1[t * LD + i] = sg * (s_a1[t * LD + i] > 0.f ? 1.f : kSlope);
-        }
-        __syncthreads();
-        // thread t owns row t of dA2, column t of dA3, row t of dA1
-        for (int r = 0; r < R; ++r) {
-            const float gr2 = s_g2[r * LD + t], gr1 = s_g1[r * LD + t], ar2 = s_a2[r * LD + t];
-#pragma unroll
-            for (int i = 0; i < kAH; ++i) acc2[i] += gr2 * s_a1[r * LD + i];
-#pragma unroll
-            for (int k = 0; k < NCH; ++k) acc3[k] += s_gl[r * LC + k] * ar2;
-#pragma unroll
-            for (int f = 0; f < NF; ++f) acc1[f] += gr1 * s_f[r * LF + f];
-            gc1 += gr1;
-            gc2 += gr2;
-            if (t < NCH) gc3 += s_gl[r * LC + t];
-        }
-        __syncthreads();
-    }
-    float *out = a.part + static_cast<long long>(blockIdx.x) * L.total;
-#pragma unroll
-    for (int i = 0; i < kAH; ++i) out[L.a2 + t * kAH + i] = acc2[i];
-#pragma unroll
-    for (int k = 0; k < NCH; ++k)
-        if (k < L.nch) out[L.a3 + k * kAH + t] = acc3[k];
-#pragma unroll
-    for (int f = 0; f < NF; ++f)
-        if (f < L.F) out[L.a1 + t * L.F + f] = acc1[f];
-    out[L.c1 + t] = gc1;
-    out[L.c2 + t] = gc2;
-    if (t < L.nch) out[L.c3 + t] = gc3;
-    // loss partial
-    __shared__ double red[kAlphaBlock];
-    red[t] = lsum;
-    __syncthreads();
-    if (t == 0) {
-        double sl = 0;
-        for (int i = 0; i < R; ++i) sl += red[i];
-        a.loss_part[blockIdx.x] = sl;
-    }
-}
-
-template <int NCH, int NF>
-constexpr size_t alpha_train_smem(int total) {
-    return sizeof(float) * (((total + 3) & ~3) + 4 * kAlphaBlock * (kAH + 1) + kAlphaBlock * (NCH + 1) +
-                            kAlphaBlock * (NF + 1));
-}
-
 // Flow-path points, step 2, after the phased weight pass of a tile: every
 // channel's density D_k = dens_k vw_k, w0 = 1 / sum_k beta_k / D_k, the
-// integrand. Training: log F (F = f D_c / F_scale), features and log prior
-// of the batch row. Sampling: the channel-weight network and
-// v = alpha_c f D_c / (beta_c q_c) at the point's index (NaN when not finite).
-// The channel-weight network as the sampling pass keeps it in shared memory:
-// every block 16-byte aligned and W1's rows padded to NF columns, so that the
-// products read four weights per shared load.
-template <int NCH, int NF>
-struct AlphaSmem {
-    static constexpr int kC1 = 0, kA1 = kAH, kC2 = kA1 + kAH * NF, kA2 = kC2 + kAH, kC3 = kA2 + kAH * kAH,
-                         kA3 = kC3 + NCH, kTotal = kA3 + NCH * kAH;
-};
-
-template <int NCH, int NF>
-__device__ __forceinline__ void alpha_to_smem(const float *__restrict__ w, const AlphaLayout &L, float *s) {
-    using S = AlphaSmem<NCH, NF>;
-    for (int q = threadIdx.x; q < S::kTotal; q += blockDim.x) {
-        float v = 0.f;
-        if (q < S::kA1) v = w[L.c1 + q];
-        else if (q < S::kC2) {
-            const int i = (q - S::kA1) / NF, f = (q - S::kA1) % NF;
-            v = f < L.F ? w[L.a1 + i * L.F + f] : 0.f;
-        } else if (q < S::kA2) v = w[L.c2 + q - S::kC2];
-        else if (q < S::kC3) v = w[L.a2 + q - S::kA2];
-        else if (q < S::kA3) v = (q - S::kC3) < L.nch ? w[L.c3 + q - S::kC3] : 0.f;
-        else {
-            const int k = (q - S::kA3) / kAH, j = (q - S::kA3) % kAH;
-            v = k < L.nch ? w[L.a3 + k * kAH + j] : 0.f;
-        }
-        s[q] = v;
-    }
-}
-
-// alpha_forward on the shared-memory copy (float4 weight reads).
-template <int NCH, int NF>
-__device__ __forceinline__ void alpha_forward_smem(const float *__restrict__ s, int nch, const float (&feat)[NF],
-                                                   const float *logprior, float (&lg)[NCH], float &lse) {
-    using S = AlphaSmem<NCH, NF>;
-    float a1[kAH];
-#pragma unroll
-    for (int i = 0; i < kAH; ++i) {
-        float acc = s[S::kC1 + i];
-        const float4 *wr = reinterpret_cast<const float4 *>(s + S::kA1 + i * NF);
-#pragma unroll
-        for (int q = 0; q < NF / 4; ++q) {
-            const float4 w4 = wr[q];
-            acc += w4.x * feat[4 * q] + w4.y * feat[4 * q + 1] + w4.z * feat[4 * q + 2] + w4.w * feat[4 * q + 3];
-        }
-        a1[i] = lrelu(acc);
-    }
-#pragma unroll
-    for (int k = 0; k < NCH; ++k) lg[k] = k < nch ? s[S::kC3 + k] + logprior[k] : -INFINITY;
-    // the second hidden layer four units at a time, each group added into
-    // the logits at once (the same order of additions as a whole second
-    // layer followed by the last one, without holding all of it; a rolled
-    // loop, so that the registers hold the first layer and one group)
-#pragma unroll 1
-    for (int q = 0; q < kAH / 4; ++q) {
-        float h[4];
-#pragma unroll
-        for (int jj = 0; jj < 4; ++jj) {
-            const int j = 4 * q + jj;
-            float acc = s[S::kC2 + j];
-            const float4 *wr = reinterpret_cast<const float4 *>(s + S::kA2 + j * kAH);
-#pragma unroll
-            for (int r = 0; r < kAH / 4; ++r) {
-                const float4 w4 = wr[r];
-                acc += w4.x * a1[4 * r] + w4.y * a1[4 * r + 1] + w4.z * a1[4 * r + 2] + w4.w * a1[4 * r + 3];
-            }
-            h[jj] = lrelu(acc);
-        }
-#pragma unroll
-        for (int k = 0; k < NCH; ++k) {
-            if (k < nch) {
-                const float4 w4 = reinterpret_cast<const float4 *>(s + S::kA3 + k * kAH)[q];
-                lg[k] += w4.x * h[0] + w4.y * h[1] + w4.z * h[2] + w4.w * h[3];
-            }
-        }
-    }
-    float mx = -INFINITY;
-#pragma unroll
-    for (int k = 0; k < NCH; ++k) mx = fmaxf(mx, lg[k]);
-    float se = 0.f;
-#pragma unroll
-    for (int k = 0; k < NCH; ++k)
-        if (k < nch) se += expf(lg[k] - mx);
-    lse = mx + logf(se);
-}
-
+// integrand; the point's row for the channel-weight network (flow_alpha_tc.cuh):
+// log F (F = f D_c / F_scale, and F itself when fval is given), features and
+// log prior. Rows of points without a value keep log F = -inf.
 // log(x) of a positive double to float precision: exponent exactly, the
 // mantissa's log in f32 (the log priors are f32 values).
 __device__ __forceinline__ float log_d2f(double x) {
@@ -373,26 +127,15 @@ struct CombineArgs {
     double sqrts;
     const IntegrandDesc *f;
     const float *beta, *logbeta;
-    // training
     double log_fscale;
     float *logf;       // [m]
     double *fval;      // [m] or null
     float *feat;       // [F][m]
     float *logprior;   // [nch][m]
-    // sampling
-    const float *logq; // [m]
-    const float *w;    // network parameters
-    AlphaLayout L;
-    double *v;         // [m]
 };
 
-template <bool TRAIN, int NCH, int NF>
-__global__ void __launch_bounds__(128, TRAIN ? 1 : 4) k_flow_combine(CombineArgs a) {
-    extern __shared__ __align__(16) float cw[];  // the network (sampling), AlphaSmem layout
-    if (!TRAIN) {
-        alpha_to_smem<NCH, NF>(a.w, a.L, cw);
-        __syncthreads();
-    }
+template <int NCH>
+__global__ void __launch_bounds__(128) k_flow_combine(CombineArgs a) {
     const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
     const long long r = a.base + i;
     if (i >= a.T || r >= *a.count) return;
@@ -416,45 +159,20 @@ __global__ void __launch_bounds__(128, TRAIN ? 1 : 4) k_flow_combine(CombineArgs
     const double fv = eval_momenta(a.f, mom, a.n_ext);
     const double F = fv * Dc;
     ok = ok && isfinite(Dc) && (w0 > 0) && isfinite(w0) && (F > 0) && isfinite(F);
+    if (!ok) return;  // the row keeps logf = -inf
     float lp[NCH > 0 ? NCH : 1];
-    if (ok) {
-        const float lw0 = log_d2f(w0);
-        for (int j = 0; j < a.nch; ++j) {
-            const double Dj = a.dcv[static_cast<long long>(j) * a.T + i] * a.vwv[static_cast<long long>(j) * a.T + i];
-            lp[j] = isinf(Dj) ? -INFINITY : a.logbeta[j] - log_d2f(Dj) + lw0;
-        }
+    const float lw0 = log_d2f(w0);
+    for (int j = 0; j < a.nch; ++j) {
+        const double Dj = a.dcv[static_cast<long long>(j) * a.T + i] * a.vwv[static_cast<long long>(j) * a.T + i];
+        lp[j] = isinf(Dj) ? -INFINITY : a.logbeta[j] - log_d2f(Dj) + lw0;
     }
     float featv[kMaxFeat];
-    if (ok) point_features(mom, a.n_ext, a.sqrts, featv);
-    if (TRAIN) {
-        if (!ok) return;  // the row keeps logf = -inf
-        if (a.fval) a.fval[k] = F;
-        a.logf[k] = static_cast<float>(log(F) - a.log_fscale);
-        const int nf = n_features(a.n_ext);
-        for (int q = 0; q < nf; ++q) a.feat[q * a.m + k] = featv[q];
-        for (int j = 0; j < a.nch; ++j) a.logprior[j * a.m + k] = lp[j];
-    } else {
-        double v = 0;
-        if (ok) {
-            // the network's padded input columns must read 0, not whatever
-            // the local memory beyond this point's nf features holds (0 x
-            // inf would be NaN)
-            const int nf = n_features(a.n_ext);
-            float feat[NF];
-#pragma unroll
-            for (int q = 0; q < NF; ++q) feat[q] = (q < nf && q < kMaxFeat) ? featv[q] : 0.f;
-            float lg[NCH], lse;
-            alpha_forward_smem<NCH, NF>(cw, a.L.nch, feat, lp, lg, lse);
-            float lac = lg[0];
-#pragma unroll
-            for (int q = 1; q < NCH; ++q)
-                if (q == c) lac = lg[q];
-            lac -= lse;
-            v = exp(static_cast<double>(lac - a.logbeta[c] - a.logq[k])) * F;
-            if (!isfinite(v)) v = CUDART_NAN;
-        }
-        a.v[k] = v;
-    }
+    point_features(mom, a.n_ext, a.sqrts, featv);
+    if (a.fval) a.fval[k] = F;
+    a.logf[k] = static_cast<float>(log(F) - a.log_fscale);
+    const int nf = n_features(a.n_ext);
+    for (int q = 0; q < nf; ++q) a.feat[q * a.m + k] = featv[q];
+    for (int j = 0; j < a.nch; ++j) a.logprior[j * a.m + k] = lp[j];
 }
 
 #ifndef CHILI_FLOW_LAYERS_ONLY

@@ -664,8 +664,10 @@ __global__ void k_iter_init(long long *__restrict__ iter, long long needed) {
 }
 
 // Ordered-prefix accumulation of the records [0, ctl->n_acc): StatsData
-// partials, histogram adds, alpha-training terms val^2 w / dens_j
-// (MultiChannel.hh:167-180).  Dynamic shared memory: (kWgtBlock/32) * nch.
+// partials, histogram adds (hist non-null; else k_mc_hist does them; the
+// out-of-range slots are counted here either way), alpha-training terms
+// val^2 w / dens_j (MultiChannel.hh:167-180).  Dynamic shared memory:
+// (kWgtBlock/32) * nch.
 __global__ void __launch_bounds__(kWgtBlock) k_mc_accum(
     const RoundCtl *__restrict__ ctl, long long n_rec, int nch, int dims, int hist_size,
     const double *__restrict__ rec_val,
@@ -685,8 +687,11 @@ __global__ void __launch_bounds__(kWgtBlock) k_mc_accum(
     if (active && should_opt) {
         for (int j = 0; j < dims; ++j) {
             const int s = rec_slot[j * n_rec + i];
-            if (s >= 0 && s < hist_size) atomicAdd(hist + s, val2);
-            else dropped += 1;
+            if (s >= 0 && s < hist_size) {
+                if (hist) atomicAdd(hist + s, val2);
+            } else {
+                dropped += 1;
+            }
         }
     }
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -735,6 +740,37 @@ __global__ void __launch_bounds__(kWgtBlock) k_mc_accum(
             for (int v = 0; v < kWgtBlock / 32; ++v) s += atr_s[v * nch + j];
             P[kPartFixed + j] = s;
         }
+    }
+}
+
+// The histogram adds of the records [0, ctl->n_acc) (val^2 into the bin of
+// each dimension of the record's channel, MultiChannel.hh:167-180), staged
+// in shared memory: every block sums its records' adds into a private copy
+// of the whole histogram (hist_size doubles of dynamic shared memory) with
+// shared-memory atomics, then adds its nonzero bins to the global histogram
+// -- one global atomic per (block, bin) instead of one per (record, dim).
+// The bins' sums agree with k_mc_accum's direct adds up to the order of
+// addition.
+__global__ void __launch_bounds__(1024) k_mc_hist(const RoundCtl *__restrict__ ctl, long long n_rec, int dims,
+                                                  int hist_size, const double *__restrict__ rec_val,
+                                                  const int32_t *__restrict__ rec_slot, double *__restrict__ hist) {
+    extern __shared__ double sh[];
+    for (int k = threadIdx.x; k < hist_size; k += blockDim.x) sh[k] = 0.0;
+    __syncthreads();
+    const long long n = ctl->n_acc < n_rec ? ctl->n_acc : n_rec;
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n; i += stride) {
+        const double v = rec_val[i];
+        const double v2 = v * v;
+        for (int j = 0; j < dims; ++j) {
+            const int s = rec_slot[j * n_rec + i];
+            if (s >= 0 && s < hist_size) atomicAdd(sh + s, v2);
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < hist_size; k += blockDim.x) {
+        const double v = sh[k];
+        if (v != 0.0) atomicAdd(hist + k, v);
     }
 }
 

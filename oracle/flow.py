@@ -350,28 +350,33 @@ def flow_backward(spec, p, cache, ch, g_logq, use_bf16=False):
 
 
 # ------------------------------------------------- the channel-weight network
-def alpha_forward(spec, p, feat, logprior):
-    """log alpha [N, nch] = log softmax(MLP(features) + log prior)."""
-    a1 = lrelu(feat @ p["A1"].T + p["c1"])
-    a2 = lrelu(a1 @ p["A2"].T + p["c2"])
-    logits = a2 @ p["A3"].T + p["c3"] + logprior
+def alpha_forward(spec, p, feat, logprior, use_bf16=False):
+    """log alpha [N, nch] = log softmax(MLP(features) + log prior). With
+    use_bf16 the three products take bf16 operands (the GPU runs them on the
+    tensor cores); biases, log prior and the softmax stay unrounded."""
+    a1 = lrelu(_mm(feat, p["A1"].T, use_bf16) + p["c1"])
+    a2 = lrelu(_mm(a1, p["A2"].T, use_bf16) + p["c2"])
+    logits = _mm(a2, p["A3"].T, use_bf16) + p["c3"] + logprior
     m = logits.max(axis=1, keepdims=True)
     lse = m[:, 0] + np.log(np.exp(logits - m).sum(axis=1))
     return logits - lse[:, None], (feat, a1, a2)
 
 
-def alpha_backward(spec, p, cache, logalpha, g_logalpha_sel, ch):
-    """Gradients of sum_i g[i] * log alpha_{c_i}(p_i)."""
+def alpha_backward(spec, p, cache, logalpha, g_logalpha_sel, ch, use_bf16=False):
+    """Gradients of sum_i g[i] * log alpha_{c_i}(p_i). With use_bf16 every
+    product's operands are rounded to bf16, the bias gradients included (the
+    GPU sums the bf16 gradient rows against a constant-1 operand column)."""
     feat, a1, a2 = cache
     n = feat.shape[0]
+    q = bf16 if use_bf16 else (lambda v: v)
     al = np.exp(logalpha)
     g_logits = -al * g_logalpha_sel[:, None]
     g_logits[np.arange(n), ch] += g_logalpha_sel
-    g = {"A3": g_logits.T @ a2, "c3": g_logits.sum(0)}
-    g2 = (g_logits @ p["A3"]) * dlrelu(a2)
-    g["A2"], g["c2"] = g2.T @ a1, g2.sum(0)
-    g1 = (g2 @ p["A2"]) * dlrelu(a1)
-    g["A1"], g["c1"] = g1.T @ feat, g1.sum(0)
+    g = {"A3": _mm(g_logits.T, a2, use_bf16), "c3": q(g_logits).sum(0)}
+    g2 = _mm(g_logits, p["A3"], use_bf16) * dlrelu(a2)
+    g["A2"], g["c2"] = _mm(g2.T, a1, use_bf16), q(g2).sum(0)
+    g1 = _mm(g2, p["A2"], use_bf16) * dlrelu(a1)
+    g["A1"], g["c1"] = _mm(g1.T, feat, use_bf16), q(g1).sum(0)
     return g
 
 
@@ -393,12 +398,12 @@ def loss_and_grads(spec, p, batch, use_bf16=False):
     u, ch, logf = batch["u"], batch["ch"], batch["logf"]
     n = u.shape[0]
     _, logq, fcache = flow_forward(spec, p, u, ch, use_bf16)
-    logalpha, acache = alpha_forward(spec, p, batch["feat"], batch["logprior"])
+    logalpha, acache = alpha_forward(spec, p, batch["feat"], batch["logprior"], use_bf16)
     las = logalpha[np.arange(n), ch]
     ell = loss_terms(las, logf, batch["logbeta"][ch], logq)
     L = ell.mean()
     grads = flow_backward(spec, p, fcache, ch, -ell / n, use_bf16)
-    grads.update(alpha_backward(spec, p, acache, logalpha, 2 * ell / n, ch))
+    grads.update(alpha_backward(spec, p, acache, logalpha, 2 * ell / n, ch, use_bf16))
     return L, grads, {"logq": logq, "logalpha": logalpha, "ell": ell}
 
 
