@@ -470,10 +470,9 @@ int flow_points(chili_ctx *ctx, bool train, long long m, uint64_t seed, uint64_t
         else k_flow_gen<false><<<gb, 128, 0, ctx->stream>>>(g);
     }
     LAUNCHED();
-    long long n_acc = 0;
-    CK(cudaMemcpyAsync(&n_acc, S.fcount.p, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    if (n_acc > 0) {
+    {
+        // the listed count stays on the device: the weight pass and the rows
+        // are launched for all m points and end at the device's count
         CombineArgs c{};
         c.list = S.flist.as<int32_t>();
         c.count = S.fcount.as<long long>();
@@ -490,7 +489,7 @@ int flow_points(chili_ctx *ctx, bool train, long long m, uint64_t seed, uint64_t
         c.feat = feat;
         c.logprior = logprior;
         if (int rc = pipeline_run(ctx, S.fmom.as<double>(), m, S.flist.as<int32_t>(), ch, S.fcount.as<long long>(),
-                                  n_acc, ctx->bins, false, nullptr, nullptr, [&](long long base, long long T) -> int {
+                                  m, ctx->bins, false, nullptr, nullptr, [&](long long base, long long T) -> int {
                                       CombineArgs t = c;
                                       t.node_soa = ctx->node_soa.as<double>();
                                       t.dcv = ctx->dcv.as<double>();
