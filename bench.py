@@ -571,12 +571,19 @@ def measure_flow(ctx, args, dev, stream, plain, train_steps=None):
     ctx.flow_init(fp)
     k0 = {k: ctx.kernel_time(k) for k in FLOW_KERNELS}
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    em = torch.cuda.Event(enable_timing=True)
+    w0 = time.perf_counter()
     e0.record(stream)
     loss = ctx.flow_train(train_steps, seed=SEED + 77, counter=0)
+    em.record(stream)
+    w1 = time.perf_counter()
     ctx.flow_iterate(n, seed=SEED + 78, counter=0, adapt_beta=True)
     e1.record(stream)
     torch.cuda.synchronize(dev)
+    w2 = time.perf_counter()
     train_s = e0.elapsed_time(e1) / 1e3
+    split = {"steps_device_s": e0.elapsed_time(em) / 1e3, "beta_pass_device_s": em.elapsed_time(e1) / 1e3,
+             "steps_wall_s": w1 - w0, "beta_pass_wall_s": w2 - w1}
     k1 = {k: ctx.kernel_time(k) for k in FLOW_KERNELS}
     ctx.flow_iterate(n, seed=SEED + 79, counter=0)  # warm-up
     torch.cuda.synchronize(dev)
@@ -631,7 +638,7 @@ def measure_flow(ctx, args, dev, stream, plain, train_steps=None):
                      "hidden": f"{WL['flow_depth']} x {WL['flow_hidden']} (unit {WL['flow_hidden'] - 1} the "
                                f"constant 1; " + ("weights resident in shared memory" if WL["flow_hidden"] == 128
                                                    and WL["flow_depth"] == 2 else "weights streamed per tile") + ")",
-                     "seconds": train_s,
+                     "seconds": train_s, "split": split,
                      "loss_first": float(np.mean(loss[:10])), "loss_last": float(np.mean(loss[-10:])),
                      "kernel_ms": {k: round(k1[k][0] - k0[k][0], 3) for k in FLOW_KERNELS if k1[k][0] > k0[k][0]}},
         "kernel_ms": {k: round(k2[k][0] - k1[k][0], 3) for k in FLOW_KERNELS if k2[k][0] > k1[k][0]},

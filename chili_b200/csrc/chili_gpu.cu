@@ -487,6 +487,10 @@ int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value) {
         ctx->batch_phased = value != 0;
         return CHILI_OK;
     }
+    if (std::strcmp(name, "pipeline_sync") == 0) {
+        ctx->pipe_sync = value != 0;
+        return CHILI_OK;
+    }
     if (std::strcmp(name, "hist_shared") == 0) {
         ctx->hist_shared = value != 0;
         return CHILI_OK;
@@ -1212,11 +1216,12 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
             }
             if (pipe) {
                 // the launches are sized by the accepted count, read back here;
-                // a queued host-uniform round does not wait for it: its
-                // launches cover all mm points and the threads past the
-                // device-side count return at once
+                // a queued host-uniform round (or any round with the option
+                // "pipeline_sync" 0) does not wait for it: its launches cover
+                // all mm points and the threads past the device-side count
+                // return at once
                 long long n_pre = mm;
-                if (!u_host || mm > ctx->pipe_tile) {
+                if ((!u_host && ctx->pipe_sync) || mm > ctx->pipe_tile) {
                     CK(cudaMemcpyAsync(ctx->ctl_host, ctl_pre, sizeof(RoundCtl), cudaMemcpyDeviceToHost,
                                        ctx->stream));
                     CK(cudaStreamSynchronize(ctx->stream));

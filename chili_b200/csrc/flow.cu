@@ -894,8 +894,9 @@ int chili_gpu_flow_iterate(chili_ctx *ctx, uint64_t ncalls, uint64_t seed, uint6
         k_flow_stats<<<nbk, kPhysBlock, 0, ctx->stream>>>(S.fv.as<double>(), S.sch.as<int32_t>(), S.beta.as<float>(),
                                                           S.nch, m, S.spart.as<double>());
         LAUNCHED();
-        k_flow_fold<<<1, 256, 0, ctx->stream>>>(S.spart.as<double>(), static_cast<int>(nbk), width,
-                                                S.sfold.as<double>());
+        k_flow_fold<<<static_cast<unsigned>(width), 256, 0, ctx->stream>>>(S.spart.as<double>(),
+                                                                            static_cast<int>(nbk), width,
+                                                                            S.sfold.as<double>());
         LAUNCHED();
         CK(cudaMemcpyAsync(fold.data(), S.sfold.p, sizeof(double) * width, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));

@@ -302,6 +302,7 @@ __device__ __forceinline__ void theta_window(uint32_t lane_addr, int j, float (&
 
 template <int DB, int MODE, bool SAVE>
 __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
+    static_assert(DB >= 1 && DB <= kFwdGroups, "one spline dimension per thread group");
     extern __shared__ uint8_t smem_raw[];
     uint8_t *sm = align1024(smem_raw);
     uint8_t *sW1 = sm, *sW2 = sm + kW1Bytes, *sW3 = sm + kW1Bytes + kW2Bytes;  // sW3: kPF padded rows
@@ -347,6 +348,11 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
     for (long long tile = blockIdx.x; __syncthreads_and(ok) && tile < ntiles; tile += gridDim.x) {
         const long long row = tile * 128 + r;
         const bool valid = row < n;
+        // this thread's spline input and (group 0) the point's log q, loaded
+        // now so that their latency hides behind the three products
+        const int dsp = grp < DB ? a.L.trans[grp] : 0;
+        const float xsp = (valid && grp < DB) ? a.xin[dsp * n + row] : 0.5f;
+        const float lq0 = (valid && grp == 0) ? a.logq[row] : 0.f;
         if (grp < 2) {
             // A tile row, bf16: group 0 the conditioning coordinates (columns
             // 0..15) and one-hot columns 16..31, group 1 one-hot columns 32..63
@@ -439,11 +445,11 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
         ok = mbar_wait(bar + 1, phase, kWaitLimit) && ok;
         phase ^= 1;
         tc_fence_after();
-        // splines: dimension j on group j; one copy of the spline code, the
-        // dimension a runtime value
+        // splines: dimension j = grp on group grp (DB <= kFwdGroups); one
+        // copy of the spline code, the dimension a runtime value
         float lsum = 0.f;
-#pragma unroll 1
-        for (int j = grp; j < DB; j += kFwdGroups) {
+        if (grp < DB) {
+            const int j = grp;
             float th[64];
             theta_window(lane_addr, j, th);  // th[0 .. 48]: this dimension's parameters
             const int b0 = j * kPerDim;
@@ -451,17 +457,16 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
 #pragma unroll
                 for (int i = 0; i < kPerDim; ++i) a.theta[(b0 + i) * n + row] = th[i];
             }
-            const int d = a.L.trans[j];
-            const float x = valid ? fminf(fmaxf(a.xin[d * n + row], 0.f), 1.f) : 0.5f;
+            const float x = fminf(fmaxf(xsp, 0.f), 1.f);
             float lj;
             const float y = MODE == 0 ? rqs_forward(th, x, lj) : rqs_inverse(th, x, lj);
-            if (valid) a.xout[d * n + row] = y;
+            if (valid) a.xout[dsp * n + row] = y;
             lsum += lj;
         }
         if (grp > 0) sL[(grp - 1) * 128 + r] = lsum;
         tc_fence_before();
         __syncthreads();
-        if (grp == 0 && valid) a.logq[row] += lsum + sL[r] + sL[128 + r] + sL[256 + r] + sL[384 + r];
+        if (grp == 0 && valid) a.logq[row] = lq0 + (lsum + sL[r] + sL[128 + r] + sL[256 + r] + sL[384 + r]);
     }
     if (!ok && t == 0) atomicExch(a.err, 1);
     // every issued MMA has been waited for (or the wait gave up): release TMEM

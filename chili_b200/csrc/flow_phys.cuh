@@ -301,16 +301,27 @@ __global__ void __launch_bounds__(kPhysBlock) k_flow_stats(const double *__restr
 
 
 // Ordered fold of the block partials: out[0..5] = n, sum, sum2, max,
-// nonzero, nonfinite; out[6..] = per channel n_c, sum T_c^2.
-__global__ void k_flow_fold(const double *__restrict__ part, int nblocks, int width, double *__restrict__ out) {
-    const int q = threadIdx.x + blockIdx.x * blockDim.x;
-    if (q >= width) return;
+// nonzero, nonfinite; out[6..] = per channel n_c, sum T_c^2. One CTA per
+// field (gridDim.x = width): thread t folds partials t, t + 256, ... in
+// order, then a fixed tree over the threads (deterministic).
+__global__ void __launch_bounds__(256) k_flow_fold(const double *__restrict__ part, int nblocks, int width,
+                                                   double *__restrict__ out) {
+    const int q = blockIdx.x;
+    const bool mx = q == 3;
     double s = 0;
-    for (int b = 0; b < nblocks; ++b) {
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
         const double v = part[static_cast<long long>(b) * width + q];
-        s = q == 3 ? fmax(s, v) : s + v;
+        s = mx ? fmax(s, v) : s + v;
     }
-    out[q] = s;
+    __shared__ double red[256];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (threadIdx.x < h) red[threadIdx.x] = mx ? fmax(red[threadIdx.x], red[threadIdx.x + h])
+                                                   : red[threadIdx.x] + red[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[q] = red[0];
 }
 
 // Ordered sum of the loss partials.

@@ -326,6 +326,11 @@ __global__ void __launch_bounds__(kWFwdThreads, 1) k_flow_layer_wide(WideFwdArgs
             }
             const long long row = tile * 128 + r;
             const bool valid = row < n;
+            // this thread's spline input and (group 0) the point's log q,
+            // loaded now so that their latency hides behind the products
+            const int dsp = grp < DB ? a.L.trans[grp] : 0;
+            const float xsp = (valid && grp < DB) ? a.xin[dsp * n + row] : 0.5f;
+            const float lq0 = (valid && grp == 0) ? a.logq[row] : 0.f;
             if (grp < 2) {
                 int c = valid ? a.ch[row] : 0;
                 c = (c >= 0 && c < a.L.nch) ? c : 0;  // channel indices come from callers
@@ -427,8 +432,8 @@ __global__ void __launch_bounds__(kWFwdThreads, 1) k_flow_layer_wide(WideFwdArgs
             acc_phase ^= 1;
             tc_fence_after();
             float lsum = 0.f;
-#pragma unroll 1
-            for (int j = grp; j < DB; j += 5) {
+            if (grp < DB) {  // dimension grp on group grp (DB <= 5)
+                const int j = grp;
                 float th[64];
                 tmem_ld64(lane_addr + static_cast<uint32_t>(64 * j), th);
                 const int b0 = j * kPerDim;
@@ -436,17 +441,16 @@ __global__ void __launch_bounds__(kWFwdThreads, 1) k_flow_layer_wide(WideFwdArgs
 #pragma unroll
                     for (int i = 0; i < kPerDim; ++i) a.theta[(b0 + i) * n + row] = th[i];
                 }
-                const int d = a.L.trans[j];
-                const float x = valid ? fminf(fmaxf(a.xin[d * n + row], 0.f), 1.f) : 0.5f;
+                const float x = fminf(fmaxf(xsp, 0.f), 1.f);
                 float lj;
                 const float y = MODE == 0 ? rqs_forward(th, x, lj) : rqs_inverse(th, x, lj);
-                if (valid) a.xout[d * n + row] = y;
+                if (valid) a.xout[dsp * n + row] = y;
                 lsum += lj;
             }
             if (grp > 0) sL[(grp - 1) * 128 + r] = lsum;
             tc_fence_before();
             cbar_sync(kWFwdCompute);
-            if (grp == 0 && valid) a.logq[row] += lsum + sL[r] + sL[128 + r] + sL[256 + r] + sL[384 + r];
+            if (grp == 0 && valid) a.logq[row] = lq0 + (lsum + sL[r] + sL[128 + r] + sL[256 + r] + sL[384 + r]);
         }
         if (!ok && t == 0) {
             *abort_flag = 1;
