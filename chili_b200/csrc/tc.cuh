@@ -95,6 +95,14 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
                  : "memory");
 }
 
+// 4-byte asynchronous copy global -> shared (both 4-byte aligned), grouped by
+// cp_async_commit and awaited by the issuing thread with cp_async_wait_all.
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // --------------------------------------------------------------------- TMEM
 // Whole warp: allocates `ncols` columns and writes the base address to *dst.
 __device__ __forceinline__ void tmem_alloc(uint32_t *dst, uint32_t ncols) {
