@@ -214,6 +214,63 @@ __device__ __forceinline__ float rqs_backward(const float *th, float x, float gy
     return g_xi / b.wk;
 }
 
+// rqs_backward with the 49 parameter gradients written straight into row r
+// of a bf16 SW128 tile (columns c0 .. c0 + 48) instead of an array: the same
+// value for every gradient, fewer live registers. Returns d/dx.
+__device__ __forceinline__ float rqs_backward_st(const float *th, float x, float gy, float gj, uint8_t *tile, int r,
+                                                 int c0) {
+    float smw[kBins], w[kBins], smh[kBins], h[kBins];
+    bin_sizes(th, kMinW, smw, w);
+    bin_sizes(th + kBins, kMinH, smh, h);
+    const SplineBin b = locate(th, w, h, x, false);
+    const float xi = (x - b.x0) / b.wk;
+    const float s = b.hk / b.wk;
+    const float om = xi * (1.f - xi);
+    const float dl = b.d0 + b.d1 - 2.f * s;
+    const float A = s * xi * xi + b.d0 * om;
+    const float B = s + dl * om;
+    const float C = b.d1 * xi * xi + 2.f * s * om + b.d0 * (1.f - xi) * (1.f - xi);
+    const float A_xi = 2.f * s * xi + b.d0 * (1.f - 2.f * xi), A_s = xi * xi, A_d0 = om;
+    const float B_xi = dl * (1.f - 2.f * xi), B_s = 1.f - 2.f * om, B_d = om;
+    const float C_xi = 2.f * b.d1 * xi + 2.f * s * (1.f - 2.f * xi) - 2.f * b.d0 * (1.f - xi);
+    const float C_s = 2.f * om, C_d0 = (1.f - xi) * (1.f - xi), C_d1 = xi * xi;
+    const float hB2 = b.hk / (B * B);
+    const float iB = 1.f / B, iC = 1.f / C;
+    const float g_xi = gy * hB2 * (A_xi * B - A * B_xi) + gj * (C_xi * iC - 2.f * B_xi * iB);
+    const float g_s = gy * hB2 * (A_s * B - A * B_s) + gj * (2.f / s + C_s * iC - 2.f * B_s * iB);
+    const float g_d0 = gy * hB2 * (A_d0 * B - A * B_d) + gj * (C_d0 * iC - 2.f * B_d * iB);
+    const float g_d1 = gy * hB2 * (-A * B_d) + gj * (C_d1 * iC - 2.f * B_d * iB);
+    const float g_hk = gy * A * iB + g_s / b.wk;
+    const float g_x0 = -g_xi / b.wk;
+    const float g_wk = -(g_xi * xi + g_s * s) / b.wk;
+    const float g_y0 = gy;
+    const float scw = 1.f - kBins * kMinW, sch = 1.f - kBins * kMinH;
+    float dotw = 0.f, doth = 0.f;
+#pragma unroll
+    for (int m = 0; m < kBins; ++m) {
+        const float gw = (m < b.k ? g_x0 : 0.f) + (m == b.k ? g_wk : 0.f);
+        const float gh = (m < b.k ? g_y0 : 0.f) + (m == b.k ? g_hk : 0.f);
+        dotw += (scw * gw) * smw[m];
+        doth += (sch * gh) * smh[m];
+    }
+    auto put = [&](int col, float v) {
+        *reinterpret_cast<uint16_t *>(tile + sw128_off(r, c0 + col, 128)) =
+            static_cast<uint16_t>(pack_bf16x2(v, 0.f) & 0xFFFFu);
+    };
+#pragma unroll
+    for (int m = 0; m < kBins; ++m) {
+        const float gw = (m < b.k ? g_x0 : 0.f) + (m == b.k ? g_wk : 0.f);
+        const float gh = (m < b.k ? g_y0 : 0.f) + (m == b.k ? g_hk : 0.f);
+        put(m, smw[m] * (scw * gw - dotw));
+        put(kBins + m, smh[m] * (sch * gh - doth));
+    }
+    const float s0 = sigmoid_f(b.t0), s1 = sigmoid_f(b.t1);
+#pragma unroll
+    for (int m = 0; m <= kBins; ++m)
+        put(2 * kBins + m, (m == b.k ? g_d0 * s0 : 0.f) + (m == b.k + 1 ? g_d1 * s1 : 0.f));
+    return g_xi / b.wk;
+}
+
 // ------------------------------------------------------------- helpers
 __device__ __forceinline__ uint8_t *align1024(uint8_t *p) {
     const uint32_t a = smem_u32(p);
@@ -277,14 +334,16 @@ struct LayerArgs {
 };
 
 // Shared memory of the forward kernel: W1, W2, the padded W3, A tile, H tile,
-// and the log-det partials of the four other thread groups of a point.
+// the log-det partials of the four other thread groups of a point, and the
+// next tile's conditioning coordinates [16][128] and channels [128], copied
+// asynchronously while the current tile's splines run.
 // Five thread groups of 128 (one thread per point each; TMEM lanes are shared
 // by warps w, w+4, ..., w+16): groups 0-3 split the 128 hidden columns of the
 // epilogues, group j evaluates the spline of dimension j.
 constexpr int kFwdGroups = 5;
 constexpr int kFwdThreads = 128 * kFwdGroups;
-constexpr int kFwdSmem = kW1Bytes + kW2Bytes + kW3FBytes + 128 * 64 * 2 + kHTile + (kFwdGroups - 1) * 128 * 4 + 64 +
-                         1024;
+constexpr int kFwdSmem = kW1Bytes + kW2Bytes + kW3FBytes + 128 * 64 * 2 + kHTile + (kFwdGroups - 1) * 128 * 4 +
+                         kMaxDA * 128 * 4 + 128 * 4 + 64 + 1024;
 
 // theta of dimension j: the 64 accumulator columns 128 + 64 j .. (the first
 // 49 used), two loads in flight.
@@ -309,7 +368,9 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
     uint8_t *sA = sW3 + kW3FBytes;
     uint8_t *sH = sA + 128 * 64 * 2;
     float *sL = reinterpret_cast<float *>(sH + kHTile);  // [4][128] log-det partials of groups 1..4
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sL + (kFwdGroups - 1) * 128);
+    float *sX = sL + (kFwdGroups - 1) * 128;                // [kMaxDA][128] conditioning coordinates
+    int *sCh = reinterpret_cast<int *>(sX + kMaxDA * 128);  // [128] channels
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sCh + 128);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
     const int t = threadIdx.x, wp = t >> 5;
     const int grp = wp >> 2;                 // 0..4: the thread group of this warp
@@ -344,6 +405,21 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
     constexpr uint32_t id_p2 = idesc_bf16(128, 64, false, false);
     uint32_t phase = 0;
     const int da = a.L.da;
+    // a tile's conditioning coordinates and channels into sX / sCh (rows past
+    // n are not copied: the tile's users read them as invalid rows)
+    auto prefetch = [&](long long tl) {
+        const long long base = tl * 128;
+        for (int e = t; e < (da + 1) * 128; e += kFwdThreads) {
+            const int i = e >> 7, p = e & 127;
+            const long long rw = base + p;
+            if (rw >= n) continue;
+            if (i < da) cp_async4(sX + e, a.xin + static_cast<long long>(a.L.cond[i]) * n + rw);
+            else cp_async4(sCh + p, a.ch + rw);
+        }
+        cp_async_commit();
+    };
+    if (blockIdx.x < ntiles) prefetch(blockIdx.x);
+    cp_async_wait_all();
 
     for (long long tile = blockIdx.x; __syncthreads_and(ok) && tile < ntiles; tile += gridDim.x) {
         const long long row = tile * 128 + r;
@@ -356,14 +432,14 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
         if (grp < 2) {
             // A tile row, bf16: group 0 the conditioning coordinates (columns
             // 0..15) and one-hot columns 16..31, group 1 one-hot columns 32..63
-            int c = valid ? a.ch[row] : 0;
+            int c = valid ? sCh[r] : 0;
             c = (c >= 0 && c < a.L.nch) ? c : 0;  // channel indices come from callers: keep E reads in bounds
             float av[32];
             if (grp == 0) {
 #pragma unroll
                 for (int i = 0; i < 16; ++i) {
                     float v = 0.f;
-                    if (i < da && valid) v = 2.f * fminf(fmaxf(a.xin[a.L.cond[i] * n + row], 0.f), 1.f) - 1.f;
+                    if (i < da && valid) v = 2.f * fminf(fmaxf(sX[i * 128 + r], 0.f), 1.f) - 1.f;
                     av[i] = v;
                 }
 #pragma unroll
@@ -375,7 +451,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
             store_row32(sA, 128, r, 32 * grp, av);
         } else if (grp == 2 && valid) {
             // identity coordinates pass through
-            for (int i = 0; i < da; ++i) a.xout[a.L.cond[i] * n + row] = a.xin[a.L.cond[i] * n + row];
+            for (int i = 0; i < da; ++i) a.xout[a.L.cond[i] * n + row] = sX[i * 128 + r];
         }
         fence_async_smem();
         tc_fence_before();
@@ -447,6 +523,9 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
         tc_fence_after();
         // splines: dimension j = grp on group grp (DB <= kFwdGroups); one
         // copy of the spline code, the dimension a runtime value
+        // sX / sCh were read before the first product of this tile: the next
+        // tile's copies run beside the splines
+        if (tile + gridDim.x < ntiles) prefetch(tile + gridDim.x);
         float lsum = 0.f;
         if (grp < DB) {
             const int j = grp;
@@ -464,6 +543,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_flow_layer(LayerArgs a) {
             lsum += lj;
         }
         if (grp > 0) sL[(grp - 1) * 128 + r] = lsum;
+        cp_async_wait_all();  // the next tile's copies of this thread, before the barrier publishes them
         tc_fence_before();
         __syncthreads();
         if (grp == 0 && valid) a.logq[row] = lq0 + (lsum + sL[r] + sL[128 + r] + sL[256 + r] + sL[384 + r]);
@@ -495,21 +575,27 @@ struct BwdArgs {
     int *err;
 };
 
-constexpr int kBwdSmem = kWBytes + kGTile + kHTile + 16 * 128 * 4 + 64 + 1024;
-constexpr int kBwdThreads = 256;  // two threads per point
+// Five thread groups of 128 (one thread per point each, as in the forward
+// kernel): group j runs the spline backward of dimension j; groups 0-3 split
+// the epilogues' 128 hidden columns. The g_a partials of groups 1-3 reuse the
+// g_theta tile's memory once its product and copy are done.
+constexpr int kBwdGroups = 5;
+constexpr int kBwdThreads = 128 * kBwdGroups;
+constexpr int kBwdSmem = kWBytes + kGTile + kHTile + 64 + 1024;
 
 template <int DB>
 __global__ void __launch_bounds__(kBwdThreads, 1) k_flow_layer_bwd(BwdArgs a) {
+    static_assert(DB >= 1 && DB <= kBwdGroups, "one spline dimension per thread group");
     extern __shared__ uint8_t smem_raw[];
     uint8_t *sm = align1024(smem_raw);
     uint8_t *sW1 = sm, *sW2 = sm + kW1Bytes, *sW3 = sm + kW1Bytes + kW2Bytes;
     uint8_t *sG = sm + kWBytes;
     uint8_t *sP = sG + kGTile;
-    float *sGA = reinterpret_cast<float *>(sP + kHTile);  // [16][128] g_a partials of the second half
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sGA + 16 * 128);
+    float *sGA = reinterpret_cast<float *>(sG);  // [3][16][128] g_a partials of groups 1-3 (after g_theta's use)
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sP + kHTile);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
     const int t = threadIdx.x, wp = t >> 5;
-    const int half = wp >> 2;
+    const int grp = wp >> 2;
     const int r = (wp & 3) * 32 + (t & 31);
     const long long n = a.n;
     const long long ntiles = (n + 127) / 128;
@@ -533,30 +619,26 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_flow_layer_bwd(BwdArgs a) {
     constexpr uint32_t id_mn = idesc_bf16(128, 128, false, true);
     uint32_t phase = 0;
     const int da = a.L.da;
+    // the group that zeroes g_theta's padding columns DB*49 .. 255
+    constexpr int kPadGroup = DB < kBwdGroups ? DB : kBwdGroups - 1;
     for (long long tile = blockIdx.x; __syncthreads_and(ok) && tile < ntiles; tile += gridDim.x) {
         const long long row = tile * 128 + r;
         const bool valid = row < n;
-        const float gl = valid ? a.glogq[row] : 0.f;
-        // spline backward -> g_theta (bf16 tile, row r): dims 0, 2, 4 | 1, 3;
-        // one copy of the spline code, the dimension a runtime loop
-#pragma unroll 1
-        for (int j = half; j < DB; j += 2) {
-            const int b0 = j * kPerDim;
-            float th[kPerDim], g[kPerDim];
+        // spline backward of dimension grp -> g_theta (bf16 tile, row r)
+        if (grp < DB) {
+            const int b0 = grp * kPerDim;
+            const int d = a.L.trans[grp];
+            const long long rr = valid ? row : 0;
+            float th[kPerDim];
 #pragma unroll
-            for (int i = 0; i < kPerDim; ++i) th[i] = valid ? a.theta[(b0 + i) * n + row] : 0.f;
-            const int d = a.L.trans[j];
-            const float x = valid ? fminf(fmaxf(a.xin[d * n + row], 0.f), 1.f) : 0.5f;
+            for (int i = 0; i < kPerDim; ++i) th[i] = a.theta[(b0 + i) * n + rr];
+            const float x = fminf(fmaxf(a.xin[d * n + rr], 0.f), 1.f);
             const float gy = (valid && a.gout) ? a.gout[d * n + row] : 0.f;
-            const float gx = rqs_backward(th, x, gy, valid ? gl : 0.f, g);
+            const float gl = valid ? a.glogq[row] : 0.f;
+            const float gx = rqs_backward_st(th, x, gy, gl, sG, r, b0);
             if (valid) a.gin[d * n + row] = gx;
-#pragma unroll
-            for (int i = 0; i < kPerDim; ++i) {
-                const uint32_t pk = pack_bf16x2(valid ? g[i] : 0.f, 0.f);
-                *reinterpret_cast<uint16_t *>(sG + sw128_off(r, b0 + i, 128)) = static_cast<uint16_t>(pk & 0xFFFFu);
-            }
         }
-        if (half == 1)
+        if (grp == kPadGroup)
             for (int col = DB * kPerDim; col < kP; ++col)
                 *reinterpret_cast<uint16_t *>(sG + sw128_off(r, col, 128)) = 0;
         fence_async_smem();
@@ -573,11 +655,10 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_flow_layer_bwd(BwdArgs a) {
         ok = mbar_wait(bar + 1, phase, kWaitLimit) && ok;
         phase ^= 1;
         tc_fence_after();
-        // g_p2 = g_h2 * lrelu'(h2), unit 127 -> 0; this half's 64 columns
-        const uint8_t *h2t = a.h2s + tile * kHTile;
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int c0 = 64 * half + 32 * q;
+        // g_p2 = g_h2 * lrelu'(h2), unit 127 -> 0; groups 0-3, 32 columns each
+        if (grp < 4) {
+            const uint8_t *h2t = a.h2s + tile * kHTile;
+            const int c0 = 32 * grp;
             float v[32], hv[32];
             tmem_ld32(lane_addr + c0, v);
             load_row32(h2t, 128, r, c0, hv);
@@ -601,15 +682,15 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_flow_layer_bwd(BwdArgs a) {
         ok = mbar_wait(bar + 1, phase, kWaitLimit) && ok;
         phase ^= 1;
         tc_fence_after();
-        __syncthreads();  // the copy of g_p2 is complete before g_p1 overwrites it
-        // g_p1 = g_h1 * lrelu'(h1); g_a = bf16(g_p1) W1 on the CUDA cores, this half's units
-        const uint8_t *h1t = a.h1s + tile * kHTile;
+        __syncthreads();  // the copies of g_theta and g_p2 are complete before their tiles are reused
+        // g_p1 = g_h1 * lrelu'(h1); g_a = bf16(g_p1) W1 on the CUDA cores,
+        // this group's 32 units
         float ga[kMaxDA];
 #pragma unroll
         for (int i = 0; i < kMaxDA; ++i) ga[i] = 0.f;
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int c0 = 64 * half + 32 * q;
+        if (grp < 4) {
+            const uint8_t *h1t = a.h1s + tile * kHTile;
+            const int c0 = 32 * grp;
             float v[32], hv[32];
             tmem_ld32(lane_addr + c0, v);
             load_row32(h1t, 128, r, c0, hv);
@@ -635,19 +716,20 @@ __global__ void __launch_bounds__(kBwdThreads, 1) k_flow_layer_bwd(BwdArgs a) {
                 ga[12] += gq * bf16_lo(w1.z); ga[13] += gq * bf16_hi(w1.z);
                 ga[14] += gq * bf16_lo(w1.w); ga[15] += gq * bf16_hi(w1.w);
             }
-        }
-        if (half == 1) {
+            if (grp > 0) {
 #pragma unroll
-            for (int i = 0; i < kMaxDA; ++i) sGA[i * 128 + r] = ga[i];
+                for (int i = 0; i < kMaxDA; ++i) sGA[((grp - 1) * kMaxDA + i) * 128 + r] = ga[i];
+            }
         }
         __syncthreads();
         copy_block(a.gp1s + tile * kHTile, sP, kHTile);
-        if (half == 0 && valid) {
+        if (grp == 0 && valid) {
 #pragma unroll
             for (int i = 0; i < kMaxDA; ++i)
                 if (i < da) {
                     const int d = a.L.cond[i];
-                    a.gin[d * n + row] = (a.gout ? a.gout[d * n + row] : 0.f) + 2.f * (ga[i] + sGA[i * 128 + r]);
+                    const float s3 = sGA[i * 128 + r] + sGA[(kMaxDA + i) * 128 + r] + sGA[(2 * kMaxDA + i) * 128 + r];
+                    a.gin[d * n + row] = (a.gout ? a.gout[d * n + row] : 0.f) + 2.f * (ga[i] + s3);
                 }
         }
         tc_fence_before();
