@@ -149,6 +149,42 @@ __device__ __forceinline__ int find_bin_hinted(const double *__restrict__ e, con
     return first - 1;
 }
 
+// The hint table of one (grid, dimension) row of edges e[0..bins], its
+// widths w[k] = e[k+1] - e[k] and its monotone flag, built by one block
+// (every thread of the block calls this).  hint[j] = first k in [0, bins)
+// with cell(e[k]) >= j, packed with hint[j+1] in the upper 16 bits.
+__device__ __forceinline__ void build_hint_row(const double *__restrict__ e, int bins, uint32_t *__restrict__ h,
+                                               uint8_t *__restrict__ sorted, double *__restrict__ w) {
+    const int H = kHintPerBin * bins;
+    int bad = 0;
+    for (int k = threadIdx.x; k < bins; k += blockDim.x) {
+        const double a = e[k];
+        if (a != a) bad = 1;
+        if (k + 1 < bins && !(a <= e[k + 1])) bad = 1;
+        w[k] = __dsub_rn(e[k + 1], a);
+    }
+    bad = __syncthreads_or(bad);
+    if (threadIdx.x == 0) *sorted = bad ? 0 : 1;
+    if (bad) return;
+    for (int j = threadIdx.x; j < H; j += blockDim.x) {
+        int lo[2];
+        for (int q = 0; q < 2; ++q) {
+            int first = 0, len = bins;
+            while (len > 0) {
+                const int half = len >> 1, mid = first + half;
+                if (edge_cell(e[mid], H) < j + q) {
+                    first = mid + 1;
+                    len = len - half - 1;
+                } else {
+                    len = half;
+                }
+            }
+            lo[q] = first;
+        }
+        h[j] = static_cast<uint32_t>(lo[0]) | (static_cast<uint32_t>(lo[1]) << 16);
+    }
+}
+
 // width(dim, bin) from the precomputed table wt[dim*bins + bin] (the same
 // subtraction as bin_width, done once per grid), the reference's reading of
 // bin == SIZE_MAX from the edges.

@@ -38,38 +38,9 @@ namespace chili_dev {
 __global__ void k_build_hints(const double *__restrict__ grids, int dims, int bins, uint32_t *__restrict__ hints,
                               uint8_t *__restrict__ sorted, double *__restrict__ widths) {
     const int d = blockIdx.x, c = blockIdx.y;
-    const int H = kHintPerBin * bins;
-    const double *e = grids + (static_cast<size_t>(c) * dims + d) * (bins + 1);
-    uint32_t *h = hints + (static_cast<size_t>(c) * dims + d) * H;
-    double *w = widths + (static_cast<size_t>(c) * dims + d) * bins;
-    int bad = 0;
-    for (int k = threadIdx.x; k < bins; k += blockDim.x) {
-        const double a = e[k];
-        if (a != a) bad = 1;
-        if (k + 1 < bins && !(a <= e[k + 1])) bad = 1;
-        w[k] = __dsub_rn(e[k + 1], a);
-    }
-    bad = __syncthreads_or(bad);
-    if (threadIdx.x == 0) sorted[static_cast<size_t>(c) * dims + d] = bad ? 0 : 1;
-    if (bad) return;
-    for (int j = threadIdx.x; j < H; j += blockDim.x) {
-        // first k in [0, bins) with cell(e[k]) >= j, and the same for j+1
-        int lo[2];
-        for (int q = 0; q < 2; ++q) {
-            int first = 0, len = bins;
-            while (len > 0) {
-                const int half = len >> 1, mid = first + half;
-                if (edge_cell(e[mid], H) < j + q) {
-                    first = mid + 1;
-                    len = len - half - 1;
-                } else {
-                    len = half;
-                }
-            }
-            lo[q] = first;
-        }
-        h[j] = static_cast<uint32_t>(lo[0]) | (static_cast<uint32_t>(lo[1]) << 16);
-    }
+    const size_t row = static_cast<size_t>(c) * dims + d;
+    build_hint_row(grids + row * (bins + 1), bins, hints + row * (kHintPerBin * bins), sorted + row,
+                   widths + row * bins);
 }
 
 __global__ void k_grid_map(const double *__restrict__ g, int dims, int bins, const double *__restrict__ u,
