@@ -222,32 +222,31 @@ namespace {
 // Host uniforms u[m][D+1]: rows [0, m) are copied into the staging buffer
 // in slices on the context's copy stream, slice s followed by
 // copy_events[s]: slices that double from kFirstSlice rows (the only copy
-// nothing overlaps) up to kUploadSlice rows, so that the weight passes start
-// early and the copies, a little faster per row than the weight pass, stay
-// ahead.  The rounds of the iteration take one slice each, so that the
-// upload of the next slices overlaps the whole weight pass of this one.
-constexpr long long kFirstSlice = 1ll << 16;   // rows; both multiples of kFwdBlock
-constexpr long long kUploadSlice = 1ll << 19;
+// nothing overlaps) up to the option "upload_slice" (2^19 rows), so that the
+// weight passes start early and the copies, a little faster per row than
+// the weight pass, stay ahead.  The rounds of the iteration take one slice
+// each, so that the upload of the next slices overlaps the whole weight pass
+// of this one.
+constexpr long long kFirstSlice = 1ll << 16;   // rows, a multiple of kFwdBlock
 
-long long slice_rows(long long s) { return s >= 3 ? kUploadSlice : std::min(kUploadSlice, kFirstSlice << s); }
-long long slice_begin(long long s) {
-    long long b = 0;
-    for (long long j = 0; j < s && j < 3; ++j) b += slice_rows(j);
-    if (s > 3) b += (s - 3) * kUploadSlice;
+// Slice boundaries of a chunk of m rows: slices that double from kFirstSlice
+// rows up to `top` rows (option "upload_slice", default kUploadSlice).
+std::vector<long long> slice_bounds(long long m, long long top) {
+    std::vector<long long> b{0};
+    long long len = kFirstSlice;
+    while (b.back() < m) {
+        b.push_back(std::min(b.back() + len, m));
+        len = std::min(2 * len, top);
+    }
     return b;
 }
-long long slice_count(long long m) {
-    long long n = 0;
-    while (slice_begin(n) < m) ++n;
-    return std::max(n, 1ll);
-}
 
-int upload_host(chili_ctx *ctx, const double *u, long long m) {
+int upload_host(chili_ctx *ctx, const double *u, long long m, const std::vector<long long> &sb) {
     const int D = ctx->ndims;
     const size_t row = sizeof(double) * (D + 1);
     CK(ctx->stage[0].ensure(row * static_cast<size_t>(m)));
     if (!ctx->copy_stream) CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
-    const long long nslices = slice_count(m);
+    const long long nslices = static_cast<long long>(sb.size()) - 1;
     while (static_cast<long long>(ctx->copy_events.size()) < nslices + 1) {
         cudaEvent_t e;
         CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -259,7 +258,7 @@ int upload_host(chili_ctx *ctx, const double *u, long long m) {
     CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->copy_events[nslices], 0));
     double *dst = ctx->stage[0].as<double>();
     for (long long s = 0; s < nslices; ++s) {
-        const long long s0 = slice_begin(s), len = std::min(slice_begin(s + 1), m) - s0;
+        const long long s0 = sb[s], len = sb[s + 1] - s0;
         CK(cudaMemcpyAsync(dst + s0 * (D + 1), u + s0 * (D + 1), row * static_cast<size_t>(len),
                            cudaMemcpyHostToDevice, ctx->copy_stream));
         CK(cudaEventRecord(ctx->copy_events[s], ctx->copy_stream));
@@ -485,6 +484,12 @@ int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value) {
     }
     if (std::strcmp(name, "batch_phased") == 0) {
         ctx->batch_phased = value != 0;
+        return CHILI_OK;
+    }
+    if (std::strcmp(name, "upload_slice") == 0) {
+        if (value < kFirstSlice || value > (1ll << 24) || value % kFwdBlock)
+            return fail(ctx, CHILI_ERR_INVALID_ARG, "upload_slice in [2^16, 2^24] rows, a multiple of 256");
+        ctx->upload_slice = value;
         return CHILI_OK;
     }
     if (std::strcmp(name, "pipeline_sync") == 0) {
@@ -1117,8 +1122,9 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         // keeps the count still needed and the chunk's totals (iter), and the
         // rounds after the one that completes the iteration do no work.
         // Otherwise the chunk is one round, its record read back at its end.
-        const long long S = u_host ? std::min(m, kUploadSlice) : m;  // rows of the largest round
-        const long long n_rounds = u_host ? slice_count(m) : 1;
+        const std::vector<long long> sb = u_host ? slice_bounds(m, ctx->upload_slice) : std::vector<long long>{0, m};
+        const long long S = u_host ? std::min(m, std::max(ctx->upload_slice, kFirstSlice)) : m;  // rows of the largest round
+        const long long n_rounds = static_cast<long long>(sb.size()) - 1;
         drawn += m;
         ++chunks;
         if (u_host) {
@@ -1127,7 +1133,7 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
             // the forward stream) wait on
             k_iter_init<<<1, 1, 0, ctx->stream>>>(iter, needed);
             LAUNCHED();
-            if ((rc = upload_host(ctx, u + tried * (D + 1), m))) return rc;
+            if ((rc = upload_host(ctx, u + tried * (D + 1), m, sb))) return rc;
         }
         // buffers for a whole number of 2^16 points (the chunk size follows
         // the acceptance rate and would otherwise reallocate, synchronising
@@ -1161,8 +1167,8 @@ int chili_gpu_multichannel_iterate(chili_ctx *ctx, const chili_multichannel_para
         }
         for (long long q = 0; q < n_rounds; ++q) {
             // this round's rows of the chunk: [r0, r0 + mm)
-            const long long r0 = u_host ? slice_begin(q) : 0;
-            const long long mm = u_host ? std::min(slice_begin(q + 1), m) - r0 : m;
+            const long long r0 = sb[q];
+            const long long mm = sb[q + 1] - r0;
             const long long nbf = (mm + kFwdBlock - 1) / kFwdBlock, nbw = (mm + kWgtBlock - 1) / kWgtBlock;
             const long long *gate = u_host ? iter : nullptr;
             // records with stride mm

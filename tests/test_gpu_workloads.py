@@ -141,10 +141,11 @@ def test_optimize_writes_one_json_line_per_iteration(ctx_factory):
     assert lines[-1]["pooled"] == mean and mean > 0 and 0 < err < mean
 
 
-@pytest.mark.parametrize("pipeline", [1, 0])
-def test_host_uniforms_in_slices_match_device_uniforms(ctx_factory, pipeline):
-    """Host uniforms (pinned) are uploaded in slices (2^16, 2^18, then 2^19 rows)
-    and each slice is mapped and weighted as its own queued round; the same uniforms in
+# (1, 500_000): chunks of more slices
+@pytest.mark.parametrize("pipeline,ncalls", [(1, 200_000), (0, 200_000), (1, 500_000)])
+def test_host_uniforms_in_slices_match_device_uniforms(ctx_factory, pipeline, ncalls):
+    """Host uniforms (pinned) are uploaded in slices (2^16, 2^17, 2^18, then
+    2^19 rows) and each slice is mapped and weighted as its own queued round; the same uniforms in
     device memory are read in place in one round.  Both take the same points
     (counts exact) and agree to the rounding of the partial-sum folds, over
     two adapting iterations with the physical-region cuts (the first one on
@@ -162,10 +163,16 @@ def test_host_uniforms_in_slices_match_device_uniforms(ctx_factory, pipeline):
         ctx.set_preprocess_cuts(1000.0)
         ctx.set_option("pipeline", pipeline)
         ctxs.append(ctx)
-    params = workloads.mc_params(200_000)
+    params = workloads.mc_params(ncalls)
+    if ncalls > 200_000:
+        # adapted grids first (uniform grids accept too few points under the
+        # cuts for the uniforms below), the same on both contexts
+        ctxs[0].multichannel_iterate(params, seed=3)
+        ctxs[1].set_grids(ctxs[0].get_grids())
+        ctxs[1].set_alpha(ctxs[0].get_alpha()[0])
     rng = np.random.default_rng(29)
     for it in range(2):
-        n_u = 2_500_000
+        n_u = 2_500_000 if ncalls <= 200_000 else 4_000_000
         host = torch.empty((n_u, ctxs[0].ndims + 1), dtype=torch.float64, pin_memory=True)
         host.numpy()[:] = workloads.uniforms53(rng, tuple(host.shape))
         dev = host.to("cuda")
