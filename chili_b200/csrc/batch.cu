@@ -54,6 +54,9 @@ struct BatchTask {
     long long unit0, units;    // first work unit, number of units
     long long grid_off;        // doubles: nch * dims * (bins+1)
     long long hist_off;        // doubles: nch * dims * bins
+    long long hint_off;        // bin-search hints (uint32): nch * dims * kHintPerBin * bins
+    long long width_off;       // bin widths (doubles): nch * dims * bins
+    long long sorted_off;      // monotone flags (bytes): nch * dims
     int32_t ch_off;            // first ChannelProgram / channel-weight slot
     int32_t desc;              // IntegrandDesc index
     int32_t pp;                // PointProgram index, -1: per-channel weights
@@ -80,6 +83,9 @@ struct BatchDev {
     const PointProgram *pps;
     const IntegrandDesc *descs;
     double *grids, *grids_new, *hist, *atrain;  // atrain per channel slot
+    uint32_t *hints;                            // bin-search tables of the grids (BatchTask offsets)
+    double *widths;
+    uint8_t *sorted;
     double *alpha, *best, *mindiff, *cp;        // per channel slot; mindiff per task
     double *part;                              // [nunits][6], task-contiguous
     double *stats;                             // [iter slot][ntasks][6]
@@ -378,6 +384,9 @@ struct Piece {
     long long p0, mm, ms;
     const PointProgram *pp;
     const double *grids, *alpha;
+    const uint32_t *hints;  // the task's bin-search tables (rows of its grids)
+    const double *widths;
+    const uint8_t *sorted;
     const IntegrandDesc *f;
     double *mom;
     int32_t *ich;
@@ -401,6 +410,7 @@ struct WaveDev {
     const Piece *pieces;
     int n;
     const long long *prefix;  // [kGroupSteps][n + 1]
+    int ch_pts;               // points per block of the channel step (a multiple of 128)
 };
 
 // The piece k in [lo, hi) of a step whose blocks [prefix[k], prefix[k+1])
@@ -455,26 +465,48 @@ __global__ void __launch_bounds__(256) k_g_chains(WaveDev W, int lo, int hi, lon
 }
 
 // Pieces [lo, hi) of the wave have DIMS dimensions. A block works on one
-// channel c of one piece; TAB: the block first stages channel c's edges
-// (DIMS x (bins + 1) doubles, dynamic shared memory) and its bin searches
-// read them there instead of through L1 from global memory.
+// channel c of one piece; TAB: the block first stages channel c's edges,
+// bin widths, hint tables and monotone flags (dynamic shared memory) and runs
+// the hinted bin search of the single-integrand path on them, instead of a
+// plain binary search through L1 on the edges in global memory.
 template <int DIMS, bool TAB>
 __global__ void __launch_bounds__(128) k_g_channel(WaveDev W, int lo, int hi, long long blk0) {
     CHILI_PIECE(GS_CHANNEL)
     const int c = static_cast<int>(lb % P.nch);
-    const long long i = (lb / P.nch) * 128 + threadIdx.x;
-    const double *g = P.grids;
+    const long long i0 = (lb / P.nch) * W.ch_pts;  // W.ch_pts points per block: one table copy for all of them
+    const long long n = P.ctl->n_acc;
     if constexpr (TAB) {
         extern __shared__ double se[];
-        const int ne = DIMS * (P.bins + 1);
-        const double *ge = P.grids + static_cast<size_t>(c) * ne;
+        const int bins = P.bins, H = kHintPerBin * bins;
+        const int ne = DIMS * (bins + 1), nw = DIMS * bins, nh = DIMS * H;
+        double *sw = se + ne;
+        uint32_t *sh = reinterpret_cast<uint32_t *>(sw + nw);
+        uint8_t *ss = reinterpret_cast<uint8_t *>(sh + nh);
+        const size_t row0 = static_cast<size_t>(c) * DIMS;
+        const double *ge = P.grids + row0 * (bins + 1);
+        const double *gw = P.widths + row0 * bins;
+        const uint32_t *gh = P.hints + row0 * H;
         for (int k = threadIdx.x; k < ne; k += 128) se[k] = __ldg(ge + k);
+        for (int k = threadIdx.x; k < nw; k += 128) sw[k] = __ldg(gw + k);
+        for (int k = threadIdx.x; k < nh; k += 128) sh[k] = __ldg(gh + k);
+        if (threadIdx.x < DIMS) ss[threadIdx.x] = __ldg(P.sorted + row0 + threadIdx.x);
         __syncthreads();
-        g = se;
+#pragma unroll 1
+        for (int j = 0; j < W.ch_pts; j += 128) {
+            const long long i = i0 + j + threadIdx.x;
+            if (i < P.ms && i < n)
+                pp_channel_point<DIMS, true, true>(P.pp, se, sh, ss, sw, bins, P.memo, P.cfail, P.ich_tile, P.ms,
+                                                   P.ms, 1, P.dcv, P.vwv, P.slot, P.dens, i, i, c);
+        }
+    } else {
+#pragma unroll 1
+        for (int j = 0; j < W.ch_pts; j += 128) {
+            const long long i = i0 + j + threadIdx.x;
+            if (i < P.ms && i < n)
+                pp_channel_point<DIMS, false>(P.pp, P.grids, nullptr, nullptr, nullptr, P.bins, P.memo, P.cfail,
+                                              P.ich_tile, P.ms, P.ms, 1, P.dcv, P.vwv, P.slot, P.dens, i, i, c);
+        }
     }
-    if (i < P.ms && i < P.ctl->n_acc)
-        pp_channel_point<DIMS, false, TAB>(P.pp, g, nullptr, nullptr, nullptr, P.bins, P.memo, P.cfail, P.ich_tile,
-                                           P.ms, P.ms, 1, P.dcv, P.vwv, P.slot, P.dens, i, i, c);
 }
 
 __global__ void __launch_bounds__(256) k_g_combine(WaveDev W, int lo, int hi, long long blk0) {
@@ -563,8 +595,26 @@ __global__ void k_batch_commit(BatchDev B, const AdaptJob *__restrict__ jobs, in
     if (j >= njobs) return;
     const AdaptJob J = jobs[j];
     const BatchTask T = B.tasks[J.task];
-    const size_t off = T.grid_off + (static_cast<size_t>(J.ch) * T.dims + J.dim) * (T.bins + 1);
+    const size_t row = static_cast<size_t>(J.ch) * T.dims + J.dim;
+    const size_t off = T.grid_off + row * (T.bins + 1);
     for (int k = threadIdx.x; k <= T.bins; k += blockDim.x) B.grids[off + k] = B.grids_new[off + k];
+    __syncthreads();
+    // the row's bin-search tables for the next iteration's channel step
+    build_hint_row(B.grids + off, T.bins, B.hints + T.hint_off + row * (kHintPerBin * T.bins),
+                   B.sorted + T.sorted_off + row, B.widths + T.width_off + row * T.bins);
+}
+
+// The bin-search tables of every (task, channel, dimension) row, one block
+// per row (after the grids are set).
+__global__ void k_batch_hints(BatchDev B, const AdaptJob *__restrict__ jobs, int njobs) {
+    const int j = blockIdx.x;
+    if (j >= njobs) return;
+    const AdaptJob J = jobs[j];
+    const BatchTask T = B.tasks[J.task];
+    const size_t row = static_cast<size_t>(J.ch) * T.dims + J.dim;
+    build_hint_row(B.grids + T.grid_off + row * (T.bins + 1), T.bins,
+                   B.hints + T.hint_off + row * (kHintPerBin * T.bins), B.sorted + T.sorted_off + row,
+                   B.widths + T.width_off + row * T.bins);
 }
 
 __global__ void k_batch_next(BatchDev B) {
@@ -583,7 +633,7 @@ struct BatchState {
     int max_bins = 2, nslots = 0;
     long long total_points = 0, nunits = 0;
     DevBuf d_tasks, d_umap, d_pps, d_progs, d_descs, d_grids, d_grids_new, d_hist, d_atrain, d_alpha, d_best, d_mindiff,
-        d_cp, d_part, d_stats, d_counters, d_jobs, d_status;
+        d_cp, d_part, d_stats, d_counters, d_jobs, d_status, d_hints, d_widths, d_sorted;
     int block = 0, ppt = 0, grid_blocks = 0;
     long long n_pulled = 0;  // units k_batch_eval pulls (the tasks that are not phased)
     // phased multichannel tasks: host copies of the point programs (launch
@@ -613,6 +663,7 @@ struct BatchState {
     DevBuf d_pieces, d_prefix;
     DevBuf d_arena[kMaxWaveStreams];  // wave w uses arena w % nstreams and stream w % nstreams
     int wave_streams = 2;
+    int ch_pts = 2048;  // points per block of the channel step (option "batch_channel_points" at planning)
     bool tuned = false;
     cudaGraphExec_t graph = nullptr;
     unsigned long long graph_launches = 0;  // kernels of one replay
@@ -641,6 +692,9 @@ BatchDev batch_dev(chili_ctx *ctx) {
     B.descs = S.d_descs.as<IntegrandDesc>();
     B.grids = S.d_grids.as<double>();
     B.grids_new = S.d_grids_new.as<double>();
+    B.hints = S.d_hints.as<uint32_t>();
+    B.widths = S.d_widths.as<double>();
+    B.sorted = S.d_sorted.as<uint8_t>();
     B.hist = S.d_hist.as<double>();
     B.atrain = S.d_atrain.as<double>();
     B.alpha = S.d_alpha.as<double>();
@@ -760,7 +814,7 @@ int enqueue_waves(chili_ctx *ctx, const BatchDev &B) {
     for (size_t wi = 0; wi < S.waves.size(); ++wi) {
         const auto &w = S.waves[wi];
         ctx->stream = S.ph_streams[wi % S.wave_streams];  // the wave's arena belongs to this stream
-        const WaveDev W{S.d_pieces.as<Piece>() + w.first, w.n, S.d_prefix.as<long long>() + w.prefix_off};
+        const WaveDev W{S.d_pieces.as<Piece>() + w.first, w.n, S.d_prefix.as<long long>() + w.prefix_off, S.ch_pts};
         const long long *pre = S.prefix_host.data() + w.prefix_off;
         auto blocks = [&](int step) { return static_cast<unsigned>(w.blocks[static_cast<size_t>(step)]); };
         k_g_forward<<<blocks(GS_FWD), kFwdBlock, 0, ctx->stream>>>(B, W, 0, w.n, 0);
@@ -791,8 +845,10 @@ int enqueue_waves(chili_ctx *ctx, const BatchDev &B) {
         for (const auto &g : w.dgroups) {
             const long long b0 = pc[g[1]], nbk = pc[g[2]] - b0;
             if (nbk <= 0) continue;
-            // one channel's edges in shared memory when they fit the default 48 KB
-            const size_t tab = sizeof(double) * static_cast<size_t>(g[0]) * (g[3] + 1);
+            // one channel's edges, widths, hints and flags in shared memory
+            // when they fit the default 48 KB
+            const size_t tab = sizeof(double) * static_cast<size_t>(g[0]) * (2 * g[3] + 1) +
+                               sizeof(uint32_t) * static_cast<size_t>(g[0]) * kHintPerBin * g[3] + g[0];
             const bool use_tab = ctx->channel_tables && tab <= 48 * 1024;
             switch (g[0]) {
 #define CHILI_GCH(D)                                                                                        \
@@ -958,6 +1014,7 @@ constexpr long long kPieceMax = 1ll << 20;
 
 int plan_waves(chili_ctx *ctx, const std::vector<PointProgram> &pps) {
     BatchState &S = *ctx->batch;
+    S.ch_pts = static_cast<int>(ctx->batch_ch_pts);
     // a piece never exceeds a wave (small waves, for tests, cut the tasks finer)
     const long long wave_max = std::max<long long>(ctx->batch_wave / kFwdBlock * kFwdBlock, kFwdBlock);
     const long long piece_max = std::min(kPieceMax, wave_max);
@@ -1046,6 +1103,9 @@ int plan_waves(chili_ctx *ctx, const std::vector<PointProgram> &pps) {
             P.bins = T.bins;
             P.pp = S.d_pps.as<PointProgram>() + T.pp;
             P.grids = S.d_grids.as<double>() + T.grid_off;
+            P.hints = S.d_hints.as<uint32_t>() + T.hint_off;
+            P.widths = S.d_widths.as<double>() + T.width_off;
+            P.sorted = S.d_sorted.as<uint8_t>() + T.sorted_off;
             P.alpha = S.d_alpha.as<double>() + T.ch_off;
             P.f = S.d_descs.as<IntegrandDesc>() + T.desc;
             size_t sz[18];
@@ -1073,7 +1133,7 @@ int plan_waves(chili_ctx *ctx, const std::vector<PointProgram> &pps) {
             P.ok = static_cast<uint8_t *>(ptr[15]);
             P.slot = static_cast<int32_t *>(ptr[16]);
             P.dens = static_cast<double *>(ptr[17]);
-            const long long gx = (P.ms + 255) / 256, gy = (P.ms + 127) / 128;
+            const long long gx = (P.ms + 255) / 256, gy = (P.ms + S.ch_pts - 1) / S.ch_pts;
             const long long nblk[kGroupSteps] = {P.nb, P.nb, gx, P.n_items[0] * gx, P.n_items[1] * gx,
                                                  P.n_items[2] * gx, P.n_chains * gx, P.nch * gy, gx, P.nb};
             for (int st = 0; st < kGroupSteps; ++st) pre[static_cast<size_t>(st)][k + 1] = pre[st][k] + nblk[st];
@@ -1120,6 +1180,7 @@ void batch_release(chili_ctx *ctx) {
     BatchState &S = *ctx->batch;
     if (S.graph) cudaGraphExecDestroy(S.graph);
     for (DevBuf *b : {&S.d_tasks, &S.d_umap, &S.d_pps, &S.d_progs, &S.d_descs, &S.d_grids, &S.d_grids_new, &S.d_hist,
+                      &S.d_hints, &S.d_widths, &S.d_sorted,
                       &S.d_atrain, &S.d_alpha, &S.d_best, &S.d_mindiff, &S.d_cp, &S.d_part, &S.d_stats,
                       &S.d_counters, &S.d_jobs, &S.d_status, &S.d_pieces, &S.d_prefix, &S.d_arena[0],
                       &S.d_arena[1], &S.d_arena[2], &S.d_arena[3]})
@@ -1146,7 +1207,7 @@ int chili_gpu_batch_set(chili_ctx *ctx, const chili_task *tasks, int ntasks) {
     std::vector<PointProgram> pps;
     std::vector<IntegrandDesc> descs;
     std::vector<double> grids, alpha;
-    long long goff = 0, hoff = 0;
+    long long goff = 0, hoff = 0, hnoff = 0, woff = 0, soff = 0;
     for (int k = 0; k < ntasks; ++k) {
         const chili_task &t = tasks[k];
         BatchTask T{};
@@ -1227,6 +1288,12 @@ int chili_gpu_batch_set(chili_ctx *ctx, const chili_task *tasks, int ntasks) {
         T.before = edge_before_table(T.dims, T.bins);
         T.grid_off = goff;
         T.hist_off = hoff;
+        T.hint_off = hnoff;
+        T.width_off = woff;
+        T.sorted_off = soff;
+        hnoff += static_cast<long long>(T.nch) * T.dims * kHintPerBin * T.bins;
+        woff += static_cast<long long>(T.nch) * T.dims * T.bins;
+        soff += static_cast<long long>(T.nch) * T.dims;
         const long long per = static_cast<long long>(T.dims) * (T.bins + 1);
         for (int c = 0; c < T.nch; ++c)
             for (int dd = 0; dd < T.dims; ++dd)
@@ -1313,6 +1380,9 @@ int chili_gpu_batch_set(chili_ctx *ctx, const chili_task *tasks, int ntasks) {
     CK(S.d_grids.ensure(sizeof(double) * grids.size()));
     CK(S.d_grids_new.ensure(sizeof(double) * grids.size()));
     CK(cudaMemcpyAsync(S.d_grids.p, grids.data(), sizeof(double) * grids.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CK(S.d_hints.ensure(sizeof(uint32_t) * std::max<long long>(hnoff, 1)));
+    CK(S.d_widths.ensure(sizeof(double) * std::max<long long>(woff, 1)));
+    CK(S.d_sorted.ensure(std::max<long long>(soff, 1)));
     CK(S.d_hist.ensure(sizeof(double) * std::max<size_t>(S.hist_doubles, 1)));
     CK(S.d_atrain.ensure(sizeof(double) * nslot));
     CK(S.d_alpha.ensure(sizeof(double) * nslot));
@@ -1348,7 +1418,16 @@ int chili_gpu_batch_set(chili_ctx *ctx, const chili_task *tasks, int ntasks) {
     CK(cudaStreamSynchronize(ctx->stream));
     if (S.grouped)
         if (int rc = plan_waves(ctx, pps)) return rc;
-    return layout_units(ctx, 256, 1);
+    if (int rc = layout_units(ctx, 256, 1)) return rc;
+    // the bin-search tables of the initial grids (k_batch_commit keeps them
+    // current after every adaptation)
+    if (!S.jobs.empty()) {
+        k_batch_hints<<<static_cast<unsigned>(S.jobs.size()), 128, 0, ctx->stream>>>(
+            batch_dev(ctx), S.d_jobs.as<AdaptJob>(), static_cast<int>(S.jobs.size()));
+        LAUNCHED();
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHILI_OK;
 }
 
 int chili_gpu_batch_iterate(chili_ctx *ctx, int iterations, uint64_t seed, int adapt, chili_stats *stats,

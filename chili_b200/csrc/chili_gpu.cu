@@ -482,6 +482,12 @@ int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value) {
         ctx->batch_wave = value;
         return CHILI_OK;
     }
+    if (std::strcmp(name, "batch_channel_points") == 0) {
+        if (value < 128 || value > 4096 || value % 128)
+            return fail(ctx, CHILI_ERR_INVALID_ARG, "batch_channel_points: a multiple of 128 in [128, 4096]");
+        ctx->batch_ch_pts = value;
+        return CHILI_OK;
+    }
     if (std::strcmp(name, "batch_phased") == 0) {
         ctx->batch_phased = value != 0;
         return CHILI_OK;
