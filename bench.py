@@ -398,20 +398,21 @@ def compact_other_workloads(args, dev, rank):
         ctx.close()
         # the 512 batched integrands
         tasks = workloads.batched_tasks(seed=BATCH_SEED + rank)
-        npts = sum(t["ncalls"] for t in tasks)
         ctx = gpu.Context(dev.index)
         ctx.set_stream(stream.cuda_stream)
         ctx.batch_set(tasks)
         ctx.batch_iterate(1, seed=BATCH_SEED)
         ctx.batch_iterate(1, seed=BATCH_SEED)
         l0 = ctx.launches
-        bms = 0.0
+        bms, calls = 0.0, 0.0
         for _ in range(3):
-            _, info = ctx.batch_iterate(1, seed=BATCH_SEED)
+            st, info = ctx.batch_iterate(1, seed=BATCH_SEED)
             bms += info.ms_per_iteration
+            calls += float(st[0][:, 0].sum())
         out["batched"] = {"workload": "512 integrands (256 camels D 2-12, 256 multichannel 2->n), one adapting "
-                                      "iteration each per step", "ms_per_iteration": bms / 3,
-                          "points_per_s": npts / (bms / 3 / 1e3), "launches_per_iteration": (ctx.launches - l0) / 3,
+                                      "iteration each per step (fixed budget)",
+                          "ms_per_iteration": bms / 3,
+                          "points_per_s": calls / (bms / 1e3), "launches_per_iteration": (ctx.launches - l0) / 3,
                           "full_line": "python bench.py --workload batched"}
         ctx.close()
         # 2->6, 45 channels, 200 bins, 1e7 points per iteration
@@ -1195,7 +1196,9 @@ def batched_config(tasks, world):
     return {"workload": "512 batched integrands: 256 camel functions (dims 2-12, sigma in [0.05, 0.2], centres in "
                         "[0.2, 0.8], 50 bins, grid alpha 1.5) + 256 multichannel 2->n propagator integrands "
                         "(n = 2..5, sqrt(S) in [200, 2000] GeV, 50 bins, channel weights adapted); points per "
-                        "integrand log-uniform in [1e4, 1e6]; every drawn point is one call (fixed budget)",
+                        "integrand log-uniform in [1e4, 1e6]; every drawn point is one call (fixed budget: the "
+                        "reference's retry loop, option batch_retry, never finishes this batch: one task's channel "
+                        "weights turn NaN after three iterations under it, as the C oracle shows)",
             "tasks": len(tasks), "camel_tasks": kinds.count("camel"),
             "multichannel_tasks": kinds.count("multichannel"),
             "points_per_iteration": int(sum(t["ncalls"] for t in tasks)), "seed": BATCH_SEED,
@@ -1265,6 +1268,7 @@ def run_batched(args, rank, world, local_rank):
     barrier()
     l0 = ctx.launches
     dev_ms, wall = 0.0, 0.0
+    retry_rounds = 0
     pooled = np.zeros((len(tasks), 6))
     with ClockSampler(local_rank) as clk:
         for _ in range(args.steps):
@@ -1275,6 +1279,7 @@ def run_batched(args, rank, world, local_rank):
             st, info = ctx.batch_iterate(1, seed=BATCH_SEED)  # host StatsData read back inside the call
             wall += time.perf_counter() - w0
             dev_ms += info.ms_per_iteration
+            retry_rounds += info.retry_rounds
             pooled += st[0]
     torch.cuda.synchronize(dev)
     launches = ctx.launches - l0
@@ -1290,7 +1295,10 @@ def run_batched(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline_batched()
     if rank == 0:
-        value = npts * world * args.steps / (ms_max / 1e3)
+        # points = StatsData calls (with the fixed budget, every drawn point;
+        # the reference arm counts its calls, rejections included)
+        calls = float(pooled[:, 0].sum())
+        value = calls * world / (ms_max / 1e3)
         per_iter = ms_max / args.steps
         kinds = np.array([t["kind"] == "camel" for t in tasks])
         line = {
@@ -1301,8 +1309,10 @@ def run_batched(args, rank, world, local_rank):
             "config": batched_config(tasks, world),
             "autotune": {"block": info.block, "points_per_thread": info.points_per_thread,
                          "units_per_iteration": info.units, "first_call_s": setup_s},
+            "calls_per_iteration": calls / args.steps, "accepted_per_iteration": npts,
+            "retry_rounds_timed": retry_rounds,
             "sequential": None if seq_ms is None else {
-                "ms_per_iteration": seq_ms, "points_per_s": npts / (seq_ms / 1e3),
+                "ms_per_iteration": seq_ms, "points_per_s": calls / args.steps / (seq_ms / 1e3),
                 "batched_speedup": seq_ms / per_iter,
                 "path": "one chili_gpu_vegas_iterate / chili_gpu_multichannel_iterate call per task "
                         "(multichannel with the reference's retry loop)"},
@@ -1310,8 +1320,8 @@ def run_batched(args, rank, world, local_rank):
                                  "multichannel": float(pooled[~kinds, 5].sum() / pooled[~kinds, 0].sum())},
             "clocks": clk.summary(),
             "gpu_launches": launches,
-            "roofline": batched_roofline(per_iter, tasks, dev),
-            "e2e": {"value": npts * world * args.steps / wall_max, "unit": BATCH_UNIT, "h2d_bytes_per_step": 0,
+            "roofline": batched_roofline(per_iter, calls / args.steps, dev),
+            "e2e": {"value": calls * world / wall_max, "unit": BATCH_UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": int(st.nbytes),
                     "path": "chili_gpu_batch_iterate (graph replay + host StatsData of every task) by wall clock; "
                             "the uniforms are counter-based and drawn in the kernel, as the reference draws its "
@@ -1330,14 +1340,14 @@ BATCH_COUNTERS = {"fp64_ops_per_point": 3623.3, "dram_bytes_per_point": 651.0,
                   "source": "profiles/batched_integrands.md"}
 
 
-def batched_roofline(ms_per_iter, tasks, dev):
+def batched_roofline(ms_per_iter, npts, dev):
     """The iteration's kernels together (k_batch_eval for the camel tasks;
     k_bt_forward, the phased k_pp_* weight pass and k_bt_accum for the
-    multichannel ones) against the FP64 peak measured in this run; the
-    algorithmic HBM traffic is nil (counter-based uniforms, grids and
-    histograms in L2; the phased buffers of one task tile)."""
+    multichannel ones) against the FP64 peak measured in this run, over the
+    iteration's npts calls; the algorithmic HBM traffic is nil
+    (counter-based uniforms, grids and histograms in L2; the phased buffers
+    of one task tile)."""
     peak = fp64_peak_tflops(dev)
-    npts = sum(t["ncalls"] for t in tasks)
     c = BATCH_COUNTERS
     achieved = c["fp64_ops_per_point"] * npts / (ms_per_iter / 1e3) / 1e12
     return {"kernel": "k_batch_eval + k_bt_forward + k_pp_* + k_bt_accum (one iteration)", "bound": "fp64",

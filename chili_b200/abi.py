@@ -165,7 +165,7 @@ class Task(C.Structure):
 
 class BatchInfo(C.Structure):
     _fields_ = [("block", C.c_uint32), ("points_per_thread", C.c_uint32), ("ms_per_iteration", C.c_double),
-                ("units", C.c_uint64), ("points", C.c_uint64)]
+                ("units", C.c_uint64), ("points", C.c_uint64), ("retry_rounds", C.c_uint64)]
 
 
 class ChannelSet:

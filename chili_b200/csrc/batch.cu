@@ -8,9 +8,16 @@
 // histogram, AdaptiveMap::Adapt) or a multichannel FSMapper integrand with
 // the combined weight of all its channels (Integrand::GenerateWeight,
 // Integrand.hh:112-123), its channel histograms and alpha training
-// (MultiChannel.hh:167-194), on a fixed budget of ncalls drawn points per
-// iteration (PreProcess rejections count as zero-valued calls; there is no
-// retry loop in the batched mode).
+// (MultiChannel.hh:167-194).  A multichannel task's iteration keeps the
+// reference's retry loop (MultiChannel.hh:214-248): points are drawn until
+// ncalls of them pass PreProcess with a finite value, and the rejected ones
+// enter StatsData as zero-valued calls (option batch_retry; with it off, the
+// default, a fixed budget of ncalls drawn points).  The retry loop runs in
+// rounds: round 0 draws the task's planned count (ncalls at first, then the
+// points the previous iterations needed, plus a margin) and cuts the task at
+// its ncalls-th accepted point; a task still short of ncalls after a round
+// (too few accepted points, or NaN values) draws again from the counter after
+// the last one counted, in further rounds sized on the device.
 //
 // Work units are tiles of blockDim * points_per_thread points of one task;
 // a persistent grid (resident blocks of every SM) pulls units from an atomic
@@ -51,6 +58,9 @@ constexpr int kMaxWaveStreams = 4;
 struct BatchTask {
     int32_t kind, dims, bins, nch;
     long long ncalls;
+    long long draw;            // points a round may draw (phased tasks; ncalls with a fixed budget)
+    int32_t retry;             // 1: the reference's retry loop (rounds, RetryState)
+    int32_t pad_;
     long long unit0, units;    // first work unit, number of units
     long long grid_off;        // doubles: nch * dims * (bins+1)
     long long hist_off;        // doubles: nch * dims * bins
@@ -64,6 +74,22 @@ struct BatchTask {
     double grid_alpha, beta, min_alpha;
     double before;             // edge_before_table(dims, bins)
     uint64_t key;              // Philox key of the task
+};
+
+// Retry loop of one multichannel task in the current iteration (reset by
+// k_rt_begin, advanced by k_rt_end after every round).
+struct RetryState {
+    long long need;       // accepted points with a finite value still wanted
+    long long ctr0;       // counter offset of the next round (points counted so far)
+    long long lim;        // points the next round draws (at most the task's draw)
+    long long rounds;
+    // this round, summed over the task's pieces (their RoundCtl lives in the
+    // wave's arena, which a later wave on the same stream reuses)
+    unsigned long long counted_round;   // points before the pieces' cuts
+    unsigned long long accepted_round;  // accepted points before the cuts
+    unsigned long long nan_round;       // of those, NaN values
+    unsigned long long nan_total;       // NaN values of the iteration
+    double acc[6];        // StatsData of the rounds so far
 };
 
 // Work unit u of the iteration: unit `unit` of task `task`.  Units are
@@ -92,6 +118,8 @@ struct BatchDev {
     int stat_slots;
     unsigned long long *next_unit;
     unsigned long long *iter;
+    RetryState *retry;  // [ntasks]
+    int *rflag;         // after a round: 1 some task needs another round, 2 counter space exhausted
     int ppt;
 };
 
@@ -231,17 +259,19 @@ __global__ void __launch_bounds__(256) k_batch_eval(BatchDev B) {
 // them (Philox key of the task, counters (iteration << 32) + point), the
 // channel, VEGAS map, FSMapper and PreProcess; accepted points' external
 // momenta to mom_soa [slot][component][ms], per block of kFwdBlock points
-// the accepted count.
+// the accepted count.  ctr_off: the retry round's counter offset (the points
+// the task's earlier rounds of this iteration counted).
 __device__ __forceinline__ void bt_forward_block(const BatchDev &B, int ti, long long p0, long long mm,
                                                  double *__restrict__ mom_soa, long long ms,
                                                  int32_t *__restrict__ ich_out, uint8_t *__restrict__ flag,
-                                                 int32_t *__restrict__ block_count, long long bx) {
+                                                 int32_t *__restrict__ block_count, long long bx,
+                                                 long long ctr_off = 0) {
     const BatchTask T = B.tasks[ti];
     const long long k = bx * static_cast<long long>(kFwdBlock) + threadIdx.x;
     int acc = 0;
     if (k < mm) {
         const int D = T.dims, bins = T.bins;
-        const uint64_t ctr = (*B.iter << 32) + static_cast<uint64_t>(p0 + k);
+        const uint64_t ctr = (*B.iter << 32) + static_cast<uint64_t>(ctr_off + p0 + k);
         double r[CHILI_MAX_DIMS + 1];
         load_uniforms(T.key, ctr, nullptr, D + 1, r);
         const int c = select_channel(B.cp + T.ch_off, T.nch, r[D]);
@@ -281,7 +311,10 @@ __global__ void __launch_bounds__(kFwdBlock) k_bt_forward(BatchDev B, int ti, lo
 // block_off[b] .. + block_count[b] (the list keeps point order), the others
 // are calls of value 0.  StatsData partial of the unit, AddTrainData
 // (MultiChannel.hh:167-180) histogram adds and channel-training terms, as
-// k_batch_eval does per point (NaN values count as 0).
+// k_batch_eval does per point (NaN values count as 0).  ctl (retry rounds):
+// only the points before the round's cut are calls and only the first n_acc
+// accepted points are records; R: the round's NaN values are counted (they
+// do not count towards ncalls, MultiChannel.hh:229-235).
 __device__ __forceinline__ void bt_accum_block(const BatchDev &B, int ti, long long p0, long long mm,
                                                const int32_t *__restrict__ block_count,
                                                const long long *__restrict__ block_off,
@@ -289,7 +322,9 @@ __device__ __forceinline__ void bt_accum_block(const BatchDev &B, int ti, long l
                                                const double *__restrict__ rec_wgt,
                                                const uint8_t *__restrict__ rec_ok,
                                                const int32_t *__restrict__ rec_slot,
-                                               const double *__restrict__ rec_dens, long long mr, long long bx) {
+                                               const double *__restrict__ rec_dens, long long mr, long long bx,
+                                               const RoundCtl *__restrict__ ctl = nullptr,
+                                               RetryState *__restrict__ R = nullptr) {
     __shared__ double ws[kFwdBlock / 32][6];
     __shared__ double s_atr[kBatchMaxCh];
     const BatchTask T = B.tasks[ti];
@@ -297,9 +332,25 @@ __device__ __forceinline__ void bt_accum_block(const BatchDev &B, int ti, long l
     if (t < kBatchMaxCh) s_atr[t] = 0.0;
     __syncthreads();
     const long long k0 = bx * static_cast<long long>(kFwdBlock);
-    const long long active = mm - k0 < kFwdBlock ? mm - k0 : kFwdBlock;
-    const int nrec = block_count[bx];
+    const long long upto = ctl ? (ctl->cut < mm ? ctl->cut : mm) : mm;  // points counted in this piece
+    const long long active = upto - k0 <= 0 ? 0 : (upto - k0 < kFwdBlock ? upto - k0 : kFwdBlock);
+    int nrec = block_count[bx];
+    if (ctl) {
+        // a block past the cut has no records; where the whole piece lies
+        // past it (the task had its ncalls before the piece) the scan wrote
+        // no offsets, so block_off is not read
+        if (active == 0) {
+            nrec = 0;
+        } else {
+            const long long left = ctl->n_acc - block_off[bx];
+            nrec = left <= 0 ? 0 : (left < nrec ? static_cast<int>(left) : nrec);
+        }
+    }
     const long long r = block_off[bx] + t;
+    if (R) {
+        const int nan_recs = __syncthreads_count(t < nrec && !rec_ok[r]);
+        if (t == 0 && nan_recs) atomicAdd(&R->nan_round, static_cast<unsigned long long>(nan_recs));
+    }
     double val = 0, vw = 0;
     if (t < nrec) {
         val = rec_ok[r] ? rec_val[r] : 0.0;
@@ -431,14 +482,56 @@ __device__ __forceinline__ int find_piece(const long long *__restrict__ pre, int
     const Piece &P = W.pieces[k_];                                               \
     const long long lb = b_ - pre_[k_];
 
-__global__ void __launch_bounds__(kFwdBlock) k_g_forward(BatchDev B, WaveDev W, int lo, int hi, long long blk0) {
-    CHILI_PIECE(GS_FWD)
-    bt_forward_block(B, P.ti, P.p0, P.mm, P.mom, P.ms, P.ich, P.flag, P.bcount, lb);
+// Points of piece P that the task's current retry round draws: the round's
+// limit R.lim (from the task's first point), none once the task has its
+// ncalls.
+__device__ __forceinline__ long long round_points(const RetryState &R, const Piece &P) {
+    if (R.need <= 0) return 0;
+    const long long m = R.lim - P.p0;
+    return m <= 0 ? 0 : (m < P.mm ? m : P.mm);
 }
 
-__global__ void __launch_bounds__(1024) k_g_scan(WaveDev W) {
+__global__ void __launch_bounds__(kFwdBlock) k_g_forward(BatchDev B, WaveDev W, int lo, int hi, long long blk0) {
+    CHILI_PIECE(GS_FWD)
+    if (B.tasks[P.ti].retry) {
+        const RetryState &R = B.retry[P.ti];
+        bt_forward_block(B, P.ti, P.p0, round_points(R, P), P.mom, P.ms, P.ich, P.flag, P.bcount, lb, R.ctr0);
+    } else {
+        bt_forward_block(B, P.ti, P.p0, P.mm, P.mom, P.ms, P.ich, P.flag, P.bcount, lb);
+    }
+}
+
+// Per piece, the ordered offsets of its accepted points.  Retry rounds: the
+// piece is cut at the point that brings its task to ncalls accepted points,
+// counting the accepted points of the task's earlier pieces (adjacent in the
+// wave, in counter order) first.
+__global__ void __launch_bounds__(1024) k_g_scan(BatchDev B, WaveDev W) {
     const Piece &P = W.pieces[blockIdx.x];
-    mc_scan_body(P.bcount, P.nb, P.flag, P.mm, P.mm + 1, nullptr, 0, P.boff, P.ctl);
+    if (!B.tasks[P.ti].retry) {
+        mc_scan_body(P.bcount, P.nb, P.flag, P.mm, P.mm + 1, nullptr, 0, P.boff, P.ctl);
+        return;
+    }
+    const RetryState &R = B.retry[P.ti];  // need, lim, ctr0: fixed during the round
+    __shared__ unsigned long long before_s;
+    __shared__ long long rem_s;
+    if (threadIdx.x == 0) before_s = 0;
+    __syncthreads();
+    for (int j = static_cast<int>(blockIdx.x) - 1; j >= 0 && W.pieces[j].ti == P.ti; --j) {
+        const Piece &Q = W.pieces[j];
+        unsigned long long c = 0;
+        for (int b = threadIdx.x; b < Q.nb; b += blockDim.x) c += static_cast<unsigned long long>(Q.bcount[b]);
+        if (c) atomicAdd(&before_s, c);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) rem_s = R.need - static_cast<long long>(before_s);
+    __syncthreads();
+    mc_scan_body(P.bcount, P.nb, P.flag, round_points(R, P), 0, &rem_s, 1, P.boff, P.ctl);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        RetryState &Rw = B.retry[P.ti];
+        atomicAdd(&Rw.counted_round, static_cast<unsigned long long>(P.ctl->cut));
+        atomicAdd(&Rw.accepted_round, static_cast<unsigned long long>(P.ctl->n_acc));
+    }
 }
 
 __global__ void __launch_bounds__(kFwdBlock) k_g_compact(WaveDev W, int lo, int hi, long long blk0) {
@@ -518,7 +611,9 @@ __global__ void __launch_bounds__(256) k_g_combine(WaveDev W, int lo, int hi, lo
 
 __global__ void __launch_bounds__(kFwdBlock) k_g_accum(BatchDev B, WaveDev W, int lo, int hi, long long blk0) {
     CHILI_PIECE(GS_ACCUM)
-    bt_accum_block(B, P.ti, P.p0, P.mm, P.bcount, P.boff, P.val, P.wgt, P.ok, P.slot, P.dens, P.ms, lb);
+    const bool retry = B.tasks[P.ti].retry != 0;
+    bt_accum_block(B, P.ti, P.p0, P.mm, P.bcount, P.boff, P.val, P.wgt, P.ok, P.slot, P.dens, P.ms, lb,
+                   retry ? P.ctl : nullptr, retry ? B.retry + P.ti : nullptr);
 }
 #undef CHILI_PIECE
 
@@ -565,11 +660,101 @@ __global__ void __launch_bounds__(kFoldThreads) k_batch_finalize(BatchDev B, int
     if (t == 0) {
         const uint64_t slot = *B.iter % static_cast<uint64_t>(B.stat_slots);
         double *o = B.stats + (slot * B.ntasks + ti) * 6;
-        for (int k = 0; k < 6; ++k) o[k] = sh[k][0];
+        // retry tasks: the StatsData that k_rt_end folded round by round
+        for (int k = 0; k < 6; ++k) o[k] = T.retry ? B.retry[ti].acc[k] : sh[k][0];
         if (adapt && T.kind == CHILI_TASK_MULTICHANNEL)
             alpha_update(B.alpha + T.ch_off, B.best + T.ch_off, B.mindiff + ti, B.cp + T.ch_off,
                          B.atrain + T.ch_off, T.nch, T.beta, T.min_alpha, 1);
     }
+}
+
+// Retry loop: the state of every retry task at the start of an iteration
+// (one thread per task).
+__global__ void k_rt_begin(BatchDev B) {
+    const int ti = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ti >= B.ntasks) return;
+    const BatchTask &T = B.tasks[ti];
+    if (!T.retry) return;
+    RetryState &R = B.retry[ti];
+    R.need = T.ncalls;
+    R.ctr0 = 0;
+    R.lim = T.draw;
+    R.rounds = 0;
+    R.counted_round = 0;
+    R.accepted_round = 0;
+    R.nan_round = 0;
+    R.nan_total = 0;
+    const double e[6] = {0, 1.7976931348623157e308, 2.2250738585072014e-308, 0, 0, 0};
+    for (int k = 0; k < 6; ++k) R.acc[k] = e[k];
+}
+
+// After a round (one block of kFoldThreads per task): the round's unit
+// partials folded in unit order into the task's StatsData, the accepted
+// points with a finite value subtracted from need, the counter offset moved
+// past the points counted; a task still short of ncalls flags another round,
+// sized from this round's rate of accepted points per point drawn.
+__global__ void __launch_bounds__(kFoldThreads) k_rt_end(BatchDev B) {
+    __shared__ double sh[6][kFoldThreads];
+    const int ti = blockIdx.x, t = threadIdx.x;
+    const BatchTask T = B.tasks[ti];
+    if (!T.retry) return;
+    RetryState &R = B.retry[ti];
+    if (R.need <= 0) return;  // finished in an earlier round: this round drew nothing for it
+    double a[6] = {0, 1.7976931348623157e308, 2.2250738585072014e-308, 0, 0, 0};
+    for (long long u = T.unit0 + t; u < T.unit0 + T.units; u += kFoldThreads) {
+        const double *p = B.part + u * 6;
+        a[0] += p[0];
+        a[1] = std_min(a[1], p[1]);
+        a[2] = std_max(a[2], p[2]);
+        a[3] += p[3];
+        a[4] += p[4];
+        a[5] += p[5];
+    }
+    for (int k = 0; k < 6; ++k) sh[k][t] = a[k];
+    __syncthreads();
+    for (int w = kFoldThreads / 2; w > 0; w >>= 1) {
+        if (t < w) {
+            sh[0][t] += sh[0][t + w];
+            sh[1][t] = std_min(sh[1][t], sh[1][t + w]);
+            sh[2][t] = std_max(sh[2][t], sh[2][t + w]);
+            sh[3][t] += sh[3][t + w];
+            sh[4][t] += sh[4][t + w];
+            sh[5][t] += sh[5][t + w];
+        }
+        __syncthreads();
+    }
+    if (t != 0) return;
+    R.acc[0] += sh[0][0];
+    R.acc[1] = std_min(R.acc[1], sh[1][0]);
+    R.acc[2] = std_max(R.acc[2], sh[2][0]);
+    R.acc[3] += sh[3][0];
+    R.acc[4] += sh[4][0];
+    R.acc[5] += sh[5][0];
+    const long long counted = static_cast<long long>(R.counted_round);
+    const long long valid = static_cast<long long>(R.accepted_round) - static_cast<long long>(R.nan_round);
+    R.need -= valid;
+    R.ctr0 += counted;
+    R.nan_total += R.nan_round;
+    R.counted_round = 0;
+    R.accepted_round = 0;
+    R.nan_round = 0;
+    R.rounds += 1;
+    if (R.need <= 0) return;
+    if (R.ctr0 + T.draw >= (1ll << 32)) {  // counters (iteration << 32) + point
+        R.need = 0;
+        atomicMax(B.rflag, 2);
+        return;
+    }
+    // the next round: the points this round's rate predicts, 1/4 more and two
+    // blocks' worth besides, at most the task's draw (the pieces cover no more)
+    long long lim = T.draw;
+    if (valid > 0 && counted > 0) {
+        const double want = static_cast<double>(R.need) * static_cast<double>(counted) / static_cast<double>(valid);
+        const double l = 1.25 * want + 2.0 * kFwdBlock;
+        if (l < static_cast<double>(T.draw)) lim = static_cast<long long>(l);
+    }
+    R.lim = lim;
+    atomicMax(B.rflag, 1);
 }
 
 // Grid adaptation of every (task, channel, dimension): one block each.
@@ -667,6 +852,13 @@ struct BatchState {
     bool tuned = false;
     cudaGraphExec_t graph = nullptr;
     unsigned long long graph_launches = 0;  // kernels of one replay
+    // retry tasks (option batch_retry): the further-round and final graphs,
+    // per-task loop state, the round flag
+    bool has_retry = false;
+    cudaGraphExec_t graph_top = nullptr, graph_fin = nullptr;
+    unsigned long long top_launches = 0, fin_launches = 0;
+    DevBuf d_retry, d_rflag;
+    unsigned long long retry_rounds = 0;  // further rounds run by the last batch_iterate call
     int graph_adapt = -1;
     double last_ms = 0;
     size_t hist_doubles = 0;
@@ -706,6 +898,8 @@ BatchDev batch_dev(chili_ctx *ctx) {
     B.stat_slots = S.nslots_alloc;
     B.next_unit = S.d_counters.as<unsigned long long>();
     B.iter = S.d_counters.as<unsigned long long>() + 1;
+    B.retry = S.d_retry.as<RetryState>();
+    B.rflag = S.d_rflag.as<int>();
     B.ppt = S.ppt;
     return B;
 }
@@ -720,7 +914,7 @@ int layout_units(chili_ctx *ctx, int block, int ppt) {
         // a phased task's units are the kFwdBlock-point blocks of its tiles
         const long long tt = T.phased ? kFwdBlock : tile;
         T.unit0 = u;
-        T.units = (T.ncalls + tt - 1) / tt;
+        T.units = ((T.phased ? T.draw : T.ncalls) + tt - 1) / tt;
         u += T.units;
     }
     S.nunits = u;
@@ -819,7 +1013,7 @@ int enqueue_waves(chili_ctx *ctx, const BatchDev &B) {
         auto blocks = [&](int step) { return static_cast<unsigned>(w.blocks[static_cast<size_t>(step)]); };
         k_g_forward<<<blocks(GS_FWD), kFwdBlock, 0, ctx->stream>>>(B, W, 0, w.n, 0);
         LAUNCHED();
-        k_g_scan<<<static_cast<unsigned>(w.n), 1024, 0, ctx->stream>>>(W);
+        k_g_scan<<<static_cast<unsigned>(w.n), 1024, 0, ctx->stream>>>(B, W);
         LAUNCHED();
         k_g_compact<<<blocks(GS_COMPACT), kFwdBlock, 0, ctx->stream>>>(W, 0, w.n, 0);
         LAUNCHED();
@@ -874,13 +1068,46 @@ int enqueue_waves(chili_ctx *ctx, const BatchDev &B) {
     return CHILI_OK;
 }
 
-// The iteration as a stream of launches (captured into the graph).
+// A retry round after the first (captured into its own graph): the waves
+// again for the tasks still short of ncalls (the others draw nothing), then
+// the round's bookkeeping.
+int enqueue_retry_round(chili_ctx *ctx) {
+    BatchState &S = *ctx->batch;
+    BatchDev B = batch_dev(ctx);
+    const cudaStream_t main = ctx->stream;
+    const int ns = S.wave_streams;
+    CK(cudaMemsetAsync(S.d_rflag.p, 0, sizeof(int), main));
+    CK(cudaEventRecord(S.ph_events[ns], main));
+    for (int j = 0; j < ns; ++j) CK(cudaStreamWaitEvent(S.ph_streams[j], S.ph_events[ns], 0));
+    const int rc = enqueue_waves(ctx, B);
+    ctx->stream = main;
+    if (rc) return rc;
+    for (int j = 0; j < ns; ++j) {
+        CK(cudaEventRecord(S.ph_events[j], S.ph_streams[j]));
+        CK(cudaStreamWaitEvent(main, S.ph_events[j], 0));
+    }
+    k_rt_end<<<static_cast<unsigned>(S.tasks.size()), kFoldThreads, 0, main>>>(B);
+    LAUNCHED();
+    return CHILI_OK;
+}
+
+// The iteration's folds, channel-weight update, grid adaptation and counter
+// (captured into its own graph when retry rounds may run before it).
+int enqueue_final(chili_ctx *ctx, bool adapt);
+
+// The iteration as a stream of launches (captured into the graph); with
+// retry tasks only its first round (the final part is a graph of its own).
 int enqueue_iteration(chili_ctx *ctx, bool adapt) {
     BatchState &S = *ctx->batch;
     CK(cudaMemsetAsync(S.d_hist.p, 0, sizeof(double) * S.hist_doubles, ctx->stream));
     CK(cudaMemsetAsync(S.d_atrain.p, 0, S.d_atrain.cap, ctx->stream));
     BatchDev B = batch_dev(ctx);
     const cudaStream_t main = ctx->stream;
+    if (S.has_retry) {
+        CK(cudaMemsetAsync(S.d_rflag.p, 0, sizeof(int), main));
+        k_rt_begin<<<static_cast<unsigned>((S.tasks.size() + 127) / 128), 128, 0, main>>>(B);
+        LAUNCHED();
+    }
     if (S.grouped && !S.waves.empty()) {
         // the waves on their streams beside the camel tasks' evaluation
         const int ns = S.wave_streams;
@@ -894,6 +1121,11 @@ int enqueue_iteration(chili_ctx *ctx, bool adapt) {
         for (int j = 0; j < ns; ++j) {
             CK(cudaEventRecord(S.ph_events[j], S.ph_streams[j]));
             CK(cudaStreamWaitEvent(main, S.ph_events[j], 0));
+        }
+        if (S.has_retry) {
+            k_rt_end<<<static_cast<unsigned>(S.tasks.size()), kFoldThreads, 0, main>>>(B);
+            LAUNCHED();
+            return CHILI_OK;
         }
     } else {
     if (!S.ph.empty()) CK(cudaEventRecord(S.ph_events[kPhBranches], main));
@@ -929,6 +1161,12 @@ int enqueue_iteration(chili_ctx *ctx, bool adapt) {
             CK(cudaStreamWaitEvent(main, S.ph_events[br], 0));
         }
     }
+    return enqueue_final(ctx, adapt);
+}
+
+int enqueue_final(chili_ctx *ctx, bool adapt) {
+    BatchState &S = *ctx->batch;
+    BatchDev B = batch_dev(ctx);
     k_batch_finalize<<<static_cast<unsigned>(S.tasks.size()), kFoldThreads, 0, ctx->stream>>>(B, adapt ? 1 : 0);
     LAUNCHED();
     if (adapt && !S.jobs.empty()) {
@@ -980,17 +1218,19 @@ int autotune(chili_ctx *ctx) {
     return layout_units(ctx, bb, bp);
 }
 
-int capture(chili_ctx *ctx, bool adapt) {
-    BatchState &S = *ctx->batch;
-    if (S.graph) {
-        cudaGraphExecDestroy(S.graph);
-        S.graph = nullptr;
+void drop_graphs(BatchState &S) {
+    for (cudaGraphExec_t *g : {&S.graph, &S.graph_top, &S.graph_fin}) {
+        if (*g) cudaGraphExecDestroy(*g);
+        *g = nullptr;
     }
-    cudaGraph_t g = nullptr;
+}
+
+template <class Enqueue>
+int capture_one(chili_ctx *ctx, Enqueue enqueue, cudaGraphExec_t *out, unsigned long long *n_launches) {
     const unsigned long long launches = ctx->launches;  // replays are counted, not the capture
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    const int rc = enqueue_iteration(ctx, adapt);
-    S.graph_launches = ctx->launches - launches;
+    const int rc = enqueue();
+    *n_launches = ctx->launches - launches;
     ctx->launches = launches;
     cudaGraph_t captured = nullptr;
     const cudaError_t e = cudaStreamEndCapture(ctx->stream, &captured);
@@ -999,11 +1239,67 @@ int capture(chili_ctx *ctx, bool adapt) {
         return rc;
     }
     if (e != cudaSuccess) return fail(ctx, CHILI_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-    g = captured;
-    CK(cudaGraphInstantiate(&S.graph, g, 0));
-    cudaGraphDestroy(g);
+    const cudaError_t ei = cudaGraphInstantiate(out, captured, 0);
+    cudaGraphDestroy(captured);
+    if (ei != cudaSuccess) return fail(ctx, CHILI_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+    return CHILI_OK;
+}
+
+// The iteration's graphs: one, or with retry tasks three (the first round;
+// a further round; the final part).
+int capture(chili_ctx *ctx, bool adapt) {
+    BatchState &S = *ctx->batch;
+    drop_graphs(S);
+    if (int rc = capture_one(ctx, [&] { return enqueue_iteration(ctx, adapt); }, &S.graph, &S.graph_launches))
+        return rc;
+    if (S.has_retry) {
+        if (int rc = capture_one(ctx, [&] { return enqueue_retry_round(ctx); }, &S.graph_top, &S.top_launches))
+            return rc;
+        if (int rc = capture_one(ctx, [&] { return enqueue_final(ctx, adapt); }, &S.graph_fin, &S.fin_launches))
+            return rc;
+    }
     S.graph_adapt = adapt ? 1 : 0;
     return CHILI_OK;
+}
+
+int plan_waves(chili_ctx *ctx, const std::vector<PointProgram> &pps);
+
+// Rounds of the retry loop per iteration beyond the first, at most (and at
+// most the context's option max_rounds).
+constexpr int kMaxRetryRounds = 4096;
+
+// First-round draw of a retry task: ncalls, 1.2 times the points beyond
+// them that an iteration had to draw (rejected and NaN points) plus four
+// standard deviations of that count, and a margin of ncalls/32 and two
+// blocks for rejections that the iteration did not see.
+long long retry_draw(long long ncalls, double extra) {
+    const double d = static_cast<double>(ncalls) * (1.0 + 1.0 / 32) + 1.2 * extra + 4.0 * std::sqrt(extra) +
+                     2.0 * kFwdBlock;
+    return static_cast<long long>(std::min(d, static_cast<double>((1ll << 32) - 1)));
+}
+
+// Retry tasks whose iteration needed further rounds draw more in the first
+// round from now on (the plan grows only).  Re-plans the waves and drops the
+// graphs when a draw changed.
+int replan_draws(chili_ctx *ctx) {
+    BatchState &S = *ctx->batch;
+    std::vector<RetryState> R(S.tasks.size());
+    CK(cudaMemcpyAsync(R.data(), S.d_retry.p, sizeof(RetryState) * R.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    bool changed = false;
+    for (size_t k = 0; k < S.tasks.size(); ++k) {
+        BatchTask &T = S.tasks[k];
+        if (!T.retry || R[k].rounds <= 1) continue;
+        const long long d = retry_draw(T.ncalls, static_cast<double>(R[k].ctr0 - T.ncalls));
+        if (d > T.draw) {
+            T.draw = d;
+            changed = true;
+        }
+    }
+    if (!changed) return CHILI_OK;
+    drop_graphs(S);
+    if (int rc = plan_waves(ctx, S.pps_host)) return rc;
+    return layout_units(ctx, S.block, S.ppt);
 }
 
 // Grouped mode: the phased tasks cut into pieces of at most kPieceMax
@@ -1022,32 +1318,46 @@ int plan_waves(chili_ctx *ctx, const std::vector<PointProgram> &pps) {
     std::vector<int> order;
     for (size_t ti = 0; ti < S.tasks.size(); ++ti)
         if (S.tasks[ti].phased) order.push_back(static_cast<int>(ti));
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return S.tasks[a].ncalls > S.tasks[b].ncalls; });
-    std::vector<Piece> pcs;
-    for (int ti : order) {
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return S.tasks[a].draw > S.tasks[b].draw; });
+    // a task's pieces (of a round's draw), in counter order
+    auto task_pieces = [&](int ti) {
         const BatchTask &T = S.tasks[static_cast<size_t>(ti)];
-        for (long long p0 = 0; p0 < T.ncalls; p0 += piece_max) {
+        std::vector<Piece> v;
+        for (long long p0 = 0; p0 < T.draw; p0 += piece_max) {
             Piece P{};
             P.ti = ti;
             P.p0 = p0;
-            P.mm = std::min(piece_max, T.ncalls - p0);
+            P.mm = std::min(piece_max, T.draw - p0);
             P.ms = (P.mm + kFwdBlock - 1) / kFwdBlock * kFwdBlock;
             P.nb = static_cast<int32_t>(P.ms / kFwdBlock);
-            pcs.push_back(P);
+            v.push_back(P);
         }
-    }
-    // waves: first fit in that order
+        return v;
+    };
+    // waves: first fit in that order; the pieces of a retry task all in one
+    // wave, adjacent (its cut counts the accepted points of its earlier
+    // pieces), a wave grown to the task where the task is larger
     std::vector<std::vector<Piece>> waves;
     std::vector<long long> load;
-    for (const Piece &P : pcs) {
+    auto place = [&](const std::vector<Piece> &v, long long need) {
         size_t w = 0;
-        while (w < waves.size() && load[w] + P.ms > wave_max) ++w;
+        while (w < waves.size() && load[w] > 0 && load[w] + need > wave_max) ++w;
         if (w == waves.size()) {
             waves.emplace_back();
             load.push_back(0);
         }
-        waves[w].push_back(P);
-        load[w] += P.ms;
+        for (const Piece &P : v) waves[w].push_back(P);
+        load[w] += need;
+    };
+    for (int ti : order) {
+        const std::vector<Piece> v = task_pieces(ti);
+        if (S.tasks[static_cast<size_t>(ti)].retry) {
+            long long tot = 0;
+            for (const Piece &P : v) tot += P.ms;
+            place(v, tot);
+        } else {
+            for (const Piece &P : v) place({P}, P.ms);
+        }
     }
     // per piece: constants and buffer sizes
     auto sizes = [&](const Piece &P, const PointProgram &PP, size_t *out) {
@@ -1160,15 +1470,17 @@ int plan_waves(chili_ctx *ctx, const std::vector<PointProgram> &pps) {
     CK(cudaMemcpyAsync(S.d_prefix.p, S.prefix_host.data(), sizeof(long long) * S.prefix_host.size(),
                        cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));  // the host vectors are the copies' sources
-    for (int j = 0; j < ns; ++j) {
-        cudaStream_t st;
-        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-        S.ph_streams.push_back(st);
-    }
-    for (int k = 0; k <= ns; ++k) {
-        cudaEvent_t e;
-        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        S.ph_events.push_back(e);
+    if (S.ph_streams.empty()) {  // the first plan (later ones re-plan the retry tasks' draws)
+        for (int j = 0; j < ns; ++j) {
+            cudaStream_t st;
+            CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+            S.ph_streams.push_back(st);
+        }
+        for (int k = 0; k <= ns; ++k) {
+            cudaEvent_t e;
+            CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            S.ph_events.push_back(e);
+        }
     }
     return CHILI_OK;
 }
@@ -1178,7 +1490,9 @@ int plan_waves(chili_ctx *ctx, const std::vector<PointProgram> &pps) {
 void batch_release(chili_ctx *ctx) {
     if (!ctx || !ctx->batch) return;
     BatchState &S = *ctx->batch;
-    if (S.graph) cudaGraphExecDestroy(S.graph);
+    drop_graphs(S);
+    S.d_retry.release();
+    S.d_rflag.release();
     for (DevBuf *b : {&S.d_tasks, &S.d_umap, &S.d_pps, &S.d_progs, &S.d_descs, &S.d_grids, &S.d_grids_new, &S.d_hist,
                       &S.d_hints, &S.d_widths, &S.d_sorted,
                       &S.d_atrain, &S.d_alpha, &S.d_best, &S.d_mindiff, &S.d_cp, &S.d_part, &S.d_stats,
@@ -1214,6 +1528,7 @@ int chili_gpu_batch_set(chili_ctx *ctx, const chili_task *tasks, int ntasks) {
         T.kind = t.kind;
         T.bins = t.bins;
         T.ncalls = static_cast<long long>(t.ncalls);
+        T.draw = T.ncalls;
         T.grid_alpha = t.grid_alpha;
         T.beta = t.beta;
         T.min_alpha = t.min_alpha;
@@ -1328,6 +1643,21 @@ int chili_gpu_batch_set(chili_ctx *ctx, const chili_task *tasks, int ntasks) {
         const size_t T = static_cast<size_t>(std::max<long long>(S.ph_tile, kFwdBlock));
         const size_t nb = T / kFwdBlock;
         S.grouped = ctx->batch_grouped && S.ph_tile > 0;  // waves planned once the device tables exist
+        // the reference's retry loop: multichannel tasks weighted in the waves
+        if (ctx->batch_retry) {
+            for (auto &Tk : S.tasks) {
+                if (Tk.kind != CHILI_TASK_MULTICHANNEL) continue;
+                if (!Tk.phased || !S.grouped) {
+                    batch_release(ctx);
+                    return fail(ctx, CHILI_ERR_INVALID_ARG,
+                                "the retry loop (option batch_retry) runs in the grouped phased pass: options "
+                                "batch_grouped and batch_phased on, or batch_retry 0 for a fixed budget");
+                }
+                Tk.retry = 1;
+                Tk.draw = retry_draw(Tk.ncalls, 0.0);
+                S.has_retry = true;
+            }
+        }
         if (!S.grouped && S.ph_tile > 0) {
             S.ph.resize(kPhBranches);
             for (auto &b : S.ph) {
@@ -1415,6 +1745,10 @@ int chili_gpu_batch_set(chili_ctx *ctx, const chili_task *tasks, int ntasks) {
                        ctx->stream));
     CK(S.d_status.ensure(sizeof(int)));
     CK(cudaMemsetAsync(S.d_status.p, 0, sizeof(int), ctx->stream));
+    CK(S.d_retry.ensure(sizeof(RetryState) * S.tasks.size()));
+    CK(cudaMemsetAsync(S.d_retry.p, 0, sizeof(RetryState) * S.tasks.size(), ctx->stream));
+    CK(S.d_rflag.ensure(sizeof(int)));
+    CK(cudaMemsetAsync(S.d_rflag.p, 0, sizeof(int), ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     if (S.grouped)
         if (int rc = plan_waves(ctx, pps)) return rc;
@@ -1455,10 +1789,7 @@ int chili_gpu_batch_iterate(chili_ctx *ctx, int iterations, uint64_t seed, int a
     if (S.nslots_alloc < iterations) {
         CK(S.d_stats.ensure(sizeof(double) * 6 * static_cast<size_t>(iterations) * nt));
         S.nslots_alloc = iterations;
-        if (S.graph) {
-            cudaGraphExecDestroy(S.graph);
-            S.graph = nullptr;
-        }
+        drop_graphs(S);
     }
     if (!S.graph || S.graph_adapt != (adapt ? 1 : 0))
         if (int rc = capture(ctx, adapt != 0)) return rc;
@@ -1469,14 +1800,56 @@ int chili_gpu_batch_iterate(chili_ctx *ctx, int iterations, uint64_t seed, int a
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     CK(cudaEventRecord(e0, ctx->stream));
-    for (int it = 0; it < iterations; ++it) CK(cudaGraphLaunch(S.graph, ctx->stream));
+    S.retry_rounds = 0;
+    for (int it = 0; it < iterations; ++it) {
+        if (!S.graph)  // dropped by a re-plan of the retry tasks' draws
+            if (int rc = capture(ctx, adapt != 0)) return rc;
+        CK(cudaGraphLaunch(S.graph, ctx->stream));
+        ctx->launches += S.graph_launches;
+        if (!S.has_retry) continue;
+        // further rounds while a task is short of ncalls (one flag read per round)
+        int flag = 0, rounds = 0;
+        CK(cudaMemcpyAsync(&flag, S.d_rflag.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        const long long max_rounds = std::min<long long>(kMaxRetryRounds, ctx->max_rounds);
+        while (flag == 1 && rounds < max_rounds) {
+            CK(cudaGraphLaunch(S.graph_top, ctx->stream));
+            ctx->launches += S.top_launches;
+            ++rounds;
+            CK(cudaMemcpyAsync(&flag, S.d_rflag.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+        }
+        if (flag != 0) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            // the first task still short of ncalls, for the message
+            std::vector<RetryState> R(S.tasks.size());
+            CK(cudaMemcpy(R.data(), S.d_retry.p, sizeof(RetryState) * R.size(), cudaMemcpyDeviceToHost));
+            std::string who;
+            for (size_t k = 0; k < R.size() && who.empty(); ++k)
+                if (S.tasks[k].retry && R[k].need > 0)
+                    who = ": task " + std::to_string(k) + " still needs " + std::to_string(R[k].need) + " of " +
+                          std::to_string(S.tasks[k].ncalls) + " after " + std::to_string(R[k].ctr0) +
+                          " points counted in " + std::to_string(R[k].rounds) + " rounds (" +
+                          std::to_string(R[k].nan_total) + " NaN values)";
+            // the reference's loop never ends on a task whose every point is
+            // rejected or NaN; this one gives up like the single-integrand path
+            return fail(ctx, flag == 2 ? CHILI_ERR_LIMIT : CHILI_ERR_TIMEOUT,
+                        std::string(flag == 2 ? "retry loop: a task's counters ran out (2^32 per iteration)"
+                                              : "retry loop: too many rounds") + who);
+        }
+        CK(cudaGraphLaunch(S.graph_fin, ctx->stream));
+        ctx->launches += S.fin_launches;
+        S.retry_rounds += static_cast<unsigned long long>(rounds);
+        if (rounds > 0)
+            if (int rc = replan_draws(ctx)) return rc;
+    }
     CK(cudaEventRecord(e1, ctx->stream));
     CK(cudaEventSynchronize(e1));
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    ctx->launches += static_cast<unsigned long long>(iterations) * S.graph_launches;
     S.last_ms = ms / iterations;
     if (stats) {
         std::vector<double> all(6 * static_cast<size_t>(S.nslots_alloc) * nt);
@@ -1496,6 +1869,7 @@ int chili_gpu_batch_iterate(chili_ctx *ctx, int iterations, uint64_t seed, int a
         info->ms_per_iteration = S.last_ms;
         info->units = static_cast<uint64_t>(S.nunits);
         info->points = static_cast<uint64_t>(S.total_points);
+        info->retry_rounds = S.retry_rounds;
     }
     return CHILI_OK;
 }

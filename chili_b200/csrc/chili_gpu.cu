@@ -468,6 +468,10 @@ int chili_gpu_set_option(chili_ctx *ctx, const char *name, int64_t value) {
         ctx->defer_train = value != 0;
         return CHILI_OK;
     }
+    if (std::strcmp(name, "batch_retry") == 0) {
+        ctx->batch_retry = value != 0;
+        return CHILI_OK;
+    }
     if (std::strcmp(name, "batch_grouped") == 0) {
         ctx->batch_grouped = value != 0;
         return CHILI_OK;

@@ -139,6 +139,7 @@ struct chili_ctx {
     bool defer_train = false;  // option "defer_train": iterations collect training data, Train is the caller's
     bool batch_phased = true;  // option "batch_phased": batched multichannel tasks by the phased weight pass
     bool batch_grouped = true;  // option "batch_grouped": the phased tasks in waves, one launch per step and wave
+    bool batch_retry = false;   // option "batch_retry": batched multichannel tasks keep the reference's retry loop
     long long batch_wave = 1ll << 24;  // option "batch_wave_points": points per wave of the grouped mode
     long long batch_ch_pts = 2048;  // option "batch_channel_points": points per block of the grouped channel step
     long long upload_slice = 1ll << 19;  // option "upload_slice": largest host-uniform slice (rows)

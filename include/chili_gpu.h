@@ -210,6 +210,16 @@ uint64_t chili_gpu_launch_count(const chili_ctx *ctx);
  * channel set has a shared-entry program with the phased weight pass (task
  * chains as parallel graph branches); 0 evaluates every point in one thread
  * of the persistent batch kernel.  Read by chili_gpu_batch_set.
+ * "batch_retry": 1 keeps the reference's retry loop for batched multichannel
+ * tasks (MultiChannel.hh:214-248: points are drawn until ncalls of them pass
+ * PreProcess with a finite value, the others count as zero-valued calls), in
+ * rounds; an iteration that still lacks points after max_rounds further
+ * rounds fails with CHILI_ERR_TIMEOUT (the reference's loop never ends on a
+ * task whose values are all NaN).  It needs the grouped phased pass
+ * (batch_grouped and batch_phased on; chili_gpu_batch_set fails otherwise).
+ * 0 (default): a fixed budget of ncalls drawn points per task and iteration,
+ * rejected points and NaN values counting as zero-valued calls.  Read by
+ * chili_gpu_batch_set.
  * "channel_tables": 1 (default) stages each channel's edge, hint and width
  * tables in shared memory for the bin searches of the phased weight pass
  * (tables up to 112 KB), 0 reads them from global memory; the same numbers.
@@ -607,7 +617,9 @@ typedef struct {
     uint32_t points_per_thread; /* points per thread per work unit             */
     double ms_per_iteration;    /* device time per iteration of the last call  */
     uint64_t units;             /* work units per iteration                    */
-    uint64_t points;            /* points per iteration, all tasks             */
+    uint64_t points;            /* calls per iteration, all tasks (ncalls)     */
+    uint64_t retry_rounds;      /* retry rounds beyond each iteration's first,
+                                   summed over the last call's iterations      */
 } chili_batch_info;
 
 /* Replace the context's batch with ntasks tasks (uniform grids, equal channel

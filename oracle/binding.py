@@ -291,7 +291,8 @@ class MultiChannel:
 
     def set_fixed_budget(self, on=True):
         """Every drawn point counts as a call, no retries: the semantics of
-        the CUDA library's batched integrands (the C port only)."""
+        the CUDA library's batched integrands with option batch_retry 0 (the C
+        port only)."""
         self.oracle().ref_mc_set_fixed_budget(self.h, 1 if on else 0)
 
     def train(self, hist, atrain):

@@ -54,7 +54,7 @@ int main(void) {
   O(chili_multichannel_params, should_optimize) O(chili_multichannel_params, grid_alpha)
   O(chili_cuts, etamax) O(chili_mc_iter_info, weight_max) O(chili_mc_iter_info, points_weighted) O(chili_mc_iter_info, chunks)
   S(chili_task) S(chili_batch_info) O(chili_task, ncalls) O(chili_task, params) O(chili_task, descs)
-  O(chili_task, sqrts) O(chili_task, n_ext) O(chili_task, pre_cuts) O(chili_batch_info, points)
+  O(chili_task, sqrts) O(chili_task, n_ext) O(chili_task, pre_cuts) O(chili_batch_info, points) O(chili_batch_info, retry_rounds)
   return 0;
 }''')
     exe = tmp_path / "layout"
@@ -79,6 +79,7 @@ int main(void) {
     for f in ("ncalls", "params", "descs", "sqrts", "n_ext", "pre_cuts"):
         assert int(got["chili_task." + f]) == getattr(abi.Task, f).offset, f
     assert int(got["chili_batch_info.points"]) == abi.BatchInfo.points.offset
+    assert int(got["chili_batch_info.retry_rounds"]) == abi.BatchInfo.retry_rounds.offset
 
 
 def test_header_limits_match_the_mirror():

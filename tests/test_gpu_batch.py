@@ -5,8 +5,10 @@ counter-based uniforms (task k: Philox key seed + k, counters
 
 Camel tasks follow Vegas::operator() + AdaptiveMap::Adapt
 (Vegas.cc:18-52); multichannel tasks follow MultiChannel::operator() +
-Train (MultiChannel.hh:182-251) with a fixed budget of ncalls drawn points
-(the oracle's set_fixed_budget).  Bars: counts and finite counts exact,
+Train (MultiChannel.hh:182-251) with its retry loop (points drawn until
+ncalls of them pass PreProcess with a finite value; option batch_retry 1),
+or with a fixed budget of ncalls drawn points (option batch_retry 0, the
+default; the oracle's set_fixed_budget).  Bars: counts and finite counts exact,
 sums within 1e-11 relative on the first iteration (CUDA's and the C
 library's exp and log differ by an ulp), 1e-9 on later ones (the
 histograms are summed with atomics, so later iterations run on grids that
@@ -54,19 +56,26 @@ def oracle_camel(t, seed, iterations):
     return out
 
 
-def oracle_mc(t, seed, iterations):
+def oracle_mc(t, seed, iterations, retry=True):
+    """The oracle on the task's uniforms (Philox key seed, counters
+    (iteration << 32) + point): with the retry loop it consumes rows until
+    ncalls points are accepted, with a fixed budget exactly ncalls rows."""
     cs = t["channels"]
     params = workloads.mc_params(t["ncalls"], beta=t["beta"], min_alpha=t["min_alpha"],
                                  grid_alpha=t["grid_alpha"])
     O = port.MultiChannel(cs, t["bins"], params, t["fkind"], t["params"], pre=abi.CHILI_PRE_FINITE)
     if t["pre"] == abi.CHILI_PRE_CUTS:
         O.set_cuts(*t["pre_cuts"])
-    O.set_fixed_budget(True)
+    O.set_fixed_budget(not retry)
+    rows = 16 * t["ncalls"] + 4096 if retry else t["ncalls"]
     out = []
     for it in range(iterations):
-        u = port.philox_uniforms(seed, it << 32, t["ncalls"], cs.ndims + 1)
+        u = port.philox_uniforms(seed, it << 32, rows, cs.ndims + 1)
         st, info = O.iterate(u)
-        assert info.points_tried == t["ncalls"]
+        if retry:
+            assert info.points_tried >= t["ncalls"] and st.n == info.points_tried
+        else:
+            assert info.points_tried == t["ncalls"]
         out.append((st.as_tuple(), O.get_grids(), O.get_alpha()[0]))
     return out
 
@@ -83,55 +92,81 @@ def check_task(k, st_gpu, edges, alpha, want, it):
         assert np.max(rel(alpha, a_o)) < 1e3 * tol, (k, it)
 
 
-def run_and_check(ctx, tasks, seed, iterations):
+def run_and_check(ctx, tasks, seed, iterations, retry=True):
     ctx.batch_set(tasks)
-    want = [oracle_camel(t, seed + k, iterations) if t["kind"] == "camel" else oracle_mc(t, seed + k, iterations)
-            for k, t in enumerate(tasks)]
+    want = [oracle_camel(t, seed + k, iterations) if t["kind"] == "camel" else
+            oracle_mc(t, seed + k, iterations, retry=retry) for k, t in enumerate(tasks)]
     stats = []
     grids = []
+    infos = []
     for it in range(iterations):
         st, info = ctx.batch_iterate(1, seed=seed, adapt=True)
         stats.append(st[0])
+        infos.append((info.retry_rounds, info.ms_per_iteration))
         grids.append([ctx.batch_get_grid(k) for k in range(len(tasks))])
     for it in range(iterations):
         for k in range(len(tasks)):
             e, a = grids[it][k]
             check_task(k, stats[it][k], e, a, want[k][it], it)
-    return info
+    return info, infos
 
 
 def test_camel_tasks_match_the_oracle(ctx_factory):
     rng = np.random.default_rng(3)
     tasks = [camel_task(rng, 2, 3000, 20), camel_task(rng, 5, 70001, 50), camel_task(rng, 9, 12345, 30),
              camel_task(rng, 12, 1, 40)]
-    info = run_and_check(ctx_factory(), tasks, seed=5, iterations=3)
+    info, _ = run_and_check(ctx_factory(), tasks, seed=5, iterations=3)
     assert info.points == sum(t["ncalls"] for t in tasks)
     assert info.block in (128, 256) and info.points_per_thread in (1, 2, 4)
 
 
-@pytest.mark.parametrize("mode", ["grouped", "grouped_small_waves", "task_chains", "one_kernel"])
+@pytest.mark.parametrize("mode", ["grouped", "grouped_small_waves", "grouped_fixed", "grouped_fixed_small_waves",
+                                  "task_chains", "one_kernel"])
 def test_multichannel_tasks_match_the_oracle(ctx_factory, mode):
     """Every weight pass of the batched multichannel tasks: the phased pass
     in waves of pieces, one launch per step and wave (the default; with
     waves of 2^16 points the tasks are cut into several pieces and the
     pieces spread over several waves), the phased pass as one chain of
     launches per task tile (option batch_grouped 0), and every point in one
-    thread of the persistent kernel (option batch_phased 0)."""
+    thread of the persistent kernel (option batch_phased 0).  The grouped
+    modes keep the reference's retry loop (the default) or run a fixed budget
+    (option batch_retry 0, which the other two modes need).  The 2->4 task
+    with cuts rejects most points: its first iteration needs further rounds
+    (the first draws ncalls points and a small margin), after which its draws
+    are re-planned and a later iteration needs few if any."""
     # the 2->4 task spans two phased tiles (2^18 points each)
     tasks = [mc_task(2, 500.0, 20000, 20), mc_task(3, 1500.0, 5000, 30), mc_task(4, 1000.0, 265000, 25, cuts=True),
              mc_task(5, 800.0, 20000, 15)]
+    retry = mode in ("grouped", "grouped_small_waves")
     ctx = ctx_factory()
-    if mode == "grouped_small_waves":
+    if mode.endswith("small_waves"):
+        # waves on one stream: each reuses the buffers of the one before
         ctx.set_option("batch_wave_points", 1 << 16)
+        ctx.set_option("batch_wave_streams", 1)
     ctx.set_option("batch_grouped", 0 if mode == "task_chains" else 1)
     ctx.set_option("batch_phased", 0 if mode == "one_kernel" else 1)
-    run_and_check(ctx, tasks, seed=11, iterations=2)
+    ctx.set_option("batch_retry", 1 if retry else 0)
+    _, infos = run_and_check(ctx, tasks, seed=11, iterations=2, retry=retry)
+    assert (infos[0][0] > 2) == retry, infos
     l0 = ctx.launches
-    ctx.batch_iterate(1, seed=11, adapt=True)
+    _, info = ctx.batch_iterate(1, seed=11, adapt=True)
     launches = ctx.launches - l0
     if mode.startswith("grouped"):
-        # a handful of launches per wave, not a chain per task tile
-        assert launches < (30 if mode == "grouped" else 200), launches
+        # a handful of launches per wave and round, not a chain per task tile
+        assert info.retry_rounds <= 2, info.retry_rounds
+        per_round = 30 if mode in ("grouped", "grouped_fixed") else 200
+        assert launches < per_round * (1 + info.retry_rounds), launches
+
+
+def test_retry_loop_needs_the_grouped_phased_pass(ctx_factory):
+    from chili_b200.gpu import ChiliError
+    ctx = ctx_factory()
+    ctx.set_option("batch_retry", 1)
+    ctx.set_option("batch_grouped", 0)
+    with pytest.raises(ChiliError):
+        ctx.batch_set([mc_task(2, 500.0, 1000, 20)])
+    ctx.set_option("batch_retry", 0)
+    ctx.batch_set([mc_task(2, 500.0, 1000, 20)])
 
 
 def test_mixed_batch_matches_the_oracle(ctx_factory):
@@ -142,6 +177,7 @@ def test_mixed_batch_matches_the_oracle(ctx_factory):
     tasks = [camel_task(rng, 3, 40000, 30), mc_task(2, 300.0, 10000, 20), camel_task(rng, 7, 777, 25),
              mc_task(5, 800.0, 4000, 15)]
     ctx = ctx_factory()
+    ctx.set_option("batch_retry", 1)
     ctx.batch_set(tasks)
     st, info = ctx.batch_iterate(3, seed=21, adapt=True)
     want = [oracle_camel(t, 21 + k, 3) if t["kind"] == "camel" else oracle_mc(t, 21 + k, 3)
