@@ -838,6 +838,7 @@ struct BatchState {
     bool grouped = false;
     struct WaveHost {
         int first = 0, n = 0;                        // pieces [first, first + n)
+        int sidx = 0;                                // stream (and arena) of the wave
         long long prefix_off = 0;                    // into d_prefix
         std::vector<long long> blocks;               // per step: total blocks
         std::vector<std::array<int, 4>> dgroups;     // (dims, k0, k1, bins): pieces [k0, k1) of one dimension, their most bins
@@ -852,12 +853,16 @@ struct BatchState {
     bool tuned = false;
     cudaGraphExec_t graph = nullptr;
     unsigned long long graph_launches = 0;  // kernels of one replay
-    // retry tasks (option batch_retry): the further-round and final graphs,
-    // per-task loop state, the round flag
+    // retry tasks (option batch_retry): the final graph, per-task loop state,
+    // the round flag; the waves of a further round (the pieces of the tasks
+    // still short of ncalls) and their device copies
     bool has_retry = false;
-    cudaGraphExec_t graph_top = nullptr, graph_fin = nullptr;
-    unsigned long long top_launches = 0, fin_launches = 0;
-    DevBuf d_retry, d_rflag;
+    cudaGraphExec_t graph_fin = nullptr;
+    unsigned long long fin_launches = 0;
+    DevBuf d_retry, d_rflag, d_top_pieces, d_top_prefix;
+    std::vector<WaveHost> top_waves;
+    std::vector<Piece> top_pieces;
+    std::vector<long long> top_prefix;
     unsigned long long retry_rounds = 0;  // further rounds run by the last batch_iterate call
     int graph_adapt = -1;
     double last_ms = 0;
@@ -1002,14 +1007,15 @@ int enqueue_phased_task(chili_ctx *ctx, const BatchDev &B, int ti, BatchState::P
 
 // The phased tasks' waves, one after another on ctx->stream: one launch per
 // step and wave.
-int enqueue_waves(chili_ctx *ctx, const BatchDev &B) {
+int enqueue_waves(chili_ctx *ctx, const BatchDev &B, const std::vector<BatchState::WaveHost> &waves,
+                  const Piece *d_pieces, const long long *d_prefix, const std::vector<long long> &prefix_host) {
     BatchState &S = *ctx->batch;
     const cudaStream_t caller = ctx->stream;
-    for (size_t wi = 0; wi < S.waves.size(); ++wi) {
-        const auto &w = S.waves[wi];
-        ctx->stream = S.ph_streams[wi % S.wave_streams];  // the wave's arena belongs to this stream
-        const WaveDev W{S.d_pieces.as<Piece>() + w.first, w.n, S.d_prefix.as<long long>() + w.prefix_off, S.ch_pts};
-        const long long *pre = S.prefix_host.data() + w.prefix_off;
+    for (size_t wi = 0; wi < waves.size(); ++wi) {
+        const auto &w = waves[wi];
+        ctx->stream = S.ph_streams[static_cast<size_t>(w.sidx)];  // the wave's arena belongs to this stream
+        const WaveDev W{d_pieces + w.first, w.n, d_prefix + w.prefix_off, S.ch_pts};
+        const long long *pre = prefix_host.data() + w.prefix_off;
         auto blocks = [&](int step) { return static_cast<unsigned>(w.blocks[static_cast<size_t>(step)]); };
         k_g_forward<<<blocks(GS_FWD), kFwdBlock, 0, ctx->stream>>>(B, W, 0, w.n, 0);
         LAUNCHED();
@@ -1068,18 +1074,67 @@ int enqueue_waves(chili_ctx *ctx, const BatchDev &B) {
     return CHILI_OK;
 }
 
-// A retry round after the first (captured into its own graph): the waves
-// again for the tasks still short of ncalls (the others draw nothing), then
-// the round's bookkeeping.
-int enqueue_retry_round(chili_ctx *ctx) {
+// A retry round after the first, launched directly: the waves cut down to
+// the pieces of the tasks still short of ncalls (read back from the device),
+// each kept on its wave's stream and buffers, then the round's bookkeeping.
+int run_retry_round(chili_ctx *ctx) {
     BatchState &S = *ctx->batch;
     BatchDev B = batch_dev(ctx);
     const cudaStream_t main = ctx->stream;
     const int ns = S.wave_streams;
+    std::vector<RetryState> R(S.tasks.size());
+    CK(cudaMemcpyAsync(R.data(), S.d_retry.p, sizeof(RetryState) * R.size(), cudaMemcpyDeviceToHost, main));
+    CK(cudaStreamSynchronize(main));
+    // the filtered waves: a task's pieces stay together and in order
+    S.top_waves.clear();
+    S.top_pieces.clear();
+    S.top_prefix.clear();
+    for (const auto &w : S.waves) {
+        std::vector<int> keep;
+        for (int k = 0; k < w.n; ++k) {
+            const int ti = S.pieces[static_cast<size_t>(w.first + k)].ti;
+            if (S.tasks[static_cast<size_t>(ti)].retry && R[static_cast<size_t>(ti)].need > 0) keep.push_back(k);
+        }
+        if (keep.empty()) continue;
+        BatchState::WaveHost fw;
+        fw.sidx = w.sidx;
+        fw.first = static_cast<int>(S.top_pieces.size());
+        fw.n = static_cast<int>(keep.size());
+        fw.prefix_off = static_cast<long long>(S.top_prefix.size());
+        for (int st = 0; st < kGroupSteps; ++st) {
+            const long long *po = S.prefix_host.data() + w.prefix_off + static_cast<size_t>(st) * (w.n + 1);
+            long long acc = 0;
+            S.top_prefix.push_back(0);
+            for (int k : keep) {
+                acc += po[k + 1] - po[k];
+                S.top_prefix.push_back(acc);
+            }
+            fw.blocks.push_back(acc);
+        }
+        for (size_t j = 0; j < keep.size(); ++j) {
+            const Piece &P = S.pieces[static_cast<size_t>(w.first + keep[j])];
+            S.top_pieces.push_back(P);
+            const int kj = static_cast<int>(j);
+            if (fw.dgroups.empty() || fw.dgroups.back()[0] != P.dims) {
+                fw.dgroups.push_back({P.dims, kj, kj + 1, P.bins});
+            } else {
+                fw.dgroups.back()[2] = kj + 1;
+                fw.dgroups.back()[3] = std::max(fw.dgroups.back()[3], P.bins);
+            }
+        }
+        S.top_waves.push_back(fw);
+    }
+    CK(S.d_top_pieces.ensure(sizeof(Piece) * std::max<size_t>(1, S.top_pieces.size())));
+    CK(S.d_top_prefix.ensure(sizeof(long long) * std::max<size_t>(1, S.top_prefix.size())));
+    CK(cudaMemcpyAsync(S.d_top_pieces.p, S.top_pieces.data(), sizeof(Piece) * S.top_pieces.size(),
+                       cudaMemcpyHostToDevice, main));
+    CK(cudaMemcpyAsync(S.d_top_prefix.p, S.top_prefix.data(), sizeof(long long) * S.top_prefix.size(),
+                       cudaMemcpyHostToDevice, main));
     CK(cudaMemsetAsync(S.d_rflag.p, 0, sizeof(int), main));
     CK(cudaEventRecord(S.ph_events[ns], main));
     for (int j = 0; j < ns; ++j) CK(cudaStreamWaitEvent(S.ph_streams[j], S.ph_events[ns], 0));
-    const int rc = enqueue_waves(ctx, B);
+    const int rc = enqueue_waves(ctx, B, S.top_waves, S.d_top_pieces.as<Piece>(), S.d_top_prefix.as<long long>(),
+                                 S.top_prefix);
     ctx->stream = main;
     if (rc) return rc;
     for (int j = 0; j < ns; ++j) {
@@ -1115,7 +1170,7 @@ int enqueue_iteration(chili_ctx *ctx, bool adapt) {
         for (int j = 0; j < ns; ++j) CK(cudaStreamWaitEvent(S.ph_streams[j], S.ph_events[ns], 0));
         k_batch_eval<<<S.grid_blocks, S.block, 0, ctx->stream>>>(B);
         LAUNCHED();
-        const int rc = enqueue_waves(ctx, B);
+        const int rc = enqueue_waves(ctx, B, S.waves, S.d_pieces.as<Piece>(), S.d_prefix.as<long long>(), S.prefix_host);
         ctx->stream = main;
         if (rc) return rc;
         for (int j = 0; j < ns; ++j) {
@@ -1219,7 +1274,7 @@ int autotune(chili_ctx *ctx) {
 }
 
 void drop_graphs(BatchState &S) {
-    for (cudaGraphExec_t *g : {&S.graph, &S.graph_top, &S.graph_fin}) {
+    for (cudaGraphExec_t *g : {&S.graph, &S.graph_fin}) {
         if (*g) cudaGraphExecDestroy(*g);
         *g = nullptr;
     }
@@ -1245,19 +1300,16 @@ int capture_one(chili_ctx *ctx, Enqueue enqueue, cudaGraphExec_t *out, unsigned 
     return CHILI_OK;
 }
 
-// The iteration's graphs: one, or with retry tasks three (the first round;
-// a further round; the final part).
+// The iteration's graphs: one, or with retry tasks two (the first round;
+// the final part; further rounds are launched directly between them).
 int capture(chili_ctx *ctx, bool adapt) {
     BatchState &S = *ctx->batch;
     drop_graphs(S);
     if (int rc = capture_one(ctx, [&] { return enqueue_iteration(ctx, adapt); }, &S.graph, &S.graph_launches))
         return rc;
-    if (S.has_retry) {
-        if (int rc = capture_one(ctx, [&] { return enqueue_retry_round(ctx); }, &S.graph_top, &S.top_launches))
-            return rc;
+    if (S.has_retry)
         if (int rc = capture_one(ctx, [&] { return enqueue_final(ctx, adapt); }, &S.graph_fin, &S.fin_launches))
             return rc;
-    }
     S.graph_adapt = adapt ? 1 : 0;
     return CHILI_OK;
 }
@@ -1394,6 +1446,7 @@ int plan_waves(chili_ctx *ctx, const std::vector<PointProgram> &pps) {
             return S.tasks[static_cast<size_t>(a.ti)].dims < S.tasks[static_cast<size_t>(b.ti)].dims;
         });
         BatchState::WaveHost wh;
+        wh.sidx = static_cast<int>(wi % ns);
         wh.first = static_cast<int>(S.pieces.size());
         wh.n = static_cast<int>(w.size());
         wh.prefix_off = static_cast<long long>(S.prefix_host.size());
@@ -1493,6 +1546,8 @@ void batch_release(chili_ctx *ctx) {
     drop_graphs(S);
     S.d_retry.release();
     S.d_rflag.release();
+    S.d_top_pieces.release();
+    S.d_top_prefix.release();
     for (DevBuf *b : {&S.d_tasks, &S.d_umap, &S.d_pps, &S.d_progs, &S.d_descs, &S.d_grids, &S.d_grids_new, &S.d_hist,
                       &S.d_hints, &S.d_widths, &S.d_sorted,
                       &S.d_atrain, &S.d_alpha, &S.d_best, &S.d_mindiff, &S.d_cp, &S.d_part, &S.d_stats,
@@ -1813,8 +1868,11 @@ int chili_gpu_batch_iterate(chili_ctx *ctx, int iterations, uint64_t seed, int a
         CK(cudaStreamSynchronize(ctx->stream));
         const long long max_rounds = std::min<long long>(kMaxRetryRounds, ctx->max_rounds);
         while (flag == 1 && rounds < max_rounds) {
-            CK(cudaGraphLaunch(S.graph_top, ctx->stream));
-            ctx->launches += S.top_launches;
+            if (int rc = run_retry_round(ctx)) {
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                return rc;
+            }
             ++rounds;
             CK(cudaMemcpyAsync(&flag, S.d_rflag.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
             CK(cudaStreamSynchronize(ctx->stream));
