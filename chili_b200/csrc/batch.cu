@@ -1316,6 +1316,16 @@ int capture(chili_ctx *ctx, bool adapt) {
 
 int plan_waves(chili_ctx *ctx, const std::vector<PointProgram> &pps);
 
+// Two CUDA events released with their owner (batch_iterate's timing events,
+// on its error returns too).
+struct EventPair {
+    cudaEvent_t a = nullptr, b = nullptr;
+    ~EventPair() {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+};
+
 // Rounds of the retry loop per iteration beyond the first, at most (and at
 // most the context's option max_rounds).
 constexpr int kMaxRetryRounds = 4096;
@@ -1851,10 +1861,10 @@ int chili_gpu_batch_iterate(chili_ctx *ctx, int iterations, uint64_t seed, int a
     unsigned long long iter0 = 0;
     CK(cudaMemcpyAsync(&iter0, S.d_counters.as<unsigned long long>() + 1, sizeof(iter0), cudaMemcpyDeviceToHost,
                        ctx->stream));
-    cudaEvent_t e0, e1;
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventCreate(&e1));
-    CK(cudaEventRecord(e0, ctx->stream));
+    EventPair ev;  // destroyed on every return
+    CK(cudaEventCreate(&ev.a));
+    CK(cudaEventCreate(&ev.b));
+    CK(cudaEventRecord(ev.a, ctx->stream));
     S.retry_rounds = 0;
     for (int it = 0; it < iterations; ++it) {
         if (!S.graph)  // dropped by a re-plan of the retry tasks' draws
@@ -1868,18 +1878,12 @@ int chili_gpu_batch_iterate(chili_ctx *ctx, int iterations, uint64_t seed, int a
         CK(cudaStreamSynchronize(ctx->stream));
         const long long max_rounds = std::min<long long>(kMaxRetryRounds, ctx->max_rounds);
         while (flag == 1 && rounds < max_rounds) {
-            if (int rc = run_retry_round(ctx)) {
-                cudaEventDestroy(e0);
-                cudaEventDestroy(e1);
-                return rc;
-            }
+            if (int rc = run_retry_round(ctx)) return rc;
             ++rounds;
             CK(cudaMemcpyAsync(&flag, S.d_rflag.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
             CK(cudaStreamSynchronize(ctx->stream));
         }
         if (flag != 0) {
-            cudaEventDestroy(e0);
-            cudaEventDestroy(e1);
             // the first task still short of ncalls, for the message
             std::vector<RetryState> R(S.tasks.size());
             CK(cudaMemcpy(R.data(), S.d_retry.p, sizeof(RetryState) * R.size(), cudaMemcpyDeviceToHost));
@@ -1902,12 +1906,10 @@ int chili_gpu_batch_iterate(chili_ctx *ctx, int iterations, uint64_t seed, int a
         if (rounds > 0)
             if (int rc = replan_draws(ctx)) return rc;
     }
-    CK(cudaEventRecord(e1, ctx->stream));
-    CK(cudaEventSynchronize(e1));
+    CK(cudaEventRecord(ev.b, ctx->stream));
+    CK(cudaEventSynchronize(ev.b));
     float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    cudaEventElapsedTime(&ms, ev.a, ev.b);
     S.last_ms = ms / iterations;
     if (stats) {
         std::vector<double> all(6 * static_cast<size_t>(S.nslots_alloc) * nt);
