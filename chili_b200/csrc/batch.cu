@@ -26,8 +26,10 @@
 // of its partials (deterministic), then the channel-weight update and a
 // batched grid adaptation over every (task, channel, dimension). The
 // iteration (resets, evaluation, folds, adaptation, iteration counter) is
-// captured once in a CUDA graph and replayed; block size and points per
-// thread are chosen by timing the candidates on the first call.
+// captured once in a CUDA graph and replayed (with the retry loop: the first
+// round and the final part as two graphs, further rounds launched directly
+// between them); block size and points per thread are chosen by timing the
+// candidates on the first call.
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
