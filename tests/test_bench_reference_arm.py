@@ -31,7 +31,7 @@ def reference_line(*extra):
 
 
 @needs_ref
-@pytest.mark.parametrize("workload", ["multichannel", "vegas", "batched"])
+@pytest.mark.parametrize("workload", ["multichannel", "vegas", "batched", "large"])
 def test_reference_arm_prints_the_contract_line(workload):
     d = reference_line(*(() if workload == "multichannel" else ("--workload", workload)))
     assert d["impl"] == "reference"
